@@ -1,0 +1,25 @@
+"""galsim_b200: GalSim's FFT drawing path on NVIDIA B200 (sm_100a).
+
+A drop-in for ``GSObject.drawImage(method='fft')`` and ``drawKImage`` on
+Convolve / Sum / Transform trees of Gaussian, Exponential, Sersic, Moffat, Kolmogorov, Airy
+and Box / Pixel.  The host code here mirrors the reference's Python API; every numerical
+step of drawing (FP64 sizing and Sersic tables, k-space evaluation, Hermitian wrap, inverse
+FFT, crop and flux sum) runs in the hand-written CUDA kernels of libgsb.so, called through
+the C ABI declared in include/gsb.h.  There is no CPU fallback.
+"""
+from .errors import *
+from .gsparams import GSParams
+from .position import Position, PositionD, PositionI, _PositionD, _PositionI
+from .bounds import Bounds, BoundsD, BoundsI, _BoundsI
+from .angle import Angle, AngleUnit, _Angle, radians, degrees, hours, arcmin, arcsec
+from .shear import Shear, _Shear
+from .wcs import BaseWCS, PixelScale
+from .image import Image, _Image, ImageF, ImageD, ImageI, ImageS, ImageCF, ImageCD
+from .gsobject import GSObject
+from .profiles import Gaussian, Exponential, Sersic, DeVaucouleurs, Moffat, Kolmogorov, Airy
+from .box import Box, Pixel
+from .compound import Convolve, Convolution, Add, Sum, Transform, Transformation, _Transform
+from .batch import draw_batch, StampBatch
+from ._lib import set_device
+
+__version__ = '0.1.0'

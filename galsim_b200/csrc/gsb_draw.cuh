@@ -1,0 +1,341 @@
+// Fused FFT drawing kernels.
+//
+// draw_fused_kernel<T, N, W_IN_SMEM>: one CTA draws one stamp at a time (persistent loop over
+// the stamps of an FFT-size bucket):
+//   1. column phase: each warp takes columns kx = 0..N/2 of the wrapped k-image; every lane
+//      builds the wrapped value of its rows by summing the program over all aliases
+//      (kx + a N, ky + b N) inside the Nk x Nk evaluation grid -- the Hermitian wrap of
+//      wrapImage(hermx=True) (src/Image.cpp:578-727) done as a gather -- then the warp
+//      inverse-transforms the column (length N) and stores it into W (shared memory, or a
+//      per-CTA global slab when it does not fit);
+//   2. row phase: each warp packs two needed image rows as one complex row
+//      (row1 + i row2, each Hermitian-extended in kx), inverse-transforms it and writes the
+//      pixels that fall inside the stamp, scaled by 1/N^2, with the compensated flux sum.
+// This is drawFFT (gsobject.py:2014-2045) = drawFFT_makeKImage + _drawKImage + wrap +
+// irfft(shift_in, shift_out) (src/Image.cpp:815-912) + drawFFT_finish, with no k-image in
+// HBM.  The output pixel (px, py) is the inverse DFT at (px mod N, py mod N), which is what
+// irfft's half swap and (-1)^(i+j) pre-multiplication produce.
+#pragma once
+#include <algorithm>
+#include <string>
+
+#include "gsb_fft.cuh"
+#include "gsb_internal.cuh"
+#include "gsb_profiles.cuh"
+
+namespace gsb {
+
+
+constexpr int kWarps = 8;
+constexpr int kThreads = kWarps * 32;
+
+struct StampSmem {
+    LeafParams leaf[GSB_MAX_LEAVES];
+    SersicTableView sersic[GSB_MAX_LEAVES];
+    gsb_phase phase[GSB_MAX_PHASES];
+    double phase_ax[GSB_MAX_PHASES];   // phase turns per k index, x and y
+    double phase_ay[GSB_MAX_PHASES];
+    double scale[GSB_MAX_SCALES];
+    gsb_stamp geom;
+    double flux_part[kWarps];
+};
+
+struct DrawArgs {
+    gsb_template tpl;
+    int n_stamps;
+    const gsb_leaf* leaves;
+    const gsb_phase* phases;
+    const double* scales;
+    const gsb_stamp* stamps;
+    const double* sersic_header;
+    const double4* sersic_node;
+    int sersic_stride;
+    void* out;
+    int out_dtype;
+    int add;
+    double* added_flux;
+    void* work;          // per-CTA W slabs when W does not fit in shared memory
+};
+
+__device__ inline int floor_div(int a, int n) { return a >= 0 ? a / n : -((-a + n - 1) / n); }
+__device__ inline int ceil_div(int a, int n) { return -floor_div(-a, n); }
+__device__ inline int pmod(int a, int n) { const int r = a % n; return r < 0 ? r + n : r; }
+
+// Load stamp s's leaves / phases / scales into shared memory.
+__device__ inline void load_stamp(StampSmem& S, const gsb_template& tpl, int s, const gsb_leaf* leaves,
+                           const gsb_phase* phases, const double* scales, const gsb_stamp* stamps,
+                           const double* sh, const double4* snode, int sstride, double dk_over_2pi)
+{
+    const int t = threadIdx.x;
+    if (t < tpl.n_leaves) {
+        const gsb_leaf& g = leaves[(size_t)s * tpl.n_leaves + t];
+        LeafParams& L = S.leaf[t];
+        for (int i = 0; i < 4; ++i) L.jac[i] = g.jac[i];
+        L.flux = g.flux;
+        for (int i = 0; i < 8; ++i) L.d[i] = g.d[i];
+        L.flags = g.flags;
+        L.type = tpl.leaf_type[t];
+        L.table = t;
+        if (L.type == GSB_SERSIC && sh) {
+            const double* H = sh + (size_t)g.table * kSersicHeader;
+            SersicTableView& v = S.sersic[t];
+            v.n = int(H[kSH_NUSED]);
+            v.front = H[kSH_FRONT];
+            v.da = H[kSH_DA];
+            v.ksq_min = H[kSH_KSQMIN];
+            v.ksq_max = H[kSH_KSQMAX];
+            v.kderiv2 = H[kSH_KD2];
+            v.kderiv4 = H[kSH_KD4];
+            v.highk_a = H[kSH_HIGHA];
+            v.highk_b = H[kSH_HIGHB];
+            v.node = snode + (size_t)g.table * sstride;
+        }
+    }
+    if (t >= 32 && t < 32 + tpl.n_phases) {
+        const int i = t - 32;
+        const gsb_phase& P = phases[(size_t)s * tpl.n_phases + i];
+        S.phase[i] = P;
+        // exp(-i (kx' cx + ky' cy)) with k' = jac^T k and k = (i, j) dk:
+        // argument = 2 pi (i ax + j ay), ax = (A cx + B cy) dk / 2 pi, ay = (C cx + D cy) dk / 2 pi
+        S.phase_ax[i] = (P.jac[0] * P.cenx + P.jac[1] * P.ceny) * dk_over_2pi;
+        S.phase_ay[i] = (P.jac[2] * P.cenx + P.jac[3] * P.ceny) * dk_over_2pi;
+    }
+    if (t >= 64 && t < 64 + tpl.n_scales) S.scale[t - 64] = scales[(size_t)s * tpl.n_scales + (t - 64)];
+    if (t == 96 && stamps) S.geom = stamps[s];
+}
+
+// Evaluate the program at k index (i, j) (kx = i dk, ky = j dk) of grid g.
+template <typename T>
+__device__ __noinline__ Cx<T> eval_program(const gsb_template& tpl, const StampSmem& S, double dk, int i, int j,
+                              const GridRef& g)
+{
+    Cx<T> stack[GSB_MAX_OPS];
+    int sp = 0;
+    const T kx = T(i * dk), ky = T(j * dk);
+    const int gi = i - g.x0, gj = j - g.y0;
+    for (int o = 0; o < tpl.n_ops; ++o) {
+        const int code = tpl.op_code[o], arg = tpl.op_arg[o];
+        if (code == GSB_OP_LEAF) {
+            stack[sp++] = cx<T>(leaf_kvalue<T>(S.leaf[arg], S.sersic, kx, ky, g, gi, gj), T(0));
+        } else if (code == GSB_OP_MUL) {
+            --sp;
+            stack[sp - 1] = cmul<T>(stack[sp - 1], stack[sp]);
+        } else if (code == GSB_OP_ADD) {
+            --sp;
+            stack[sp - 1] = cadd<T>(stack[sp - 1], stack[sp]);
+        } else if (code == GSB_OP_PHASE) {
+            double tt = i * S.phase_ax[arg] + j * S.phase_ay[arg];
+            tt -= rint(tt);
+            T sn, cs;
+            sincospi(T(-2. * tt), &sn, &cs);
+            const T fs = T(S.phase[arg].flux_scaling);
+            stack[sp - 1] = cmul<T>(stack[sp - 1], cx<T>(fs * cs, fs * sn));
+        } else if (code == GSB_OP_SCALE) {
+            stack[sp - 1] = cscale<T>(stack[sp - 1], T(S.scale[arg]));
+        }
+    }
+    return stack[0];
+}
+
+template <typename T>
+__device__ inline void store_pixel(void* out, int dtype, int add, long long idx, T v)
+{
+    if (dtype == GSB_F32) {
+        float* o = reinterpret_cast<float*>(out) + idx;
+        *o = add ? *o + float(v) : float(v);
+    } else {
+        double* o = reinterpret_cast<double*>(out) + idx;
+        *o = add ? *o + double(v) : double(v);
+    }
+}
+
+template <typename T, int N, bool WSMEM>
+__global__ void __launch_bounds__(kThreads) draw_fused_kernel(DrawArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int H = N / 2 + 1;
+    constexpr int WS = N + 1;   // column stride of W (padding against bank conflicts)
+    StampSmem& S = *reinterpret_cast<StampSmem*>(smem_raw);
+    size_t off = (sizeof(StampSmem) + 15) & ~size_t(15);
+    Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw + off);
+    off += sizeof(Cx<T>) * N;
+    Cx<T>* scratch = reinterpret_cast<Cx<T>*>(smem_raw + off);
+    off += sizeof(Cx<T>) * N * kWarps;
+    Cx<T>* W = WSMEM ? reinterpret_cast<Cx<T>*>(smem_raw + off)
+                     : reinterpret_cast<Cx<T>*>(a.work) + (size_t)blockIdx.x * H * WS;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    Cx<T>* buf = scratch + warp * N;
+    fill_twiddles<T>(tw, N);
+    const double dk = 2. * kPi / N;
+    const T inv_n2 = T(1) / (T(N) * T(N));
+
+    for (int s = blockIdx.x; s < a.n_stamps; s += gridDim.x) {
+        __syncthreads();
+        load_stamp(S, a.tpl, s, a.leaves, a.phases, a.scales, a.stamps, a.sersic_header,
+                   a.sersic_node, a.sersic_stride, 1. / N);
+        __syncthreads();
+        const int Nk = S.geom.Nk;
+        const int hk = Nk / 2;
+        const GridRef g{dk, 0, -hk, hk + 1, Nk + 1};
+
+        // ---- column phase: wrapped k-values, inverse DFT along ky ----
+        for (int c = warp; c < H; c += kWarps) {
+            const int alo = ceil_div(-hk - c, N), ahi = floor_div(hk - c, N);
+            for (int r = lane; r < N; r += 32) {
+                const int kyc = r < N / 2 ? r : r - N;
+                const int blo = ceil_div(-hk - kyc, N), bhi = floor_div(hk - kyc, N);
+                Cx<T> acc = cx<T>(T(0), T(0));
+                for (int ia = alo; ia <= ahi; ++ia) {
+                    const int kx = c + ia * N;
+                    for (int ib = blo; ib <= bhi; ++ib) {
+                        const int ky = kyc + ib * N;
+                        if (kx >= 0) acc = cadd<T>(acc, eval_program<T>(a.tpl, S, dk, kx, ky, g));
+                        else acc = cadd<T>(acc, cconj<T>(eval_program<T>(a.tpl, S, dk, -kx, -ky, g)));
+                    }
+                }
+                buf[r] = acc;
+            }
+            __syncwarp();
+            warp_fft<T, N, +1>(buf, tw);
+            for (int r = lane; r < N; r += 32) W[(size_t)c * WS + r] = buf[r];
+            __syncwarp();
+        }
+        __syncthreads();
+
+        // ---- row phase: two image rows per complex transform ----
+        const gsb_stamp& G = S.geom;
+        const int npairs = (G.ny + 1) / 2;
+        double fsum = 0., fcomp = 0.;
+        for (int p = warp; p < npairs; p += kWarps) {
+            const int py1 = G.ymin + 2 * p;
+            const bool two = 2 * p + 1 < G.ny;
+            const int y1 = pmod(py1, N), y2 = pmod(py1 + 1, N);
+            for (int kx = lane; kx < N; kx += 32) {
+                Cx<T> a1, a2;
+                if (kx < H) {
+                    a1 = W[(size_t)kx * WS + y1];
+                    a2 = two ? W[(size_t)kx * WS + y2] : cx<T>(T(0), T(0));
+                } else {
+                    a1 = cconj<T>(W[(size_t)(N - kx) * WS + y1]);
+                    a2 = two ? cconj<T>(W[(size_t)(N - kx) * WS + y2]) : cx<T>(T(0), T(0));
+                }
+                buf[kx] = cx<T>(a1.x - a2.y, a1.y + a2.x);
+            }
+            __syncwarp();
+            warp_fft<T, N, +1>(buf, tw);
+            const long long row1 = G.out_offset + (long long)(2 * p) * G.nx;
+            for (int i = lane; i < G.nx; i += 32) {
+                const Cx<T> v = buf[pmod(G.xmin + i, N)];
+                const T v1 = v.x * inv_n2;
+                store_pixel<T>(a.out, a.out_dtype, a.add, row1 + i, v1);
+                // Neumaier compensated sum in FP64
+                const double x1 = double(v1);
+                double tsum = fsum + x1;
+                fcomp += fabs(fsum) >= fabs(x1) ? (fsum - tsum) + x1 : (x1 - tsum) + fsum;
+                fsum = tsum;
+                if (two) {
+                    const T v2 = v.y * inv_n2;
+                    store_pixel<T>(a.out, a.out_dtype, a.add, row1 + G.nx + i, v2);
+                    const double x2 = double(v2);
+                    tsum = fsum + x2;
+                    fcomp += fabs(fsum) >= fabs(x2) ? (fsum - tsum) + x2 : (x2 - tsum) + fsum;
+                    fsum = tsum;
+                }
+            }
+            __syncwarp();
+        }
+        if (a.added_flux) {
+            double v = fsum + fcomp;
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) S.flux_part[warp] = v;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double tot = 0.;
+                for (int w = 0; w < kWarps; ++w) tot += S.flux_part[w];
+                a.added_flux[s] = tot;
+            }
+        }
+    }
+}
+
+template <typename T>
+__global__ void draw_kimage_kernel(gsb_template tpl, int n_stamps, const gsb_leaf* leaves,
+                                   const gsb_phase* phases, const double* scales,
+                                   const double* sh, const double4* snode, int sstride, double dk,
+                                   int kxmin, int kymin, int nkx, int nky, void* out, int dtype)
+{
+    __shared__ StampSmem S;
+    const long long per = (long long)nkx * nky;
+    for (int s = blockIdx.y; s < n_stamps; s += gridDim.y) {
+        __syncthreads();
+        load_stamp(S, tpl, s, leaves, phases, scales, nullptr, sh, snode, sstride, dk / (2. * kPi));
+        __syncthreads();
+        const GridRef g{dk, kxmin, kymin, nkx, nky};
+        for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < per;
+             p += (long long)gridDim.x * blockDim.x) {
+            const int i = int(p % nkx), j = int(p / nkx);
+            const Cx<T> v = eval_program<T>(tpl, S, dk, kxmin + i, kymin + j, g);
+            const long long o = (s * per + p) * 2;
+            if (dtype == GSB_F32) {
+                reinterpret_cast<float*>(out)[o] = float(v.x);
+                reinterpret_cast<float*>(out)[o + 1] = float(v.y);
+            } else {
+                reinterpret_cast<double*>(out)[o] = double(v.x);
+                reinterpret_cast<double*>(out)[o + 1] = double(v.y);
+            }
+        }
+    }
+}
+
+template <typename T, int N>
+constexpr size_t smem_bytes(bool wsmem)
+{
+    size_t off = (sizeof(StampSmem) + 15) & ~size_t(15);
+    off += sizeof(Cx<T>) * N * (1 + kWarps);
+    if (wsmem) off += sizeof(Cx<T>) * (N / 2 + 1) * (N + 1);
+    return off;
+}
+
+constexpr size_t kSmemLimit = 227 * 1024;
+
+template <typename T, int N>
+constexpr bool w_fits_smem()
+{
+    return ((sizeof(StampSmem) + 15) & ~size_t(15)) + sizeof(Cx<T>) * N * (1 + kWarps) +
+           sizeof(Cx<T>) * (N / 2 + 1) * (N + 1) <= kSmemLimit;
+}
+
+template <typename T, int N>
+int draw_grid(int n_stamps)
+{
+    DeviceState* st = device_state();
+    const size_t sm = smem_bytes<T, N>(w_fits_smem<T, N>());
+    int per_sm = int(std::min<size_t>(kSmemLimit / sm, 4));
+    if (per_sm < 1) per_sm = 1;
+    return std::max(1, std::min(n_stamps, st->sm_count * per_sm));
+}
+
+template <typename T, int N>
+size_t workspace_bytes_for(int n_stamps)
+{
+    if (w_fits_smem<T, N>()) return 0;
+    return sizeof(Cx<T>) * (size_t)(N / 2 + 1) * (N + 1) * draw_grid<T, N>(n_stamps);
+}
+
+template <typename T, int N>
+int launch_fused(const DrawArgs& args, size_t work_bytes, cudaStream_t stream)
+{
+    constexpr bool wsmem = w_fits_smem<T, N>();
+    constexpr size_t sm = smem_bytes<T, N>(wsmem);
+    const int grid = draw_grid<T, N>(args.n_stamps);
+    if (!wsmem && (args.work == nullptr || work_bytes < workspace_bytes_for<T, N>(args.n_stamps)))
+        return set_error(GSB_ERR_INVALID, "draw workspace too small");
+    GSB_CUDA_CHECK(cudaFuncSetAttribute(draw_fused_kernel<T, N, wsmem>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    draw_fused_kernel<T, N, wsmem><<<grid, kThreads, sm, stream>>>(args);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    return GSB_OK;
+}
+
+}  // namespace gsb

@@ -1,0 +1,139 @@
+// Internal definitions shared by the libgsb translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string>
+
+#include "gsb.h"
+#include "gsb_math.cuh"
+
+namespace gsb {
+
+// Records the message for gsb_last_error() and returns the code.
+int set_error(int code, const std::string& msg);
+
+#define GSB_CUDA_CHECK(expr)                                                              \
+    do {                                                                                  \
+        cudaError_t e_ = (expr);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return ::gsb::set_error(GSB_ERR_CUDA, std::string(#expr) + ": " +            \
+                                    cudaGetErrorString(e_));                              \
+    } while (0)
+
+// One leaf as used inside kernels (gsb_leaf plus its type).
+struct LeafParams {
+    double jac[4];
+    double flux;
+    double d[8];
+    int flags;
+    int table;
+    int type;
+};
+
+// Sersic FT table slot: header plus nodes (arg - front, value, y2, 0).
+// Header layout (doubles): see kSersicHeader* below.
+struct SersicTableView {
+    int n;              // number of nodes in the spline
+    double front, da;   // first arg, equal-spacing step for the index lookup
+    double ksq_min, ksq_max, kderiv2, kderiv4, highk_a, highk_b;
+    const double4* node;
+};
+
+enum {
+    kSH_N = 0, kSH_NUSED, kSH_FRONT, kSH_DA, kSH_KSQMIN, kSH_KSQMAX, kSH_KD2, kSH_KD4,
+    kSH_HIGHA, kSH_HIGHB, kSH_MAXK, kSH_STEPK, kSH_RE, kSH_DLOGK, kSH_NCAND, kSH_STATUS,
+    kSersicHeader = 16
+};
+
+// The reference k-image grid a point belongs to (for clip rules that depend on the grid).
+struct GridRef {
+    double dk;
+    int x0, y0;   // integer k index of column 0 / row 0
+    int m, n;     // columns, rows
+};
+
+// Airy annulus autocorrelation (SBAiry.cpp:259-329 obscured, :395-408 unobscured);
+// t = k^2 / (pi D)^2.
+template <typename T>
+__device__ inline T airy_chord(T r, T h, T rsq, T hsq)
+{
+    if (r == T(0)) return T(0);
+    return rsq * asin(h / r) - h * sqrt(rsq - hsq);
+}
+
+template <typename T>
+__device__ inline T airy_circle_same(T r, T rsq, T tsq)
+{
+    if (tsq >= T(4) * rsq) return T(0);
+    if (tsq == T(0)) return T(kPi) * rsq;
+    const T hsq = rsq - tsq / T(4);
+    const T h = sqrt(hsq);
+    return T(2) * airy_chord<T>(r, h, rsq, hsq);
+}
+
+template <typename T>
+__device__ inline T airy_circle_two(T r, T s, T rsq, T ssq, T tsq)
+{
+    const T rps_sq = (r + s) * (r + s);
+    if (tsq >= rps_sq) return T(0);
+    const T rms_sq = (r - s) * (r - s);
+    if (tsq <= rms_sq) return T(kPi) * ssq;
+    const T hsq = T(0.5) * (rsq + ssq) - (tsq * tsq + rps_sq * rms_sq) / (T(4) * tsq);
+    const T h = sqrt(hsq);
+    if (tsq < rsq - ssq)
+        return T(kPi) * ssq - airy_chord<T>(s, h, ssq, hsq) + airy_chord<T>(r, h, rsq, hsq);
+    return airy_chord<T>(s, h, ssq, hsq) + airy_chord<T>(r, h, rsq, hsq);
+}
+
+template <typename T>
+__device__ inline T airy_kvalue(T t, T obs, T obssq)
+{
+    if (obs == T(0)) {
+        if (t >= T(4)) return T(0);
+        if (t == T(0)) return T(kPi);
+        const T hsq = T(1) - t / T(4);
+        const T h = sqrt(hsq);
+        return T(2) * (asin(h) - h * sqrt(T(1) - hsq));
+    }
+    return airy_circle_same<T>(T(1), T(1), t) - T(2) * airy_circle_two<T>(T(1), obs, T(1), obssq, t) +
+           airy_circle_same<T>(obs, obssq, t);
+}
+
+// Device-side Ogata node tables (built once per device by gsb_init).
+struct OgataTables {
+    int lev_min, lev_max;            // h = 2^-lev for lev in [lev_min, lev_max]
+    long long off[32];               // node offset of each level (index lev - lev_min)
+    long long cnt[32];               // node count of each level
+    const double2* xw;               // (x, w) per node
+    const double2* root;             // (j0 zero, Y0(z)/J1(z)) for s = 1..nroot
+    long long nroot;
+};
+
+// Library state per device.
+struct DeviceState {
+    bool ready = false;
+    int sm_count = 0;
+    double2* d_xw = nullptr;
+    double2* d_root = nullptr;
+    OgataTables og{};
+    // Kolmogorov stepk factors cached per GSParams key
+    double kolm_key[13] = {0};
+    double kolm_stepk = 0.;
+    bool kolm_valid = false;
+};
+
+DeviceState* device_state();
+
+}  // namespace gsb
+
+// Opaque table set (device memory owned by the library).
+struct gsb_tables {
+    int count = 0;
+    int stride = 0;               // nodes per slot
+    double* d_header = nullptr;   // count * kSersicHeader
+    double4* d_node = nullptr;    // count * stride
+    double* d_val = nullptr;      // scratch: count * stride Hankel values
+    size_t cap_slots = 0, cap_nodes = 0;
+};

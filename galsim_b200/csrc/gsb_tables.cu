@@ -1,0 +1,671 @@
+// FP64 on-device construction of the FT tables and the leaf sizing (stepk / maxk).
+//
+//   ogata_*      Ogata (2005) nodes and weights for h = 2^-5 .. 2^-20, plus the first 10^6
+//                zeros of J0, built once per device (gsb_init).
+//   hankel_*     the reference's adaptive Hankel transform (src/math/Hankel.cpp:179-249),
+//                one warp per transform, terms summed 32 at a time with a warp prefix sum.
+//   sersic_*     SersicInfo (src/SBSersic.cpp:301-667): HLR and missing-flux radii by
+//                Brent, the ln k table of the Hankel transform, its high-k fit and maxk,
+//                and the natural cubic spline (src/Table.cpp:634-686).
+//   kolmogorov_* KolmogorovInfo stepk (src/SBKolmogorov.cpp:338-420).
+//   prepare_*    per-leaf derived constants and stepk / maxk.
+#include <algorithm>
+#include <vector>
+
+#include "gsb_internal.cuh"
+
+namespace gsb {
+
+namespace {
+
+constexpr int kLevMin = 5;
+constexpr int kLevMax = 20;
+constexpr long long kNroot = 1000000;
+
+__global__ void ogata_root_kernel(double2* root, long long nroot)
+{
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= nroot) return;
+    const double z = bessel_j0_zero(i + 1);
+    root[i] = make_double2(z, y0(z) / j1(z));
+}
+
+__device__ inline double2 ogata_node(const double2* root, double h, long long i)
+{
+    const double2 r = root[i];
+    const double t = h * r.x / kPi;
+    const double x = kPi / h * ogata_psi(t);
+    const double w = r.y * kPi * x * j0(x) * ogata_dpsi(t);
+    return make_double2(x, w);
+}
+
+__global__ void ogata_level_kernel(double2* xw, const double2* root, double h, long long n)
+{
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    xw[i] = ogata_node(root, h, i);
+}
+
+// Sum_i w_i f(x_i / k) / k^2 for h = 2^-lev with the reference's stopping rule: stop at the
+// first term whose magnitude is below 1e-15 |running sum| (Hankel.cpp:117-141).
+template <class F>
+__device__ double warp_ogata_sum(const OgataTables& og, const F& f, double k, int lev)
+{
+    const int lane = threadIdx.x & 31;
+    const double h = ldexp(1.0, -lev);
+    const long long nmax = (long long)fmin(kPi / h, 1e6);
+    const bool tab = lev >= og.lev_min && lev <= og.lev_max;
+    const double2* xw = tab ? og.xw + og.off[lev - og.lev_min] : nullptr;
+    double ans = 0.;
+    for (long long base = 0; base < nmax; base += 32) {
+        const long long i = base + lane;
+        const bool valid = i < nmax;
+        double step = 0.;
+        if (valid) {
+            const double2 n = tab ? xw[i] : ogata_node(og.root, h, i);
+            step = n.y * f(n.x / k);
+        }
+        double pre = step;
+        for (int o = 1; o < 32; o <<= 1) {
+            const double v = __shfl_up_sync(0xffffffffu, pre, o);
+            if (lane >= o) pre += v;
+        }
+        const double ans_i = ans + pre;
+        const bool stop = valid && fabs(step) < 1e-15 * fabs(ans_i);
+        const unsigned mask = __ballot_sync(0xffffffffu, stop);
+        if (mask) {
+            ans = __shfl_sync(0xffffffffu, ans_i, __ffs(mask) - 1);
+            return ans / (k * k);
+        }
+        ans = __shfl_sync(0xffffffffu, ans_i, 31);
+    }
+    return ans / (k * k);
+}
+
+// AdaptiveHankelIntegrator::integrate (Hankel.cpp:179-219).  `status` is set to 1 when
+// the halving ran past 2^-60 without meeting the tolerance.
+template <class F>
+__device__ double warp_hankel(const OgataTables& og, const F& f, double k, double relerr,
+                              double abserr, int* status)
+{
+    int lev = 5;
+    double h0 = 1. / 32.;
+    while (h0 > 100. * k && lev < 60) { h0 *= 0.5; ++lev; }
+    double ans0 = warp_ogata_sum(og, f, k, lev);
+    double ans1 = warp_ogata_sum(og, f, k, lev + 1);
+    double err = fabs(ans1 - ans0);
+    while ((err > relerr * ans1 && (err > abserr || fabs(ans1) > 2. * fabs(ans0))) || ans1 == 0.) {
+        ++lev;
+        if (lev > 60) { if (status) *status = 1; break; }
+        ans0 = ans1;
+        ans1 = warp_ogata_sum(og, f, k, lev + 1);
+        err = fabs(ans1 - ans0);
+    }
+    return ans1;
+}
+
+struct SersicRadial {
+    double invn;
+    __device__ double operator()(double r) const { return exp(-pow(r, invn)); }
+};
+
+struct KolmKValue {
+    __device__ double operator()(double k) const { return exp(-pow(k, 5. / 3.)); }
+};
+
+// (1 - P(2n, z)) Gamma(2n) - target   (SersicMissingFlux, SBSersic.cpp:541-556)
+struct SersicMissingFlux {
+    double twon, gam, target;
+    __device__ double operator()(double z) const { return (1. - gamma_p(twon, z)) * gam - target; }
+};
+
+// CalculateB (SBSersic.cpp:627-658)
+__device__ RootResult sersic_b(double n, double gamma2n, double flux_fraction)
+{
+    const double invn = 1. / n, invnsq = invn * invn;
+    const double b1 = 2. * n - 1. / 3.;
+    const double b2 = b1 + (8. / 405.) * invn + (46. / 25515.) * invnsq +
+                      (131. / 1148175.) * invn * invnsq;
+    SersicMissingFlux f{2. * n, gamma2n, (1. - 0.5 * flux_fraction) * gamma2n};
+    return solve_bracket_lower_limit(f, b1, b2, 0.);
+}
+
+// calculateMissingFluxRadius (SBSersic.cpp:558-625); result in units of r0.
+__device__ RootResult sersic_missing_flux_radius(double n, double gamma2n, double b,
+                                                 double missing_frac)
+{
+    const double missing_flux = missing_frac * gamma2n;
+    double z1 = -log(missing_flux);
+    double z;
+    if (n == 0.5) {
+        z = z1;
+    } else {
+        z = 4. * (n + 1.);
+        const double twonm1 = 2. * n - 1.;
+        double z2 = z1 + twonm1 * log(z) + twonm1 / z + twonm1 * (2. * n - 3.) / (2. * z * z);
+        if (z2 > z1 && z2 - z1 < 0.01) z2 = z1 + 0.01;
+        else if (z2 < z1 && z2 - z1 > -0.01) z2 = z1 - 0.01;
+        if (z1 < 0.) z1 = b;
+        SersicMissingFlux f{2. * n, gamma2n, missing_flux};
+        RootResult r = solve_bracket_upper(f, z1, z2);
+        if (!r.ok) return {0., false};
+        z = r.x;
+    }
+    return {pow(z, n), true};
+}
+
+__global__ void sersic_setup_kernel(const double* n_arr, int count, gsb_gsparams gsp,
+                                    double* header, int stride)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    double* H = header + (size_t)s * kSersicHeader;
+    const double n = n_arr[s];
+    const double gamma2n = tgamma(2. * n);
+    const double gamma4n = tgamma(4. * n);
+    const double gamma6n = tgamma(6. * n);
+    const double gamma8n = tgamma(8. * n);
+    // buildFT low-k series (SBSersic.cpp:386-424); untruncated, flux fraction 1
+    const double kderiv2 = -gamma4n / (4. * gamma2n);
+    const double kderiv4 = gamma6n / (64. * gamma2n);
+    const double kderiv6 = gamma8n / (2304. * gamma2n);
+    const double kmin = pow(gsp.kvalue_accuracy / kderiv6, 1. / 6.);
+    const double dlogk = gsp.table_spacing * sqrt(sqrt(gsp.kvalue_accuracy / 10.));
+    int ncand = 0;
+    const double logk_end = log(500.);
+    for (double logk = log(kmin) - 0.001; logk < logk_end && ncand < stride; logk += dlogk)
+        ++ncand;
+    int status = 0;
+    RootResult rb = sersic_b(n, gamma2n, 1.);
+    if (!rb.ok) status = 2;
+    const double b = rb.x;
+    RootResult rr = sersic_missing_flux_radius(n, gamma2n, b, gsp.folding_threshold);
+    if (!rr.ok) status = 3;
+    double R = rr.x;
+    R = fmax(R, gsp.stepk_minimum_hlr);
+    H[kSH_N] = n;
+    H[kSH_NUSED] = 0;
+    H[kSH_FRONT] = log(kmin) - 0.001;
+    H[kSH_DA] = dlogk;
+    H[kSH_KSQMIN] = kmin * kmin;
+    H[kSH_KSQMAX] = 0.;
+    H[kSH_KD2] = kderiv2;
+    H[kSH_KD4] = kderiv4;
+    H[kSH_HIGHA] = 0.;
+    H[kSH_HIGHB] = 0.;
+    H[kSH_MAXK] = kmin;
+    H[kSH_STEPK] = kPi / R;
+    H[kSH_RE] = pow(b, n);
+    H[kSH_DLOGK] = dlogk;
+    H[kSH_NCAND] = ncand;
+    H[kSH_STATUS] = status;
+}
+
+// One warp per (slot, node): val = Hankel transform at k_i / hankel_norm.
+__global__ void sersic_nodes_kernel(const double* header, int count, int stride, gsb_gsparams gsp,
+                                    OgataTables og, double* vals, int* status_out)
+{
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long s = warp / stride;
+    const int i = int(warp % stride);
+    if (s >= count) return;
+    const double* H = header + s * kSersicHeader;
+    if (i >= int(H[kSH_NCAND])) return;
+    const double n = H[kSH_N];
+    const double logk = H[kSH_FRONT] + i * H[kSH_DLOGK];
+    const double k = exp(logk);
+    const double hankel_norm = n * tgamma(2. * n);
+    SersicRadial f{1. / n};
+    int st = 0;
+    const double v = warp_hankel(og, f, k, gsp.integration_relerr,
+                                 gsp.integration_abserr * hankel_norm, &st) / hankel_norm;
+    if ((threadIdx.x & 31) == 0) {
+        vals[s * stride + i] = v;
+        if (st) atomicOr(status_out, 1);
+    }
+}
+
+// Sequential part of buildFT (SBSersic.cpp:436-527) and the spline (Table.cpp:634-686).
+__global__ void sersic_finalize_kernel(double* header, int count, int stride, gsb_gsparams gsp,
+                                       const double* vals, double4* nodes)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    double* H = header + (size_t)s * kSersicHeader;
+    const double* v = vals + (size_t)s * stride;
+    double4* nd = nodes + (size_t)s * stride;
+    const int ncand = int(H[kSH_NCAND]);
+    const double front = H[kSH_FRONT], dlogk = H[kSH_DLOGK];
+    const int n_fit = 10;
+    double fitbuf[10];
+    int fit_size = 0, fit_head = 0;   // ring buffer; head = index of the oldest entry
+    double sf = 0., skf = 0., sk = 0., sk2 = 0.;
+    double ksq_max = -1., maxk = sqrt(H[kSH_KSQMIN]);
+    double a = 0., b = 0.;
+    bool found_maxk = false;
+    int n_correct = 0, nused = 0;
+    for (int i = 0; i < ncand; ++i) {
+        const double logk = front + i * dlogk;
+        const double k = exp(logk), ksq = k * k;
+        const double val = v[i];
+        const double f0 = val * ksq;
+        nd[i] = make_double4(logk, f0, 0., 0.);
+        nused = i + 1;
+        if (fabs(val) > gsp.maxk_threshold) { maxk = k; n_correct = 0; }
+        else {
+            found_maxk = true;
+            a = (sf * sk2 - sk * skf) / (n_fit * sk2 - sk * sk);
+            b = (n_fit * skf - sk * sf) / (n_fit * sk2 - sk * sk);
+            const double f0_pred = a + b / k;
+            if (fabs(f0 - f0_pred) / ksq < gsp.kvalue_accuracy) ++n_correct;
+            else n_correct = 0;
+            if (n_correct >= 5) { ksq_max = ksq; break; }
+        }
+        const double inv_k = 1. / k;
+        if (fit_size == n_fit) {
+            const double k_back = exp(logk - n_fit * dlogk);
+            const double f_back = fitbuf[fit_head];
+            const double inv_k_back = 1. / k_back;
+            sf += f0 - f_back;
+            skf += f0 * inv_k - f_back * inv_k_back;
+            sk += inv_k - inv_k_back;
+            sk2 += inv_k * inv_k - inv_k_back * inv_k_back;
+            fitbuf[fit_head] = f0;
+            fit_head = (fit_head + 1) % n_fit;
+        } else {
+            sf += f0;
+            skf += f0 * inv_k;
+            sk += inv_k;
+            sk2 += inv_k * inv_k;
+            fitbuf[fit_size++] = f0;
+        }
+    }
+    if (ksq_max <= 0.) ksq_max = exp(2. * nd[nused - 1].x);
+    if (found_maxk) {
+        maxk *= exp(dlogk);
+    } else {
+        a = (sf * sk2 - sk * skf) / (n_fit * sk2 - sk * sk);
+        b = (n_fit * skf - sk * sf) / (n_fit * sk2 - sk * sk);
+        maxk = sqrt(a / gsp.maxk_threshold);
+        for (int it = 0; it < 3; ++it) maxk = sqrt((a - b / maxk) / gsp.maxk_threshold);
+    }
+    // Natural cubic spline second derivatives (Thomas algorithm), stored in .z
+    const int N = nused;
+    for (int i = 0; i < N; ++i) nd[i].z = 0.;
+    if (N == 3) {
+        nd[1].z = 3. * ((nd[2].y - nd[1].y) / (nd[2].x - nd[1].x) -
+                        (nd[1].y - nd[0].y) / (nd[1].x - nd[0].x)) / (nd[2].x - nd[0].x);
+    } else if (N > 3) {
+        // c[] is stashed in .w
+        for (int i = 1; i <= N - 2; ++i)
+            nd[i].z = 6. * ((nd[i + 1].y - nd[i].y) / (nd[i + 1].x - nd[i].x) -
+                            (nd[i].y - nd[i - 1].y) / (nd[i].x - nd[i - 1].x));
+        double bb = 2. * (nd[2].x - nd[0].x);
+        for (int i = 1; i <= N - 2; ++i) {
+            nd[i].z /= bb;
+            if (i == N - 2) break;
+            const double aa = nd[i + 1].x - nd[i].x;
+            const double c = aa / bb;
+            nd[i - 1].w = c;
+            bb = 2. * (nd[i + 2].x - nd[i].x);
+            bb -= aa * c;
+            nd[i + 1].z -= aa * nd[i].z;
+        }
+        for (int i = N - 3; i > 0; --i) nd[i].z -= nd[i - 1].w * nd[i + 1].z;
+    }
+    const double back = nd[N - 1].x;
+    for (int i = 0; i < N; ++i) { nd[i].x -= front; nd[i].w = 0.; }
+    H[kSH_NUSED] = N;
+    H[kSH_DA] = N > 1 ? (back - front) / (N - 1) : dlogk;
+    H[kSH_KSQMAX] = ksq_max;
+    H[kSH_HIGHA] = a;
+    H[kSH_HIGHB] = b;
+    H[kSH_MAXK] = maxk;
+}
+
+// KolmogorovInfo: x-space radial profile by Hankel transform of exp(-k^{5/3}) at
+// r = exp(-3 + i dlogr); only the last tabulated point matters for stepk.
+__global__ void kolmogorov_nodes_kernel(int ncand, double dlogr, gsb_gsparams gsp, OgataTables og,
+                                        double* vals, int* status_out)
+{
+    const int i = int((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    if (i >= ncand) return;
+    const double r = exp(-3. + i * dlogr);
+    KolmKValue f;
+    int st = 0;
+    const double v = warp_hankel(og, f, r, gsp.integration_relerr, gsp.integration_abserr, &st) /
+                     (2. * kPi);
+    if ((threadIdx.x & 31) == 0) {
+        vals[i] = v;
+        if (st) atomicOr(status_out, 1);
+    }
+}
+
+__global__ void kolmogorov_finalize_kernel(int ncand, double dlogr, gsb_gsparams gsp,
+                                           const double* vals, double* out)
+{
+    const double thresh = gsp.shoot_accuracy / (2. * kPi);
+    double r1 = 0., F1 = 0.;
+    for (int i = 0; i < ncand; ++i) {
+        const double r = exp(-3. + i * dlogr);
+        r1 = r; F1 = vals[i];
+        if (vals[i] * r * r / 1.67 < thresh) break;
+    }
+    const double n = 11. / 3.;
+    double R = pow(2. * kPi * F1 * pow(r1, n) / ((n - 2.) * gsp.folding_threshold), 1. / (n - 2.));
+    const double hlr = 2.992939911888651 * 0.5548101137;
+    R = fmax(R, gsp.stepk_minimum_hlr * hlr);
+    out[0] = kPi / R;
+}
+
+// kV2 for the Moffat maxk solve (MoffatMaxKSolver, SBMoffat.cpp:481-520), normalised to 1
+// at k = 0, as a function of ksq.
+struct MoffatKV2 {
+    int mode;
+    double nu, thresh;
+    __device__ double operator()(double ksq) const
+    {
+        const double k = sqrt(ksq);
+        double v;
+        if (mode == 1) v = exp(-k);
+        else if (mode == 2) v = exp(-k) * (1. + k);
+        else if (mode == 3) v = exp(-k) * (3. + (3. + k) * k) / 3.;
+        else v = moffat_kv_fp64(nu, k);
+        return v - thresh;
+    }
+};
+
+__global__ void prepare_leaves_kernel(gsb_template tpl, int n_stamps, gsb_gsparams gsp,
+                                      gsb_leaf* leaves, const double* sersic_header,
+                                      double kolm_stepk, double* info, int* status_out)
+{
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= (long long)n_stamps * tpl.n_leaves) return;
+    const int l = int(idx % tpl.n_leaves);
+    gsb_leaf& L = leaves[idx];
+    const int type = tpl.leaf_type[l];
+    double stepk = 0., maxk = 0.;
+    for (int i = 0; i < 8; ++i) L.d[i] = 0.;
+    switch (type) {
+      case GSB_GAUSSIAN: {
+        // gaussian.py:148-155 and SBGaussian.cpp:63-73
+        const double sigma = L.p[0];
+        L.d[0] = sigma;
+        L.d[1] = -2. * log(gsp.kvalue_accuracy);
+        L.d[2] = pow(gsp.kvalue_accuracy * 48., 1. / 3.);
+        maxk = sqrt(-2. * log(gsp.maxk_threshold)) / sigma;
+        const double R = fmax(sqrt(-2. * log(gsp.folding_threshold)),
+                              gsp.stepk_minimum_hlr * 1.1774100225154747);
+        stepk = kPi / (R * sigma);
+        break;
+      }
+      case GSB_EXPONENTIAL: {
+        // exponential.py:131-136, SBExponential.cpp:65-79 and ExponentialInfo :513-543
+        const double r0 = L.p[0];
+        const double ksq_max = pow(gsp.kvalue_accuracy, -1. / 1.5) - 1.;
+        L.d[0] = r0;
+        L.d[1] = ksq_max;
+        L.d[2] = sqrt(ksq_max);
+        maxk = pow(gsp.maxk_threshold, -1. / 3.) / r0;
+        const double logx = log(gsp.folding_threshold);
+        double R = -logx;
+        for (int i = 0; i < 3; ++i) R = log(1. + R) - logx;
+        R = fmax(R, gsp.stepk_minimum_hlr * 1.6783469900166605);
+        stepk = kPi / R / r0;
+        break;
+      }
+      case GSB_SERSIC: {
+        // SBSersic.cpp:71-90 (r0 from hlr via SersicHLR, sersic.py:224-227), :301-324
+        const double* H = sersic_header + (size_t)L.table * kSersicHeader;
+        const double r0 = (L.flags & GSB_LEAF_SIZE_IS_HLR) ? L.p[1] / H[kSH_RE] : L.p[1];
+        L.d[0] = r0;
+        maxk = H[kSH_MAXK] / r0;
+        stepk = H[kSH_STEPK] / r0;
+        if (H[kSH_STATUS] != 0.) atomicOr(status_out, 2);
+        break;
+      }
+      case GSB_MOFFAT: {
+        // SBMoffat.cpp:163-244 (kV selection), :481-549 (maxK, stepK); untruncated
+        const double beta = L.p[0], rD = L.p[1];
+        const double kacc = gsp.kvalue_accuracy;
+        int mode = 0;
+        double nu = beta - 1., knorm = L.flux;
+        if (fabs(beta - 1.5) < kacc) { mode = 1; }
+        else if (fabs(beta - 2.) < kacc) { nu = 1.; }
+        else if (fabs(beta - 2.5) < kacc) { mode = 2; }
+        else if (fabs(beta - 3.) < kacc) { nu = 2.; }
+        else if (fabs(beta - 3.5) < kacc) { mode = 3; }
+        else if (fabs(beta - 4.) < kacc) { nu = 3.; }
+        L.d[0] = rD;
+        L.d[1] = knorm;
+        L.d[2] = mode;
+        L.d[3] = nu;
+        L.d[4] = (1. - nu) * log(2.) - lgamma(nu);
+        MoffatKV2 f{mode, nu, gsp.maxk_threshold};
+        RootResult r = solve_bracket_upper(f, 0., 100.);
+        if (!r.ok) atomicOr(status_out, 4);
+        maxk = sqrt(r.x) / rD;
+        const double maxRrD = sqrt(pow(gsp.xvalue_accuracy, 1. / (1. - beta)) - 1.);
+        const double maxR = maxRrD * rD;
+        if (beta <= 1.1) {
+            stepk = kPi / maxR;
+        } else {
+            double R = pow(gsp.folding_threshold, 0.5 / (1. - beta)) * rD;
+            if (R > maxR) R = maxR;
+            const double hlr = rD * sqrt(pow(1. - 0.5, 1. / (1. - beta)) - 1.);
+            R = fmax(R, gsp.stepk_minimum_hlr * hlr);
+            stepk = kPi / R;
+        }
+        break;
+      }
+      case GSB_KOLMOGOROV: {
+        // kolmogorov.py:163-226 (k0), :281-287; SBKolmogorov.cpp:117-121
+        const double k0 = 2.992939911888651 / L.p[0];
+        L.d[0] = 1. / k0;
+        maxk = pow(-log(gsp.kvalue_accuracy), 0.6) * k0;
+        stepk = kolm_stepk * k0;
+        break;
+      }
+      case GSB_AIRY: {
+        // airy.py:217-222, SBAiry.cpp:66-81, 332-356, 432-445
+        const double lod = L.p[0], obs = L.p[1];
+        const double D = 1. / lod;
+        L.d[0] = 1. / (D * kPi);
+        L.d[1] = L.flux / (kPi * (1. - obs * obs));
+        L.d[2] = obs;
+        L.d[3] = obs * obs;
+        maxk = 2. * kPi / lod;
+        double R = (obs == 0.) ? 1. / (gsp.folding_threshold * 0.5 * kPi * kPi)
+                               : 1. / (gsp.folding_threshold * 0.5 * kPi * kPi * (1. - obs));
+        R = fmax(R, gsp.stepk_minimum_hlr * 0.5348321477);
+        stepk = kPi / R * D;
+        break;
+      }
+      case GSB_BOX: {
+        // box.py:100-106, SBBox.cpp:74-77
+        const double w = L.p[0], hgt = L.p[1];
+        L.d[0] = w / (2. * kPi);
+        L.d[1] = hgt / (2. * kPi);
+        maxk = 2. / (gsp.maxk_threshold * fmin(w, hgt));
+        stepk = kPi / fmax(w, hgt);
+        break;
+      }
+      default:
+        atomicOr(status_out, 8);
+    }
+    info[2 * idx] = stepk;
+    info[2 * idx + 1] = maxk;
+}
+
+}  // namespace
+
+int ogata_init(DeviceState* st)
+{
+    GSB_CUDA_CHECK(cudaMalloc(&st->d_root, sizeof(double2) * kNroot));
+    ogata_root_kernel<<<(unsigned)((kNroot + 255) / 256), 256>>>(st->d_root, kNroot);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    long long total = 0;
+    OgataTables og{};
+    og.lev_min = kLevMin;
+    og.lev_max = kLevMax;
+    for (int lev = kLevMin; lev <= kLevMax; ++lev) {
+        const double h = ldexp(1.0, -lev);
+        const long long n = (long long)std::min(M_PI / h, 1e6);
+        og.off[lev - kLevMin] = total;
+        og.cnt[lev - kLevMin] = n;
+        total += n;
+    }
+    GSB_CUDA_CHECK(cudaMalloc(&st->d_xw, sizeof(double2) * total));
+    for (int lev = kLevMin; lev <= kLevMax; ++lev) {
+        const long long n = og.cnt[lev - kLevMin];
+        ogata_level_kernel<<<(unsigned)((n + 255) / 256), 256>>>(
+            st->d_xw + og.off[lev - kLevMin], st->d_root, ldexp(1.0, -lev), n);
+        GSB_CUDA_CHECK(cudaGetLastError());
+    }
+    GSB_CUDA_CHECK(cudaDeviceSynchronize());
+    og.xw = st->d_xw;
+    og.root = st->d_root;
+    og.nroot = kNroot;
+    st->og = og;
+    return GSB_OK;
+}
+
+// Upper bound on the Sersic table length for these n values and GSParams.
+static int sersic_stride(const double* h_n, int count, const gsb_gsparams* gsp)
+{
+    double nmax = 0.;
+    for (int i = 0; i < count; ++i) nmax = std::max(nmax, h_n[i]);
+    const double kderiv6 = std::exp(std::lgamma(8. * nmax) - std::lgamma(2. * nmax)) / 2304.;
+    const double kmin = std::pow(gsp->kvalue_accuracy / kderiv6, 1. / 6.);
+    const double dlogk = gsp->table_spacing * std::sqrt(std::sqrt(gsp->kvalue_accuracy / 10.));
+    const double span = std::log(500.) - (std::log(kmin) - 0.001);
+    return int(span / dlogk) + 4;
+}
+
+int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc, int count,
+                        const gsb_gsparams* gsp, cudaStream_t stream)
+{
+    DeviceState* st = device_state();
+    if (!st->ready) return set_error(GSB_ERR_INVALID, "gsb_init has not been called");
+    for (int i = 0; i < count; ++i) {
+        if (!(h_n[i] >= 0.3 && h_n[i] <= 6.2))
+            return set_error(GSB_ERR_INVALID, "Sersic index out of range [0.3, 6.2]");
+        if (h_trunc && h_trunc[i] != 0.)
+            return set_error(GSB_ERR_UNSUPPORTED, "truncated Sersic profiles are not built");
+    }
+    if (count <= 0) { t->count = 0; return GSB_OK; }
+    const int stride = sersic_stride(h_n, count, gsp);
+    if ((size_t)count > t->cap_slots || (size_t)count * stride > t->cap_nodes) {
+        cudaFree(t->d_header); cudaFree(t->d_node); cudaFree(t->d_val);
+        t->d_header = nullptr; t->d_node = nullptr; t->d_val = nullptr;
+        t->cap_slots = std::max<size_t>(count, t->cap_slots);
+        t->cap_nodes = std::max<size_t>((size_t)count * stride, t->cap_nodes);
+        GSB_CUDA_CHECK(cudaMalloc(&t->d_header, sizeof(double) * kSersicHeader * t->cap_slots));
+        GSB_CUDA_CHECK(cudaMalloc(&t->d_node, sizeof(double4) * t->cap_nodes));
+        GSB_CUDA_CHECK(cudaMalloc(&t->d_val, sizeof(double) * t->cap_nodes));
+    }
+    t->count = count;
+    t->stride = stride;
+    double* d_n = nullptr;
+    int* d_status = nullptr;
+    GSB_CUDA_CHECK(cudaMallocAsync(&d_n, sizeof(double) * count, stream));
+    GSB_CUDA_CHECK(cudaMallocAsync(&d_status, sizeof(int), stream));
+    GSB_CUDA_CHECK(cudaMemcpyAsync(d_n, h_n, sizeof(double) * count, cudaMemcpyHostToDevice, stream));
+    GSB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), stream));
+    sersic_setup_kernel<<<(count + 127) / 128, 128, 0, stream>>>(d_n, count, *gsp, t->d_header, stride);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    const long long nwarps = (long long)count * stride;
+    const int threads = 256;
+    const long long blocks = (nwarps * 32 + threads - 1) / threads;
+    sersic_nodes_kernel<<<(unsigned)blocks, threads, 0, stream>>>(t->d_header, count, stride, *gsp,
+                                                                  st->og, t->d_val, d_status);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    sersic_finalize_kernel<<<(count + 63) / 64, 64, 0, stream>>>(t->d_header, count, stride, *gsp,
+                                                                 t->d_val, t->d_node);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    int h_status = 0;
+    GSB_CUDA_CHECK(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    GSB_CUDA_CHECK(cudaFreeAsync(d_n, stream));
+    GSB_CUDA_CHECK(cudaFreeAsync(d_status, stream));
+    GSB_CUDA_CHECK(cudaStreamSynchronize(stream));
+    if (h_status) return set_error(GSB_ERR_NUMERIC, "Sersic Hankel transform did not converge");
+    return GSB_OK;
+}
+
+int kolmogorov_stepk(const gsb_gsparams* gsp, cudaStream_t stream, double* out)
+{
+    DeviceState* st = device_state();
+    const double key[13] = {double(gsp->minimum_fft_size), double(gsp->maximum_fft_size),
+                            gsp->folding_threshold, gsp->stepk_minimum_hlr, gsp->maxk_threshold,
+                            gsp->kvalue_accuracy, gsp->xvalue_accuracy, gsp->table_spacing,
+                            gsp->realspace_relerr, gsp->realspace_abserr, gsp->integration_relerr,
+                            gsp->integration_abserr, gsp->shoot_accuracy};
+    if (st->kolm_valid && std::equal(key, key + 13, st->kolm_key)) { *out = st->kolm_stepk; return GSB_OK; }
+    const double dlogr = gsp->table_spacing * std::sqrt(std::sqrt(gsp->xvalue_accuracy / 10.));
+    int ncand = 0;
+    for (double logr = -3.; logr < std::log(1.e4); logr += dlogr) ++ncand;
+    double* d_vals = nullptr;
+    int* d_status = nullptr;
+    double* d_out = nullptr;
+    GSB_CUDA_CHECK(cudaMallocAsync(&d_vals, sizeof(double) * ncand, stream));
+    GSB_CUDA_CHECK(cudaMallocAsync(&d_status, sizeof(int), stream));
+    GSB_CUDA_CHECK(cudaMallocAsync(&d_out, sizeof(double), stream));
+    GSB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), stream));
+    kolmogorov_nodes_kernel<<<(ncand * 32 + 255) / 256, 256, 0, stream>>>(ncand, dlogr, *gsp, st->og,
+                                                                          d_vals, d_status);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    kolmogorov_finalize_kernel<<<1, 1, 0, stream>>>(ncand, dlogr, *gsp, d_vals, d_out);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    double h_out = 0.;
+    int h_status = 0;
+    GSB_CUDA_CHECK(cudaMemcpyAsync(&h_out, d_out, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    GSB_CUDA_CHECK(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    GSB_CUDA_CHECK(cudaFreeAsync(d_vals, stream));
+    GSB_CUDA_CHECK(cudaFreeAsync(d_status, stream));
+    GSB_CUDA_CHECK(cudaFreeAsync(d_out, stream));
+    GSB_CUDA_CHECK(cudaStreamSynchronize(stream));
+    if (h_status) return set_error(GSB_ERR_NUMERIC, "Kolmogorov Hankel transform did not converge");
+    std::copy(key, key + 13, st->kolm_key);
+    st->kolm_stepk = h_out;
+    st->kolm_valid = true;
+    *out = h_out;
+    return GSB_OK;
+}
+
+int prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp, gsb_leaf* d_leaves,
+                   const gsb_tables* t, double* d_info, cudaStream_t stream)
+{
+    DeviceState* st = device_state();
+    if (!st->ready) return set_error(GSB_ERR_INVALID, "gsb_init has not been called");
+    bool need_kolm = false, need_sersic = false;
+    for (int l = 0; l < tpl->n_leaves; ++l) {
+        if (tpl->leaf_type[l] == GSB_KOLMOGOROV) need_kolm = true;
+        if (tpl->leaf_type[l] == GSB_SERSIC) need_sersic = true;
+    }
+    if (need_sersic && (!t || t->count == 0))
+        return set_error(GSB_ERR_INVALID, "Sersic leaves need built FT tables");
+    double kolm = 0.;
+    if (need_kolm) {
+        const int rc = kolmogorov_stepk(gsp, stream, &kolm);
+        if (rc) return rc;
+    }
+    int* d_status = nullptr;
+    GSB_CUDA_CHECK(cudaMallocAsync(&d_status, sizeof(int), stream));
+    GSB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), stream));
+    const long long n = (long long)n_stamps * tpl->n_leaves;
+    if (n > 0) {
+        prepare_leaves_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(
+            *tpl, n_stamps, *gsp, d_leaves, t ? t->d_header : nullptr, kolm, d_info, d_status);
+        GSB_CUDA_CHECK(cudaGetLastError());
+    }
+    int h_status = 0;
+    GSB_CUDA_CHECK(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    GSB_CUDA_CHECK(cudaFreeAsync(d_status, stream));
+    GSB_CUDA_CHECK(cudaStreamSynchronize(stream));
+    if (h_status & 8) return set_error(GSB_ERR_INVALID, "unknown leaf type");
+    if (h_status & 2) return set_error(GSB_ERR_NUMERIC, "Sersic radius root finding failed");
+    if (h_status & 4) return set_error(GSB_ERR_NUMERIC, "Moffat maxk root finding failed");
+    return GSB_OK;
+}
+
+}  // namespace gsb

@@ -1,0 +1,277 @@
+"""Flattening of GSObject trees into device programs, GalSim-exact FFT sizing, and the calls
+into libgsb that draw them.
+
+A *program* is the profile tree of every stamp of a batch written as a postfix op list
+(LEAF / MUL / ADD / PHASE / SCALE, see include/gsb.h) plus per-stamp numeric records.  All
+stamps of a batch share the topology; parameters may differ per stamp.  This replaces the
+reference's Python tree walk of _drawKImage (convolve.py:420-426, sum.py:341-347,
+transform.py:592-602), which issues one C++ call per leaf and one numpy pass per node.
+
+Sizing (stepk / maxk -> N, Nk) follows the reference exactly: the leaf stepK()/maxK() values
+are computed in FP64 on the GPU (gsb_prepare_leaves), and the composition rules
+(convolve.py:296-305, sum.py:243-251, transform.py:490-516) and the integer sizing of
+drawFFT_makeKImage (gsobject.py:1900-1963) run here in vectorised FP64 numpy, in the same
+order of operations as the reference's Python.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from .errors import GalSimError, galsim_warn_fft
+
+
+class Builder(object):
+    def __init__(self, B, gsparams):
+        self.B = B
+        self.gsparams = gsparams
+        self.ops = []
+        self.leaf_types = []
+        self.leaves = []
+        self.phases = []
+        self.scales = []
+
+    def _bcast(self, v):
+        a = np.asarray(v, dtype=np.float64)
+        return np.broadcast_to(a, (self.B,)) if a.ndim == 0 else a.reshape(self.B)
+
+    def _bjac(self, jac):
+        if jac is None:
+            return None
+        j = np.asarray(jac, dtype=np.float64)
+        return np.broadcast_to(j, (self.B, 2, 2))
+
+    def add_leaf(self, ltype, jac, flux, params, flags=0):
+        if len(self.leaves) >= _lib.MAX_LEAVES:
+            raise GalSimError("profile tree has more than %d leaves" % _lib.MAX_LEAVES)
+        rec = np.zeros(self.B, dtype=_lib.LEAF_DTYPE)
+        j = self._bjac(jac)
+        if j is None:
+            rec['jac'][:] = (1., 0., 0., 1.)
+            general = np.zeros(self.B, bool)
+        else:
+            rec['jac'] = j.reshape(self.B, 4)
+            general = (j[:, 0, 1] != 0.) | (j[:, 1, 0] != 0.)
+        rec['flux'] = self._bcast(flux)
+        for i, p in enumerate(params):
+            rec['p'][:, i] = self._bcast(p)
+        rec['flags'] = np.where(general, _lib.LEAF_JAC_GENERAL, 0) | flags
+        self.ops.append((_lib.OP_LEAF, len(self.leaves)))
+        self.leaf_types.append(ltype)
+        self.leaves.append(rec)
+
+    def add_op(self, code):
+        self.ops.append((code, 0))
+
+    def add_phase(self, jac, cx, cy, fs):
+        if len(self.phases) >= _lib.MAX_PHASES:
+            raise GalSimError("profile tree has more than %d shifted transformations" % _lib.MAX_PHASES)
+        rec = np.zeros(self.B, dtype=_lib.PHASE_DTYPE)
+        j = self._bjac(jac)
+        rec['jac'] = (1., 0., 0., 1.) if j is None else j.reshape(self.B, 4)
+        rec['cenx'] = self._bcast(cx)
+        rec['ceny'] = self._bcast(cy)
+        rec['flux_scaling'] = self._bcast(fs)
+        self.ops.append((_lib.OP_PHASE, len(self.phases)))
+        self.phases.append(rec)
+
+    def add_scale(self, s):
+        if len(self.scales) >= _lib.MAX_SCALES:
+            raise GalSimError("profile tree has more than %d flux scalings" % _lib.MAX_SCALES)
+        self.ops.append((_lib.OP_SCALE, len(self.scales)))
+        self.scales.append(self._bcast(s))
+
+    def template(self):
+        if len(self.ops) > _lib.MAX_OPS:
+            raise GalSimError("profile tree needs more than %d program ops" % _lib.MAX_OPS)
+        t = _lib.TemplateC()
+        t.n_ops = len(self.ops)
+        t.n_leaves = len(self.leaves)
+        t.n_phases = len(self.phases)
+        t.n_scales = len(self.scales)
+        for i, (c, a) in enumerate(self.ops):
+            t.op_code[i] = c
+            t.op_arg[i] = a
+        for i, lt in enumerate(self.leaf_types):
+            t.leaf_type[i] = lt
+        return t
+
+
+def batch_size(obj):
+    return obj._batch
+
+
+class Program(object):
+    """A flattened batch of profile trees resident on the device, ready to size and draw."""
+
+    def __init__(self, obj, gsparams=None):
+        self.obj = obj
+        self.B = batch_size(obj)
+        self.gsparams = gsparams if gsparams is not None else obj.gsparams
+        bld = Builder(self.B, self.gsparams)
+        obj._flatten(bld, None)
+        self.bld = bld
+        self.tpl = bld.template()
+        self.L = len(bld.leaves)
+        self.gsp_c = _lib.gsparams_c(self.gsparams)
+        self._prepared = False
+
+    # -- device preparation ------------------------------------------------------------------
+    def prepare(self):
+        """Build FT tables, upload the leaves and compute their stepk / maxk on the GPU."""
+        if self._prepared:
+            return
+        import torch
+        B, L = self.B, self.L
+        leaves = np.stack(self.bld.leaves, axis=1)            # (B, L)
+        self.tables = None
+        sersic = [l for l in range(L) if self.bld.leaf_types[l] == _lib.SERSIC]
+        if sersic:
+            nvals = np.concatenate([leaves[:, l]['p'][:, 0] for l in sersic])
+            uniq, inv = np.unique(nvals, return_inverse=True)
+            self.tables = _lib.Tables()
+            self.tables.build_sersic(uniq, self.gsparams)
+            inv = inv.reshape(len(sersic), B)
+            for k, l in enumerate(sersic):
+                leaves['table'][:, l] = inv[k]
+        self.d_leaves = _lib.to_device(leaves)
+        self.d_info = torch.empty(B * L * 2, dtype=torch.float64, device=_lib.Device.torch_device())
+        _lib.check(_lib.lib().gsb_prepare_leaves(
+            ctypes.byref(self.tpl), B, ctypes.byref(self.gsp_c), _lib.ptr(self.d_leaves),
+            self.tables.handle if self.tables else None, _lib.ptr(self.d_info), _lib.Device.stream()))
+        info = self.d_info.cpu().numpy().reshape(B, L, 2)
+        self.leaf_stepk = info[:, :, 0]
+        self.leaf_maxk = info[:, :, 1]
+        self._prepared = True
+
+    def stepk_maxk(self):
+        """Composite stepk / maxk per stamp, by the reference's composition rules."""
+        self.prepare()
+        it = iter(range(self.L))
+        return self.obj._size(self, it)
+
+    def leaf_size(self, l):
+        return self.leaf_stepk[:, l], self.leaf_maxk[:, l]
+
+    # -- drawing ---------------------------------------------------------------------------
+    def draw_stamps(self, N, Nk, xmin, ymin, nx, ny, dtype, add_to=None, precision=_lib.F32):
+        """Run the fused kernels for every stamp.  Arrays are per stamp.  Returns the device
+        output buffer (flat), per-stamp offsets and the device added-flux array."""
+        import torch
+        self.prepare()
+        B, L = self.B, self.L
+        dev = _lib.Device.torch_device()
+        N = np.asarray(N, np.int64)
+        order = np.argsort(N, kind='stable')
+        nx = np.asarray(nx, np.int64)
+        ny = np.asarray(ny, np.int64)
+        sizes = nx * ny
+        offsets = np.zeros(B, np.int64)
+        offsets[1:] = np.cumsum(sizes)[:-1]
+        total = int(sizes.sum())
+        stamps = np.zeros(B, dtype=_lib.STAMP_DTYPE)
+        stamps['N'] = N
+        stamps['Nk'] = Nk
+        stamps['xmin'] = xmin
+        stamps['ymin'] = ymin
+        stamps['nx'] = nx
+        stamps['ny'] = ny
+        stamps['out_offset'] = offsets
+        tdt = torch.float32 if dtype == _lib.F32 else torch.float64
+        if add_to is not None:
+            out = add_to
+        else:
+            out = torch.empty(max(total, 1), dtype=tdt, device=dev)
+        flux = torch.empty(B, dtype=torch.float64, device=dev)
+        perm = torch.from_numpy(order).to(dev)
+        lv = self.d_leaves.view(B, L * _lib.LEAF_DTYPE.itemsize).index_select(0, perm).contiguous()
+        ph = (_lib.to_device(np.stack(self.bld.phases, axis=1)[order]) if self.bld.phases else None)
+        sc = (_lib.to_device(np.stack(self.bld.scales, axis=1)[order]) if self.bld.scales else None)
+        st = _lib.to_device(stamps[order])
+        flux_sorted = torch.empty(B, dtype=torch.float64, device=dev)
+        Ns = N[order]
+        bounds = np.flatnonzero(np.diff(Ns)) + 1
+        starts = np.concatenate([[0], bounds])
+        ends = np.concatenate([bounds, [B]])
+        stream = _lib.Device.stream()
+        lib = _lib.lib()
+        for s0, s1 in zip(starts, ends):
+            n = int(s1 - s0)
+            NN = int(Ns[s0])
+            wbytes = lib.gsb_draw_workspace_size(NN, n, precision)
+            work = torch.empty(max(int(wbytes), 8), dtype=torch.uint8, device=dev) if wbytes else None
+            _lib.check(lib.gsb_draw_images(
+                ctypes.byref(self.tpl), n, ctypes.byref(self.gsp_c),
+                ctypes.c_void_p(lv.data_ptr() + int(s0) * L * _lib.LEAF_DTYPE.itemsize),
+                ctypes.c_void_p(ph.data_ptr() + int(s0) * len(self.bld.phases) * 64) if ph is not None else None,
+                ctypes.c_void_p(sc.data_ptr() + int(s0) * len(self.bld.scales) * 8) if sc is not None else None,
+                ctypes.c_void_p(st.data_ptr() + int(s0) * _lib.STAMP_DTYPE.itemsize),
+                self.tables.handle if self.tables else None,
+                _lib.ptr(out), dtype, 1 if add_to is not None else 0,
+                ctypes.c_void_p(flux_sorted.data_ptr() + int(s0) * 8),
+                precision, _lib.ptr(work), ctypes.c_size_t(int(wbytes)), stream))
+        flux[perm] = flux_sorted
+        return out, offsets, flux
+
+    def draw_kimage(self, dk, kxmin, kymin, nkx, nky, dtype):
+        """Evaluate the program on a k grid; returns a host complex array (B, nky, nkx)."""
+        import torch
+        self.prepare()
+        dev = _lib.Device.torch_device()
+        tdt = torch.float32 if dtype == _lib.F32 else torch.float64
+        out = torch.empty(self.B * nkx * nky * 2, dtype=tdt, device=dev)
+        ph = _lib.to_device(np.stack(self.bld.phases, axis=1)) if self.bld.phases else None
+        sc = _lib.to_device(np.stack(self.bld.scales, axis=1)) if self.bld.scales else None
+        _lib.check(_lib.lib().gsb_draw_kimages(
+            ctypes.byref(self.tpl), self.B, ctypes.byref(self.gsp_c), _lib.ptr(self.d_leaves),
+            _lib.ptr(ph) if ph is not None else None, _lib.ptr(sc) if sc is not None else None,
+            self.tables.handle if self.tables else None, float(dk), int(kxmin), int(kymin),
+            int(nkx), int(nky), _lib.ptr(out), dtype, _lib.Device.stream()))
+        a = out.cpu().numpy().reshape(self.B, nky, nkx, 2)
+        cdt = np.complex64 if dtype == _lib.F32 else np.complex128
+        return (a[..., 0] + 1j * a[..., 1]).astype(cdt)
+
+
+# ---- GalSim-exact sizing helpers (gsobject.py:1900-1963) -------------------------------------
+_GOOD_SIZES = np.array(sorted(set([2 ** a for a in range(1, 31)] + [3 * 2 ** a for a in range(1, 30)])),
+                       dtype=np.float64)
+
+
+def good_fft_size_array(n):
+    """goodFFTSize (src/Image.cpp:1141-1153) vectorised: the smallest 2^a or 3*2^a (>= 6) that is
+    >= (1 - 1e-5) n, and 2 for n <= 2."""
+    n = np.asarray(n, np.int64)
+    insize = (1. - 1.e-5) * n.astype(np.float64)
+    idx = np.searchsorted(_GOOD_SIZES, insize, side='left')
+    out = _GOOD_SIZES[np.minimum(idx, len(_GOOD_SIZES) - 1)].astype(np.int64)
+    return np.where(n <= 2, 2, out)
+
+
+def good_image_size(stepk, pixel_scale):
+    """getGoodImageSize (gsobject.py:1900-1925), per stamp."""
+    stepk = np.atleast_1d(np.asarray(stepk, np.float64))
+    Nd = 2. * math.pi / (pixel_scale * stepk)
+    N = np.ceil(Nd * (1. - 1.e-12)).astype(np.int64)
+    return 2 * ((N + 1) // 2)
+
+
+def fft_sizes(stepk, maxk, xmin, xmax, ymin, ymax, gsparams, scale=1.0):
+    """(N, Nk) per stamp as in drawFFT_makeKImage (gsobject.py:1927-1963).  (xmin..ymax) are
+    the bounds of each stamp's centred image view."""
+    stepk = np.atleast_1d(np.asarray(stepk, np.float64))
+    maxk = np.atleast_1d(np.asarray(maxk, np.float64))
+    xmin, xmax, ymin, ymax = [np.broadcast_to(np.asarray(v, np.int64), stepk.shape)
+                              for v in (xmin, xmax, ymin, ymax)]
+    N = good_image_size(stepk, scale)
+    absmax = np.max(np.abs(np.stack([xmin, xmax, ymin, ymax])), axis=0)
+    image_N = np.maximum(absmax * 2, np.maximum(ymax - ymin + 1, xmax - xmin + 1))
+    N = np.maximum(N, image_N)
+    N = good_fft_size_array(N)
+    N = np.maximum(N, gsparams.minimum_fft_size)
+    dk = 2. * np.pi / (N * scale)
+    Nk = np.where(N * dk / 2 > maxk, N, np.ceil(maxk / dk).astype(np.int64) * 2)
+    big = Nk > gsparams.maximum_fft_size
+    if np.any(big):
+        galsim_warn_fft("drawFFT requires a very large FFT.", int(Nk[big].max()))
+    return N.astype(np.int64), Nk.astype(np.int64)

@@ -1,0 +1,201 @@
+/*
+ * gsb.h -- C ABI of the B200 FFT drawing path (libgsb.so).
+ *
+ * The reference binds its drawing path through the pybind11 module `_galsim`
+ * (pysrc/module.cpp:63-111).  This library replaces the calls that
+ * GSObject.drawFFT / drawKImage make through that module (galsim/gsobject.py:1927-2045,
+ * 2464-2582) with batched CUDA kernels for sm_100a.  Every entry point:
+ *   - is `extern "C"`, takes plain pointers and sizes, and never aborts;
+ *   - returns 0 (GSB_OK) on success or a negative GSB_ERR_* code, with a message
+ *     available from gsb_last_error() (reference: SBError / ImageError turned into
+ *     RuntimeError by pybind11, include/galsim/SBProfile.h:49-52, include/galsim/Image.h:65-82);
+ *   - takes the CUDA stream to launch on as a `void*` (a cudaStream_t, NULL = default stream);
+ *   - reads and writes device memory that the caller owns, except the FT tables, which
+ *     live in a gsb_tables object created and destroyed through this API.
+ *
+ * Units follow the reference: every profile is drawn in image coordinates (pixel = 1) after
+ * the world-to-image transform, and k-space images have spacing dk = 2 pi / N.
+ */
+#ifndef GSB_H
+#define GSB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GSB_OK                0
+#define GSB_ERR_INVALID      -1   /* bad argument (size, pointer, parameter range) */
+#define GSB_ERR_CUDA         -2   /* a CUDA call failed */
+#define GSB_ERR_UNSUPPORTED  -3   /* valid in the reference but not built here */
+#define GSB_ERR_NUMERIC      -4   /* a root finder or integral did not converge */
+
+#define GSB_MAX_OPS     32
+#define GSB_MAX_LEAVES   8
+#define GSB_MAX_PHASES   8
+#define GSB_MAX_SCALES   8
+
+/* Leaf profile types (reference: src/SB{Gaussian,Exponential,Sersic,Moffat,Kolmogorov,Airy,Box}.cpp). */
+enum {
+    GSB_GAUSSIAN    = 0,   /* p = {sigma}                                  */
+    GSB_EXPONENTIAL = 1,   /* p = {r0}                                     */
+    GSB_SERSIC      = 2,   /* p = {n, r0 or hlr (GSB_LEAF_SIZE_IS_HLR), trunc} */
+    GSB_MOFFAT      = 3,   /* p = {beta, r0, trunc}                        */
+    GSB_KOLMOGOROV  = 4,   /* p = {lam_over_r0}                            */
+    GSB_AIRY        = 5,   /* p = {lam_over_diam, obscuration}             */
+    GSB_BOX         = 6    /* p = {width, height}                          */
+};
+
+/* Program opcodes.  A program is evaluated per k-point on a small stack of complex values:
+ *   LEAF i   push leaf i's kValue at (A kx + C ky, B kx + D ky)        (SBProfile::drawK)
+ *   MUL      pop b, a; push a*b                                  (Convolution._drawKImage)
+ *   ADD      pop b, a; push a+b                                          (Sum._drawKImage)
+ *   PHASE i  top *= fs * exp(-i (kx' cx + ky' cy)), k' from phase i's Jacobian
+ *                                                   (ApplyKImagePhases, transform.py:597-599)
+ *   SCALE i  top *= scale[i]                                         (transform.py:600-601) */
+enum { GSB_OP_LEAF = 1, GSB_OP_MUL = 2, GSB_OP_ADD = 3, GSB_OP_PHASE = 4, GSB_OP_SCALE = 5 };
+
+/* gsb_leaf.flags */
+#define GSB_LEAF_JAC_GENERAL   1  /* Jacobian has off-diagonal terms: the reference's 2-d
+                                     fillKImage rules apply (clipping differs, see
+                                     SBGaussian.cpp:194-260, SBExponential.cpp:442-510) */
+#define GSB_LEAF_SIZE_IS_HLR   2  /* Sersic p[1] is a half-light radius (sersic.py:224-227) */
+
+/* gsb_phase.flags */
+#define GSB_PHASE_JAC_GENERAL  1
+
+/* Accuracy / size parameters, same meaning and order as the reference's GSParams
+ * (include/galsim/GSParams.h:96-108, galsim/gsparams.py:127-135). */
+typedef struct gsb_gsparams {
+    int    minimum_fft_size;
+    int    maximum_fft_size;
+    double folding_threshold;
+    double stepk_minimum_hlr;
+    double maxk_threshold;
+    double kvalue_accuracy;
+    double xvalue_accuracy;
+    double table_spacing;
+    double realspace_relerr;
+    double realspace_abserr;
+    double integration_relerr;
+    double integration_abserr;
+    double shoot_accuracy;
+} gsb_gsparams;
+
+/* Topology shared by every stamp of a batch: the flattened profile tree. */
+typedef struct gsb_template {
+    int n_ops;
+    int n_leaves;
+    int n_phases;
+    int n_scales;
+    int op_code[GSB_MAX_OPS];
+    int op_arg[GSB_MAX_OPS];
+    int leaf_type[GSB_MAX_LEAVES];
+} gsb_template;
+
+/* One leaf of one stamp (device memory, stamp-major: leaves[s * n_leaves + l]). */
+typedef struct gsb_leaf {
+    double jac[4];     /* composed Jacobian [A, B, C, D] (row-major 2x2, transform.py:593) */
+    double flux;
+    double p[3];       /* profile parameters, see the type enum */
+    double d[8];       /* derived values, written by gsb_prepare_leaves */
+    int32_t flags;     /* GSB_LEAF_* */
+    int32_t table;     /* FT table slot (Sersic), set by the caller */
+} gsb_leaf;
+
+/* One phase / flux factor of one stamp (stamp-major: phases[s * n_phases + i]). */
+typedef struct gsb_phase {
+    double jac[4];     /* Jacobian of the enclosing transforms (the `jac` argument of
+                          Transformation._drawKImage, transform.py:592) */
+    double cenx, ceny; /* shift of the Transformation */
+    double flux_scaling;
+    int32_t flags;     /* GSB_PHASE_* */
+    int32_t pad;
+} gsb_phase;
+
+/* Geometry of one stamp (stamp-major). */
+typedef struct gsb_stamp {
+    int32_t N;         /* FFT size (wrap size), even; gsobject.py:1938-1955 */
+    int32_t Nk;        /* k-evaluation size, even, >= N; gsobject.py:1957-1963 */
+    int32_t xmin, ymin;/* stamp bounds relative to the profile centre (image view after
+                          `imview._shift(-image.center)`, gsobject.py:1776) */
+    int32_t nx, ny;
+    int64_t out_offset;/* element offset of the stamp's (xmin, ymin) pixel in the output */
+} gsb_stamp;
+
+/* Output dtypes */
+enum { GSB_F32 = 0, GSB_F64 = 1 };
+
+typedef struct gsb_tables gsb_tables;   /* opaque: device-resident FT tables */
+
+/* ------------------------------------------------------------------------------------ */
+const char* gsb_last_error(void);
+int gsb_version(void);
+
+/* Select the CUDA device for this thread and build the Ogata node tables on it. */
+int gsb_init(int device);
+
+/* Smallest 2^a or 3*2^a >= input (and >= 2).  Reference: goodFFTSize,
+ * src/Image.cpp:1141-1153, bound at pysrc/Image.cpp:82. */
+int gsb_good_fft_size(int input);
+
+/* FT tables ---------------------------------------------------------------------------- */
+int gsb_tables_create(gsb_tables** out);
+int gsb_tables_destroy(gsb_tables* t);
+
+/* Build `count` Sersic FT tables in FP64 on the device, slots 0..count-1 (replacing any
+ * earlier content).  Per slot: the Hankel-transform table on a uniform ln k grid with its
+ * natural-spline coefficients, the low-k quartic and high-k asymptote, maxk, stepk and the
+ * half-light radius in units of r0.  Reference: SersicInfo (src/SBSersic.cpp:301-667),
+ * hankel_inf (src/math/Hankel.cpp:231-249), TSpline (src/Table.cpp:553-686).
+ * h_n / h_trunc_over_r0 are host arrays.  Truncated profiles (trunc > 0) are not built. */
+int gsb_sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc_over_r0,
+                            int count, const gsb_gsparams* gsp, void* stream);
+
+/* Copy slot headers back (16 doubles per slot: see gsb_tables.cu) for inspection. */
+int gsb_sersic_tables_info(const gsb_tables* t, double* h_out, int count, void* stream);
+
+/* Leaves -------------------------------------------------------------------------------- */
+/* Fill the derived values of every leaf and write its stepk and maxk (d_info[2*(s*L+l)]).
+ * Reference: the leaf constructors and stepK()/maxK() (SBGaussian.cpp:55-89,
+ * SBExponential.cpp:65-92 and 513-554, SBSersic.cpp:71-90 and 301-324,
+ * SBMoffat.cpp:163-244 and 481-549, SBKolmogorov.cpp:84-100 and 338-420,
+ * SBAiry.cpp:66-81 and 332-445, SBBox.cpp:40-60) and the Python overrides
+ * (gaussian.py:148-155, exponential.py:131-132, kolmogorov.py:281-284, airy.py:217-219,
+ * box.py:100-106).  Sersic leaves must already name a built table slot. */
+int gsb_prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp,
+                       gsb_leaf* d_leaves, const gsb_tables* t, double* d_info, void* stream);
+
+/* Drawing -------------------------------------------------------------------------------- */
+/* Scratch bytes gsb_draw_images needs for a bucket of stamps that all have FFT size N. */
+size_t gsb_draw_workspace_size(int N, int n_stamps, int precision);
+
+/* drawImage(method='fft') for a bucket of stamps that share one FFT size N:
+ * k-space evaluation of the program at the Nk x Nk grid points, Hermitian wrap onto N,
+ * c2r inverse FFT, crop into the stamp, cast, optional add, and the stamp's flux sum.
+ * Reference: drawFFT_makeKImage / _drawKImage / drawFFT_finish (gsobject.py:1927-2045)
+ * with wrapImage (src/Image.cpp:578-727) and irfft (src/Image.cpp:815-912).
+ * precision: GSB_F32 or GSB_F64 arithmetic.  d_added_flux (may be NULL): per stamp,
+ * the compensated sum of the drawn pixels (gsobject.py:2011). */
+int gsb_draw_images(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp,
+                    const gsb_leaf* d_leaves, const gsb_phase* d_phases, const double* d_scales,
+                    const gsb_stamp* d_stamps, const gsb_tables* t,
+                    void* d_out, int out_dtype, int add_to_image, double* d_added_flux,
+                    int precision, void* d_workspace, size_t workspace_bytes, void* stream);
+
+/* drawKImage: evaluate the program on an (nkx x nky) grid of k points
+ * kx = (kxmin + i) dk, ky = (kymin + j) dk, into complex output (interleaved re, im) with
+ * row stride nkx.  One grid per stamp, stamp s at d_out + s * nkx * nky complex elements.
+ * Reference: GSObject.drawKImage / _drawKImage (gsobject.py:2464-2582). */
+int gsb_draw_kimages(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp,
+                     const gsb_leaf* d_leaves, const gsb_phase* d_phases, const double* d_scales,
+                     const gsb_tables* t, double dk, int kxmin, int kymin, int nkx, int nky,
+                     void* d_out, int out_dtype, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GSB_H */

@@ -1,0 +1,1031 @@
+"""ORACLE: FP64 numpy restatement of the reference's FFT drawing path.
+
+TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline may import this module, and only as the checker; nothing in galsim_b200/ uses it.
+
+It restates, in double precision and with its own tree classes (independent of the
+product's host code), the reference algorithm of
+    GSObject.drawImage(method='fft' | 'no_pixel')    galsim/gsobject.py:1283-1844
+    drawFFT_makeKImage / drawFFT_finish / drawFFT    galsim/gsobject.py:1900-2045
+    drawKImage                                       galsim/gsobject.py:2464-2582
+    Convolution / Sum / Transformation _drawKImage   convolve.py:420-426, sum.py:341-347,
+                                                     transform.py:592-602
+    SBProfile::drawK + per-profile fillKImage        src/SBProfile.cpp:383-588 and
+                                                     src/SB{Gaussian,Exponential,Sersic,Moffat,
+                                                     Kolmogorov,Airy,Box}.cpp
+    ApplyKImagePhases                                src/SBTransform.cpp:740-883
+    wrapImage (hermx)                                src/Image.cpp:395-727 (pointer walk restated)
+    irfft(shift_in, shift_out)                       src/Image.cpp:815-912 (FFTW c2r -> numpy)
+    goodFFTSize                                      src/Image.cpp:1141-1153
+    SersicInfo (HLR, missing flux, FT table)         src/SBSersic.cpp:301-667
+    hankel_inf (Ogata 2005, adaptive h)              src/math/Hankel.cpp:79-249
+    natural cubic spline                             src/Table.cpp:553-686
+    KolmogorovInfo stepk                             src/SBKolmogorov.cpp:338-420
+    Moffat kValue / maxK / stepK                     src/SBMoffat.cpp:163-549
+Special functions come from scipy (kv, j0, j1, y0, gammainc, gamma).  Its results are pinned
+against fixtures made by the reference itself (tests/golden/).
+"""
+import math
+
+import numpy as np
+from scipy import special
+
+PI = math.pi
+
+
+# ---------------------------------------------------------------------------------------------
+# GSParams
+# ---------------------------------------------------------------------------------------------
+class OGSParams(object):
+    def __init__(self, minimum_fft_size=128, maximum_fft_size=8192, folding_threshold=5.e-3,
+                 stepk_minimum_hlr=5, maxk_threshold=1.e-3, kvalue_accuracy=1.e-5,
+                 xvalue_accuracy=1.e-5, table_spacing=1, realspace_relerr=1.e-4,
+                 realspace_abserr=1.e-6, integration_relerr=1.e-6, integration_abserr=1.e-8,
+                 shoot_accuracy=1.e-5):
+        self.minimum_fft_size = minimum_fft_size
+        self.maximum_fft_size = maximum_fft_size
+        self.folding_threshold = folding_threshold
+        self.stepk_minimum_hlr = stepk_minimum_hlr
+        self.maxk_threshold = maxk_threshold
+        self.kvalue_accuracy = kvalue_accuracy
+        self.xvalue_accuracy = xvalue_accuracy
+        self.table_spacing = table_spacing
+        self.integration_relerr = integration_relerr
+        self.integration_abserr = integration_abserr
+        self.shoot_accuracy = shoot_accuracy
+
+
+DEFAULT = OGSParams()
+
+
+# ---------------------------------------------------------------------------------------------
+# Root finding: Brent with the reference's bracket expansion (include/galsim/Solve.h)
+# ---------------------------------------------------------------------------------------------
+def _zbrent(f, a, b, fa, fb, xtol=1e-7, max_steps=40):
+    if (fa > 0 and fb > 0) or (fa < 0 and fb < 0):
+        raise ValueError("root not bracketed")
+    c, fc = b, fb
+    d = e = b - a
+    for _ in range(max_steps + 1):
+        if (fb > 0 and fc > 0) or (fb < 0 and fc < 0):
+            c, fc = a, fa
+            e = d = b - a
+        if abs(fc) < abs(fb):
+            a, b, c = b, c, b
+            fa, fb, fc = fb, fc, fb
+        tol1 = 2. * np.finfo(float).eps * abs(b) + 0.5 * xtol
+        xm = 0.5 * (c - b)
+        if abs(xm) <= tol1 or fb == 0.:
+            return b
+        if abs(e) >= tol1 and abs(fa) > abs(fb):
+            s = fb / fa
+            if a == c:
+                p = 2. * xm * s
+                q = 1. - s
+            else:
+                q = fa / fc
+                r = fb / fc
+                p = s * (2. * xm * q * (q - r) - (b - a) * (r - 1.))
+                q = (q - 1.) * (r - 1.) * (s - 1.)
+            if p > 0:
+                q = -q
+            p = abs(p)
+            if 2. * p < min(3. * xm * q - abs(tol1 * q), abs(e * q)):
+                e = d
+                d = p / q
+            else:
+                d = xm
+                e = d
+        else:
+            d = xm
+            e = d
+        a, fa = b, fb
+        b += d if abs(d) > tol1 else (abs(tol1) if xm >= 0 else -abs(tol1))
+        fb = f(b)
+    raise RuntimeError("zbrent did not converge")
+
+
+def solve_upper(f, lo, hi):
+    flo, fhi = f(lo), f(hi)
+    delta = hi - lo
+    for _ in range(1, 40):
+        if flo * fhi <= 0:
+            break
+        lo, flo = hi, fhi
+        delta *= 2.
+        hi += delta
+        fhi = f(hi)
+    return _zbrent(f, lo, hi, flo, fhi)
+
+
+def solve_lower_limit(f, lo, hi, limit):
+    fa, fb = f(hi), f(lo)
+    a, b = hi, lo
+    for _ in range(1, 40):
+        if fa * fb <= 0:
+            break
+        bma, cmb = b - a, limit - b
+        a, fa = b, fb
+        b = (2. * limit / cmb + a / bma) / (2. / cmb + 1. / bma)
+        fb = f(b)
+    return _zbrent(f, b, a, fb, fa)
+
+
+# ---------------------------------------------------------------------------------------------
+# Ogata Hankel transform (src/math/Hankel.cpp)
+# ---------------------------------------------------------------------------------------------
+_ZEROS = {}
+
+
+def _j0_zeros(n):
+    z = _ZEROS.get('z')
+    if z is None or len(z) < n:
+        s = np.arange(1, max(n, 1024) + 1, dtype=np.float64)
+        beta = (s - 0.25) * PI
+        ib = 1. / (8. * beta)
+        x = beta + ib * (1. + ib * ib * (-124. / 3. + ib * ib * (120928. / 15.)))
+        for _ in range(4):
+            x = x + special.j0(x) / special.j1(x)
+        _ZEROS['z'] = x
+        _ZEROS['c'] = special.y0(x) / special.j1(x)
+    return _ZEROS['z'][:n], _ZEROS['c'][:n]
+
+
+_NODES = {}
+
+
+def _ogata_nodes(h):
+    key = h
+    if key not in _NODES:
+        nmax = int(min(PI / h, 1e6))
+        z, c = _j0_zeros(nmax)
+        t = h * z / PI
+        with np.errstate(over='ignore'):
+            psi = t * np.tanh(0.5 * PI * np.sinh(t))
+            ch = np.cosh(0.5 * PI * np.sinh(t))
+            dpsi = t * 0.5 * PI * np.cosh(t) / (ch * ch) + psi / t
+        x = PI / h * psi
+        w = c * PI * x * special.j0(x) * dpsi
+        _NODES[key] = (x, w)
+    return _NODES[key]
+
+
+def _ogata_sum(f, k, h):
+    x, w = _ogata_nodes(h)
+    terms = w * f(x / k)
+    cs = np.cumsum(terms)
+    stop = np.flatnonzero(np.abs(terms) < 1e-15 * np.abs(cs))
+    ans = cs[stop[0]] if len(stop) else cs[-1]
+    return ans / (k * k)
+
+
+def hankel_inf(f, k, relerr, abserr):
+    """AdaptiveHankelIntegrator::integrate (Hankel.cpp:179-219)."""
+    h0 = 1. / 32.
+    while h0 > 100. * k:
+        h0 *= 0.5
+    ans0 = _ogata_sum(f, k, h0)
+    h1 = 0.5 * h0
+    ans1 = _ogata_sum(f, k, h1)
+    err = abs(ans1 - ans0)
+    while (err > relerr * ans1 and (err > abserr or abs(ans1) > 2 * abs(ans0))) or ans1 == 0.:
+        h0 = h1
+        ans0 = ans1
+        h1 *= 0.5
+        ans1 = _ogata_sum(f, k, h1)
+        err = abs(ans1 - ans0)
+    return ans1
+
+
+# ---------------------------------------------------------------------------------------------
+# Natural cubic spline (src/Table.cpp:553-686)
+# ---------------------------------------------------------------------------------------------
+class Spline(object):
+    def __init__(self, args, vals):
+        self.x = np.asarray(args, float)
+        self.y = np.asarray(vals, float)
+        n = len(self.x)
+        y2 = np.zeros(n)
+        if n == 3:
+            y2[1] = 3. * ((self.y[2] - self.y[1]) / (self.x[2] - self.x[1]) -
+                          (self.y[1] - self.y[0]) / (self.x[1] - self.x[0])) / (self.x[2] - self.x[0])
+        elif n > 3:
+            x, y = self.x, self.y
+            c = np.zeros(n)
+            for i in range(1, n - 1):
+                y2[i] = 6. * ((y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1]))
+            bb = 2. * (x[2] - x[0])
+            for i in range(1, n - 1):
+                y2[i] /= bb
+                if i == n - 2:
+                    break
+                a = x[i + 1] - x[i]
+                c[i - 1] = a / bb
+                bb = 2. * (x[i + 2] - x[i]) - a * c[i - 1]
+                y2[i + 1] -= a * y2[i]
+            for i in range(n - 3, 0, -1):
+                y2[i] -= c[i - 1] * y2[i + 1]
+        self.y2 = y2
+        self.da = (self.x[-1] - self.x[0]) / (n - 1)
+
+    def __call__(self, a):
+        a = np.asarray(a, float)
+        n = len(self.x)
+        i = np.ceil((a - self.x[0]) / self.da).astype(int)
+        i = np.clip(i, 1, n - 1)
+        h = self.x[i] - self.x[i - 1]
+        aa = self.x[i] - a
+        bb = h - aa
+        return (aa * self.y[i - 1] + bb * self.y[i] -
+                (1. / 6.) * aa * bb * ((aa + h) * self.y2[i - 1] + (bb + h) * self.y2[i])) / h
+
+
+# ---------------------------------------------------------------------------------------------
+# Sersic info (src/SBSersic.cpp:301-667)
+# ---------------------------------------------------------------------------------------------
+_SERSIC = {}
+
+
+class SersicInfo(object):
+    def __init__(self, n, gsp):
+        self.n = n
+        self.gsp = gsp
+        self.gamma2n = special.gamma(2 * n)
+        self.b = self._calc_b()
+        self.re = self.b ** n
+        R = self._missing_flux_radius(gsp.folding_threshold)
+        R = max(R, gsp.stepk_minimum_hlr)
+        self.stepk = PI / R
+        self._build_ft()
+
+    def _missing(self, target):
+        twon, gam = 2 * self.n, self.gamma2n
+        return lambda z: (1. - special.gammainc(twon, z)) * gam - target
+
+    def _calc_b(self):
+        n = self.n
+        invn = 1. / n
+        b1 = 2. * n - 1. / 3.
+        b2 = b1 + (8. / 405.) * invn + (46. / 25515.) * invn ** 2 + (131. / 1148175.) * invn ** 3
+        return solve_lower_limit(self._missing(0.5 * self.gamma2n), b1, b2, 0.)
+
+    def _missing_flux_radius(self, frac):
+        n = self.n
+        missing = frac * self.gamma2n
+        z1 = -math.log(missing)
+        if n == 0.5:
+            z = z1
+        else:
+            z = 4. * (n + 1.)
+            t = 2. * n - 1.
+            z2 = z1 + t * math.log(z) + t / z + t * (2. * n - 3.) / (2. * z * z)
+            if z2 > z1 and z2 - z1 < 0.01:
+                z2 = z1 + 0.01
+            elif z2 < z1 and z2 - z1 > -0.01:
+                z2 = z1 - 0.01
+            if z1 < 0.:
+                z1 = self.b
+            z = solve_upper(self._missing(missing), z1, z2)
+        return z ** n
+
+    def _build_ft(self):
+        n, gsp = self.n, self.gsp
+        g2, g4, g6, g8 = (special.gamma(m * n) for m in (2, 4, 6, 8))
+        self.kd2 = -g4 / (4. * g2)
+        self.kd4 = g6 / (64. * g2)
+        kd6 = g8 / (2304. * g2)
+        kmin = (gsp.kvalue_accuracy / kd6) ** (1. / 6.)
+        self.ksq_min = kmin * kmin
+        hankel_norm = n * g2
+        dlogk = gsp.table_spacing * math.sqrt(math.sqrt(gsp.kvalue_accuracy / 10.))
+        f = lambda r: np.exp(-np.power(r, 1. / n))
+        n_fit = 10
+        fit = []
+        sf = skf = sk = sk2 = 0.
+        ksq_max = -1.
+        maxk = kmin
+        found = False
+        n_correct = 0
+        args, vals = [], []
+        a = b = 0.
+        logk = math.log(kmin) - 0.001
+        i = 0
+        while logk < math.log(500.):
+            lk = math.log(kmin) - 0.001 + i * dlogk
+            k = math.exp(lk)
+            ksq = k * k
+            val = hankel_inf(f, k, gsp.integration_relerr, gsp.integration_abserr * hankel_norm) / hankel_norm
+            f0 = val * ksq
+            args.append(lk)
+            vals.append(f0)
+            if abs(val) > gsp.maxk_threshold:
+                maxk = k
+                n_correct = 0
+            else:
+                found = True
+                a = (sf * sk2 - sk * skf) / (n_fit * sk2 - sk * sk)
+                b = (n_fit * skf - sk * sf) / (n_fit * sk2 - sk * sk)
+                if abs(f0 - (a + b / k)) / ksq < gsp.kvalue_accuracy:
+                    n_correct += 1
+                else:
+                    n_correct = 0
+                if n_correct >= 5:
+                    ksq_max = ksq
+                    break
+            inv_k = 1. / k
+            if len(fit) == n_fit:
+                k_back = math.exp(lk - n_fit * dlogk)
+                f_back = fit.pop()
+                ikb = 1. / k_back
+                sf += f0 - f_back
+                skf += f0 * inv_k - f_back * ikb
+                sk += inv_k - ikb
+                sk2 += inv_k * inv_k - ikb * ikb
+            else:
+                sf += f0
+                skf += f0 * inv_k
+                sk += inv_k
+                sk2 += inv_k * inv_k
+            fit.insert(0, f0)
+            i += 1
+            logk = math.log(kmin) - 0.001 + i * dlogk
+        self.spline = Spline(args, vals)
+        if ksq_max <= 0.:
+            ksq_max = math.exp(2. * args[-1])
+        if found:
+            maxk *= math.exp(dlogk)
+        else:
+            a = (sf * sk2 - sk * skf) / (n_fit * sk2 - sk * sk)
+            b = (n_fit * skf - sk * sf) / (n_fit * sk2 - sk * sk)
+            maxk = math.sqrt(a / gsp.maxk_threshold)
+            for _ in range(3):
+                maxk = math.sqrt((a - b / maxk) / gsp.maxk_threshold)
+        self.ksq_max = ksq_max
+        self.highk_a, self.highk_b = a, b
+        self.maxk = maxk
+
+    def kvalue(self, ksq):
+        ksq = np.asarray(ksq, float)
+        out = np.empty_like(ksq)
+        hi = ksq >= self.ksq_max
+        lo = ksq < self.ksq_min
+        mid = ~hi & ~lo
+        out[hi] = (self.highk_a + self.highk_b / np.sqrt(ksq[hi])) / ksq[hi]
+        out[lo] = 1. + ksq[lo] * (self.kd2 + ksq[lo] * self.kd4)
+        out[mid] = self.spline(0.5 * np.log(ksq[mid])) / ksq[mid]
+        return out
+
+
+def sersic_info(n, gsp=DEFAULT):
+    key = (n, id(gsp))
+    if key not in _SERSIC:
+        _SERSIC[key] = SersicInfo(n, gsp)
+    return _SERSIC[key]
+
+
+# ---------------------------------------------------------------------------------------------
+# Kolmogorov stepk (src/SBKolmogorov.cpp:338-420)
+# ---------------------------------------------------------------------------------------------
+_KOLM = {}
+
+
+def kolmogorov_stepk_factor(gsp=DEFAULT):
+    if id(gsp) in _KOLM:
+        return _KOLM[id(gsp)]
+    dlogr = gsp.table_spacing * math.sqrt(math.sqrt(gsp.xvalue_accuracy / 10.))
+    thresh = gsp.shoot_accuracy / (2. * PI)
+    f = lambda k: np.exp(-np.power(k, 5. / 3.))
+    i = 0
+    r1 = F1 = 0.
+    while -3. + i * dlogr < math.log(1.e4):
+        r = math.exp(-3. + i * dlogr)
+        val = hankel_inf(f, r, gsp.integration_relerr, gsp.integration_abserr) / (2. * PI)
+        r1, F1 = r, val
+        if val * r * r / 1.67 < thresh:
+            break
+        i += 1
+    nn = 11. / 3.
+    R = (2. * PI * F1 * r1 ** nn / ((nn - 2.) * gsp.folding_threshold)) ** (1. / (nn - 2.))
+    R = max(R, gsp.stepk_minimum_hlr * 2.992939911888651 * 0.5548101137)
+    _KOLM[id(gsp)] = PI / R
+    return PI / R
+
+
+# ---------------------------------------------------------------------------------------------
+# Clip ranges (src/SBProfile.cpp:508-588)
+# ---------------------------------------------------------------------------------------------
+def range_1d(m, kmax, ksqmax, kx0, dkx, ky):
+    if abs(ky) >= kmax:
+        return m, m
+    dsq = ksqmax - ky * ky
+    if kx0 * kx0 > dsq or (kx0 + m * dkx) ** 2 > dsq:
+        d = math.sqrt(dsq)
+        i1 = math.ceil((-kx0 - d) / dkx)
+        i2 = math.floor((-kx0 + d) / dkx)
+        if i1 > i2:
+            i1, i2 = i2, i1
+        i2 += 1
+        if i2 <= 0 or i1 >= m:
+            return m, m
+        return max(i1, 0), min(i2, m)
+    return 0, m
+
+
+def range_2d(m, kmax, ksqmax, kx0, dkx, ky0, dky):
+    if abs(kx0) > kmax or abs(kx0 + m * dkx) > kmax or abs(ky0) > kmax or abs(ky0 + m + dky) > kmax:
+        a = dkx * dkx + dky * dky
+        b = dkx * kx0 + dky * ky0
+        c = kx0 * kx0 + ky0 * ky0 - ksqmax
+        d = b * b - a * c
+        if d <= 0.:
+            return m, m
+        d = math.sqrt(d)
+        i1 = math.ceil((-b - d) / a)
+        i2 = math.floor((-b + d) / a)
+        if i1 > i2:
+            i1, i2 = i2, i1
+        i2 += 1
+        if i2 <= 0 or i1 >= m:
+            return m, m
+        return max(i1, 0), min(i2, m)
+    return 0, m
+
+
+# ---------------------------------------------------------------------------------------------
+# Profile tree
+# ---------------------------------------------------------------------------------------------
+class OObj(object):
+    gsp = DEFAULT
+
+    def shear(self, g1, g2):
+        gsq = g1 * g1 + g2 * g2
+        m = np.array([[1. + g1, g2], [g2, 1. - g1]]) / math.sqrt(1. - gsq)
+        return OTransform(self, jac=m)
+
+    def shift(self, dx, dy):
+        return OTransform(self, offset=(dx, dy))
+
+    def __mul__(self, s):
+        return OTransform(self, flux_ratio=s)
+
+    __rmul__ = __mul__
+
+    def drawK(self, kimage, xmin, ymin, dk, jac):
+        """Draw into a complex k-image (numpy, [row, col]) whose corner is (xmin, ymin)."""
+        raise NotImplementedError
+
+
+class OLeaf(OObj):
+    axisym_separable = False
+
+    def drawK(self, kimage, xmin, ymin, dk, jac):
+        """SBProfile::drawK (SBProfile.cpp:383-425)."""
+        nrow, m = kimage.shape
+        x0 = xmin * dk
+        y0 = ymin * dk
+        izero = -xmin if xmin < 0 else 0
+        jzero = -ymin if ymin < 0 else 0
+        if jac is None or (jac[0, 1] == 0. and jac[1, 0] == 0.):
+            mA = 1. if jac is None else jac[0, 0]
+            mD = 1. if jac is None else jac[1, 1]
+            self.fill_1d(kimage, x0 * mA, dk * mA, izero, y0 * mD, dk * mD, jzero)
+        else:
+            mA, mB, mC, mD = jac[0, 0], jac[0, 1], jac[1, 0], jac[1, 1]
+            self.fill_2d(kimage, mA * x0 + mC * y0, mA * dk, mC * dk, mB * x0 + mD * y0, mD * dk, mB * dk)
+
+    def fill_1d(self, im, kx0, dkx, izero, ky0, dky, jzero):
+        if izero != 0 or jzero != 0:
+            # FillQuadrant (SBProfile.cpp:434-488)
+            n, m = im.shape
+            m1, n1 = izero, jzero
+            m2, n2 = m - m1 - 1, n - n1 - 1
+            q = np.zeros((max(n1, n2) + 1, max(m1, m2) + 1), dtype=im.dtype)
+            self.fill_1d(q, kx0 if m1 == 0 else 0., dkx, 0, ky0 if n1 == 0 else 0., dky, 0)
+            iq = np.abs(np.arange(m) - m1)
+            jq = np.abs(np.arange(n) - n1)
+            im[...] = q[jq][:, iq]
+            return
+        n, m = im.shape
+        kx = kx0 + np.arange(m) * dkx
+        ky = ky0 + np.arange(n) * dky
+        im[...] = self.kv_1d(kx, ky)
+
+    def kv_1d(self, kx, ky):
+        KX, KY = np.meshgrid(kx, ky)
+        return self.kvalue(KX, KY)
+
+    def fill_2d(self, im, kx0, dkx, dkxy, ky0, dky, dkyx):
+        n, m = im.shape
+        i = np.arange(m)[None, :]
+        j = np.arange(n)[:, None]
+        KX = kx0 + j * dkxy + i * dkx
+        KY = ky0 + j * dky + i * dkyx
+        im[...] = self.kv_2d(KX, KY, kx0, dkx, dkxy, ky0, dky, dkyx, m)
+
+    def kv_2d(self, KX, KY, *grid):
+        return self.kvalue(KX, KY)
+
+    def kvalue(self, kx, ky):
+        raise NotImplementedError
+
+
+class OGaussian(OLeaf):
+    def __init__(self, sigma, flux=1.):
+        self.sigma, self.flux = float(sigma), float(flux)
+
+    def stepk_maxk(self):
+        gsp = self.gsp
+        maxk = math.sqrt(-2. * math.log(gsp.maxk_threshold)) / self.sigma
+        R = max(math.sqrt(-2. * math.log(gsp.folding_threshold)), gsp.stepk_minimum_hlr * 1.1774100225154747)
+        return PI / (R * self.sigma), maxk
+
+    def kv_1d(self, kx, ky):
+        gx = np.exp(-0.5 * (kx * self.sigma) ** 2)
+        gy = np.exp(-0.5 * (ky * self.sigma) ** 2)
+        return self.flux * gy[:, None] * gx[None, :]
+
+    def kv_2d(self, KX, KY, *grid):
+        ksq = (KX ** 2 + KY ** 2) * self.sigma ** 2
+        ksq_max = -2. * math.log(self.gsp.kvalue_accuracy)
+        ksq_min = (self.gsp.kvalue_accuracy * 48.) ** (1. / 3.)
+        out = self.flux * np.exp(-0.5 * ksq)
+        out = np.where(ksq < ksq_min, self.flux * (1. - 0.5 * ksq * (1. - 0.25 * ksq)), out)
+        return np.where(ksq > ksq_max, 0., out)
+
+
+class OExponential(OLeaf):
+    def __init__(self, r0, flux=1.):
+        self.r0, self.flux = float(r0), float(flux)
+
+    def stepk_maxk(self):
+        gsp = self.gsp
+        maxk = gsp.maxk_threshold ** (-1. / 3.) / self.r0
+        logx = math.log(gsp.folding_threshold)
+        R = -logx
+        for _ in range(3):
+            R = math.log(1. + R) - logx
+        R = max(R, gsp.stepk_minimum_hlr * 1.6783469900166605)
+        return PI / R / self.r0, maxk
+
+    def _consts(self):
+        ksq_max = self.gsp.kvalue_accuracy ** (-1. / 1.5) - 1.
+        return ksq_max, math.sqrt(ksq_max)
+
+    def fill_1d(self, im, kx0, dkx, izero, ky0, dky, jzero):
+        if izero != 0 or jzero != 0:
+            return OLeaf.fill_1d(self, im, kx0, dkx, izero, ky0, dky, jzero)
+        n, m = im.shape
+        r0 = self.r0
+        kx0, dkx, ky0, dky = kx0 * r0, dkx * r0, ky0 * r0, dky * r0
+        ksq_max, k_max = self._consts()
+        im[...] = 0.
+        for j in range(n):
+            ky = ky0 + j * dky
+            i1, i2 = range_1d(m, k_max, ksq_max, kx0, dkx, ky)
+            if i1 == m:
+                continue
+            kx = kx0 + np.arange(i1, i2) * dkx
+            ksqp1 = kx * kx + ky * ky + 1.
+            im[j, i1:i2] = self.flux / (ksqp1 * np.sqrt(ksqp1))
+
+    def fill_2d(self, im, kx0, dkx, dkxy, ky0, dky, dkyx):
+        n, m = im.shape
+        r0 = self.r0
+        kx0, dkx, dkxy, ky0, dky, dkyx = (v * r0 for v in (kx0, dkx, dkxy, ky0, dky, dkyx))
+        ksq_max, k_max = self._consts()
+        im[...] = 0.
+        for j in range(n):
+            kxj = kx0 + j * dkxy
+            kyj = ky0 + j * dky
+            i1, i2 = range_2d(m, k_max, ksq_max, kxj, dkx, kyj, dkyx)
+            if i1 == m:
+                continue
+            ii = np.arange(i1, i2)
+            kx = kxj + ii * dkx
+            ky = kyj + ii * dkyx
+            ksqp1 = 1. + kx * kx + ky * ky
+            im[j, i1:i2] = self.flux / (ksqp1 * np.sqrt(ksqp1))
+
+
+class OSersic(OLeaf):
+    def __init__(self, n, r0=None, hlr=None, flux=1.):
+        self.n, self.flux = float(n), float(flux)
+        self.info = sersic_info(self.n, self.gsp)
+        self.r0 = float(r0) if r0 is not None else float(hlr) / self.info.re
+
+    def stepk_maxk(self):
+        return self.info.stepk / self.r0, self.info.maxk / self.r0
+
+    def kvalue(self, kx, ky):
+        ksq = (kx ** 2 + ky ** 2) * self.r0 ** 2
+        return self.flux * self.info.kvalue(ksq)
+
+
+class OMoffat(OLeaf):
+    def __init__(self, beta, r0=None, fwhm=None, hlr=None, flux=1.):
+        self.beta, self.flux = float(beta), float(flux)
+        if fwhm is not None:
+            r0 = fwhm / (2. * math.sqrt(2. ** (1. / self.beta) - 1.))
+        elif hlr is not None:
+            r0 = hlr / math.sqrt(0.5 ** (1. / (1. - self.beta)) - 1.)
+        self.r0 = float(r0)
+        kacc = self.gsp.kvalue_accuracy
+        b = self.beta
+        self.mode, self.nu = 0, b - 1.
+        for val, mode, nu in ((1.5, 1, None), (2., 0, 1.), (2.5, 2, None), (3., 0, 2.), (3.5, 3, None),
+                              (4., 0, 3.)):
+            if abs(b - val) < kacc:
+                self.mode = mode
+                if nu is not None:
+                    self.nu = nu
+                break
+
+    def kv2(self, k):
+        """kV normalised to 1 at k = 0 (SBMoffat.cpp:274-345)."""
+        k = np.asarray(k, float)
+        if self.mode == 1:
+            return np.exp(-k)
+        if self.mode == 2:
+            return np.exp(-k) * (1. + k)
+        if self.mode == 3:
+            return np.exp(-k) * (3. + (3. + k) * k) / 3.
+        nu = self.nu
+        with np.errstate(invalid='ignore', over='ignore'):
+            v = special.kv(nu, k) * np.power(k, nu) * 2. ** (1. - nu) / special.gamma(nu)
+        return np.where(k == 0., 1., v)
+
+    def stepk_maxk(self):
+        gsp = self.gsp
+        b, rD = self.beta, self.r0
+        ksq = solve_upper(lambda q: float(self.kv2(math.sqrt(q))) - gsp.maxk_threshold, 0., 100.)
+        maxk = math.sqrt(ksq) / rD
+        maxR = math.sqrt(gsp.xvalue_accuracy ** (1. / (1. - b)) - 1.) * rD
+        R = gsp.folding_threshold ** (0.5 / (1. - b)) * rD
+        if R > maxR:
+            R = maxR
+        hlr = rD * math.sqrt(0.5 ** (1. / (1. - b)) - 1.)
+        R = max(R, gsp.stepk_minimum_hlr * hlr)
+        return PI / R, maxk
+
+    def kvalue(self, kx, ky):
+        k = np.sqrt(kx ** 2 + ky ** 2) * self.r0
+        return self.flux * self.kv2(k)
+
+
+class OKolmogorov(OLeaf):
+    def __init__(self, lam_over_r0=None, fwhm=None, flux=1.):
+        if fwhm is not None:
+            lam_over_r0 = fwhm / 0.9758634299
+        self.lor0, self.flux = float(lam_over_r0), float(flux)
+        self.k0 = 2.992939911888651 / self.lor0
+
+    def stepk_maxk(self):
+        return kolmogorov_stepk_factor(self.gsp) * self.k0, \
+            (-math.log(self.gsp.kvalue_accuracy)) ** 0.6 * self.k0
+
+    def kvalue(self, kx, ky):
+        ksq = (kx ** 2 + ky ** 2) / self.k0 ** 2
+        return self.flux * np.exp(-np.power(ksq, 5. / 6.))
+
+
+class OAiry(OLeaf):
+    def __init__(self, lam_over_diam, obscuration=0., flux=1.):
+        self.lod, self.obs, self.flux = float(lam_over_diam), float(obscuration), float(flux)
+
+    def stepk_maxk(self):
+        gsp = self.gsp
+        D = 1. / self.lod
+        if self.obs == 0.:
+            R = 1. / (gsp.folding_threshold * 0.5 * PI * PI)
+        else:
+            R = 1. / (gsp.folding_threshold * 0.5 * PI * PI * (1. - self.obs))
+        R = max(R, gsp.stepk_minimum_hlr * 0.5348321477)
+        return PI / R * D, 2. * PI / self.lod
+
+    def kvalue(self, kx, ky):
+        D = 1. / self.lod
+        t = (kx ** 2 + ky ** 2) / (D * PI) ** 2
+        knorm = self.flux / (PI * (1. - self.obs ** 2))
+        return knorm * _airy_k(t, self.obs)
+
+
+def _chord(r, h, rsq, hsq):
+    return np.where(r == 0., 0., rsq * np.arcsin(np.clip(h / np.where(r == 0, 1, r), -1, 1)) -
+                    h * np.sqrt(np.maximum(rsq - hsq, 0.)))
+
+
+def _circ_same(r, rsq, tsq):
+    hsq = np.maximum(rsq - tsq / 4., 0.)
+    h = np.sqrt(hsq)
+    out = 2. * _chord(r, h, rsq, hsq)
+    out = np.where(tsq == 0., PI * rsq, out)
+    return np.where(tsq >= 4. * rsq, 0., out)
+
+
+def _circ_two(r, s, rsq, ssq, tsq):
+    rps = (r + s) ** 2
+    rms = (r - s) ** 2
+    with np.errstate(divide='ignore', invalid='ignore'):
+        hsq = 0.5 * (rsq + ssq) - (tsq * tsq + rps * rms) / (4. * tsq)
+    hsq = np.where(np.isfinite(hsq), np.maximum(hsq, 0.), 0.)
+    h = np.sqrt(hsq)
+    inner = np.where(tsq < rsq - ssq, PI * ssq - _chord(s, h, ssq, hsq) + _chord(r, h, rsq, hsq),
+                     _chord(s, h, ssq, hsq) + _chord(r, h, rsq, hsq))
+    out = np.where(tsq <= rms, PI * ssq, inner)
+    return np.where(tsq >= rps, 0., out)
+
+
+def _airy_k(t, obs):
+    t = np.asarray(t, float)
+    if obs == 0.:
+        hsq = np.clip(1. - t / 4., 0., 1.)
+        h = np.sqrt(hsq)
+        out = 2. * (np.arcsin(h) - h * np.sqrt(1. - hsq))
+        out = np.where(t == 0., PI, out)
+        return np.where(t >= 4., 0., out)
+    return _circ_same(1., 1., t) - 2. * _circ_two(1., obs, 1., obs * obs, t) + _circ_same(obs, obs * obs, t)
+
+
+class OBox(OLeaf):
+    def __init__(self, width, height=None, flux=1.):
+        self.w = float(width)
+        self.h = float(width if height is None else height)
+        self.flux = float(flux)
+
+    def stepk_maxk(self):
+        return PI / max(self.w, self.h), 2. / (self.gsp.maxk_threshold * min(self.w, self.h))
+
+    @staticmethod
+    def _sinc(x):
+        x = np.asarray(x, float)
+        with np.errstate(invalid='ignore', divide='ignore'):
+            v = np.sin(PI * x) / (PI * x)
+        return np.where(np.abs(x) < 1.e-4, 1. - (PI * PI / 6.) * x * x, v)
+
+    def kv_1d(self, kx, ky):
+        sx = self._sinc(kx * self.w / (2. * PI))
+        sy = self._sinc(ky * self.h / (2. * PI))
+        return self.flux * sy[:, None] * sx[None, :]
+
+    def kvalue(self, kx, ky):
+        return self.flux * self._sinc(kx * self.w / (2. * PI)) * self._sinc(ky * self.h / (2. * PI))
+
+
+class OConvolve(OObj):
+    def __init__(self, *objs):
+        self.objs = list(objs)
+
+    def stepk_maxk(self):
+        s = [o.stepk_maxk() for o in self.objs]
+        inv = 0
+        for sk, _ in s:
+            inv = inv + sk ** (-2)
+        return inv ** (-0.5), min(mk for _, mk in s)
+
+    def drawK(self, kimage, xmin, ymin, dk, jac):
+        self.objs[0].drawK(kimage, xmin, ymin, dk, jac)
+        tmp = np.empty_like(kimage)
+        for o in self.objs[1:]:
+            o.drawK(tmp, xmin, ymin, dk, jac)
+            kimage *= tmp
+
+
+class OSum(OObj):
+    def __init__(self, *objs):
+        self.objs = list(objs)
+
+    def stepk_maxk(self):
+        s = [o.stepk_maxk() for o in self.objs]
+        return min(sk for sk, _ in s), max(mk for _, mk in s)
+
+    def drawK(self, kimage, xmin, ymin, dk, jac):
+        self.objs[0].drawK(kimage, xmin, ymin, dk, jac)
+        tmp = np.empty_like(kimage)
+        for o in self.objs[1:]:
+            o.drawK(tmp, xmin, ymin, dk, jac)
+            kimage += tmp
+
+
+class OTransform(OObj):
+    """transform.py:83-604, including the flattening of nested transformations."""
+
+    def __init__(self, obj, jac=None, offset=(0., 0.), flux_ratio=1.):
+        self.jac = None if jac is None else np.asarray(jac, float).reshape(2, 2)
+        self.dx, self.dy = float(offset[0]), float(offset[1])
+        self.flux_ratio = float(flux_ratio)
+        if isinstance(obj, OTransform):
+            if obj.dx != 0. or obj.dy != 0.:
+                if jac is None:
+                    dx1, dy1 = obj.dx, obj.dy
+                else:
+                    dx1 = self.jac[0, 0] * obj.dx + self.jac[0, 1] * obj.dy
+                    dy1 = self.jac[1, 0] * obj.dx + self.jac[1, 1] * obj.dy
+                self.dx += dx1
+                self.dy += dy1
+            if jac is None:
+                self.jac = obj.jac
+            else:
+                self.jac = self.jac if obj.jac is None else self.jac.dot(obj.jac)
+            self.flux_ratio *= obj.flux_ratio
+            self.original = obj.original
+        else:
+            self.original = obj
+
+    def det(self):
+        j = self.jac
+        if j is None:
+            return 1.
+        if j[0, 1] == 0. and j[1, 0] == 0.:
+            return j[0, 0] * j[1, 1]
+        return j[0, 0] * j[1, 1] - j[0, 1] * j[1, 0]
+
+    def stepk_maxk(self):
+        sk, mk = self.original.stepk_maxk()
+        if self.jac is None:
+            major = minor = 1.
+        else:
+            j = self.jac
+            h1 = math.hypot(j[0, 0] + j[1, 1], j[0, 1] - j[1, 0])
+            h2 = math.hypot(j[0, 0] - j[1, 1], j[0, 1] + j[1, 0])
+            major, minor = 0.5 * abs(h1 + h2), 0.5 * abs(h1 - h2)
+        sk = sk / major
+        if self.dx != 0. or self.dy != 0.:
+            sk = PI / (PI / sk + math.hypot(self.dx, self.dy))
+        return sk, mk / minor
+
+    def drawK(self, kimage, xmin, ymin, dk, jac):
+        jac1 = self.jac if jac is None else jac if self.jac is None else jac.dot(self.jac)
+        self.original.drawK(kimage, xmin, ymin, dk, jac1)
+        fs = abs(self.det()) * self.flux_ratio
+        if self.dx != 0. or self.dy != 0.:
+            apply_phases(kimage, xmin, ymin, dk, jac, self.dx, self.dy, fs)
+        elif abs(fs - 1.) > self.original.gsp.kvalue_accuracy:
+            kimage *= fs
+
+
+def apply_phases(kimage, xmin, ymin, dk, jac, cx, cy, fs):
+    """ApplyKImagePhases (SBTransform.cpp:843-883): *= fs exp(-i (kx' cx + ky' cy))."""
+    n, m = kimage.shape
+    kx = (xmin + np.arange(m))[None, :] * dk
+    ky = (ymin + np.arange(n))[:, None] * dk
+    if jac is None:
+        kxp, kyp = kx, ky
+    else:
+        kxp = jac[0, 0] * kx + jac[1, 0] * ky
+        kyp = jac[0, 1] * kx + jac[1, 1] * ky
+    kimage *= fs * np.exp(-1j * (kxp * cx + kyp * cy))
+
+
+# ---------------------------------------------------------------------------------------------
+# Image-level steps
+# ---------------------------------------------------------------------------------------------
+def good_fft_size(n):
+    """goodFFTSize (src/Image.cpp:1141-1153)."""
+    if n <= 2:
+        return 2
+    insize = (1. - 1.e-5) * n
+    log2n = math.log(2.) * math.ceil(math.log(insize) / math.log(2.))
+    log2n3 = math.log(3.) + math.log(2.) * math.ceil((math.log(insize) - math.log(3.)) / math.log(2.))
+    log2n3 = max(log2n3, math.log(6.))
+    return int(math.ceil(math.exp(min(log2n, log2n3)) - 1.e-5))
+
+
+def wrap_hermx(im, ky_min, N):
+    """wrapImage(hermx=True) of a complex k-image whose rows are ky = ky_min.. and columns
+    kx = 0..m-1, onto rows -N/2..N/2-1 and columns 0..N/2; the pointer walk of
+    src/Image.cpp:482-576 and 578-715 restated.  Modifies im in place; returns the subimage."""
+    n, m = im.shape
+    mwrap = N // 2 + 1
+    j1 = -N // 2 - ky_min
+    j2 = j1 + N
+    nwrap = N
+    cj = np.conj
+    mid = (n - 1) // 2
+    for j in range(mid):
+        A = im[j]
+        B = im[n - 1 - j]
+        p1 = p1w = p2 = p2w = mwrap - 1
+        i = mwrap - 1
+        while True:
+            temp = A[p1]
+            A[p1w] += cj(B[p2])
+            B[p2w] += cj(temp)
+            p1 += 1; p2 += 1; p1w -= 1; p2w -= 1; i += 1
+            for _ in range(min(m - i, mwrap - 2)):
+                A[p1w] += cj(B[p2])
+                B[p2w] += cj(A[p1])
+                p1w -= 1; p2w -= 1; p1 += 1; p2 += 1; i += 1
+            if i == m:
+                break
+            A[p1w] += cj(B[p2])
+            B[p2w] += cj(A[p1])
+            for _ in range(min(m - i, mwrap - 1)):
+                A[p1w] += A[p1]
+                B[p2w] += B[p2]
+                p1w += 1; p2w += 1; p1 += 1; p2 += 1; i += 1
+            if i == m:
+                break
+            A[p1w] += A[p1]
+            B[p2w] += B[p2]
+    R = im[mid]
+    p = pw = mwrap - 1
+    i = mwrap - 1
+    while True:
+        for _ in range(min(m - i, mwrap - 1)):
+            R[pw] += cj(R[p])
+            pw -= 1; p += 1; i += 1
+        if i == m:
+            break
+        R[pw] += cj(R[p])
+        for _ in range(min(m - i, mwrap - 1)):
+            R[pw] += R[p]
+            pw += 1; p += 1; i += 1
+        if i == m:
+            break
+        R[pw] += R[p]
+    # rows (non-Hermitian y direction), src/Image.cpp:690-712
+    jj = j2 - (j2 % nwrap)
+    if jj == j2:
+        jj = j1
+    j = 0
+    while j < n:
+        if j == j1:
+            j = j2
+        for _ in range(min(n - j, j2 - jj)):
+            im[jj] += im[j]
+            j += 1
+            jj += 1
+        jj = j1
+    return im[j1:j2, 0:mwrap]
+
+
+def irfft_shifted(kw, N):
+    """irfft(kimage, out, shift_in=True, shift_out=True) (src/Image.cpp:815-912): input rows
+    ky = -N/2..N/2-1, columns kx = 0..N/2; output real image [y, x] for x, y = -N/2..N/2-1."""
+    K = np.concatenate([kw[N // 2:], kw[:N // 2]], axis=0)          # shift_in: ky = 0 first
+    r = np.arange(N)[:, None]
+    i = np.arange(N // 2 + 1)[None, :]
+    K = K * np.where((r + i) % 2 == 0, 1., -1.)                      # shift_out
+    return np.fft.irfft2(K, s=(N, N))                                # includes 1/(Nx Ny)
+
+
+def size_for_image(obj, bounds, gsp=DEFAULT):
+    """drawFFT_makeKImage sizing (gsobject.py:1900-1963) for an image view with the given
+    (centred) bounds (xmin, xmax, ymin, ymax)."""
+    stepk, maxk = obj.stepk_maxk()
+    Nd = 2. * PI / stepk
+    N = int(math.ceil(Nd * (1. - 1.e-12)))
+    N = 2 * ((N + 1) // 2)
+    image_N = max(max(abs(v) for v in bounds) * 2, max(bounds[3] - bounds[2] + 1, bounds[1] - bounds[0] + 1))
+    N = max(N, image_N)
+    N = good_fft_size(N)
+    N = max(N, gsp.minimum_fft_size)
+    dk = 2. * PI / N
+    if N * dk / 2 > maxk:
+        Nk = N
+    else:
+        Nk = int(np.ceil(maxk / dk)) * 2
+    return N, Nk
+
+
+def draw_fft(obj, bounds, gsp=DEFAULT):
+    """drawFFT (gsobject.py:2014-2045) into a float64 image with centred bounds
+    (xmin, xmax, ymin, ymax).  Returns (array[ny, nx], added_flux, N, Nk)."""
+    N, Nk = size_for_image(obj, bounds, gsp)
+    dk = 2. * PI / N
+    kim = np.zeros((Nk + 1, Nk // 2 + 1), dtype=np.complex128)
+    obj.drawK(kim, 0, -Nk // 2, dk, None)
+    kw = wrap_hermx(kim, -Nk // 2, N)
+    real = irfft_shifted(np.array(kw), N)
+    xmin, xmax, ymin, ymax = bounds
+    sub = real[ymin + N // 2:ymax + N // 2 + 1, xmin + N // 2:xmax + N // 2 + 1]
+    return sub.copy(), float(sub.sum(dtype=float)), N, Nk
+
+
+def draw_image(prof, nx, ny, scale, offset=(0., 0.), method='fft', use_true_center=True,
+               gsp=DEFAULT):
+    """drawImage(nx=, ny=, scale=, method='fft' | 'no_pixel', offset=) (gsobject.py:1283-1844)
+    for a world-coordinate profile.  Returns (array, added_flux, N, Nk)."""
+    dx, dy = float(offset[0]), float(offset[1])
+    if use_true_center:
+        if nx % 2 == 0:
+            dx -= 0.5
+        if ny % 2 == 0:
+            dy -= 0.5
+    inv = 1. / scale
+    jac = None if scale == 1. else np.array([[inv, 0.], [0., inv]])
+    img_prof = OTransform(prof, jac=jac, offset=(dx, dy), flux_ratio=scale ** 2)
+    if method == 'fft':
+        img_prof = OConvolve(img_prof, OBox(1.0))
+    # bounds 1..nx, 1..ny shifted by -center
+    cx = 1 + nx // 2
+    cy = 1 + ny // 2
+    bounds = (1 - cx, nx - cx, 1 - cy, ny - cy)
+    return draw_fft(img_prof, bounds, gsp)
+
+
+def draw_kimage(obj, nkx, nky, kxmin, kymin, dk):
+    """_drawKImage on a grid with corner (kxmin, kymin) (gsobject.py:2575-2582)."""
+    kim = np.zeros((nky, nkx), dtype=np.complex128)
+    obj.drawK(kim, kxmin, kymin, dk, None)
+    return kim

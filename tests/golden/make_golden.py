@@ -1,0 +1,152 @@
+"""Make the golden fixtures in tests/golden/ by running the reference GalSim itself.
+
+    make -C oracle ref               # build the reference C++ into oracle/_ref (once)
+    python tests/golden/make_golden.py /path/to/reference
+
+The reference Python package is imported from its checkout with the extension built from
+its own C++ sources (oracle/ref_import.py).  Everything drawn here goes through the
+reference's drawImage / drawKImage / wrap / irfft / stepk / maxk; the fixtures record the
+inputs next to the outputs.  These files are the pin for both the numpy oracle and the GPU
+kernels; the GPU tests read only these .npz files, never the reference checkout.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+
+
+def profile(galsim, spec):
+    """Build a reference object from a plain-data description (shared with the tests)."""
+    kind = spec[0]
+    if kind == 'gauss':
+        return galsim.Gaussian(sigma=spec[1], flux=spec[2])
+    if kind == 'exp':
+        return galsim.Exponential(half_light_radius=spec[1], flux=spec[2])
+    if kind == 'sersic':
+        return galsim.Sersic(n=spec[1], half_light_radius=spec[2], flux=spec[3])
+    if kind == 'moffat':
+        return galsim.Moffat(beta=spec[1], fwhm=spec[2], flux=spec[3])
+    if kind == 'kolmogorov':
+        return galsim.Kolmogorov(fwhm=spec[1], flux=spec[2])
+    if kind == 'airy':
+        return galsim.Airy(lam_over_diam=spec[1], obscuration=spec[2], flux=spec[3])
+    if kind == 'box':
+        return galsim.Box(spec[1], spec[2], flux=spec[3])
+    if kind == 'pixel':
+        return galsim.Pixel(spec[1])
+    if kind == 'shear':
+        return profile(galsim, spec[3]).shear(g1=spec[1], g2=spec[2])
+    if kind == 'shift':
+        return profile(galsim, spec[3]).shift(spec[1], spec[2])
+    if kind == 'dilate':
+        return profile(galsim, spec[2]).dilate(spec[1])
+    if kind == 'rotate':
+        return profile(galsim, spec[2]).rotate(spec[1] * galsim.degrees)
+    if kind == 'scaleflux':
+        return profile(galsim, spec[2]) * spec[1]
+    if kind == 'conv':
+        return galsim.Convolve([profile(galsim, s) for s in spec[1]])
+    if kind == 'sum':
+        return galsim.Add([profile(galsim, s) for s in spec[1]])
+    raise ValueError(kind)
+
+
+# ---- cases ------------------------------------------------------------------------------
+C1 = ('conv', [('shift', 0.13, -0.07, ('shear', 0.05, -0.03, ('exp', 1.0, 1.e4))),
+               ('moffat', 3.0, 0.7, 1.0), ('pixel', 0.2)])
+
+DRAW_CASES = [
+    # (name, spec, nx, ny, scale, dtype, offset)
+    ('c1_exp_moffat_pixel', C1, 64, 64, 0.2, 'f8', (0., 0.)),
+    ('gauss_sheared', ('shear', 0.2, 0.1, ('gauss', 0.8, 100.)), 32, 32, 0.2, 'f8', (0., 0.)),
+    ('gauss_round_odd', ('gauss', 0.5, 10.), 33, 31, 0.25, 'f4', (0.3, -0.2)),
+    ('exp_sheared_shift', ('shift', 0.4, 0.2, ('shear', -0.3, 0.2, ('exp', 0.7, 50.))), 40, 40, 0.2, 'f8', (0., 0.)),
+    ('sersic_25_kolm', ('conv', [('shear', 0.1, -0.25, ('sersic', 2.5, 0.5, 1.e4)),
+                                  ('kolmogorov', 0.75, 1.0), ('pixel', 0.2)]), 48, 48, 0.2, 'f4', (0., 0.)),
+    ('sersic_1_moffat25', ('conv', [('sersic', 1.0, 0.8, 1.e3), ('moffat', 2.5, 0.8, 1.0),
+                                     ('pixel', 0.2)]), 48, 48, 0.2, 'f8', (0.1, 0.05)),
+    ('bulge_disk_moffat_gen', ('conv', [('sum', [('shear', 0.2, 0.1, ('sersic', 4.0, 0.4, 300.)),
+                                                 ('shear', -0.3, 0.2, ('exp', 0.8, 700.))]),
+                                        ('moffat', 3.7, 0.7, 1.0), ('pixel', 0.2)]), 48, 48, 0.2, 'f4', (0., 0.)),
+    ('airy_obsc', ('conv', [('sersic', 0.8, 0.3, 10.), ('airy', 0.1, 0.3, 1.0)]), 40, 40, 0.05, 'f8', (0., 0.)),
+    ('airy_unobsc', ('airy', 0.2, 0.0, 5.), 32, 32, 0.1, 'f8', (0., 0.)),
+    ('box_rotate', ('conv', [('rotate', 30., ('box', 0.6, 0.3, 2.)), ('gauss', 0.3, 1.)]), 32, 32, 0.1, 'f8', (0., 0.)),
+    ('moffat_15_dilate', ('dilate', 1.3, ('moffat', 1.5, 0.9, 20.)), 32, 32, 0.2, 'f8', (0., 0.)),
+    ('moffat_2', ('moffat', 2.0, 0.9, 20.), 32, 32, 0.2, 'f8', (0., 0.)),
+    ('moffat_35_4', ('conv', [('moffat', 3.5, 0.9, 20.), ('moffat', 4.0, 0.5, 1.)]), 32, 32, 0.2, 'f8', (0., 0.)),
+    ('kolm_scaled', ('scaleflux', 3.0, ('kolmogorov', 0.6, 7.)), 32, 32, 0.2, 'f8', (0., 0.)),
+    ('sum_shifted', ('sum', [('shift', 0.5, 0., ('gauss', 0.3, 5.)), ('shift', -0.5, 0.3, ('exp', 0.4, 5.))]),
+     40, 40, 0.15, 'f8', (0., 0.)),
+]
+
+KIMAGE_CASES = [
+    ('k_gauss', ('gauss', 0.8, 3.), 0.3, 21),
+    ('k_gauss_shear', ('shear', 0.2, 0.1, ('gauss', 0.8, 3.)), 0.3, 21),
+    ('k_exp', ('exp', 0.7, 2.), 0.25, 21),
+    ('k_exp_shear_shift', ('shift', 0.2, -0.1, ('shear', 0.3, -0.2, ('exp', 0.7, 2.))), 0.25, 25),
+    ('k_sersic', ('sersic', 3.3, 0.6, 1.), 0.2, 21),
+    ('k_moffat_gen', ('moffat', 2.7, 1.0, 1.), 0.3, 21),
+    ('k_kolm', ('kolmogorov', 0.8, 1.), 0.3, 21),
+    ('k_airy', ('airy', 0.5, 0.2, 1.), 0.5, 21),
+    ('k_box', ('box', 0.5, 0.8, 1.), 0.5, 21),
+]
+
+SIZE_CASES = [('gauss', 0.7, 1.), ('exp', 0.9, 1.), ('moffat', 3.0, 0.7, 1.), ('moffat', 2.5, 0.8, 1.),
+              ('moffat', 3.7, 0.6, 1.), ('moffat', 4.5, 1.0, 1.), ('moffat', 1.5, 0.8, 1.),
+              ('kolmogorov', 0.7, 1.), ('airy', 0.1, 0.3, 1.), ('airy', 0.1, 0.0, 1.),
+              ('box', 0.2, 0.2, 1.)] + \
+             [('sersic', n, 0.5, 1.) for n in (0.5, 0.8, 1.0, 1.5, 2.5, 4.0, 6.0)]
+
+
+def main(ref_root):
+    from ref_import import import_reference_galsim
+    galsim = import_reference_galsim(ref_root)
+    out = {}
+    # drawImage cases
+    for name, spec, nx, ny, scale, dt, off in DRAW_CASES:
+        obj = profile(galsim, spec)
+        im = obj.drawImage(nx=nx, ny=ny, scale=scale, dtype=np.dtype(dt).type, method='fft',
+                           offset=off)
+        out['draw_' + name] = im.array
+        out['draw_' + name + '_flux'] = np.array(im.added_flux)
+    # drawKImage cases (odd-sized grid centred on k = 0, given dk)
+    for name, spec, dk, n in KIMAGE_CASES:
+        obj = profile(galsim, spec)
+        im = obj.drawKImage(nx=n, ny=n, scale=dk)
+        out['kimg_' + name] = im.array
+        out['kimg_' + name + '_xmin'] = np.array([im.bounds.xmin, im.bounds.ymin])
+    # stepk / maxk of leaves
+    sizes = []
+    for spec in SIZE_CASES:
+        obj = profile(galsim, spec)
+        sizes.append((obj.stepk, obj.maxk))
+    out['sizes'] = np.array(sizes)
+    # Sersic scale radii from hlr
+    out['sersic_r0'] = np.array([galsim.Sersic(n=n, half_light_radius=1.).scale_radius
+                                 for n in (0.5, 0.8, 1.0, 1.5, 2.5, 4.0, 6.0)])
+    # goodFFTSize
+    gs = np.arange(1, 3000)
+    out['good_fft_in'] = gs
+    out['good_fft_out'] = np.array([galsim.Image.good_fft_size(int(v)) for v in gs])
+    # wrap + irfft of random Hermitian-layout k-images (image.py:789-796, fft.py)
+    rng = np.random.default_rng(77)
+    for Nk, N in ((16, 8), (20, 8), (12, 12), (24, 12)):
+        kim = galsim.ImageCD((rng.normal(size=(Nk + 1, Nk // 2 + 1)) +
+                              1j * rng.normal(size=(Nk + 1, Nk // 2 + 1))),
+                             xmin=0, ymin=-Nk // 2)
+        out['wrap_in_%d_%d' % (Nk, N)] = kim.array.copy()
+        w = kim.wrap(galsim.BoundsI(0, N // 2, -N // 2, N // 2 - 1), hermitian='x')
+        out['wrap_out_%d_%d' % (Nk, N)] = w.array.copy()
+        real = galsim.Image(galsim.BoundsI(-N // 2, N // 2 + 1, -N // 2, N // 2 - 1), dtype=float)
+        galsim._galsim.irfft(w._image, real._image, True, True)
+        out['irfft_out_%d_%d' % (Nk, N)] = real.array[:, :N].copy()
+    np.savez_compressed(os.path.join(HERE, 'reference_draws.npz'), **out)
+    print('wrote', os.path.join(HERE, 'reference_draws.npz'), len(out), 'arrays')
+
+
+if __name__ == '__main__':
+    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
