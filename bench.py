@@ -1,0 +1,337 @@
+#!/usr/bin/env python
+"""Benchmark of the batched FFT drawing path (stamps/s) on B200.
+
+Workload (the batched-forward configuration): 4096 stamps, seed 1234.  Each stamp is
+Sersic(n ~ U[0.5, 4], hlr lognormal(median 0.5", sigma_ln 0.3), flux lognormal(median 1e4,
+sigma_ln 1)) sheared by g1, g2 ~ N(0, 0.2) clipped to |g| < 0.7, convolved with
+Kolmogorov(fwhm ~ U[0.6, 0.9]") and Pixel(0.2), drawn with drawImage(method='fft') at scale
+0.2 into an automatically sized float32 image, default GSParams (FFT sizes 128/192/256).
+Synthetic parameters; there is no dataset.
+
+One step = the whole device path for the batch: FP64 Sersic FT tables and leaf sizing on the
+GPU, GalSim's integer sizing on the host, and the fused k-space/wrap/FFT/crop kernels.
+`value` is stamps/s with the flattened inputs resident in HBM; `e2e` is the same through
+the public API (galsim_b200.draw_batch) from host parameter arrays to host pixels.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+B_DEFAULT = 4096
+SCALE = 0.2
+
+
+def workload_params(B=B_DEFAULT, seed=1234):
+    """Per-stamp parameters, sampled stamp by stamp in the order n, hlr, flux, g1, g2, psf."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros((B, 6))
+    for i in range(B):
+        n = rng.uniform(0.5, 4.0)
+        hlr = math.exp(math.log(0.5) + 0.3 * rng.normal())
+        flux = math.exp(math.log(1e4) + 1.0 * rng.normal())
+        g1 = rng.normal(0., 0.2)
+        g2 = rng.normal(0., 0.2)
+        g = math.hypot(g1, g2)
+        if g >= 0.7:
+            g1 *= 0.699 / g
+            g2 *= 0.699 / g
+        fwhm = rng.uniform(0.6, 0.9)
+        p[i] = (n, hlr, flux, g1, g2, fwhm)
+    return p
+
+
+def gpu_object(galsim, p):
+    gal = galsim.Sersic(n=p[:, 0], half_light_radius=p[:, 1], flux=p[:, 2]).shear(g1=p[:, 3], g2=p[:, 4])
+    return galsim.Convolve(gal, galsim.Kolmogorov(fwhm=p[:, 5]), galsim.Pixel(SCALE))
+
+
+def algorithmic_bytes(N, nx, ny):
+    """Per-stamp algorithmic bytes of the FFT drawing path at FP32 storage: k-grid write,
+    FFT read, FFT write, fold read, stamp write (8 H + 8 H + 4 N^2 + 4 nx ny + 4 nx ny,
+    H = N (N/2 + 1))."""
+    N = np.asarray(N, np.float64)
+    H = N * (N // 2 + 1)
+    return 16. * H + 4. * N * N + 8. * np.asarray(nx, np.float64) * np.asarray(ny, np.float64)
+
+
+class ClockSampler(object):
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.index), '--query-gpu=' + self.QUERY,
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], 0., set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for l in getattr(self, 'lines', []):
+            f = [x.strip() for x in l.split(',')]
+            try:
+                sm.append(float(f[1]))
+                smax = max(smax, float(f[2]))
+            except (ValueError, IndexError):
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == 'active':
+                    reasons.add(nm)
+        return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': smax or None,
+                'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)['hbm_gbs']), 'measured'
+    return 6650., 'fallback'
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU reference arm: the reference's C++ drawing arithmetic (oracle/_ref/libgsref.so)
+# ---------------------------------------------------------------------------------------------
+def _ref_worker(rows):
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import ref_draw as R
+    out = []
+    for p in rows:
+        n, hlr, flux, g1, g2, fwhm = p
+        prof = R.c2_profile(n, hlr, flux, g1, g2, fwhm, SCALE)
+        t = time.perf_counter()
+        a, f, N, Nk = R.draw_image(prof, None, None, SCALE)
+        out.append(time.perf_counter() - t)
+    return out
+
+
+def cpu_reference_rate(params, budget_s=20., max_stamps=None):
+    """stamps/s of the reference's C++ path on all host cores (one process per core), over a
+    bounded leading sample of the workload sized to ~budget_s of CPU work."""
+    import multiprocessing as mp
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import ref_draw as R
+    if not R.available():
+        return None
+    cores = os.cpu_count() or 1
+    # estimate per-stamp cost on one core with a few stamps
+    t0 = time.perf_counter()
+    per = _ref_worker(params[:4])
+    est = max(np.mean(per), 1e-3)
+    n = int(min(len(params), max(cores, budget_s * cores / est)))
+    if max_stamps:
+        n = min(n, max_stamps)
+    sample = params[:n]
+    chunks = [sample[i::cores] for i in range(cores)]
+    ctx = mp.get_context('spawn')
+    with ctx.Pool(cores) as pool:
+        t = time.perf_counter()
+        pool.map(_ref_worker, chunks)
+        wall = time.perf_counter() - t
+    return {'value': n / wall, 'unit': 'stamps/s', 'cores': cores, 'kind': 'reference',
+            'sample': '%d leading stamps of the 4096-stamp batch (cold Sersic tables, one process '
+                      'per core, reference C++ with an FP64 shim in place of FFTW)' % n}
+
+
+def run_reference(args):
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return
+    params = workload_params()
+    res = cpu_reference_rate(params, budget_s=max(5., 20. / max(args.steps, 1)))
+    if res is None:
+        print(json.dumps({'impl': 'reference', 'unavailable': 'oracle/_ref/libgsref.so is not built'}))
+        return
+    line = {'metric': 'stamps/s', 'value': res['value'], 'unit': 'stamps/s', 'n_gpus': args.gpus,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * B_DEFAULT / res['value'],
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+            'data': 'synthetic', 'impl': 'reference',
+            'config': {'workload': 'sersic_kolmogorov_pixel_4096_seed1234', 'stamps': B_DEFAULT,
+                       'scale': SCALE, 'gsparams': 'default'},
+            'cpu_baseline': res,
+            'e2e': {'value': res['value'], 'unit': 'stamps/s', 'h2d_bytes_per_step': 0,
+                    'd2h_bytes_per_step': 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------------------------
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world > 1:
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    import galsim_b200 as galsim
+    from galsim_b200 import _lib
+    galsim.set_device(local)
+    dev = _lib.Device.torch_device()
+    params = workload_params()
+    obj = gpu_object(galsim, params)
+    plan = galsim.plan_batch(obj, scale=SCALE, dtype=np.float32)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        st = galsim.run_batch(plan)
+    barrier()
+    # L2 note: the working set (tables ~100 MB, stamp outputs ~50 MB, per-CTA W slabs) is
+    # rewritten every step by the table build; inputs are re-read from HBM each step.
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        start.record()
+        for _ in range(args.steps):
+            st = galsim.run_batch(plan)
+        stop.record()
+        barrier()
+    ms = start.elapsed_time(stop) / args.steps
+    t_step = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t_step, op=dist.ReduceOp.MAX)
+    ms = float(t_step.item())
+    B = plan.prog.B
+    value = world * B / (ms * 1e-3)
+
+    # kernel-only timing of the fused draw (dominant kernel) at the sizes of the last step
+    prog = plan.prog
+    N, Nk, nx, ny = st.N, st.Nk, st.nx, st.ny
+    xmin, ymin = st.xmin, st.ymin
+    prog.draw_stamps(N, Nk, xmin, ymin, nx, ny, _lib.F32)
+    torch.cuda.synchronize(dev)
+    nb = len(np.unique(N))
+    ks, ke = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = max(args.steps, 3)
+    ks.record()
+    for _ in range(reps):
+        prog.draw_stamps(N, Nk, xmin, ymin, nx, ny, _lib.F32)
+    ke.record()
+    torch.cuda.synchronize(dev)
+    k_ms = ks.elapsed_time(ke) / reps
+    alg = float(algorithmic_bytes(N, nx, ny).sum())
+    peak, peak_kind = measured_peak_hbm()
+    achieved = alg / (k_ms * 1e-3) / 1e9
+
+    # e2e through the public API: host parameters -> draw_batch -> host pixels
+    barrier()
+    t0 = time.perf_counter()
+    es, ee = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    es.record()
+    for _ in range(args.steps):
+        o = gpu_object(galsim, params)
+        sb = galsim.draw_batch(o, scale=SCALE, dtype=np.float32)
+        pix = sb.flat.cpu()
+        flux = sb.added_flux
+    ee.record()
+    barrier()
+    e2e_ms = es.elapsed_time(ee) / args.steps
+    t_e = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t_e.item())
+    L = prog.L
+    h2d = B * (L * 136 + len(prog.bld.phases) * 64 + len(prog.bld.scales) * 8 + 32)
+    d2h = int(pix.numel() * 4 + B * 8 + B * L * 16)
+
+    # plain one-stamp-per-launch GPU path on a sample (the metric's denominator)
+    n_plain = 64
+    sub = gpu_object(galsim, params[:1])
+    tp0 = torch.cuda.Event(enable_timing=True)
+    tp1 = torch.cuda.Event(enable_timing=True)
+    single_objs = [gpu_object(galsim, params[i:i + 1]) for i in range(n_plain)]
+    for o in single_objs[:3]:
+        galsim.draw_batch(o, scale=SCALE, dtype=np.float32)
+    torch.cuda.synchronize(dev)
+    tp0.record()
+    for o in single_objs:
+        galsim.draw_batch(o, scale=SCALE, dtype=np.float32)
+    tp1.record()
+    torch.cuda.synchronize(dev)
+    plain_rate = n_plain / (tp0.elapsed_time(tp1) * 1e-3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_reference_rate(params, budget_s=15.)
+
+    if rank == 0:
+        line = {
+            'metric': 'stamps/s', 'value': value, 'unit': 'stamps/s', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
+            'data': 'synthetic',
+            'config': {'workload': 'sersic_kolmogorov_pixel_4096_seed1234', 'stamps_per_gpu': B,
+                       'scale': SCALE, 'gsparams': 'default', 'fft_sizes': sorted(set(int(v) for v in N)),
+                       'parallelism': 'replicas x%d' % world,
+                       'l2': 'no flush; per-step table build and stamp outputs exceed L2 reuse'},
+            'e2e': {'value': world * B / (e2e_ms * 1e-3), 'unit': 'stamps/s',
+                    'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': d2h},
+            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                         'frac': achieved / peak, 'traffic': None, 'peak_kind': peak_kind,
+                         'kernel': 'draw_fused_kernel (all FFT-size buckets)',
+                         'kernel_ms': k_ms},
+            'gpu_launches': int(args.steps * (nb + 5)),
+            'plain_one_stamp_per_launch': {'value': plain_rate, 'unit': 'stamps/s', 'sample': n_plain},
+            'clocks': clk.summary(),
+        }
+        if cpu is not None:
+            line['cpu_baseline'] = cpu
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='gsb', choices=['gsb', 'reference'])
+    ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline measurement')
+    args = ap.parse_args()
+    if args.impl == 'reference':
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == '__main__':
+    main()

@@ -19,7 +19,7 @@ from .gsobject import GSObject
 from .profiles import Gaussian, Exponential, Sersic, DeVaucouleurs, Moffat, Kolmogorov, Airy
 from .box import Box, Pixel
 from .compound import Convolve, Convolution, Add, Sum, Transform, Transformation, _Transform
-from .batch import draw_batch, StampBatch
+from .batch import draw_batch, plan_batch, run_batch, StampBatch
 from ._lib import set_device
 
 __version__ = '0.1.0'

@@ -24,8 +24,11 @@ class StampBatch(object):
     ``ymin`` (numpy, per stamp, bounds relative to each stamp's centre), ``N``, ``Nk`` (FFT
     sizes), ``added_flux`` (numpy), ``dtype``."""
 
-    def __init__(self, flat, offsets, nx, ny, xmin, ymin, N, Nk, added_flux, dtype, scale, bounds):
+    def __init__(self, flat, offsets, nx, ny, xmin, ymin, N, Nk, flux_dev, dtype, scale, bounds,
+                 flux_scale=1.):
         self.flat = flat
+        self._flux_dev = flux_dev
+        self._flux_scale = flux_scale
         self.offsets = offsets
         self.nx = nx
         self.ny = ny
@@ -33,10 +36,14 @@ class StampBatch(object):
         self.ymin = ymin
         self.N = N
         self.Nk = Nk
-        self.added_flux = added_flux
         self.dtype = dtype
         self.scale = scale
         self.bounds = bounds
+
+    @property
+    def added_flux(self):
+        """Per-stamp drawn flux / flux_scale (image.added_flux, gsobject.py:1840)."""
+        return self._flux_dev.cpu().numpy() / self._flux_scale
 
     def __len__(self):
         return len(self.offsets)
@@ -71,18 +78,27 @@ class StampBatch(object):
         return out
 
 
-def draw_batch(obj, nx=None, ny=None, scale=None, dtype=np.float32, method='fft', area=1.,
-               exptime=1., gain=1., offset=None, use_true_center=True, precision='fp32',
-               return_device=False):
-    """Draw every stamp of a batched GSObject (or a list of same-topology scalar objects).
+class BatchPlan(object):
+    """A flattened batch ready to be drawn (see draw_batch)."""
 
-    Each stamp is drawn like ``obj_i.drawImage(nx=nx, ny=ny, scale=scale, dtype=dtype,
-    method=method, ...)``; without nx, ny every stamp gets its automatic size
-    (getGoodImageSize).  ``offset`` may be an (B, 2) array.  Returns a StampBatch."""
+    def __init__(self, prog, nx, ny, fixed, flux_scale, dtype, scale, precision):
+        self.prog = prog
+        self.nx = nx
+        self.ny = ny
+        self.fixed = fixed
+        self.flux_scale = flux_scale
+        self.dtype = dtype
+        self.scale = scale
+        self.precision = precision
+
+
+def plan_batch(obj, nx=None, ny=None, scale=None, dtype=np.float32, method='fft', area=1.,
+               exptime=1., gain=1., offset=None, use_true_center=True, precision='fp32'):
+    """Host set-up of draw_batch: drawImage's argument handling and world-to-image transform
+    (gsobject.py:1647-1764) applied to the batched object, flattened into a device program."""
     from . import box, compound
-    from .program import Program, fft_sizes, good_image_size
-    if isinstance(obj, (list, tuple)):
-        obj = stack_objects(obj)
+    from .compound import _Transform
+    from .program import Program
     if method not in ('fft', 'auto', 'no_pixel', 'sb'):
         raise GalSimValueError("draw_batch supports the FFT path only", method,
                                ('fft', 'auto', 'no_pixel', 'sb'))
@@ -98,50 +114,62 @@ def draw_batch(obj, nx=None, ny=None, scale=None, dtype=np.float32, method='fft'
         flux_scale /= gain
     off = np.zeros((B, 2)) if offset is None else np.broadcast_to(np.asarray(offset, float), (B, 2))
     off = off.copy()
-    if nx is not None and use_true_center:
-        # _adjust_offset for even-sized images (gsobject.py:1234-1253)
-        if nx % 2 == 0:
+    if use_true_center:
+        # _adjust_offset (gsobject.py:1234-1253); automatically sized images are even.
+        if nx is None or nx % 2 == 0:
             off[:, 0] -= 0.5
-        if ny % 2 == 0:
+        if ny is None or ny % 2 == 0:
             off[:, 1] -= 0.5
-    from .compound import _Transform
     inv = 1. / scale
     jac = None if scale == 1. else np.array(((inv, 0.), (0., inv)))
-    if nx is None:
-        # Automatic size: needs the stepk of the image-coordinate profile first.
-        prof0 = _Transform(obj, jac, flux_ratio=scale ** 2 * flux_scale, offset=(off[:, 0], off[:, 1]))
-        if method in ('fft', 'auto'):
-            prof0 = compound.Convolve(prof0, box.Pixel(scale=1.0, gsparams=obj.gsparams),
-                                      real_space=False, gsparams=obj.gsparams)
-        sk, _ = Program(prof0).stepk_maxk()
-        Nimg = good_image_size(sk, 1.0)
-        nxs = Nimg.copy()
-        nys = Nimg.copy()
-        # Automatic images are even sized: apply the even-size half-pixel offset per stamp.
-        if use_true_center:
-            off[:, 0] -= 0.5
-            off[:, 1] -= 0.5
-    else:
-        nxs = np.full(B, int(nx), np.int64)
-        nys = np.full(B, int(ny), np.int64)
     prof = _Transform(obj, jac, flux_ratio=scale ** 2 * flux_scale, offset=(off[:, 0], off[:, 1]))
     if method in ('fft', 'auto'):
         prof = compound.Convolve(prof, box.Pixel(scale=1.0, gsparams=obj.gsparams),
                                  real_space=False, gsparams=obj.gsparams)
     prog = Program(prof)
+    prog.upload()
+    return BatchPlan(prog, nx, ny, nx is not None, flux_scale, dtype, scale, precision)
+
+
+def run_batch(plan, recompute=True):
+    """Device part of draw_batch: FP64 tables and leaf sizing, GalSim sizing on the host, and
+    the fused draw kernels.  recompute=False reuses the leaf sizing of an earlier run."""
+    from .program import fft_sizes, good_image_size
+    prog = plan.prog
+    B = prog.B
+    if recompute or not prog._prepared:
+        prog.compute_leaves()
     stepk, maxk = prog.stepk_maxk()
+    if plan.fixed:
+        nxs = np.full(B, int(plan.nx), np.int64)
+        nys = np.full(B, int(plan.ny), np.int64)
+    else:
+        nxs = good_image_size(stepk, 1.0)
+        nys = nxs.copy()
     # Image bounds (1..nx, 1..ny) shifted so that the centre is (0, 0)
-    xmin = 1 - (1 + nxs // 2)
-    ymin = 1 - (1 + nys // 2)
-    xmax = xmin + nxs - 1
-    ymax = ymin + nys - 1
-    N, Nk = fft_sizes(stepk, maxk, xmin, xmax, ymin, ymax, prof.gsparams)
-    dt = _lib.F32 if np.dtype(dtype) == np.float32 else _lib.F64
-    prec = _lib.F64 if precision == 'fp64' else _lib.F32
+    xmin = -(nxs // 2)
+    ymin = -(nys // 2)
+    N, Nk = fft_sizes(stepk, maxk, xmin, xmin + nxs - 1, ymin, ymin + nys - 1, prog.gsparams)
+    dt = _lib.F32 if np.dtype(plan.dtype) == np.float32 else _lib.F64
+    prec = _lib.F64 if plan.precision == 'fp64' else _lib.F32
     flat, offsets, flux = prog.draw_stamps(N, Nk, xmin, ymin, nxs, nys, dt, precision=prec)
-    added = flux.cpu().numpy() / flux_scale
     bounds = [(1, int(x), 1, int(y)) for x, y in zip(nxs, nys)]
-    return StampBatch(flat, offsets, nxs, nys, xmin, ymin, N, Nk, added, dtype, scale, bounds)
+    return StampBatch(flat, offsets, nxs, nys, xmin, ymin, N, Nk, flux, plan.dtype, plan.scale,
+                      bounds, plan.flux_scale)
+
+
+def draw_batch(obj, nx=None, ny=None, scale=None, dtype=np.float32, method='fft', area=1.,
+               exptime=1., gain=1., offset=None, use_true_center=True, precision='fp32'):
+    """Draw every stamp of a batched GSObject.
+
+    Each stamp is drawn like ``obj_i.drawImage(nx=nx, ny=ny, scale=scale, dtype=dtype,
+    method=method, ...)``; without nx, ny every stamp gets its automatic size
+    (getGoodImageSize).  ``offset`` may be a (B, 2) array.  Returns a StampBatch whose pixels
+    stay on the device until read."""
+    if isinstance(obj, (list, tuple)):
+        obj = stack_objects(obj)
+    return run_batch(plan_batch(obj, nx, ny, scale, dtype, method, area, exptime, gain, offset,
+                                use_true_center, precision))
 
 
 def stack_objects(objs):

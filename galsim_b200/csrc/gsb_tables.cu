@@ -236,6 +236,7 @@ __global__ void sersic_finalize_kernel(double* header, int count, int stride, gs
     double4* nd = nodes + (size_t)s * stride;
     const int ncand = int(H[kSH_NCAND]);
     const double front = H[kSH_FRONT], dlogk = H[kSH_DLOGK];
+    if (ncand < 2) { H[kSH_STATUS] = 5; H[kSH_NUSED] = 0; return; }
     const int n_fit = 10;
     double fitbuf[10];
     int fit_size = 0, fit_head = 0;   // ring buffer; head = index of the oldest entry

@@ -118,25 +118,32 @@ class Program(object):
         self._prepared = False
 
     # -- device preparation ------------------------------------------------------------------
-    def prepare(self):
-        """Build FT tables, upload the leaves and compute their stepk / maxk on the GPU."""
-        if self._prepared:
+    def upload(self):
+        """Pack the leaf records, assign Sersic table slots and copy the leaves to the device."""
+        if getattr(self, 'd_leaves', None) is not None:
             return
         import torch
         B, L = self.B, self.L
         leaves = np.stack(self.bld.leaves, axis=1)            # (B, L)
-        self.tables = None
+        self.sersic_n = None
         sersic = [l for l in range(L) if self.bld.leaf_types[l] == _lib.SERSIC]
         if sersic:
             nvals = np.concatenate([leaves[:, l]['p'][:, 0] for l in sersic])
             uniq, inv = np.unique(nvals, return_inverse=True)
-            self.tables = _lib.Tables()
-            self.tables.build_sersic(uniq, self.gsparams)
+            self.sersic_n = uniq
             inv = inv.reshape(len(sersic), B)
             for k, l in enumerate(sersic):
                 leaves['table'][:, l] = inv[k]
         self.d_leaves = _lib.to_device(leaves)
         self.d_info = torch.empty(B * L * 2, dtype=torch.float64, device=_lib.Device.torch_device())
+        self.tables = _lib.Tables() if self.sersic_n is not None else None
+
+    def compute_leaves(self):
+        """FP64 on the GPU: build the Sersic FT tables, then every leaf's derived constants,
+        stepk and maxk; copy stepk / maxk back for the host-side composition."""
+        B, L = self.B, self.L
+        if self.tables is not None:
+            self.tables.build_sersic(self.sersic_n, self.gsparams)
         _lib.check(_lib.lib().gsb_prepare_leaves(
             ctypes.byref(self.tpl), B, ctypes.byref(self.gsp_c), _lib.ptr(self.d_leaves),
             self.tables.handle if self.tables else None, _lib.ptr(self.d_info), _lib.Device.stream()))
@@ -144,6 +151,12 @@ class Program(object):
         self.leaf_stepk = info[:, :, 0]
         self.leaf_maxk = info[:, :, 1]
         self._prepared = True
+
+    def prepare(self):
+        if self._prepared:
+            return
+        self.upload()
+        self.compute_leaves()
 
     def stepk_maxk(self):
         """Composite stepk / maxk per stamp, by the reference's composition rules."""

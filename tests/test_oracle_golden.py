@@ -37,7 +37,9 @@ def test_leaf_sizes_match_reference():
     ref = GOLD['sizes']
     for spec, (sk, mk) in zip(MG.SIZE_CASES, ref):
         s, m = specs.oracle_profile(spec).stepk_maxk()
-        assert abs(s - sk) <= 1e-9 * sk, spec
+        # Kolmogorov's stepk goes through fmath::expd, the reference's approximate exp
+        # (include/galsim/fmath/fmath.hpp:457-478), which moves it at the 1e-8 level.
+        assert abs(s - sk) <= 1e-7 * sk, spec
         assert abs(m - mk) <= 1e-6 * mk, spec
 
 
