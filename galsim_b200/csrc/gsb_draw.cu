@@ -13,8 +13,14 @@ GSB_GROUP(f64_small)
 GSB_GROUP(f64_large)
 #undef GSB_GROUP
 
+bool is_large_fft(int N);
+size_t large_workspace_size(int N, int n_stamps, int precision);
+int draw_large(const DrawArgs& args, int N, int precision, void* work, size_t work_bytes,
+               cudaStream_t stream);
+
 size_t draw_workspace_size(int N, int n_stamps, int precision)
 {
+    if (is_large_fft(N)) return large_workspace_size(N, n_stamps, precision);
     size_t b = 0;
     if (precision == GSB_F64) {
         if (fused_workspace_f64_small(N, n_stamps, &b) || fused_workspace_f64_large(N, n_stamps, &b)) return b;
@@ -46,6 +52,7 @@ int draw_images(const gsb_template* tpl, int n_stamps, const gsb_leaf* d_leaves,
     args.added_flux = d_added_flux;
     args.work = d_work;
     if (n_stamps <= 0) return GSB_OK;
+    if (is_large_fft(N)) return draw_large(args, N, precision, d_work, work_bytes, stream);
     bool handled = false;
     int rc;
     if (precision == GSB_F64) {
@@ -57,7 +64,7 @@ int draw_images(const gsb_template* tpl, int n_stamps, const gsb_leaf* d_leaves,
     }
     if (!handled)
         return set_error(GSB_ERR_UNSUPPORTED, "FFT size " + std::to_string(N) +
-                                              " is not built (supported: 2^a or 3*2^a, 32..1024)");
+                                              " is not built (supported: 2^a or 3*2^a, 32..16384)");
     return rc;
 }
 

@@ -1,0 +1,275 @@
+// Large-FFT drawing path (1024 < N <= 16384): two kernels per chunk of stamps.
+//
+//   large_col_kernel: one CTA per (column group, stamp).  For each column kx = 0..N/2 it
+//     builds the wrapped k-values of all N rows (alias sums of the program, as in the fused
+//     kernel), inverse-transforms them with a block-wide Stockham FFT in shared memory and
+//     stores the column into the stamp's slab W (column-major, coalesced).
+//   large_row_kernel: one CTA per (row pair, stamp).  It gathers two image rows of W,
+//     packs them as one complex row (row1 + i row2, Hermitian-extended in kx), transforms it,
+//     writes the pixels inside the stamp scaled by 1/N^2 and adds the compensated flux sum.
+// The slab W is the only HBM round trip; the chunk size keeps it inside the workspace.
+#include <algorithm>
+#include <map>
+
+#include "gsb_draw.cuh"
+
+namespace gsb {
+
+namespace {
+
+constexpr int kLargeThreads = 1024;
+constexpr int kMaxPerThread = 4;     // supports N / R <= 4096 butterflies per pass, N <= 16384
+
+// Block-wide in-place Stockham FFT of length N (2^a or 3 * 2^a) in shared memory.
+// tw: exp(+2 pi i m / N) for m < N (global, FP64).
+template <typename T, int SIGN>
+__device__ void block_fft(Cx<T>* buf, int N, const double2* __restrict__ tw)
+{
+    int NS = 1;
+    while (NS < N) {
+        const int rem = N / NS;
+        const int R = (NS == 1 && N % 3 == 0) ? 3 : ((rem % 4) == 0 ? 4 : 2);
+        const int NB = N / R;
+        const int tstep = N / (NS * R);
+        Cx<T> v[kMaxPerThread][4];
+#pragma unroll
+        for (int t = 0; t < kMaxPerThread; ++t) {
+            const int b = threadIdx.x + t * blockDim.x;
+            if (b < NB) {
+                const int k = b % NS;
+                for (int r = 0; r < R; ++r) v[t][r] = buf[b + r * NB];
+                for (int r = 1; r < R; ++r) {
+                    const double2 w = __ldg(&tw[(long long)(r * k) * tstep % N]);
+                    v[t][r] = cmul<T>(v[t][r], cx<T>(T(w.x), SIGN > 0 ? T(w.y) : T(-w.y)));
+                }
+                if (R == 4) dft_small<T, 4, SIGN>(v[t]);
+                else if (R == 3) dft_small<T, 3, SIGN>(v[t]);
+                else dft_small<T, 2, SIGN>(v[t]);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int t = 0; t < kMaxPerThread; ++t) {
+            const int b = threadIdx.x + t * blockDim.x;
+            if (b < NB) {
+                const int k = b % NS;
+                const int base = (b / NS) * NS * R + k;
+                for (int r = 0; r < R; ++r) buf[base + r * NS] = v[t][r];
+            }
+        }
+        __syncthreads();
+        NS *= R;
+    }
+}
+
+struct LargeArgs {
+    DrawArgs a;          // leaves/phases/scales/stamps already offset to the chunk
+    int N;
+    const double2* tw;
+    void* W;             // n_stamps slabs of (N/2+1) x N complex
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kLargeThreads) large_col_kernel(LargeArgs la)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    StampSmem& S = *reinterpret_cast<StampSmem*>(smem_raw);
+    Cx<T>* buf = reinterpret_cast<Cx<T>*>(smem_raw + ((sizeof(StampSmem) + 15) & ~size_t(15)));
+    const DrawArgs& a = la.a;
+    const int N = la.N, H = N / 2 + 1;
+    const int s = blockIdx.y;
+    const double dk = 2. * kPi / N;
+    load_stamp(S, a.tpl, s, a.leaves, a.phases, a.scales, a.stamps, a.sersic_header, a.sersic_node,
+               a.sersic_stride, 1. / N);
+    __syncthreads();
+    const int Nk = S.geom.Nk, hk = Nk / 2;
+    const GridRef g{dk, 0, -hk, hk + 1, Nk + 1};
+    Cx<T>* W = reinterpret_cast<Cx<T>*>(la.W) + (size_t)s * H * N;
+    for (int c = blockIdx.x; c < H; c += gridDim.x) {
+        const int alo = ceil_div(-hk - c, N), ahi = floor_div(hk - c, N);
+        for (int r = threadIdx.x; r < N; r += blockDim.x) {
+            const int kyc = r < N / 2 ? r : r - N;
+            const int blo = ceil_div(-hk - kyc, N), bhi = floor_div(hk - kyc, N);
+            Cx<T> acc = cx<T>(T(0), T(0));
+            for (int ia = alo; ia <= ahi; ++ia) {
+                const int kx = c + ia * N;
+                for (int ib = blo; ib <= bhi; ++ib) {
+                    const int ky = kyc + ib * N;
+                    if (kx >= 0) acc = cadd<T>(acc, eval_program<T>(a.tpl, S, dk, kx, ky, g));
+                    else acc = cadd<T>(acc, cconj<T>(eval_program<T>(a.tpl, S, dk, -kx, -ky, g)));
+                }
+            }
+            buf[r] = acc;
+        }
+        __syncthreads();
+        block_fft<T, +1>(buf, N, la.tw);
+        for (int r = threadIdx.x; r < N; r += blockDim.x) W[(size_t)c * N + r] = buf[r];
+        __syncthreads();
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kLargeThreads) large_row_kernel(LargeArgs la)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    StampSmem& S = *reinterpret_cast<StampSmem*>(smem_raw);
+    Cx<T>* buf = reinterpret_cast<Cx<T>*>(smem_raw + ((sizeof(StampSmem) + 15) & ~size_t(15)));
+    const DrawArgs& a = la.a;
+    const int N = la.N, H = N / 2 + 1;
+    const int s = blockIdx.y;
+    if (threadIdx.x == 0) S.geom = a.stamps[s];
+    __syncthreads();
+    const gsb_stamp G = S.geom;
+    const Cx<T>* W = reinterpret_cast<const Cx<T>*>(la.W) + (size_t)s * H * N;
+    const T inv_n2 = T(1) / (T(N) * T(N));
+    const int npairs = (G.ny + 1) / 2;
+    double fsum = 0., fcomp = 0.;
+    for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
+        const int py1 = G.ymin + 2 * p;
+        const bool two = 2 * p + 1 < G.ny;
+        const int y1 = pmod(py1, N), y2 = pmod(py1 + 1, N);
+        for (int kx = threadIdx.x; kx < N; kx += blockDim.x) {
+            Cx<T> a1, a2;
+            if (kx < H) {
+                a1 = W[(size_t)kx * N + y1];
+                a2 = two ? W[(size_t)kx * N + y2] : cx<T>(T(0), T(0));
+            } else {
+                a1 = cconj<T>(W[(size_t)(N - kx) * N + y1]);
+                a2 = two ? cconj<T>(W[(size_t)(N - kx) * N + y2]) : cx<T>(T(0), T(0));
+            }
+            buf[kx] = cx<T>(a1.x - a2.y, a1.y + a2.x);
+        }
+        __syncthreads();
+        block_fft<T, +1>(buf, N, la.tw);
+        const long long row1 = G.out_offset + (long long)(2 * p) * G.nx;
+        for (int i = threadIdx.x; i < G.nx; i += blockDim.x) {
+            const Cx<T> v = buf[pmod(G.xmin + i, N)];
+            const T v1 = v.x * inv_n2;
+            store_pixel<T>(a.out, a.out_dtype, a.add, row1 + i, v1);
+            double x = double(v1), t = fsum + x;
+            fcomp += fabs(fsum) >= fabs(x) ? (fsum - t) + x : (x - t) + fsum;
+            fsum = t;
+            if (two) {
+                const T v2 = v.y * inv_n2;
+                store_pixel<T>(a.out, a.out_dtype, a.add, row1 + G.nx + i, v2);
+                x = double(v2);
+                t = fsum + x;
+                fcomp += fabs(fsum) >= fabs(x) ? (fsum - t) + x : (x - t) + fsum;
+                fsum = t;
+            }
+        }
+        __syncthreads();
+    }
+    if (a.added_flux) {
+        double v = fsum + fcomp;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        __shared__ double part[kLargeThreads / 32];
+        if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += part[w];
+            atomicAdd(&a.added_flux[s], tot);
+        }
+    }
+}
+
+__global__ void twiddle_kernel(double2* tw, int N)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= N) return;
+    double s, c;
+    sincospi(2.0 * m / N, &s, &c);
+    tw[m] = make_double2(c, s);
+}
+
+std::map<int, double2*>& twiddle_cache()
+{
+    static std::map<int, double2*> cache[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return cache[dev & 63];
+}
+
+int twiddles(int N, cudaStream_t stream, const double2** out)
+{
+    auto& c = twiddle_cache();
+    auto it = c.find(N);
+    if (it != c.end()) { *out = it->second; return GSB_OK; }
+    double2* tw = nullptr;
+    GSB_CUDA_CHECK(cudaMalloc(&tw, sizeof(double2) * N));
+    twiddle_kernel<<<(N + 255) / 256, 256, 0, stream>>>(tw, N);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    GSB_CUDA_CHECK(cudaStreamSynchronize(stream));
+    c[N] = tw;
+    *out = tw;
+    return GSB_OK;
+}
+
+template <typename T>
+size_t slab_bytes(int N) { return sizeof(Cx<T>) * (size_t)(N / 2 + 1) * N; }
+
+template <typename T>
+size_t large_smem() { return ((sizeof(StampSmem) + 15) & ~size_t(15)); }
+
+template <typename T>
+int launch_large(const DrawArgs& args, int N, void* work, size_t work_bytes, cudaStream_t stream)
+{
+    const size_t slab = slab_bytes<T>(N);
+    if (!work || work_bytes < slab) return set_error(GSB_ERR_INVALID, "draw workspace too small");
+    const size_t sm = large_smem<T>() + sizeof(Cx<T>) * N;
+    if (sm > kSmemLimit) return set_error(GSB_ERR_UNSUPPORTED, "FFT size too large for this precision");
+    const double2* tw = nullptr;
+    int rc = twiddles(N, stream, &tw);
+    if (rc) return rc;
+    GSB_CUDA_CHECK(cudaFuncSetAttribute(large_col_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    GSB_CUDA_CHECK(cudaFuncSetAttribute(large_row_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    const int chunk = int(std::max<size_t>(1, std::min<size_t>(work_bytes / slab, 65535)));
+    DeviceState* st = device_state();
+    if (args.added_flux)
+        GSB_CUDA_CHECK(cudaMemsetAsync(args.added_flux, 0, sizeof(double) * args.n_stamps, stream));
+    for (int s0 = 0; s0 < args.n_stamps; s0 += chunk) {
+        const int n = std::min(chunk, args.n_stamps - s0);
+        LargeArgs la;
+        la.a = args;
+        la.a.n_stamps = n;
+        la.a.leaves = args.leaves + (size_t)s0 * args.tpl.n_leaves;
+        la.a.phases = args.phases ? args.phases + (size_t)s0 * args.tpl.n_phases : nullptr;
+        la.a.scales = args.scales ? args.scales + (size_t)s0 * args.tpl.n_scales : nullptr;
+        la.a.stamps = args.stamps + s0;
+        la.a.added_flux = args.added_flux ? args.added_flux + s0 : nullptr;
+        la.N = N;
+        la.tw = tw;
+        la.W = work;
+        const int cols = N / 2 + 1;
+        const int gx = std::max(1, std::min(cols, (2 * st->sm_count + n - 1) / n));
+        large_col_kernel<T><<<dim3(gx, n), kLargeThreads, sm, stream>>>(la);
+        GSB_CUDA_CHECK(cudaGetLastError());
+        const int gr = std::max(1, std::min(N / 2, (2 * st->sm_count + n - 1) / n));
+        large_row_kernel<T><<<dim3(gr, n), kLargeThreads, sm, stream>>>(la);
+        GSB_CUDA_CHECK(cudaGetLastError());
+    }
+    return GSB_OK;
+}
+
+}  // namespace
+
+bool is_large_fft(int N) { return N > 1024 && N <= 16384; }
+
+size_t large_workspace_size(int N, int n_stamps, int precision)
+{
+    const size_t slab = precision == GSB_F64 ? slab_bytes<double>(N) : slab_bytes<float>(N);
+    // up to 8 GiB of slabs per chunk, at least one stamp
+    const size_t budget = size_t(8) << 30;
+    const size_t k = std::max<size_t>(1, std::min<size_t>((size_t)n_stamps, budget / slab));
+    return k * slab;
+}
+
+int draw_large(const DrawArgs& args, int N, int precision, void* work, size_t work_bytes,
+               cudaStream_t stream)
+{
+    return precision == GSB_F64 ? launch_large<double>(args, N, work, work_bytes, stream)
+                                : launch_large<float>(args, N, work, work_bytes, stream);
+}
+
+}  // namespace gsb

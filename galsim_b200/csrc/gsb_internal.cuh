@@ -60,7 +60,8 @@ template <typename T>
 __device__ inline T airy_chord(T r, T h, T rsq, T hsq)
 {
     if (r == T(0)) return T(0);
-    return rsq * asin(h / r) - h * sqrt(rsq - hsq);
+    // Clamps keep rounding at the overlap boundaries inside the domains of asin / sqrt.
+    return rsq * asin(fmin(h / r, T(1))) - h * sqrt(fmax(rsq - hsq, T(0)));
 }
 
 template <typename T>
@@ -68,7 +69,7 @@ __device__ inline T airy_circle_same(T r, T rsq, T tsq)
 {
     if (tsq >= T(4) * rsq) return T(0);
     if (tsq == T(0)) return T(kPi) * rsq;
-    const T hsq = rsq - tsq / T(4);
+    const T hsq = fmax(rsq - tsq / T(4), T(0));
     const T h = sqrt(hsq);
     return T(2) * airy_chord<T>(r, h, rsq, hsq);
 }
@@ -80,7 +81,7 @@ __device__ inline T airy_circle_two(T r, T s, T rsq, T ssq, T tsq)
     if (tsq >= rps_sq) return T(0);
     const T rms_sq = (r - s) * (r - s);
     if (tsq <= rms_sq) return T(kPi) * ssq;
-    const T hsq = T(0.5) * (rsq + ssq) - (tsq * tsq + rps_sq * rms_sq) / (T(4) * tsq);
+    const T hsq = fmax(T(0.5) * (rsq + ssq) - (tsq * tsq + rps_sq * rms_sq) / (T(4) * tsq), T(0));
     const T h = sqrt(hsq);
     if (tsq < rsq - ssq)
         return T(kPi) * ssq - airy_chord<T>(s, h, ssq, hsq) + airy_chord<T>(r, h, rsq, hsq);
@@ -93,9 +94,9 @@ __device__ inline T airy_kvalue(T t, T obs, T obssq)
     if (obs == T(0)) {
         if (t >= T(4)) return T(0);
         if (t == T(0)) return T(kPi);
-        const T hsq = T(1) - t / T(4);
+        const T hsq = fmax(T(1) - t / T(4), T(0));
         const T h = sqrt(hsq);
-        return T(2) * (asin(h) - h * sqrt(T(1) - hsq));
+        return T(2) * (asin(fmin(h, T(1))) - h * sqrt(fmax(T(1) - hsq, T(0))));
     }
     return airy_circle_same<T>(T(1), T(1), t) - T(2) * airy_circle_two<T>(T(1), obs, T(1), obssq, t) +
            airy_circle_same<T>(obs, obssq, t);
