@@ -194,6 +194,21 @@ int gsb_draw_kimages(const gsb_template* tpl, int n_stamps, const gsb_gsparams* 
                      const gsb_tables* t, double dk, int kxmin, int kymin, int nkx, int nky,
                      void* d_out, int out_dtype, void* stream);
 
+/* gsb_draw_images without any device allocation.  This entry point has no counterpart in
+ * the reference; it exists for callers that cannot allocate device memory while they draw
+ * (an application that owns a fixed GPU memory budget, or a plugin inside another program's
+ * memory pool).  Same inputs and outputs as gsb_draw_images for one FFT-size bucket, with the
+ * bucket's FFT size N passed explicitly (32 <= N <= 1024, 2^a or 3*2^a).  The scratch that
+ * gsb_draw_images takes from the caller comes instead from a 32 MiB array compiled into the
+ * library (held by every GPU that loads it until exit).  The first call on a device looks up
+ * that array's address and should come before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race, so serialise them on one stream. */
+int gsb_draw_images_noalloc(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp,
+                            const gsb_leaf* d_leaves, const gsb_phase* d_phases,
+                            const double* d_scales, const gsb_stamp* d_stamps,
+                            const gsb_tables* t, int N, void* d_out, int out_dtype,
+                            int add_to_image, double* d_added_flux, int precision, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
