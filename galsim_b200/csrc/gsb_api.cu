@@ -142,6 +142,9 @@ int gsb_tables_destroy(gsb_tables* t)
     cudaFree(t->d_header);
     cudaFree(t->d_node);
     cudaFree(t->d_val);
+    cudaFree(t->d_scan);
+    cudaFree(t->d_n);
+    cudaFree(t->d_status);
     delete t;
     return GSB_OK;
 }

@@ -26,7 +26,7 @@
 namespace gsb {
 
 
-constexpr int kWarps = 8;
+constexpr int kWarps = 16;
 constexpr int kThreads = kWarps * 32;
 
 struct StampSmem {
@@ -38,7 +38,16 @@ struct StampSmem {
     double scale[GSB_MAX_SCALES];
     gsb_stamp geom;
     double flux_part[kWarps];
+    // Per-stamp shared-memory caches (offsets in bytes into the cache area, -1 = not cached):
+    // separable leaf factors X[i], Y[j + Nk/2]; phase factors PX[i], PY[j + Nk/2]; Sersic nodes.
+    int leaf_cache[GSB_MAX_LEAVES];
+    int phase_cache[GSB_MAX_PHASES];
+    int sersic_cache[GSB_MAX_LEAVES];
+    int regstack;      // the program fits the 4-deep register stack
 };
+
+// Bytes of shared memory reserved for the per-stamp caches.
+constexpr int kCacheBytes = 24 * 1024;
 
 struct DrawArgs {
     gsb_template tpl;
@@ -137,6 +146,174 @@ __device__ __noinline__ Cx<T> eval_program(const gsb_template& tpl, const StampS
     return stack[0];
 }
 
+template <typename T> struct NodeT;
+template <> struct NodeT<float> { using type = float4; };
+template <> struct NodeT<double> { using type = double4; };
+
+// Decide which factors of this stamp are cached in shared memory (thread 0), in order:
+// Sersic spline nodes, phase factors, separable leaf factors, until kCacheBytes is used.
+template <typename T>
+__device__ inline void plan_caches(StampSmem& S, const gsb_template& tpl, int Nk)
+{
+    const int hk = Nk / 2;
+    int used = 0;
+    for (int l = 0; l < tpl.n_leaves; ++l) {
+        S.sersic_cache[l] = -1;
+        S.leaf_cache[l] = -1;
+        if (S.leaf[l].type == GSB_SERSIC) {
+            const int bytes = (S.sersic[l].n * (int)sizeof(typename NodeT<T>::type) + 15) & ~15;
+            if (used + bytes <= kCacheBytes) { S.sersic_cache[l] = used; used += bytes; }
+        }
+    }
+    for (int p = 0; p < tpl.n_phases; ++p) {
+        S.phase_cache[p] = -1;
+        const int bytes = ((hk + 1 + Nk + 1) * (int)sizeof(Cx<T>) + 15) & ~15;
+        if (used + bytes <= kCacheBytes) { S.phase_cache[p] = used; used += bytes; }
+    }
+    for (int l = 0; l < tpl.n_leaves; ++l) {
+        const LeafParams& L = S.leaf[l];
+        const bool sep = !(L.flags & GSB_LEAF_JAC_GENERAL) && (L.type == GSB_BOX || L.type == GSB_GAUSSIAN);
+        if (!sep) continue;
+        const int bytes = ((hk + 1 + Nk + 1) * (int)sizeof(T) + 15) & ~15;
+        if (used + bytes <= kCacheBytes) { S.leaf_cache[l] = used; used += bytes; }
+    }
+    int depth = 0, maxd = 0;
+    for (int o = 0; o < tpl.n_ops; ++o) {
+        const int c = tpl.op_code[o];
+        if (c == GSB_OP_LEAF) ++depth;
+        else if (c == GSB_OP_MUL || c == GSB_OP_ADD) --depth;
+        maxd = depth > maxd ? depth : maxd;
+    }
+    S.regstack = maxd <= 4;
+}
+
+// Fill the planned caches (whole block).
+template <typename T>
+__device__ inline void fill_caches(const StampSmem& S, const gsb_template& tpl, unsigned char* cache,
+                                   double dk, int Nk)
+{
+    const int hk = Nk / 2;
+    for (int l = 0; l < tpl.n_leaves; ++l) {
+        if (S.sersic_cache[l] >= 0) {
+            typename NodeT<T>::type* dst = reinterpret_cast<typename NodeT<T>::type*>(cache + S.sersic_cache[l]);
+            const double4* src = S.sersic[l].node;
+            for (int i = threadIdx.x; i < S.sersic[l].n; i += blockDim.x) {
+                const double4 v = src[i];
+                dst[i].x = T(v.x); dst[i].y = T(v.y); dst[i].z = T(v.z); dst[i].w = T(0);
+            }
+        }
+        if (S.leaf_cache[l] >= 0) {
+            const LeafParams& L = S.leaf[l];
+            T* X = reinterpret_cast<T*>(cache + S.leaf_cache[l]);
+            T* Y = X + hk + 1;
+            const bool box = L.type == GSB_BOX;
+            const double ax = L.jac[0] * dk * (box ? L.d[0] : L.d[0]);
+            const double ay = L.jac[3] * dk * (box ? L.d[1] : L.d[0]);
+            for (int i = threadIdx.x; i < hk + 1 + Nk + 1; i += blockDim.x) {
+                const bool isx = i <= hk;
+                const int idx = isx ? i : i - (hk + 1) - hk;
+                const T u = T(idx * (isx ? ax : ay));
+                const T v = box ? sinc_ref<T>(u) : exp(T(-0.5) * u * u);
+                if (isx) X[i] = v; else Y[i - (hk + 1)] = v;
+            }
+        }
+    }
+    for (int p = 0; p < tpl.n_phases; ++p) {
+        if (S.phase_cache[p] < 0) continue;
+        Cx<T>* PX = reinterpret_cast<Cx<T>*>(cache + S.phase_cache[p]);
+        Cx<T>* PY = PX + hk + 1;
+        for (int i = threadIdx.x; i < hk + 1 + Nk + 1; i += blockDim.x) {
+            const bool isx = i <= hk;
+            const int idx = isx ? i : i - (hk + 1) - hk;
+            double tt = idx * (isx ? S.phase_ax[p] : S.phase_ay[p]);
+            tt -= rint(tt);
+            T sn, cs;
+            sincospi(T(-2. * tt), &sn, &cs);
+            if (isx) PX[i] = cx<T>(cs, sn); else PY[i - (hk + 1)] = cx<T>(cs, sn);
+        }
+    }
+}
+
+// Sersic FT from shared-memory nodes (same arithmetic as sersic_kvalue).
+template <typename T>
+__device__ inline T sersic_kvalue_smem(const SersicTableView& tb, const typename NodeT<T>::type* node, T ksq)
+{
+    if (ksq >= T(tb.ksq_max)) return (T(tb.highk_a) + T(tb.highk_b) / sqrt(ksq)) / ksq;
+    if (ksq < T(tb.ksq_min)) return T(1) + ksq * (T(tb.kderiv2) + ksq * T(tb.kderiv4));
+    const T lk = T(0.5) * log(ksq) - T(tb.front);
+    int i = int(ceil(lk / T(tb.da)));
+    if (i >= tb.n) i = tb.n - 1;
+    if (i <= 0) i = 1;
+    const typename NodeT<T>::type n0 = node[i - 1], n1 = node[i];
+    const T h = n1.x - n0.x;
+    const T aa = n1.x - lk;
+    const T bb = h - aa;
+    return (aa * n0.y + bb * n1.y - (T(1) / T(6)) * aa * bb * ((aa + h) * n0.z + (bb + h) * n1.z)) / h / ksq;
+}
+
+// Program evaluation with the caches and a 4-deep register stack (warp-uniform branches).
+template <typename T>
+__device__ __forceinline__ Cx<T> eval_fast(const gsb_template& tpl, const StampSmem& S,
+                                           const unsigned char* cache, double dk, int i, int j,
+                                           const GridRef& g)
+{
+    const int hk = g.n / 2;
+    Cx<T> s0 = cx<T>(T(0), T(0)), s1 = s0, s2 = s0, s3 = s0;
+    int sp = 0;
+    const T kx = T(i * dk), ky = T(j * dk);
+    for (int o = 0; o < tpl.n_ops; ++o) {
+        const int code = tpl.op_code[o], arg = tpl.op_arg[o];
+        if (code == GSB_OP_LEAF) {
+            const LeafParams& L = S.leaf[arg];
+            T v;
+            if (S.leaf_cache[arg] >= 0) {
+                const T* X = reinterpret_cast<const T*>(cache + S.leaf_cache[arg]);
+                v = T(L.flux) * X[i] * X[hk + 1 + j + hk];
+            } else if (S.sersic_cache[arg] >= 0) {
+                const T A = T(L.jac[0]), B = T(L.jac[1]), C = T(L.jac[2]), D = T(L.jac[3]);
+                const T kxp = A * kx + C * ky, kyp = B * kx + D * ky;
+                const T r0 = T(L.d[0]);
+                v = T(L.flux) * sersic_kvalue_smem<T>(
+                        S.sersic[arg], reinterpret_cast<const typename NodeT<T>::type*>(cache + S.sersic_cache[arg]),
+                        (kxp * kxp + kyp * kyp) * r0 * r0);
+            } else {
+                v = leaf_kvalue<T>(L, S.sersic, kx, ky, g, i - g.x0, j - g.y0);
+            }
+            const Cx<T> c = cx<T>(v, T(0));
+            if (sp == 0) s0 = c; else if (sp == 1) s1 = c; else if (sp == 2) s2 = c; else s3 = c;
+            ++sp;
+        } else if (code == GSB_OP_MUL || code == GSB_OP_ADD) {
+            --sp;
+            const bool mul = code == GSB_OP_MUL;
+            if (sp == 1) s0 = mul ? cmul<T>(s0, s1) : cadd<T>(s0, s1);
+            else if (sp == 2) s1 = mul ? cmul<T>(s1, s2) : cadd<T>(s1, s2);
+            else s2 = mul ? cmul<T>(s2, s3) : cadd<T>(s2, s3);
+        } else {
+            Cx<T> f;
+            if (code == GSB_OP_PHASE) {
+                const T fs = T(S.phase[arg].flux_scaling);
+                if (S.phase_cache[arg] >= 0) {
+                    const Cx<T>* PX = reinterpret_cast<const Cx<T>*>(cache + S.phase_cache[arg]);
+                    f = cscale<T>(cmul<T>(PX[i], PX[hk + 1 + j + hk]), fs);
+                } else {
+                    double tt = i * S.phase_ax[arg] + j * S.phase_ay[arg];
+                    tt -= rint(tt);
+                    T sn, cs;
+                    sincospi(T(-2. * tt), &sn, &cs);
+                    f = cx<T>(fs * cs, fs * sn);
+                }
+            } else {
+                f = cx<T>(T(S.scale[arg]), T(0));
+            }
+            if (sp == 1) s0 = cmul<T>(s0, f);
+            else if (sp == 2) s1 = cmul<T>(s1, f);
+            else if (sp == 3) s2 = cmul<T>(s2, f);
+            else s3 = cmul<T>(s3, f);
+        }
+    }
+    return s0;
+}
+
 template <typename T>
 __device__ inline void store_pixel(void* out, int dtype, int add, long long idx, T v)
 {
@@ -163,6 +340,8 @@ __global__ void __launch_bounds__(kThreads) draw_fused_kernel(DrawArgs a)
     off += sizeof(Cx<T>) * N * kWarps;
     Cx<T>* W = WSMEM ? reinterpret_cast<Cx<T>*>(smem_raw + off)
                      : reinterpret_cast<Cx<T>*>(a.work) + (size_t)blockIdx.x * H * WS;
+    if (WSMEM) off += sizeof(Cx<T>) * H * WS;
+    unsigned char* cache = smem_raw + ((off + 15) & ~size_t(15));
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Cx<T>* buf = scratch + warp * N;
@@ -178,6 +357,11 @@ __global__ void __launch_bounds__(kThreads) draw_fused_kernel(DrawArgs a)
         const int Nk = S.geom.Nk;
         const int hk = Nk / 2;
         const GridRef g{dk, 0, -hk, hk + 1, Nk + 1};
+        if (threadIdx.x == 0) plan_caches<T>(S, a.tpl, Nk);
+        __syncthreads();
+        fill_caches<T>(S, a.tpl, cache, dk, Nk);
+        __syncthreads();
+        const bool fast = S.regstack;
 
         // ---- column phase: wrapped k-values, inverse DFT along ky ----
         for (int c = warp; c < H; c += kWarps) {
@@ -190,8 +374,12 @@ __global__ void __launch_bounds__(kThreads) draw_fused_kernel(DrawArgs a)
                     const int kx = c + ia * N;
                     for (int ib = blo; ib <= bhi; ++ib) {
                         const int ky = kyc + ib * N;
-                        if (kx >= 0) acc = cadd<T>(acc, eval_program<T>(a.tpl, S, dk, kx, ky, g));
-                        else acc = cadd<T>(acc, cconj<T>(eval_program<T>(a.tpl, S, dk, -kx, -ky, g)));
+                        const bool pos = kx >= 0;
+                        const int ii = pos ? kx : -kx, jj = pos ? ky : -ky;
+                        Cx<T> v = fast ? eval_fast<T>(a.tpl, S, cache, dk, ii, jj, g)
+                                       : eval_program<T>(a.tpl, S, dk, ii, jj, g);
+                        if (!pos) v = cconj<T>(v);
+                        acc = cadd<T>(acc, v);
                     }
                 }
                 buf[r] = acc;
@@ -294,7 +482,7 @@ constexpr size_t smem_bytes(bool wsmem)
     size_t off = (sizeof(StampSmem) + 15) & ~size_t(15);
     off += sizeof(Cx<T>) * N * (1 + kWarps);
     if (wsmem) off += sizeof(Cx<T>) * (N / 2 + 1) * (N + 1);
-    return off;
+    return ((off + 15) & ~size_t(15)) + kCacheBytes;
 }
 
 constexpr size_t kSmemLimit = 227 * 1024;
@@ -302,8 +490,7 @@ constexpr size_t kSmemLimit = 227 * 1024;
 template <typename T, int N>
 constexpr bool w_fits_smem()
 {
-    return ((sizeof(StampSmem) + 15) & ~size_t(15)) + sizeof(Cx<T>) * N * (1 + kWarps) +
-           sizeof(Cx<T>) * (N / 2 + 1) * (N + 1) <= kSmemLimit;
+    return smem_bytes<T, N>(true) <= kSmemLimit;
 }
 
 template <typename T, int N>

@@ -107,7 +107,7 @@ struct OgataTables {
     int lev_min, lev_max;            // h = 2^-lev for lev in [lev_min, lev_max]
     long long off[32];               // node offset of each level (index lev - lev_min)
     long long cnt[32];               // node count of each level
-    const double2* xw;               // (x, w) per node
+    const double2* xw;               // (log x, w) per node
     const double2* root;             // (j0 zero, Y0(z)/J1(z)) for s = 1..nroot
     long long nroot;
 };
@@ -118,6 +118,7 @@ struct DeviceState {
     int sm_count = 0;
     double2* d_xw = nullptr;
     double2* d_root = nullptr;
+    int* d_status = nullptr;      // status word of gsb_prepare_leaves
     OgataTables og{};
     // Kolmogorov stepk factors cached per GSParams key
     double kolm_key[13] = {0};
@@ -136,5 +137,8 @@ struct gsb_tables {
     double* d_header = nullptr;   // count * kSersicHeader
     double4* d_node = nullptr;    // count * stride
     double* d_val = nullptr;      // scratch: count * stride Hankel values
+    void* d_scan = nullptr;       // scratch: per-slot state of the table's stopping scan
+    double* d_n = nullptr;        // Sersic indices of the slots
+    int* d_status = nullptr;      // convergence status word
     size_t cap_slots = 0, cap_nodes = 0;
 };

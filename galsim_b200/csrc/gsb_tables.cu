@@ -30,13 +30,14 @@ __global__ void ogata_root_kernel(double2* root, long long nroot)
     root[i] = make_double2(z, y0(z) / j1(z));
 }
 
+// Node i of level h: (log x, w) with x = pi/h psi(h xi) and the Ogata weight w.
 __device__ inline double2 ogata_node(const double2* root, double h, long long i)
 {
     const double2 r = root[i];
     const double t = h * r.x / kPi;
     const double x = kPi / h * ogata_psi(t);
     const double w = r.y * kPi * x * j0(x) * ogata_dpsi(t);
-    return make_double2(x, w);
+    return make_double2(log(x), w);
 }
 
 __global__ void ogata_level_kernel(double2* xw, const double2* root, double h, long long n)
@@ -47,7 +48,9 @@ __global__ void ogata_level_kernel(double2* xw, const double2* root, double h, l
 }
 
 // Sum_i w_i f(x_i / k) / k^2 for h = 2^-lev with the reference's stopping rule: stop at the
-// first term whose magnitude is below 1e-15 |running sum| (Hankel.cpp:117-141).
+// first term whose magnitude is below 1e-15 |running sum| (Hankel.cpp:117-141).  The integrand
+// is called with log(x_i / k) = log x_i - log k (nodes store log x), which spares a division
+// and a logarithm per term.
 template <class F>
 __device__ double warp_ogata_sum(const OgataTables& og, const F& f, double k, int lev)
 {
@@ -56,6 +59,7 @@ __device__ double warp_ogata_sum(const OgataTables& og, const F& f, double k, in
     const long long nmax = (long long)fmin(kPi / h, 1e6);
     const bool tab = lev >= og.lev_min && lev <= og.lev_max;
     const double2* xw = tab ? og.xw + og.off[lev - og.lev_min] : nullptr;
+    const double logk = log(k);
     double ans = 0.;
     for (long long base = 0; base < nmax; base += 32) {
         const long long i = base + lane;
@@ -63,7 +67,7 @@ __device__ double warp_ogata_sum(const OgataTables& og, const F& f, double k, in
         double step = 0.;
         if (valid) {
             const double2 n = tab ? xw[i] : ogata_node(og.root, h, i);
-            step = n.y * f(n.x / k);
+            step = n.y * f(n.x - logk);
         }
         double pre = step;
         for (int o = 1; o < 32; o <<= 1) {
@@ -104,13 +108,14 @@ __device__ double warp_hankel(const OgataTables& og, const F& f, double k, doubl
     return ans1;
 }
 
+// Integrands as functions of log r: exp(-r^(1/n)) and exp(-k^(5/3)).
 struct SersicRadial {
     double invn;
-    __device__ double operator()(double r) const { return exp(-pow(r, invn)); }
+    __device__ double operator()(double logr) const { return exp(-exp(logr * invn)); }
 };
 
 struct KolmKValue {
-    __device__ double operator()(double k) const { return exp(-pow(k, 5. / 3.)); }
+    __device__ double operator()(double logk) const { return exp(-exp(logk * (5. / 3.))); }
 };
 
 // (1 - P(2n, z)) Gamma(2n) - target   (SersicMissingFlux, SBSersic.cpp:541-556)
@@ -201,14 +206,38 @@ __global__ void sersic_setup_kernel(const double* n_arr, int count, gsb_gsparams
     H[kSH_STATUS] = status;
 }
 
-// One warp per (slot, node): val = Hankel transform at k_i / hankel_norm.
-__global__ void sersic_nodes_kernel(const double* header, int count, int stride, gsb_gsparams gsp,
-                                    OgataTables og, double* vals, int* status_out)
+// Running state of the serial part of buildFT for one table (SBSersic.cpp:436-509): the
+// maxk bookkeeping and the 10-point high-k least-squares fit, advanced one round of nodes at a
+// time so that nodes past the stopping point are never integrated.
+struct SersicScan {
+    double sf, skf, sk, sk2, maxk, ksq_max, a, b;
+    double fit[10];
+    int fit_size, fit_head, n_correct, found, nused, done;
+};
+
+__global__ void sersic_scan_init_kernel(const double* header, int count, SersicScan* scan)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    SersicScan& S = scan[s];
+    S.sf = S.skf = S.sk = S.sk2 = 0.;
+    S.maxk = sqrt(header[(size_t)s * kSersicHeader + kSH_KSQMIN]);
+    S.ksq_max = -1.;
+    S.a = S.b = 0.;
+    S.fit_size = S.fit_head = S.n_correct = S.found = S.nused = 0;
+    S.done = int(header[(size_t)s * kSersicHeader + kSH_NCAND]) < 2 ? 1 : 0;
+}
+
+// One warp per (slot, node) of this round: val = Hankel transform at k_i / hankel_norm.
+__global__ void sersic_nodes_kernel(const double* header, int count, int stride, int i0, int nround,
+                                    gsb_gsparams gsp, OgataTables og, const SersicScan* scan,
+                                    double* vals, int* status_out)
 {
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-    const long long s = warp / stride;
-    const int i = int(warp % stride);
+    const long long s = warp / nround;
+    const int i = i0 + int(warp % nround);
     if (s >= count) return;
+    if (scan[s].done) return;
     const double* H = header + s * kSersicHeader;
     if (i >= int(H[kSH_NCAND])) return;
     const double n = H[kSH_N];
@@ -225,73 +254,87 @@ __global__ void sersic_nodes_kernel(const double* header, int count, int stride,
     }
 }
 
-// Sequential part of buildFT (SBSersic.cpp:436-527) and the spline (Table.cpp:634-686).
-__global__ void sersic_finalize_kernel(double* header, int count, int stride, gsb_gsparams gsp,
-                                       const double* vals, double4* nodes)
+// Advance each table's scan over this round's nodes (SBSersic.cpp:436-509).
+__global__ void sersic_scan_kernel(const double* header, int count, int stride, int i0, int nround,
+                                   gsb_gsparams gsp, const double* vals, double4* nodes,
+                                   SersicScan* scan)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= count) return;
-    double* H = header + (size_t)s * kSersicHeader;
+    SersicScan& S = scan[s];
+    if (S.done) return;
+    const double* H = header + (size_t)s * kSersicHeader;
     const double* v = vals + (size_t)s * stride;
     double4* nd = nodes + (size_t)s * stride;
     const int ncand = int(H[kSH_NCAND]);
     const double front = H[kSH_FRONT], dlogk = H[kSH_DLOGK];
-    if (ncand < 2) { H[kSH_STATUS] = 5; H[kSH_NUSED] = 0; return; }
     const int n_fit = 10;
-    double fitbuf[10];
-    int fit_size = 0, fit_head = 0;   // ring buffer; head = index of the oldest entry
-    double sf = 0., skf = 0., sk = 0., sk2 = 0.;
-    double ksq_max = -1., maxk = sqrt(H[kSH_KSQMIN]);
-    double a = 0., b = 0.;
-    bool found_maxk = false;
-    int n_correct = 0, nused = 0;
-    for (int i = 0; i < ncand; ++i) {
+    const int iend = min(i0 + nround, ncand);
+    for (int i = i0; i < iend; ++i) {
         const double logk = front + i * dlogk;
         const double k = exp(logk), ksq = k * k;
         const double val = v[i];
         const double f0 = val * ksq;
         nd[i] = make_double4(logk, f0, 0., 0.);
-        nused = i + 1;
-        if (fabs(val) > gsp.maxk_threshold) { maxk = k; n_correct = 0; }
+        S.nused = i + 1;
+        if (fabs(val) > gsp.maxk_threshold) { S.maxk = k; S.n_correct = 0; }
         else {
-            found_maxk = true;
-            a = (sf * sk2 - sk * skf) / (n_fit * sk2 - sk * sk);
-            b = (n_fit * skf - sk * sf) / (n_fit * sk2 - sk * sk);
-            const double f0_pred = a + b / k;
-            if (fabs(f0 - f0_pred) / ksq < gsp.kvalue_accuracy) ++n_correct;
-            else n_correct = 0;
-            if (n_correct >= 5) { ksq_max = ksq; break; }
+            S.found = 1;
+            const double den = n_fit * S.sk2 - S.sk * S.sk;
+            S.a = (S.sf * S.sk2 - S.sk * S.skf) / den;
+            S.b = (n_fit * S.skf - S.sk * S.sf) / den;
+            const double f0_pred = S.a + S.b / k;
+            if (fabs(f0 - f0_pred) / ksq < gsp.kvalue_accuracy) ++S.n_correct;
+            else S.n_correct = 0;
+            if (S.n_correct >= 5) { S.ksq_max = ksq; S.done = 1; return; }
         }
         const double inv_k = 1. / k;
-        if (fit_size == n_fit) {
+        if (S.fit_size == n_fit) {
             const double k_back = exp(logk - n_fit * dlogk);
-            const double f_back = fitbuf[fit_head];
+            const double f_back = S.fit[S.fit_head];
             const double inv_k_back = 1. / k_back;
-            sf += f0 - f_back;
-            skf += f0 * inv_k - f_back * inv_k_back;
-            sk += inv_k - inv_k_back;
-            sk2 += inv_k * inv_k - inv_k_back * inv_k_back;
-            fitbuf[fit_head] = f0;
-            fit_head = (fit_head + 1) % n_fit;
+            S.sf += f0 - f_back;
+            S.skf += f0 * inv_k - f_back * inv_k_back;
+            S.sk += inv_k - inv_k_back;
+            S.sk2 += inv_k * inv_k - inv_k_back * inv_k_back;
+            S.fit[S.fit_head] = f0;
+            S.fit_head = (S.fit_head + 1) % n_fit;
         } else {
-            sf += f0;
-            skf += f0 * inv_k;
-            sk += inv_k;
-            sk2 += inv_k * inv_k;
-            fitbuf[fit_size++] = f0;
+            S.sf += f0;
+            S.skf += f0 * inv_k;
+            S.sk += inv_k;
+            S.sk2 += inv_k * inv_k;
+            S.fit[S.fit_size++] = f0;
         }
     }
-    if (ksq_max <= 0.) ksq_max = exp(2. * nd[nused - 1].x);
-    if (found_maxk) {
+    if (iend >= ncand) S.done = 1;
+}
+
+// End of buildFT (SBSersic.cpp:510-537) and the natural spline (Table.cpp:634-686).
+__global__ void sersic_finalize_kernel(double* header, int count, int stride, gsb_gsparams gsp,
+                                       const SersicScan* scan, double4* nodes)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    double* H = header + (size_t)s * kSersicHeader;
+    double4* nd = nodes + (size_t)s * stride;
+    const SersicScan& S = scan[s];
+    const int N = S.nused;
+    if (N < 2) { H[kSH_STATUS] = 5; H[kSH_NUSED] = 0; return; }
+    const double front = H[kSH_FRONT], dlogk = H[kSH_DLOGK];
+    const int n_fit = 10;
+    double ksq_max = S.ksq_max, maxk = S.maxk, a = S.a, b = S.b;
+    if (ksq_max <= 0.) ksq_max = exp(2. * nd[N - 1].x);
+    if (S.found) {
         maxk *= exp(dlogk);
     } else {
-        a = (sf * sk2 - sk * skf) / (n_fit * sk2 - sk * sk);
-        b = (n_fit * skf - sk * sf) / (n_fit * sk2 - sk * sk);
+        const double den = n_fit * S.sk2 - S.sk * S.sk;
+        a = (S.sf * S.sk2 - S.sk * S.skf) / den;
+        b = (n_fit * S.skf - S.sk * S.sf) / den;
         maxk = sqrt(a / gsp.maxk_threshold);
         for (int it = 0; it < 3; ++it) maxk = sqrt((a - b / maxk) / gsp.maxk_threshold);
     }
     // Natural cubic spline second derivatives (Thomas algorithm), stored in .z
-    const int N = nused;
     for (int i = 0; i < N; ++i) nd[i].z = 0.;
     if (N == 3) {
         nd[1].z = 3. * ((nd[2].y - nd[1].y) / (nd[2].x - nd[1].x) -
@@ -317,7 +360,7 @@ __global__ void sersic_finalize_kernel(double* header, int count, int stride, gs
     const double back = nd[N - 1].x;
     for (int i = 0; i < N; ++i) { nd[i].x -= front; nd[i].w = 0.; }
     H[kSH_NUSED] = N;
-    H[kSH_DA] = N > 1 ? (back - front) / (N - 1) : dlogk;
+    H[kSH_DA] = (back - front) / (N - 1);
     H[kSH_KSQMAX] = ksq_max;
     H[kSH_HIGHA] = a;
     H[kSH_HIGHB] = b;
@@ -502,6 +545,7 @@ __global__ void prepare_leaves_kernel(gsb_template tpl, int n_stamps, gsb_gspara
 
 int ogata_init(DeviceState* st)
 {
+    GSB_CUDA_CHECK(cudaMalloc(&st->d_status, sizeof(int)));
     GSB_CUDA_CHECK(cudaMalloc(&st->d_root, sizeof(double2) * kNroot));
     ogata_root_kernel<<<(unsigned)((kNroot + 255) / 256), 256>>>(st->d_root, kNroot);
     GSB_CUDA_CHECK(cudaGetLastError());
@@ -557,37 +601,48 @@ int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc,
     if (count <= 0) { t->count = 0; return GSB_OK; }
     const int stride = sersic_stride(h_n, count, gsp);
     if ((size_t)count > t->cap_slots || (size_t)count * stride > t->cap_nodes) {
-        cudaFree(t->d_header); cudaFree(t->d_node); cudaFree(t->d_val);
-        t->d_header = nullptr; t->d_node = nullptr; t->d_val = nullptr;
+        cudaFree(t->d_header); cudaFree(t->d_node); cudaFree(t->d_val); cudaFree(t->d_scan);
+        cudaFree(t->d_n); cudaFree(t->d_status);
+        t->d_header = nullptr; t->d_node = nullptr; t->d_val = nullptr; t->d_scan = nullptr;
+        t->d_n = nullptr; t->d_status = nullptr;
         t->cap_slots = std::max<size_t>(count, t->cap_slots);
         t->cap_nodes = std::max<size_t>((size_t)count * stride, t->cap_nodes);
         GSB_CUDA_CHECK(cudaMalloc(&t->d_header, sizeof(double) * kSersicHeader * t->cap_slots));
         GSB_CUDA_CHECK(cudaMalloc(&t->d_node, sizeof(double4) * t->cap_nodes));
         GSB_CUDA_CHECK(cudaMalloc(&t->d_val, sizeof(double) * t->cap_nodes));
+        GSB_CUDA_CHECK(cudaMalloc(&t->d_scan, sizeof(SersicScan) * t->cap_slots));
+        GSB_CUDA_CHECK(cudaMalloc(&t->d_n, sizeof(double) * t->cap_slots));
+        GSB_CUDA_CHECK(cudaMalloc(&t->d_status, sizeof(int)));
     }
     t->count = count;
     t->stride = stride;
-    double* d_n = nullptr;
-    int* d_status = nullptr;
-    GSB_CUDA_CHECK(cudaMallocAsync(&d_n, sizeof(double) * count, stream));
-    GSB_CUDA_CHECK(cudaMallocAsync(&d_status, sizeof(int), stream));
+    double* d_n = t->d_n;
+    int* d_status = t->d_status;
     GSB_CUDA_CHECK(cudaMemcpyAsync(d_n, h_n, sizeof(double) * count, cudaMemcpyHostToDevice, stream));
     GSB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), stream));
     sersic_setup_kernel<<<(count + 127) / 128, 128, 0, stream>>>(d_n, count, *gsp, t->d_header, stride);
     GSB_CUDA_CHECK(cudaGetLastError());
-    const long long nwarps = (long long)count * stride;
-    const int threads = 256;
-    const long long blocks = (nwarps * 32 + threads - 1) / threads;
-    sersic_nodes_kernel<<<(unsigned)blocks, threads, 0, stream>>>(t->d_header, count, stride, *gsp,
-                                                                  st->og, t->d_val, d_status);
+    sersic_scan_init_kernel<<<(count + 127) / 128, 128, 0, stream>>>(t->d_header, count, static_cast<SersicScan*>(t->d_scan));
     GSB_CUDA_CHECK(cudaGetLastError());
+    // Rounds of kRound ln k nodes: integrate, then advance each table's stopping scan.
+    constexpr int kRound = 32;
+    const int threads = 256;
+    for (int i0 = 0; i0 < stride; i0 += kRound) {
+        const long long nwarps = (long long)count * kRound;
+        const long long blocks = (nwarps * 32 + threads - 1) / threads;
+        sersic_nodes_kernel<<<(unsigned)blocks, threads, 0, stream>>>(t->d_header, count, stride, i0, kRound,
+                                                                      *gsp, st->og, static_cast<const SersicScan*>(t->d_scan), t->d_val,
+                                                                      d_status);
+        GSB_CUDA_CHECK(cudaGetLastError());
+        sersic_scan_kernel<<<(count + 63) / 64, 64, 0, stream>>>(t->d_header, count, stride, i0, kRound,
+                                                                 *gsp, t->d_val, t->d_node, static_cast<SersicScan*>(t->d_scan));
+        GSB_CUDA_CHECK(cudaGetLastError());
+    }
     sersic_finalize_kernel<<<(count + 63) / 64, 64, 0, stream>>>(t->d_header, count, stride, *gsp,
-                                                                 t->d_val, t->d_node);
+                                                                 static_cast<const SersicScan*>(t->d_scan), t->d_node);
     GSB_CUDA_CHECK(cudaGetLastError());
     int h_status = 0;
     GSB_CUDA_CHECK(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    GSB_CUDA_CHECK(cudaFreeAsync(d_n, stream));
-    GSB_CUDA_CHECK(cudaFreeAsync(d_status, stream));
     GSB_CUDA_CHECK(cudaStreamSynchronize(stream));
     if (h_status) return set_error(GSB_ERR_NUMERIC, "Sersic Hankel transform did not converge");
     return GSB_OK;
@@ -650,8 +705,7 @@ int prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gs
         const int rc = kolmogorov_stepk(gsp, stream, &kolm);
         if (rc) return rc;
     }
-    int* d_status = nullptr;
-    GSB_CUDA_CHECK(cudaMallocAsync(&d_status, sizeof(int), stream));
+    int* d_status = st->d_status;
     GSB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), stream));
     const long long n = (long long)n_stamps * tpl->n_leaves;
     if (n > 0) {
@@ -661,7 +715,6 @@ int prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gs
     }
     int h_status = 0;
     GSB_CUDA_CHECK(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    GSB_CUDA_CHECK(cudaFreeAsync(d_status, stream));
     GSB_CUDA_CHECK(cudaStreamSynchronize(stream));
     if (h_status & 8) return set_error(GSB_ERR_INVALID, "unknown leaf type");
     if (h_status & 2) return set_error(GSB_ERR_NUMERIC, "Sersic radius root finding failed");
