@@ -241,14 +241,17 @@ __device__ inline T sersic_kvalue_smem(const SersicTableView& tb, const typename
     if (ksq >= T(tb.ksq_max)) return (T(tb.highk_a) + T(tb.highk_b) / sqrt(ksq)) / ksq;
     if (ksq < T(tb.ksq_min)) return T(1) + ksq * (T(tb.kderiv2) + ksq * T(tb.kderiv4));
     const T lk = T(0.5) * log(ksq) - T(tb.front);
-    int i = int(ceil(lk / T(tb.da)));
+    const T inv_da = T(1. / tb.da);
+    int i = int(ceil(lk * inv_da));
     if (i >= tb.n) i = tb.n - 1;
     if (i <= 0) i = 1;
     const typename NodeT<T>::type n0 = node[i - 1], n1 = node[i];
+    // The table is equally spaced (spacing da), so 1/h = 1/da up to rounding.
     const T h = n1.x - n0.x;
     const T aa = n1.x - lk;
     const T bb = h - aa;
-    return (aa * n0.y + bb * n1.y - (T(1) / T(6)) * aa * bb * ((aa + h) * n0.z + (bb + h) * n1.z)) / h / ksq;
+    const T num = aa * n0.y + bb * n1.y - (T(1) / T(6)) * aa * bb * ((aa + h) * n0.z + (bb + h) * n1.z);
+    return num * inv_da / ksq;
 }
 
 // Program evaluation with the caches and a 4-deep register stack (warp-uniform branches).
@@ -260,7 +263,7 @@ __device__ __forceinline__ Cx<T> eval_fast(const gsb_template& tpl, const StampS
     const int hk = g.n / 2;
     Cx<T> s0 = cx<T>(T(0), T(0)), s1 = s0, s2 = s0, s3 = s0;
     int sp = 0;
-    const T kx = T(i * dk), ky = T(j * dk);
+    const T kx = T(i) * T(dk), ky = T(j) * T(dk);
     for (int o = 0; o < tpl.n_ops; ++o) {
         const int code = tpl.op_code[o], arg = tpl.op_arg[o];
         if (code == GSB_OP_LEAF) {
@@ -327,7 +330,7 @@ __device__ inline void store_pixel(void* out, int dtype, int add, long long idx,
 }
 
 template <typename T, int N, bool WSMEM>
-__global__ void __launch_bounds__(kThreads) draw_fused_kernel(DrawArgs a)
+__global__ void __launch_bounds__(kThreads) draw_fused_kernel(const __grid_constant__ DrawArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int H = N / 2 + 1;
@@ -448,7 +451,7 @@ __global__ void __launch_bounds__(kThreads) draw_fused_kernel(DrawArgs a)
 }
 
 template <typename T>
-__global__ void draw_kimage_kernel(gsb_template tpl, int n_stamps, const gsb_leaf* leaves,
+__global__ void draw_kimage_kernel(const __grid_constant__ gsb_template tpl, int n_stamps, const gsb_leaf* leaves,
                                    const gsb_phase* phases, const double* scales,
                                    const double* sh, const double4* snode, int sstride, double dk,
                                    int kxmin, int kymin, int nkx, int nky, void* out, int dtype)

@@ -70,7 +70,7 @@ struct LargeArgs {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(kLargeThreads) large_col_kernel(LargeArgs la)
+__global__ void __launch_bounds__(kLargeThreads) large_col_kernel(const __grid_constant__ LargeArgs la)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     StampSmem& S = *reinterpret_cast<StampSmem*>(smem_raw);
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(kLargeThreads) large_col_kernel(LargeArgs la)
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kLargeThreads) large_row_kernel(LargeArgs la)
+__global__ void __launch_bounds__(kLargeThreads) large_row_kernel(const __grid_constant__ LargeArgs la)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     StampSmem& S = *reinterpret_cast<StampSmem*>(smem_raw);

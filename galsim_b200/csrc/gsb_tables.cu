@@ -229,8 +229,8 @@ __global__ void sersic_scan_init_kernel(const double* header, int count, SersicS
 }
 
 // One warp per (slot, node) of this round: val = Hankel transform at k_i / hankel_norm.
-__global__ void sersic_nodes_kernel(const double* header, int count, int stride, int i0, int nround,
-                                    gsb_gsparams gsp, OgataTables og, const SersicScan* scan,
+__global__ void __launch_bounds__(256, 4) sersic_nodes_kernel(const double* header, int count, int stride, int i0, int nround,
+                                    gsb_gsparams gsp, const __grid_constant__ OgataTables og, const SersicScan* scan,
                                     double* vals, int* status_out)
 {
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
@@ -369,7 +369,7 @@ __global__ void sersic_finalize_kernel(double* header, int count, int stride, gs
 
 // KolmogorovInfo: x-space radial profile by Hankel transform of exp(-k^{5/3}) at
 // r = exp(-3 + i dlogr); only the last tabulated point matters for stepk.
-__global__ void kolmogorov_nodes_kernel(int ncand, double dlogr, gsb_gsparams gsp, OgataTables og,
+__global__ void kolmogorov_nodes_kernel(int ncand, double dlogr, gsb_gsparams gsp, const __grid_constant__ OgataTables og,
                                         double* vals, int* status_out)
 {
     const int i = int((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
@@ -419,7 +419,7 @@ struct MoffatKV2 {
     }
 };
 
-__global__ void prepare_leaves_kernel(gsb_template tpl, int n_stamps, gsb_gsparams gsp,
+__global__ void prepare_leaves_kernel(const __grid_constant__ gsb_template tpl, int n_stamps, gsb_gsparams gsp,
                                       gsb_leaf* leaves, const double* sersic_header,
                                       double kolm_stepk, double* info, int* status_out)
 {
