@@ -188,6 +188,29 @@ def run_reference(args):
 # ---------------------------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------------------------
+def run_stage(args):
+    """Small single-stage runs for profiling (--stage draw | tables): no e2e / CPU legs."""
+    import torch
+    import galsim_b200 as galsim
+    from galsim_b200 import _lib
+    params = workload_params(args.stamps)
+    obj = gpu_object(galsim, params)
+    if args.stage == 'tables':
+        t = _lib.Tables()
+        n = params[:, 0]
+        for _ in range(args.warmup + args.steps):
+            t.build_sersic(n, galsim.GSParams())
+        torch.cuda.synchronize()
+        print(json.dumps({'stage': 'tables', 'tables': len(n)}))
+        return
+    plan = galsim.plan_batch(obj, nx=args.nx, ny=args.nx, scale=SCALE, dtype=np.float32)
+    for _ in range(args.warmup + args.steps):
+        st = galsim.run_batch(plan)
+    torch.cuda.synchronize()
+    u, c = np.unique(st.N, return_counts=True)
+    print(json.dumps({'stage': 'draw', 'stamps': len(st), 'buckets': dict(zip(map(int, u), map(int, c)))}))
+
+
 def run_gpu(args):
     import torch
     import torch.distributed as dist
@@ -201,7 +224,7 @@ def run_gpu(args):
     from galsim_b200 import _lib
     galsim.set_device(local)
     dev = _lib.Device.torch_device()
-    params = workload_params()
+    params = workload_params(args.stamps)
     obj = gpu_object(galsim, params)
     plan = galsim.plan_batch(obj, scale=SCALE, dtype=np.float32)
 
@@ -326,9 +349,15 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='gsb', choices=['gsb', 'reference'])
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline measurement')
+    ap.add_argument('--stamps', type=int, default=B_DEFAULT, help='stamps per GPU (leading subset)')
+    ap.add_argument('--nx', type=int, default=None, help='fixed stamp size (default: automatic)')
+    ap.add_argument('--stage', default='all', choices=['all', 'draw', 'tables'],
+                    help="'draw' / 'tables': run only that stage (for profiling)")
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)
+    elif args.stage != 'all':
+        run_stage(args)
     else:
         run_gpu(args)
 
