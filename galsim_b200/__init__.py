@@ -21,5 +21,6 @@ from .box import Box, Pixel
 from .compound import Convolve, Convolution, Add, Sum, Transform, Transformation, _Transform
 from .batch import draw_batch, plan_batch, run_batch, StampBatch
 from ._lib import set_device
+from . import autodiff
 
 __version__ = '0.1.0'

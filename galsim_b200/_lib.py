@@ -21,6 +21,8 @@ OP_LEAF, OP_MUL, OP_ADD, OP_PHASE, OP_SCALE = 1, 2, 3, 4, 5
 LEAF_JAC_GENERAL, LEAF_SIZE_IS_HLR = 1, 2
 PHASE_JAC_GENERAL = 1
 F32, F64 = 0, 1
+TABLES_DN = 1
+GRAD_PER_LEAF, GRAD_PER_PHASE = 6, 7
 
 
 class GSParamsC(ctypes.Structure):
@@ -72,7 +74,12 @@ def lib():
             'gsb_tables_create': (i, [ctypes.POINTER(vp)]),
             'gsb_tables_destroy': (i, [vp]),
             'gsb_sersic_tables_build': (i, [vp, vp, vp, i, ctypes.POINTER(GSParamsC), vp]),
+            'gsb_sersic_tables_build_ex': (i, [vp, vp, vp, i, ctypes.POINTER(GSParamsC), i, vp]),
             'gsb_sersic_tables_info': (i, [vp, vp, i, vp]),
+            'gsb_adjoint_grad_count': (i, [ctypes.POINTER(TemplateC)]),
+            'gsb_adjoint_workspace_size': (sz, [i, i, i]),
+            'gsb_adjoint_images': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp,
+                                       vp, vp, vp, i, vp, i, vp, i, vp, sz, vp]),
             'gsb_prepare_leaves': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp,
                                        vp, vp]),
             'gsb_draw_workspace_size': (sz, [i, i, i]),
@@ -162,11 +169,15 @@ class Tables(object):
         check(lib().gsb_tables_create(ctypes.byref(h)))
         self.handle = h
 
-    def build_sersic(self, n_values, gsp):
+    def build_sersic(self, n_values, gsp, with_dn=False):
+        """Build one table per Sersic index; with_dn also builds the d/dn tables that the
+        adjoint needs (the tables themselves are the same either way)."""
         n = np.ascontiguousarray(n_values, dtype=np.float64)
-        check(lib().gsb_sersic_tables_build(self.handle, n.ctypes.data_as(ctypes.c_void_p), None,
-                                            len(n), ctypes.byref(gsparams_c(gsp)), Device.stream()))
+        check(lib().gsb_sersic_tables_build_ex(self.handle, n.ctypes.data_as(ctypes.c_void_p), None,
+                                               len(n), ctypes.byref(gsparams_c(gsp)),
+                                               TABLES_DN if with_dn else 0, Device.stream()))
         self.count = len(n)
+        self.with_dn = with_dn
 
     def sersic_info(self, count=None):
         count = self.count if count is None else count

@@ -11,7 +11,13 @@ namespace gsb {
 
 int ogata_init(DeviceState* st);
 int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc, int count,
-                        const gsb_gsparams* gsp, cudaStream_t stream);
+                        const gsb_gsparams* gsp, bool with_dn, cudaStream_t stream);
+int adjoint_grad_count(const gsb_template* tpl);
+size_t adjoint_workspace_size(int N, int n_stamps, int precision);
+int adjoint_images(const gsb_template* tpl, int n_stamps, const gsb_leaf* d_leaves,
+                   const gsb_phase* d_phases, const double* d_scales, const gsb_stamp* d_stamps,
+                   const gsb_tables* t, int N, const void* d_cot, int cot_dtype, double* d_grad,
+                   int precision, void* d_work, size_t work_bytes, cudaStream_t stream);
 int prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp, gsb_leaf* d_leaves,
                    const gsb_tables* t, double* d_info, cudaStream_t stream);
 size_t draw_workspace_size(int N, int n_stamps, int precision);
@@ -145,6 +151,9 @@ int gsb_tables_destroy(gsb_tables* t)
     cudaFree(t->d_scan);
     cudaFree(t->d_n);
     cudaFree(t->d_status);
+    cudaFree(t->d_dheader);
+    cudaFree(t->d_dnode);
+    cudaFree(t->d_dval);
     delete t;
     return GSB_OK;
 }
@@ -154,7 +163,17 @@ int gsb_sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_tr
 {
     if (!t || !gsp || (count > 0 && !h_n)) return set_error(GSB_ERR_INVALID, "null argument");
     if (count < 0) return set_error(GSB_ERR_INVALID, "negative count");
-    return sersic_tables_build(t, h_n, h_trunc_over_r0, count, gsp, (cudaStream_t)stream);
+    return sersic_tables_build(t, h_n, h_trunc_over_r0, count, gsp, false, (cudaStream_t)stream);
+}
+
+int gsb_sersic_tables_build_ex(gsb_tables* t, const double* h_n, const double* h_trunc_over_r0,
+                               int count, const gsb_gsparams* gsp, int flags, void* stream)
+{
+    if (!t || !gsp || (count > 0 && !h_n)) return set_error(GSB_ERR_INVALID, "null argument");
+    if (count < 0) return set_error(GSB_ERR_INVALID, "negative count");
+    if (flags & ~GSB_TABLES_DN) return set_error(GSB_ERR_INVALID, "unknown table flags");
+    return sersic_tables_build(t, h_n, h_trunc_over_r0, count, gsp, (flags & GSB_TABLES_DN) != 0,
+                               (cudaStream_t)stream);
 }
 
 int gsb_sersic_tables_info(const gsb_tables* t, double* h_out, int count, void* stream)
@@ -225,6 +244,40 @@ int gsb_draw_kimages(const gsb_template* tpl, int n_stamps, const gsb_gsparams* 
     if (!(dk > 0.)) return set_error(GSB_ERR_INVALID, "dk must be > 0");
     return draw_kimages(tpl, n_stamps, d_leaves, d_phases, d_scales, t, dk, kxmin, kymin, nkx, nky,
                         d_out, out_dtype, (cudaStream_t)stream);
+}
+
+int gsb_adjoint_grad_count(const gsb_template* tpl)
+{
+    const int rc = validate_template(tpl);
+    if (rc) return rc;
+    return adjoint_grad_count(tpl);
+}
+
+size_t gsb_adjoint_workspace_size(int N, int n_stamps, int precision)
+{
+    if (!good_fft_size_ok(N) || n_stamps <= 0) return 0;
+    return adjoint_workspace_size(N, n_stamps, precision);
+}
+
+int gsb_adjoint_images(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp,
+                       const gsb_leaf* d_leaves, const gsb_phase* d_phases, const double* d_scales,
+                       const gsb_stamp* d_stamps, const gsb_tables* t, int N,
+                       const void* d_cotangent, int cot_dtype, double* d_grad, int precision,
+                       void* d_workspace, size_t workspace_bytes, void* stream)
+{
+    int rc = validate_template(tpl);
+    if (rc) return rc;
+    if (!gsp) return set_error(GSB_ERR_INVALID, "null gsparams");
+    if (n_stamps < 0) return set_error(GSB_ERR_INVALID, "negative stamp count");
+    if (n_stamps == 0) return GSB_OK;
+    if (!d_leaves || !d_stamps || !d_cotangent || !d_grad || (tpl->n_phases && !d_phases) ||
+        (tpl->n_scales && !d_scales))
+        return set_error(GSB_ERR_INVALID, "null device pointer");
+    if (cot_dtype != GSB_F32 && cot_dtype != GSB_F64) return set_error(GSB_ERR_INVALID, "bad cot_dtype");
+    if (precision != GSB_F32 && precision != GSB_F64) return set_error(GSB_ERR_INVALID, "bad precision");
+    if (!good_fft_size_ok(N)) return set_error(GSB_ERR_INVALID, "N is not 2^a or 3*2^a");
+    return adjoint_images(tpl, n_stamps, d_leaves, d_phases, d_scales, d_stamps, t, N, d_cotangent,
+                          cot_dtype, d_grad, precision, d_workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
 }  // extern "C"

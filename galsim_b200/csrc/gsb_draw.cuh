@@ -26,7 +26,7 @@
 namespace gsb {
 
 
-constexpr int kWarps = 16;
+constexpr int kWarps = 16;          // warps per CTA (fewer where their FFT scratch does not fit)
 constexpr int kThreads = kWarps * 32;
 
 struct StampSmem {
@@ -48,6 +48,18 @@ struct StampSmem {
 
 // Bytes of shared memory reserved for the per-stamp caches.
 constexpr int kCacheBytes = 24 * 1024;
+
+constexpr size_t kSmemLimit = 227 * 1024;
+
+// Warps per CTA of the fused kernels for (T, N): 16, or 8 where 16 per-warp FFT buffers of N
+// complex T (plus twiddles, stamp state and caches) exceed the 227 KB of shared memory
+// (double at N >= 768).
+template <typename T, int N>
+__host__ __device__ constexpr int fused_warps()
+{
+    return ((sizeof(StampSmem) + 15) / 16 * 16 + sizeof(Cx<T>) * N * (1 + kWarps) + kCacheBytes + 4096 <=
+            kSmemLimit) ? kWarps : kWarps / 2;
+}
 
 struct DrawArgs {
     gsb_template tpl;
@@ -330,8 +342,9 @@ __device__ inline void store_pixel(void* out, int dtype, int add, long long idx,
 }
 
 template <typename T, int N, bool WSMEM>
-__global__ void __launch_bounds__(kThreads) draw_fused_kernel(const __grid_constant__ DrawArgs a)
+__global__ void __launch_bounds__(fused_warps<T, N>() * 32) draw_fused_kernel(const __grid_constant__ DrawArgs a)
 {
+    constexpr int NW = fused_warps<T, N>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int H = N / 2 + 1;
     constexpr int WS = N + 1;   // column stride of W (padding against bank conflicts)
@@ -340,7 +353,7 @@ __global__ void __launch_bounds__(kThreads) draw_fused_kernel(const __grid_const
     Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw + off);
     off += sizeof(Cx<T>) * N;
     Cx<T>* scratch = reinterpret_cast<Cx<T>*>(smem_raw + off);
-    off += sizeof(Cx<T>) * N * kWarps;
+    off += sizeof(Cx<T>) * N * NW;
     Cx<T>* W = WSMEM ? reinterpret_cast<Cx<T>*>(smem_raw + off)
                      : reinterpret_cast<Cx<T>*>(a.work) + (size_t)blockIdx.x * H * WS;
     if (WSMEM) off += sizeof(Cx<T>) * H * WS;
@@ -367,7 +380,7 @@ __global__ void __launch_bounds__(kThreads) draw_fused_kernel(const __grid_const
         const bool fast = S.regstack;
 
         // ---- column phase: wrapped k-values, inverse DFT along ky ----
-        for (int c = warp; c < H; c += kWarps) {
+        for (int c = warp; c < H; c += NW) {
             const int alo = ceil_div(-hk - c, N), ahi = floor_div(hk - c, N);
             for (int r = lane; r < N; r += 32) {
                 const int kyc = r < N / 2 ? r : r - N;
@@ -398,7 +411,7 @@ __global__ void __launch_bounds__(kThreads) draw_fused_kernel(const __grid_const
         const gsb_stamp& G = S.geom;
         const int npairs = (G.ny + 1) / 2;
         double fsum = 0., fcomp = 0.;
-        for (int p = warp; p < npairs; p += kWarps) {
+        for (int p = warp; p < npairs; p += NW) {
             const int py1 = G.ymin + 2 * p;
             const bool two = 2 * p + 1 < G.ny;
             const int y1 = pmod(py1, N), y2 = pmod(py1 + 1, N);
@@ -443,7 +456,7 @@ __global__ void __launch_bounds__(kThreads) draw_fused_kernel(const __grid_const
             __syncthreads();
             if (threadIdx.x == 0) {
                 double tot = 0.;
-                for (int w = 0; w < kWarps; ++w) tot += S.flux_part[w];
+                for (int w = 0; w < NW; ++w) tot += S.flux_part[w];
                 a.added_flux[s] = tot;
             }
         }
@@ -483,12 +496,10 @@ template <typename T, int N>
 constexpr size_t smem_bytes(bool wsmem)
 {
     size_t off = (sizeof(StampSmem) + 15) & ~size_t(15);
-    off += sizeof(Cx<T>) * N * (1 + kWarps);
+    off += sizeof(Cx<T>) * N * (1 + fused_warps<T, N>());
     if (wsmem) off += sizeof(Cx<T>) * (N / 2 + 1) * (N + 1);
     return ((off + 15) & ~size_t(15)) + kCacheBytes;
 }
-
-constexpr size_t kSmemLimit = 227 * 1024;
 
 template <typename T, int N>
 constexpr bool w_fits_smem()
@@ -523,7 +534,7 @@ int launch_fused(const DrawArgs& args, size_t work_bytes, cudaStream_t stream)
         return set_error(GSB_ERR_INVALID, "draw workspace too small");
     GSB_CUDA_CHECK(cudaFuncSetAttribute(draw_fused_kernel<T, N, wsmem>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-    draw_fused_kernel<T, N, wsmem><<<grid, kThreads, sm, stream>>>(args);
+    draw_fused_kernel<T, N, wsmem><<<grid, fused_warps<T, N>() * 32, sm, stream>>>(args);
     GSB_CUDA_CHECK(cudaGetLastError());
     return GSB_OK;
 }

@@ -17,9 +17,11 @@ int set_error(int code, const std::string& msg);
 #define GSB_CUDA_CHECK(expr)                                                              \
     do {                                                                                  \
         cudaError_t e_ = (expr);                                                          \
-        if (e_ != cudaSuccess)                                                            \
+        if (e_ != cudaSuccess) {                                                          \
+            (void)cudaGetLastError(); /* clear a non-sticky error for the next call */    \
             return ::gsb::set_error(GSB_ERR_CUDA, std::string(#expr) + ": " +            \
                                     cudaGetErrorString(e_));                              \
+        }                                                                                 \
     } while (0)
 
 // One leaf as used inside kernels (gsb_leaf plus its type).
@@ -45,6 +47,22 @@ enum {
     kSH_N = 0, kSH_NUSED, kSH_FRONT, kSH_DA, kSH_KSQMIN, kSH_KSQMAX, kSH_KD2, kSH_KD4,
     kSH_HIGHA, kSH_HIGHB, kSH_MAXK, kSH_STEPK, kSH_RE, kSH_DLOGK, kSH_NCAND, kSH_STATUS,
     kSersicHeader = 16
+};
+
+// Per-slot derivative header (doubles) of tables built with n-derivatives: d/dn (at fixed
+// r0) of the low-k coefficients and of the high-k fit, and d ln(r_e / r0) / dn.
+// The table's grid starts at front = ln k_min(n) - 0.001, so its nodes k_i move with n:
+// node derivatives are total derivatives along k_i(n), and dfront/dn is kept to shift the
+// spline argument.
+enum {
+    kSD_DKD2 = 0, kSD_DKD4, kSD_DHIGHA, kSD_DHIGHB, kSD_DLNRE, kSD_DFRONT,
+    kSersicDHeader = 8
+};
+
+// d/dn of a Sersic table: spline nodes (x, dy/dn, d2y/dn, 0) on the table's own x grid.
+struct SersicDnView {
+    double dkd2, dkd4, dhigha, dhighb, dlnre, dfront;
+    const double4* node;
 };
 
 // The reference k-image grid a point belongs to (for clip rules that depend on the grid).
@@ -141,4 +159,10 @@ struct gsb_tables {
     double* d_n = nullptr;        // Sersic indices of the slots
     int* d_status = nullptr;      // convergence status word
     size_t cap_slots = 0, cap_nodes = 0;
+    // n-derivative tables (built on request)
+    bool has_dn = false;
+    double* d_dheader = nullptr;  // count * kSersicDHeader
+    double4* d_dnode = nullptr;   // count * stride
+    double* d_dval = nullptr;     // scratch: count * stride d/dn Hankel values
+    size_t cap_dn_slots = 0, cap_dn_nodes = 0;
 };

@@ -55,6 +55,28 @@ __device__ inline double gamma_p(double a, double x)
 }
 
 // ---------------------------------------------------------------------------------------
+// Digamma psi(x) = d ln Gamma / dx for x > 0: the recurrence psi(x) = psi(x + 1) - 1/x
+// (A&S 6.3.5) up to x >= 10, then the asymptotic series
+// psi(x) ~ ln x - 1/(2x) - sum_k B_2k / (2k x^2k)  (A&S 6.3.18), five terms.
+// ---------------------------------------------------------------------------------------
+__device__ inline double digamma(double x)
+{
+    double r = 0.;
+    while (x < 10.) { r -= 1. / x; x += 1.; }
+    const double ix2 = 1. / (x * x);
+    const double series = ix2 * (1. / 12. - ix2 * (1. / 120. - ix2 * (1. / 252. - ix2 * (1. / 240. - ix2 * (1. / 132.)))));
+    return r + log(x) - 0.5 / x - series;
+}
+
+// dP(a, x)/da by a central difference of gamma_p in FP64 (relative step 1e-5): P is smooth
+// in a and accurate to ~1e-16, so the difference is good to ~1e-10.
+__device__ inline double gamma_p_da(double a, double x)
+{
+    const double h = 1e-5 * a;
+    return (gamma_p(a + h, x) - gamma_p(a - h, x)) / (2. * h);
+}
+
+// ---------------------------------------------------------------------------------------
 // Brent's root finder with the reference's bracket expansion rules
 // (include/galsim/Solve.h: defaultTolerance 1e-7, defaultMaxSteps 40, bracket1 :217-232,
 // bracket1WithLimit :264-326, zbrent :385-447).  Brent's method itself follows the

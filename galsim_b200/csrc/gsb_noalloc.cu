@@ -82,7 +82,7 @@ int launch_noalloc(DrawArgs args, cudaStream_t stream)
     }
     GSB_CUDA_CHECK(cudaFuncSetAttribute(draw_fused_kernel<T, N, wsmem>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-    draw_fused_kernel<T, N, wsmem><<<grid, kThreads, sm, stream>>>(args);
+    draw_fused_kernel<T, N, wsmem><<<grid, fused_warps<T, N>() * 32, sm, stream>>>(args);
     GSB_CUDA_CHECK(cudaGetLastError());
     return GSB_OK;
 }

@@ -108,10 +108,86 @@ __device__ double warp_hankel(const OgataTables& og, const F& f, double k, doubl
     return ans1;
 }
 
+// The same quadrature for a pair of integrands (f, df/dn) evaluated together: the stopping
+// rules and the level halving follow the first component only, so the first component is
+// bit-identical to warp_ogata_sum / warp_hankel and the second is integrated on the same nodes.
+template <class F>
+__device__ double2 warp_ogata_sum2(const OgataTables& og, const F& f, double k, int lev)
+{
+    const int lane = threadIdx.x & 31;
+    const double h = ldexp(1.0, -lev);
+    const long long nmax = (long long)fmin(kPi / h, 1e6);
+    const bool tab = lev >= og.lev_min && lev <= og.lev_max;
+    const double2* xw = tab ? og.xw + og.off[lev - og.lev_min] : nullptr;
+    const double logk = log(k);
+    double ans = 0., dans = 0.;
+    for (long long base = 0; base < nmax; base += 32) {
+        const long long i = base + lane;
+        const bool valid = i < nmax;
+        double step = 0., dstep = 0.;
+        if (valid) {
+            const double2 n = tab ? xw[i] : ogata_node(og.root, h, i);
+            const double2 v = f(n.x - logk);
+            step = n.y * v.x;
+            dstep = n.y * v.y;
+        }
+        double pre = step, dpre = dstep;
+        for (int o = 1; o < 32; o <<= 1) {
+            const double v = __shfl_up_sync(0xffffffffu, pre, o);
+            const double dv = __shfl_up_sync(0xffffffffu, dpre, o);
+            if (lane >= o) { pre += v; dpre += dv; }
+        }
+        const double ans_i = ans + pre, dans_i = dans + dpre;
+        const bool stop = valid && fabs(step) < 1e-15 * fabs(ans_i);
+        const unsigned mask = __ballot_sync(0xffffffffu, stop);
+        if (mask) {
+            ans = __shfl_sync(0xffffffffu, ans_i, __ffs(mask) - 1);
+            dans = __shfl_sync(0xffffffffu, dans_i, __ffs(mask) - 1);
+            return make_double2(ans / (k * k), dans / (k * k));
+        }
+        ans = __shfl_sync(0xffffffffu, ans_i, 31);
+        dans = __shfl_sync(0xffffffffu, dans_i, 31);
+    }
+    return make_double2(ans / (k * k), dans / (k * k));
+}
+
+template <class F>
+__device__ double2 warp_hankel2(const OgataTables& og, const F& f, double k, double relerr,
+                                double abserr, int* status)
+{
+    int lev = 5;
+    double h0 = 1. / 32.;
+    while (h0 > 100. * k && lev < 60) { h0 *= 0.5; ++lev; }
+    double2 ans0 = warp_ogata_sum2(og, f, k, lev);
+    double2 ans1 = warp_ogata_sum2(og, f, k, lev + 1);
+    double err = fabs(ans1.x - ans0.x);
+    while ((err > relerr * ans1.x && (err > abserr || fabs(ans1.x) > 2. * fabs(ans0.x))) || ans1.x == 0.) {
+        ++lev;
+        if (lev > 60) { if (status) *status = 1; break; }
+        ans0 = ans1;
+        ans1 = warp_ogata_sum2(og, f, k, lev + 1);
+        err = fabs(ans1.x - ans0.x);
+    }
+    return ans1;
+}
+
 // Integrands as functions of log r: exp(-r^(1/n)) and exp(-k^(5/3)).
 struct SersicRadial {
     double invn;
     __device__ double operator()(double logr) const { return exp(-exp(logr * invn)); }
+};
+
+// (f, g) with f = exp(-r^(1/n)) and g = df/dn + c r df/dr:  the quadrature sum
+// T(k) = sum_j w_j f(x_j / k) has dT/dn along k = k(n) with d ln k / dn = c equal to
+// sum_j w_j [df/dn - c r df/dr](x_j / k); df/dn = f u ln r / n^2, r df/dr = -f u / n, u = r^(1/n).
+struct SersicRadialDn {
+    double invn, c;
+    __device__ double2 operator()(double logr) const
+    {
+        const double u = exp(logr * invn);
+        const double f = exp(-u);
+        return make_double2(f, f * u * invn * (logr * invn + c));
+    }
 };
 
 struct KolmKValue {
@@ -160,7 +236,7 @@ __device__ RootResult sersic_missing_flux_radius(double n, double gamma2n, doubl
 }
 
 __global__ void sersic_setup_kernel(const double* n_arr, int count, gsb_gsparams gsp,
-                                    double* header, int stride)
+                                    double* header, int stride, double* dheader)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= count) return;
@@ -204,6 +280,21 @@ __global__ void sersic_setup_kernel(const double* n_arr, int count, gsb_gsparams
     H[kSH_DLOGK] = dlogk;
     H[kSH_NCAND] = ncand;
     H[kSH_STATUS] = status;
+    if (dheader) {
+        // d/dn of the low-k coefficients (ratios of Gamma functions) and of ln(r_e / r0) =
+        // n ln b, with db/dn from P(2n, b) = 1/2 by implicit differentiation.
+        double* D = dheader + (size_t)s * kSersicDHeader;
+        const double psi2 = digamma(2. * n);
+        D[kSD_DKD2] = kderiv2 * (4. * digamma(4. * n) - 2. * psi2);
+        D[kSD_DKD4] = kderiv4 * (6. * digamma(6. * n) - 2. * psi2);
+        D[kSD_DHIGHA] = 0.;
+        D[kSD_DHIGHB] = 0.;
+        // front = ln k_min - 0.001 with k_min = (kvalue_accuracy / kderiv6)^(1/6)
+        D[kSD_DFRONT] = -(8. * digamma(8. * n) - 2. * psi2) / 6.;
+        const double dPdb = exp(-b + (2. * n - 1.) * log(b) - lgamma(2. * n));
+        const double dbdn = -2. * gamma_p_da(2. * n, b) / dPdb;
+        D[kSD_DLNRE] = log(b) + n * dbdn / b;
+    }
 }
 
 // Running state of the serial part of buildFT for one table (SBSersic.cpp:436-509): the
@@ -229,9 +320,10 @@ __global__ void sersic_scan_init_kernel(const double* header, int count, SersicS
 }
 
 // One warp per (slot, node) of this round: val = Hankel transform at k_i / hankel_norm.
+template <bool DN>
 __global__ void __launch_bounds__(256, 4) sersic_nodes_kernel(const double* header, int count, int stride, int i0, int nround,
                                     gsb_gsparams gsp, const __grid_constant__ OgataTables og, const SersicScan* scan,
-                                    double* vals, int* status_out)
+                                    double* vals, const double* dheader, double* dvals, int* status_out)
 {
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long s = warp / nround;
@@ -244,8 +336,22 @@ __global__ void __launch_bounds__(256, 4) sersic_nodes_kernel(const double* head
     const double logk = H[kSH_FRONT] + i * H[kSH_DLOGK];
     const double k = exp(logk);
     const double hankel_norm = n * tgamma(2. * n);
-    SersicRadial f{1. / n};
     int st = 0;
+    if (DN) {
+        // node value y = v k^2 = T(k) / norm with norm = n Gamma(2n) and k = k_i(n):
+        // dy/dn = (dT/dn) / norm - y (1/n + 2 psi(2n)), dT/dn from the second integrand.
+        SersicRadialDn f{1. / n, dheader[s * kSersicDHeader + kSD_DFRONT]};
+        const double2 hv = warp_hankel2(og, f, k, gsp.integration_relerr,
+                                        gsp.integration_abserr * hankel_norm, &st);
+        const double v = hv.x / hankel_norm;
+        if ((threadIdx.x & 31) == 0) {
+            vals[s * stride + i] = v;
+            dvals[s * stride + i] = (hv.y / hankel_norm - v * (1. / n + 2. * digamma(2. * n))) * k * k;
+            if (st) atomicOr(status_out, 1);
+        }
+        return;
+    }
+    SersicRadial f{1. / n};
     const double v = warp_hankel(og, f, k, gsp.integration_relerr,
                                  gsp.integration_abserr * hankel_norm, &st) / hankel_norm;
     if ((threadIdx.x & 31) == 0) {
@@ -257,7 +363,7 @@ __global__ void __launch_bounds__(256, 4) sersic_nodes_kernel(const double* head
 // Advance each table's scan over this round's nodes (SBSersic.cpp:436-509).
 __global__ void sersic_scan_kernel(const double* header, int count, int stride, int i0, int nround,
                                    gsb_gsparams gsp, const double* vals, double4* nodes,
-                                   SersicScan* scan)
+                                   SersicScan* scan, const double* dvals, double4* dnodes)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= count) return;
@@ -276,6 +382,7 @@ __global__ void sersic_scan_kernel(const double* header, int count, int stride, 
         const double val = v[i];
         const double f0 = val * ksq;
         nd[i] = make_double4(logk, f0, 0., 0.);
+        if (dnodes) dnodes[(size_t)s * stride + i] = make_double4(logk, dvals[(size_t)s * stride + i], 0., 0.);
         S.nused = i + 1;
         if (fabs(val) > gsp.maxk_threshold) { S.maxk = k; S.n_correct = 0; }
         else {
@@ -311,8 +418,36 @@ __global__ void sersic_scan_kernel(const double* header, int count, int stride, 
 }
 
 // End of buildFT (SBSersic.cpp:510-537) and the natural spline (Table.cpp:634-686).
+// Natural cubic spline second derivatives (Thomas algorithm) of nodes (x, y) into .z;
+// .w is scratch.  TSpline setup, src/Table.cpp:634-686.
+__device__ void natural_spline(double4* nd, int N)
+{
+    for (int i = 0; i < N; ++i) nd[i].z = 0.;
+    if (N == 3) {
+        nd[1].z = 3. * ((nd[2].y - nd[1].y) / (nd[2].x - nd[1].x) -
+                        (nd[1].y - nd[0].y) / (nd[1].x - nd[0].x)) / (nd[2].x - nd[0].x);
+    } else if (N > 3) {
+        for (int i = 1; i <= N - 2; ++i)
+            nd[i].z = 6. * ((nd[i + 1].y - nd[i].y) / (nd[i + 1].x - nd[i].x) -
+                            (nd[i].y - nd[i - 1].y) / (nd[i].x - nd[i - 1].x));
+        double bb = 2. * (nd[2].x - nd[0].x);
+        for (int i = 1; i <= N - 2; ++i) {
+            nd[i].z /= bb;
+            if (i == N - 2) break;
+            const double aa = nd[i + 1].x - nd[i].x;
+            const double c = aa / bb;
+            nd[i - 1].w = c;
+            bb = 2. * (nd[i + 2].x - nd[i].x);
+            bb -= aa * c;
+            nd[i + 1].z -= aa * nd[i].z;
+        }
+        for (int i = N - 3; i > 0; --i) nd[i].z -= nd[i - 1].w * nd[i + 1].z;
+    }
+}
+
 __global__ void sersic_finalize_kernel(double* header, int count, int stride, gsb_gsparams gsp,
-                                       const SersicScan* scan, double4* nodes)
+                                       const SersicScan* scan, double4* nodes, double4* dnodes,
+                                       double* dheader)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= count) return;
@@ -334,31 +469,40 @@ __global__ void sersic_finalize_kernel(double* header, int count, int stride, gs
         maxk = sqrt(a / gsp.maxk_threshold);
         for (int it = 0; it < 3; ++it) maxk = sqrt((a - b / maxk) / gsp.maxk_threshold);
     }
-    // Natural cubic spline second derivatives (Thomas algorithm), stored in .z
-    for (int i = 0; i < N; ++i) nd[i].z = 0.;
-    if (N == 3) {
-        nd[1].z = 3. * ((nd[2].y - nd[1].y) / (nd[2].x - nd[1].x) -
-                        (nd[1].y - nd[0].y) / (nd[1].x - nd[0].x)) / (nd[2].x - nd[0].x);
-    } else if (N > 3) {
-        // c[] is stashed in .w
-        for (int i = 1; i <= N - 2; ++i)
-            nd[i].z = 6. * ((nd[i + 1].y - nd[i].y) / (nd[i + 1].x - nd[i].x) -
-                            (nd[i].y - nd[i - 1].y) / (nd[i].x - nd[i - 1].x));
-        double bb = 2. * (nd[2].x - nd[0].x);
-        for (int i = 1; i <= N - 2; ++i) {
-            nd[i].z /= bb;
-            if (i == N - 2) break;
-            const double aa = nd[i + 1].x - nd[i].x;
-            const double c = aa / bb;
-            nd[i - 1].w = c;
-            bb = 2. * (nd[i + 2].x - nd[i].x);
-            bb -= aa * c;
-            nd[i + 1].z -= aa * nd[i].z;
-        }
-        for (int i = N - 3; i > 0; --i) nd[i].z -= nd[i - 1].w * nd[i + 1].z;
-    }
+    natural_spline(nd, N);
     const double back = nd[N - 1].x;
     for (int i = 0; i < N; ++i) { nd[i].x -= front; nd[i].w = 0.; }
+    if (dnodes) {
+        // The spline is linear in its node values, so d/dn of the interpolant is the spline of
+        // the node derivatives on the same grid.  Likewise the high-k fit is linear in the f0
+        // values of its window: the 10 nodes before the stopping node, or the last 10 nodes
+        // when the scan ran to the end of the candidate grid.
+        double4* dn = dnodes + (size_t)s * stride;
+        natural_spline(dn, N);
+        for (int i = 0; i < N; ++i) { dn[i].x -= front; dn[i].w = 0.; }
+        // The fit's 1/k_i move too: d(1/k_i)/dn = -c / k_i with c = dfront/dn.
+        double* D = dheader + (size_t)s * kSersicDHeader;
+        const double c = D[kSD_DFRONT];
+        const int wend = S.ksq_max > 0. ? N - 1 : N;
+        const int wbeg = wend - n_fit > 0 ? wend - n_fit : 0;
+        double sk = 0., sk2 = 0., sf = 0., skf = 0., dsf = 0., dskf = 0.;
+        for (int i = wbeg; i < wend; ++i) {
+            const double inv_k = exp(-(front + i * dlogk));
+            const double f0 = nd[i].y, df0 = dn[i].y;
+            sk += inv_k;
+            sk2 += inv_k * inv_k;
+            sf += f0;
+            skf += f0 * inv_k;
+            dsf += df0;
+            dskf += (df0 - c * f0) * inv_k;
+        }
+        const double dsk = -c * sk, dsk2 = -2. * c * sk2;
+        const double den = n_fit * sk2 - sk * sk, dden = n_fit * dsk2 - 2. * sk * dsk;
+        const double na = sf * sk2 - sk * skf, dna = dsf * sk2 + sf * dsk2 - dsk * skf - sk * dskf;
+        const double nb = n_fit * skf - sk * sf, dnb = n_fit * dskf - dsk * sf - sk * dsf;
+        D[kSD_DHIGHA] = (dna * den - na * dden) / (den * den);
+        D[kSD_DHIGHB] = (dnb * den - nb * dden) / (den * den);
+    }
     H[kSH_NUSED] = N;
     H[kSH_DA] = (back - front) / (N - 1);
     H[kSH_KSQMAX] = ksq_max;
@@ -588,7 +732,7 @@ static int sersic_stride(const double* h_n, int count, const gsb_gsparams* gsp)
 }
 
 int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc, int count,
-                        const gsb_gsparams* gsp, cudaStream_t stream)
+                        const gsb_gsparams* gsp, bool with_dn, cudaStream_t stream)
 {
     DeviceState* st = device_state();
     if (!st->ready) return set_error(GSB_ERR_INVALID, "gsb_init has not been called");
@@ -614,13 +758,26 @@ int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc,
         GSB_CUDA_CHECK(cudaMalloc(&t->d_n, sizeof(double) * t->cap_slots));
         GSB_CUDA_CHECK(cudaMalloc(&t->d_status, sizeof(int)));
     }
+    if (with_dn && ((size_t)count > t->cap_dn_slots || (size_t)count * stride > t->cap_dn_nodes)) {
+        cudaFree(t->d_dheader); cudaFree(t->d_dnode); cudaFree(t->d_dval);
+        t->d_dheader = nullptr; t->d_dnode = nullptr; t->d_dval = nullptr;
+        t->cap_dn_slots = std::max<size_t>(count, t->cap_dn_slots);
+        t->cap_dn_nodes = std::max<size_t>((size_t)count * stride, t->cap_dn_nodes);
+        GSB_CUDA_CHECK(cudaMalloc(&t->d_dheader, sizeof(double) * kSersicDHeader * t->cap_dn_slots));
+        GSB_CUDA_CHECK(cudaMalloc(&t->d_dnode, sizeof(double4) * t->cap_dn_nodes));
+        GSB_CUDA_CHECK(cudaMalloc(&t->d_dval, sizeof(double) * t->cap_dn_nodes));
+    }
+    t->has_dn = with_dn;
+    double* dheader = with_dn ? t->d_dheader : nullptr;
+    double4* dnode = with_dn ? t->d_dnode : nullptr;
+    double* dval = with_dn ? t->d_dval : nullptr;
     t->count = count;
     t->stride = stride;
     double* d_n = t->d_n;
     int* d_status = t->d_status;
     GSB_CUDA_CHECK(cudaMemcpyAsync(d_n, h_n, sizeof(double) * count, cudaMemcpyHostToDevice, stream));
     GSB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), stream));
-    sersic_setup_kernel<<<(count + 127) / 128, 128, 0, stream>>>(d_n, count, *gsp, t->d_header, stride);
+    sersic_setup_kernel<<<(count + 127) / 128, 128, 0, stream>>>(d_n, count, *gsp, t->d_header, stride, dheader);
     GSB_CUDA_CHECK(cudaGetLastError());
     sersic_scan_init_kernel<<<(count + 127) / 128, 128, 0, stream>>>(t->d_header, count, static_cast<SersicScan*>(t->d_scan));
     GSB_CUDA_CHECK(cudaGetLastError());
@@ -630,16 +787,23 @@ int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc,
     for (int i0 = 0; i0 < stride; i0 += kRound) {
         const long long nwarps = (long long)count * kRound;
         const long long blocks = (nwarps * 32 + threads - 1) / threads;
-        sersic_nodes_kernel<<<(unsigned)blocks, threads, 0, stream>>>(t->d_header, count, stride, i0, kRound,
-                                                                      *gsp, st->og, static_cast<const SersicScan*>(t->d_scan), t->d_val,
-                                                                      d_status);
+        if (with_dn)
+            sersic_nodes_kernel<true><<<(unsigned)blocks, threads, 0, stream>>>(
+                t->d_header, count, stride, i0, kRound, *gsp, st->og,
+                static_cast<const SersicScan*>(t->d_scan), t->d_val, dheader, dval, d_status);
+        else
+            sersic_nodes_kernel<false><<<(unsigned)blocks, threads, 0, stream>>>(
+                t->d_header, count, stride, i0, kRound, *gsp, st->og,
+                static_cast<const SersicScan*>(t->d_scan), t->d_val, nullptr, nullptr, d_status);
         GSB_CUDA_CHECK(cudaGetLastError());
         sersic_scan_kernel<<<(count + 63) / 64, 64, 0, stream>>>(t->d_header, count, stride, i0, kRound,
-                                                                 *gsp, t->d_val, t->d_node, static_cast<SersicScan*>(t->d_scan));
+                                                                 *gsp, t->d_val, t->d_node, static_cast<SersicScan*>(t->d_scan),
+                                                                 dval, dnode);
         GSB_CUDA_CHECK(cudaGetLastError());
     }
     sersic_finalize_kernel<<<(count + 63) / 64, 64, 0, stream>>>(t->d_header, count, stride, *gsp,
-                                                                 static_cast<const SersicScan*>(t->d_scan), t->d_node);
+                                                                 static_cast<const SersicScan*>(t->d_scan), t->d_node,
+                                                                 dnode, dheader);
     GSB_CUDA_CHECK(cudaGetLastError());
     int h_status = 0;
     GSB_CUDA_CHECK(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));

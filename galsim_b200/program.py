@@ -116,6 +116,7 @@ class Program(object):
         self.L = len(bld.leaves)
         self.gsp_c = _lib.gsparams_c(self.gsparams)
         self._prepared = False
+        self.need_dn = False      # build the Sersic d/dn tables (for the adjoint)
 
     # -- device preparation ------------------------------------------------------------------
     def upload(self):
@@ -136,14 +137,18 @@ class Program(object):
                 leaves['table'][:, l] = inv[k]
         self.d_leaves = _lib.to_device(leaves)
         self.d_info = torch.empty(B * L * 2, dtype=torch.float64, device=_lib.Device.torch_device())
-        self.tables = _lib.Tables() if self.sersic_n is not None else None
+        if self.sersic_n is None:
+            self.tables = None
+        elif getattr(self, 'tables', None) is None:
+            self.tables = _lib.Tables()
 
     def compute_leaves(self):
         """FP64 on the GPU: build the Sersic FT tables, then every leaf's derived constants,
         stepk and maxk; copy stepk / maxk back for the host-side composition."""
+        self.upload()
         B, L = self.B, self.L
         if self.tables is not None:
-            self.tables.build_sersic(self.sersic_n, self.gsparams)
+            self.tables.build_sersic(self.sersic_n, self.gsparams, with_dn=self.need_dn)
         _lib.check(_lib.lib().gsb_prepare_leaves(
             ctypes.byref(self.tpl), B, ctypes.byref(self.gsp_c), _lib.ptr(self.d_leaves),
             self.tables.handle if self.tables else None, _lib.ptr(self.d_info), _lib.Device.stream()))
@@ -168,21 +173,26 @@ class Program(object):
         return self.leaf_stepk[:, l], self.leaf_maxk[:, l]
 
     # -- drawing ---------------------------------------------------------------------------
-    def draw_stamps(self, N, Nk, xmin, ymin, nx, ny, dtype, add_to=None, precision=_lib.F32):
-        """Run the fused kernels for every stamp.  Arrays are per stamp.  Returns the device
-        output buffer (flat), per-stamp offsets and the device added-flux array."""
+    def reset_records(self):
+        """Forget the device copy and sizing after the host records (bld.leaves / phases /
+        scales) were changed in place."""
+        self.d_leaves = None
+        self._prepared = False
+        self._geom = None
+
+    def _stamp_geometry(self, N, Nk, xmin, ymin, nx, ny):
+        """Device stamp records sorted by FFT size, with the bucket boundaries; kept for the
+        adjoint of the same draw."""
         import torch
-        self.prepare()
         B, L = self.B, self.L
         dev = _lib.Device.torch_device()
         N = np.asarray(N, np.int64)
         order = np.argsort(N, kind='stable')
-        nx = np.asarray(nx, np.int64)
-        ny = np.asarray(ny, np.int64)
+        nx = np.broadcast_to(np.asarray(nx, np.int64), (B,))
+        ny = np.broadcast_to(np.asarray(ny, np.int64), (B,))
         sizes = nx * ny
         offsets = np.zeros(B, np.int64)
         offsets[1:] = np.cumsum(sizes)[:-1]
-        total = int(sizes.sum())
         stamps = np.zeros(B, dtype=_lib.STAMP_DTYPE)
         stamps['N'] = N
         stamps['Nk'] = Nk
@@ -191,41 +201,86 @@ class Program(object):
         stamps['nx'] = nx
         stamps['ny'] = ny
         stamps['out_offset'] = offsets
-        tdt = torch.float32 if dtype == _lib.F32 else torch.float64
-        if add_to is not None:
-            out = add_to
-        else:
-            out = torch.empty(max(total, 1), dtype=tdt, device=dev)
-        flux = torch.empty(B, dtype=torch.float64, device=dev)
         perm = torch.from_numpy(order).to(dev)
         lv = self.d_leaves.view(B, L * _lib.LEAF_DTYPE.itemsize).index_select(0, perm).contiguous()
         ph = (_lib.to_device(np.stack(self.bld.phases, axis=1)[order]) if self.bld.phases else None)
         sc = (_lib.to_device(np.stack(self.bld.scales, axis=1)[order]) if self.bld.scales else None)
         st = _lib.to_device(stamps[order])
-        flux_sorted = torch.empty(B, dtype=torch.float64, device=dev)
         Ns = N[order]
         bounds = np.flatnonzero(np.diff(Ns)) + 1
-        starts = np.concatenate([[0], bounds])
-        ends = np.concatenate([bounds, [B]])
+        starts = np.concatenate([[0], bounds]).astype(np.int64)
+        ends = np.concatenate([bounds, [B]]).astype(np.int64)
+        self._geom = dict(order=order, perm=perm, lv=lv, ph=ph, sc=sc, st=st, Ns=Ns, starts=starts,
+                          ends=ends, offsets=offsets, total=int(sizes.sum()))
+        return self._geom
+
+    def _bucket_ptrs(self, g, s0):
+        L, P, S = self.L, len(self.bld.phases), len(self.bld.scales)
+        return (ctypes.c_void_p(g['lv'].data_ptr() + int(s0) * L * _lib.LEAF_DTYPE.itemsize),
+                ctypes.c_void_p(g['ph'].data_ptr() + int(s0) * P * _lib.PHASE_DTYPE.itemsize) if P else None,
+                ctypes.c_void_p(g['sc'].data_ptr() + int(s0) * S * 8) if S else None,
+                ctypes.c_void_p(g['st'].data_ptr() + int(s0) * _lib.STAMP_DTYPE.itemsize))
+
+    def draw_stamps(self, N, Nk, xmin, ymin, nx, ny, dtype, add_to=None, precision=_lib.F32):
+        """Run the fused kernels for every stamp.  Arrays are per stamp.  Returns the device
+        output buffer (flat), per-stamp offsets and the device added-flux array."""
+        import torch
+        self.prepare()
+        B = self.B
+        dev = _lib.Device.torch_device()
+        g = self._stamp_geometry(N, Nk, xmin, ymin, nx, ny)
+        tdt = torch.float32 if dtype == _lib.F32 else torch.float64
+        out = add_to if add_to is not None else torch.empty(max(g['total'], 1), dtype=tdt, device=dev)
+        flux = torch.empty(B, dtype=torch.float64, device=dev)
+        flux_sorted = torch.empty(B, dtype=torch.float64, device=dev)
         stream = _lib.Device.stream()
         lib = _lib.lib()
-        for s0, s1 in zip(starts, ends):
+        for s0, s1 in zip(g['starts'], g['ends']):
             n = int(s1 - s0)
-            NN = int(Ns[s0])
+            NN = int(g['Ns'][s0])
             wbytes = lib.gsb_draw_workspace_size(NN, n, precision)
             work = torch.empty(max(int(wbytes), 8), dtype=torch.uint8, device=dev) if wbytes else None
+            lvp, php, scp, stp = self._bucket_ptrs(g, s0)
             _lib.check(lib.gsb_draw_images(
-                ctypes.byref(self.tpl), n, ctypes.byref(self.gsp_c),
-                ctypes.c_void_p(lv.data_ptr() + int(s0) * L * _lib.LEAF_DTYPE.itemsize),
-                ctypes.c_void_p(ph.data_ptr() + int(s0) * len(self.bld.phases) * 64) if ph is not None else None,
-                ctypes.c_void_p(sc.data_ptr() + int(s0) * len(self.bld.scales) * 8) if sc is not None else None,
-                ctypes.c_void_p(st.data_ptr() + int(s0) * _lib.STAMP_DTYPE.itemsize),
+                ctypes.byref(self.tpl), n, ctypes.byref(self.gsp_c), lvp, php, scp, stp,
                 self.tables.handle if self.tables else None,
                 _lib.ptr(out), dtype, 1 if add_to is not None else 0,
                 ctypes.c_void_p(flux_sorted.data_ptr() + int(s0) * 8),
                 precision, _lib.ptr(work), ctypes.c_size_t(int(wbytes)), stream))
-        flux[perm] = flux_sorted
-        return out, offsets, flux
+        flux[g['perm']] = flux_sorted
+        return out, g['offsets'], flux
+
+    def grad_count(self):
+        return _lib.lib().gsb_adjoint_grad_count(ctypes.byref(self.tpl))
+
+    def adjoint_stamps(self, cot, cot_dtype, precision=_lib.F32):
+        """Reverse mode of the last draw_stamps call: cot is the flat device cotangent in the
+        output's layout.  Returns the (B, grad_count) FP64 device tensor of record gradients
+        (see gsb_adjoint_grad_count for the entry order)."""
+        import torch
+        g = self._geom
+        if g is None:
+            raise GalSimError("adjoint_stamps needs a preceding draw_stamps")
+        B = self.B
+        dev = _lib.Device.torch_device()
+        ng = self.grad_count()
+        grad_sorted = torch.empty((B, ng), dtype=torch.float64, device=dev)
+        stream = _lib.Device.stream()
+        lib = _lib.lib()
+        for s0, s1 in zip(g['starts'], g['ends']):
+            n = int(s1 - s0)
+            NN = int(g['Ns'][s0])
+            wbytes = lib.gsb_adjoint_workspace_size(NN, n, precision)
+            work = torch.empty(max(int(wbytes), 8), dtype=torch.uint8, device=dev) if wbytes else None
+            lvp, php, scp, stp = self._bucket_ptrs(g, s0)
+            _lib.check(lib.gsb_adjoint_images(
+                ctypes.byref(self.tpl), n, ctypes.byref(self.gsp_c), lvp, php, scp, stp,
+                self.tables.handle if self.tables else None, NN,
+                _lib.ptr(cot), cot_dtype, ctypes.c_void_p(grad_sorted.data_ptr() + int(s0) * ng * 8),
+                precision, _lib.ptr(work), ctypes.c_size_t(int(wbytes)), stream))
+        grad = torch.empty_like(grad_sorted)
+        grad[g['perm']] = grad_sorted
+        return grad
 
     def draw_kimage(self, dk, kxmin, kymin, nkx, nky, dtype):
         """Evaluate the program on a k grid; returns a host complex array (B, nky, nkx)."""

@@ -154,6 +154,16 @@ int gsb_tables_destroy(gsb_tables* t);
 int gsb_sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc_over_r0,
                             int count, const gsb_gsparams* gsp, void* stream);
 
+/* gsb_sersic_tables_build with options.  flags: GSB_TABLES_DN also builds, per slot, the
+ * derivative of the table with respect to the Sersic index n at fixed r0 (a second Hankel
+ * integrand on the same quadrature nodes, its spline, and the derivatives of the low-k and
+ * high-k forms) and d ln(r_e / r0) / dn, which gsb_adjoint_images needs for Sersic leaves.
+ * The tables themselves are identical with or without the flag.  No reference counterpart
+ * (the reference has no derivatives). */
+#define GSB_TABLES_DN 1
+int gsb_sersic_tables_build_ex(gsb_tables* t, const double* h_n, const double* h_trunc_over_r0,
+                               int count, const gsb_gsparams* gsp, int flags, void* stream);
+
 /* Copy slot headers back (16 doubles per slot: see gsb_tables.cu) for inspection. */
 int gsb_sersic_tables_info(const gsb_tables* t, double* h_out, int count, void* stream);
 
@@ -208,6 +218,34 @@ int gsb_draw_images_noalloc(const gsb_template* tpl, int n_stamps, const gsb_gsp
                             const double* d_scales, const gsb_stamp* d_stamps,
                             const gsb_tables* t, int N, void* d_out, int out_dtype,
                             int add_to_image, double* d_added_flux, int precision, void* stream);
+
+/* Adjoint ------------------------------------------------------------------------------ */
+/* Gradient entries per stamp for this template, in this order:
+ *   per leaf l   (6): d/dflux, d/djac[0..3], d/dp[0] (Sersic n, else 0)
+ *   per phase i  (7): d/dcenx, d/dceny, d/dflux_scaling, d/djac[0..3]
+ *   per scale i  (1): d/dscale
+ * Returns the count (>= 6) or a negative GSB_ERR_* code.  Size parameters have no entry of
+ * their own: each leaf depends on its size s and Jacobian J only through s J, so
+ * d/d(ln s) = sum_ij J_ij d/dJ_ij (Box: width with J[0], J[2]; height with J[1], J[3]).
+ * For a Sersic leaf with GSB_LEAF_SIZE_IS_HLR the n entry is at fixed half-light radius. */
+int gsb_adjoint_grad_count(const gsb_template* tpl);
+
+/* Scratch bytes gsb_adjoint_images needs for a bucket of stamps of FFT size N. */
+size_t gsb_adjoint_workspace_size(int N, int n_stamps, int precision);
+
+/* Reverse mode of gsb_draw_images for one FFT-size bucket (N in 32..1024): given
+ * d_cotangent = dL/d(image), laid out exactly as the images gsb_draw_images writes for the same
+ * stamps (out_offset, nx, ny; dtype cot_dtype), write d_grad[s * count + e] = dL/d(entry e of
+ * stamp s) (FP64, count from gsb_adjoint_grad_count).  The derivatives are analytic (each
+ * profile's dkValue/dparameter, the phase and the products of the program) and are taken on
+ * the stamp's fixed grid (N, Nk); clipped k-points contribute zero.  Sersic leaves need tables
+ * built with GSB_TABLES_DN.  No reference counterpart (the reference has no derivatives); it
+ * is the adjoint of gsobject.py:1927-2045 + src/Image.cpp:578-912 for fixed sizes. */
+int gsb_adjoint_images(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp,
+                       const gsb_leaf* d_leaves, const gsb_phase* d_phases, const double* d_scales,
+                       const gsb_stamp* d_stamps, const gsb_tables* t, int N,
+                       const void* d_cotangent, int cot_dtype, double* d_grad, int precision,
+                       void* d_workspace, size_t workspace_bytes, void* stream);
 
 #ifdef __cplusplus
 }

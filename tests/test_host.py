@@ -84,3 +84,29 @@ def test_draw_requires_gpu_without_fallback():
         pytest.skip('a GPU is present')
     with pytest.raises(galsim.GalSimError):
         galsim.Gaussian(sigma=1.).drawImage(nx=16, ny=16, scale=0.2)
+
+
+def test_adjoint_gradient_layout_from_library():
+    """gsb_adjoint_grad_count is host logic: 6 entries per leaf, 7 per phase, 1 per scale."""
+    import ctypes
+    from galsim_b200 import _lib
+    from galsim_b200.program import Program
+    obj = galsim.Convolve(galsim.Sersic(n=2., half_light_radius=0.5).shear(g1=0.1, g2=0.).shift(0.1, 0.),
+                          galsim.Moffat(beta=2.5, fwhm=0.8) * 2., galsim.Pixel(0.2))
+    prog = Program(obj)
+    L, P, S = len(prog.bld.leaves), len(prog.bld.phases), len(prog.bld.scales)
+    assert (L, P, S) == (3, 1, 1)
+    n = _lib.lib().gsb_adjoint_grad_count(ctypes.byref(prog.tpl))
+    assert n == 6 * L + 7 * P + S
+    bad = _lib.TemplateC()
+    assert _lib.lib().gsb_adjoint_grad_count(ctypes.byref(bad)) < 0   # empty template
+
+
+def test_torch_shear_matrix_matches_shear():
+    import torch
+    from galsim_b200.autodiff import shear_matrix
+    g1 = np.array([0.1, -0.3, 0.0, 0.25])
+    g2 = np.array([0.05, 0.2, 0.0, -0.4])
+    m = shear_matrix(torch.as_tensor(g1), torch.as_tensor(g2)).numpy()
+    ref = galsim.Shear(g1=g1, g2=g2).getMatrix()
+    np.testing.assert_allclose(m, ref, rtol=1e-15, atol=1e-15)
