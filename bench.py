@@ -13,6 +13,12 @@ GPU, GalSim's integer sizing on the host, and the fused k-space/wrap/FFT/crop ke
 `value` is stamps/s with the flattened inputs resident in HBM; `e2e` is the same through
 the public API (galsim_b200.draw_batch) from host parameter arrays to host pixels.
 
+`grad_evals` is the differentiable fit step: 1024 stamps of 48x48 of
+Convolve(Sersic(n, hlr, flux).shear(g1, g2).shift(dx, dy), Moffat(2.5, fwhm=0.8), Pixel(0.2)),
+chi^2 against a noisy target (SNR 50) and its gradient in the seven parameters through the
+adjoint kernels (galsim_b200.autodiff), timed from host parameters to host gradients.
+Both carry the plain one-stamp-per-call rate of the same path beside them.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
 import argparse
@@ -49,6 +55,78 @@ def workload_params(B=B_DEFAULT, seed=1234):
         fwhm = rng.uniform(0.6, 0.9)
         p[i] = (n, hlr, flux, g1, g2, fwhm)
     return p
+
+
+FIT_B = 1024
+FIT_NX = 48
+
+
+def fit_params(B=FIT_B, seed=4321):
+    """Fit-step parameters (flux, hlr, n, g1, g2, dx, dy): n ~ U[1, 3], hlr ~ U[0.3, 1.2]",
+    flux lognormal(median 1e4, sigma_ln 0.5), g1, g2 ~ N(0, 0.1), dx, dy ~ N(0, 0.1)"; the target
+    is drawn at parameters perturbed by 3% (0.02 absolute for g and the centroid) plus Gaussian
+    noise at SNR 50."""
+    rng = np.random.default_rng(seed)
+    true = np.stack([1e4 * np.exp(rng.normal(0., 0.5, B)), rng.uniform(0.3, 1.2, B),
+                     rng.uniform(1., 3., B), rng.normal(0., 0.1, B), rng.normal(0., 0.1, B),
+                     rng.normal(0., 0.1, B), rng.normal(0., 0.1, B)], -1)
+    pert = true * (1. + rng.normal(0., 0.03, true.shape)) + \
+        rng.normal(0., 0.02, true.shape) * np.array([0., 0., 0., 1., 1., 1., 1.])
+    return true, pert, rng
+
+
+def run_fit_step(args, galsim, dev, steps, warmup):
+    """grad-evals/s of the chi^2 fit step: 1024 stamps of 48x48, Convolve(Sersic(n, hlr, flux)
+    .shear(g1, g2).shift(dx, dy), Moffat(2.5, fwhm=0.8), Pixel(0.2)); one grad-eval = forward
+    draw + chi^2 + adjoint for one stamp (FP32 kernels, FP64 tables and sizing on the GPU)."""
+    import torch
+    from galsim_b200 import autodiff
+    psf = galsim.Convolve(galsim.Moffat(beta=2.5, fwhm=0.8), galsim.Pixel(SCALE))
+    true, pert, rng = fit_params()
+    B = len(pert)
+    m64 = autodiff.GalaxyModel(psf, FIT_NX, FIT_NX, SCALE, dtype=np.float64, precision='fp64')
+    timg = m64(torch.as_tensor(true, device=dev)).detach()
+    sigma = torch.sqrt((timg ** 2).sum(dim=(1, 2))) / 50.
+    target = (timg + sigma[:, None, None] * torch.as_tensor(
+        rng.standard_normal(tuple(timg.shape)), device=dev)).float()
+    model = autodiff.GalaxyModel(psf, FIT_NX, FIT_NX, SCALE, dtype=np.float32, precision='fp32')
+    isig = (1. / sigma).float()[:, None, None]
+
+    def step(p_host):
+        p = torch.as_tensor(p_host, device=dev).requires_grad_(True)
+        chi2 = (((model(p) - target) * isig) ** 2).sum()
+        chi2.backward()
+        return p.grad
+
+    for _ in range(warmup):
+        step(pert)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        g = step(pert).cpu()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    # plain: one stamp per call
+    n_plain = 16
+    for i in range(2):
+        step(pert[i:i + 1])
+    torch.cuda.synchronize(dev)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record()
+    for i in range(n_plain):
+        p = torch.as_tensor(pert[i:i + 1], device=dev).requires_grad_(True)
+        (((model(p) - target[i:i + 1]) * isig[i:i + 1]) ** 2).sum().backward()
+    p1.record()
+    torch.cuda.synchronize(dev)
+    plain = n_plain / (p0.elapsed_time(p1) * 1e-3)
+    N = model.plan.last.N
+    return {'value': B / (ms * 1e-3), 'unit': 'grad-evals/s', 'ms_per_step': ms, 'stamps': B,
+            'workload': 'sersic_moffat25_pixel_48x48_1024_seed4321 chi2 gradient (flux, hlr, n, g1, g2, dx, dy)',
+            'fft_sizes': sorted(set(int(v) for v in N)),
+            'timed': 'host parameters -> forward + chi2 + adjoint -> host gradients',
+            'plain_one_stamp_per_launch': {'value': plain, 'unit': 'grad-evals/s', 'sample': n_plain}}
 
 
 def gpu_object(galsim, p):
@@ -311,6 +389,8 @@ def run_gpu(args):
     torch.cuda.synchronize(dev)
     plain_rate = n_plain / (tp0.elapsed_time(tp1) * 1e-3)
 
+    fit = run_fit_step(args, galsim, dev, max(args.steps, 3), max(args.warmup, 2))
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference_rate(params, budget_s=15.)
@@ -333,6 +413,7 @@ def run_gpu(args):
                          'kernel_ms': k_ms},
             'gpu_launches': int(args.steps * (nb + 5)),
             'plain_one_stamp_per_launch': {'value': plain_rate, 'unit': 'stamps/s', 'sample': n_plain},
+            'grad_evals': fit,
             'clocks': clk.summary(),
         }
         if cpu is not None:

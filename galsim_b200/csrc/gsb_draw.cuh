@@ -258,12 +258,13 @@ __device__ inline T sersic_kvalue_smem(const SersicTableView& tb, const typename
     if (i >= tb.n) i = tb.n - 1;
     if (i <= 0) i = 1;
     const typename NodeT<T>::type n0 = node[i - 1], n1 = node[i];
-    // The table is equally spaced (spacing da), so 1/h = 1/da up to rounding.
+    // Divide by h formed from the same (rounded) node positions as aa and bb, so that the
+    // interpolation weights aa / h + bb / h sum to 1 exactly; 1/da instead costs ~1e-6 in FP32.
     const T h = n1.x - n0.x;
     const T aa = n1.x - lk;
     const T bb = h - aa;
     const T num = aa * n0.y + bb * n1.y - (T(1) / T(6)) * aa * bb * ((aa + h) * n0.z + (bb + h) * n1.z);
-    return num * inv_da / ksq;
+    return num / h / ksq;
 }
 
 // Program evaluation with the caches and a 4-deep register stack (warp-uniform branches).
