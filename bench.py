@@ -273,20 +273,32 @@ def run_stage(args):
     from galsim_b200 import _lib
     params = workload_params(args.stamps)
     obj = gpu_object(galsim, params)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if args.stage == 'tables':
         t = _lib.Tables()
         n = params[:, 0]
-        for _ in range(args.warmup + args.steps):
+        for _ in range(args.warmup):
             t.build_sersic(n, galsim.GSParams())
         torch.cuda.synchronize()
-        print(json.dumps({'stage': 'tables', 'tables': len(n)}))
+        e0.record()
+        for _ in range(args.steps):
+            t.build_sersic(n, galsim.GSParams())
+        e1.record()
+        torch.cuda.synchronize()
+        print(json.dumps({'stage': 'tables', 'tables': len(n), 'ms_per_build': e0.elapsed_time(e1) / args.steps}))
         return
     plan = galsim.plan_batch(obj, nx=args.nx, ny=args.nx, scale=SCALE, dtype=np.float32)
-    for _ in range(args.warmup + args.steps):
+    for _ in range(args.warmup):
         st = galsim.run_batch(plan)
     torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        st = galsim.run_batch(plan)
+    e1.record()
+    torch.cuda.synchronize()
     u, c = np.unique(st.N, return_counts=True)
-    print(json.dumps({'stage': 'draw', 'stamps': len(st), 'buckets': dict(zip(map(int, u), map(int, c)))}))
+    print(json.dumps({'stage': 'draw', 'stamps': len(st), 'ms_per_step': e0.elapsed_time(e1) / args.steps,
+                      'buckets': dict(zip(map(int, u), map(int, c)))}))
 
 
 def run_gpu(args):

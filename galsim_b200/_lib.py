@@ -85,6 +85,8 @@ def lib():
             'gsb_draw_workspace_size': (sz, [i, i, i]),
             'gsb_draw_images': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp, vp,
                                     vp, vp, vp, i, i, vp, i, vp, sz, vp]),
+            'gsb_draw_bucket': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp, vp,
+                                    vp, vp, i, vp, i, i, vp, i, vp, sz, vp]),
             'gsb_draw_kimages': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp,
                                      vp, vp, d, i, i, i, i, vp, i, vp]),
         }
@@ -139,6 +141,18 @@ class Device(object):
     def stream(cls):
         import torch
         return ctypes.c_void_p(torch.cuda.current_stream(cls.torch_device()).cuda_stream)
+
+    _side = {}
+
+    @classmethod
+    def side_streams(cls, n):
+        """n reusable side streams of the current device (for concurrent FFT-size buckets)."""
+        import torch
+        dev = cls.torch_device()
+        lst = cls._side.setdefault(dev.index, [])
+        while len(lst) < n:
+            lst.append(torch.cuda.Stream(device=dev))
+        return lst[:n]
 
 
 def set_device(index):

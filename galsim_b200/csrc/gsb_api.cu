@@ -230,6 +230,27 @@ int gsb_draw_images(const gsb_template* tpl, int n_stamps, const gsb_gsparams* g
                        (cudaStream_t)stream);
 }
 
+int gsb_draw_bucket(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp,
+                    const gsb_leaf* d_leaves, const gsb_phase* d_phases, const double* d_scales,
+                    const gsb_stamp* d_stamps, const gsb_tables* t, int N,
+                    void* d_out, int out_dtype, int add_to_image, double* d_added_flux,
+                    int precision, void* d_workspace, size_t workspace_bytes, void* stream)
+{
+    int rc = validate_template(tpl);
+    if (rc) return rc;
+    if (!gsp) return set_error(GSB_ERR_INVALID, "null gsparams");
+    if (n_stamps < 0) return set_error(GSB_ERR_INVALID, "negative stamp count");
+    if (n_stamps == 0) return GSB_OK;
+    if (!d_leaves || !d_stamps || !d_out || (tpl->n_phases && !d_phases) || (tpl->n_scales && !d_scales))
+        return set_error(GSB_ERR_INVALID, "null device pointer");
+    if (out_dtype != GSB_F32 && out_dtype != GSB_F64) return set_error(GSB_ERR_INVALID, "bad out_dtype");
+    if (precision != GSB_F32 && precision != GSB_F64) return set_error(GSB_ERR_INVALID, "bad precision");
+    if (!good_fft_size_ok(N)) return set_error(GSB_ERR_INVALID, "N is not 2^a or 3*2^a");
+    return draw_images(tpl, n_stamps, d_leaves, d_phases, d_scales, d_stamps, t, N, d_out,
+                       out_dtype, add_to_image, d_added_flux, precision, d_workspace, workspace_bytes,
+                       (cudaStream_t)stream);
+}
+
 int gsb_draw_kimages(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp,
                      const gsb_leaf* d_leaves, const gsb_phase* d_phases, const double* d_scales,
                      const gsb_tables* t, double dk, int kxmin, int kymin, int nkx, int nky,

@@ -47,10 +47,23 @@ __global__ void ogata_level_kernel(double2* xw, const double2* root, double h, l
     xw[i] = ogata_node(root, h, i);
 }
 
+__device__ inline double warp_total(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Running-sum estimate refresh: every chunk for the first kEagerChunks chunks (short sums stop
+// there), then every kLazyChunks chunks.
+constexpr int kEagerChunks = 2;
+constexpr int kLazyChunks = 8;
+
 // Sum_i w_i f(x_i / k) / k^2 for h = 2^-lev with the reference's stopping rule: stop at the
 // first term whose magnitude is below 1e-15 |running sum| (Hankel.cpp:117-141).  The integrand
 // is called with log(x_i / k) = log x_i - log k (nodes store log x), which spares a division
-// and a logarithm per term.
+// and a logarithm per term.  Each lane keeps the sum of its own terms; the warp total is formed
+// only every few chunks, and the stopping test uses that total.  The stop can therefore move by
+// terms below 1e-15 of the sum, which changes the result only at that level.
 template <class F>
 __device__ double warp_ogata_sum(const OgataTables& og, const F& f, double k, int lev)
 {
@@ -60,8 +73,9 @@ __device__ double warp_ogata_sum(const OgataTables& og, const F& f, double k, in
     const bool tab = lev >= og.lev_min && lev <= og.lev_max;
     const double2* xw = tab ? og.xw + og.off[lev - og.lev_min] : nullptr;
     const double logk = log(k);
-    double ans = 0.;
-    for (long long base = 0; base < nmax; base += 32) {
+    double acc = 0., thresh = 0.;
+    int chunk = 0;
+    for (long long base = 0; base < nmax; base += 32, ++chunk) {
         const long long i = base + lane;
         const bool valid = i < nmax;
         double step = 0.;
@@ -69,21 +83,16 @@ __device__ double warp_ogata_sum(const OgataTables& og, const F& f, double k, in
             const double2 n = tab ? xw[i] : ogata_node(og.root, h, i);
             step = n.y * f(n.x - logk);
         }
-        double pre = step;
-        for (int o = 1; o < 32; o <<= 1) {
-            const double v = __shfl_up_sync(0xffffffffu, pre, o);
-            if (lane >= o) pre += v;
-        }
-        const double ans_i = ans + pre;
-        const bool stop = valid && fabs(step) < 1e-15 * fabs(ans_i);
-        const unsigned mask = __ballot_sync(0xffffffffu, stop);
+        const unsigned mask = __ballot_sync(0xffffffffu, valid && fabs(step) < thresh);
         if (mask) {
-            ans = __shfl_sync(0xffffffffu, ans_i, __ffs(mask) - 1);
-            return ans / (k * k);
+            const int last = __ffs(mask) - 1;
+            return warp_total(acc + (lane <= last ? step : 0.)) / (k * k);
         }
-        ans = __shfl_sync(0xffffffffu, ans_i, 31);
+        acc += step;
+        if (chunk < kEagerChunks || (chunk % kLazyChunks) == kLazyChunks - 1)
+            thresh = 1e-15 * fabs(warp_total(acc));
     }
-    return ans / (k * k);
+    return warp_total(acc) / (k * k);
 }
 
 // AdaptiveHankelIntegrator::integrate (Hankel.cpp:179-219).  `status` is set to 1 when
@@ -111,6 +120,7 @@ __device__ double warp_hankel(const OgataTables& og, const F& f, double k, doubl
 // The same quadrature for a pair of integrands (f, df/dn) evaluated together: the stopping
 // rules and the level halving follow the first component only, so the first component is
 // bit-identical to warp_ogata_sum / warp_hankel and the second is integrated on the same nodes.
+// (Same lane-local accumulation and lagged stopping test as warp_ogata_sum.)
 template <class F>
 __device__ double2 warp_ogata_sum2(const OgataTables& og, const F& f, double k, int lev)
 {
@@ -120,8 +130,9 @@ __device__ double2 warp_ogata_sum2(const OgataTables& og, const F& f, double k, 
     const bool tab = lev >= og.lev_min && lev <= og.lev_max;
     const double2* xw = tab ? og.xw + og.off[lev - og.lev_min] : nullptr;
     const double logk = log(k);
-    double ans = 0., dans = 0.;
-    for (long long base = 0; base < nmax; base += 32) {
+    double acc = 0., dacc = 0., thresh = 0.;
+    int chunk = 0;
+    for (long long base = 0; base < nmax; base += 32, ++chunk) {
         const long long i = base + lane;
         const bool valid = i < nmax;
         double step = 0., dstep = 0.;
@@ -131,24 +142,19 @@ __device__ double2 warp_ogata_sum2(const OgataTables& og, const F& f, double k, 
             step = n.y * v.x;
             dstep = n.y * v.y;
         }
-        double pre = step, dpre = dstep;
-        for (int o = 1; o < 32; o <<= 1) {
-            const double v = __shfl_up_sync(0xffffffffu, pre, o);
-            const double dv = __shfl_up_sync(0xffffffffu, dpre, o);
-            if (lane >= o) { pre += v; dpre += dv; }
-        }
-        const double ans_i = ans + pre, dans_i = dans + dpre;
-        const bool stop = valid && fabs(step) < 1e-15 * fabs(ans_i);
-        const unsigned mask = __ballot_sync(0xffffffffu, stop);
+        const unsigned mask = __ballot_sync(0xffffffffu, valid && fabs(step) < thresh);
         if (mask) {
-            ans = __shfl_sync(0xffffffffu, ans_i, __ffs(mask) - 1);
-            dans = __shfl_sync(0xffffffffu, dans_i, __ffs(mask) - 1);
-            return make_double2(ans / (k * k), dans / (k * k));
+            const int last = __ffs(mask) - 1;
+            const bool in = lane <= last;
+            return make_double2(warp_total(acc + (in ? step : 0.)) / (k * k),
+                                warp_total(dacc + (in ? dstep : 0.)) / (k * k));
         }
-        ans = __shfl_sync(0xffffffffu, ans_i, 31);
-        dans = __shfl_sync(0xffffffffu, dans_i, 31);
+        acc += step;
+        dacc += dstep;
+        if (chunk < kEagerChunks || (chunk % kLazyChunks) == kLazyChunks - 1)
+            thresh = 1e-15 * fabs(warp_total(acc));
     }
-    return make_double2(ans / (k * k), dans / (k * k));
+    return make_double2(warp_total(acc) / (k * k), warp_total(dacc) / (k * k));
 }
 
 template <class F>

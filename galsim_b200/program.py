@@ -233,20 +233,29 @@ class Program(object):
         out = add_to if add_to is not None else torch.empty(max(g['total'], 1), dtype=tdt, device=dev)
         flux = torch.empty(B, dtype=torch.float64, device=dev)
         flux_sorted = torch.empty(B, dtype=torch.float64, device=dev)
-        stream = _lib.Device.stream()
         lib = _lib.lib()
-        for s0, s1 in zip(g['starts'], g['ends']):
-            n = int(s1 - s0)
-            NN = int(g['Ns'][s0])
-            wbytes = lib.gsb_draw_workspace_size(NN, n, precision)
-            work = torch.empty(max(int(wbytes), 8), dtype=torch.uint8, device=dev) if wbytes else None
+        # One stream per FFT-size bucket, largest N first: the few long-running stamps of the
+        # big-N buckets take their SMs first and overlap the large small-N buckets.  The
+        # workspaces are allocated on the current stream before the fork and released after
+        # the join, so the caching allocator cannot hand them out while a bucket runs.
+        main = torch.cuda.current_stream(dev)
+        buckets = sorted(zip(g['starts'], g['ends']), key=lambda se: -int(g['Ns'][se[0]]))
+        works = []
+        for s0, s1 in buckets:
+            wbytes = int(lib.gsb_draw_workspace_size(int(g['Ns'][s0]), int(s1 - s0), precision))
+            works.append((wbytes, torch.empty(max(wbytes, 8), dtype=torch.uint8, device=dev) if wbytes else None))
+        streams = _lib.Device.side_streams(len(buckets))
+        for (s0, s1), (wbytes, work), st in zip(buckets, works, streams):
+            st.wait_stream(main)
             lvp, php, scp, stp = self._bucket_ptrs(g, s0)
-            _lib.check(lib.gsb_draw_images(
-                ctypes.byref(self.tpl), n, ctypes.byref(self.gsp_c), lvp, php, scp, stp,
-                self.tables.handle if self.tables else None,
+            _lib.check(lib.gsb_draw_bucket(
+                ctypes.byref(self.tpl), int(s1 - s0), ctypes.byref(self.gsp_c), lvp, php, scp, stp,
+                self.tables.handle if self.tables else None, int(g['Ns'][s0]),
                 _lib.ptr(out), dtype, 1 if add_to is not None else 0,
                 ctypes.c_void_p(flux_sorted.data_ptr() + int(s0) * 8),
-                precision, _lib.ptr(work), ctypes.c_size_t(int(wbytes)), stream))
+                precision, _lib.ptr(work), ctypes.c_size_t(wbytes), ctypes.c_void_p(st.cuda_stream)))
+        for st in streams:
+            main.wait_stream(st)
         flux[g['perm']] = flux_sorted
         return out, g['offsets'], flux
 

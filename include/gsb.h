@@ -195,6 +195,16 @@ int gsb_draw_images(const gsb_template* tpl, int n_stamps, const gsb_gsparams* g
                     void* d_out, int out_dtype, int add_to_image, double* d_added_flux,
                     int precision, void* d_workspace, size_t workspace_bytes, void* stream);
 
+/* gsb_draw_images for a bucket whose FFT size N the caller passes (every stamp's N must equal
+ * it): no host synchronisation, so buckets can run concurrently on several streams and the
+ * call can be captured in a CUDA graph (after a first call with the same N and precision,
+ * which may set up device state).  Same contract as gsb_draw_images otherwise. */
+int gsb_draw_bucket(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp,
+                    const gsb_leaf* d_leaves, const gsb_phase* d_phases, const double* d_scales,
+                    const gsb_stamp* d_stamps, const gsb_tables* t, int N,
+                    void* d_out, int out_dtype, int add_to_image, double* d_added_flux,
+                    int precision, void* d_workspace, size_t workspace_bytes, void* stream);
+
 /* drawKImage: evaluate the program on an (nkx x nky) grid of k points
  * kx = (kxmin + i) dk, ky = (kymin + j) dk, into complex output (interleaved re, im) with
  * row stride nkx.  One grid per stamp, stamp s at d_out + s * nkx * nky complex elements.
