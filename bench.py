@@ -129,6 +129,126 @@ def run_fit_step(args, galsim, dev, steps, warmup):
             'plain_one_stamp_per_launch': {'value': plain, 'unit': 'grad-evals/s', 'sample': n_plain}}
 
 
+MIX_B = 16384
+LARGE_B = 64
+
+
+def mixed_params(B=MIX_B, seed=2468):
+    """Bulge + disk batch: total flux lognormal(median 1e4, sigma_ln 0.5), bulge fraction
+    U[0, 0.6], bulge hlr lognormal(median 0.4", sigma_ln 0.3), disk hlr lognormal(median 0.8",
+    sigma_ln 0.3), independent shears N(0, 0.2) clipped to |g| < 0.6, Moffat beta ~ U[2.5, 4.5]
+    and fwhm ~ U[0.5, 1.0]"."""
+    rng = np.random.default_rng(seed)
+    flux = 1e4 * np.exp(rng.normal(0., 0.5, B))
+    bf = rng.uniform(0., 0.6, B)
+    bh = 0.4 * np.exp(rng.normal(0., 0.3, B))
+    dh = 0.8 * np.exp(rng.normal(0., 0.3, B))
+
+    def shear():
+        g = rng.normal(0., 0.2, (B, 2))
+        a = np.hypot(g[:, 0], g[:, 1])
+        return g * np.where(a >= 0.6, 0.599 / np.maximum(a, 1e-300), 1.)[:, None]
+
+    g_b, g_d = shear(), shear()
+    beta = rng.uniform(2.5, 4.5, B)
+    fwhm = rng.uniform(0.5, 1.0, B)
+    return dict(flux=flux, bf=bf, bh=bh, dh=dh, g_b=g_b, g_d=g_d, beta=beta, fwhm=fwhm)
+
+
+def mixed_object(galsim, m, gsp):
+    bulge = galsim.Sersic(n=4., half_light_radius=m['bh'], flux=m['flux'] * m['bf'], gsparams=gsp) \
+        .shear(g1=m['g_b'][:, 0], g2=m['g_b'][:, 1])
+    disk = galsim.Exponential(half_light_radius=m['dh'], flux=m['flux'] * (1. - m['bf']), gsparams=gsp) \
+        .shear(g1=m['g_d'][:, 0], g2=m['g_d'][:, 1])
+    psf = galsim.Moffat(beta=m['beta'], fwhm=m['fwhm'], gsparams=gsp)
+    return galsim.Convolve(galsim.Add(bulge, disk), psf, galsim.Pixel(SCALE, gsparams=gsp))
+
+
+def run_mixed(galsim, dev, steps, warmup):
+    """Mixed-size batch: stamps/s forward and forward+adjoint (record gradients for a random
+    cotangent), automatically sized stamps with minimum_fft_size=32 (FFT sizes 32..1024)."""
+    import torch
+    from galsim_b200 import _lib
+    gsp = galsim.GSParams(minimum_fft_size=32)
+    m = mixed_params()
+    plan = galsim.plan_batch(mixed_object(galsim, m, gsp), scale=SCALE, dtype=np.float32)
+    prog = plan.prog
+    prog.need_dn = True
+    st = galsim.run_batch(plan)
+    cot = torch.randn(st.flat.numel(), device=dev, dtype=torch.float32)
+
+    def fwd():
+        return galsim.run_batch(plan)
+
+    def fwd_adj():
+        s = galsim.run_batch(plan)
+        return prog.adjoint_stamps(cot[:s.flat.numel()], _lib.F32)
+
+    out = {}
+    for name, fn in (('forward', fwd), ('forward_adjoint', fwd_adj)):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        out[name] = MIX_B / (e0.elapsed_time(e1) / steps * 1e-3)
+    u, c = np.unique(st.N, return_counts=True)
+    return {'value': out['forward'], 'unit': 'stamps/s', 'forward_adjoint': out['forward_adjoint'],
+            'forward_adjoint_unit': 'grad-evals/s', 'stamps': MIX_B,
+            'workload': 'bulge_disk_moffat_gen_pixel_16384_seed2468 (Sersic n=4 + Exponential, Moffat beta U[2.5,4.5])',
+            'gsparams': 'minimum_fft_size=32', 'fft_sizes': dict(zip(map(int, u), map(int, c)))}
+
+
+def run_large(galsim, dev):
+    """Large-stamp precision study: 64 stamps of Sersic(n ~ U[4, 6], hlr ~ U[2, 5]") x
+    Airy(lam/D = 0.1", obscuration 0.3) x Pixel(0.05), default GSParams (folding 5e-3, maxk
+    1e-3), automatic sizes; FP32 and FP64 renders, FP32 error per stamp against FP64 (which
+    matches the reference to 1e-9 x peak on the large-FFT fixtures)."""
+    import torch
+    rng = np.random.default_rng(97531)
+    n = rng.uniform(4., 6., LARGE_B)
+    hlr = rng.uniform(2., 5., LARGE_B)
+    flux = np.full(LARGE_B, 1e5)
+    times = {'fp32': 0., 'fp64': 0.}
+    N_all, err, ferr, npix = [], [], [], []
+    chunk = 8
+    for c0 in range(0, LARGE_B, chunk):
+        sub = galsim.Convolve(galsim.Sersic(n=n[c0:c0 + chunk], half_light_radius=hlr[c0:c0 + chunk],
+                                            flux=flux[c0:c0 + chunk]),
+                              galsim.Airy(lam_over_diam=0.1, obscuration=0.3), galsim.Pixel(0.05))
+        res = {}
+        for prec, dt in (('fp32', np.float32), ('fp64', np.float64)):
+            plan = galsim.plan_batch(sub, scale=0.05, dtype=dt, precision=prec)
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            sb = galsim.run_batch(plan)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            times[prec] += e0.elapsed_time(e1) * 1e-3
+            res[prec] = sb
+        a, b = res['fp32'], res['fp64']
+        fa, fb = a.added_flux, b.added_flux
+        for i in range(len(a)):
+            o, m_ = int(a.offsets[i]), int(a.nx[i] * a.ny[i])
+            d = (a.flat[o:o + m_].double() - b.flat[o:o + m_]).abs().max().item()
+            pk = b.flat[o:o + m_].abs().max().item()
+            err.append(d / pk)
+            ferr.append(abs(fa[i] - fb[i]) / abs(fb[i]))
+            N_all.append(int(a.N[i]))
+            npix.append(m_)
+        del res, a, b
+    return {'value': LARGE_B / times['fp32'], 'unit': 'stamps/s', 'fp64_stamps_per_s': LARGE_B / times['fp64'],
+            'stamps': LARGE_B, 'workload': 'sersic_n4to6_airy_pixel005_64_seed97531',
+            'fft_sizes': N_all, 'pixels': npix,
+            'fp32_max_abs_err_over_peak': err, 'fp32_flux_rel_err': ferr,
+            'reference_check': 'FP64 renders match the reference C++ to 1e-9 x peak on tests/golden/reference_large.npz'}
+
+
 def gpu_object(galsim, p):
     gal = galsim.Sersic(n=p[:, 0], half_light_radius=p[:, 1], flux=p[:, 2]).shear(g1=p[:, 3], g2=p[:, 4])
     return galsim.Convolve(gal, galsim.Kolmogorov(fwhm=p[:, 5]), galsim.Pixel(SCALE))
@@ -152,26 +272,41 @@ class ClockSampler(object):
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.lines = []
 
     def __enter__(self):
+        import threading
         try:
             self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.index), '--query-gpu=' + self.QUERY,
-                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                          '--format=csv,noheader,nounits', '-lms', '100'],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return self
+
+        def reader():
+            for line in self.proc.stdout:
+                if line.strip():
+                    self.lines.append(line)
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
         return self
 
+    def wait_first(self, timeout=5.):
+        """Block until the sampler has produced its first line (so the timed region is covered)."""
+        t0 = time.time()
+        while self.proc is not None and not self.lines and time.time() - t0 < timeout:
+            time.sleep(0.02)
+
     def __exit__(self, *a):
-        self.lines = []
         if self.proc is not None:
             self.proc.terminate()
             try:
-                out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+                self.proc.wait()
+            self.thread.join(timeout=5)
 
     def summary(self):
         sm, smax, reasons = [], 0., set()
@@ -187,7 +322,8 @@ class ClockSampler(object):
                 if v.lower() == 'active':
                     reasons.add(nm)
         return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': smax or None,
-                'reasons': sorted(reasons), 'samples': len(sm)}
+                'reasons': sorted(reasons), 'samples': len(sm),
+                'window': 'every 100 ms across the warm-up, the timed steps and the e2e steps'}
 
 
 def measured_peak_hbm():
@@ -323,20 +459,23 @@ def run_gpu(args):
         if world > 1:
             dist.barrier()
 
+    # Clocks are sampled (every 100 ms) from before the warm-up until after the e2e region; the
+    # timed loop starts only once the sampler is producing.
+    clk = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
         st = galsim.run_batch(plan)
     barrier()
+    clk.wait_first()
     # L2 note: the working set (tables ~100 MB, stamp outputs ~50 MB, per-CTA W slabs) is
     # rewritten every step by the table build; inputs are re-read from HBM each step.
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        barrier()
-        start.record()
-        for _ in range(args.steps):
-            st = galsim.run_batch(plan)
-        stop.record()
-        barrier()
+    barrier()
+    start.record()
+    for _ in range(args.steps):
+        st = galsim.run_batch(plan)
+    stop.record()
+    barrier()
     ms = start.elapsed_time(stop) / args.steps
     t_step = torch.tensor([ms], device=dev, dtype=torch.float64)
     if world > 1:
@@ -377,6 +516,7 @@ def run_gpu(args):
     ee.record()
     barrier()
     e2e_ms = es.elapsed_time(ee) / args.steps
+    clk.__exit__(None, None, None)
     t_e = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
     if world > 1:
         dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
@@ -402,6 +542,8 @@ def run_gpu(args):
     plain_rate = n_plain / (tp0.elapsed_time(tp1) * 1e-3)
 
     fit = run_fit_step(args, galsim, dev, max(args.steps, 3), max(args.warmup, 2))
+    mixed = run_mixed(galsim, dev, max(args.steps, 3), max(args.warmup, 2)) if not args.no_extra else None
+    large = run_large(galsim, dev) if not args.no_extra else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -426,6 +568,8 @@ def run_gpu(args):
             'gpu_launches': int(args.steps * (nb + 5)),
             'plain_one_stamp_per_launch': {'value': plain_rate, 'unit': 'stamps/s', 'sample': n_plain},
             'grad_evals': fit,
+            'mixed_batch': mixed,
+            'large_stamps': large,
             'clocks': clk.summary(),
         }
         if cpu is not None:
@@ -442,6 +586,8 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='gsb', choices=['gsb', 'reference'])
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline measurement')
+    ap.add_argument('--no-extra', action='store_true',
+                    help='skip the mixed-batch and large-stamp measurements')
     ap.add_argument('--stamps', type=int, default=B_DEFAULT, help='stamps per GPU (leading subset)')
     ap.add_argument('--nx', type=int, default=None, help='fixed stamp size (default: automatic)')
     ap.add_argument('--stage', default='all', choices=['all', 'draw', 'tables'],

@@ -192,6 +192,7 @@ class Tables(object):
                                                TABLES_DN if with_dn else 0, Device.stream()))
         self.count = len(n)
         self.with_dn = with_dn
+        self.generation = getattr(self, 'generation', 0) + 1
 
     def sersic_info(self, count=None):
         count = self.count if count is None else count

@@ -34,12 +34,13 @@ class RecordPlan(object):
     numeric records can be replaced from tensors before each draw."""
 
     def __init__(self, obj, nx, ny, scale, dtype=np.float32, precision='fp32', offset=None,
-                 use_true_center=True):
+                 use_true_center=True, tables=None):
         from .batch import plan_batch
         if nx is None or ny is None:
             raise GalSimValueError("differentiable drawing needs fixed stamp sizes nx, ny", (nx, ny))
         self.batch_plan = plan_batch(obj, nx, ny, scale, dtype, offset=offset,
-                                     use_true_center=use_true_center, precision=precision)
+                                     use_true_center=use_true_center, precision=precision,
+                                     tables=tables)
         self.prog = self.batch_plan.prog
         self.prog.need_dn = True
         self.B = self.prog.B
@@ -123,6 +124,8 @@ class RecordPlan(object):
         from .batch import run_batch
         sb = run_batch(self.batch_plan)
         self.last = sb
+        t = self.prog.tables
+        self._tables_gen = (t, t.generation) if t is not None else None
         return sb.stack()
 
     def adjoint(self, cot):
@@ -131,6 +134,10 @@ class RecordPlan(object):
         if self.last is None:
             raise GalSimError("RecordPlan.adjoint needs a preceding draw")
         B, L, P, S = self.B, self.L, self.P, self.S
+        if self._tables_gen is not None and self._tables_gen[0].generation != self._tables_gen[1]:
+            # a shared table set was rebuilt for another draw since ours: rebuild our slots
+            self.prog.tables.build_sersic(self.prog.sersic_n, self.prog.gsparams, with_dn=True)
+            self._tables_gen = (self.prog.tables, self.prog.tables.generation)
         dt = _lib.F32 if self.dtype == np.float32 else _lib.F64
         tdt = torch.float32 if dt == _lib.F32 else torch.float64
         c = cot.to(dtype=tdt).contiguous().reshape(-1)
@@ -216,6 +223,7 @@ class GalaxyModel(object):
         self.precision = precision
         self.gsparams = gsparams
         self.plan = None
+        self.tables = None        # device Sersic tables, rebuilt in place on every call
 
     def build(self, p):
         """The batched GSObject for parameters p ((B, 7) numpy)."""
@@ -232,7 +240,10 @@ class GalaxyModel(object):
     def __call__(self, params):
         import torch
         p = params.detach().to('cpu', torch.float64).numpy()
-        plan = RecordPlan(self.build(p), self.nx, self.ny, self.scale, self.dtype, self.precision)
+        if self.tables is None:
+            self.tables = _lib.Tables()
+        plan = RecordPlan(self.build(p), self.nx, self.ny, self.scale, self.dtype, self.precision,
+                          tables=self.tables)
         if plan.types[0] != _lib.SERSIC or plan.P < 1:
             raise GalSimError("unexpected program layout for GalaxyModel")
         self.plan = plan

@@ -93,9 +93,11 @@ class BatchPlan(object):
 
 
 def plan_batch(obj, nx=None, ny=None, scale=None, dtype=np.float32, method='fft', area=1.,
-               exptime=1., gain=1., offset=None, use_true_center=True, precision='fp32'):
+               exptime=1., gain=1., offset=None, use_true_center=True, precision='fp32',
+               tables=None):
     """Host set-up of draw_batch: drawImage's argument handling and world-to-image transform
-    (gsobject.py:1647-1764) applied to the batched object, flattened into a device program."""
+    (gsobject.py:1647-1764) applied to the batched object, flattened into a device program.
+    `tables` (a galsim_b200._lib.Tables) is reused for the Sersic tables when given."""
     from . import box, compound
     from .compound import _Transform
     from .program import Program
@@ -126,7 +128,7 @@ def plan_batch(obj, nx=None, ny=None, scale=None, dtype=np.float32, method='fft'
     if method in ('fft', 'auto'):
         prof = compound.Convolve(prof, box.Pixel(scale=1.0, gsparams=obj.gsparams),
                                  real_space=False, gsparams=obj.gsparams)
-    prog = Program(prof)
+    prog = Program(prof, tables=tables)
     prog.upload()
     return BatchPlan(prog, nx, ny, nx is not None, flux_scale, dtype, scale, precision)
 

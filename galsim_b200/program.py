@@ -105,8 +105,9 @@ def batch_size(obj):
 class Program(object):
     """A flattened batch of profile trees resident on the device, ready to size and draw."""
 
-    def __init__(self, obj, gsparams=None):
+    def __init__(self, obj, gsparams=None, tables=None):
         self.obj = obj
+        self.tables = tables      # a _lib.Tables to (re)build into; one is made when needed
         self.B = batch_size(obj)
         self.gsparams = gsparams if gsparams is not None else obj.gsparams
         bld = Builder(self.B, self.gsparams)

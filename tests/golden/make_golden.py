@@ -102,6 +102,44 @@ SIZE_CASES = [('gauss', 0.7, 1.), ('exp', 0.9, 1.), ('moffat', 3.0, 0.7, 1.), ('
              [('sersic', n, 0.5, 1.) for n in (0.5, 0.8, 1.0, 1.5, 2.5, 4.0, 6.0)]
 
 
+# Large-FFT cases (N > 1024, the precision-study configuration: Sersic n 3..5.5 with an
+# obscured Airy at 0.05" pixels).  The images have millions of pixels, so the fixture keeps a
+# sample: the central 64 x 64 block, a strided grid, and the added flux.
+LARGE_CASES = [
+    ('sersic3_airy_1200', ('conv', [('sersic', 3.0, 1.0, 1e4), ('airy', 0.1, 0.3, 1.0), ('pixel', 0.05)]),
+     1200, 1200, 0.05, 'f4'),
+    ('sersic45_airy_auto', ('conv', [('sersic', 4.5, 2.0, 1e5), ('airy', 0.1, 0.3, 1.0), ('pixel', 0.05)]),
+     None, None, 0.05, 'f4'),
+    ('sersic55_airy_auto_f8', ('conv', [('shear', 0.1, -0.05, ('sersic', 5.5, 2.5, 1e5)),
+                                        ('airy', 0.1, 0.3, 1.0), ('pixel', 0.05)]),
+     None, None, 0.05, 'f8'),
+]
+LARGE_STRIDE = (29, 31)
+
+
+def large_sample(a):
+    """(central 64 x 64 block, strided grid) of an image array."""
+    ny, nx = a.shape
+    cy, cx = ny // 2, nx // 2
+    return a[cy - 32:cy + 32, cx - 32:cx + 32].copy(), a[::LARGE_STRIDE[0], ::LARGE_STRIDE[1]].copy()
+
+
+def main_large(ref_root):
+    from ref_import import import_reference_galsim
+    galsim = import_reference_galsim(ref_root)
+    out = {}
+    for name, spec, nx, ny, scale, dt in LARGE_CASES:
+        im = profile(galsim, spec).drawImage(nx=nx, ny=ny, scale=scale, dtype=np.dtype(dt).type, method='fft')
+        block, grid = large_sample(im.array)
+        out['large_' + name + '_block'] = block
+        out['large_' + name + '_grid'] = grid
+        out['large_' + name + '_shape'] = np.array(im.array.shape)
+        out['large_' + name + '_flux'] = np.array(im.added_flux)
+        out['large_' + name + '_peak'] = np.array(np.abs(im.array).max())
+    np.savez_compressed(os.path.join(HERE, 'reference_large.npz'), **out)
+    print('wrote', os.path.join(HERE, 'reference_large.npz'), len(out), 'arrays')
+
+
 def main(ref_root):
     from ref_import import import_reference_galsim
     galsim = import_reference_galsim(ref_root)
@@ -149,4 +187,8 @@ def main(ref_root):
 
 
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    args = [a for a in sys.argv[1:] if not a.startswith('--')]
+    root = args[0] if args else '/root/reference'
+    if '--large-only' not in sys.argv:
+        main(root)
+    main_large(root)

@@ -213,3 +213,23 @@ def test_adjoint_requires_dn_tables_for_sersic():
     img = plan.draw()
     with pytest.raises(galsim.GalSimError):
         plan.adjoint(torch.ones_like(img))
+
+
+def test_backward_after_a_later_forward_with_shared_tables():
+    """GalaxyModel reuses one device table set; a graph whose tables were rebuilt by a later
+    forward call still gets its own gradients."""
+    psf = galsim.Convolve(galsim.Moffat(beta=2.5, fwhm=0.8), galsim.Pixel(0.2))
+    _, pert, _ = _fit_problem(B=3, seed=9)
+    dev = galsim._lib.Device.torch_device()
+    m = autodiff.GalaxyModel(psf, 48, 48, 0.2, dtype=np.float64, precision='fp64')
+    w = torch.as_tensor(np.random.default_rng(4).standard_normal((3, 48, 48)), device=dev)
+    p1 = torch.as_tensor(pert, device=dev).requires_grad_(True)
+    (m(p1) * w).sum().backward()
+    ref = p1.grad.clone()
+    p1.grad = None
+    loss1 = (m(p1) * w).sum()
+    q = pert.copy()
+    q[:, 2] += 0.7                      # different Sersic n: the shared tables are rebuilt
+    m(torch.as_tensor(q, device=dev))
+    loss1.backward()
+    assert torch.allclose(p1.grad, ref, rtol=1e-12, atol=0.)
