@@ -410,6 +410,28 @@ def run_stage(args):
     params = workload_params(args.stamps)
     obj = gpu_object(galsim, params)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.stage == 'fit':
+        from galsim_b200 import autodiff
+        psf = galsim.Convolve(galsim.Moffat(beta=2.5, fwhm=0.8), galsim.Pixel(SCALE))
+        _, pert, _ = fit_params(min(args.stamps, FIT_B))
+        model = autodiff.GalaxyModel(psf, FIT_NX, FIT_NX, SCALE, dtype=np.float32, precision='fp32')
+        dev = _lib.Device.torch_device()
+        w = torch.randn((len(pert), FIT_NX, FIT_NX), device=dev)
+
+        def step():
+            p = torch.as_tensor(pert, device=dev).requires_grad_(True)
+            (model(p) * w).sum().backward()
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        print(json.dumps({'stage': 'fit', 'stamps': len(pert), 'ms_per_step': e0.elapsed_time(e1) / args.steps}))
+        return
     if args.stage == 'tables':
         t = _lib.Tables()
         n = params[:, 0]
@@ -590,8 +612,8 @@ def main():
                     help='skip the mixed-batch and large-stamp measurements')
     ap.add_argument('--stamps', type=int, default=B_DEFAULT, help='stamps per GPU (leading subset)')
     ap.add_argument('--nx', type=int, default=None, help='fixed stamp size (default: automatic)')
-    ap.add_argument('--stage', default='all', choices=['all', 'draw', 'tables'],
-                    help="'draw' / 'tables': run only that stage (for profiling)")
+    ap.add_argument('--stage', default='all', choices=['all', 'draw', 'tables', 'fit'],
+                    help="'draw' / 'tables' / 'fit': run only that stage (for profiling)")
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)

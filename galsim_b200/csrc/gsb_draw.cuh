@@ -44,6 +44,17 @@ struct StampSmem {
     int phase_cache[GSB_MAX_PHASES];
     int sersic_cache[GSB_MAX_LEAVES];
     int regstack;      // the program fits the 4-deep register stack
+    // Factored form of the program (see plan_factored): the root is a product of atoms; the
+    // separable atoms (diagonal Box / Gaussian leaves, phases, scales) are folded into
+    // XS[i] YS[j + Nk/2] (complex, at offset xy_cache, -1 = not factored) and the others are
+    // evaluated per k-point over their postfix op ranges [atom_o0, atom_o1).
+    int xy_cache;
+    int n_atoms;
+    short atom_o0[GSB_MAX_OPS];
+    short atom_o1[GSB_MAX_OPS];
+    unsigned char leaf_sep[GSB_MAX_LEAVES];    // leaf folded into XS / YS
+    unsigned char phase_sep[GSB_MAX_PHASES];   // phase folded into XS / YS
+    unsigned char scale_sep[GSB_MAX_SCALES];   // scale folded into XS / YS
 };
 
 // Bytes of shared memory reserved for the per-stamp caches.
@@ -164,11 +175,92 @@ template <> struct NodeT<double> { using type = double4; };
 
 // Decide which factors of this stamp are cached in shared memory (thread 0), in order:
 // Sersic spline nodes, phase factors, separable leaf factors, until kCacheBytes is used.
+// Split the program's root product into atoms (thread 0).  MUL nodes are flattened; PHASE and
+// SCALE nodes contribute a separable factor and pass their child on; a LEAF is separable when
+// its value is X(i) Y(j) (Box or Gaussian with a diagonal Jacobian: the reference's 1-d fill);
+// every other LEAF and every ADD subtree is an atom evaluated per point.  Returns false when
+// the atoms do not fit the fixed arrays (the program is then evaluated unfactored).
+__device__ inline bool plan_factored(StampSmem& S, const gsb_template& tpl)
+{
+    short c1[GSB_MAX_OPS], c2[GSB_MAX_OPS], start[GSB_MAX_OPS];
+    short st[GSB_MAX_OPS];
+    int sp = 0;
+    for (int o = 0; o < tpl.n_ops; ++o) {
+        const int code = tpl.op_code[o];
+        c1[o] = c2[o] = -1;
+        if (code == GSB_OP_LEAF) {
+            start[o] = o;
+            st[sp++] = o;
+        } else if (code == GSB_OP_MUL || code == GSB_OP_ADD) {
+            c2[o] = st[--sp];
+            c1[o] = st[sp - 1];
+            start[o] = start[c1[o]];
+            st[sp - 1] = o;
+        } else {
+            c1[o] = st[sp - 1];
+            start[o] = start[c1[o]];
+            st[sp - 1] = o;
+        }
+    }
+    for (int l = 0; l < GSB_MAX_LEAVES; ++l) S.leaf_sep[l] = 0;
+    for (int p = 0; p < GSB_MAX_PHASES; ++p) S.phase_sep[p] = 0;
+    for (int q = 0; q < GSB_MAX_SCALES; ++q) S.scale_sep[q] = 0;
+    S.n_atoms = 0;
+    sp = 0;
+    st[sp++] = tpl.n_ops - 1;
+    while (sp > 0) {
+        const int o = st[--sp];
+        const int code = tpl.op_code[o], arg = tpl.op_arg[o];
+        if (code == GSB_OP_MUL) {
+            st[sp++] = c1[o];
+            st[sp++] = c2[o];
+        } else if (code == GSB_OP_PHASE) {
+            S.phase_sep[arg] = 1;
+            st[sp++] = c1[o];
+        } else if (code == GSB_OP_SCALE) {
+            S.scale_sep[arg] = 1;
+            st[sp++] = c1[o];
+        } else {
+            if (code == GSB_OP_LEAF) {
+                const LeafParams& L = S.leaf[arg];
+                if ((L.type == GSB_BOX || L.type == GSB_GAUSSIAN) && !(L.flags & GSB_LEAF_JAC_GENERAL)) {
+                    S.leaf_sep[arg] = 1;
+                    continue;
+                }
+            }
+            S.atom_o0[S.n_atoms] = start[o];
+            S.atom_o1[S.n_atoms] = o + 1;
+            ++S.n_atoms;
+        }
+    }
+    return true;
+}
+
 template <typename T>
 __device__ inline void plan_caches(StampSmem& S, const gsb_template& tpl, int Nk)
 {
     const int hk = Nk / 2;
     int used = 0;
+    int depth = 0, maxd = 0;
+    for (int o = 0; o < tpl.n_ops; ++o) {
+        const int c = tpl.op_code[o];
+        if (c == GSB_OP_LEAF) ++depth;
+        else if (c == GSB_OP_MUL || c == GSB_OP_ADD) --depth;
+        maxd = depth > maxd ? depth : maxd;
+    }
+    S.regstack = maxd <= 4;
+    S.xy_cache = -1;
+    {
+        const int bytes = ((hk + 1 + Nk + 1) * (int)sizeof(Cx<T>) + 15) & ~15;
+        if (S.regstack && bytes <= kCacheBytes && plan_factored(S, tpl)) {
+            S.xy_cache = used;
+            used += bytes;
+        } else {
+            for (int l = 0; l < GSB_MAX_LEAVES; ++l) S.leaf_sep[l] = 0;
+            for (int p = 0; p < GSB_MAX_PHASES; ++p) S.phase_sep[p] = 0;
+            for (int q = 0; q < GSB_MAX_SCALES; ++q) S.scale_sep[q] = 0;
+        }
+    }
     for (int l = 0; l < tpl.n_leaves; ++l) {
         S.sersic_cache[l] = -1;
         S.leaf_cache[l] = -1;
@@ -179,24 +271,17 @@ __device__ inline void plan_caches(StampSmem& S, const gsb_template& tpl, int Nk
     }
     for (int p = 0; p < tpl.n_phases; ++p) {
         S.phase_cache[p] = -1;
+        if (S.phase_sep[p]) continue;
         const int bytes = ((hk + 1 + Nk + 1) * (int)sizeof(Cx<T>) + 15) & ~15;
         if (used + bytes <= kCacheBytes) { S.phase_cache[p] = used; used += bytes; }
     }
     for (int l = 0; l < tpl.n_leaves; ++l) {
         const LeafParams& L = S.leaf[l];
         const bool sep = !(L.flags & GSB_LEAF_JAC_GENERAL) && (L.type == GSB_BOX || L.type == GSB_GAUSSIAN);
-        if (!sep) continue;
+        if (!sep || S.leaf_sep[l]) continue;
         const int bytes = ((hk + 1 + Nk + 1) * (int)sizeof(T) + 15) & ~15;
         if (used + bytes <= kCacheBytes) { S.leaf_cache[l] = used; used += bytes; }
     }
-    int depth = 0, maxd = 0;
-    for (int o = 0; o < tpl.n_ops; ++o) {
-        const int c = tpl.op_code[o];
-        if (c == GSB_OP_LEAF) ++depth;
-        else if (c == GSB_OP_MUL || c == GSB_OP_ADD) --depth;
-        maxd = depth > maxd ? depth : maxd;
-    }
-    S.regstack = maxd <= 4;
 }
 
 // Fill the planned caches (whole block).
@@ -228,6 +313,41 @@ __device__ inline void fill_caches(const StampSmem& S, const gsb_template& tpl, 
                 const T v = box ? sinc_ref<T>(u) : exp(T(-0.5) * u * u);
                 if (isx) X[i] = v; else Y[i - (hk + 1)] = v;
             }
+        }
+    }
+    if (S.xy_cache >= 0) {
+        // XS[i] = prod over folded atoms of their kx factor (flux, fs and scales in XS),
+        // YS[j + hk] = prod of their ky factor.
+        Cx<T>* XS = reinterpret_cast<Cx<T>*>(cache + S.xy_cache);
+        Cx<T>* YS = XS + hk + 1;
+        for (int t = threadIdx.x; t < hk + 1 + Nk + 1; t += blockDim.x) {
+            const bool isx = t <= hk;
+            const int idx = isx ? t : t - (hk + 1) - hk;
+            Cx<T> v = cx<T>(T(1), T(0));
+            for (int l = 0; l < tpl.n_leaves; ++l) {
+                if (!S.leaf_sep[l]) continue;
+                const LeafParams& L = S.leaf[l];
+                const bool box = L.type == GSB_BOX;
+                const double ax = L.jac[0] * dk * L.d[0];
+                const double ay = L.jac[3] * dk * (box ? L.d[1] : L.d[0]);
+                const T u = T(idx * (isx ? ax : ay));
+                T f = box ? sinc_ref<T>(u) : exp(T(-0.5) * u * u);
+                if (isx) f *= T(L.flux);
+                v = cscale<T>(v, f);
+            }
+            for (int p = 0; p < tpl.n_phases; ++p) {
+                if (!S.phase_sep[p]) continue;
+                double tt = idx * (isx ? S.phase_ax[p] : S.phase_ay[p]);
+                tt -= rint(tt);
+                T sn, cs;
+                sincospi(T(-2. * tt), &sn, &cs);
+                v = cmul<T>(v, cx<T>(cs, sn));
+                if (isx) v = cscale<T>(v, T(S.phase[p].flux_scaling));
+            }
+            if (isx)
+                for (int q = 0; q < tpl.n_scales; ++q)
+                    if (S.scale_sep[q]) v = cscale<T>(v, T(S.scale[q]));
+            if (isx) XS[t] = v; else YS[t - (hk + 1)] = v;
         }
     }
     for (int p = 0; p < tpl.n_phases; ++p) {
@@ -267,34 +387,43 @@ __device__ inline T sersic_kvalue_smem(const SersicTableView& tb, const typename
     return num / h / ksq;
 }
 
-// Program evaluation with the caches and a 4-deep register stack (warp-uniform branches).
+// One leaf at k index (i, j) with the shared-memory caches.
 template <typename T>
-__device__ __forceinline__ Cx<T> eval_fast(const gsb_template& tpl, const StampSmem& S,
-                                           const unsigned char* cache, double dk, int i, int j,
-                                           const GridRef& g)
+__device__ __forceinline__ T leaf_fast(const StampSmem& S, const unsigned char* cache, int arg, T kx, T ky,
+                                       int i, int j, const GridRef& g)
+{
+    const int hk = g.n / 2;
+    const LeafParams& L = S.leaf[arg];
+    if (S.leaf_cache[arg] >= 0) {
+        const T* X = reinterpret_cast<const T*>(cache + S.leaf_cache[arg]);
+        return T(L.flux) * X[i] * X[hk + 1 + j + hk];
+    }
+    if (S.sersic_cache[arg] >= 0) {
+        const T A = T(L.jac[0]), B = T(L.jac[1]), C = T(L.jac[2]), D = T(L.jac[3]);
+        const T kxp = A * kx + C * ky, kyp = B * kx + D * ky;
+        const T r0 = T(L.d[0]);
+        return T(L.flux) * sersic_kvalue_smem<T>(
+                   S.sersic[arg], reinterpret_cast<const typename NodeT<T>::type*>(cache + S.sersic_cache[arg]),
+                   (kxp * kxp + kyp * kyp) * r0 * r0);
+    }
+    return leaf_kvalue<T>(L, S.sersic, kx, ky, g, i - g.x0, j - g.y0);
+}
+
+// Evaluation of the ops [o0, o1) (a complete subtree, or the whole program) with the caches and
+// a 4-deep register stack (warp-uniform branches).
+template <typename T>
+__device__ __forceinline__ Cx<T> eval_range(const gsb_template& tpl, const StampSmem& S,
+                                            const unsigned char* cache, double dk, int i, int j,
+                                            const GridRef& g, int o0, int o1)
 {
     const int hk = g.n / 2;
     Cx<T> s0 = cx<T>(T(0), T(0)), s1 = s0, s2 = s0, s3 = s0;
     int sp = 0;
     const T kx = T(i) * T(dk), ky = T(j) * T(dk);
-    for (int o = 0; o < tpl.n_ops; ++o) {
+    for (int o = o0; o < o1; ++o) {
         const int code = tpl.op_code[o], arg = tpl.op_arg[o];
         if (code == GSB_OP_LEAF) {
-            const LeafParams& L = S.leaf[arg];
-            T v;
-            if (S.leaf_cache[arg] >= 0) {
-                const T* X = reinterpret_cast<const T*>(cache + S.leaf_cache[arg]);
-                v = T(L.flux) * X[i] * X[hk + 1 + j + hk];
-            } else if (S.sersic_cache[arg] >= 0) {
-                const T A = T(L.jac[0]), B = T(L.jac[1]), C = T(L.jac[2]), D = T(L.jac[3]);
-                const T kxp = A * kx + C * ky, kyp = B * kx + D * ky;
-                const T r0 = T(L.d[0]);
-                v = T(L.flux) * sersic_kvalue_smem<T>(
-                        S.sersic[arg], reinterpret_cast<const typename NodeT<T>::type*>(cache + S.sersic_cache[arg]),
-                        (kxp * kxp + kyp * kyp) * r0 * r0);
-            } else {
-                v = leaf_kvalue<T>(L, S.sersic, kx, ky, g, i - g.x0, j - g.y0);
-            }
+            const T v = leaf_fast<T>(S, cache, arg, kx, ky, i, j, g);
             const Cx<T> c = cx<T>(v, T(0));
             if (sp == 0) s0 = c; else if (sp == 1) s1 = c; else if (sp == 2) s2 = c; else s3 = c;
             ++sp;
@@ -328,6 +457,35 @@ __device__ __forceinline__ Cx<T> eval_fast(const gsb_template& tpl, const StampS
         }
     }
     return s0;
+}
+
+template <typename T>
+__device__ __forceinline__ Cx<T> eval_fast(const gsb_template& tpl, const StampSmem& S,
+                                           const unsigned char* cache, double dk, int i, int j,
+                                           const GridRef& g)
+{
+    return eval_range<T>(tpl, S, cache, dk, i, j, g, 0, tpl.n_ops);
+}
+
+// The factored program at (i, j): product of the per-point atoms (real leaves, complex
+// subtrees) times the folded separable factors XS[i] YS[j + hk].
+template <typename T>
+__device__ __forceinline__ Cx<T> eval_factored(const gsb_template& tpl, const StampSmem& S,
+                                               const unsigned char* cache, double dk, int i, int j,
+                                               const GridRef& g)
+{
+    const int hk = g.n / 2;
+    const T kx = T(i) * T(dk), ky = T(j) * T(dk);
+    T r = T(1);
+    Cx<T> c = cx<T>(T(1), T(0));
+    for (int a = 0; a < S.n_atoms; ++a) {
+        const int o0 = S.atom_o0[a], o1 = S.atom_o1[a];
+        if (o1 - o0 == 1) r *= leaf_fast<T>(S, cache, tpl.op_arg[o0], kx, ky, i, j, g);
+        else c = cmul<T>(c, eval_range<T>(tpl, S, cache, dk, i, j, g, o0, o1));
+    }
+    const Cx<T>* XS = reinterpret_cast<const Cx<T>*>(cache + S.xy_cache);
+    const Cx<T> xy = cmul<T>(XS[i], XS[hk + 1 + j + hk]);
+    return cscale<T>(cmul<T>(c, xy), r);
 }
 
 template <typename T>
@@ -379,6 +537,7 @@ __global__ void __launch_bounds__(fused_warps<T, N>() * 32) draw_fused_kernel(co
         fill_caches<T>(S, a.tpl, cache, dk, Nk);
         __syncthreads();
         const bool fast = S.regstack;
+        const bool factored = S.xy_cache >= 0;
 
         // ---- column phase: wrapped k-values, inverse DFT along ky ----
         for (int c = warp; c < H; c += NW) {
@@ -393,8 +552,9 @@ __global__ void __launch_bounds__(fused_warps<T, N>() * 32) draw_fused_kernel(co
                         const int ky = kyc + ib * N;
                         const bool pos = kx >= 0;
                         const int ii = pos ? kx : -kx, jj = pos ? ky : -ky;
-                        Cx<T> v = fast ? eval_fast<T>(a.tpl, S, cache, dk, ii, jj, g)
-                                       : eval_program<T>(a.tpl, S, dk, ii, jj, g);
+                        Cx<T> v = factored ? eval_factored<T>(a.tpl, S, cache, dk, ii, jj, g)
+                                  : fast ? eval_fast<T>(a.tpl, S, cache, dk, ii, jj, g)
+                                         : eval_program<T>(a.tpl, S, dk, ii, jj, g);
                         if (!pos) v = cconj<T>(v);
                         acc = cadd<T>(acc, v);
                     }
