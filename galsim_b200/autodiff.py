@@ -52,6 +52,7 @@ class RecordPlan(object):
         self.precision = _lib.F64 if precision == 'fp64' else _lib.F32
         self.nx, self.ny = int(nx), int(ny)
         self.last = None
+        self._rec_dev = {}
 
     # -- records <-> tensors ----------------------------------------------------------------
     def records(self):
@@ -82,13 +83,29 @@ class RecordPlan(object):
             out['phase_fs'] = np.zeros((B, 0))
             out['phase_jac'] = np.zeros((B, 0, 4))
         out['scales'] = np.stack(bld.scales, axis=1) if S else np.zeros((B, 0))
-        return {k: torch.as_tensor(np.ascontiguousarray(v, dtype=np.float64), device=dev)
-                for k, v in out.items()}
+        # one host-to-device copy for all fields
+        flat = np.concatenate([np.ascontiguousarray(out[k], dtype=np.float64).ravel() for k in RECORD_FIELDS])
+        dflat = torch.as_tensor(flat, device=dev)
+        res, o = {}, 0
+        for k in RECORD_FIELDS:
+            n = out[k].size
+            res[k] = dflat[o:o + n].view(out[k].shape)
+            o += n
+        return res
 
     def set_records(self, rec):
         """Write record tensors (any subset of RECORD_FIELDS) into the host records."""
+        import torch
         bld = self.prog.bld
-        host = {k: v.detach().to('cpu', dtype=__import__('torch').float64).numpy() for k, v in rec.items()}
+        keys = [k for k in RECORD_FIELDS if k in rec]
+        vals = [rec[k].detach().to(torch.float64) for k in keys]
+        self._rec_dev = {k: v for k, v in zip(keys, vals)}
+        flat = torch.cat([v.reshape(-1) for v in vals]).cpu().numpy() if vals else np.zeros(0)
+        host, o = {}, 0
+        for k, v in zip(keys, vals):
+            n = v.numel()
+            host[k] = flat[o:o + n].reshape(tuple(v.shape))
+            o += n
         for l, t in enumerate(self.types):
             r = bld.leaves[l]
             if 'leaf_flux' in host:
@@ -146,7 +163,7 @@ class RecordPlan(object):
         gp = g[:, _lib.GRAD_PER_LEAF * L:_lib.GRAD_PER_LEAF * L + _lib.GRAD_PER_PHASE * P].reshape(
             B, P, _lib.GRAD_PER_PHASE)
         gs = g[:, _lib.GRAD_PER_LEAF * L + _lib.GRAD_PER_PHASE * P:]
-        rec = self.records()
+        rec = self._rec_dev if all(k in self._rec_dev for k in ('leaf_jac', 'leaf_size')) else self.records()
         jac = rec['leaf_jac']
         gjac = gl[..., 1:5]
         size = rec['leaf_size']

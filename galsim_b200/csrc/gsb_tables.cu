@@ -424,91 +424,124 @@ __global__ void sersic_scan_kernel(const double* header, int count, int stride, 
 }
 
 // End of buildFT (SBSersic.cpp:510-537) and the natural spline (Table.cpp:634-686).
-// Natural cubic spline second derivatives (Thomas algorithm) of nodes (x, y) into .z;
-// .w is scratch.  TSpline setup, src/Table.cpp:634-686.
-__device__ void natural_spline(double4* nd, int N)
+// Natural cubic spline second derivatives z of nodes (x, y) (Thomas algorithm; c is scratch).
+// TSpline setup, src/Table.cpp:634-686.
+__device__ void natural_spline(const double* x, const double* y, double* z, double* c, int N)
 {
-    for (int i = 0; i < N; ++i) nd[i].z = 0.;
+    for (int i = 0; i < N; ++i) z[i] = 0.;
     if (N == 3) {
-        nd[1].z = 3. * ((nd[2].y - nd[1].y) / (nd[2].x - nd[1].x) -
-                        (nd[1].y - nd[0].y) / (nd[1].x - nd[0].x)) / (nd[2].x - nd[0].x);
+        z[1] = 3. * ((y[2] - y[1]) / (x[2] - x[1]) - (y[1] - y[0]) / (x[1] - x[0])) / (x[2] - x[0]);
     } else if (N > 3) {
         for (int i = 1; i <= N - 2; ++i)
-            nd[i].z = 6. * ((nd[i + 1].y - nd[i].y) / (nd[i + 1].x - nd[i].x) -
-                            (nd[i].y - nd[i - 1].y) / (nd[i].x - nd[i - 1].x));
-        double bb = 2. * (nd[2].x - nd[0].x);
+            z[i] = 6. * ((y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1]));
+        double bb = 2. * (x[2] - x[0]);
         for (int i = 1; i <= N - 2; ++i) {
-            nd[i].z /= bb;
+            z[i] /= bb;
             if (i == N - 2) break;
-            const double aa = nd[i + 1].x - nd[i].x;
-            const double c = aa / bb;
-            nd[i - 1].w = c;
-            bb = 2. * (nd[i + 2].x - nd[i].x);
-            bb -= aa * c;
-            nd[i + 1].z -= aa * nd[i].z;
+            const double aa = x[i + 1] - x[i];
+            const double cc = aa / bb;
+            c[i - 1] = cc;
+            bb = 2. * (x[i + 2] - x[i]);
+            bb -= aa * cc;
+            z[i + 1] -= aa * z[i];
         }
-        for (int i = N - 3; i > 0; --i) nd[i].z -= nd[i - 1].w * nd[i + 1].z;
+        for (int i = N - 3; i > 0; --i) z[i] -= c[i - 1] * z[i + 1];
     }
 }
 
-__global__ void sersic_finalize_kernel(double* header, int count, int stride, gsb_gsparams gsp,
-                                       const SersicScan* scan, double4* nodes, double4* dnodes,
-                                       double* dheader)
+// End of buildFT (SBSersic.cpp:510-537) and the natural spline, one warp per table: the warp
+// stages the table's nodes in shared memory (coalesced), lane 0 runs the serial parts there.
+// Dynamic shared memory: 4 * stride doubles.
+__global__ void __launch_bounds__(32) sersic_finalize_kernel(double* header, int count, int stride,
+                                                             gsb_gsparams gsp, const SersicScan* scan,
+                                                             double4* nodes, double4* dnodes, double* dheader)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    extern __shared__ double fsm[];
+    const int s = blockIdx.x;
+    const int lane = threadIdx.x;
     if (s >= count) return;
+    double* xs = fsm;
+    double* ys = xs + stride;
+    double* zs = ys + stride;
+    double* cs = zs + stride;
     double* H = header + (size_t)s * kSersicHeader;
     double4* nd = nodes + (size_t)s * stride;
     const SersicScan& S = scan[s];
     const int N = S.nused;
-    if (N < 2) { H[kSH_STATUS] = 5; H[kSH_NUSED] = 0; return; }
+    if (N < 2) {
+        if (lane == 0) { H[kSH_STATUS] = 5; H[kSH_NUSED] = 0; }
+        return;
+    }
     const double front = H[kSH_FRONT], dlogk = H[kSH_DLOGK];
     const int n_fit = 10;
-    double ksq_max = S.ksq_max, maxk = S.maxk, a = S.a, b = S.b;
-    if (ksq_max <= 0.) ksq_max = exp(2. * nd[N - 1].x);
-    if (S.found) {
-        maxk *= exp(dlogk);
-    } else {
-        const double den = n_fit * S.sk2 - S.sk * S.sk;
-        a = (S.sf * S.sk2 - S.sk * S.skf) / den;
-        b = (n_fit * S.skf - S.sk * S.sf) / den;
-        maxk = sqrt(a / gsp.maxk_threshold);
-        for (int it = 0; it < 3; ++it) maxk = sqrt((a - b / maxk) / gsp.maxk_threshold);
+    for (int i = lane; i < N; i += 32) {
+        const double4 v = nd[i];
+        xs[i] = v.x;
+        ys[i] = v.y;
     }
-    natural_spline(nd, N);
-    const double back = nd[N - 1].x;
-    for (int i = 0; i < N; ++i) { nd[i].x -= front; nd[i].w = 0.; }
+    __syncwarp();
+    double ksq_max = 0., maxk = 0., a = 0., b = 0.;
+    if (lane == 0) {
+        ksq_max = S.ksq_max;
+        maxk = S.maxk;
+        a = S.a;
+        b = S.b;
+        if (ksq_max <= 0.) ksq_max = exp(2. * xs[N - 1]);
+        if (S.found) {
+            maxk *= exp(dlogk);
+        } else {
+            const double den = n_fit * S.sk2 - S.sk * S.sk;
+            a = (S.sf * S.sk2 - S.sk * S.skf) / den;
+            b = (n_fit * S.skf - S.sk * S.sf) / den;
+            maxk = sqrt(a / gsp.maxk_threshold);
+            for (int it = 0; it < 3; ++it) maxk = sqrt((a - b / maxk) / gsp.maxk_threshold);
+        }
+        natural_spline(xs, ys, zs, cs, N);
+    }
+    __syncwarp();
+    for (int i = lane; i < N; i += 32) nd[i] = make_double4(xs[i] - front, ys[i], zs[i], 0.);
+    const double back = xs[N - 1];
     if (dnodes) {
         // The spline is linear in its node values, so d/dn of the interpolant is the spline of
         // the node derivatives on the same grid.  Likewise the high-k fit is linear in the f0
         // values of its window: the 10 nodes before the stopping node, or the last 10 nodes
         // when the scan ran to the end of the candidate grid.
         double4* dn = dnodes + (size_t)s * stride;
-        natural_spline(dn, N);
-        for (int i = 0; i < N; ++i) { dn[i].x -= front; dn[i].w = 0.; }
-        // The fit's 1/k_i move too: d(1/k_i)/dn = -c / k_i with c = dfront/dn.
-        double* D = dheader + (size_t)s * kSersicDHeader;
-        const double c = D[kSD_DFRONT];
-        const int wend = S.ksq_max > 0. ? N - 1 : N;
-        const int wbeg = wend - n_fit > 0 ? wend - n_fit : 0;
-        double sk = 0., sk2 = 0., sf = 0., skf = 0., dsf = 0., dskf = 0.;
-        for (int i = wbeg; i < wend; ++i) {
-            const double inv_k = exp(-(front + i * dlogk));
-            const double f0 = nd[i].y, df0 = dn[i].y;
-            sk += inv_k;
-            sk2 += inv_k * inv_k;
-            sf += f0;
-            skf += f0 * inv_k;
-            dsf += df0;
-            dskf += (df0 - c * f0) * inv_k;
+        __syncwarp();
+        for (int i = lane; i < N; i += 32) cs[i] = ys[i];     // keep f0 for the fit window
+        __syncwarp();
+        for (int i = lane; i < N; i += 32) ys[i] = dn[i].y;
+        __syncwarp();
+        double* f0s = zs;   // reuse: z of the main table is already written out
+        if (lane == 0) {
+            // The fit's 1/k_i move too: d(1/k_i)/dn = -c / k_i with c = dfront/dn.
+            double* D = dheader + (size_t)s * kSersicDHeader;
+            const double c = D[kSD_DFRONT];
+            const int wend = S.ksq_max > 0. ? N - 1 : N;
+            const int wbeg = wend - n_fit > 0 ? wend - n_fit : 0;
+            double sk = 0., sk2 = 0., sf = 0., skf = 0., dsf = 0., dskf = 0.;
+            for (int i = wbeg; i < wend; ++i) {
+                const double inv_k = exp(-(front + i * dlogk));
+                const double f0 = cs[i], df0 = ys[i];
+                sk += inv_k;
+                sk2 += inv_k * inv_k;
+                sf += f0;
+                skf += f0 * inv_k;
+                dsf += df0;
+                dskf += (df0 - c * f0) * inv_k;
+            }
+            const double dsk = -c * sk, dsk2 = -2. * c * sk2;
+            const double den = n_fit * sk2 - sk * sk, dden = n_fit * dsk2 - 2. * sk * dsk;
+            const double na = sf * sk2 - sk * skf, dna = dsf * sk2 + sf * dsk2 - dsk * skf - sk * dskf;
+            const double nb = n_fit * skf - sk * sf, dnb = n_fit * dskf - dsk * sf - sk * dsf;
+            D[kSD_DHIGHA] = (dna * den - na * dden) / (den * den);
+            D[kSD_DHIGHB] = (dnb * den - nb * dden) / (den * den);
+            natural_spline(xs, ys, f0s, cs, N);
         }
-        const double dsk = -c * sk, dsk2 = -2. * c * sk2;
-        const double den = n_fit * sk2 - sk * sk, dden = n_fit * dsk2 - 2. * sk * dsk;
-        const double na = sf * sk2 - sk * skf, dna = dsf * sk2 + sf * dsk2 - dsk * skf - sk * dskf;
-        const double nb = n_fit * skf - sk * sf, dnb = n_fit * dskf - dsk * sf - sk * dsf;
-        D[kSD_DHIGHA] = (dna * den - na * dden) / (den * den);
-        D[kSD_DHIGHB] = (dnb * den - nb * dden) / (den * den);
+        __syncwarp();
+        for (int i = lane; i < N; i += 32) dn[i] = make_double4(xs[i] - front, ys[i], f0s[i], 0.);
     }
+    if (lane != 0) return;
     H[kSH_NUSED] = N;
     H[kSH_DA] = (back - front) / (N - 1);
     H[kSH_KSQMAX] = ksq_max;
@@ -807,9 +840,14 @@ int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc,
                                                                  dval, dnode);
         GSB_CUDA_CHECK(cudaGetLastError());
     }
-    sersic_finalize_kernel<<<(count + 63) / 64, 64, 0, stream>>>(t->d_header, count, stride, *gsp,
-                                                                 static_cast<const SersicScan*>(t->d_scan), t->d_node,
-                                                                 dnode, dheader);
+    const size_t fsm = sizeof(double) * 4 * (size_t)stride;
+    if (fsm > 48 * 1024)
+        GSB_CUDA_CHECK(cudaFuncSetAttribute(sersic_finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            int(std::min<size_t>(fsm, 227 * 1024))));
+    if (fsm > 227 * 1024) return set_error(GSB_ERR_UNSUPPORTED, "Sersic table too long");
+    sersic_finalize_kernel<<<count, 32, fsm, stream>>>(t->d_header, count, stride, *gsp,
+                                                        static_cast<const SersicScan*>(t->d_scan), t->d_node,
+                                                        dnode, dheader);
     GSB_CUDA_CHECK(cudaGetLastError());
     int h_status = 0;
     GSB_CUDA_CHECK(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
