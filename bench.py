@@ -165,8 +165,9 @@ def mixed_object(galsim, m, gsp):
 
 
 def run_mixed(galsim, dev, steps, warmup):
-    """Mixed-size batch: stamps/s forward and forward+adjoint (record gradients for a random
-    cotangent), automatically sized stamps with minimum_fft_size=32 (FFT sizes 32..1024)."""
+    """Mixed-size batch: stamps/s forward and forward+adjoint (gradients of the bulge and disk
+    records -- flux, Jacobian, size, Sersic n -- for a random cotangent), automatically sized
+    stamps with minimum_fft_size=32 (FFT sizes 32..1024)."""
     import torch
     from galsim_b200 import _lib
     gsp = galsim.GSParams(minimum_fft_size=32)
@@ -182,7 +183,7 @@ def run_mixed(galsim, dev, steps, warmup):
 
     def fwd_adj():
         s = galsim.run_batch(plan)
-        return prog.adjoint_stamps(cot[:s.flat.numel()], _lib.F32)
+        return prog.adjoint_stamps(cot[:s.flat.numel()], _lib.F32, want=0b11)   # bulge, disk
 
     out = {}
     for name, fn in (('forward', fwd), ('forward_adjoint', fwd_adj)):

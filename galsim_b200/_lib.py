@@ -22,6 +22,7 @@ LEAF_JAC_GENERAL, LEAF_SIZE_IS_HLR = 1, 2
 PHASE_JAC_GENERAL = 1
 F32, F64 = 0, 1
 TABLES_DN = 1
+WANT_ALL = 0xffffffff
 GRAD_PER_LEAF, GRAD_PER_PHASE = 6, 7
 
 
@@ -79,7 +80,7 @@ def lib():
             'gsb_adjoint_grad_count': (i, [ctypes.POINTER(TemplateC)]),
             'gsb_adjoint_workspace_size': (sz, [i, i, i]),
             'gsb_adjoint_images': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp,
-                                       vp, vp, vp, i, vp, i, vp, i, vp, sz, vp]),
+                                       vp, vp, vp, i, vp, i, vp, ctypes.c_uint, i, vp, sz, vp]),
             'gsb_prepare_leaves': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp,
                                        vp, vp]),
             'gsb_draw_workspace_size': (sz, [i, i, i]),

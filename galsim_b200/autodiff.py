@@ -53,6 +53,9 @@ class RecordPlan(object):
         self.nx, self.ny = int(nx), int(ny)
         self.last = None
         self._rec_dev = {}
+        # records whose gradients the adjoint computes (leaf l: bit l, phase p: bit 8 + p,
+        # scale q: bit 16 + q); the others get zero gradients
+        self.want = _lib.WANT_ALL
 
     # -- records <-> tensors ----------------------------------------------------------------
     def records(self):
@@ -158,7 +161,7 @@ class RecordPlan(object):
         dt = _lib.F32 if self.dtype == np.float32 else _lib.F64
         tdt = torch.float32 if dt == _lib.F32 else torch.float64
         c = cot.to(dtype=tdt).contiguous().reshape(-1)
-        g = self.prog.adjoint_stamps(c, dt, self.precision)
+        g = self.prog.adjoint_stamps(c, dt, self.precision, self.want)
         gl = g[:, :_lib.GRAD_PER_LEAF * L].reshape(B, L, _lib.GRAD_PER_LEAF)
         gp = g[:, _lib.GRAD_PER_LEAF * L:_lib.GRAD_PER_LEAF * L + _lib.GRAD_PER_PHASE * P].reshape(
             B, P, _lib.GRAD_PER_PHASE)
@@ -263,6 +266,7 @@ class GalaxyModel(object):
                           tables=self.tables)
         if plan.types[0] != _lib.SERSIC or plan.P < 1:
             raise GalSimError("unexpected program layout for GalaxyModel")
+        plan.want = 1 | (1 << 8)          # the galaxy leaf and its shift
         self.plan = plan
         rec = plan.records()
         B = plan.B

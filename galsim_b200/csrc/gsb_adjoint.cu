@@ -21,10 +21,10 @@ size_t adjoint_workspace_size(int N, int n_stamps, int precision)
 int adjoint_images(const gsb_template* tpl, int n_stamps, const gsb_leaf* d_leaves,
                    const gsb_phase* d_phases, const double* d_scales, const gsb_stamp* d_stamps,
                    const gsb_tables* t, int N, const void* d_cot, int cot_dtype, double* d_grad,
-                   int precision, void* d_work, size_t work_bytes, cudaStream_t stream)
+                   unsigned want, int precision, void* d_work, size_t work_bytes, cudaStream_t stream)
 {
     bool sersic = false;
-    for (int l = 0; l < tpl->n_leaves; ++l) sersic |= tpl->leaf_type[l] == GSB_SERSIC;
+    for (int l = 0; l < tpl->n_leaves; ++l) sersic |= tpl->leaf_type[l] == GSB_SERSIC && ((want >> l) & 1u);
     if (sersic && (!t || !t->has_dn))
         return set_error(GSB_ERR_INVALID, "the adjoint of Sersic leaves needs tables built with n-derivatives");
     AdjArgs args;
@@ -42,6 +42,7 @@ int adjoint_images(const gsb_template* tpl, int n_stamps, const gsb_leaf* d_leav
     args.cot = d_cot;
     args.cot_dtype = cot_dtype;
     args.grad = d_grad;
+    args.want = want;
     args.work = d_work;
     if (n_stamps <= 0) return GSB_OK;
     bool handled = false;

@@ -45,8 +45,12 @@ struct AdjArgs {
     const void* cot;      // cotangent images, same layout as the forward output
     int cot_dtype;
     double* grad;         // n_stamps * grad_count(tpl)
+    unsigned want;        // records whose gradients are wanted (leaf l: bit l, phase p: 8 + p, scale q: 16 + q)
     void* work;           // per-CTA W slabs when W does not fit in shared memory
 };
+
+// Atoms of the factored adjoint held in registers.
+constexpr int kAdjAtoms = 3;
 
 struct AdjSmem {
     StampSmem S;
@@ -77,11 +81,11 @@ __device__ inline void program_children(const gsb_template& tpl, int* c1, int* c
     }
 }
 
-// Reverse-mode pass of the program at k index (i, j) with output cotangent u
-// (contribution Re(u * dF)); gradients are added into acc.
+// Reverse-mode pass of the ops [o0, o1) (a complete subtree, or the whole program) at k index
+// (i, j) with output cotangent u (contribution Re(u * dF)); gradients are added into acc.
 template <typename T>
-__device__ __noinline__ void adjoint_point(const gsb_template& tpl, const AdjSmem& A, double dk, int i,
-                                           int j, const GridRef& g, Cx<T> u, T* acc)
+__device__ __noinline__ void adjoint_range(const gsb_template& tpl, const AdjSmem& A, double dk, int i,
+                                           int j, const GridRef& g, Cx<T> u, T* acc, int o0, int o1)
 {
     const StampSmem& S = A.S;
     Cx<T> val[GSB_MAX_OPS];
@@ -89,8 +93,8 @@ __device__ __noinline__ void adjoint_point(const gsb_template& tpl, const AdjSme
     LeafD<T> ld[GSB_MAX_LEAVES];
     Cx<T> pe[GSB_MAX_PHASES];
     const T kx = T(i) * T(dk), ky = T(j) * T(dk);
-    const int n_ops = tpl.n_ops;
-    for (int o = 0; o < n_ops; ++o) {
+    const int n_ops = o1;
+    for (int o = o0; o < n_ops; ++o) {
         const int code = tpl.op_code[o], arg = tpl.op_arg[o];
         const int a = A.child1[o], b = A.child2[o];
         if (code == GSB_OP_LEAF) {
@@ -115,7 +119,7 @@ __device__ __noinline__ void adjoint_point(const gsb_template& tpl, const AdjSme
     adj[n_ops - 1] = u;
     const int pbase = kGradPerLeaf * tpl.n_leaves;
     const int sbase = pbase + kGradPerPhase * tpl.n_phases;
-    for (int o = n_ops - 1; o >= 0; --o) {
+    for (int o = n_ops - 1; o >= o0; --o) {
         const int code = tpl.op_code[o], arg = tpl.op_arg[o];
         const int a = A.child1[o], b = A.child2[o];
         const Cx<T> w = adj[o];
@@ -158,6 +162,94 @@ __device__ __noinline__ void adjoint_point(const gsb_template& tpl, const AdjSme
     }
 }
 
+// Factored reverse pass at (i, j): F = prod_a atom_a * XS[i] YS[j]; the cotangent of atom a
+// is u XS YS prod_{b != a} atom_b (prefix and suffix products, no division).  Leaf, phase and
+// scale atoms accumulate into ga[a][*] (registers); subtree atoms run adjoint_range into acc.
+template <typename T>
+__device__ __forceinline__ void adjoint_point_factored(const gsb_template& tpl, const AdjSmem& A,
+                                                       const unsigned char* cache, unsigned want, double dk,
+                                                       int i, int j, const GridRef& g, Cx<T> u,
+                                                       T (&ga)[kAdjAtoms][kGradPerPhase], T* acc)
+{
+    const StampSmem& S = A.S;
+    const int hk = g.n / 2;
+    const T kx = T(i) * T(dk), ky = T(j) * T(dk);
+    const int na = S.n_atoms;
+    Cx<T> val[kAdjAtoms], e[kAdjAtoms], pre[kAdjAtoms];
+    LeafD<T> ld[kAdjAtoms];
+    Cx<T> run = cx<T>(T(1), T(0));
+#pragma unroll
+    for (int a = 0; a < kAdjAtoms; ++a) {
+        val[a] = cx<T>(T(1), T(0));
+        e[a] = val[a];
+        ld[a] = LeafD<T>{T(0), T(0), T(0), T(0), T(0)};
+        if (a < na) {
+            const int kind = S.atom_kind[a];
+            const int o0 = S.atom_o0[a], o1 = S.atom_o1[a];
+            if (kind == kAtomPhase) {
+                const int p = S.atom_arg[a];
+                double tt = i * S.phase_ax[p] + j * S.phase_ay[p];
+                tt -= rint(tt);
+                T sn, cs;
+                sincospi(T(-2. * tt), &sn, &cs);
+                e[a] = cx<T>(cs, sn);
+                val[a] = cscale<T>(e[a], T(S.phase[p].flux_scaling));
+            } else if (kind == kAtomScale) {
+                val[a] = cx<T>(T(S.scale[S.atom_arg[a]]), T(0));
+            } else if (o1 - o0 == 1) {
+                const int l = tpl.op_arg[o0];
+                if (want_leaf(want, l)) {
+                    ld[a] = leaf_grad<T>(S.leaf[l], S.sersic, A.dn, kx, ky, g, i - g.x0, j - g.y0);
+                    val[a] = cx<T>(ld[a].v, T(0));
+                } else {
+                    val[a] = cx<T>(leaf_fast<T>(S, cache, l, kx, ky, i, j, g), T(0));
+                }
+            } else {
+                val[a] = eval_range<T>(tpl, S, cache, dk, i, j, g, o0, o1);
+            }
+        }
+        pre[a] = run;
+        run = cmul<T>(run, val[a]);
+    }
+    const Cx<T>* XS = reinterpret_cast<const Cx<T>*>(cache + S.xy_cache);
+    const Cx<T> us = cmul<T>(u, cmul<T>(XS[i], XS[hk + 1 + j + hk]));
+    Cx<T> suf = cx<T>(T(1), T(0));
+#pragma unroll
+    for (int a = kAdjAtoms - 1; a >= 0; --a) {
+        if (a < na) {
+            const Cx<T> w = cmul<T>(cmul<T>(us, pre[a]), suf);
+            const int kind = S.atom_kind[a];
+            const int o0 = S.atom_o0[a], o1 = S.atom_o1[a];
+            if (kind == kAtomPhase) {
+                const gsb_phase& P = S.phase[S.atom_arg[a]];
+                const Cx<T> we = cmul<T>(w, e[a]);
+                const T z = T(P.flux_scaling) * we.y;
+                const T cxp = T(P.cenx), cyp = T(P.ceny);
+                ga[a][0] += z * (T(P.jac[0]) * kx + T(P.jac[2]) * ky);
+                ga[a][1] += z * (T(P.jac[1]) * kx + T(P.jac[3]) * ky);
+                ga[a][2] += we.x;
+                ga[a][3] += z * kx * cxp;
+                ga[a][4] += z * kx * cyp;
+                ga[a][5] += z * ky * cxp;
+                ga[a][6] += z * ky * cyp;
+            } else if (kind == kAtomScale) {
+                ga[a][0] += w.x;
+            } else if (o1 - o0 == 1) {
+                const T ar = w.x;
+                ga[a][0] += ar * ld[a].unit;
+                ga[a][1] += ar * ld[a].gx * kx;
+                ga[a][2] += ar * ld[a].gy * kx;
+                ga[a][3] += ar * ld[a].gx * ky;
+                ga[a][4] += ar * ld[a].gy * ky;
+                ga[a][5] += ar * ld[a].gn;
+            } else {
+                adjoint_range<T>(tpl, A, dk, i, j, g, w, acc, o0, o1);
+            }
+            suf = cmul<T>(suf, val[a]);
+        }
+    }
+}
+
 template <typename T>
 __device__ inline T load_cot(const void* p, int dtype, long long idx)
 {
@@ -169,8 +261,8 @@ __device__ inline T load_cot(const void* p, int dtype, long long idx)
 template <typename T, int N>
 __host__ __device__ constexpr int adj_warps()
 {
-    return ((sizeof(AdjSmem) + 15) / 16 * 16 + sizeof(Cx<T>) * N * (1 + kWarps) + 4096 <= kSmemLimit)
-               ? kWarps : kWarps / 2;
+    return ((sizeof(AdjSmem) + 15) / 16 * 16 + sizeof(Cx<T>) * N * (1 + kWarps) + kCacheBytes + 4096 <=
+            kSmemLimit) ? kWarps : kWarps / 2;
 }
 
 template <typename T, int N, bool WSMEM>
@@ -189,6 +281,8 @@ __global__ void __launch_bounds__(adj_warps<T, N>() * 32) adjoint_fused_kernel(c
     off += sizeof(Cx<T>) * N * NW;
     Cx<T>* W = WSMEM ? reinterpret_cast<Cx<T>*>(smem_raw + off)
                      : reinterpret_cast<Cx<T>*>(a.work) + (size_t)blockIdx.x * H * WS;
+    if (WSMEM) off += sizeof(Cx<T>) * H * WS;
+    unsigned char* cache = smem_raw + ((off + 15) & ~size_t(15));
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Cx<T>* buf = scratch + warp * N;
@@ -220,6 +314,15 @@ __global__ void __launch_bounds__(adj_warps<T, N>() * 32) adjoint_fused_kernel(c
         const int Nk = G.Nk;
         const int hk = Nk / 2;
         const GridRef g{dk, 0, -hk, hk + 1, Nk + 1};
+        if (threadIdx.x == 0) plan_caches<T>(S, a.tpl, Nk, a.want);
+        __syncthreads();
+        fill_caches<T>(S, a.tpl, cache, dk, Nk);
+        __syncthreads();
+        const bool factored = S.xy_cache >= 0 && S.n_atoms <= kAdjAtoms;
+        bool subtree = !factored;
+        if (factored)
+            for (int t = 0; t < S.n_atoms; ++t)
+                subtree |= S.atom_kind[t] == kAtomRange && S.atom_o1[t] - S.atom_o0[t] > 1;
 
         // ---- row phase: forward-sign DFT of pairs of cotangent rows ----
         const int npairs = (G.ny + 1) / 2;
@@ -248,12 +351,18 @@ __global__ void __launch_bounds__(adj_warps<T, N>() * 32) adjoint_fused_kernel(c
 
         // ---- column phase: forward-sign DFT along y, then the reverse pass per alias ----
         T acc[kMaxGrad];
+        T ga[kAdjAtoms][kGradPerPhase];
         for (int c = warp; c < H; c += NW) {
             for (int y = lane; y < N; y += 32)
                 buf[y] = pmod(y - G.ymin, N) < G.ny ? W[(size_t)c * WS + y] : cx<T>(T(0), T(0));
             __syncwarp();
             warp_fft<T, N, +1>(buf, tw);
-            for (int k = 0; k < ng; ++k) acc[k] = T(0);
+            if (subtree)
+                for (int k = 0; k < ng; ++k) acc[k] = T(0);
+#pragma unroll
+            for (int t = 0; t < kAdjAtoms; ++t)
+#pragma unroll
+                for (int e = 0; e < kGradPerPhase; ++e) ga[t][e] = T(0);
             const T wc = (c == 0 || 2 * c == N) ? inv_n2 : T(2) * inv_n2;
             const int alo = ceil_div(-hk - c, N), ahi = floor_div(hk - c, N);
             for (int r = lane; r < N; r += 32) {
@@ -266,22 +375,50 @@ __global__ void __launch_bounds__(adj_warps<T, N>() * 32) adjoint_fused_kernel(c
                         const int ky = kyc + ib * N;
                         const bool pos = kx >= 0;
                         // an alias taken as conj(F(-k)) contributes Re(Ghat conj(dF)) = Re(conj(Ghat) dF)
-                        adjoint_point<T>(a.tpl, A, dk, pos ? kx : -kx, pos ? ky : -ky, g,
-                                         pos ? gh : cconj<T>(gh), acc);
+                        if (factored)
+                            adjoint_point_factored<T>(a.tpl, A, cache, a.want, dk, pos ? kx : -kx,
+                                                      pos ? ky : -ky, g, pos ? gh : cconj<T>(gh), ga, acc);
+                        else
+                            adjoint_range<T>(a.tpl, A, dk, pos ? kx : -kx, pos ? ky : -ky, g,
+                                             pos ? gh : cconj<T>(gh), acc, 0, a.tpl.n_ops);
                     }
                 }
             }
-            for (int k = 0; k < ng; ++k) {
-                double v = double(acc[k]);
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-                if (lane == 0) atomicAdd(&A.gacc[k], v);
+            if (subtree) {
+                for (int k = 0; k < ng; ++k) {
+                    double v = double(acc[k]);
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                    if (lane == 0) atomicAdd(&A.gacc[k], v);
+                }
+            }
+            if (factored) {
+                const int pbase = kGradPerLeaf * a.tpl.n_leaves;
+                const int sbase = pbase + kGradPerPhase * a.tpl.n_phases;
+#pragma unroll
+                for (int t = 0; t < kAdjAtoms; ++t) {
+                    if (t >= S.n_atoms) break;
+                    const int kind = S.atom_kind[t];
+                    int base, cnt;
+                    if (kind == kAtomPhase) { base = pbase + kGradPerPhase * S.atom_arg[t]; cnt = kGradPerPhase; }
+                    else if (kind == kAtomScale) { base = sbase + S.atom_arg[t]; cnt = 1; }
+                    else if (S.atom_o1[t] - S.atom_o0[t] == 1 && want_leaf(a.want, S.atom_arg[t])) {
+                        base = kGradPerLeaf * S.atom_arg[t]; cnt = kGradPerLeaf;
+                    } else continue;
+#pragma unroll
+                    for (int e = 0; e < kGradPerPhase; ++e) {
+                        if (e >= cnt) break;
+                        double v = double(ga[t][e]);
+                        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                        if (lane == 0) atomicAdd(&A.gacc[base + e], v);
+                    }
+                }
             }
             __syncwarp();
         }
         __syncthreads();
         // Sersic leaves given by half-light radius: r0 = hlr / r_e(n), so at fixed hlr
         // d/dn picks up -d ln r_e/dn * d/d ln r0, and d/d ln r0 = sum_ij J_ij d/dJ_ij.
-        if (threadIdx.x < a.tpl.n_leaves) {
+        if (threadIdx.x < a.tpl.n_leaves && want_leaf(a.want, threadIdx.x)) {
             const LeafParams& L = S.leaf[threadIdx.x];
             if (L.type == GSB_SERSIC && (L.flags & GSB_LEAF_SIZE_IS_HLR)) {
                 double* gl = A.gacc + kGradPerLeaf * threadIdx.x;
@@ -290,7 +427,15 @@ __global__ void __launch_bounds__(adj_warps<T, N>() * 32) adjoint_fused_kernel(c
             }
         }
         __syncthreads();
-        for (int k = threadIdx.x; k < ng; k += blockDim.x) a.grad[(size_t)s * ng + k] = A.gacc[k];
+        // entries of records outside the want mask are written as zero
+        const int pbase = kGradPerLeaf * a.tpl.n_leaves;
+        const int sbase = pbase + kGradPerPhase * a.tpl.n_phases;
+        for (int k = threadIdx.x; k < ng; k += blockDim.x) {
+            const bool w = k < pbase ? want_leaf(a.want, k / kGradPerLeaf)
+                         : k < sbase ? want_phase(a.want, (k - pbase) / kGradPerPhase)
+                                     : want_scale(a.want, k - sbase);
+            a.grad[(size_t)s * ng + k] = w ? A.gacc[k] : 0.;
+        }
     }
 }
 
@@ -300,7 +445,7 @@ constexpr size_t adj_smem_bytes(bool wsmem)
     size_t off = (sizeof(AdjSmem) + 15) & ~size_t(15);
     off += sizeof(Cx<T>) * N * (1 + adj_warps<T, N>());
     if (wsmem) off += sizeof(Cx<T>) * (N / 2 + 1) * (N + 1);
-    return off;
+    return ((off + 15) & ~size_t(15)) + kCacheBytes;
 }
 
 template <typename T, int N>

@@ -17,7 +17,7 @@ size_t adjoint_workspace_size(int N, int n_stamps, int precision);
 int adjoint_images(const gsb_template* tpl, int n_stamps, const gsb_leaf* d_leaves,
                    const gsb_phase* d_phases, const double* d_scales, const gsb_stamp* d_stamps,
                    const gsb_tables* t, int N, const void* d_cot, int cot_dtype, double* d_grad,
-                   int precision, void* d_work, size_t work_bytes, cudaStream_t stream);
+                   unsigned want, int precision, void* d_work, size_t work_bytes, cudaStream_t stream);
 int prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp, gsb_leaf* d_leaves,
                    const gsb_tables* t, double* d_info, cudaStream_t stream);
 size_t draw_workspace_size(int N, int n_stamps, int precision);
@@ -283,8 +283,8 @@ size_t gsb_adjoint_workspace_size(int N, int n_stamps, int precision)
 int gsb_adjoint_images(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp,
                        const gsb_leaf* d_leaves, const gsb_phase* d_phases, const double* d_scales,
                        const gsb_stamp* d_stamps, const gsb_tables* t, int N,
-                       const void* d_cotangent, int cot_dtype, double* d_grad, int precision,
-                       void* d_workspace, size_t workspace_bytes, void* stream)
+                       const void* d_cotangent, int cot_dtype, double* d_grad, unsigned int want_mask,
+                       int precision, void* d_workspace, size_t workspace_bytes, void* stream)
 {
     int rc = validate_template(tpl);
     if (rc) return rc;
@@ -298,7 +298,8 @@ int gsb_adjoint_images(const gsb_template* tpl, int n_stamps, const gsb_gsparams
     if (precision != GSB_F32 && precision != GSB_F64) return set_error(GSB_ERR_INVALID, "bad precision");
     if (!good_fft_size_ok(N)) return set_error(GSB_ERR_INVALID, "N is not 2^a or 3*2^a");
     return adjoint_images(tpl, n_stamps, d_leaves, d_phases, d_scales, d_stamps, t, N, d_cotangent,
-                          cot_dtype, d_grad, precision, d_workspace, workspace_bytes, (cudaStream_t)stream);
+                          cot_dtype, d_grad, want_mask, precision, d_workspace, workspace_bytes,
+                          (cudaStream_t)stream);
 }
 
 }  // extern "C"

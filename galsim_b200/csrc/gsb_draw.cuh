@@ -52,6 +52,8 @@ struct StampSmem {
     int n_atoms;
     short atom_o0[GSB_MAX_OPS];
     short atom_o1[GSB_MAX_OPS];
+    unsigned char atom_kind[GSB_MAX_OPS];      // kAtomRange, kAtomPhase (arg), kAtomScale (arg)
+    unsigned char atom_arg[GSB_MAX_OPS];
     unsigned char leaf_sep[GSB_MAX_LEAVES];    // leaf folded into XS / YS
     unsigned char phase_sep[GSB_MAX_PHASES];   // phase folded into XS / YS
     unsigned char scale_sep[GSB_MAX_SCALES];   // scale folded into XS / YS
@@ -175,12 +177,21 @@ template <> struct NodeT<double> { using type = double4; };
 
 // Decide which factors of this stamp are cached in shared memory (thread 0), in order:
 // Sersic spline nodes, phase factors, separable leaf factors, until kCacheBytes is used.
+enum { kAtomRange = 0, kAtomPhase = 1, kAtomScale = 2 };
+
+// want bits: leaf l = bit l, phase p = bit 8 + p, scale q = bit 16 + q.
+__device__ __forceinline__ bool want_leaf(unsigned want, int l) { return (want >> l) & 1u; }
+__device__ __forceinline__ bool want_phase(unsigned want, int p) { return (want >> (8 + p)) & 1u; }
+__device__ __forceinline__ bool want_scale(unsigned want, int q) { return (want >> (16 + q)) & 1u; }
+
 // Split the program's root product into atoms (thread 0).  MUL nodes are flattened; PHASE and
 // SCALE nodes contribute a separable factor and pass their child on; a LEAF is separable when
 // its value is X(i) Y(j) (Box or Gaussian with a diagonal Jacobian: the reference's 1-d fill);
-// every other LEAF and every ADD subtree is an atom evaluated per point.  Returns false when
-// the atoms do not fit the fixed arrays (the program is then evaluated unfactored).
-__device__ inline bool plan_factored(StampSmem& S, const gsb_template& tpl)
+// every other LEAF and every ADD subtree is an atom evaluated per point.  Factors named in
+// `want` (the adjoint's differentiated records) are not folded: a wanted separable leaf stays a
+// leaf atom, a wanted phase or scale becomes an atom of its own.  Returns false when the atoms
+// do not fit the fixed arrays (the program is then evaluated unfactored).
+__device__ inline bool plan_factored(StampSmem& S, const gsb_template& tpl, unsigned want = 0u)
 {
     short c1[GSB_MAX_OPS], c2[GSB_MAX_OPS], start[GSB_MAX_OPS];
     short st[GSB_MAX_OPS];
@@ -214,14 +225,22 @@ __device__ inline bool plan_factored(StampSmem& S, const gsb_template& tpl)
         if (code == GSB_OP_MUL) {
             st[sp++] = c1[o];
             st[sp++] = c2[o];
-        } else if (code == GSB_OP_PHASE) {
-            S.phase_sep[arg] = 1;
-            st[sp++] = c1[o];
-        } else if (code == GSB_OP_SCALE) {
-            S.scale_sep[arg] = 1;
+        } else if (code == GSB_OP_PHASE || code == GSB_OP_SCALE) {
+            const bool ph = code == GSB_OP_PHASE;
+            if (ph ? want_phase(want, arg) : want_scale(want, arg)) {
+                S.atom_o0[S.n_atoms] = o;
+                S.atom_o1[S.n_atoms] = o + 1;
+                S.atom_kind[S.n_atoms] = ph ? kAtomPhase : kAtomScale;
+                S.atom_arg[S.n_atoms] = (unsigned char)arg;
+                ++S.n_atoms;
+            } else if (ph) {
+                S.phase_sep[arg] = 1;
+            } else {
+                S.scale_sep[arg] = 1;
+            }
             st[sp++] = c1[o];
         } else {
-            if (code == GSB_OP_LEAF) {
+            if (code == GSB_OP_LEAF && !want_leaf(want, arg)) {
                 const LeafParams& L = S.leaf[arg];
                 if ((L.type == GSB_BOX || L.type == GSB_GAUSSIAN) && !(L.flags & GSB_LEAF_JAC_GENERAL)) {
                     S.leaf_sep[arg] = 1;
@@ -230,6 +249,8 @@ __device__ inline bool plan_factored(StampSmem& S, const gsb_template& tpl)
             }
             S.atom_o0[S.n_atoms] = start[o];
             S.atom_o1[S.n_atoms] = o + 1;
+            S.atom_kind[S.n_atoms] = kAtomRange;
+            S.atom_arg[S.n_atoms] = (unsigned char)(code == GSB_OP_LEAF ? arg : 0);
             ++S.n_atoms;
         }
     }
@@ -237,7 +258,7 @@ __device__ inline bool plan_factored(StampSmem& S, const gsb_template& tpl)
 }
 
 template <typename T>
-__device__ inline void plan_caches(StampSmem& S, const gsb_template& tpl, int Nk)
+__device__ inline void plan_caches(StampSmem& S, const gsb_template& tpl, int Nk, unsigned want = 0u)
 {
     const int hk = Nk / 2;
     int used = 0;
@@ -252,7 +273,7 @@ __device__ inline void plan_caches(StampSmem& S, const gsb_template& tpl, int Nk
     S.xy_cache = -1;
     {
         const int bytes = ((hk + 1 + Nk + 1) * (int)sizeof(Cx<T>) + 15) & ~15;
-        if (S.regstack && bytes <= kCacheBytes && plan_factored(S, tpl)) {
+        if (S.regstack && bytes <= kCacheBytes && plan_factored(S, tpl, want)) {
             S.xy_cache = used;
             used += bytes;
         } else {

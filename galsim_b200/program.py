@@ -263,10 +263,11 @@ class Program(object):
     def grad_count(self):
         return _lib.lib().gsb_adjoint_grad_count(ctypes.byref(self.tpl))
 
-    def adjoint_stamps(self, cot, cot_dtype, precision=_lib.F32):
+    def adjoint_stamps(self, cot, cot_dtype, precision=_lib.F32, want=_lib.WANT_ALL):
         """Reverse mode of the last draw_stamps call: cot is the flat device cotangent in the
         output's layout.  Returns the (B, grad_count) FP64 device tensor of record gradients
-        (see gsb_adjoint_grad_count for the entry order)."""
+        (see gsb_adjoint_grad_count for the entry order); records outside the `want` bit mask
+        (leaf l: bit l, phase p: bit 8 + p, scale q: bit 16 + q) get zeros."""
         import torch
         g = self._geom
         if g is None:
@@ -287,7 +288,8 @@ class Program(object):
                 ctypes.byref(self.tpl), n, ctypes.byref(self.gsp_c), lvp, php, scp, stp,
                 self.tables.handle if self.tables else None, NN,
                 _lib.ptr(cot), cot_dtype, ctypes.c_void_p(grad_sorted.data_ptr() + int(s0) * ng * 8),
-                precision, _lib.ptr(work), ctypes.c_size_t(int(wbytes)), stream))
+                ctypes.c_uint(int(want) & 0xffffffff), precision, _lib.ptr(work),
+                ctypes.c_size_t(int(wbytes)), stream))
         grad = torch.empty_like(grad_sorted)
         grad[g['perm']] = grad_sorted
         return grad

@@ -250,12 +250,16 @@ size_t gsb_adjoint_workspace_size(int N, int n_stamps, int precision);
  * profile's dkValue/dparameter, the phase and the products of the program) and are taken on
  * the stamp's fixed grid (N, Nk); clipped k-points contribute zero.  Sersic leaves need tables
  * built with GSB_TABLES_DN.  No reference counterpart (the reference has no derivatives); it
- * is the adjoint of gsobject.py:1927-2045 + src/Image.cpp:578-912 for fixed sizes. */
+ * is the adjoint of gsobject.py:1927-2045 + src/Image.cpp:578-912 for fixed sizes.
+ * want_mask names the records to differentiate (leaf l: bit l, phase p: bit 8 + p, scale q:
+ * bit 16 + q; GSB_WANT_ALL for every record); the entries of the others are written as 0 and
+ * their factors are folded into per-stamp 1-d tables, which makes the pass cheaper. */
+#define GSB_WANT_ALL 0xffffffffu
 int gsb_adjoint_images(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp,
                        const gsb_leaf* d_leaves, const gsb_phase* d_phases, const double* d_scales,
                        const gsb_stamp* d_stamps, const gsb_tables* t, int N,
-                       const void* d_cotangent, int cot_dtype, double* d_grad, int precision,
-                       void* d_workspace, size_t workspace_bytes, void* stream);
+                       const void* d_cotangent, int cot_dtype, double* d_grad, unsigned int want_mask,
+                       int precision, void* d_workspace, size_t workspace_bytes, void* stream);
 
 #ifdef __cplusplus
 }
