@@ -463,24 +463,21 @@ def run_stage(args):
 def run_gpu(args):
     import torch
     import torch.distributed as dist
-    world = int(os.environ.get('WORLD_SIZE', '1'))
-    rank = int(os.environ.get('RANK', '0'))
-    local = int(os.environ.get('LOCAL_RANK', '0'))
-    if world > 1:
-        import datetime
-        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    from galsim_b200 import replicas
+    rank, world, local = replicas.rank_info()
     import galsim_b200 as galsim
     from galsim_b200 import _lib
     galsim.set_device(local)
     dev = _lib.Device.torch_device()
-    params = workload_params(args.stamps)
+    replicas.init('nccl')
+    # weak scaling: every rank draws its own batch of the configuration (seed 1234 + rank)
+    params = workload_params(args.stamps, seed=1234 + rank)
     obj = gpu_object(galsim, params)
     plan = galsim.plan_batch(obj, scale=SCALE, dtype=np.float32)
 
     def barrier():
         torch.cuda.synchronize(dev)
-        if world > 1:
-            dist.barrier()
+        replicas.barrier()
 
     # Clocks are sampled (every 100 ms) from before the warm-up until after the e2e region; the
     # timed loop starts only once the sampler is producing.
@@ -499,11 +496,7 @@ def run_gpu(args):
         st = galsim.run_batch(plan)
     stop.record()
     barrier()
-    ms = start.elapsed_time(stop) / args.steps
-    t_step = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t_step, op=dist.ReduceOp.MAX)
-    ms = float(t_step.item())
+    ms = replicas.max_over_ranks(start.elapsed_time(stop) / args.steps)
     B = plan.prog.B
     value = world * B / (ms * 1e-3)
 
@@ -538,12 +531,8 @@ def run_gpu(args):
         flux = sb.added_flux
     ee.record()
     barrier()
-    e2e_ms = es.elapsed_time(ee) / args.steps
+    e2e_ms = replicas.max_over_ranks(es.elapsed_time(ee) / args.steps)
     clk.__exit__(None, None, None)
-    t_e = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
-    e2e_ms = float(t_e.item())
     L = prog.L
     h2d = B * (L * 136 + len(prog.bld.phases) * 64 + len(prog.bld.scales) * 8 + 32)
     d2h = int(pix.numel() * 4 + B * 8 + B * L * 16)
