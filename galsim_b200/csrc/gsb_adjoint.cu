@@ -3,10 +3,37 @@
 
 namespace gsb {
 
-int adjoint_launch_f32(int N, const AdjArgs& args, size_t work_bytes, cudaStream_t stream, bool* handled);
-bool adjoint_workspace_f32(int N, int n_stamps, size_t* bytes);
-int adjoint_launch_f64(int N, const AdjArgs& args, size_t work_bytes, cudaStream_t stream, bool* handled);
-bool adjoint_workspace_f64(int N, int n_stamps, size_t* bytes);
+#define GSB_ADJ_GROUP(name)                                                                       \
+    int adjoint_launch_##name(int N, const AdjArgs& args, size_t work_bytes, cudaStream_t stream,  \
+                              bool* handled);                                                      \
+    bool adjoint_workspace_##name(int N, int n_stamps, size_t* bytes);
+GSB_ADJ_GROUP(f32_small)
+GSB_ADJ_GROUP(f32_large)
+GSB_ADJ_GROUP(f64_small)
+GSB_ADJ_GROUP(f64_large)
+#undef GSB_ADJ_GROUP
+
+static int adjoint_launch_f32(int N, const AdjArgs& args, size_t work_bytes, cudaStream_t stream, bool* handled)
+{
+    const int rc = adjoint_launch_f32_small(N, args, work_bytes, stream, handled);
+    return *handled ? rc : adjoint_launch_f32_large(N, args, work_bytes, stream, handled);
+}
+
+static int adjoint_launch_f64(int N, const AdjArgs& args, size_t work_bytes, cudaStream_t stream, bool* handled)
+{
+    const int rc = adjoint_launch_f64_small(N, args, work_bytes, stream, handled);
+    return *handled ? rc : adjoint_launch_f64_large(N, args, work_bytes, stream, handled);
+}
+
+static bool adjoint_workspace_f32(int N, int n_stamps, size_t* bytes)
+{
+    return adjoint_workspace_f32_small(N, n_stamps, bytes) || adjoint_workspace_f32_large(N, n_stamps, bytes);
+}
+
+static bool adjoint_workspace_f64(int N, int n_stamps, size_t* bytes)
+{
+    return adjoint_workspace_f64_small(N, n_stamps, bytes) || adjoint_workspace_f64_large(N, n_stamps, bytes);
+}
 
 int adjoint_grad_count(const gsb_template* tpl) { return grad_count(*tpl); }
 

@@ -176,7 +176,7 @@ template <> struct NodeT<float> { using type = float4; };
 template <> struct NodeT<double> { using type = double4; };
 
 // Decide which factors of this stamp are cached in shared memory (thread 0), in order:
-// Sersic spline nodes, phase factors, separable leaf factors, until kCacheBytes is used.
+// Sersic spline nodes, phase factors, separable leaf factors, until the budget is used.
 enum { kAtomRange = 0, kAtomPhase = 1, kAtomScale = 2 };
 
 // want bits: leaf l = bit l, phase p = bit 8 + p, scale q = bit 16 + q.
@@ -258,7 +258,8 @@ __device__ inline bool plan_factored(StampSmem& S, const gsb_template& tpl, unsi
 }
 
 template <typename T>
-__device__ inline void plan_caches(StampSmem& S, const gsb_template& tpl, int Nk, unsigned want = 0u)
+__device__ inline void plan_caches(StampSmem& S, const gsb_template& tpl, int Nk, unsigned want = 0u,
+                                   int budget = kCacheBytes)
 {
     const int hk = Nk / 2;
     int used = 0;
@@ -273,7 +274,7 @@ __device__ inline void plan_caches(StampSmem& S, const gsb_template& tpl, int Nk
     S.xy_cache = -1;
     {
         const int bytes = ((hk + 1 + Nk + 1) * (int)sizeof(Cx<T>) + 15) & ~15;
-        if (S.regstack && bytes <= kCacheBytes && plan_factored(S, tpl, want)) {
+        if (S.regstack && bytes <= budget && plan_factored(S, tpl, want)) {
             S.xy_cache = used;
             used += bytes;
         } else {
@@ -287,21 +288,21 @@ __device__ inline void plan_caches(StampSmem& S, const gsb_template& tpl, int Nk
         S.leaf_cache[l] = -1;
         if (S.leaf[l].type == GSB_SERSIC) {
             const int bytes = (S.sersic[l].n * (int)sizeof(typename NodeT<T>::type) + 15) & ~15;
-            if (used + bytes <= kCacheBytes) { S.sersic_cache[l] = used; used += bytes; }
+            if (used + bytes <= budget) { S.sersic_cache[l] = used; used += bytes; }
         }
     }
     for (int p = 0; p < tpl.n_phases; ++p) {
         S.phase_cache[p] = -1;
         if (S.phase_sep[p]) continue;
         const int bytes = ((hk + 1 + Nk + 1) * (int)sizeof(Cx<T>) + 15) & ~15;
-        if (used + bytes <= kCacheBytes) { S.phase_cache[p] = used; used += bytes; }
+        if (used + bytes <= budget) { S.phase_cache[p] = used; used += bytes; }
     }
     for (int l = 0; l < tpl.n_leaves; ++l) {
         const LeafParams& L = S.leaf[l];
         const bool sep = !(L.flags & GSB_LEAF_JAC_GENERAL) && (L.type == GSB_BOX || L.type == GSB_GAUSSIAN);
         if (!sep || S.leaf_sep[l]) continue;
         const int bytes = ((hk + 1 + Nk + 1) * (int)sizeof(T) + 15) & ~15;
-        if (used + bytes <= kCacheBytes) { S.leaf_cache[l] = used; used += bytes; }
+        if (used + bytes <= budget) { S.leaf_cache[l] = used; used += bytes; }
     }
 }
 

@@ -67,16 +67,18 @@ struct LargeArgs {
     int N;
     const double2* tw;
     void* W;             // n_stamps slabs of (N/2+1) x N complex
+    int cache_bytes;     // shared memory for the per-stamp caches (factored program)
 };
 
-template <typename T>
-__global__ void __launch_bounds__(kLargeThreads) large_col_kernel(const __grid_constant__ LargeArgs la)
+template <typename T, int THREADS>
+__global__ void __launch_bounds__(THREADS) large_col_kernel(const __grid_constant__ LargeArgs la)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     StampSmem& S = *reinterpret_cast<StampSmem*>(smem_raw);
     Cx<T>* buf = reinterpret_cast<Cx<T>*>(smem_raw + ((sizeof(StampSmem) + 15) & ~size_t(15)));
     const DrawArgs& a = la.a;
     const int N = la.N, H = N / 2 + 1;
+    unsigned char* cache = reinterpret_cast<unsigned char*>(buf + N);
     const int s = blockIdx.y;
     const double dk = 2. * kPi / N;
     load_stamp(S, a.tpl, s, a.leaves, a.phases, a.scales, a.stamps, a.sersic_header, a.sersic_node,
@@ -84,6 +86,11 @@ __global__ void __launch_bounds__(kLargeThreads) large_col_kernel(const __grid_c
     __syncthreads();
     const int Nk = S.geom.Nk, hk = Nk / 2;
     const GridRef g{dk, 0, -hk, hk + 1, Nk + 1};
+    if (threadIdx.x == 0) plan_caches<T>(S, a.tpl, Nk, 0u, la.cache_bytes);
+    __syncthreads();
+    fill_caches<T>(S, a.tpl, cache, dk, Nk);
+    __syncthreads();
+    const bool factored = S.xy_cache >= 0, fast = S.regstack;
     Cx<T>* W = reinterpret_cast<Cx<T>*>(la.W) + (size_t)s * H * N;
     for (int c = blockIdx.x; c < H; c += gridDim.x) {
         const int alo = ceil_div(-hk - c, N), ahi = floor_div(hk - c, N);
@@ -95,8 +102,12 @@ __global__ void __launch_bounds__(kLargeThreads) large_col_kernel(const __grid_c
                 const int kx = c + ia * N;
                 for (int ib = blo; ib <= bhi; ++ib) {
                     const int ky = kyc + ib * N;
-                    if (kx >= 0) acc = cadd<T>(acc, eval_program<T>(a.tpl, S, dk, kx, ky, g));
-                    else acc = cadd<T>(acc, cconj<T>(eval_program<T>(a.tpl, S, dk, -kx, -ky, g)));
+                    const bool pos = kx >= 0;
+                    const int ii = pos ? kx : -kx, jj = pos ? ky : -ky;
+                    const Cx<T> v = factored ? eval_factored<T>(a.tpl, S, cache, dk, ii, jj, g)
+                                    : fast ? eval_fast<T>(a.tpl, S, cache, dk, ii, jj, g)
+                                           : eval_program<T>(a.tpl, S, dk, ii, jj, g);
+                    acc = cadd<T>(acc, pos ? v : cconj<T>(v));
                 }
             }
             buf[r] = acc;
@@ -108,8 +119,8 @@ __global__ void __launch_bounds__(kLargeThreads) large_col_kernel(const __grid_c
     }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kLargeThreads) large_row_kernel(const __grid_constant__ LargeArgs la)
+template <typename T, int THREADS>
+__global__ void __launch_bounds__(THREADS) large_row_kernel(const __grid_constant__ LargeArgs la)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     StampSmem& S = *reinterpret_cast<StampSmem*>(smem_raw);
@@ -212,18 +223,22 @@ size_t slab_bytes(int N) { return sizeof(Cx<T>) * (size_t)(N / 2 + 1) * N; }
 template <typename T>
 size_t large_smem() { return ((sizeof(StampSmem) + 15) & ~size_t(15)); }
 
-template <typename T>
-int launch_large(const DrawArgs& args, int N, void* work, size_t work_bytes, cudaStream_t stream)
+template <typename T, int THREADS>
+int launch_large_t(const DrawArgs& args, int N, void* work, size_t work_bytes, cudaStream_t stream)
 {
     const size_t slab = slab_bytes<T>(N);
     if (!work || work_bytes < slab) return set_error(GSB_ERR_INVALID, "draw workspace too small");
-    const size_t sm = large_smem<T>() + sizeof(Cx<T>) * N;
-    if (sm > kSmemLimit) return set_error(GSB_ERR_UNSUPPORTED, "FFT size too large for this precision");
+    const size_t base = large_smem<T>() + sizeof(Cx<T>) * N;
+    if (base > kSmemLimit) return set_error(GSB_ERR_UNSUPPORTED, "FFT size too large for this precision");
+    // the rest of shared memory (up to 192 KB) holds the per-stamp caches of the column kernel
+    const size_t room = kSmemLimit - base > 1024 ? kSmemLimit - base - 1024 : 0;
+    const int cache_bytes = int(std::min<size_t>(room, 192 * 1024) & ~size_t(15));
+    const size_t sm = base + cache_bytes;
     const double2* tw = nullptr;
     int rc = twiddles(N, stream, &tw);
     if (rc) return rc;
-    GSB_CUDA_CHECK(cudaFuncSetAttribute(large_col_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-    GSB_CUDA_CHECK(cudaFuncSetAttribute(large_row_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    GSB_CUDA_CHECK(cudaFuncSetAttribute(large_col_kernel<T, THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    GSB_CUDA_CHECK(cudaFuncSetAttribute(large_row_kernel<T, THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(base)));
     const int chunk = int(std::max<size_t>(1, std::min<size_t>(work_bytes / slab, 65535)));
     DeviceState* st = device_state();
     if (args.added_flux)
@@ -241,15 +256,25 @@ int launch_large(const DrawArgs& args, int N, void* work, size_t work_bytes, cud
         la.N = N;
         la.tw = tw;
         la.W = work;
+        la.cache_bytes = cache_bytes;
         const int cols = N / 2 + 1;
         const int gx = std::max(1, std::min(cols, (2 * st->sm_count + n - 1) / n));
-        large_col_kernel<T><<<dim3(gx, n), kLargeThreads, sm, stream>>>(la);
+        large_col_kernel<T, THREADS><<<dim3(gx, n), THREADS, sm, stream>>>(la);
         GSB_CUDA_CHECK(cudaGetLastError());
         const int gr = std::max(1, std::min(N / 2, (2 * st->sm_count + n - 1) / n));
-        large_row_kernel<T><<<dim3(gr, n), kLargeThreads, sm, stream>>>(la);
+        large_row_kernel<T, THREADS><<<dim3(gr, n), THREADS, base, stream>>>(la);
         GSB_CUDA_CHECK(cudaGetLastError());
     }
     return GSB_OK;
+}
+
+// Threads per CTA: one per row, 256 to 1024.
+template <typename T>
+int launch_large(const DrawArgs& args, int N, void* work, size_t work_bytes, cudaStream_t stream)
+{
+    if (N <= 256) return launch_large_t<T, 256>(args, N, work, work_bytes, stream);
+    if (N <= 512) return launch_large_t<T, 512>(args, N, work, work_bytes, stream);
+    return launch_large_t<T, kLargeThreads>(args, N, work, work_bytes, stream);
 }
 
 }  // namespace
