@@ -570,6 +570,10 @@ def run_gpu(args):
             'config': {'workload': 'sersic_kolmogorov_pixel_4096_seed1234', 'stamps_per_gpu': B,
                        'scale': SCALE, 'gsparams': 'default', 'fft_sizes': sorted(set(int(v) for v in N)),
                        'parallelism': 'replicas x%d' % world,
+                       'draw_stage': ('one CUDA graph replay per step (FFT-size buckets on forked streams)'
+                                      if getattr(prog, '_graph_state', None) and prog._graph_state.get('graph')
+                                      else 'eager launches'),
+                       'autotuned_variants': _lib.tune_report().splitlines(),
                        'l2': 'no flush; per-step table build and stamp outputs exceed L2 reuse'},
             'e2e': {'value': world * B / (e2e_ms * 1e-3), 'unit': 'stamps/s',
                     'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': d2h},

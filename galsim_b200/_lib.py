@@ -88,6 +88,8 @@ def lib():
                                     vp, vp, vp, i, i, vp, i, vp, sz, vp]),
             'gsb_draw_bucket': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp, vp,
                                     vp, vp, i, vp, i, i, vp, i, vp, sz, vp]),
+            'gsb_draw_set_variant': (i, [i]),
+            'gsb_draw_tune_report': (i, [ctypes.c_char_p, sz]),
             'gsb_draw_kimages': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp,
                                      vp, vp, d, i, i, i, i, vp, i, vp]),
         }
@@ -154,6 +156,19 @@ class Device(object):
         while len(lst) < n:
             lst.append(torch.cuda.Stream(device=dev))
         return lst[:n]
+
+
+def set_draw_variant(variant):
+    """0 automatic (autotuned), 1 fused kernel only, 2 split kernels where N >= 192."""
+    check(lib().gsb_draw_set_variant(int(variant)))
+
+
+def tune_report():
+    """The autotuner's choices, one line per (device, precision, N, stamp-count class)."""
+    n = lib().gsb_draw_tune_report(None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    lib().gsb_draw_tune_report(buf, n + 1)
+    return buf.value.decode()
 
 
 def set_device(index):

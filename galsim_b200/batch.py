@@ -133,9 +133,11 @@ def plan_batch(obj, nx=None, ny=None, scale=None, dtype=np.float32, method='fft'
     return BatchPlan(prog, nx, ny, nx is not None, flux_scale, dtype, scale, precision)
 
 
-def run_batch(plan, recompute=True):
+def run_batch(plan, recompute=True, graph=True):
     """Device part of draw_batch: FP64 tables and leaf sizing, GalSim sizing on the host, and
-    the fused draw kernels.  recompute=False reuses the leaf sizing of an earlier run."""
+    the fused draw kernels.  recompute=False reuses the leaf sizing of an earlier run.
+    graph=True: when the plan is run again with the same stamp geometry, its draw stage is
+    captured as one CUDA graph (on the second run) and replayed (see Program.draw_stamps)."""
     from .program import fft_sizes, good_image_size
     prog = plan.prog
     B = prog.B
@@ -154,7 +156,7 @@ def run_batch(plan, recompute=True):
     N, Nk = fft_sizes(stepk, maxk, xmin, xmin + nxs - 1, ymin, ymin + nys - 1, prog.gsparams)
     dt = _lib.F32 if np.dtype(plan.dtype) == np.float32 else _lib.F64
     prec = _lib.F64 if plan.precision == 'fp64' else _lib.F32
-    flat, offsets, flux = prog.draw_stamps(N, Nk, xmin, ymin, nxs, nys, dt, precision=prec)
+    flat, offsets, flux = prog.draw_stamps(N, Nk, xmin, ymin, nxs, nys, dt, precision=prec, graph=graph)
     bounds = [(1, int(x), 1, int(y)) for x, y in zip(nxs, nys)]
     return StampBatch(flat, offsets, nxs, nys, xmin, ymin, N, Nk, flux, plan.dtype, plan.scale,
                       bounds, plan.flux_scale)

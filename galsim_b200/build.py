@@ -43,9 +43,16 @@ def build(force=False, verbose=False):
     build_dir = os.path.join(HERE, '_build')
     os.makedirs(build_dir, exist_ok=True)
     procs = []
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith('.cuh')] + \
+        [os.path.join(ROOT, 'include', 'gsb.h'), os.path.abspath(__file__)]
+    newest_header = max(os.path.getmtime(h) for h in headers)
     for src in SOURCES:
         obj = os.path.join(build_dir, src.replace('.cu', '.o'))
         objs.append(obj)
+        # an object is rebuilt when it is older than its source or than any header
+        if (not force and os.path.exists(obj) and
+                os.path.getmtime(obj) >= max(os.path.getmtime(os.path.join(CSRC, src)), newest_header)):
+            continue
         cmd = [nvcc(), *ARCH, '-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC',
                '-I', os.path.join(ROOT, 'include'), '-I', CSRC, '-c', os.path.join(CSRC, src), '-o', obj]
         if verbose:

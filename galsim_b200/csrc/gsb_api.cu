@@ -21,6 +21,8 @@ int adjoint_images(const gsb_template* tpl, int n_stamps, const gsb_leaf* d_leav
 int prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp, gsb_leaf* d_leaves,
                    const gsb_tables* t, double* d_info, cudaStream_t stream);
 size_t draw_workspace_size(int N, int n_stamps, int precision);
+int draw_set_variant(int v);
+int draw_tune_report(char* buf, size_t len);
 int draw_images(const gsb_template* tpl, int n_stamps, const gsb_leaf* d_leaves,
                 const gsb_phase* d_phases, const double* d_scales, const gsb_stamp* d_stamps,
                 const gsb_tables* t, int N, void* d_out, int out_dtype, int add,
@@ -266,6 +268,10 @@ int gsb_draw_kimages(const gsb_template* tpl, int n_stamps, const gsb_gsparams* 
     return draw_kimages(tpl, n_stamps, d_leaves, d_phases, d_scales, t, dk, kxmin, kymin, nkx, nky,
                         d_out, out_dtype, (cudaStream_t)stream);
 }
+
+int gsb_draw_set_variant(int variant) { return draw_set_variant(variant); }
+
+int gsb_draw_tune_report(char* buf, size_t len) { return draw_tune_report(buf, len); }
 
 int gsb_adjoint_grad_count(const gsb_template* tpl)
 {

@@ -180,6 +180,7 @@ class Program(object):
         self.d_leaves = None
         self._prepared = False
         self._geom = None
+        self._graph_state = None
 
     def _stamp_geometry(self, N, Nk, xmin, ymin, nx, ny):
         """Device stamp records sorted by FFT size, with the bucket boundaries; kept for the
@@ -222,42 +223,89 @@ class Program(object):
                 ctypes.c_void_p(g['sc'].data_ptr() + int(s0) * S * 8) if S else None,
                 ctypes.c_void_p(g['st'].data_ptr() + int(s0) * _lib.STAMP_DTYPE.itemsize))
 
-    def draw_stamps(self, N, Nk, xmin, ymin, nx, ny, dtype, add_to=None, precision=_lib.F32):
-        """Run the fused kernels for every stamp.  Arrays are per stamp.  Returns the device
-        output buffer (flat), per-stamp offsets and the device added-flux array."""
+    def _launch_buckets(self, g, out, flux, flux_sorted, works, dtype, add, precision):
+        """Draw every FFT-size bucket of geometry g (one stream per bucket, largest N first: the
+        few long-running stamps of the big-N buckets take their SMs first and overlap the large
+        small-N buckets).  The workspaces are allocated by the caller on the current stream
+        before the fork and outlive the join, so the caching allocator cannot hand them out
+        while a bucket runs."""
         import torch
-        self.prepare()
-        B = self.B
-        dev = _lib.Device.torch_device()
-        g = self._stamp_geometry(N, Nk, xmin, ymin, nx, ny)
-        tdt = torch.float32 if dtype == _lib.F32 else torch.float64
-        out = add_to if add_to is not None else torch.empty(max(g['total'], 1), dtype=tdt, device=dev)
-        flux = torch.empty(B, dtype=torch.float64, device=dev)
-        flux_sorted = torch.empty(B, dtype=torch.float64, device=dev)
         lib = _lib.lib()
-        # One stream per FFT-size bucket, largest N first: the few long-running stamps of the
-        # big-N buckets take their SMs first and overlap the large small-N buckets.  The
-        # workspaces are allocated on the current stream before the fork and released after
-        # the join, so the caching allocator cannot hand them out while a bucket runs.
+        dev = _lib.Device.torch_device()
         main = torch.cuda.current_stream(dev)
-        buckets = sorted(zip(g['starts'], g['ends']), key=lambda se: -int(g['Ns'][se[0]]))
-        works = []
-        for s0, s1 in buckets:
-            wbytes = int(lib.gsb_draw_workspace_size(int(g['Ns'][s0]), int(s1 - s0), precision))
-            works.append((wbytes, torch.empty(max(wbytes, 8), dtype=torch.uint8, device=dev) if wbytes else None))
-        streams = _lib.Device.side_streams(len(buckets))
-        for (s0, s1), (wbytes, work), st in zip(buckets, works, streams):
+        streams = _lib.Device.side_streams(len(g['buckets']))
+        for (s0, s1), (wbytes, work), st in zip(g['buckets'], works, streams):
             st.wait_stream(main)
             lvp, php, scp, stp = self._bucket_ptrs(g, s0)
             _lib.check(lib.gsb_draw_bucket(
                 ctypes.byref(self.tpl), int(s1 - s0), ctypes.byref(self.gsp_c), lvp, php, scp, stp,
                 self.tables.handle if self.tables else None, int(g['Ns'][s0]),
-                _lib.ptr(out), dtype, 1 if add_to is not None else 0,
+                _lib.ptr(out), dtype, add,
                 ctypes.c_void_p(flux_sorted.data_ptr() + int(s0) * 8),
                 precision, _lib.ptr(work), ctypes.c_size_t(wbytes), ctypes.c_void_p(st.cuda_stream)))
         for st in streams:
             main.wait_stream(st)
-        flux[g['perm']] = flux_sorted
+        flux.index_copy_(0, g['perm'], flux_sorted)
+
+    def _workspaces(self, g, precision):
+        import torch
+        lib = _lib.lib()
+        dev = _lib.Device.torch_device()
+        works = []
+        for s0, s1 in g['buckets']:
+            wbytes = int(lib.gsb_draw_workspace_size(int(g['Ns'][s0]), int(s1 - s0), precision))
+            works.append((wbytes, torch.empty(max(wbytes, 8), dtype=torch.uint8, device=dev) if wbytes else None))
+        return works
+
+    def draw_stamps(self, N, Nk, xmin, ymin, nx, ny, dtype, add_to=None, precision=_lib.F32,
+                    graph=False):
+        """Run the fused kernels for every stamp.  Arrays are per stamp.  Returns the device
+        output buffer (flat), per-stamp offsets and the device added-flux array.
+
+        graph=True: the draw stage of a repeated geometry (same N, Nk, bounds, dtype and
+        precision as the previous call) is captured once as a CUDA graph, on the second such
+        call, and replayed from then on, with the current leaf / phase / scale records copied
+        into its input buffers first.  The returned buffers are copies."""
+        import torch
+        self.prepare()
+        B = self.B
+        dev = _lib.Device.torch_device()
+        tdt = torch.float32 if dtype == _lib.F32 else torch.float64
+        key = None
+        if graph and add_to is None:
+            # the captured launches hold the table pointers: the same Sersic indices keep them
+            key = tuple(np.asarray(v, np.int64).tobytes() for v in (N, Nk, xmin, ymin, nx, ny)) + \
+                (dtype, precision, b'' if self.sersic_n is None else self.sersic_n.tobytes())
+            gs = getattr(self, '_graph_state', None)
+            if gs is not None and gs['key'] == key:
+                g = gs['geom']
+                # refresh the inputs in place (the records may have changed since)
+                torch.index_select(self.d_leaves.view(B, self.L * _lib.LEAF_DTYPE.itemsize), 0, g['perm'],
+                                   out=g['lv'])
+                if g['ph'] is not None:
+                    g['ph'].copy_(_lib.to_device(np.stack(self.bld.phases, axis=1)[g['order']]))
+                if g['sc'] is not None:
+                    g['sc'].copy_(_lib.to_device(np.stack(self.bld.scales, axis=1)[g['order']]))
+                if gs['graph'] is None:
+                    cg = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(cg, capture_error_mode='thread_local'):
+                        self._launch_buckets(g, gs['out'], gs['flux'], gs['flux_sorted'], gs['works'],
+                                             dtype, 0, precision)
+                    gs['graph'] = cg
+                gs['graph'].replay()
+                self._geom = g
+                return gs['out'].clone(), g['offsets'], gs['flux'].clone()
+        g = self._stamp_geometry(N, Nk, xmin, ymin, nx, ny)
+        g['buckets'] = sorted(zip(g['starts'], g['ends']), key=lambda se: -int(g['Ns'][se[0]]))
+        out = add_to if add_to is not None else torch.empty(max(g['total'], 1), dtype=tdt, device=dev)
+        flux = torch.empty(B, dtype=torch.float64, device=dev)
+        flux_sorted = torch.empty(B, dtype=torch.float64, device=dev)
+        works = self._workspaces(g, precision)
+        self._launch_buckets(g, out, flux, flux_sorted, works, dtype, 1 if add_to is not None else 0, precision)
+        if key is not None:
+            self._graph_state = dict(key=key, geom=g, out=out, flux=flux, flux_sorted=flux_sorted,
+                                     works=works, graph=None)
+            return out.clone(), g['offsets'], flux.clone()
         return out, g['offsets'], flux
 
     def grad_count(self):

@@ -205,6 +205,18 @@ int gsb_draw_bucket(const gsb_template* tpl, int n_stamps, const gsb_gsparams* g
                     void* d_out, int out_dtype, int add_to_image, double* d_added_flux,
                     int precision, void* d_workspace, size_t workspace_bytes, void* stream);
 
+/* Kernel variant for buckets of FFT size N <= 1024: 0 = automatic (default), 1 = always the
+ * fused one-CTA-per-stamp kernel, 2 = the split column/row kernels where N >= 192.  In automatic
+ * mode the first draw of each (device, precision, N, floor(log2 stamps)) class with fewer than
+ * 2 stamps per SM times both on its inputs (when it overwrites its output and the stream is
+ * not being captured) and keeps the faster; the choice then holds for the process.  Results of
+ * the two variants agree to floating-point rounding.  No reference counterpart. */
+int gsb_draw_set_variant(int variant);
+
+/* Text report of the tuned classes, one line each; returns its length (writes at most len-1
+ * characters and a terminating zero to buf when buf is not NULL). */
+int gsb_draw_tune_report(char* buf, size_t len);
+
 /* drawKImage: evaluate the program on an (nkx x nky) grid of k points
  * kx = (kxmin + i) dk, ky = (kymin + j) dk, into complex output (interleaved re, im) with
  * row stride nkx.  One grid per stamp, stamp s at d_out + s * nkx * nky complex elements.

@@ -112,3 +112,48 @@ def test_add_to_image():
     im = obj.drawImage(nx=32, ny=32, scale=0.2, dtype=np.float64, method='fft')
     im2 = obj.drawImage(image=im.copy(), method='fft', add_to_image=True)
     assert np.allclose(im2.array, 2 * im.array, rtol=0, atol=1e-12 * im.array.max())
+
+
+def test_fused_and_split_variants_agree():
+    """The two kernels a bucket can run on (fused one-CTA-per-stamp, split column/row) give
+    the same stamps to FP32 rounding, and the autotuner records its choice per class."""
+    from galsim_b200 import _lib
+    rng = np.random.default_rng(21)
+    B = 24
+    gal = galsim.Sersic(n=rng.uniform(1., 4., B), half_light_radius=rng.uniform(0.6, 1.5, B),
+                        flux=1e4).shear(g1=rng.uniform(-0.2, 0.2, B), g2=rng.uniform(-0.2, 0.2, B))
+    obj = galsim.Convolve(gal, galsim.Kolmogorov(fwhm=0.7), galsim.Pixel(0.2))
+    res = {}
+    try:
+        for v in (1, 2, 0):
+            _lib.set_draw_variant(v)
+            st = galsim.draw_batch(obj, scale=0.2, dtype=np.float32)
+            res[v] = (st.arrays(), st.added_flux, st.N.copy())
+    finally:
+        _lib.set_draw_variant(0)
+    assert max(res[1][2]) >= 192
+    for v in (2, 0):
+        for a, b in zip(res[v][0], res[1][0]):
+            assert np.abs(a.astype(float) - b).max() <= 2e-6 * np.abs(b).max()
+        assert np.allclose(res[v][1], res[1][1], rtol=1e-6, atol=0)
+    assert 'variant=' in _lib.tune_report()
+
+
+def test_graph_replay_matches_eager_draw():
+    """run_batch captures the draw stage of a repeated geometry as a CUDA graph on its second
+    run and replays it afterwards: every run gives the stamps of an eager draw."""
+    rng = np.random.default_rng(5)
+    B = 40
+    gal = galsim.Sersic(n=rng.uniform(0.8, 3.5, B), half_light_radius=rng.uniform(0.3, 1.0, B),
+                        flux=1e3).shear(g1=rng.uniform(-0.2, 0.2, B), g2=rng.uniform(-0.2, 0.2, B))
+    obj = galsim.Convolve(gal, galsim.Kolmogorov(fwhm=0.7), galsim.Pixel(0.2))
+    eager = galsim.run_batch(galsim.plan_batch(obj, scale=0.2), graph=False)
+    ref = eager.flat.cpu().numpy()
+    plan = galsim.plan_batch(obj, scale=0.2)
+    runs = [galsim.run_batch(plan) for _ in range(4)]
+    assert plan.prog._graph_state['graph'] is not None
+    for r in runs:
+        assert np.array_equal(r.flat.cpu().numpy(), ref)
+        assert np.array_equal(r.added_flux, eager.added_flux)
+    # results of earlier runs are not overwritten by later replays
+    assert np.array_equal(runs[1].flat.cpu().numpy(), ref)
