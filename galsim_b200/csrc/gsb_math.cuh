@@ -55,6 +55,44 @@ __device__ inline double gamma_p(double a, double x)
 }
 
 // ---------------------------------------------------------------------------------------
+// FP64 exponential for the Hankel quadrature, by the table-driven method of P. T. P. Tang,
+// "Table-driven implementation of the exponential function in IEEE floating-point arithmetic",
+// ACM TOMS 15 (1989) 144-157:  x = (32 m + j) ln2/32 + r with |r| <= ln2/64 (the reduction in
+// two FMA steps with ln2/32 split into a double and its remainder), exp(x) = 2^m 2^(j/32) p(r),
+// p the degree-6 Taylor polynomial of e^r (truncation < 4e-18 relative), 2^(j/32) correctly
+// rounded.  Within ~2 ulp of exp for -708 <= x <= 709; 0 below -708 (the terms that reach it
+// are far below the quadrature's stopping threshold).
+// ---------------------------------------------------------------------------------------
+__device__ const double kExp2Tab[32] = {
+    1.0, 1.0218971486541166, 1.0442737824274138, 1.0671404006768237, 1.0905077326652577,
+    1.1143867425958924, 1.1387886347566916, 1.1637248587775775, 1.189207115002721,
+    1.215247359980469, 1.241857812073484, 1.2690509571917332, 1.2968395546510096,
+    1.3252366431597413, 1.3542555469368927, 1.383909881963832, 1.4142135623730951,
+    1.4451808069770467, 1.4768261459394993, 1.5091644275934228, 1.5422108254079407,
+    1.5759808451078865, 1.6104903319492543, 1.645755478153965, 1.681792830507429,
+    1.718619298122478, 1.7562521603732995, 1.7947090750031072, 1.8340080864093424,
+    1.8741676341103, 1.9152065613971474, 1.9571441241754002};
+
+__device__ __forceinline__ double exp_tab(double x)
+{
+    if (x < -708.) return 0.;
+    const double t = rint(x * 46.16624130844683);           // 32 / ln2
+    double r = fma(-t, 0.02166084939249829, x);              // ln2/32, leading double
+    r = fma(-t, 7.247021293269686e-19, r);                   // ln2/32, remainder
+    const long long n = (long long)t;
+    const int j = int(n & 31);
+    const long long m = n >> 5;
+    double p = fma(r, 1. / 720., 1. / 120.);
+    p = fma(p, r, 1. / 24.);
+    p = fma(p, r, 1. / 6.);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.);
+    p = fma(p, r, 1.);
+    const double v = __ldg(&kExp2Tab[j]) * p;
+    return __longlong_as_double(__double_as_longlong(v) + (m << 52));
+}
+
+// ---------------------------------------------------------------------------------------
 // Digamma psi(x) = d ln Gamma / dx for x > 0: the recurrence psi(x) = psi(x + 1) - 1/x
 // (A&S 6.3.5) up to x >= 10, then the asymptotic series
 // psi(x) ~ ln x - 1/(2x) - sum_k B_2k / (2k x^2k)  (A&S 6.3.18), five terms.

@@ -180,7 +180,7 @@ __device__ double2 warp_hankel2(const OgataTables& og, const F& f, double k, dou
 // Integrands as functions of log r: exp(-r^(1/n)) and exp(-k^(5/3)).
 struct SersicRadial {
     double invn;
-    __device__ double operator()(double logr) const { return exp(-exp(logr * invn)); }
+    __device__ double operator()(double logr) const { return exp_tab(-exp_tab(logr * invn)); }
 };
 
 // (f, g) with f = exp(-r^(1/n)) and g = df/dn + c r df/dr:  the quadrature sum
@@ -190,14 +190,14 @@ struct SersicRadialDn {
     double invn, c;
     __device__ double2 operator()(double logr) const
     {
-        const double u = exp(logr * invn);
-        const double f = exp(-u);
+        const double u = exp_tab(logr * invn);
+        const double f = exp_tab(-u);
         return make_double2(f, f * u * invn * (logr * invn + c));
     }
 };
 
 struct KolmKValue {
-    __device__ double operator()(double logk) const { return exp(-exp(logk * (5. / 3.))); }
+    __device__ double operator()(double logk) const { return exp_tab(-exp_tab(logk * (5. / 3.))); }
 };
 
 // (1 - P(2n, z)) Gamma(2n) - target   (SersicMissingFlux, SBSersic.cpp:541-556)
@@ -725,6 +725,22 @@ __global__ void prepare_leaves_kernel(const __grid_constant__ gsb_template tpl, 
 }
 
 }  // namespace
+
+namespace {
+__global__ void exp_tab_kernel(const double* x, double* y, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = exp_tab(x[i]);
+}
+}  // namespace
+
+int exp_fp64(const double* d_x, double* d_y, int n, cudaStream_t stream)
+{
+    if (n <= 0) return GSB_OK;
+    exp_tab_kernel<<<(n + 255) / 256, 256, 0, stream>>>(d_x, d_y, n);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    return GSB_OK;
+}
 
 int ogata_init(DeviceState* st)
 {

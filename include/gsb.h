@@ -213,6 +213,11 @@ int gsb_draw_bucket(const gsb_template* tpl, int n_stamps, const gsb_gsparams* g
  * the two variants agree to floating-point rounding.  No reference counterpart. */
 int gsb_draw_set_variant(int variant);
 
+/* The FP64 exponential that the Hankel quadratures of the table stage use (table-driven,
+ * after P. T. P. Tang, ACM TOMS 15 (1989) 144-157), applied to n device values; exposed so that
+ * its accuracy can be checked against the CUDA math library.  No reference counterpart. */
+int gsb_exp_fp64(const double* d_x, double* d_y, int n, void* stream);
+
 /* Text report of the tuned classes, one line each; returns its length (writes at most len-1
  * characters and a terminating zero to buf when buf is not NULL). */
 int gsb_draw_tune_report(char* buf, size_t len);
