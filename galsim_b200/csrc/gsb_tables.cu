@@ -332,9 +332,11 @@ __global__ void __launch_bounds__(256, 4) sersic_nodes_kernel(const double* head
                                     double* vals, const double* dheader, double* dvals, int* status_out)
 {
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-    const long long s = warp / nround;
+    // slots hold ascending n; the costly large-n tables are taken first so that they do not
+    // form the tail of the launch
+    const long long s = count - 1 - warp / nround;
     const int i = i0 + int(warp % nround);
-    if (s >= count) return;
+    if (s < 0) return;
     if (scan[s].done) return;
     const double* H = header + s * kSersicHeader;
     if (i >= int(H[kSH_NCAND])) return;
