@@ -527,7 +527,7 @@ def run_gpu(args):
     for _ in range(args.steps):
         o = gpu_object(galsim, params)
         sb = galsim.draw_batch(o, scale=SCALE, dtype=np.float32)
-        pix = sb.flat.cpu()
+        pix = sb.host(copy=False)      # read into a reused page-locked host buffer
         flux = sb.added_flux
     ee.record()
     barrier()
@@ -535,7 +535,7 @@ def run_gpu(args):
     clk.__exit__(None, None, None)
     L = prog.L
     h2d = B * (L * 136 + len(prog.bld.phases) * 64 + len(prog.bld.scales) * 8 + 32)
-    d2h = int(pix.numel() * 4 + B * 8 + B * L * 16)
+    d2h = int(pix.size * 4 + B * 8 + B * L * 16)
 
     # plain one-stamp-per-launch GPU path on a sample (the metric's denominator)
     n_plain = 64

@@ -224,3 +224,28 @@ class Tables(object):
                 lib().gsb_tables_destroy(self.handle)
         except Exception:
             pass
+
+
+class TablePool(object):
+    """Idle table sets of the current process, reused by later programs: freeing device memory
+    synchronises the device and is slow for table sets of hundreds of MB, and a new set would
+    only allocate the same memory again."""
+    _idle = {}
+
+    @classmethod
+    def acquire(cls):
+        dev = Device.torch_device().index
+        lst = cls._idle.setdefault(dev, [])
+        return lst.pop() if lst else Tables()
+
+    @classmethod
+    def release(cls, t):
+        if t is None:
+            return
+        try:
+            dev = Device.torch_device().index
+        except Exception:
+            return
+        lst = cls._idle.setdefault(dev, [])
+        if len(lst) < 4:
+            lst.append(t)

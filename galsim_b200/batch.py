@@ -17,6 +17,9 @@ from .gsparams import GSParams
 from .position import _PositionD
 
 
+_PINNED = {}
+
+
 class StampBatch(object):
     """The drawn stamps: a flat device buffer plus per-stamp geometry.
 
@@ -54,8 +57,23 @@ class StampBatch(object):
         o = int(self.offsets[i])
         return self.flat[o:o + n].cpu().numpy().reshape(int(self.ny[i]), int(self.nx[i]))
 
+    def host(self, copy=True):
+        """All pixels as one flat host numpy array, read through page-locked memory (a buffer
+        reused by calls of the same size).  copy=False returns a view of that buffer, valid
+        until the next host() call of the same size."""
+        import torch
+        n = self.flat.numel()
+        buf = _PINNED.get((n, self.flat.dtype))
+        if buf is None:
+            buf = torch.empty(n, dtype=self.flat.dtype, pin_memory=True)
+            _PINNED.clear()
+            _PINNED[(n, self.flat.dtype)] = buf
+        buf.copy_(self.flat, non_blocking=True)
+        torch.cuda.current_stream(self.flat.device).synchronize()
+        return buf.numpy().copy() if copy else buf.numpy()
+
     def arrays(self):
-        host = self.flat.cpu().numpy()
+        host = self.host()
         return [host[o:o + int(x * y)].reshape(int(y), int(x))
                 for o, x, y in zip(self.offsets, self.nx, self.ny)]
 

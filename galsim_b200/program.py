@@ -141,7 +141,8 @@ class Program(object):
         if self.sersic_n is None:
             self.tables = None
         elif getattr(self, 'tables', None) is None:
-            self.tables = _lib.Tables()
+            self.tables = _lib.TablePool.acquire()
+            self._pooled_tables = True
 
     def compute_leaves(self):
         """FP64 on the GPU: build the Sersic FT tables, then every leaf's derived constants,
@@ -174,6 +175,13 @@ class Program(object):
         return self.leaf_stepk[:, l], self.leaf_maxk[:, l]
 
     # -- drawing ---------------------------------------------------------------------------
+    def __del__(self):
+        # graphs hold the table pointers; drop them before the tables go back to the pool
+        self._graph_state = None
+        if getattr(self, '_pooled_tables', False):
+            _lib.TablePool.release(self.tables)
+            self.tables = None
+
     def reset_records(self):
         """Forget the device copy and sizing after the host records (bld.leaves / phases /
         scales) were changed in place."""
