@@ -179,7 +179,10 @@ class Program(object):
         # graphs hold the table pointers; drop them before the tables go back to the pool
         self._graph_state = None
         if getattr(self, '_pooled_tables', False):
-            _lib.TablePool.release(self.tables)
+            try:
+                _lib.TablePool.release(self.tables)
+            except Exception:      # interpreter shutdown
+                pass
             self.tables = None
 
     def reset_records(self):
