@@ -255,6 +255,20 @@ def gpu_object(galsim, p):
     return galsim.Convolve(gal, galsim.Kolmogorov(fwhm=p[:, 5]), galsim.Pixel(SCALE))
 
 
+# Measured DRAM bytes per stamp of the fused draw kernel by FFT size (ncu, 600-stamp case of
+# this workload; profiles/draw_fused_kernel_dram_per_stamp.md).  Larger N scale as N^2.
+DRAM_BYTES_PER_STAMP = {128: 8732., 192: 110406., 256: 18898.}
+
+
+def measured_traffic(N):
+    N = np.asarray(N)
+    tot = 0.
+    for n in N:
+        n = int(n)
+        tot += DRAM_BYTES_PER_STAMP.get(n, DRAM_BYTES_PER_STAMP[256] * (n / 256.) ** 2)
+    return tot
+
+
 def algorithmic_bytes(N, nx, ny):
     """Per-stamp algorithmic bytes of the FFT drawing path at FP32 storage: k-grid write,
     FFT read, FFT write, fold read, stamp write (8 H + 8 H + 4 N^2 + 4 nx ny + 4 nx ny,
@@ -584,7 +598,10 @@ def run_gpu(args):
             'e2e': {'value': world * B / (e2e_ms * 1e-3), 'unit': 'stamps/s',
                     'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': d2h},
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
-                         'frac': achieved / peak, 'traffic': None, 'peak_kind': peak_kind,
+                         'frac': achieved / peak, 'traffic': measured_traffic(N),
+                         'traffic_note': 'ncu DRAM read+write bytes per stamp by N (600-stamp capture) '
+                                         'scaled to this step; algorithmic bytes %.0f' % alg,
+                         'peak_kind': peak_kind,
                          'kernel': 'draw_fused_kernel, all FFT-size buckets concurrent (one draw-graph replay)',
                          'kernel_ms': k_ms},
             'gpu_launches': int(args.steps * (nb + 5)),
