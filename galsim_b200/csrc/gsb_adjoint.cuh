@@ -162,6 +162,29 @@ __device__ __noinline__ void adjoint_range(const gsb_template& tpl, const AdjSme
     }
 }
 
+// Gradients of the leaves of a Sum atom (LEAF and ADD ops [o0, o1)) with cotangent w: each
+// leaf receives w unchanged.
+template <typename T>
+__device__ __noinline__ void sum_atom_grads(const gsb_template& tpl, const AdjSmem& A, unsigned want,
+                                            T kx, T ky, int i, int j, const GridRef& g, Cx<T> w, T* acc,
+                                            int o0, int o1)
+{
+    const T ar = w.x;
+    for (int o = o0; o < o1; ++o) {
+        if (tpl.op_code[o] != GSB_OP_LEAF) continue;
+        const int l = tpl.op_arg[o];
+        if (!want_leaf(want, l)) continue;
+        const LeafD<T> d = leaf_grad<T>(A.S.leaf[l], A.S.sersic, A.dn, kx, ky, g, i - g.x0, j - g.y0);
+        T* gl = acc + kGradPerLeaf * l;
+        gl[0] += ar * d.unit;
+        gl[1] += ar * d.gx * kx;
+        gl[2] += ar * d.gy * kx;
+        gl[3] += ar * d.gx * ky;
+        gl[4] += ar * d.gy * ky;
+        gl[5] += ar * d.gn;
+    }
+}
+
 // Factored reverse pass at (i, j): F = prod_a atom_a * XS[i] YS[j]; the cotangent of atom a
 // is u XS YS prod_{b != a} atom_b (prefix and suffix products, no division).  Leaf, phase and
 // scale atoms accumulate into ga[a][*] (registers); subtree atoms run adjoint_range into acc.
@@ -242,6 +265,8 @@ __device__ __forceinline__ void adjoint_point_factored(const gsb_template& tpl, 
                 ga[a][3] += ar * ld[a].gx * ky;
                 ga[a][4] += ar * ld[a].gy * ky;
                 ga[a][5] += ar * ld[a].gn;
+            } else if (kind == kAtomSum) {
+                sum_atom_grads<T>(tpl, A, want, kx, ky, i, j, g, w, acc, o0, o1);
             } else {
                 adjoint_range<T>(tpl, A, dk, i, j, g, w, acc, o0, o1);
             }
@@ -322,7 +347,8 @@ __global__ void __launch_bounds__(adj_warps<T, N>() * 32) adjoint_fused_kernel(c
         bool subtree = !factored;
         if (factored)
             for (int t = 0; t < S.n_atoms; ++t)
-                subtree |= S.atom_kind[t] == kAtomRange && S.atom_o1[t] - S.atom_o0[t] > 1;
+                subtree |= (S.atom_kind[t] == kAtomRange || S.atom_kind[t] == kAtomSum) &&
+                           S.atom_o1[t] - S.atom_o0[t] > 1;
 
         // ---- row phase: forward-sign DFT of pairs of cotangent rows ----
         const int npairs = (G.ny + 1) / 2;

@@ -177,7 +177,9 @@ template <> struct NodeT<double> { using type = double4; };
 
 // Decide which factors of this stamp are cached in shared memory (thread 0), in order:
 // Sersic spline nodes, phase factors, separable leaf factors, until the budget is used.
-enum { kAtomRange = 0, kAtomPhase = 1, kAtomScale = 2 };
+// kAtomSum: a subtree of LEAF and ADD ops only (e.g. bulge + disk), whose cotangent passes
+// unchanged to each of its leaves.
+enum { kAtomRange = 0, kAtomPhase = 1, kAtomScale = 2, kAtomSum = 3 };
 
 // want bits: leaf l = bit l, phase p = bit 8 + p, scale q = bit 16 + q.
 __device__ __forceinline__ bool want_leaf(unsigned want, int l) { return (want >> l) & 1u; }
@@ -247,9 +249,12 @@ __device__ inline bool plan_factored(StampSmem& S, const gsb_template& tpl, unsi
                     continue;
                 }
             }
+            bool sum = code == GSB_OP_ADD;
+            for (int q = start[o]; q <= o && sum; ++q)
+                sum = tpl.op_code[q] == GSB_OP_LEAF || tpl.op_code[q] == GSB_OP_ADD;
             S.atom_o0[S.n_atoms] = start[o];
             S.atom_o1[S.n_atoms] = o + 1;
-            S.atom_kind[S.n_atoms] = kAtomRange;
+            S.atom_kind[S.n_atoms] = sum ? kAtomSum : kAtomRange;
             S.atom_arg[S.n_atoms] = (unsigned char)(code == GSB_OP_LEAF ? arg : 0);
             ++S.n_atoms;
         }

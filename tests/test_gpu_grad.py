@@ -233,3 +233,30 @@ def test_backward_after_a_later_forward_with_shared_tables():
     m(torch.as_tensor(q, device=dev))
     loss1.backward()
     assert torch.allclose(p1.grad, ref, rtol=1e-12, atol=0.)
+
+
+def test_want_mask_factored_sum_atom_matches_full_adjoint():
+    """Gradients of the bulge and disk of Sum(Sersic, Exponential) (x Moffat x Pixel) computed
+    with a want mask (factored pass; the Sum is one atom whose cotangent reaches both leaves)
+    equal those of the full reverse pass over every record; unwanted entries are zero."""
+    rng = np.random.default_rng(13)
+    B = 4
+    bulge = galsim.Sersic(n=4., half_light_radius=rng.uniform(0.3, 0.5, B), flux=rng.uniform(100., 300., B))
+    disk = galsim.Exponential(half_light_radius=rng.uniform(0.6, 1.0, B), flux=rng.uniform(300., 700., B))
+    obj = galsim.Convolve(galsim.Add(bulge.shear(g1=rng.uniform(-0.2, 0.2, B), g2=rng.uniform(-0.2, 0.2, B)),
+                                     disk.shear(g1=rng.uniform(-0.2, 0.2, B), g2=rng.uniform(-0.2, 0.2, B))),
+                          galsim.Moffat(beta=3.7, fwhm=0.7), galsim.Pixel(0.2))
+    for prec, dt, tol in (('fp64', np.float64, 1e-9), ('fp32', np.float32, 2e-5)):
+        plan = autodiff.RecordPlan(obj, 48, 48, 0.2, dtype=dt, precision=prec)
+        img = plan.draw()
+        w = torch.as_tensor(np.random.default_rng(1).standard_normal(tuple(img.shape)), device=img.device)
+        full = plan.adjoint(w)
+        plan.want = 0b11
+        part = plan.adjoint(w)
+        for k in ('leaf_flux', 'leaf_jac', 'leaf_size', 'leaf_n'):
+            a, b = part[k].cpu().numpy(), full[k].cpu().numpy()
+            scale = np.abs(b[:, :2]).max()
+            assert np.abs(a[:, :2] - b[:, :2]).max() <= tol * scale, (prec, k)
+            assert np.all(a[:, 2:] == 0.)
+        for k in ('phase_cen', 'phase_fs', 'phase_jac', 'scales'):
+            assert np.all(part[k].cpu().numpy() == 0.)
