@@ -573,6 +573,22 @@ def run_gpu(args):
     torch.cuda.synchronize(dev)
     plain_rate = n_plain / (tp0.elapsed_time(tp1) * 1e-3)
 
+    # FP32 error of the measured path against the FP64 kernels (which match the reference to
+    # 1e-9 x peak on its fixtures), on a leading sample of the batch
+    ns = min(256, B)
+    sub = gpu_object(galsim, params[:ns])
+    a32 = galsim.draw_batch(sub, scale=SCALE, dtype=np.float32)
+    a64 = galsim.draw_batch(sub, scale=SCALE, dtype=np.float64, precision='fp64')
+    errs = []
+    for i in range(ns):
+        o, m = int(a32.offsets[i]), int(a32.nx[i] * a32.ny[i])
+        d = (a32.flat[o:o + m].double() - a64.flat[o:o + m]).abs().max().item()
+        errs.append(d / a64.flat[o:o + m].abs().max().item())
+    ferr = np.abs(a32.added_flux - a64.added_flux) / np.abs(a64.added_flux)
+    fp32_err = {'stamps': ns, 'max_abs_over_peak_median': float(np.median(errs)),
+                'max_abs_over_peak_max': float(np.max(errs)), 'flux_rel_median': float(np.median(ferr)),
+                'flux_rel_max': float(np.max(ferr)), 'against': 'FP64 kernels of this library'}
+
     fit = run_fit_step(args, galsim, dev, max(args.steps, 3), max(args.warmup, 2))
     mixed = run_mixed(galsim, dev, max(args.steps, 3), max(args.warmup, 2)) if not args.no_extra else None
     large = run_large(galsim, dev) if not args.no_extra else None
@@ -606,6 +622,7 @@ def run_gpu(args):
                          'kernel_ms': k_ms},
             'gpu_launches': int(args.steps * (nb + 5)),
             'plain_one_stamp_per_launch': {'value': plain_rate, 'unit': 'stamps/s', 'sample': n_plain},
+            'fp32_error_vs_fp64': fp32_err,
             'grad_evals': fit,
             'mixed_batch': mixed,
             'large_stamps': large,

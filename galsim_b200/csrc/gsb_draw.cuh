@@ -323,7 +323,7 @@ __device__ inline void fill_caches(const StampSmem& S, const gsb_template& tpl, 
             const double4* src = S.sersic[l].node;
             for (int i = threadIdx.x; i < S.sersic[l].n; i += blockDim.x) {
                 const double4 v = src[i];
-                dst[i].x = T(v.x); dst[i].y = T(v.y); dst[i].z = T(v.z); dst[i].w = T(0);
+                dst[i].x = T(v.x); dst[i].y = T(v.y); dst[i].z = T(v.z); dst[i].w = T(v.w);
             }
         }
         if (S.leaf_cache[l] >= 0) {
@@ -405,10 +405,12 @@ __device__ inline T sersic_kvalue_smem(const SersicTableView& tb, const typename
     if (i >= tb.n) i = tb.n - 1;
     if (i <= 0) i = 1;
     const typename NodeT<T>::type n0 = node[i - 1], n1 = node[i];
-    // Divide by h formed from the same (rounded) node positions as aa and bb, so that the
-    // interpolation weights aa / h + bb / h sum to 1 exactly; 1/da instead costs ~1e-6 in FP32.
-    const T h = n1.x - n0.x;
-    const T aa = n1.x - lk;
+    // The offset from the upper node is 0.5 ln(k_i^2 / k^2), the log of a ratio near 1, and
+    // the spacing is the table's: both accurate in FP32 (a difference of two logs of size ~10,
+    // or of rounded node positions, would cost up to ~1e-6 of the value).  bb = h - aa keeps
+    // the weights aa / h + bb / h summing to 1.
+    const T h = T(tb.da);
+    const T aa = T(0.5) * log(n1.w / ksq);
     const T bb = h - aa;
     const T num = aa * n0.y + bb * n1.y - (T(1) / T(6)) * aa * bb * ((aa + h) * n0.z + (bb + h) * n1.z);
     return num / h / ksq;
@@ -515,6 +517,18 @@ __device__ __forceinline__ Cx<T> eval_factored(const gsb_template& tpl, const St
     return cscale<T>(cmul<T>(c, xy), r);
 }
 
+// acc += v with Kahan's compensation term comp (componentwise).
+template <typename T>
+__device__ __forceinline__ void kahan_add(Cx<T>& acc, Cx<T>& comp, Cx<T> v)
+{
+    const T yx = v.x - comp.x, yy = v.y - comp.y;
+    const T tx = acc.x + yx, ty = acc.y + yy;
+    comp.x = (tx - acc.x) - yx;
+    comp.y = (ty - acc.y) - yy;
+    acc.x = tx;
+    acc.y = ty;
+}
+
 template <typename T>
 __device__ inline void store_pixel(void* out, int dtype, int add, long long idx, T v)
 {
@@ -572,7 +586,8 @@ __global__ void __launch_bounds__(fused_warps<T, N>() * 32) draw_fused_kernel(co
             for (int r = lane; r < N; r += 32) {
                 const int kyc = r < N / 2 ? r : r - N;
                 const int blo = ceil_div(-hk - kyc, N), bhi = floor_div(hk - kyc, N);
-                Cx<T> acc = cx<T>(T(0), T(0));
+                // the fold (wrap) of the aliases, with Kahan compensation
+                Cx<T> acc = cx<T>(T(0), T(0)), comp = acc;
                 for (int ia = alo; ia <= ahi; ++ia) {
                     const int kx = c + ia * N;
                     for (int ib = blo; ib <= bhi; ++ib) {
@@ -583,7 +598,7 @@ __global__ void __launch_bounds__(fused_warps<T, N>() * 32) draw_fused_kernel(co
                                   : fast ? eval_fast<T>(a.tpl, S, cache, dk, ii, jj, g)
                                          : eval_program<T>(a.tpl, S, dk, ii, jj, g);
                         if (!pos) v = cconj<T>(v);
-                        acc = cadd<T>(acc, v);
+                        kahan_add<T>(acc, comp, v);
                     }
                 }
                 buf[r] = acc;

@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(THREADS) large_col_kernel(const __grid_constan
         for (int r = threadIdx.x; r < N; r += blockDim.x) {
             const int kyc = r < N / 2 ? r : r - N;
             const int blo = ceil_div(-hk - kyc, N), bhi = floor_div(hk - kyc, N);
-            Cx<T> acc = cx<T>(T(0), T(0));
+            Cx<T> acc = cx<T>(T(0), T(0)), comp = acc;     // Kahan-compensated fold
             for (int ia = alo; ia <= ahi; ++ia) {
                 const int kx = c + ia * N;
                 for (int ib = blo; ib <= bhi; ++ib) {
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(THREADS) large_col_kernel(const __grid_constan
                     const Cx<T> v = factored ? eval_factored<T>(a.tpl, S, cache, dk, ii, jj, g)
                                     : fast ? eval_fast<T>(a.tpl, S, cache, dk, ii, jj, g)
                                            : eval_program<T>(a.tpl, S, dk, ii, jj, g);
-                    acc = cadd<T>(acc, pos ? v : cconj<T>(v));
+                    kahan_add<T>(acc, comp, pos ? v : cconj<T>(v));
                 }
             }
             buf[r] = acc;

@@ -52,8 +52,8 @@ __device__ inline void sersic_phi_grad(const SersicTableView& tb, const SersicDn
     if (i >= tb.n) i = tb.n - 1;
     if (i <= 0) i = 1;
     const double4 n0 = tb.node[i - 1], n1 = tb.node[i];
-    const T h = T(n1.x) - T(n0.x);
-    const T aa = T(n1.x) - lk;
+    const T h = T(tb.da);
+    const T aa = T(0.5) * log(T(n1.w) / u);      // as in the forward lookup
     const T bb = h - aa;
     const T Q = (aa + h) * T(n0.z) + (bb + h) * T(n1.z);
     const T P = aa * bb;

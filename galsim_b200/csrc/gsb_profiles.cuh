@@ -96,7 +96,8 @@ __device__ inline bool exponential_keep(const LeafParams& L, double dk, int gx0,
 
 // ---------------------------------------------------------------------------------------
 // Sersic FT spline lookup (SersicInfo::kValue, src/SBSersic.cpp:363-376; TSpline::_interp,
-// src/Table.cpp:571-586 with ArgVec::upperIndex equal-spacing branch, :73-85).
+// src/Table.cpp:571-586 with ArgVec::upperIndex equal-spacing branch, :73-85).  The node's .w
+// holds its k^2.
 // ---------------------------------------------------------------------------------------
 template <typename T>
 __device__ inline T sersic_kvalue(const SersicTableView& tb, T ksq)
@@ -112,8 +113,10 @@ __device__ inline T sersic_kvalue(const SersicTableView& tb, T ksq)
         if (i <= 0) i = 1;
         const double4 n0 = tb.node[i - 1];
         const double4 n1 = tb.node[i];
-        const T h = T(n1.x) - T(n0.x);
-        const T aa = T(n1.x) - lk;
+        // the offset from the upper node as the log of a ratio near 1 (accurate in FP32, unlike
+        // the difference of two logarithms of size ~10); the spacing is the table's own
+        const T h = T(tb.da);
+        const T aa = T(0.5) * log(T(n1.w) / ksq);
         const T bb = h - aa;
         const T f = (aa * T(n0.y) + bb * T(n1.y) -
                      (T(1) / T(6)) * aa * bb * ((aa + h) * T(n0.z) + (bb + h) * T(n1.z))) / h;

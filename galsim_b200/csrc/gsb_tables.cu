@@ -501,7 +501,8 @@ __global__ void __launch_bounds__(32) sersic_finalize_kernel(double* header, int
         natural_spline(xs, ys, zs, cs, N);
     }
     __syncwarp();
-    for (int i = lane; i < N; i += 32) nd[i] = make_double4(xs[i] - front, ys[i], zs[i], 0.);
+    // .w: k^2 at the node, for the evaluators' spline offset 0.5 ln(k_i^2 / k^2)
+    for (int i = lane; i < N; i += 32) nd[i] = make_double4(xs[i] - front, ys[i], zs[i], exp(2. * xs[i]));
     const double back = xs[N - 1];
     if (dnodes) {
         // The spline is linear in its node values, so d/dn of the interpolant is the spline of

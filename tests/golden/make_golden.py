@@ -140,6 +140,41 @@ def main_large(ref_root):
     print('wrote', os.path.join(HERE, 'reference_large.npz'), len(out), 'arrays')
 
 
+# Gradients of the fit-step model by central differences of the reference's own drawImage:
+# L(p) = sum(w * image(p)) for Convolve(Sersic(n, hlr, flux).shear(g1, g2).shift(dx, dy),
+# Moffat(2.5, fwhm=0.8), Pixel(0.2)) drawn into 48 x 48 float64 at scale 0.2; step 1e-4
+# (relative for flux and hlr, absolute for the others).
+GRAD_PARAMS = [(1.2e4, 0.55, 1.7, 0.07, -0.04, 0.05, -0.08),
+               (6.0e3, 0.9, 2.6, -0.12, 0.09, -0.11, 0.03),
+               (2.0e4, 0.35, 1.1, 0.02, 0.15, 0.0, 0.12)]
+
+
+def fit_model(galsim, p):
+    flux, hlr, n, g1, g2, dx, dy = p
+    gal = galsim.Sersic(n=n, half_light_radius=hlr, flux=flux).shear(g1=g1, g2=g2).shift(dx, dy)
+    return galsim.Convolve(gal, galsim.Moffat(beta=2.5, fwhm=0.8), galsim.Pixel(0.2))
+
+
+def main_grad(ref_root):
+    from ref_import import import_reference_galsim
+    galsim = import_reference_galsim(ref_root)
+    w = np.random.default_rng(2024).standard_normal((len(GRAD_PARAMS), 48, 48))
+    grads = np.zeros((len(GRAD_PARAMS), 7))
+    for s, p in enumerate(GRAD_PARAMS):
+        for j in range(7):
+            h = 1e-4 * (p[j] if j in (0, 1) else 1.)
+            val = []
+            for sgn in (1., -1.):
+                q = list(p)
+                q[j] += sgn * h
+                im = fit_model(galsim, q).drawImage(nx=48, ny=48, scale=0.2, dtype=np.float64, method='fft')
+                val.append(float((w[s] * im.array).sum()))
+            grads[s, j] = (val[0] - val[1]) / (2. * h)
+    np.savez_compressed(os.path.join(HERE, 'reference_grad.npz'), params=np.array(GRAD_PARAMS), w=w,
+                        fd_grad=grads)
+    print('wrote', os.path.join(HERE, 'reference_grad.npz'))
+
+
 def main(ref_root):
     from ref_import import import_reference_galsim
     galsim = import_reference_galsim(ref_root)
@@ -189,6 +224,10 @@ def main(ref_root):
 if __name__ == '__main__':
     args = [a for a in sys.argv[1:] if not a.startswith('--')]
     root = args[0] if args else '/root/reference'
-    if '--large-only' not in sys.argv:
-        main(root)
-    main_large(root)
+    if '--grad-only' in sys.argv:
+        main_grad(root)
+    else:
+        if '--large-only' not in sys.argv:
+            main(root)
+        main_large(root)
+        main_grad(root)

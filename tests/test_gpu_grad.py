@@ -260,3 +260,20 @@ def test_want_mask_factored_sum_atom_matches_full_adjoint():
             assert np.all(a[:, 2:] == 0.)
         for k in ('phase_cen', 'phase_fs', 'phase_jac', 'scales'):
             assert np.all(part[k].cpu().numpy() == 0.)
+
+
+def test_gradients_vs_differenced_reference_drawimage():
+    """Adjoint gradients of sum(w * image) for the fit-step model against central differences
+    of the reference's own drawImage (tests/golden/reference_grad.npz, step 1e-4): FP64 and
+    FP32 adjoints to 1e-4 (natural units, as above)."""
+    import os
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden', 'reference_grad.npz'))
+    params, w, fd = d['params'], d['w'], d['fd_grad']
+    psf = galsim.Convolve(galsim.Moffat(beta=2.5, fwhm=0.8), galsim.Pixel(0.2))
+    dev = galsim._lib.Device.torch_device()
+    wt = torch.as_tensor(w, device=dev)
+    for prec, dt in (('fp64', np.float64), ('fp32', np.float32)):
+        m = autodiff.GalaxyModel(psf, 48, 48, 0.2, dtype=dt, precision=prec)
+        p = torch.as_tensor(params, device=dev, dtype=torch.float64).requires_grad_(True)
+        (m(p).double() * wt).sum().backward()
+        _assert_grad_close(p.grad.cpu().numpy(), fd, params, 1e-4)
