@@ -22,5 +22,7 @@ from .compound import Convolve, Convolution, Add, Sum, Transform, Transformation
 from .batch import draw_batch, plan_batch, run_batch, StampBatch
 from ._lib import set_device
 from . import autodiff
+from . import config
+from .config import draw_config
 
 __version__ = '0.1.0'

@@ -175,6 +175,43 @@ def main_grad(ref_root):
     print('wrote', os.path.join(HERE, 'reference_grad.npz'))
 
 
+# Config-driven stamps (galsim/config): the reference's BuildStamps for each object.
+CONFIG_NOBJ = 6
+CONFIG_CASE = {
+    'gal': {
+        'type': 'Sum',
+        'items': [
+            {'type': 'Sersic', 'n': {'type': 'List', 'items': [1.5, 2.5, 4.0, 0.8, 3.2, 1.1]},
+             'half_light_radius': {'type': 'List', 'items': [0.4, 0.6, 0.3, 0.8, 0.5, 0.45]},
+             'flux': {'type': 'Sequence', 'first': 300., 'step': 50.}},
+            {'type': 'Exponential', 'half_light_radius': 0.9,
+             'flux': {'type': 'List', 'items': [500., 800.]},
+             'ellip': {'type': 'E1E2', 'e1': 0.2, 'e2': {'type': 'List', 'items': [-0.1, 0.15, 0.0]}}},
+        ],
+        'ellip': {'type': 'G1G2', 'g1': {'type': 'List', 'items': [0.05, -0.12, 0.2]},
+                  'g2': {'type': 'Sequence', 'first': -0.1, 'step': 0.04}},
+        'rotate': {'type': 'List', 'items': ['10 deg', '-25 deg', '40 deg', '0 deg']},
+        'dilate': {'type': 'Sequence', 'first': 1.0, 'step': 0.05, 'repeat': 2},
+        'magnify': 1.02,
+        'shift': {'type': 'XY', 'x': {'type': 'List', 'items': [0.1, -0.05]}, 'y': 0.03},
+    },
+    'psf': {'type': 'Moffat', 'beta': {'type': 'List', 'items': [2.5, 3.0, 3.7]}, 'fwhm': 0.7},
+    'stamp': {'type': 'Basic', 'size': 48, 'offset': {'type': 'XY', 'x': 0.2, 'y': -0.1}},
+    'image': {'type': 'Single', 'pixel_scale': 0.2},
+}
+
+
+def main_config(ref_root):
+    import copy
+    from ref_import import import_reference_galsim
+    galsim = import_reference_galsim(ref_root)
+    images = galsim.config.BuildStamps(CONFIG_NOBJ, copy.deepcopy(CONFIG_CASE), do_noise=False)[0]
+    out = {'stamp_%d' % i: im.array.astype(np.float64) for i, im in enumerate(images)}
+    out['flux'] = np.array([im.array.sum() for im in images])
+    np.savez_compressed(os.path.join(HERE, 'reference_config.npz'), **out)
+    print('wrote', os.path.join(HERE, 'reference_config.npz'))
+
+
 def main(ref_root):
     from ref_import import import_reference_galsim
     galsim = import_reference_galsim(ref_root)
@@ -226,8 +263,11 @@ if __name__ == '__main__':
     root = args[0] if args else '/root/reference'
     if '--grad-only' in sys.argv:
         main_grad(root)
+    elif '--config-only' in sys.argv:
+        main_config(root)
     else:
         if '--large-only' not in sys.argv:
             main(root)
         main_large(root)
         main_grad(root)
+        main_config(root)
