@@ -1,8 +1,8 @@
 """galsim_b200: GalSim's FFT drawing path on NVIDIA B200 (sm_100a).
 
 A drop-in for ``GSObject.drawImage(method='fft')`` and ``drawKImage`` on
-Convolve / Sum / Transform trees of Gaussian, Exponential, Sersic, Moffat, Kolmogorov, Airy
-and Box / Pixel.  The host code here mirrors the reference's Python API; every numerical
+Convolve / Sum / Transform trees of Gaussian, Exponential, Sersic, Moffat, Kolmogorov, Airy,
+Box / Pixel and InterpolatedImage.  The host code here mirrors the reference's Python API; every numerical
 step of drawing (FP64 sizing and Sersic tables, k-space evaluation, Hermitian wrap, inverse
 FFT, crop and flux sum) runs in the hand-written CUDA kernels of libgsb.so, called through
 the C ABI declared in include/gsb.h.  There is no CPU fallback.
@@ -18,6 +18,9 @@ from .image import Image, _Image, ImageF, ImageD, ImageI, ImageS, ImageCF, Image
 from .gsobject import GSObject
 from .profiles import Gaussian, Exponential, Sersic, DeVaucouleurs, Moffat, Kolmogorov, Airy
 from .box import Box, Pixel
+from .interpolant import (Interpolant, Delta, Nearest, SincInterpolant, Linear, Cubic, Quintic,
+                          Lanczos, convert_interpolant)
+from .interpolatedimage import InterpolatedImage
 from .compound import Convolve, Convolution, Add, Sum, Transform, Transformation, _Transform
 from .batch import draw_batch, plan_batch, run_batch, StampBatch
 from ._lib import set_device

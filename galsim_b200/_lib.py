@@ -16,7 +16,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, 'libgsb.so')
 
 MAX_OPS, MAX_LEAVES, MAX_PHASES, MAX_SCALES = 32, 8, 8, 8
-GAUSSIAN, EXPONENTIAL, SERSIC, MOFFAT, KOLMOGOROV, AIRY, BOX = range(7)
+GAUSSIAN, EXPONENTIAL, SERSIC, MOFFAT, KOLMOGOROV, AIRY, BOX, INTERPOLATED = range(8)
+INTERP_DELTA, INTERP_NEAREST, INTERP_LINEAR, INTERP_CUBIC, INTERP_QUINTIC = range(5)
+IMAGE_STEPK, IMAGE_MAXK, IMAGE_MAX_N = 1, 2, 4096
 OP_LEAF, OP_MUL, OP_ADD, OP_PHASE, OP_SCALE = 1, 2, 3, 4, 5
 LEAF_JAC_GENERAL, LEAF_SIZE_IS_HLR = 1, 2
 PHASE_JAC_GENERAL = 1
@@ -51,6 +53,13 @@ STAMP_DTYPE = np.dtype({'names': ['N', 'Nk', 'xmin', 'ymin', 'nx', 'ny', 'out_of
                         'formats': ['i4', 'i4', 'i4', 'i4', 'i4', 'i4', 'i8'],
                         'offsets': [0, 4, 8, 12, 16, 20, 24], 'itemsize': 32})
 
+IMAGE_DESC_DTYPE = np.dtype({'names': ['N', 'nx', 'ny', 'x0', 'y0', 'bx0', 'bx1', 'by0', 'by1',
+                                         'x_interp', 'flags', 'pix_offset', 'flux', 'stepk_target',
+                                         'maxk_limit'],
+                              'formats': ['i4'] * 11 + ['i8', 'f8', 'f8', 'f8'],
+                              'offsets': [0, 4, 8, 12, 16, 20, 24, 28, 32, 36, 40, 48, 56, 64, 72],
+                              'itemsize': 80})
+
 SERSIC_HEADER = 16
 SH_N, SH_NUSED, SH_FRONT, SH_DA, SH_KSQMIN, SH_KSQMAX, SH_KD2, SH_KD4, SH_HIGHA, SH_HIGHB, \
     SH_MAXK, SH_STEPK, SH_RE, SH_DLOGK, SH_NCAND, SH_STATUS = range(16)
@@ -77,6 +86,8 @@ def lib():
             'gsb_sersic_tables_build': (i, [vp, vp, vp, i, ctypes.POINTER(GSParamsC), vp]),
             'gsb_sersic_tables_build_ex': (i, [vp, vp, vp, i, ctypes.POINTER(GSParamsC), i, vp]),
             'gsb_sersic_tables_info': (i, [vp, vp, i, vp]),
+            'gsb_images_build': (i, [vp, i, vp, vp, ctypes.POINTER(GSParamsC), vp]),
+            'gsb_images_info': (i, [vp, vp, i, vp]),
             'gsb_adjoint_grad_count': (i, [ctypes.POINTER(TemplateC)]),
             'gsb_adjoint_workspace_size': (sz, [i, i, i]),
             'gsb_adjoint_images': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp,
@@ -210,6 +221,23 @@ class Tables(object):
         self.count = len(n)
         self.with_dn = with_dn
         self.generation = getattr(self, 'generation', 0) + 1
+
+    def build_images(self, desc, pixels, gsp):
+        """Build the k-images (and stepk / maxk scans) of the InterpolatedImage sources:
+        desc an IMAGE_DESC_DTYPE array, pixels the packed FP64 pixels (a device tensor)."""
+        desc = np.ascontiguousarray(desc, dtype=IMAGE_DESC_DTYPE)
+        check(lib().gsb_images_build(self.handle, len(desc), desc.ctypes.data_as(ctypes.c_void_p),
+                                     ptr(pixels), ctypes.byref(gsparams_c(gsp)), Device.stream()))
+        self.n_images = len(desc)
+        self.generation = getattr(self, 'generation', 0) + 1
+
+    def image_info(self, count=None):
+        """(R, maxk) per image slot, image units."""
+        count = self.n_images if count is None else count
+        out = np.zeros((count, 2))
+        check(lib().gsb_images_info(self.handle, out.ctypes.data_as(ctypes.c_void_p), count,
+                                    Device.stream()))
+        return out
 
     def sersic_info(self, count=None):
         count = self.count if count is None else count

@@ -22,8 +22,10 @@ from . import _lib
 from .errors import GalSimError, GalSimValueError
 
 # p index of each leaf type's size parameter (Box: width, height = p[0], p[1])
+# (InterpolatedImage leaves have no size record: their p holds the interpolant codes, and
+# the adjoint gives them no gradient entries.)
 _SIZE_INDEX = {_lib.GAUSSIAN: 0, _lib.EXPONENTIAL: 0, _lib.SERSIC: 1, _lib.MOFFAT: 1,
-               _lib.KOLMOGOROV: 0, _lib.AIRY: 0, _lib.BOX: 0}
+               _lib.KOLMOGOROV: 0, _lib.AIRY: 0, _lib.BOX: 0, _lib.INTERPOLATED: None}
 
 RECORD_FIELDS = ('leaf_flux', 'leaf_jac', 'leaf_size', 'leaf_n', 'phase_cen', 'phase_fs',
                  'phase_jac', 'scales')
@@ -69,6 +71,8 @@ class RecordPlan(object):
         nval = np.zeros((B, L))
         for l, t in enumerate(self.types):
             i = _SIZE_INDEX[t]
+            if i is None:
+                continue
             size[:, l, 0] = lv['p'][:, l, i]
             if t == _lib.BOX:
                 size[:, l, 1] = lv['p'][:, l, 1]
@@ -118,7 +122,7 @@ class RecordPlan(object):
                 r['jac'] = j
                 general = (j[:, 1] != 0.) | (j[:, 2] != 0.)
                 r['flags'] = (r['flags'] & ~_lib.LEAF_JAC_GENERAL) | np.where(general, _lib.LEAF_JAC_GENERAL, 0)
-            if 'leaf_size' in host:
+            if 'leaf_size' in host and _SIZE_INDEX[t] is not None:
                 r['p'][:, _SIZE_INDEX[t]] = host['leaf_size'][:, l, 0]
                 if t == _lib.BOX:
                     r['p'][:, 1] = host['leaf_size'][:, l, 1]
@@ -156,7 +160,9 @@ class RecordPlan(object):
         B, L, P, S = self.B, self.L, self.P, self.S
         if self._tables_gen is not None and self._tables_gen[0].generation != self._tables_gen[1]:
             # a shared table set was rebuilt for another draw since ours: rebuild our slots
-            self.prog.tables.build_sersic(self.prog.sersic_n, self.prog.gsparams, with_dn=True)
+            # and prepare the leaves again (they hold the image slots' device addresses)
+            self.prog.need_dn = True
+            self.prog.compute_leaves()
             self._tables_gen = (self.prog.tables, self.prog.tables.generation)
         dt = _lib.F32 if self.dtype == np.float32 else _lib.F64
         tdt = torch.float32 if dt == _lib.F32 else torch.float64
@@ -172,6 +178,8 @@ class RecordPlan(object):
         size = rec['leaf_size']
         gsize = torch.zeros_like(size)
         for l, t in enumerate(self.types):
+            if t == _lib.INTERPOLATED:
+                continue
             if t == _lib.BOX:
                 gsize[:, l, 0] = (jac[:, l, 0] * gjac[:, l, 0] + jac[:, l, 2] * gjac[:, l, 2]) / size[:, l, 0]
                 gsize[:, l, 1] = (jac[:, l, 1] * gjac[:, l, 1] + jac[:, l, 3] * gjac[:, l, 3]) / size[:, l, 1]

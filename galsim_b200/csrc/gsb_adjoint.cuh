@@ -98,8 +98,14 @@ __device__ __noinline__ void adjoint_range(const gsb_template& tpl, const AdjSme
         const int code = tpl.op_code[o], arg = tpl.op_arg[o];
         const int a = A.child1[o], b = A.child2[o];
         if (code == GSB_OP_LEAF) {
-            ld[arg] = leaf_grad<T>(S.leaf[arg], S.sersic, A.dn, kx, ky, g, i - g.x0, j - g.y0);
-            val[o] = cx<T>(ld[arg].v, T(0));
+            if (S.leaf[arg].type == GSB_INTERPOLATED) {
+                // an image leaf enters with its complex value and no gradient entries of its own
+                ld[arg] = LeafD<T>{T(0), T(0), T(0), T(0), T(0)};
+                val[o] = ii_kvalue<T>(S.leaf[arg], dk, i, j);
+            } else {
+                ld[arg] = leaf_grad<T>(S.leaf[arg], S.sersic, A.dn, kx, ky, g, i - g.x0, j - g.y0);
+                val[o] = cx<T>(ld[arg].v, T(0));
+            }
         } else if (code == GSB_OP_MUL) {
             val[o] = cmul<T>(val[a], val[b]);
         } else if (code == GSB_OP_ADD) {
@@ -221,11 +227,11 @@ __device__ __forceinline__ void adjoint_point_factored(const gsb_template& tpl, 
                 val[a] = cx<T>(T(S.scale[S.atom_arg[a]]), T(0));
             } else if (o1 - o0 == 1) {
                 const int l = tpl.op_arg[o0];
-                if (want_leaf(want, l)) {
+                if (want_leaf(want, l) && S.leaf[l].type != GSB_INTERPOLATED) {
                     ld[a] = leaf_grad<T>(S.leaf[l], S.sersic, A.dn, kx, ky, g, i - g.x0, j - g.y0);
                     val[a] = cx<T>(ld[a].v, T(0));
                 } else {
-                    val[a] = cx<T>(leaf_fast<T>(S, cache, l, kx, ky, i, j, g), T(0));
+                    val[a] = leaf_cfast<T>(S, cache, l, kx, ky, i, j, g);
                 }
             } else {
                 val[a] = eval_range<T>(tpl, S, cache, dk, i, j, g, o0, o1);

@@ -72,7 +72,7 @@ int validate_template(const gsb_template* tpl)
     }
     if (depth != 1) return set_error(GSB_ERR_INVALID, "program must leave exactly one value");
     for (int l = 0; l < tpl->n_leaves; ++l)
-        if (tpl->leaf_type[l] < GSB_GAUSSIAN || tpl->leaf_type[l] > GSB_BOX)
+        if (tpl->leaf_type[l] < GSB_GAUSSIAN || tpl->leaf_type[l] > GSB_INTERPOLATED)
             return set_error(GSB_ERR_INVALID, "unknown leaf type");
     return GSB_OK;
 }
@@ -157,6 +157,11 @@ int gsb_tables_destroy(gsb_tables* t)
     cudaFree(t->d_dheader);
     cudaFree(t->d_dnode);
     cudaFree(t->d_dval);
+    cudaFree(t->d_images);
+    cudaFree(t->d_image_info);
+    cudaFree(t->d_k64);
+    cudaFree(t->d_k32);
+    cudaFree(t->d_krows);
     delete t;
     return GSB_OK;
 }

@@ -21,13 +21,13 @@
 
 #include "gsb_fft.cuh"
 #include "gsb_internal.cuh"
+#include "gsb_interp.cuh"
 #include "gsb_profiles.cuh"
 
 namespace gsb {
 
 
 constexpr int kWarps = 16;          // warps per CTA (fewer where their FFT scratch does not fit)
-constexpr int kThreads = kWarps * 32;
 
 struct StampSmem {
     LeafParams leaf[GSB_MAX_LEAVES];
@@ -150,7 +150,9 @@ __device__ __noinline__ Cx<T> eval_program(const gsb_template& tpl, const StampS
     for (int o = 0; o < tpl.n_ops; ++o) {
         const int code = tpl.op_code[o], arg = tpl.op_arg[o];
         if (code == GSB_OP_LEAF) {
-            stack[sp++] = cx<T>(leaf_kvalue<T>(S.leaf[arg], S.sersic, kx, ky, g, gi, gj), T(0));
+            stack[sp++] = S.leaf[arg].type == GSB_INTERPOLATED
+                              ? ii_kvalue<T>(S.leaf[arg], dk, i, j)
+                              : cx<T>(leaf_kvalue<T>(S.leaf[arg], S.sersic, kx, ky, g, gi, gj), T(0));
         } else if (code == GSB_OP_MUL) {
             --sp;
             stack[sp - 1] = cmul<T>(stack[sp - 1], stack[sp]);
@@ -438,6 +440,15 @@ __device__ __forceinline__ T leaf_fast(const StampSmem& S, const unsigned char* 
     return leaf_kvalue<T>(L, S.sersic, kx, ky, g, i - g.x0, j - g.y0);
 }
 
+// One leaf as a complex value: InterpolatedImage leaves are complex, the others real.
+template <typename T>
+__device__ __forceinline__ Cx<T> leaf_cfast(const StampSmem& S, const unsigned char* cache, int arg, T kx, T ky,
+                                            int i, int j, const GridRef& g)
+{
+    if (S.leaf[arg].type == GSB_INTERPOLATED) return ii_kvalue<T>(S.leaf[arg], g.dk, i, j);
+    return cx<T>(leaf_fast<T>(S, cache, arg, kx, ky, i, j, g), T(0));
+}
+
 // Evaluation of the ops [o0, o1) (a complete subtree, or the whole program) with the caches and
 // a 4-deep register stack (warp-uniform branches).
 template <typename T>
@@ -452,8 +463,7 @@ __device__ __forceinline__ Cx<T> eval_range(const gsb_template& tpl, const Stamp
     for (int o = o0; o < o1; ++o) {
         const int code = tpl.op_code[o], arg = tpl.op_arg[o];
         if (code == GSB_OP_LEAF) {
-            const T v = leaf_fast<T>(S, cache, arg, kx, ky, i, j, g);
-            const Cx<T> c = cx<T>(v, T(0));
+            const Cx<T> c = leaf_cfast<T>(S, cache, arg, kx, ky, i, j, g);
             if (sp == 0) s0 = c; else if (sp == 1) s1 = c; else if (sp == 2) s2 = c; else s3 = c;
             ++sp;
         } else if (code == GSB_OP_MUL || code == GSB_OP_ADD) {
@@ -509,8 +519,13 @@ __device__ __forceinline__ Cx<T> eval_factored(const gsb_template& tpl, const St
     Cx<T> c = cx<T>(T(1), T(0));
     for (int a = 0; a < S.n_atoms; ++a) {
         const int o0 = S.atom_o0[a], o1 = S.atom_o1[a];
-        if (o1 - o0 == 1) r *= leaf_fast<T>(S, cache, tpl.op_arg[o0], kx, ky, i, j, g);
-        else c = cmul<T>(c, eval_range<T>(tpl, S, cache, dk, i, j, g, o0, o1));
+        if (o1 - o0 == 1) {
+            const int l = tpl.op_arg[o0];
+            if (S.leaf[l].type == GSB_INTERPOLATED) c = cmul<T>(c, ii_kvalue<T>(S.leaf[l], dk, i, j));
+            else r *= leaf_fast<T>(S, cache, l, kx, ky, i, j, g);
+        } else {
+            c = cmul<T>(c, eval_range<T>(tpl, S, cache, dk, i, j, g, o0, o1));
+        }
     }
     const Cx<T>* XS = reinterpret_cast<const Cx<T>*>(cache + S.xy_cache);
     const Cx<T> xy = cmul<T>(XS[i], XS[hk + 1 + j + hk]);

@@ -130,6 +130,14 @@ struct OgataTables {
     long long nroot;
 };
 
+// One InterpolatedImage slot on the device: the caller's gsb_image_desc plus where its
+// k-image (N rows q = 0..N-1 of N/2 + 1 columns p = 0..N/2) and row scratch live.
+struct ImageSlot {
+    gsb_image_desc desc;
+    long long k_offset;      // element offset in d_k64 / d_k32
+    long long row_offset;    // element offset in d_krows (ny rows of N/2 + 1)
+};
+
 // Library state per device.
 struct DeviceState {
     bool ready = false;
@@ -165,4 +173,12 @@ struct gsb_tables {
     double4* d_dnode = nullptr;   // count * stride
     double* d_dval = nullptr;     // scratch: count * stride d/dn Hankel values
     size_t cap_dn_slots = 0, cap_dn_nodes = 0;
+    // InterpolatedImage slots (gsb_images_build)
+    int n_images = 0;
+    gsb::ImageSlot* d_images = nullptr;   // n_images slot headers
+    double* d_image_info = nullptr;       // n_images * 2: (R, maxk) in image units
+    double2* d_k64 = nullptr;             // half-plane k-images, FP64
+    float2* d_k32 = nullptr;              // the same, FP32
+    double2* d_krows = nullptr;           // scratch: row transforms
+    size_t cap_images = 0, cap_k = 0, cap_krows = 0;
 };

@@ -1,0 +1,182 @@
+// InterpolatedImage k-values on the device.
+//
+// An InterpolatedImage leaf is the k interpolant applied to the DFT samples K(p, q) of the
+// zero-padded image, times the x interpolant's Fourier transform:
+//   v(kx, ky) = flux * U(kx / 2 pi) U(ky / 2 pi) * sum_pq w(p - kx N / 2 pi) w(q - ky N / 2 pi) K(p, q)
+// (SBInterpolatedImage::kValue and both fillKImage forms, src/SBInterpolatedImage.cpp:385-448,
+// 767-1000), with K periodic in N and Hermitian (K(-p, -q) = conj K(p, q)), so only the half
+// plane p = 0..N/2 is stored (rows q = 0..N-1 of N/2 + 1 values).  Tap positions are formed in
+// FP64 even for FP32 draws: their fractions must stay exact at indices of several hundred.
+#pragma once
+
+#include "gsb_fft.cuh"
+#include "gsb_profiles.cuh"
+
+namespace gsb {
+
+// Real-space kernels (src/Interpolant.cpp:171-176 Nearest, 245-249 Linear, 284-290 Cubic,
+// 389-432 Quintic; the quintic of Bernstein & Gruen 2014, arXiv:1401.2636, in its form with
+// vanishing fourth derivative of the step response).
+template <typename T>
+__device__ __forceinline__ T interp_xval(int code, T x)
+{
+    x = fabs(x);
+    switch (code) {
+      case GSB_INTERP_NEAREST:
+        return x > T(0.5) ? T(0) : T(1);
+      case GSB_INTERP_LINEAR:
+        return x > T(1) ? T(0) : T(1) - x;
+      case GSB_INTERP_CUBIC:
+        if (x < T(1)) return T(1) + x * x * (T(1.5) * x - T(2.5));
+        if (x < T(2)) return T(-0.5) * (x - T(1)) * (x - T(2)) * (x - T(2));
+        return T(0);
+      case GSB_INTERP_QUINTIC:
+        if (x <= T(1)) return T(1) + x * x * x * (T(-95. / 12.) + x * (T(23. / 2.) + x * T(-55. / 12.)));
+        if (x <= T(2))
+            return (x - T(1)) * (x - T(2)) *
+                   (T(-23. / 4.) + x * (T(29. / 2.) + x * (T(-83. / 8.) + x * T(55. / 24.))));
+        if (x <= T(3))
+            return (x - T(2)) * (x - T(3)) * (x - T(3)) * (T(-9. / 4.) + x * (T(25. / 12.) + x * T(-11. / 24.)));
+        return T(0);
+    }
+    return T(0);
+}
+
+// Half-width of the kernel support in samples (Interpolant::xrange, include/galsim/Interpolant.h).
+__host__ __device__ inline double interp_xrange(int code)
+{
+    switch (code) {
+      case GSB_INTERP_NEAREST: return 0.5;
+      case GSB_INTERP_LINEAR: return 1.;
+      case GSB_INTERP_CUBIC: return 2.;
+      case GSB_INTERP_QUINTIC: return 3.;
+    }
+    return 0.;
+}
+
+// Fourier transforms of the kernels, u in cycles per sample (the closed forms of
+// src/Interpolant.cpp:176, 251-255, 292-302, 435-461, derived from the piecewise polynomials).
+template <typename T>
+__device__ __forceinline__ T interp_uval(int code, T u)
+{
+    if (code == GSB_INTERP_DELTA) return T(1);
+    const T s = sinc_ref<T>(u);
+    switch (code) {
+      case GSB_INTERP_NEAREST: return s;
+      case GSB_INTERP_LINEAR: return s * s;
+      case GSB_INTERP_CUBIC: {
+        const T c = cospi(u);
+        return s * s * s * (T(3) * s - T(2) * c);
+      }
+      case GSB_INTERP_QUINTIC: {
+        const T c = cospi(u);
+        const T ssq = s * s;
+        const T piusq = T(kPi * kPi) * u * u;
+        return s * ssq * ssq * (s * (T(55) - T(19) * piusq) + T(2) * c * (piusq - T(27)));
+      }
+    }
+    return T(0);
+}
+
+// Extent of the kernel's transform, beyond which |U| < kvalue_accuracy (Interpolant::urange:
+// include/galsim/Interpolant.h:237, 278, 347; src/Interpolant.cpp:364-368, 518-523).
+__host__ __device__ inline double interp_urange(int code, double kacc)
+{
+    switch (code) {
+      case GSB_INTERP_DELTA: return 1. / kacc;
+      case GSB_INTERP_NEAREST: return 1. / (kPi * kacc);
+      case GSB_INTERP_LINEAR: return sqrt(1. / kacc) / kPi;
+      case GSB_INTERP_CUBIC: return pow((3. * sqrt(3.) / 8.) / kacc, 1. / 3.) / kPi;
+      case GSB_INTERP_QUINTIC: return pow((25. * sqrt(5.) / 108.) / kacc, 1. / 3.) / kPi;
+    }
+    return 0.;
+}
+
+// K(p, q) of the half-plane k-image for any integers p, q.
+template <typename T>
+__device__ __forceinline__ Cx<T> kimage_at(const Cx<T>* K, int N, int pm, int qm)
+{
+    // pm, qm already reduced to 0..N-1
+    const int H = N / 2 + 1;
+    if (pm <= N / 2) return K[(size_t)qm * H + pm];
+    const Cx<T> v = K[(size_t)(qm == 0 ? 0 : N - qm) * H + (N - pm)];
+    return cx<T>(v.x, -v.y);
+}
+
+constexpr int kInterpMaxTaps = 8;   // 2 xrange + 1 for the widest kernel (quintic: 7)
+
+// Tap window of one axis: first tap p1, count n, and the kernel weights w[t] = xval(p1 + t - s).
+// `shortcut`: the separable fill's single tap at (near-)integer positions
+// (SBInterpolatedImage.cpp:829-834).
+template <typename T>
+__device__ __forceinline__ void interp_taps(int code, double s, bool shortcut, int& p1, int& n,
+                                            T (&w)[kInterpMaxTaps])
+{
+    constexpr double kSmall = 10. * 2.220446049250313e-16;
+    const double fl = floor(s + 0.01);
+    int p2;
+    if (shortcut && fabs(s - fl) < kSmall * (fabs(s) + 1.)) {
+        p1 = p2 = int(fl);
+    } else {
+        const double xr = interp_xrange(code);
+        p1 = int(ceil(s - xr));
+        p2 = int(floor(s + xr));
+    }
+    n = p2 - p1 + 1;
+    if (n > kInterpMaxTaps) n = kInterpMaxTaps;
+    // p - s = (p - p1) + (p1 - s): an integer plus a fraction, exact before the rounding to T
+    const T off = T(double(p1) - s);
+#pragma unroll
+    for (int t = 0; t < kInterpMaxTaps; ++t) w[t] = t < n ? interp_xval<T>(code, T(t) + off) : T(0);
+}
+
+// InterpolatedImage leaf at k index (i, j) of a grid with spacing dk.
+// d[0] = N / 2 pi (k to sample index), d[1] = maxk1 (x interpolant cut-off), d[2] / d[3] =
+// x / k interpolant codes, d[4] = N, d[6] / d[7] = FP64 / FP32 k-image addresses.
+template <typename T>
+__device__ __noinline__ Cx<T> ii_kvalue(const LeafParams& L, double dk, int i, int j)
+{
+    const double kx = i * dk, ky = j * dk;
+    const double kxp = L.jac[0] * kx + L.jac[2] * ky;
+    const double kyp = L.jac[1] * kx + L.jac[3] * ky;
+    const double maxk1 = L.d[1];
+    if (fabs(kxp) > maxk1 || fabs(kyp) > maxk1) return cx<T>(T(0), T(0));
+    const int N = int(L.d[4]);
+    const int xc = int(L.d[2]), kc = int(L.d[3]);
+    const bool sep = !(L.flags & GSB_LEAF_JAC_GENERAL);
+    const Cx<T>* K = reinterpret_cast<const Cx<T>*>(
+        __double_as_longlong(sizeof(T) == 8 ? L.d[6] : L.d[7]));
+    int p1, np, q1, nq;
+    T wx[kInterpMaxTaps], wy[kInterpMaxTaps];
+    interp_taps<T>(kc, kxp * L.d[0], sep, p1, np, wx);
+    interp_taps<T>(kc, kyp * L.d[0], sep, q1, nq, wy);
+    int pw0 = p1 % N;
+    if (pw0 < 0) pw0 += N;
+    int qw = q1 % N;
+    if (qw < 0) qw += N;
+    Cx<T> sum = cx<T>(T(0), T(0));
+#pragma unroll
+    for (int b = 0; b < kInterpMaxTaps; ++b) {
+        if (b < nq && wy[b] != T(0)) {
+            Cx<T> row = cx<T>(T(0), T(0));
+            int pw = pw0;
+#pragma unroll
+            for (int a = 0; a < kInterpMaxTaps; ++a) {
+                if (a < np) {
+                    const Cx<T> v = kimage_at<T>(K, N, pw, qw);
+                    row.x += wx[a] * v.x;
+                    row.y += wx[a] * v.y;
+                }
+                if (++pw == N) pw = 0;
+            }
+            sum.x += wy[b] * row.x;
+            sum.y += wy[b] * row.y;
+        }
+        if (++qw == N) qw = 0;
+    }
+    constexpr double kUscale = 1. / (2. * kPi);
+    const T f = T(L.flux) * interp_uval<T>(xc, T(kxp * kUscale)) * interp_uval<T>(xc, T(kyp * kUscale));
+    return cx<T>(f * sum.x, f * sum.y);
+}
+
+}  // namespace gsb

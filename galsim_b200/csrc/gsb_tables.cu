@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "gsb_internal.cuh"
+#include "gsb_interp.cuh"
 
 namespace gsb {
 
@@ -605,9 +606,17 @@ struct MoffatKV2 {
     }
 };
 
+struct ImageRefs {
+    const ImageSlot* slots;
+    const double* info;
+    const double2* k64;
+    const float2* k32;
+    int count;
+};
+
 __global__ void prepare_leaves_kernel(const __grid_constant__ gsb_template tpl, int n_stamps, gsb_gsparams gsp,
                                       gsb_leaf* leaves, const double* sersic_header,
-                                      double kolm_stepk, double* info, int* status_out)
+                                      double kolm_stepk, ImageRefs images, double* info, int* status_out)
 {
     const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (idx >= (long long)n_stamps * tpl.n_leaves) return;
@@ -718,6 +727,29 @@ __global__ void prepare_leaves_kernel(const __grid_constant__ gsb_template tpl, 
         L.d[1] = hgt / (2. * kPi);
         maxk = 2. / (gsp.maxk_threshold * fmin(w, hgt));
         stepk = kPi / fmax(w, hgt);
+        break;
+      }
+      case GSB_INTERPOLATED: {
+        // SBInterpolatedImage.cpp:97-152: kscale = (N/2) / pi maps k to the k-image's sample
+        // index, maxk1 = urange / uscale cuts where the x interpolant's transform is
+        // negligible.  stepk holds the flux radius R and maxk the scanned maxk (image units),
+        // which the host turns into the profile's world stepk / maxk.
+        const int slot = L.table;
+        const int xc = int(L.p[0]), kc = int(L.p[1]);
+        if (slot < 0 || slot >= images.count) { atomicOr(status_out, 16); break; }
+        if (xc < GSB_INTERP_DELTA || xc > GSB_INTERP_QUINTIC || kc < GSB_INTERP_NEAREST ||
+            kc > GSB_INTERP_QUINTIC) { atomicOr(status_out, 32); break; }
+        const ImageSlot& I = images.slots[slot];
+        const int N = I.desc.N;
+        L.d[0] = (N / 2) / kPi;
+        L.d[1] = interp_urange(xc, gsp.kvalue_accuracy) / (1. / (2. * kPi));
+        L.d[2] = xc;
+        L.d[3] = kc;
+        L.d[4] = N;
+        L.d[6] = __longlong_as_double((long long)(images.k64 + I.k_offset));
+        L.d[7] = __longlong_as_double((long long)(images.k32 + I.k_offset));
+        stepk = images.info[2 * slot];
+        maxk = images.info[2 * slot + 1];
         break;
       }
       default:
@@ -920,13 +952,18 @@ int prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gs
 {
     DeviceState* st = device_state();
     if (!st->ready) return set_error(GSB_ERR_INVALID, "gsb_init has not been called");
-    bool need_kolm = false, need_sersic = false;
+    bool need_kolm = false, need_sersic = false, need_images = false;
     for (int l = 0; l < tpl->n_leaves; ++l) {
         if (tpl->leaf_type[l] == GSB_KOLMOGOROV) need_kolm = true;
         if (tpl->leaf_type[l] == GSB_SERSIC) need_sersic = true;
+        if (tpl->leaf_type[l] == GSB_INTERPOLATED) need_images = true;
     }
     if (need_sersic && (!t || t->count == 0))
         return set_error(GSB_ERR_INVALID, "Sersic leaves need built FT tables");
+    if (need_images && (!t || t->n_images == 0))
+        return set_error(GSB_ERR_INVALID, "InterpolatedImage leaves need built image slots");
+    ImageRefs images{};
+    if (t) images = ImageRefs{t->d_images, t->d_image_info, t->d_k64, t->d_k32, t->n_images};
     double kolm = 0.;
     if (need_kolm) {
         const int rc = kolmogorov_stepk(gsp, stream, &kolm);
@@ -937,13 +974,16 @@ int prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gs
     const long long n = (long long)n_stamps * tpl->n_leaves;
     if (n > 0) {
         prepare_leaves_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(
-            *tpl, n_stamps, *gsp, d_leaves, t ? t->d_header : nullptr, kolm, d_info, d_status);
+            *tpl, n_stamps, *gsp, d_leaves, t ? t->d_header : nullptr, kolm, images, d_info, d_status);
         GSB_CUDA_CHECK(cudaGetLastError());
     }
     int h_status = 0;
     GSB_CUDA_CHECK(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
     GSB_CUDA_CHECK(cudaStreamSynchronize(stream));
     if (h_status & 8) return set_error(GSB_ERR_INVALID, "unknown leaf type");
+    if (h_status & 16) return set_error(GSB_ERR_INVALID, "InterpolatedImage leaf names no built image slot");
+    if (h_status & 32) return set_error(GSB_ERR_UNSUPPORTED, "interpolant not built (x: Delta, Nearest, "
+                                                             "Linear, Cubic, Quintic; k: the same but Delta)");
     if (h_status & 2) return set_error(GSB_ERR_NUMERIC, "Sersic radius root finding failed");
     if (h_status & 4) return set_error(GSB_ERR_NUMERIC, "Moffat maxk root finding failed");
     return GSB_OK;

@@ -31,6 +31,7 @@ class Builder(object):
         self.leaves = []
         self.phases = []
         self.scales = []
+        self.image_sources = {}   # InterpolatedImage leaf -> its _ImageSource list (1 or B)
 
     def _bcast(self, v):
         a = np.asarray(v, dtype=np.float64)
@@ -136,9 +137,21 @@ class Program(object):
             inv = inv.reshape(len(sersic), B)
             for k, l in enumerate(sersic):
                 leaves['table'][:, l] = inv[k]
+        self.image_order = []
+        image_leaves = [l for l in range(L) if self.bld.leaf_types[l] == _lib.INTERPOLATED]
+        if image_leaves:
+            slot_of = {}
+            for l in image_leaves:
+                slots = []
+                for src in self.bld.image_sources[l]:
+                    if id(src) not in slot_of:
+                        slot_of[id(src)] = len(self.image_order)
+                        self.image_order.append(src)
+                    slots.append(slot_of[id(src)])
+                leaves['table'][:, l] = np.broadcast_to(np.array(slots, dtype=np.int32), (B,))
         self.d_leaves = _lib.to_device(leaves)
         self.d_info = torch.empty(B * L * 2, dtype=torch.float64, device=_lib.Device.torch_device())
-        if self.sersic_n is None:
+        if self.sersic_n is None and not self.image_order:
             self.tables = None
         elif getattr(self, 'tables', None) is None:
             self.tables = _lib.TablePool.acquire()
@@ -149,8 +162,10 @@ class Program(object):
         stepk and maxk; copy stepk / maxk back for the host-side composition."""
         self.upload()
         B, L = self.B, self.L
-        if self.tables is not None:
+        if self.tables is not None and self.sersic_n is not None:
             self.tables.build_sersic(self.sersic_n, self.gsparams, with_dn=self.need_dn)
+        if self.image_order:
+            self._build_images()
         _lib.check(_lib.lib().gsb_prepare_leaves(
             ctypes.byref(self.tpl), B, ctypes.byref(self.gsp_c), _lib.ptr(self.d_leaves),
             self.tables.handle if self.tables else None, _lib.ptr(self.d_info), _lib.Device.stream()))
@@ -158,6 +173,23 @@ class Program(object):
         self.leaf_stepk = info[:, :, 0]
         self.leaf_maxk = info[:, :, 1]
         self._prepared = True
+
+    def _build_images(self):
+        """The k-images and size scans of the InterpolatedImage sources, on the GPU.  A table
+        set that already holds the same sources (kept alive by it) for the same GSParams is
+        not rebuilt."""
+        import torch
+        key = (tuple(id(src) for src in self.image_order), self.gsparams)
+        if getattr(self.tables, '_image_key', None) == key:
+            return
+        offsets = np.cumsum([0] + [src.region.size for src in self.image_order])
+        desc = np.array([src.desc(off) for src, off in zip(self.image_order, offsets[:-1])],
+                        dtype=_lib.IMAGE_DESC_DTYPE)
+        pix = np.concatenate([src.region.ravel() for src in self.image_order])
+        d_pix = torch.from_numpy(pix).to(_lib.Device.torch_device())
+        self.tables.build_images(desc, d_pix, self.gsparams)
+        self.tables._image_key = key
+        self.tables._image_sources = list(self.image_order)
 
     def prepare(self):
         if self._prepared:

@@ -45,7 +45,18 @@ enum {
     GSB_MOFFAT      = 3,   /* p = {beta, r0, trunc}                        */
     GSB_KOLMOGOROV  = 4,   /* p = {lam_over_r0}                            */
     GSB_AIRY        = 5,   /* p = {lam_over_diam, obscuration}             */
-    GSB_BOX         = 6    /* p = {width, height}                          */
+    GSB_BOX         = 6,   /* p = {width, height}                          */
+    GSB_INTERPOLATED = 7   /* p = {x interpolant, k interpolant, 0}; `table` names an image
+                              slot built by gsb_images_build (SBInterpolatedImage.cpp) */
+};
+
+/* Interpolant codes of GSB_INTERPOLATED leaves (galsim/interpolant.py, src/Interpolant.cpp). */
+enum {
+    GSB_INTERP_DELTA   = 0,   /* x interpolant only: uval = 1                            */
+    GSB_INTERP_NEAREST = 1,
+    GSB_INTERP_LINEAR  = 2,
+    GSB_INTERP_CUBIC   = 3,
+    GSB_INTERP_QUINTIC = 4
 };
 
 /* Program opcodes.  A program is evaluated per k-point on a small stack of complex values:
@@ -100,9 +111,11 @@ typedef struct gsb_leaf {
     double jac[4];     /* composed Jacobian [A, B, C, D] (row-major 2x2, transform.py:593) */
     double flux;
     double p[3];       /* profile parameters, see the type enum */
-    double d[8];       /* derived values, written by gsb_prepare_leaves */
+    double d[8];       /* derived values, written by gsb_prepare_leaves (GSB_INTERPOLATED:
+                          the slot's k-image device addresses are kept in d[6] and d[7], so
+                          the leaves must be prepared again after gsb_images_build) */
     int32_t flags;     /* GSB_LEAF_* */
-    int32_t table;     /* FT table slot (Sersic), set by the caller */
+    int32_t table;     /* FT table slot (Sersic) or image slot (GSB_INTERPOLATED), set by the caller */
 } gsb_leaf;
 
 /* One phase / flux factor of one stamp (stamp-major: phases[s * n_phases + i]). */
@@ -166,6 +179,46 @@ int gsb_sersic_tables_build_ex(gsb_tables* t, const double* h_n, const double* h
 
 /* Copy slot headers back (16 doubles per slot: see gsb_tables.cu) for inspection. */
 int gsb_sersic_tables_info(const gsb_tables* t, double* h_out, int count, void* stream);
+
+/* InterpolatedImage sources ------------------------------------------------------------ */
+/* One image of an InterpolatedImage, placed in its zero-padded N x N frame (the reference's
+ * _xim, interpolatedimage.py:590-629).  Frame coordinates X, Y run over -N/2 .. N/2-1 and the
+ * frame's (0, 0) is the profile origin (the image after setCenter(0, 0)). */
+typedef struct gsb_image_desc {
+    int32_t N;              /* padded size, even (Image.good_fft_size of pad_factor * size) */
+    int32_t nx, ny;         /* size of the nonzero region (the image, or the pad image around it) */
+    int32_t x0, y0;         /* frame coordinates of the region's first pixel */
+    int32_t bx0, bx1;       /* inclusive frame bounds of the image searched for the stepk   */
+    int32_t by0, by1;       /*   radius (CalculateSizeContainingFlux); must contain (0, 0)  */
+    int32_t x_interp;       /* GSB_INTERP_* of the x interpolant (sets the maxk scan limit)  */
+    int32_t flags;          /* GSB_IMAGE_STEPK / GSB_IMAGE_MAXK: which sizes to compute     */
+    int64_t pix_offset;     /* index of the region's first pixel in the packed pixel array
+                               (row-major, nx pixels per row, FP64) */
+    double flux;            /* flux of the nonzero region (SBInterpolatedImage::getFlux) */
+    double stepk_target;    /* (1 - folding_threshold) * image flux (interpolatedimage.py:657) */
+    double maxk_limit;      /* max_maxk of calculateMaxK in image units; 0 = the x
+                               interpolant's 2 pi urange (SBInterpolatedImage.cpp:135-151) */
+} gsb_image_desc;
+
+#define GSB_IMAGE_STEPK 1
+#define GSB_IMAGE_MAXK  2
+#define GSB_IMAGE_MAX_N 4096
+
+/* Build image slots 0..count-1 of t (replacing any earlier images; Sersic slots are kept):
+ * per image the half-plane DFT of its padded frame,
+ *     K(p, q) = sum_XY I(X, Y) exp(-2 pi i (p X + q Y) / N),  p = 0..N/2, q = 0..N-1,
+ * in FP64 and as an FP32 copy (checkK: rfft with shift_in / shift_out, src/Image.cpp:730-812);
+ * with GSB_IMAGE_STEPK the radius R = d + 1/2 of the smallest centred box holding
+ * stepk_target (CalculateSizeContainingFlux, SBInterpolatedImage.cpp:1084-1110); with
+ * GSB_IMAGE_MAXK maxk = (ix + 1) pi / (N / 2) for the last ring ix with |K|^2 above
+ * (maxk_threshold * flux)^2 (calculateMaxK, SBInterpolatedImage.cpp:1146-1213).  Both are in
+ * image units; gsb_prepare_leaves passes them on as a GSB_INTERPOLATED leaf's stepk (= R) and
+ * maxk.  d_pixels is device memory; N <= GSB_IMAGE_MAX_N. */
+int gsb_images_build(gsb_tables* t, int count, const gsb_image_desc* h_desc, const double* d_pixels,
+                     const gsb_gsparams* gsp, void* stream);
+
+/* Copy per image (R, maxk) back (2 doubles per image; 0 where not computed). */
+int gsb_images_info(const gsb_tables* t, double* h_out, int count, void* stream);
 
 /* Leaves -------------------------------------------------------------------------------- */
 /* Fill the derived values of every leaf and write its stepk and maxk (d_info[2*(s*L+l)]).

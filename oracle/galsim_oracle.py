@@ -877,6 +877,258 @@ def apply_phases(kimage, xmin, ymin, dk, jac, cx, cy, fs):
 
 
 # ---------------------------------------------------------------------------------------------
+# InterpolatedImage (interpolatedimage.py:303-685, src/SBInterpolatedImage.cpp,
+# src/Interpolant.cpp)
+# ---------------------------------------------------------------------------------------------
+def interp_xval(name, x):
+    """Real-space kernels: Nearest / Linear / Cubic / Quintic (Interpolant.cpp:171-432)."""
+    x = np.abs(np.asarray(x, dtype=float))
+    if name == 'nearest':
+        return np.where(x > 0.5, 0., 1.)
+    if name == 'linear':
+        return np.where(x > 1., 0., 1. - x)
+    if name == 'cubic':
+        return np.where(x < 1., 1. + x * x * (1.5 * x - 2.5),
+                        np.where(x < 2., -0.5 * (x - 1.) * (x - 2.) * (x - 2.), 0.))
+    if name == 'quintic':
+        a = 1. + x * x * x * (-95. / 12. + x * (23. / 2. + x * (-55. / 12.)))
+        b = (x - 1.) * (x - 2.) * (-23. / 4. + x * (29. / 2. + x * (-83. / 8. + x * (55. / 24.))))
+        c = (x - 2.) * (x - 3.) * (x - 3.) * (-9. / 4. + x * (25. / 12. + x * (-11. / 24.)))
+        return np.where(x <= 1., a, np.where(x <= 2., b, np.where(x <= 3., c, 0.)))
+    raise ValueError(name)
+
+
+def _sinc(u):
+    """math::sinc (src/math/Sinc.cpp:29-33)."""
+    u = np.asarray(u, dtype=float)
+    with np.errstate(invalid='ignore', divide='ignore'):
+        v = np.sin(PI * u) / (PI * u)
+    return np.where(np.abs(u) < 1.e-4, 1. - (PI * PI / 6.) * u * u, v)
+
+
+def interp_uval(name, u):
+    """Fourier transforms of the kernels (Interpolant.cpp:176, 251-255, 292-302, 435-461)."""
+    u = np.asarray(u, dtype=float)
+    if name == 'delta':
+        return np.ones_like(u)
+    s = _sinc(u)
+    if name == 'nearest':
+        return s
+    if name == 'linear':
+        return s * s
+    c = np.cos(PI * u)
+    if name == 'cubic':
+        return s * s * s * (3. * s - 2. * c)
+    if name == 'quintic':
+        ssq = s * s
+        piusq = (PI * u) ** 2
+        return s * ssq * ssq * (s * (55. - 19. * piusq) + 2. * c * (piusq - 27.))
+    raise ValueError(name)
+
+
+INTERP_XRANGE = {'delta': 0., 'nearest': 0.5, 'linear': 1., 'cubic': 2., 'quintic': 3.}
+
+
+def interp_urange(name, kacc):
+    """Interpolant::urange (include/galsim/Interpolant.h:237-428, Interpolant.cpp:364, 518)."""
+    return {'delta': lambda: 1. / kacc,
+            'nearest': lambda: 1. / (PI * kacc),
+            'linear': lambda: math.sqrt(1. / kacc) / PI,
+            'cubic': lambda: math.pow((3. * math.sqrt(3.) / 8.) / kacc, 1. / 3.) / PI,
+            'quintic': lambda: math.pow((25. * math.sqrt(5.) / 108.) / kacc, 1. / 3.) / PI}[name]()
+
+
+def interp_krange(name, kacc):
+    """Interpolant.krange (interpolant.py:264, 328, 462, 528, 597)."""
+    return {'delta': 2. * PI / kacc, 'nearest': 2. / kacc, 'linear': 2. / kacc ** 0.5,
+            'cubic': 1.7320508075688774 / kacc ** (1. / 3.),
+            'quintic': 1.6058208066649935 / kacc ** (1. / 3.)}[name]
+
+
+def size_containing_flux(im, x0, y0, target):
+    """CalculateSizeContainingFlux (SBInterpolatedImage.cpp:1084-1110) on an image array
+    whose pixel [0, 0] sits at centred coordinates (x0, y0)."""
+    ny, nx = im.shape
+    at = lambda x, y: im[y - y0, x - x0]
+    p = 1. if target > 0. else -1.
+    dmax = min((nx - 1) // 2, (ny - 1) // 2)
+    flux = at(0, 0)
+    d = 1
+    while d <= dmax:
+        for x in range(-d, d):
+            flux += at(x, -d)
+            flux += at(d, x)
+            flux += at(-x, d)
+            flux += at(-d, -x)
+        if p * flux >= p * target:
+            break
+        d += 1
+    return d + 0.5
+
+
+class OInterpolatedImageLeaf(OLeaf):
+    """SBInterpolatedImage in image units: the k interpolant over the padded image's DFT times
+    the x interpolant's transform (SBInterpolatedImage.cpp:385-448 kValue, 767-936 separable
+    fill with its integer shortcut, 938-1000 general fill)."""
+
+    def __init__(self, xim, x_interp='quintic', k_interp='quintic', gsp=DEFAULT):
+        N = xim.shape[0]
+        self.N = N
+        # K(p, q) = sum I(X, Y) exp(-2 pi i (p X + q Y) / N), X = column - N/2 (checkK / rfft)
+        self.K = np.fft.fft2(np.fft.ifftshift(xim))
+        self.xi, self.ki = x_interp, k_interp
+        self.xr = INTERP_XRANGE[k_interp]
+        self.kscale = (N // 2) / PI
+        self.uscale = 1. / (2. * PI)
+        self.maxk1 = interp_urange(x_interp, gsp.kvalue_accuracy) / self.uscale
+        self.gsp = gsp
+
+    def _taps(self, s, shortcut):
+        """Tap positions p[..., t] and weights w[..., t] for sample positions s."""
+        nt = int(2 * self.xr) + 1
+        p1 = np.ceil(s - self.xr)
+        t = np.arange(nt)
+        p = p1[..., None] + t
+        w = interp_xval(self.ki, p - s[..., None])
+        if shortcut:
+            small = 10. * np.finfo(float).eps
+            fl = np.floor(s + 0.01)
+            on = np.abs(s - fl) < small * (np.abs(s) + 1.)
+            p = np.where(on[..., None], fl[..., None] + t, p)
+            w1 = interp_xval(self.ki, fl - s)
+            w = np.where(on[..., None], np.where(t == 0, w1[..., None], 0.), w)
+        return p.astype(np.int64), w
+
+    def kv(self, KX, KY, shortcut):
+        KX = np.asarray(KX, float)
+        KY = np.asarray(KY, float)
+        px, wx = self._taps(KX * self.kscale, shortcut)
+        py, wy = self._taps(KY * self.kscale, shortcut)
+        N = self.N
+        vals = self.K[(py[..., :, None] % N), (px[..., None, :] % N)]
+        s = np.einsum('...ba,...a,...b->...', vals, wx, wy)
+        fac = interp_uval(self.xi, KX * self.uscale) * interp_uval(self.xi, KY * self.uscale)
+        out = fac * s
+        return np.where((np.abs(KX) > self.maxk1) | (np.abs(KY) > self.maxk1), 0., out)
+
+    def fill_1d(self, im, kx0, dkx, izero, ky0, dky, jzero):
+        n, m = im.shape
+        kx = kx0 + np.arange(m) * dkx
+        ky = ky0 + np.arange(n) * dky
+        KX, KY = np.meshgrid(kx, ky)
+        im[...] = self.kv(KX, KY, True)
+
+    def kv_2d(self, KX, KY, *grid):
+        return self.kv(KX, KY, False)
+
+    def kvalue(self, kx, ky):
+        return self.kv(kx, ky, True)
+
+    def max_k(self, flux, max_maxk=0.):
+        """calculateMaxK (SBInterpolatedImage.cpp:1146-1213), image units."""
+        N, No2 = self.N, self.N // 2
+        dk = PI / No2
+        thresh = (self.gsp.maxk_threshold * flux) ** 2
+        if max_maxk == 0.:
+            max_maxk = self.maxk1
+        max_ix = min(int(math.ceil(max_maxk / dk)), No2)
+        nrm = lambda p, q: abs(self.K[q % N, p % N]) ** 2
+        maxk_ix = 0.
+        below = 0
+        for ix in range(max_ix + 1):
+            for iy in range(ix + 1):
+                v = nrm(iy, -ix)
+                if v <= thresh and iy != ix and ix != No2:
+                    v = nrm(iy, ix)
+                if v <= thresh and iy > 0:
+                    v = nrm(ix, -iy)
+                if v <= thresh and ix > 0 and iy != No2:
+                    v = nrm(ix, iy)
+                if v > thresh:
+                    maxk_ix = ix
+                    below = 0
+                    break
+            below += 1
+            if below == 5:
+                break
+        return (maxk_ix + 1.) * dk
+
+
+class OInterpolatedImage(OObj):
+    """InterpolatedImage(image, scale=..., ...) (interpolatedimage.py:303-400, 481-500,
+    590-685): the padded frame, flux, stepk / maxk in world units, and the world profile
+    Transform(Shift(SBInterpolatedImage, -offset), scale, flux_ratio)."""
+
+    def __init__(self, array, scale, x_interp='quintic', k_interp='quintic', flux=None,
+                 normalization='flux', pad_factor=4., offset=(0., 0.), use_true_center=True,
+                 calculate_stepk=True, calculate_maxk=True, pad_image=None, force_stepk=0.,
+                 force_maxk=0., gsp=DEFAULT):
+        arr = np.asarray(array, dtype=float)
+        ny, nx = arr.shape
+        # setCenter(0, 0): pixel [0, 0] at (-(nx // 2), -(ny // 2))
+        x0, y0 = -(nx // 2), -(ny // 2)
+        dx, dy = float(offset[0]), float(offset[1])
+        if use_true_center:
+            if nx % 2 == 0:
+                dx -= 0.5
+            if ny % 2 == 0:
+                dy -= 0.5
+        pad = max(nx, ny)
+        if pad_factor > 1.:
+            pad = int(math.ceil(pad_factor * pad))
+        if pad_image is not None:
+            pad = max(pad, *np.shape(pad_image))
+        N = good_fft_size(pad)
+        xim = np.zeros((N, N))
+        nz = np.zeros((N, N), dtype=bool)
+        if pad_image is not None:
+            pim = np.asarray(pad_image, dtype=float)
+            pny, pnx = pim.shape
+            px0, py0 = -(pnx // 2), -(pny // 2)
+            xim[py0 + N // 2:py0 + N // 2 + pny, px0 + N // 2:px0 + N // 2 + pnx] = pim
+            nz[py0 + N // 2:py0 + N // 2 + pny, px0 + N // 2:px0 + N // 2 + pnx] = True
+        xim[y0 + N // 2:y0 + N // 2 + ny, x0 + N // 2:x0 + N // 2 + nx] = arr
+        nz[y0 + N // 2:y0 + N // 2 + ny, x0 + N // 2:x0 + N // 2 + nx] = True
+        self.N = N
+        self.leaf = OInterpolatedImageLeaf(xim, x_interp, k_interp, gsp)
+        image_flux = float(np.sum(arr, dtype=np.float64))
+        # getFlux of the nonzero image: the bounding box of image and pad image
+        rows, cols = np.nonzero(nz)
+        nz_flux = float(np.sum(xim[rows.min():rows.max() + 1, cols.min():cols.max() + 1]))
+        if flux is None:
+            flux = image_flux * (scale * scale if normalization.lower() in ('sb', 'surface brightness')
+                                 else 1.)
+        self.flux = flux
+        if force_stepk > 0.:
+            self.stepk = force_stepk
+        else:
+            if calculate_stepk:
+                R = size_containing_flux(arr, x0, y0, (1. - gsp.folding_threshold) * image_flux)
+            else:
+                R = max(nx, ny) / 2. - 0.5
+            self.stepk = PI / (math.hypot(R, INTERP_XRANGE[x_interp]) * scale)
+        if force_maxk > 0.:
+            self.maxk = force_maxk
+        elif calculate_maxk:
+            mm = 0. if calculate_maxk is True else float(calculate_maxk)
+            self.maxk = self.leaf.max_k(nz_flux, mm) / scale
+        else:
+            self.maxk = interp_krange(x_interp, gsp.kvalue_accuracy) / scale
+        prof = self.leaf
+        if dx != 0. or dy != 0.:
+            prof = OTransform(prof, offset=(-dx, -dy))
+        fr = flux / image_flux if flux != image_flux else 1.
+        jac = None if scale == 1. else [[scale, 0.], [0., scale]]
+        self.inner = OTransform(prof, jac=jac, flux_ratio=(1. / scale) ** 2 * fr)
+
+    def stepk_maxk(self):
+        return self.stepk, self.maxk
+
+    def drawK(self, kimage, xmin, ymin, dk, jac):
+        self.inner.drawK(kimage, xmin, ymin, dk, jac)
+
+
+# ---------------------------------------------------------------------------------------------
 # Image-level steps
 # ---------------------------------------------------------------------------------------------
 def good_fft_size(n):

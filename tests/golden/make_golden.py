@@ -52,7 +52,93 @@ def profile(galsim, spec):
         return galsim.Convolve([profile(galsim, s) for s in spec[1]])
     if kind == 'sum':
         return galsim.Add([profile(galsim, s) for s in spec[1]])
+    if kind == 'ii':
+        # ('ii', image name, scale, keyword arguments); pad_image given by image name
+        kw = dict(spec[3])
+        if 'pad_image' in kw:
+            kw['pad_image'] = galsim.Image(IMAGES[kw['pad_image']])
+        return galsim.InterpolatedImage(galsim.Image(IMAGES[spec[1]], scale=spec[2]), **kw)
     raise ValueError(kind)
+
+
+# ---- InterpolatedImage sources ---------------------------------------------------------------
+# Seeded synthetic images: sums of elliptical Gaussians sampled at pixel centres plus a little
+# Gaussian noise (a PSF-like and a galaxy-like shape, odd and even sizes), and a low-level
+# noise field used as a pad image.  The arrays are stored in the fixture; the tests use them
+# from there.
+IMAGES = {}
+
+
+def _blob(nx, ny, comps, noise, seed):
+    rng = np.random.default_rng(seed)
+    y, x = np.mgrid[0:ny, 0:nx].astype(float)
+    x -= (nx - 1) / 2.
+    y -= (ny - 1) / 2.
+    im = np.zeros((ny, nx))
+    for amp, cx, cy, sxx, syy, sxy in comps:
+        dx, dy = x - cx, y - cy
+        det = sxx * syy - sxy * sxy
+        q = (syy * dx * dx - 2 * sxy * dx * dy + sxx * dy * dy) / det
+        im += amp * np.exp(-0.5 * q)
+    return im + noise * rng.standard_normal((ny, nx))
+
+
+def source_images():
+    IMAGES['psf32'] = _blob(32, 32, [(1., 0.2, -0.1, 3.0, 2.4, 0.5), (0.08, 0.5, 0.3, 12., 10., -2.)],
+                            2e-4, 11)
+    IMAGES['psf31x33'] = _blob(31, 33, [(1., -0.3, 0.4, 2.2, 3.1, -0.6), (0.05, 0., 0., 9., 14., 1.)],
+                               1e-4, 12)
+    IMAGES['gal24'] = _blob(24, 24, [(2., 1.0, -0.5, 6.0, 3.0, 1.5), (1., -2.0, 1.5, 2.0, 2.5, 0.)],
+                            5e-3, 13)
+    IMAGES['pad40'] = 1e-3 * np.random.default_rng(14).standard_normal((40, 40))
+    return IMAGES
+
+
+II_PSF = ('ii', 'psf32', 0.2, {})
+INTERP_DRAW_CASES = [
+    # (name, spec, nx, ny, scale, dtype, offset)
+    ('ii_conv_exp', ('conv', [('shear', 0.2, 0.1, ('exp', 0.5, 2.)), II_PSF]), 48, 48, 0.2, 'f8', (0., 0.)),
+    ('ii_alone_cubic_linear_offset', ('ii', 'psf31x33', 0.25, {'x_interpolant': 'cubic',
+                                                                'k_interpolant': 'linear',
+                                                                'offset': (0.3, -0.2)}),
+     40, 40, 0.25, 'f8', (0.1, 0.05)),
+    ('ii_general_jac_sersic', ('conv', [('sersic', 1.5, 0.4, 1e3),
+                                        ('rotate', 25., ('shear', 0.1, 0.2, ('ii', 'psf32', 0.2,
+                                                                             {'flux': 5.})))]),
+     48, 48, 0.2, 'f4', (0., 0.)),
+    ('ii_sb_rescaled', ('ii', 'gal24', 0.3, {'normalization': 'sb'}), 64, 64, 0.15, 'f8', (0., 0.)),
+    ('ii_pad2_nocalc', ('conv', [('ii', 'gal24', 0.2, {'pad_factor': 2., 'calculate_stepk': False,
+                                                        'calculate_maxk': False}),
+                                 ('moffat', 3.0, 0.6, 1.)]), 40, 40, 0.2, 'f8', (0., 0.)),
+    ('ii_forced', ('conv', [('exp', 0.4, 1.), ('ii', 'psf32', 0.2, {'_force_stepk': 0.8,
+                                                                    '_force_maxk': 12.})]),
+     48, 48, 0.2, 'f8', (0., 0.)),
+    ('ii_nearest_quintic', ('conv', [('gauss', 0.3, 1.), ('ii', 'psf31x33', 0.2,
+                                                          {'x_interpolant': 'nearest'})]),
+     32, 32, 0.2, 'f8', (0., 0.)),
+    ('ii_linear_pad_image', ('conv', [('gauss', 0.25, 1.), ('ii', 'psf32', 0.2,
+                                                            {'x_interpolant': 'linear',
+                                                             'k_interpolant': 'linear',
+                                                             'pad_image': 'pad40'})]),
+     40, 40, 0.2, 'f8', (0., 0.)),
+    ('ii_delta_x', ('ii', 'gal24', 0.2, {'x_interpolant': 'delta'}), 32, 32, 0.2, 'f8', (0., 0.)),
+    ('ii_two_images', ('conv', [('sum', [('ii', 'gal24', 0.2, {'flux': 40.}), ('exp', 0.6, 20.)]),
+                                II_PSF]), 48, 48, 0.2, 'f4', (0., 0.)),
+    ('ii_calc_floats', ('conv', [('exp', 0.3, 1.), ('ii', 'psf32', 0.2, {'calculate_maxk': 3.0,
+                                                                         'calculate_stepk': 0.5})]),
+     48, 48, 0.2, 'f8', (0., 0.)),
+    ('ii_shift_dilate', ('shift', 0.3, -0.15, ('dilate', 1.4, ('ii', 'psf31x33', 0.2, {}))),
+     40, 40, 0.2, 'f8', (0., 0.)),
+]
+
+INTERP_KIMAGE_CASES = [
+    ('k_ii', ('ii', 'psf31x33', 0.25, {}), 0.3, 21),
+    ('k_ii_shear', ('shear', 0.15, -0.1, ('ii', 'psf32', 0.2, {'x_interpolant': 'cubic'})), 0.35, 21),
+]
+
+INTERP_SIZE_CASES = [c[1] for c in INTERP_DRAW_CASES if c[1][0] == 'ii'] + [
+    II_PSF, ('ii', 'psf32', 0.2, {'k_interpolant': 'cubic', 'x_interpolant': 'linear'}),
+    ('ii', 'gal24', 0.5, {'pad_factor': 6.}), ('ii', 'psf31x33', 0.1, {'use_true_center': False})]
 
 
 # ---- cases ------------------------------------------------------------------------------
@@ -212,6 +298,36 @@ def main_config(ref_root):
     print('wrote', os.path.join(HERE, 'reference_config.npz'))
 
 
+def main_interp(ref_root):
+    from ref_import import import_reference_galsim
+    galsim = import_reference_galsim(ref_root)
+    source_images()
+    out = {'img_' + k: v for k, v in IMAGES.items()}
+    for name, spec, nx, ny, scale, dt, off in INTERP_DRAW_CASES:
+        obj = profile(galsim, spec)
+        im = obj.drawImage(nx=nx, ny=ny, scale=scale, dtype=np.dtype(dt).type, method='fft',
+                           offset=off)
+        out['draw_' + name] = im.array
+        out['draw_' + name + '_flux'] = np.array(im.added_flux)
+    for name, spec, dk, n in INTERP_KIMAGE_CASES:
+        im = profile(galsim, spec).drawKImage(nx=n, ny=n, scale=dk)
+        out['kimg_' + name] = im.array
+        out['kimg_' + name + '_xmin'] = np.array([im.bounds.xmin, im.bounds.ymin])
+    out['sizes'] = np.array([(profile(galsim, sp).stepk, profile(galsim, sp).maxk)
+                             for sp in INTERP_SIZE_CASES])
+    # k values of the image-unit SBInterpolatedImage at scattered points (kValue, with the
+    # integer-position shortcut of the separable fill at integer sample positions)
+    rng = np.random.default_rng(99)
+    kpts = np.concatenate([rng.uniform(-3., 3., (40, 2)), np.array([[0., 0.], [0.5, -1.25]])])
+    ii = profile(galsim, ('ii', 'psf31x33', 0.25, {}))
+    ii._sbp
+    out['kvalue_pts'] = kpts
+    out['kvalue_ii_psf31x33'] = np.array([ii._sbii.kValue(galsim._galsim.PositionD(a, b))
+                                          for a, b in kpts])
+    np.savez_compressed(os.path.join(HERE, 'reference_interp.npz'), **out)
+    print('wrote', os.path.join(HERE, 'reference_interp.npz'), len(out), 'arrays')
+
+
 def main(ref_root):
     from ref_import import import_reference_galsim
     galsim = import_reference_galsim(ref_root)
@@ -263,6 +379,8 @@ if __name__ == '__main__':
     root = args[0] if args else '/root/reference'
     if '--grad-only' in sys.argv:
         main_grad(root)
+    elif '--interp-only' in sys.argv:
+        main_interp(root)
     elif '--config-only' in sys.argv:
         main_config(root)
     else:
@@ -271,3 +389,4 @@ if __name__ == '__main__':
         main_large(root)
         main_grad(root)
         main_config(root)
+        main_interp(root)

@@ -44,7 +44,25 @@ def oracle_profile(spec):
         return O.OConvolve(*[oracle_profile(s) for s in spec[1]])
     if kind == 'sum':
         return O.OSum(*[oracle_profile(s) for s in spec[1]])
+    if kind == 'ii':
+        from make_golden import IMAGES
+        kw = dict(spec[3])
+        names = {'x_interpolant': 'x_interp', 'k_interpolant': 'k_interp',
+                 '_force_stepk': 'force_stepk', '_force_maxk': 'force_maxk'}
+        kw = {names.get(k, k): v for k, v in kw.items()}
+        if 'pad_image' in kw:
+            kw['pad_image'] = IMAGES[kw['pad_image']]
+        return O.OInterpolatedImage(IMAGES[spec[1]], spec[2], **kw)
     raise ValueError(kind)
+
+
+def load_interp_images(npz):
+    """Register the InterpolatedImage source images stored in a fixture for the 'ii' specs."""
+    import make_golden
+    for k in npz.files:
+        if k.startswith('img_'):
+            make_golden.IMAGES[k[4:]] = npz[k]
+    return make_golden.IMAGES
 
 
 def product_profile(galsim, spec):
