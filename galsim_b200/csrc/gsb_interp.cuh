@@ -174,8 +174,11 @@ __device__ __noinline__ Cx<T> ii_kvalue(const LeafParams& L, double dk, int i, i
         }
         if (++qw == N) qw = 0;
     }
+    // The transform factor is evaluated in FP64 for every precision: the quintic's
+    // s (55 - 19 pi^2 u^2) + 2 c (pi^2 u^2 - 27) is 55 s - 54 c + O(u^2) near u = 0, which
+    // would amplify FP32 rounding of s and c 55-fold (a 3e-6 flux bias).
     constexpr double kUscale = 1. / (2. * kPi);
-    const T f = T(L.flux) * interp_uval<T>(xc, T(kxp * kUscale)) * interp_uval<T>(xc, T(kyp * kUscale));
+    const T f = T(L.flux * interp_uval<double>(xc, kxp * kUscale) * interp_uval<double>(xc, kyp * kUscale));
     return cx<T>(f * sum.x, f * sum.y);
 }
 

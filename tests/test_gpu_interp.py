@@ -106,9 +106,9 @@ def test_interp_gradients_with_image_psf_fp64_vs_finite_differences():
     model = autodiff.GalaxyModel(psf, 40, 40, 0.2, dtype=np.float64, precision='fp64')
     p0 = np.array([[2e3, 0.6, 1.8, 0.08, -0.05, 0.04, -0.03],
                    [5e3, 0.4, 2.7, -0.1, 0.12, -0.06, 0.02]])
-    w = torch.as_tensor(np.random.default_rng(5).standard_normal((2, 40, 40)),
-                        device=galsim._lib.Device.torch_device())
-    p = torch.tensor(p0, dtype=torch.float64, requires_grad=True)
+    dev = galsim._lib.Device.torch_device()
+    w = torch.as_tensor(np.random.default_rng(5).standard_normal((2, 40, 40)), device=dev)
+    p = torch.as_tensor(p0, device=dev, dtype=torch.float64).requires_grad_(True)
     loss = (model(p) * w).sum()
     loss.backward()
     g = p.grad.cpu().numpy()
@@ -120,7 +120,7 @@ def test_interp_gradients_with_image_psf_fp64_vs_finite_differences():
                 q = p0.copy()
                 q[s, j] += sgn * h
                 with torch.no_grad():
-                    vals.append(float((model(torch.tensor(q)) * w).sum()))
+                    vals.append(float((model(torch.as_tensor(q, device=dev)) * w).sum()))
             fd = (vals[0] - vals[1]) / (2. * h)
             scale = np.abs(g[s]).max()
             assert abs(g[s, j] - fd) <= 1e-5 * max(abs(fd), 1e-2 * scale), (s, j, g[s, j], fd)
