@@ -19,6 +19,11 @@ chi^2 against a noisy target (SNR 50) and its gradient in the seven parameters t
 adjoint kernels (galsim_b200.autodiff), timed from host parameters to host gradients.
 Both carry the plain one-stamp-per-call rate of the same path beside them.
 
+`interp_psf` is the InterpolatedImage workload: the same 4096 galaxies convolved with one
+image PSF (a 32 x 32 effective-PSF image, quintic interpolants) drawn with
+method='no_pixel': device step, draw stage, k-image build, e2e and the reference's C++ on
+the host cores for the same stamps.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
 import argparse
@@ -202,6 +207,97 @@ def run_mixed(galsim, dev, steps, warmup):
             'forward_adjoint_unit': 'grad-evals/s', 'stamps': MIX_B,
             'workload': 'bulge_disk_moffat_gen_pixel_16384_seed2468 (Sersic n=4 + Exponential, Moffat beta U[2.5,4.5])',
             'gsparams': 'minimum_fft_size=32', 'fft_sizes': dict(zip(map(int, u), map(int, c)))}
+
+
+INTERP_PSF_SIZE = 32
+
+
+def interp_psf_image(galsim):
+    """The PSF image of the image-PSF workload: Kolmogorov(fwhm=0.7") x Pixel(0.2") drawn by this
+    library into 32 x 32 float64 pixels (an effective PSF image, as a PSF model would give)."""
+    return galsim.Kolmogorov(fwhm=0.7).drawImage(nx=INTERP_PSF_SIZE, ny=INTERP_PSF_SIZE, scale=SCALE,
+                                                 dtype=np.float64).array.copy()
+
+
+def interp_object(galsim, params, psf):
+    n, hlr, flux, g1, g2 = [np.ascontiguousarray(params[:, i]) for i in range(5)]
+    gal = galsim.Sersic(n=n, half_light_radius=hlr, flux=flux).shear(g1=g1, g2=g2)
+    return galsim.Convolve(gal, psf)
+
+
+def run_interp(galsim, dev, params, steps, warmup, cpu=True):
+    """Image-PSF workload: the 4096 galaxies of the main workload (Sersic, sheared) convolved
+    with one InterpolatedImage PSF (the 32 x 32 effective-PSF image, quintic interpolants,
+    pad_factor 4 -> a 128 x 128 k-image), drawn with method='no_pixel' at automatic sizes.
+    Reports the device-timed step, the draw graph alone, the k-image build (1 and 256
+    images), e2e through draw_batch, and the reference C++ on the host cores."""
+    import torch
+    arr = interp_psf_image(galsim)
+    psf = galsim.InterpolatedImage(galsim.Image(arr, scale=SCALE))
+    plan = galsim.plan_batch(interp_object(galsim, params, psf), scale=SCALE, dtype=np.float32,
+                             method='no_pixel')
+    for _ in range(warmup):
+        st = galsim.run_batch(plan)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        st = galsim.run_batch(plan)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    B = plan.prog.B
+    gs = getattr(plan.prog, '_graph_state', None)
+    k_ms = None
+    if gs is not None and gs.get('graph') is not None:
+        reps = max(steps, 10)
+        e0.record()
+        for _ in range(reps):
+            gs['graph'].replay()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        k_ms = e0.elapsed_time(e1) / reps
+    # e2e: host parameters -> objects -> draw_batch -> host pixels (one PSF object, reused)
+    es, ee = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    es.record()
+    for _ in range(steps):
+        sb = galsim.draw_batch(interp_object(galsim, params, psf), scale=SCALE, dtype=np.float32,
+                               method='no_pixel')
+        pix = sb.host(copy=False)
+        flux = sb.added_flux
+    ee.record()
+    torch.cuda.synchronize(dev)
+    e2e_ms = es.elapsed_time(ee) / steps
+    # k-image build: one 32 x 32 source, and 256 distinct ones
+    from galsim_b200.program import Program
+    build = {}
+    for nimg in (1, 256):
+        imgs = [galsim.Image(arr * (1. + 1e-3 * i), scale=SCALE) for i in range(nimg)]
+        iib = galsim.InterpolatedImage(imgs if nimg > 1 else imgs[0])
+        pr = Program(galsim.Convolve(galsim.Gaussian(sigma=np.full(nimg, 0.5)), iib))
+        pr.upload()
+        pr._build_images()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(5):
+            pr.tables._image_key = None
+            pr._build_images()
+        torch.cuda.synchronize(dev)
+        build['%d_images_ms' % nimg] = (time.perf_counter() - t0) / 5 * 1e3
+    u, c = np.unique(st.N, return_counts=True)
+    out = {'value': B / (ms * 1e-3), 'unit': 'stamps/s', 'stamps': B, 'ms_per_step': ms,
+           'draw_graph_ms': k_ms,
+           'e2e': {'value': B / (e2e_ms * 1e-3), 'unit': 'stamps/s'},
+           'k_image_build': build,
+           'workload': 'sersic_4096_seed1234 x InterpolatedImage(32x32 Kolmogorov(0.7) x Pixel(0.2) '
+                       'image, quintic), method=no_pixel',
+           'fft_sizes': dict(zip(map(int, u), map(int, c)))}
+    if cpu:
+        ref = cpu_interp_rate(params, arr)
+        if ref is not None:
+            out['cpu_baseline'] = ref
+    return out
 
 
 def run_large(galsim, dev):
@@ -393,6 +489,47 @@ def cpu_reference_rate(params, budget_s=20., max_stamps=None):
                       'per core, reference C++ with an FP64 shim in place of FFTW)' % n}
 
 
+def _ref_interp_worker(args):
+    rows, psf = args
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import galsim_oracle as O
+    import ref_draw as R
+    ii = R.RInterpolatedImage(psf, SCALE)
+    out = []
+    for p in rows:
+        n, hlr, flux, g1, g2 = p[:5]
+        prof = O.OConvolve(R.RSersic(n, hlr, flux).shear(g1, g2), ii)
+        t = time.perf_counter()
+        R.draw_image(prof, None, None, SCALE, pixel=False)
+        out.append(time.perf_counter() - t)
+    return out
+
+
+def cpu_interp_rate(params, psf, budget_s=8.):
+    """stamps/s of the reference's C++ path for the image-PSF workload on all host cores, over
+    a bounded leading sample (one InterpolatedImage per process, as a reference user keeps
+    one PSF object)."""
+    import multiprocessing as mp
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import ref_draw as R
+    if not R.available():
+        return None
+    cores = os.cpu_count() or 1
+    per = _ref_interp_worker((params[:3], psf))
+    est = max(np.mean(per[1:]), 1e-3)
+    n = int(min(len(params), max(cores, budget_s * cores / est)))
+    sample = params[:n]
+    chunks = [(sample[i::cores], psf) for i in range(cores)]
+    ctx = mp.get_context('spawn')
+    with ctx.Pool(cores) as pool:
+        t = time.perf_counter()
+        pool.map(_ref_interp_worker, chunks)
+        wall = time.perf_counter() - t
+    return {'value': n / wall, 'unit': 'stamps/s', 'cores': cores, 'kind': 'reference',
+            'sample': '%d leading stamps of the 4096-stamp image-PSF batch (reference C++ '
+                      'SBInterpolatedImage and SBSersic, one process per core)' % n}
+
+
 def run_reference(args):
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
@@ -418,7 +555,8 @@ def run_reference(args):
 # GPU arm
 # ---------------------------------------------------------------------------------------------
 def run_stage(args):
-    """Small single-stage runs for profiling (--stage draw | tables): no e2e / CPU legs."""
+    """Small single-stage runs for profiling (--stage draw | tables | fit | interp): no e2e /
+    CPU legs."""
     import torch
     import galsim_b200 as galsim
     from galsim_b200 import _lib
@@ -460,7 +598,12 @@ def run_stage(args):
         torch.cuda.synchronize()
         print(json.dumps({'stage': 'tables', 'tables': len(n), 'ms_per_build': e0.elapsed_time(e1) / args.steps}))
         return
-    plan = galsim.plan_batch(obj, nx=args.nx, ny=args.nx, scale=SCALE, dtype=np.float32)
+    if args.stage == 'interp':
+        psf = galsim.InterpolatedImage(galsim.Image(interp_psf_image(galsim), scale=SCALE))
+        plan = galsim.plan_batch(interp_object(galsim, params, psf), nx=args.nx, ny=args.nx, scale=SCALE,
+                                 dtype=np.float32, method='no_pixel')
+    else:
+        plan = galsim.plan_batch(obj, nx=args.nx, ny=args.nx, scale=SCALE, dtype=np.float32)
     for _ in range(args.warmup):
         st = galsim.run_batch(plan)
     torch.cuda.synchronize()
@@ -470,7 +613,7 @@ def run_stage(args):
     e1.record()
     torch.cuda.synchronize()
     u, c = np.unique(st.N, return_counts=True)
-    print(json.dumps({'stage': 'draw', 'stamps': len(st), 'ms_per_step': e0.elapsed_time(e1) / args.steps,
+    print(json.dumps({'stage': args.stage, 'stamps': len(st), 'ms_per_step': e0.elapsed_time(e1) / args.steps,
                       'buckets': dict(zip(map(int, u), map(int, c)))}))
 
 
@@ -592,6 +735,9 @@ def run_gpu(args):
     fit = run_fit_step(args, galsim, dev, max(args.steps, 3), max(args.warmup, 2))
     mixed = run_mixed(galsim, dev, max(args.steps, 3), max(args.warmup, 2)) if not args.no_extra else None
     large = run_large(galsim, dev) if not args.no_extra else None
+    interp = (run_interp(galsim, dev, params, max(args.steps, 3), max(args.warmup, 2),
+                         cpu=(rank == 0 and world == 1 and not args.no_cpu))
+              if not args.no_extra else None)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -626,6 +772,7 @@ def run_gpu(args):
             'grad_evals': fit,
             'mixed_batch': mixed,
             'large_stamps': large,
+            'interp_psf': interp,
             'clocks': clk.summary(),
         }
         if cpu is not None:
@@ -646,8 +793,8 @@ def main():
                     help='skip the mixed-batch and large-stamp measurements')
     ap.add_argument('--stamps', type=int, default=B_DEFAULT, help='stamps per GPU (leading subset)')
     ap.add_argument('--nx', type=int, default=None, help='fixed stamp size (default: automatic)')
-    ap.add_argument('--stage', default='all', choices=['all', 'draw', 'tables', 'fit'],
-                    help="'draw' / 'tables' / 'fit': run only that stage (for profiling)")
+    ap.add_argument('--stage', default='all', choices=['all', 'draw', 'tables', 'fit', 'interp'],
+                    help="'draw' / 'tables' / 'fit' / 'interp': run only that stage (for profiling)")
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)

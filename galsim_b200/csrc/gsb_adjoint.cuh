@@ -83,7 +83,7 @@ __device__ inline void program_children(const gsb_template& tpl, int* c1, int* c
 
 // Reverse-mode pass of the ops [o0, o1) (a complete subtree, or the whole program) at k index
 // (i, j) with output cotangent u (contribution Re(u * dF)); gradients are added into acc.
-template <typename T>
+template <typename T, bool II = true>
 __device__ __noinline__ void adjoint_range(const gsb_template& tpl, const AdjSmem& A, double dk, int i,
                                            int j, const GridRef& g, Cx<T> u, T* acc, int o0, int o1)
 {
@@ -98,7 +98,7 @@ __device__ __noinline__ void adjoint_range(const gsb_template& tpl, const AdjSme
         const int code = tpl.op_code[o], arg = tpl.op_arg[o];
         const int a = A.child1[o], b = A.child2[o];
         if (code == GSB_OP_LEAF) {
-            if (S.leaf[arg].type == GSB_INTERPOLATED) {
+            if (II && S.leaf[arg].type == GSB_INTERPOLATED) {
                 // an image leaf enters with its complex value and no gradient entries of its own
                 ld[arg] = LeafD<T>{T(0), T(0), T(0), T(0), T(0)};
                 val[o] = ii_kvalue<T>(S.leaf[arg], dk, i, j);
@@ -194,7 +194,7 @@ __device__ __noinline__ void sum_atom_grads(const gsb_template& tpl, const AdjSm
 // Factored reverse pass at (i, j): F = prod_a atom_a * XS[i] YS[j]; the cotangent of atom a
 // is u XS YS prod_{b != a} atom_b (prefix and suffix products, no division).  Leaf, phase and
 // scale atoms accumulate into ga[a][*] (registers); subtree atoms run adjoint_range into acc.
-template <typename T>
+template <typename T, bool II = true>
 __device__ __forceinline__ void adjoint_point_factored(const gsb_template& tpl, const AdjSmem& A,
                                                        const unsigned char* cache, unsigned want, double dk,
                                                        int i, int j, const GridRef& g, Cx<T> u,
@@ -227,14 +227,14 @@ __device__ __forceinline__ void adjoint_point_factored(const gsb_template& tpl, 
                 val[a] = cx<T>(T(S.scale[S.atom_arg[a]]), T(0));
             } else if (o1 - o0 == 1) {
                 const int l = tpl.op_arg[o0];
-                if (want_leaf(want, l) && S.leaf[l].type != GSB_INTERPOLATED) {
+                if (want_leaf(want, l) && !(II && S.leaf[l].type == GSB_INTERPOLATED)) {
                     ld[a] = leaf_grad<T>(S.leaf[l], S.sersic, A.dn, kx, ky, g, i - g.x0, j - g.y0);
                     val[a] = cx<T>(ld[a].v, T(0));
                 } else {
-                    val[a] = leaf_cfast<T>(S, cache, l, kx, ky, i, j, g);
+                    val[a] = leaf_cfast<T, II>(S, cache, l, kx, ky, i, j, g);
                 }
             } else {
-                val[a] = eval_range<T>(tpl, S, cache, dk, i, j, g, o0, o1);
+                val[a] = eval_range<T, II>(tpl, S, cache, dk, i, j, g, o0, o1);
             }
         }
         pre[a] = run;
@@ -274,7 +274,7 @@ __device__ __forceinline__ void adjoint_point_factored(const gsb_template& tpl, 
             } else if (kind == kAtomSum) {
                 sum_atom_grads<T>(tpl, A, want, kx, ky, i, j, g, w, acc, o0, o1);
             } else {
-                adjoint_range<T>(tpl, A, dk, i, j, g, w, acc, o0, o1);
+                adjoint_range<T, II>(tpl, A, dk, i, j, g, w, acc, o0, o1);
             }
             suf = cmul<T>(suf, val[a]);
         }
@@ -296,7 +296,7 @@ __host__ __device__ constexpr int adj_warps()
             kSmemLimit) ? kWarps : kWarps / 2;
 }
 
-template <typename T, int N, bool WSMEM>
+template <typename T, int N, bool WSMEM, bool II>
 __global__ void __launch_bounds__(adj_warps<T, N>() * 32) adjoint_fused_kernel(const __grid_constant__ AdjArgs a)
 {
     constexpr int NW = adj_warps<T, N>();
@@ -345,9 +345,9 @@ __global__ void __launch_bounds__(adj_warps<T, N>() * 32) adjoint_fused_kernel(c
         const int Nk = G.Nk;
         const int hk = Nk / 2;
         const GridRef g{dk, 0, -hk, hk + 1, Nk + 1};
-        if (threadIdx.x == 0) plan_caches<T>(S, a.tpl, Nk, a.want);
+        if (threadIdx.x == 0) plan_caches<T, II>(S, a.tpl, Nk, a.want);
         __syncthreads();
-        fill_caches<T>(S, a.tpl, cache, dk, Nk);
+        fill_caches<T, II>(S, a.tpl, cache, dk, Nk);
         __syncthreads();
         const bool factored = S.xy_cache >= 0 && S.n_atoms <= kAdjAtoms;
         bool subtree = !factored;
@@ -408,10 +408,10 @@ __global__ void __launch_bounds__(adj_warps<T, N>() * 32) adjoint_fused_kernel(c
                         const bool pos = kx >= 0;
                         // an alias taken as conj(F(-k)) contributes Re(Ghat conj(dF)) = Re(conj(Ghat) dF)
                         if (factored)
-                            adjoint_point_factored<T>(a.tpl, A, cache, a.want, dk, pos ? kx : -kx,
+                            adjoint_point_factored<T, II>(a.tpl, A, cache, a.want, dk, pos ? kx : -kx,
                                                       pos ? ky : -ky, g, pos ? gh : cconj<T>(gh), ga, acc);
                         else
-                            adjoint_range<T>(a.tpl, A, dk, pos ? kx : -kx, pos ? ky : -ky, g,
+                            adjoint_range<T, II>(a.tpl, A, dk, pos ? kx : -kx, pos ? ky : -ky, g,
                                              pos ? gh : cconj<T>(gh), acc, 0, a.tpl.n_ops);
                     }
                 }
@@ -511,9 +511,16 @@ int launch_adjoint(const AdjArgs& args, size_t work_bytes, cudaStream_t stream)
     const int grid = adj_grid<T, N>(args.n_stamps);
     if (!wsmem && (args.work == nullptr || work_bytes < adj_workspace_bytes_for<T, N>(args.n_stamps)))
         return set_error(GSB_ERR_INVALID, "adjoint workspace too small");
-    GSB_CUDA_CHECK(cudaFuncSetAttribute(adjoint_fused_kernel<T, N, wsmem>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-    adjoint_fused_kernel<T, N, wsmem><<<grid, adj_warps<T, N>() * 32, sm, stream>>>(args);
+    // programs without image leaves run the instance compiled without their code
+    if (has_image_leaves(args.tpl)) {
+        GSB_CUDA_CHECK(cudaFuncSetAttribute(adjoint_fused_kernel<T, N, wsmem, true>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+        adjoint_fused_kernel<T, N, wsmem, true><<<grid, adj_warps<T, N>() * 32, sm, stream>>>(args);
+    } else {
+        GSB_CUDA_CHECK(cudaFuncSetAttribute(adjoint_fused_kernel<T, N, wsmem, false>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+        adjoint_fused_kernel<T, N, wsmem, false><<<grid, adj_warps<T, N>() * 32, sm, stream>>>(args);
+    }
     GSB_CUDA_CHECK(cudaGetLastError());
     return GSB_OK;
 }

@@ -43,6 +43,7 @@ struct StampSmem {
     int leaf_cache[GSB_MAX_LEAVES];
     int phase_cache[GSB_MAX_PHASES];
     int sersic_cache[GSB_MAX_LEAVES];
+    int ii_cache[GSB_MAX_LEAVES];      // InterpolatedImage taps per column / row (IITaps)
     int regstack;      // the program fits the 4-deep register stack
     // Factored form of the program (see plan_factored): the root is a product of atoms; the
     // separable atoms (diagonal Box / Gaussian leaves, phases, scales) are folded into
@@ -139,7 +140,8 @@ __device__ inline void load_stamp(StampSmem& S, const gsb_template& tpl, int s, 
 }
 
 // Evaluate the program at k index (i, j) (kx = i dk, ky = j dk) of grid g.
-template <typename T>
+// II: the program may hold InterpolatedImage leaves (their code is compiled in only then).
+template <typename T, bool II = true>
 __device__ __noinline__ Cx<T> eval_program(const gsb_template& tpl, const StampSmem& S, double dk, int i, int j,
                               const GridRef& g)
 {
@@ -150,9 +152,10 @@ __device__ __noinline__ Cx<T> eval_program(const gsb_template& tpl, const StampS
     for (int o = 0; o < tpl.n_ops; ++o) {
         const int code = tpl.op_code[o], arg = tpl.op_arg[o];
         if (code == GSB_OP_LEAF) {
-            stack[sp++] = S.leaf[arg].type == GSB_INTERPOLATED
-                              ? ii_kvalue<T>(S.leaf[arg], dk, i, j)
-                              : cx<T>(leaf_kvalue<T>(S.leaf[arg], S.sersic, kx, ky, g, gi, gj), T(0));
+            if (II && S.leaf[arg].type == GSB_INTERPOLATED)
+                stack[sp++] = ii_kvalue<T>(S.leaf[arg], dk, i, j);
+            else
+                stack[sp++] = cx<T>(leaf_kvalue<T>(S.leaf[arg], S.sersic, kx, ky, g, gi, gj), T(0));
         } else if (code == GSB_OP_MUL) {
             --sp;
             stack[sp - 1] = cmul<T>(stack[sp - 1], stack[sp]);
@@ -264,7 +267,7 @@ __device__ inline bool plan_factored(StampSmem& S, const gsb_template& tpl, unsi
     return true;
 }
 
-template <typename T>
+template <typename T, bool II = true>
 __device__ inline void plan_caches(StampSmem& S, const gsb_template& tpl, int Nk, unsigned want = 0u,
                                    int budget = kCacheBytes)
 {
@@ -298,6 +301,16 @@ __device__ inline void plan_caches(StampSmem& S, const gsb_template& tpl, int Nk
             if (used + bytes <= budget) { S.sersic_cache[l] = used; used += bytes; }
         }
     }
+    // InterpolatedImage leaves with a diagonal Jacobian: the taps, weights and transform
+    // factor of every column and row (the reference's separable fill caches the same per
+    // column, SBInterpolatedImage.cpp:820-866)
+    for (int l = 0; l < tpl.n_leaves; ++l) {
+        S.ii_cache[l] = -1;
+        const LeafParams& L = S.leaf[l];
+        if (!II || L.type != GSB_INTERPOLATED || (L.flags & GSB_LEAF_JAC_GENERAL)) continue;
+        const int bytes = ((hk + 1 + Nk + 1) * (int)sizeof(IITaps<T>) + 15) & ~15;
+        if (used + bytes <= budget) { S.ii_cache[l] = used; used += bytes; }
+    }
     for (int p = 0; p < tpl.n_phases; ++p) {
         S.phase_cache[p] = -1;
         if (S.phase_sep[p]) continue;
@@ -314,12 +327,23 @@ __device__ inline void plan_caches(StampSmem& S, const gsb_template& tpl, int Nk
 }
 
 // Fill the planned caches (whole block).
-template <typename T>
+template <typename T, bool II = true>
 __device__ inline void fill_caches(const StampSmem& S, const gsb_template& tpl, unsigned char* cache,
                                    double dk, int Nk)
 {
     const int hk = Nk / 2;
     for (int l = 0; l < tpl.n_leaves; ++l) {
+        if (II && S.ii_cache[l] >= 0) {
+            const LeafParams& L = S.leaf[l];
+            IITaps<T>* E = reinterpret_cast<IITaps<T>*>(cache + S.ii_cache[l]);
+            for (int t = threadIdx.x; t < hk + 1 + Nk + 1; t += blockDim.x) {
+                const bool isx = t <= hk;
+                const int idx = isx ? t : t - (hk + 1) - hk;
+                // k' as ii_kvalue forms it for a diagonal Jacobian (the zero terms are exact)
+                const double kp = isx ? L.jac[0] * (idx * dk) : L.jac[3] * (idx * dk);
+                ii_axis_taps<T>(L, kp, true, isx, E[t]);
+            }
+        }
         if (S.sersic_cache[l] >= 0) {
             typename NodeT<T>::type* dst = reinterpret_cast<typename NodeT<T>::type*>(cache + S.sersic_cache[l]);
             const double4* src = S.sersic[l].node;
@@ -441,17 +465,24 @@ __device__ __forceinline__ T leaf_fast(const StampSmem& S, const unsigned char* 
 }
 
 // One leaf as a complex value: InterpolatedImage leaves are complex, the others real.
-template <typename T>
+template <typename T, bool II = true>
 __device__ __forceinline__ Cx<T> leaf_cfast(const StampSmem& S, const unsigned char* cache, int arg, T kx, T ky,
                                             int i, int j, const GridRef& g)
 {
-    if (S.leaf[arg].type == GSB_INTERPOLATED) return ii_kvalue<T>(S.leaf[arg], g.dk, i, j);
+    if (II && S.leaf[arg].type == GSB_INTERPOLATED) {
+        if (S.ii_cache[arg] >= 0) {
+            const IITaps<T>* E = reinterpret_cast<const IITaps<T>*>(cache + S.ii_cache[arg]);
+            const int hk = g.n / 2;
+            return ii_sum<T>(S.leaf[arg], E[i], E[hk + 1 + j + hk]);
+        }
+        return ii_kvalue<T>(S.leaf[arg], g.dk, i, j);
+    }
     return cx<T>(leaf_fast<T>(S, cache, arg, kx, ky, i, j, g), T(0));
 }
 
 // Evaluation of the ops [o0, o1) (a complete subtree, or the whole program) with the caches and
 // a 4-deep register stack (warp-uniform branches).
-template <typename T>
+template <typename T, bool II = true>
 __device__ __forceinline__ Cx<T> eval_range(const gsb_template& tpl, const StampSmem& S,
                                             const unsigned char* cache, double dk, int i, int j,
                                             const GridRef& g, int o0, int o1)
@@ -463,7 +494,7 @@ __device__ __forceinline__ Cx<T> eval_range(const gsb_template& tpl, const Stamp
     for (int o = o0; o < o1; ++o) {
         const int code = tpl.op_code[o], arg = tpl.op_arg[o];
         if (code == GSB_OP_LEAF) {
-            const Cx<T> c = leaf_cfast<T>(S, cache, arg, kx, ky, i, j, g);
+            const Cx<T> c = leaf_cfast<T, II>(S, cache, arg, kx, ky, i, j, g);
             if (sp == 0) s0 = c; else if (sp == 1) s1 = c; else if (sp == 2) s2 = c; else s3 = c;
             ++sp;
         } else if (code == GSB_OP_MUL || code == GSB_OP_ADD) {
@@ -498,17 +529,17 @@ __device__ __forceinline__ Cx<T> eval_range(const gsb_template& tpl, const Stamp
     return s0;
 }
 
-template <typename T>
+template <typename T, bool II = true>
 __device__ __forceinline__ Cx<T> eval_fast(const gsb_template& tpl, const StampSmem& S,
                                            const unsigned char* cache, double dk, int i, int j,
                                            const GridRef& g)
 {
-    return eval_range<T>(tpl, S, cache, dk, i, j, g, 0, tpl.n_ops);
+    return eval_range<T, II>(tpl, S, cache, dk, i, j, g, 0, tpl.n_ops);
 }
 
 // The factored program at (i, j): product of the per-point atoms (real leaves, complex
 // subtrees) times the folded separable factors XS[i] YS[j + hk].
-template <typename T>
+template <typename T, bool II = true>
 __device__ __forceinline__ Cx<T> eval_factored(const gsb_template& tpl, const StampSmem& S,
                                                const unsigned char* cache, double dk, int i, int j,
                                                const GridRef& g)
@@ -521,10 +552,10 @@ __device__ __forceinline__ Cx<T> eval_factored(const gsb_template& tpl, const St
         const int o0 = S.atom_o0[a], o1 = S.atom_o1[a];
         if (o1 - o0 == 1) {
             const int l = tpl.op_arg[o0];
-            if (S.leaf[l].type == GSB_INTERPOLATED) c = cmul<T>(c, ii_kvalue<T>(S.leaf[l], dk, i, j));
+            if (II && S.leaf[l].type == GSB_INTERPOLATED) c = cmul<T>(c, leaf_cfast<T, II>(S, cache, l, kx, ky, i, j, g));
             else r *= leaf_fast<T>(S, cache, l, kx, ky, i, j, g);
         } else {
-            c = cmul<T>(c, eval_range<T>(tpl, S, cache, dk, i, j, g, o0, o1));
+            c = cmul<T>(c, eval_range<T, II>(tpl, S, cache, dk, i, j, g, o0, o1));
         }
     }
     const Cx<T>* XS = reinterpret_cast<const Cx<T>*>(cache + S.xy_cache);
@@ -556,8 +587,34 @@ __device__ inline void store_pixel(void* out, int dtype, int add, long long idx,
     }
 }
 
-template <typename T, int N, bool WSMEM>
-__global__ void __launch_bounds__(fused_warps<T, N>() * 32) draw_fused_kernel(const __grid_constant__ DrawArgs a)
+template <typename T, int N>
+constexpr size_t smem_bytes(bool wsmem)
+{
+    size_t off = (sizeof(StampSmem) + 15) & ~size_t(15);
+    off += sizeof(Cx<T>) * N * (1 + fused_warps<T, N>());
+    if (wsmem) off += sizeof(Cx<T>) * (N / 2 + 1) * (N + 1);
+    return ((off + 15) & ~size_t(15)) + kCacheBytes;
+}
+
+template <typename T, int N>
+constexpr bool w_fits_smem()
+{
+    return smem_bytes<T, N>(true) <= kSmemLimit;
+}
+
+// Resident CTAs per SM that the shared memory allows (at most 2): the register budget is
+// capped to match, so that code used only by some programs (the FP64 transform of image
+// leaves, the general-Jacobian paths) cannot halve the occupancy of every other program.
+constexpr size_t kSmemPerSM = 228 * 1024;
+
+template <typename T, int N>
+__host__ __device__ constexpr int fused_min_blocks()
+{
+    return kSmemPerSM / (smem_bytes<T, N>(w_fits_smem<T, N>()) + 1024) >= 2 ? 2 : 1;
+}
+
+template <typename T, int N, bool WSMEM, bool II = true>
+__global__ void __launch_bounds__(fused_warps<T, N>() * 32, fused_min_blocks<T, N>()) draw_fused_kernel(const __grid_constant__ DrawArgs a)
 {
     constexpr int NW = fused_warps<T, N>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -588,9 +645,9 @@ __global__ void __launch_bounds__(fused_warps<T, N>() * 32) draw_fused_kernel(co
         const int Nk = S.geom.Nk;
         const int hk = Nk / 2;
         const GridRef g{dk, 0, -hk, hk + 1, Nk + 1};
-        if (threadIdx.x == 0) plan_caches<T>(S, a.tpl, Nk);
+        if (threadIdx.x == 0) plan_caches<T, II>(S, a.tpl, Nk);
         __syncthreads();
-        fill_caches<T>(S, a.tpl, cache, dk, Nk);
+        fill_caches<T, II>(S, a.tpl, cache, dk, Nk);
         __syncthreads();
         const bool fast = S.regstack;
         const bool factored = S.xy_cache >= 0;
@@ -609,9 +666,9 @@ __global__ void __launch_bounds__(fused_warps<T, N>() * 32) draw_fused_kernel(co
                         const int ky = kyc + ib * N;
                         const bool pos = kx >= 0;
                         const int ii = pos ? kx : -kx, jj = pos ? ky : -ky;
-                        Cx<T> v = factored ? eval_factored<T>(a.tpl, S, cache, dk, ii, jj, g)
-                                  : fast ? eval_fast<T>(a.tpl, S, cache, dk, ii, jj, g)
-                                         : eval_program<T>(a.tpl, S, dk, ii, jj, g);
+                        Cx<T> v = factored ? eval_factored<T, II>(a.tpl, S, cache, dk, ii, jj, g)
+                                  : fast ? eval_fast<T, II>(a.tpl, S, cache, dk, ii, jj, g)
+                                         : eval_program<T, II>(a.tpl, S, dk, ii, jj, g);
                         if (!pos) v = cconj<T>(v);
                         kahan_add<T>(acc, comp, v);
                     }
@@ -710,19 +767,11 @@ __global__ void draw_kimage_kernel(const __grid_constant__ gsb_template tpl, int
     }
 }
 
-template <typename T, int N>
-constexpr size_t smem_bytes(bool wsmem)
+inline bool has_image_leaves(const gsb_template& tpl)
 {
-    size_t off = (sizeof(StampSmem) + 15) & ~size_t(15);
-    off += sizeof(Cx<T>) * N * (1 + fused_warps<T, N>());
-    if (wsmem) off += sizeof(Cx<T>) * (N / 2 + 1) * (N + 1);
-    return ((off + 15) & ~size_t(15)) + kCacheBytes;
-}
-
-template <typename T, int N>
-constexpr bool w_fits_smem()
-{
-    return smem_bytes<T, N>(true) <= kSmemLimit;
+    for (int l = 0; l < tpl.n_leaves; ++l)
+        if (tpl.leaf_type[l] == GSB_INTERPOLATED) return true;
+    return false;
 }
 
 template <typename T, int N>
@@ -750,9 +799,16 @@ int launch_fused(const DrawArgs& args, size_t work_bytes, cudaStream_t stream)
     const int grid = draw_grid<T, N>(args.n_stamps);
     if (!wsmem && (args.work == nullptr || work_bytes < workspace_bytes_for<T, N>(args.n_stamps)))
         return set_error(GSB_ERR_INVALID, "draw workspace too small");
-    GSB_CUDA_CHECK(cudaFuncSetAttribute(draw_fused_kernel<T, N, wsmem>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-    draw_fused_kernel<T, N, wsmem><<<grid, fused_warps<T, N>() * 32, sm, stream>>>(args);
+    // programs without image leaves run the instance compiled without their code
+    if (has_image_leaves(args.tpl)) {
+        GSB_CUDA_CHECK(cudaFuncSetAttribute(draw_fused_kernel<T, N, wsmem, true>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+        draw_fused_kernel<T, N, wsmem, true><<<grid, fused_warps<T, N>() * 32, sm, stream>>>(args);
+    } else {
+        GSB_CUDA_CHECK(cudaFuncSetAttribute(draw_fused_kernel<T, N, wsmem, false>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+        draw_fused_kernel<T, N, wsmem, false><<<grid, fused_warps<T, N>() * 32, sm, stream>>>(args);
+    }
     GSB_CUDA_CHECK(cudaGetLastError());
     return GSB_OK;
 }

@@ -70,7 +70,7 @@ struct LargeArgs {
     int cache_bytes;     // shared memory for the per-stamp caches (factored program)
 };
 
-template <typename T, int THREADS>
+template <typename T, int THREADS, bool II>
 __global__ void __launch_bounds__(THREADS) large_col_kernel(const __grid_constant__ LargeArgs la)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -86,9 +86,9 @@ __global__ void __launch_bounds__(THREADS) large_col_kernel(const __grid_constan
     __syncthreads();
     const int Nk = S.geom.Nk, hk = Nk / 2;
     const GridRef g{dk, 0, -hk, hk + 1, Nk + 1};
-    if (threadIdx.x == 0) plan_caches<T>(S, a.tpl, Nk, 0u, la.cache_bytes);
+    if (threadIdx.x == 0) plan_caches<T, II>(S, a.tpl, Nk, 0u, la.cache_bytes);
     __syncthreads();
-    fill_caches<T>(S, a.tpl, cache, dk, Nk);
+    fill_caches<T, II>(S, a.tpl, cache, dk, Nk);
     __syncthreads();
     const bool factored = S.xy_cache >= 0, fast = S.regstack;
     Cx<T>* W = reinterpret_cast<Cx<T>*>(la.W) + (size_t)s * H * N;
@@ -104,9 +104,9 @@ __global__ void __launch_bounds__(THREADS) large_col_kernel(const __grid_constan
                     const int ky = kyc + ib * N;
                     const bool pos = kx >= 0;
                     const int ii = pos ? kx : -kx, jj = pos ? ky : -ky;
-                    const Cx<T> v = factored ? eval_factored<T>(a.tpl, S, cache, dk, ii, jj, g)
-                                    : fast ? eval_fast<T>(a.tpl, S, cache, dk, ii, jj, g)
-                                           : eval_program<T>(a.tpl, S, dk, ii, jj, g);
+                    const Cx<T> v = factored ? eval_factored<T, II>(a.tpl, S, cache, dk, ii, jj, g)
+                                    : fast ? eval_fast<T, II>(a.tpl, S, cache, dk, ii, jj, g)
+                                           : eval_program<T, II>(a.tpl, S, dk, ii, jj, g);
                     kahan_add<T>(acc, comp, pos ? v : cconj<T>(v));
                 }
             }
@@ -237,7 +237,14 @@ int launch_large_t(const DrawArgs& args, int N, void* work, size_t work_bytes, c
     const double2* tw = nullptr;
     int rc = twiddles(N, stream, &tw);
     if (rc) return rc;
-    GSB_CUDA_CHECK(cudaFuncSetAttribute(large_col_kernel<T, THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    // programs without image leaves run the column kernel compiled without their code
+    const bool ii = has_image_leaves(args.tpl);
+    if (ii)
+        GSB_CUDA_CHECK(cudaFuncSetAttribute(large_col_kernel<T, THREADS, true>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    else
+        GSB_CUDA_CHECK(cudaFuncSetAttribute(large_col_kernel<T, THREADS, false>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
     GSB_CUDA_CHECK(cudaFuncSetAttribute(large_row_kernel<T, THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(base)));
     const int chunk = int(std::max<size_t>(1, std::min<size_t>(work_bytes / slab, 65535)));
     DeviceState* st = device_state();
@@ -259,7 +266,8 @@ int launch_large_t(const DrawArgs& args, int N, void* work, size_t work_bytes, c
         la.cache_bytes = cache_bytes;
         const int cols = N / 2 + 1;
         const int gx = std::max(1, std::min(cols, (2 * st->sm_count + n - 1) / n));
-        large_col_kernel<T, THREADS><<<dim3(gx, n), THREADS, sm, stream>>>(la);
+        if (ii) large_col_kernel<T, THREADS, true><<<dim3(gx, n), THREADS, sm, stream>>>(la);
+        else large_col_kernel<T, THREADS, false><<<dim3(gx, n), THREADS, sm, stream>>>(la);
         GSB_CUDA_CHECK(cudaGetLastError());
         const int gr = std::max(1, std::min(N / 2, (2 * st->sm_count + n - 1) / n));
         large_row_kernel<T, THREADS><<<dim3(gr, n), THREADS, base, stream>>>(la);

@@ -105,33 +105,85 @@ __device__ __forceinline__ Cx<T> kimage_at(const Cx<T>* K, int N, int pm, int qm
 
 constexpr int kInterpMaxTaps = 8;   // 2 xrange + 1 for the widest kernel (quintic: 7)
 
-// Tap window of one axis: first tap p1, count n, and the kernel weights w[t] = xval(p1 + t - s).
-// `shortcut`: the separable fill's single tap at (near-)integer positions
-// (SBInterpolatedImage.cpp:829-834).
+// The taps of one axis at one k: first sample index (already reduced mod N), count, and the
+// kernel weights w[t] = xval(p1 + t - s), with the x interpolant's transform (and, for the
+// x axis, the leaf flux) folded in.
 template <typename T>
-__device__ __forceinline__ void interp_taps(int code, double s, bool shortcut, int& p1, int& n,
-                                            T (&w)[kInterpMaxTaps])
+struct IITaps {
+    int p0;
+    int n;
+    T w[kInterpMaxTaps];
+};
+
+// Taps of the axis with k' = kp: s = kp N / 2 pi.  `shortcut`: the separable fill's single tap
+// at (near-)integer positions (SBInterpolatedImage.cpp:829-834).  Outside the x interpolant's
+// support (|k'| > maxk1, SBInterpolatedImage.cpp:394 and 786-789) there are no taps.  The
+// transform factor is evaluated in FP64 for every precision: the quintic's
+// s (55 - 19 pi^2 u^2) + 2 c (pi^2 u^2 - 27) is 55 s - 54 c + O(u^2) near u = 0, which would
+// amplify FP32 rounding of s and c 55-fold (a 3e-6 flux bias).
+template <typename T>
+__device__ __noinline__ void ii_axis_taps(const LeafParams& L, double kp, bool shortcut, bool with_flux,
+                                             IITaps<T>& e)
 {
+    e.n = 0;
+    e.p0 = 0;
+    if (fabs(kp) > L.d[1]) return;
+    const int N = int(L.d[4]);
+    const int kc = int(L.d[3]), xc = int(L.d[2]);
+    const double s = kp * L.d[0];
     constexpr double kSmall = 10. * 2.220446049250313e-16;
     const double fl = floor(s + 0.01);
-    int p2;
+    int p1, p2;
     if (shortcut && fabs(s - fl) < kSmall * (fabs(s) + 1.)) {
         p1 = p2 = int(fl);
     } else {
-        const double xr = interp_xrange(code);
+        const double xr = interp_xrange(kc);
         p1 = int(ceil(s - xr));
         p2 = int(floor(s + xr));
     }
-    n = p2 - p1 + 1;
-    if (n > kInterpMaxTaps) n = kInterpMaxTaps;
+    int n = p2 - p1 + 1;
+    n = n < 0 ? 0 : (n > kInterpMaxTaps ? kInterpMaxTaps : n);
+    constexpr double kUscale = 1. / (2. * kPi);
+    const double u = interp_uval<double>(xc, kp * kUscale) * (with_flux ? L.flux : 1.);
     // p - s = (p - p1) + (p1 - s): an integer plus a fraction, exact before the rounding to T
     const T off = T(double(p1) - s);
 #pragma unroll
-    for (int t = 0; t < kInterpMaxTaps; ++t) w[t] = t < n ? interp_xval<T>(code, T(t) + off) : T(0);
+    for (int t = 0; t < kInterpMaxTaps; ++t) e.w[t] = t < n ? T(u * double(interp_xval<T>(kc, T(t) + off))) : T(0);
+    int pw = p1 % N;
+    e.p0 = pw < 0 ? pw + N : pw;
+    e.n = n;
+}
+
+// sum_ab wy_b wx_a K(p0x + a, p0y + b) over the taps of both axes.
+template <typename T>
+__device__ __noinline__ Cx<T> ii_sum(const LeafParams& L, const IITaps<T>& ex, const IITaps<T>& ey)
+{
+    const int N = int(L.d[4]);
+    const Cx<T>* K = reinterpret_cast<const Cx<T>*>(
+        __double_as_longlong(sizeof(T) == 8 ? L.d[6] : L.d[7]));
+    Cx<T> sum = cx<T>(T(0), T(0));
+    int qw = ey.p0;
+    for (int b = 0; b < ey.n; ++b) {
+        const T wy = ey.w[b];
+        if (wy != T(0)) {
+            Cx<T> row = cx<T>(T(0), T(0));
+            int pw = ex.p0;
+            for (int a = 0; a < ex.n; ++a) {
+                const Cx<T> v = kimage_at<T>(K, N, pw, qw);
+                row.x += ex.w[a] * v.x;
+                row.y += ex.w[a] * v.y;
+                if (++pw == N) pw = 0;
+            }
+            sum.x += wy * row.x;
+            sum.y += wy * row.y;
+        }
+        if (++qw == N) qw = 0;
+    }
+    return sum;
 }
 
 // InterpolatedImage leaf at k index (i, j) of a grid with spacing dk.
-// d[0] = N / 2 pi (k to sample index), d[1] = maxk1 (x interpolant cut-off), d[2] / d[3] =
+// d[0] = (N/2) / pi (k to sample index), d[1] = maxk1 (x interpolant cut-off), d[2] / d[3] =
 // x / k interpolant codes, d[4] = N, d[6] / d[7] = FP64 / FP32 k-image addresses.
 template <typename T>
 __device__ __noinline__ Cx<T> ii_kvalue(const LeafParams& L, double dk, int i, int j)
@@ -141,45 +193,11 @@ __device__ __noinline__ Cx<T> ii_kvalue(const LeafParams& L, double dk, int i, i
     const double kyp = L.jac[1] * kx + L.jac[3] * ky;
     const double maxk1 = L.d[1];
     if (fabs(kxp) > maxk1 || fabs(kyp) > maxk1) return cx<T>(T(0), T(0));
-    const int N = int(L.d[4]);
-    const int xc = int(L.d[2]), kc = int(L.d[3]);
     const bool sep = !(L.flags & GSB_LEAF_JAC_GENERAL);
-    const Cx<T>* K = reinterpret_cast<const Cx<T>*>(
-        __double_as_longlong(sizeof(T) == 8 ? L.d[6] : L.d[7]));
-    int p1, np, q1, nq;
-    T wx[kInterpMaxTaps], wy[kInterpMaxTaps];
-    interp_taps<T>(kc, kxp * L.d[0], sep, p1, np, wx);
-    interp_taps<T>(kc, kyp * L.d[0], sep, q1, nq, wy);
-    int pw0 = p1 % N;
-    if (pw0 < 0) pw0 += N;
-    int qw = q1 % N;
-    if (qw < 0) qw += N;
-    Cx<T> sum = cx<T>(T(0), T(0));
-#pragma unroll
-    for (int b = 0; b < kInterpMaxTaps; ++b) {
-        if (b < nq && wy[b] != T(0)) {
-            Cx<T> row = cx<T>(T(0), T(0));
-            int pw = pw0;
-#pragma unroll
-            for (int a = 0; a < kInterpMaxTaps; ++a) {
-                if (a < np) {
-                    const Cx<T> v = kimage_at<T>(K, N, pw, qw);
-                    row.x += wx[a] * v.x;
-                    row.y += wx[a] * v.y;
-                }
-                if (++pw == N) pw = 0;
-            }
-            sum.x += wy[b] * row.x;
-            sum.y += wy[b] * row.y;
-        }
-        if (++qw == N) qw = 0;
-    }
-    // The transform factor is evaluated in FP64 for every precision: the quintic's
-    // s (55 - 19 pi^2 u^2) + 2 c (pi^2 u^2 - 27) is 55 s - 54 c + O(u^2) near u = 0, which
-    // would amplify FP32 rounding of s and c 55-fold (a 3e-6 flux bias).
-    constexpr double kUscale = 1. / (2. * kPi);
-    const T f = T(L.flux * interp_uval<double>(xc, kxp * kUscale) * interp_uval<double>(xc, kyp * kUscale));
-    return cx<T>(f * sum.x, f * sum.y);
+    IITaps<T> ex, ey;
+    ii_axis_taps<T>(L, kxp, sep, true, ex);
+    ii_axis_taps<T>(L, kyp, sep, false, ey);
+    return ii_sum<T>(L, ex, ey);
 }
 
 }  // namespace gsb

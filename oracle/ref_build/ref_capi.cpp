@@ -15,6 +15,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "GSParams.h"
 #include "Image.h"
@@ -22,6 +23,8 @@
 #include "SBBox.h"
 #include "SBExponential.h"
 #include "SBGaussian.h"
+#include "SBInterpolatedImage.h"
+#include "Interpolant.h"
 #include "SBKolmogorov.h"
 #include "SBMoffat.h"
 #include "SBSersic.h"
@@ -65,9 +68,85 @@ ImageView<T> view(T* data, int xmin, int xmax, int ymin, int ymax)
                         Bounds<int>(xmin, xmax, ymin, ymax));
 }
 
+std::unique_ptr<Interpolant> make_interp(int code, const GSParams& gsp)
+{
+    switch (code) {
+      case 0: return std::unique_ptr<Interpolant>(new Delta(gsp));
+      case 1: return std::unique_ptr<Interpolant>(new Nearest(gsp));
+      case 2: return std::unique_ptr<Interpolant>(new Linear(gsp));
+      case 3: return std::unique_ptr<Interpolant>(new Cubic(gsp));
+      case 4: return std::unique_ptr<Interpolant>(new Quintic(gsp));
+    }
+    throw std::runtime_error("unknown interpolant");
+}
+
+// An SBInterpolatedImage with the buffers it views (InterpolatedImage._sbp,
+// galsim/interpolatedimage.py:481-500).
+struct IIHandle {
+    GSParams gsp;
+    std::vector<double> data;
+    std::unique_ptr<Interpolant> xi, ki;
+    std::unique_ptr<SBInterpolatedImage> sb;
+    explicit IIHandle(const GSParams& g) : gsp(g) {}
+};
+
 }  // namespace
 
 extern "C" {
+
+// SBInterpolatedImage over an N x N padded image (bounds -N/2..N/2-1 both ways), with the
+// image and nonzero bounds as (xmin, xmax, ymin, ymax); stepk / maxk <= 0 are computed.
+void* gsref_ii_create(const double* xim, int N, const int* ib, const int* nb, int xcode, int kcode,
+                      double stepk, double maxk, const double* gsp)
+{
+    try {
+        std::unique_ptr<IIHandle> h(new IIHandle(make_gsp(gsp)));
+        h->data.assign(xim, xim + size_t(N) * N);
+        h->xi = make_interp(xcode, h->gsp);
+        h->ki = make_interp(kcode, h->gsp);
+        ImageView<double> im = view(h->data.data(), -N / 2, N / 2 - 1, -N / 2, N / 2 - 1);
+        h->sb.reset(new SBInterpolatedImage(im, Bounds<int>(ib[0], ib[1], ib[2], ib[3]),
+                                            Bounds<int>(nb[0], nb[1], nb[2], nb[3]), *h->xi, *h->ki,
+                                            stepk, maxk, h->gsp));
+        return h.release();
+    } catch (std::exception& e) { g_err = e.what(); return nullptr; }
+}
+
+void gsref_ii_destroy(void* h) { delete static_cast<IIHandle*>(h); }
+
+// calculateMaxK(max_maxk) then maxK() (image units).
+int gsref_ii_maxk(void* h, double max_maxk, double* out)
+{
+    try {
+        IIHandle* ii = static_cast<IIHandle*>(h);
+        ii->sb->calculateMaxK(max_maxk);
+        *out = ii->sb->maxK();
+        return 0;
+    } catch (std::exception& e) { g_err = e.what(); return -1; }
+}
+
+int gsref_ii_draw_k(void* h, double* kimage, int xmin, int xmax, int ymin, int ymax, double dk,
+                    const double* jac)
+{
+    try {
+        IIHandle* ii = static_cast<IIHandle*>(h);
+        double j[4];
+        if (jac) std::memcpy(j, jac, sizeof(j));
+        ii->sb->drawK(view(reinterpret_cast<std::complex<double>*>(kimage), xmin, xmax, ymin, ymax),
+                      dk, jac ? j : nullptr);
+        return 0;
+    } catch (std::exception& e) { g_err = e.what(); return -1; }
+}
+
+// CalculateSizeContainingFlux on an image with bounds (xmin, xmax, ymin, ymax).
+int gsref_size_containing_flux(double* im, int xmin, int xmax, int ymin, int ymax, double target,
+                               double* out)
+{
+    try {
+        *out = CalculateSizeContainingFlux(view(im, xmin, xmax, ymin, ymax), target);
+        return 0;
+    } catch (std::exception& e) { g_err = e.what(); return -1; }
+}
 
 const char* gsref_last_error() { return g_err.c_str(); }
 

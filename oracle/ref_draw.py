@@ -40,6 +40,16 @@ def lib():
         L.gsref_irfft.argtypes = [dp, ctypes.c_int, ctypes.c_int, dp]
         L.gsref_good_fft_size.argtypes = [ctypes.c_int]
         L.gsref_last_error.restype = ctypes.c_char_p
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.gsref_ii_create.restype = ctypes.c_void_p
+        L.gsref_ii_create.argtypes = [dp, ctypes.c_int, ip, ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                      ctypes.c_double, dp]
+        L.gsref_ii_destroy.argtypes = [ctypes.c_void_p]
+        L.gsref_ii_maxk.argtypes = [ctypes.c_void_p, ctypes.c_double, dp]
+        L.gsref_ii_draw_k.argtypes = [ctypes.c_void_p, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_double, dp]
+        L.gsref_size_containing_flux.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_double, dp]
         _lib = L
     return _lib
 
@@ -69,8 +79,69 @@ def _leaf_args(o):
     raise TypeError(o)
 
 
+INTERP_CODES = {'delta': 0, 'nearest': 1, 'linear': 2, 'cubic': 3, 'quintic': 4}
+
+
+class RIILeaf(object):
+    """The reference's SBInterpolatedImage (image units) over a padded image."""
+
+    def __init__(self, xim, ib, nb, xcode, kcode, stepk_img):
+        N = xim.shape[0]
+        self.xim = np.ascontiguousarray(xim, dtype=np.float64)
+        ibv = (ctypes.c_int * 4)(*ib)
+        nbv = (ctypes.c_int * 4)(*nb)
+        self.h = lib().gsref_ii_create(_p(self.xim), N, ibv, nbv, xcode, kcode, stepk_img, 0., _p(GSP))
+        if not self.h:
+            raise RuntimeError(lib().gsref_last_error().decode())
+
+    def maxk(self, max_maxk=0.):
+        out = np.zeros(1)
+        if lib().gsref_ii_maxk(self.h, max_maxk, _p(out)):
+            raise RuntimeError(lib().gsref_last_error().decode())
+        return float(out[0])
+
+    def __del__(self):
+        if getattr(self, 'h', None):
+            lib().gsref_ii_destroy(self.h)
+
+
+class RInterpolatedImage(O.OObj):
+    """InterpolatedImage(image, scale=...) on the reference's C++ (interpolatedimage.py:303-685):
+    CalculateSizeContainingFlux and calculateMaxK for the sizes, SBInterpolatedImage::drawK for
+    the k-values; the frame and the world transform follow the reference's Python."""
+
+    def __init__(self, array, scale, x_interp='quintic', k_interp='quintic', pad_factor=4.):
+        arr = np.ascontiguousarray(array, dtype=np.float64)
+        ny, nx = arr.shape
+        x0, y0 = -(nx // 2), -(ny // 2)
+        dx = -0.5 if nx % 2 == 0 else 0.
+        dy = -0.5 if ny % 2 == 0 else 0.
+        pad = max(nx, ny)
+        if pad_factor > 1.:
+            pad = int(math.ceil(pad_factor * pad))
+        N = lib().gsref_good_fft_size(pad)
+        xim = np.zeros((N, N))
+        xim[y0 + N // 2:y0 + N // 2 + ny, x0 + N // 2:x0 + N // 2 + nx] = arr
+        b = (x0, x0 + nx - 1, y0, y0 + ny - 1)
+        image_flux = float(np.sum(arr, dtype=np.float64))
+        out = np.zeros(1)
+        if lib().gsref_size_containing_flux(_p(arr), b[0], b[1], b[2], b[3], (1. - GSP[2]) * image_flux, _p(out)):
+            raise RuntimeError(lib().gsref_last_error().decode())
+        R = math.hypot(float(out[0]), O.INTERP_XRANGE[x_interp])
+        self.stepk = math.pi / (R * scale)
+        self.leaf = RIILeaf(xim, b, b, INTERP_CODES[x_interp], INTERP_CODES[k_interp], self.stepk * scale)
+        self.maxk = self.leaf.maxk() / scale
+        prof = self.leaf
+        if dx != 0. or dy != 0.:
+            prof = O.OTransform(prof, offset=(-dx, -dy))
+        jac = None if scale == 1. else [[scale, 0.], [0., scale]]
+        self.inner = O.OTransform(prof, jac=jac, flux_ratio=(1. / scale) ** 2)
+
+
 def stepk_maxk(o):
     """Leaf sizes from the reference C++; composition by the reference Python rules."""
+    if isinstance(o, RInterpolatedImage):
+        return o.stepk, o.maxk
     if isinstance(o, O.OConvolve):
         s = [stepk_maxk(x) for x in o.objs]
         inv = 0
@@ -115,6 +186,15 @@ def stepk_maxk(o):
 def draw_k(o, kim, xmin, ymin, dk, jac):
     """_drawKImage tree walk with the reference's C++ for the leaves and phases."""
     n, m = kim.shape
+    if isinstance(o, RInterpolatedImage):
+        draw_k(o.inner, kim, xmin, ymin, dk, jac)
+        return
+    if isinstance(o, RIILeaf):
+        j = None if jac is None else np.ascontiguousarray(jac, dtype=np.float64)
+        if lib().gsref_ii_draw_k(o.h, _p(kim.view(np.float64)), xmin, xmin + m - 1, ymin, ymin + n - 1,
+                                 dk, _p(j)):
+            raise RuntimeError(lib().gsref_last_error().decode())
+        return
     if isinstance(o, (O.OConvolve, O.OSum)):
         draw_k(o.objs[0], kim, xmin, ymin, dk, jac)
         tmp = np.empty_like(kim)
@@ -161,15 +241,17 @@ def c2_profile(n, hlr, flux, g1, g2, fwhm, scale):
     return O.OConvolve(RSersic(n, hlr, flux).shear(g1, g2), O.OKolmogorov(fwhm=fwhm), O.OBox(scale))
 
 
-def draw_image(prof, nx, ny, scale, offset=(0., 0.)):
-    """drawImage(nx, ny, scale, method='fft') through the reference C++ (FP64); nx = ny = None
-    sizes the image automatically (getGoodImageSize, gsobject.py:1900-1925)."""
+def draw_image(prof, nx, ny, scale, offset=(0., 0.), pixel=True):
+    """drawImage(nx, ny, scale, method='fft' | 'no_pixel' (pixel=False)) through the reference
+    C++ (FP64); nx = ny = None sizes the image automatically (getGoodImageSize,
+    gsobject.py:1900-1925)."""
     auto = nx is None
     dx = float(offset[0]) - (0.5 if auto or nx % 2 == 0 else 0.)
     dy = float(offset[1]) - (0.5 if auto or ny % 2 == 0 else 0.)
     inv = 1. / scale
-    img = O.OConvolve(O.OTransform(prof, jac=[[inv, 0.], [0., inv]], offset=(dx, dy), flux_ratio=scale ** 2),
-                      O.OBox(1.0))
+    img = O.OTransform(prof, jac=[[inv, 0.], [0., inv]], offset=(dx, dy), flux_ratio=scale ** 2)
+    if pixel:
+        img = O.OConvolve(img, O.OBox(1.0))
     if auto:
         sk, _ = stepk_maxk(img)
         nn = int(math.ceil(2. * math.pi / sk * (1. - 1.e-12)))
