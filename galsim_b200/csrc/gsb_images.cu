@@ -9,7 +9,7 @@
 // zero, so a 32 x 32 image in a 128 x 128 frame costs 32 rows and 32 terms per output rather
 // than full-frame FFTs):
 //   rows:  R(p, y) = sum_x I(x, y) tw[(p X) mod N],   p = 0..N/2, y over the region's rows
-//   cols:  K(p, q) = sum_y R(p, y) tw[(q Y) mod N],   q = 0..N-1
+//   cols:  K(p, q) = sum_y R(p, y) tw[(q Y) mod N],   q = 0..N-1, stored p-major
 // with tw[m] = exp(-2 pi i m / N) in shared memory and exact integer phase indices; FP64
 // throughout, with an FP32 copy of K for FP32 draws.
 #include <algorithm>
@@ -65,7 +65,9 @@ __global__ void kimage_rows_kernel(const ImageSlot* slots, const double* pix, do
     }
 }
 
-// Pass 2: K(p, q) for the whole half plane.  grid = (blocks, images).
+// Pass 2: K(p, q) for the whole half plane, stored p-major (K[p N + q]): the drawing kernels
+// read it with the lanes of a warp on consecutive rows, i.e. consecutive q at a shared p.
+// grid = (blocks, images).
 __global__ void kimage_cols_kernel(const ImageSlot* slots, const double2* rows, double2* k64, float2* k32)
 {
     extern __shared__ double2 tw_cols[];
@@ -79,7 +81,7 @@ __global__ void kimage_cols_kernel(const ImageSlot* slots, const double2* rows, 
     const long long total = (long long)N * H;
     for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < total;
          o += (long long)gridDim.x * blockDim.x) {
-        const int q = int(o / H), p = int(o % H);
+        const int p = int(o / N), q = int(o % N);
         int m = pmod_int((long long)q * d.y0, N);
         double re = 0., im = 0.;
         for (int y = 0; y < d.ny; ++y) {
@@ -157,9 +159,9 @@ __global__ void __launch_bounds__(kScanThreads) kimage_scan_kernel(const ImageSl
         if (max_ix > No2) max_ix = No2;
         for (int ix = threadIdx.x; ix <= max_ix; ix += blockDim.x) above[ix] = 0;
         __syncthreads();
-        // kimage(p, q) with p in 0..No2, q in -No2..No2-1
+        // kimage(p, q) with p in 0..No2, q in -No2..No2-1 (stored p-major)
         auto nrm = [&](int p, int q) -> double {
-            const double2 v = K[(size_t)(q < 0 ? q + N : q) * H + p];
+            const double2 v = K[(size_t)p * N + (q < 0 ? q + N : q)];
             return v.x * v.x + v.y * v.y;
         };
         for (int ix = 0; ix <= max_ix; ++ix) {

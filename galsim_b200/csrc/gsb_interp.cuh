@@ -5,7 +5,7 @@
 //   v(kx, ky) = flux * U(kx / 2 pi) U(ky / 2 pi) * sum_pq w(p - kx N / 2 pi) w(q - ky N / 2 pi) K(p, q)
 // (SBInterpolatedImage::kValue and both fillKImage forms, src/SBInterpolatedImage.cpp:385-448,
 // 767-1000), with K periodic in N and Hermitian (K(-p, -q) = conj K(p, q)), so only the half
-// plane p = 0..N/2 is stored (rows q = 0..N-1 of N/2 + 1 values).  Tap positions are formed in
+// plane p = 0..N/2 is stored (p-major: N/2 + 1 columns of N values q).  Tap positions are formed in
 // FP64 even for FP32 draws: their fractions must stay exact at indices of several hundred.
 #pragma once
 
@@ -92,14 +92,13 @@ __host__ __device__ inline double interp_urange(int code, double kacc)
     return 0.;
 }
 
-// K(p, q) of the half-plane k-image for any integers p, q.
+// K(p, q) of the half-plane k-image (stored p-major: K[p N + q], p = 0..N/2) for p, q already
+// reduced to 0..N-1.
 template <typename T>
 __device__ __forceinline__ Cx<T> kimage_at(const Cx<T>* K, int N, int pm, int qm)
 {
-    // pm, qm already reduced to 0..N-1
-    const int H = N / 2 + 1;
-    if (pm <= N / 2) return K[(size_t)qm * H + pm];
-    const Cx<T> v = K[(size_t)(qm == 0 ? 0 : N - qm) * H + (N - pm)];
+    if (pm <= N / 2) return K[(size_t)pm * N + qm];
+    const Cx<T> v = K[(size_t)(N - pm) * N + (qm == 0 ? 0 : N - qm)];
     return cx<T>(v.x, -v.y);
 }
 

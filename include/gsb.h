@@ -206,7 +206,8 @@ typedef struct gsb_image_desc {
 
 /* Build image slots 0..count-1 of t (replacing any earlier images; Sersic slots are kept):
  * per image the half-plane DFT of its padded frame,
- *     K(p, q) = sum_XY I(X, Y) exp(-2 pi i (p X + q Y) / N),  p = 0..N/2, q = 0..N-1,
+ *     K(p, q) = sum_XY I(X, Y) exp(-2 pi i (p X + q Y) / N),  p = 0..N/2, q = 0..N-1
+ * (stored p-major),
  * in FP64 and as an FP32 copy (checkK: rfft with shift_in / shift_out, src/Image.cpp:730-812);
  * with GSB_IMAGE_STEPK the radius R = d + 1/2 of the smallest centred box holding
  * stepk_target (CalculateSizeContainingFlux, SBInterpolatedImage.cpp:1084-1110); with

@@ -1281,3 +1281,233 @@ def draw_kimage(obj, nkx, nky, kxmin, kymin, dk):
     kim = np.zeros((nky, nkx), dtype=np.complex128)
     obj.drawK(kim, kxmin, kymin, dk, None)
     return kim
+
+
+# ---------------------------------------------------------------------------------------------
+# Noise (galsim/noise.py, galsim/random.py, src/Random.cpp with the Boost.Random 1.48 engines
+# and distributions it vendors): pure-Python restatement for small images.
+# ---------------------------------------------------------------------------------------------
+class OMersenneTwister(object):
+    """Mersenne Twister (Matsumoto & Nishimura 1998) with the init_genrand seeding of
+    2002 (mersenne_twister.hpp:154-185, 430-478)."""
+
+    def __init__(self, w, n, m, r, a, u, s, b, t, c, l, f, seed):
+        self.n, self.m, self.r, self.a = n, m, r, a
+        self.u, self.s, self.b, self.t, self.c, self.l = u, s, b, t, c, l
+        mask = 0xffffffff
+        x = [0] * n
+        x[0] = seed & mask
+        for i in range(1, n):
+            x[i] = (f * (x[i - 1] ^ (x[i - 1] >> (w - 2))) + i) & mask
+        if (x[0] & ((mask << r) & mask)) == 0 and all(v == 0 for v in x[1:]):
+            x[0] = 1 << (w - 1)
+        self.x = x
+        self.i = n
+
+    def _twist(self):
+        n, m, x = self.n, self.m, self.x
+        upper = (0xffffffff << self.r) & 0xffffffff
+        lower = (~upper) & 0xffffffff
+        for j in range(n):
+            y = (x[j] & upper) | (x[(j + 1) % n] & lower)
+            x[j] = x[(j + m) % n] ^ (y >> 1) ^ ((x[(j + 1) % n] & 1) * self.a)
+        self.i = 0
+
+    def __call__(self):
+        if self.i == self.n:
+            self._twist()
+        z = self.x[self.i]
+        self.i += 1
+        z ^= (z >> self.u)
+        z ^= (z << self.s) & self.b
+        z ^= (z << self.t) & self.c
+        z ^= (z >> self.l)
+        return z & 0xffffffff
+
+
+def mt19937(seed):
+    return OMersenneTwister(32, 624, 397, 31, 0x9908b0df, 11, 7, 0x9d2c5680, 15, 0xefc60000, 18,
+                            1812433253, seed)
+
+
+def mt11213b(seed):
+    return OMersenneTwister(32, 351, 175, 19, 0xccab8ee7, 11, 7, 0x31b6ab00, 15, 0xffe50000, 17,
+                            1812433253, seed)
+
+
+def base_deviate(seed):
+    """BaseDeviate(seed) (Random.cpp:156-191): the seed goes through 2 discarded draws of an
+    mt11213b, whose third draw seeds the mt19937 used for everything."""
+    alt = mt11213b(int(seed) & 0xffffffff)
+    alt()
+    alt()
+    return mt19937(alt())
+
+
+def uniform01(rng):
+    """boost uniform_01 on a 32-bit engine: one draw times 2^-32."""
+    return rng() * (1. / 4294967296.)
+
+
+class OGaussian(object):
+    """boost 1.48 normal_distribution: Box-Muller pairs, cos first (normal_distribution.hpp:153-175)."""
+
+    def __init__(self, mean=0., sigma=1.):
+        self.mean, self.sigma = mean, sigma
+        self.valid = False
+
+    def reset(self):
+        self.valid = False
+
+    def __call__(self, rng):
+        if not self.valid:
+            self.r1 = uniform01(rng)
+            self.r2 = uniform01(rng)
+            self.rho = math.sqrt(-2. * math.log(1. - self.r2))
+            self.valid = True
+            return self.rho * math.cos(2. * PI * self.r1) * self.sigma + self.mean
+        self.valid = False
+        return self.rho * math.sin(2. * PI * self.r1) * self.sigma + self.mean
+
+
+_LOG_FACT = [math.lgamma(k + 1.) for k in range(10)]
+
+
+def poisson_draw(mean, rng):
+    """boost 1.48 poisson_distribution: inversion below mean 10, otherwise the PTRD transformed
+    rejection of Hoermann (1993) (poisson_distribution.hpp)."""
+    if mean < 10:
+        p = math.exp(-mean)
+        x = 0
+        u = uniform01(rng)
+        while u > p:
+            u = u - p
+            x += 1
+            p = mean * p / x
+        return x
+    smu = math.sqrt(mean)
+    b = 0.931 + 2.53 * smu
+    a = -0.059 + 0.02483 * b
+    inv_alpha = 1.1239 + 1.1328 / (b - 3.4)
+    v_r = 0.9277 - 3.6224 / (b - 2)
+    while True:
+        v = uniform01(rng)
+        if v <= 0.86 * v_r:
+            u = v / v_r - 0.43
+            return int(math.floor((2 * a / (0.5 - abs(u)) + b) * u + mean + 0.445))
+        if v >= v_r:
+            u = uniform01(rng) - 0.5
+        else:
+            u = v / v_r - 0.93
+            u = (-0.5 if u < 0 else 0.5) - u
+            v = uniform01(rng) * v_r
+        us = 0.5 - abs(u)
+        if us < 0.013 and v > us:
+            continue
+        k = math.floor((2 * a / us + b) * u + mean + 0.445)
+        v = v * inv_alpha / (a / (us * us) + b)
+        if k >= 10:
+            if math.log(v * smu) <= ((k + 0.5) * math.log(mean / k) - mean - 0.91893853320467267 + k
+                                     - (1 / 12. - (1 / 360. - 1 / (1260. * k * k)) / (k * k)) / k):
+                return int(k)
+        elif k >= 0:
+            if math.log(v) <= k * math.log(mean) - mean - _LOG_FACT[int(k)]:
+                return int(k)
+
+
+class OPoissonDeviate(object):
+    """PoissonDeviate with the mean switching of Random.cpp:498-540: Gaussian above 2^30."""
+
+    def __init__(self, rng):
+        self.rng = rng
+        self.mean = -1.
+        self.gd = None
+        self.set_mean(1.)
+
+    def set_mean(self, mean):
+        if mean != self.mean:
+            self.mean = mean
+            if mean > float(1 << 30) or mean == 0.:
+                if self.gd is None:
+                    self.gd = OGaussian(mean, math.sqrt(mean))
+                else:
+                    self.gd.mean, self.gd.sigma = mean, math.sqrt(mean)
+                self.use_gd = True
+            else:
+                self.gd = None
+                self.use_gd = False
+
+    def __call__(self):
+        return self.gd(self.rng) if self.use_gd else float(poisson_draw(self.mean, self.rng))
+
+
+def gaussian_noise(image, rng, sigma):
+    """GaussianNoise._applyTo (noise.py:259-263): N(0, sigma) per pixel in row-major order,
+    cast to the image dtype and added."""
+    g = OGaussian(0., sigma)
+    noise = np.array([g(rng) for _ in range(image.size)]).reshape(image.shape)
+    image += noise.astype(image.dtype)
+    return image
+
+
+def _poisson_fill(noise, rng):
+    pd = OPoissonDeviate(rng)
+    flat = noise.reshape(-1)
+    for i in range(flat.size):
+        if flat[i] > 0.:
+            pd.set_mean(flat[i])
+            flat[i] = pd()
+
+
+def poisson_noise(image, rng, sky_level=0.):
+    """PoissonNoise._applyTo (noise.py:331-356)."""
+    noise = image.astype(np.float64)
+    # numpy scalar arithmetic as in the reference (a float image gives frac_sky = 0)
+    frac_sky = sky_level - image.dtype.type(sky_level)
+    int_sky = sky_level - frac_sky
+    if sky_level != 0.:
+        noise += sky_level
+    noise = noise.clip(0.)
+    _poisson_fill(noise, rng)
+    if frac_sky != 0.:
+        noise -= frac_sky
+    np.copyto(image, noise, casting='unsafe')
+    if int_sky != 0.:
+        _isub(image, int_sky)
+    return image
+
+
+def _isub(image, a):
+    """Image.__isub__ with a scalar (image.py:1666-1678)."""
+    if type(a) == image.dtype.type:
+        image[:, :] -= a
+    else:
+        r = image - a
+        if image.dtype.kind in 'iu':
+            r = np.around(r)
+        image[:, :] = r.astype(image.dtype, copy=False)
+
+
+def ccd_noise(image, rng, sky_level=0., gain=1., read_noise=0.):
+    """CCDNoise._applyTo (noise.py:463-486)."""
+    noise = image.astype(np.float64)
+    frac_sky = sky_level - image.dtype.type(sky_level)
+    int_sky = sky_level - frac_sky
+    if sky_level != 0.:
+        noise += sky_level
+    if gain > 0.:
+        noise *= gain
+        noise = noise.clip(0.)
+        _poisson_fill(noise, rng)
+        noise /= gain
+    if read_noise > 0.:
+        g = OGaussian(0., read_noise / gain if gain > 0. else read_noise)
+        flat = noise.reshape(-1)
+        for i in range(flat.size):
+            flat[i] += g(rng)
+    if frac_sky != 0.:
+        noise -= frac_sky
+    np.copyto(image, noise, casting='unsafe')
+    if int_sky != 0.:
+        _isub(image, int_sky)
+    return image
