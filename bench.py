@@ -19,6 +19,9 @@ chi^2 against a noisy target (SNR 50) and its gradient in the seven parameters t
 adjoint kernels (galsim_b200.autodiff), timed from host parameters to host gradients.
 Both carry the plain one-stamp-per-call rate of the same path beside them.
 
+`noise` applies the reference's CCDNoise to every stamp on the device (one seeded stream per
+stamp), beside the reference's C++ deviates on the host cores.
+
 `interp_psf` is the InterpolatedImage workload: the same 4096 galaxies convolved with one
 image PSF (a 32 x 32 effective-PSF image, quintic interpolants) drawn with
 method='no_pixel': device step, draw stage, k-image build, e2e and the reference's C++ on
@@ -207,6 +210,77 @@ def run_mixed(galsim, dev, steps, warmup):
             'forward_adjoint_unit': 'grad-evals/s', 'stamps': MIX_B,
             'workload': 'bulge_disk_moffat_gen_pixel_16384_seed2468 (Sersic n=4 + Exponential, Moffat beta U[2.5,4.5])',
             'gsparams': 'minimum_fft_size=32', 'fft_sizes': dict(zip(map(int, u), map(int, c)))}
+
+
+def _ref_noise_worker(args):
+    stamps, seeds = args
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import ctypes
+    import ref_draw as R
+    L = R.lib()
+    L.gsref_ccd_noise.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.c_longlong, ctypes.c_long,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    t = time.perf_counter()
+    for a, sd in zip(stamps, seeds):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        L.gsref_ccd_noise(a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a.size, int(sd),
+                          NOISE_SKY, NOISE_GAIN, NOISE_READ)
+    return time.perf_counter() - t
+
+
+NOISE_SKY, NOISE_GAIN, NOISE_READ = 100., 1.5, 5.
+
+
+def run_noise(galsim, dev, st, steps, warmup, cpu=True):
+    """Noise stage: CCDNoise(sky 100, gain 1.5 e-/ADU, read noise 5 e-) on every stamp of the
+    main workload's batch, stamp i with its own BaseDeviate(1 + i) (the reference's Poisson and
+    Gaussian streams), on the device before any copy to the host."""
+    import torch
+    from galsim_b200.batch import StampBatch
+    noise = galsim.CCDNoise(sky_level=NOISE_SKY, gain=NOISE_GAIN, read_noise=NOISE_READ)
+    B = len(st)
+    seeds = 1 + np.arange(B)
+    work = st.flat.clone()
+    sb = StampBatch(work, st.offsets, st.nx, st.ny, None, None, None, None, None, st.dtype, st.scale, None)
+    for _ in range(warmup):
+        work.copy_(st.flat)
+        sb.addNoise(noise, seeds)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tot = 0.
+    for _ in range(steps):
+        work.copy_(st.flat)
+        e0.record()
+        sb.addNoise(noise, seeds)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        tot += e0.elapsed_time(e1)
+    ms = tot / steps
+    npix = int((np.asarray(st.nx) * np.asarray(st.ny)).sum())
+    out = {'value': B / (ms * 1e-3), 'unit': 'stamps/s', 'ms': ms, 'pixels': npix,
+           'mpix_per_s': npix / (ms * 1e-3) / 1e6,
+           'workload': 'CCDNoise(sky 100, gain 1.5, read noise 5) on the 4096 stamps of the main '
+                       'workload, BaseDeviate(1 + i) per stamp, one warp per stamp',
+           'timed': 'gsb_add_noise including the per-call host setup (stamp records, scratch)'}
+    if cpu:
+        import multiprocessing as mp
+        sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+        import ref_draw as R
+        if R.available():
+            cores = os.cpu_count() or 1
+            n = min(B, 64 * cores)
+            arrs = [st.array(i).astype(np.float64) for i in range(n)]
+            chunks = [(arrs[i::cores], seeds[:n][i::cores]) for i in range(cores)]
+            ctx = mp.get_context('spawn')
+            with ctx.Pool(cores) as pool:
+                pool.map(_ref_noise_worker, chunks[:1])        # warm the imports
+                t = time.perf_counter()
+                pool.map(_ref_noise_worker, chunks)
+                wall = time.perf_counter() - t
+            out['cpu_baseline'] = {'value': n / wall, 'unit': 'stamps/s', 'cores': cores, 'kind': 'reference',
+                                   'sample': '%d leading stamps (reference C++ PoissonDeviate / '
+                                             'GaussianDeviate, one process per core)' % n}
+    return out
 
 
 INTERP_PSF_SIZE = 32
@@ -738,6 +812,9 @@ def run_gpu(args):
     interp = (run_interp(galsim, dev, params, max(args.steps, 3), max(args.warmup, 2),
                          cpu=(rank == 0 and world == 1 and not args.no_cpu))
               if not args.no_extra else None)
+    noise = (run_noise(galsim, dev, st, max(args.steps, 3), max(args.warmup, 2),
+                       cpu=(rank == 0 and world == 1 and not args.no_cpu))
+             if not args.no_extra else None)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -773,6 +850,7 @@ def run_gpu(args):
             'mixed_batch': mixed,
             'large_stamps': large,
             'interp_psf': interp,
+            'noise': noise,
             'clocks': clk.summary(),
         }
         if cpu is not None:

@@ -2,7 +2,8 @@
 
 A drop-in for ``GSObject.drawImage(method='fft')`` and ``drawKImage`` on
 Convolve / Sum / Transform trees of Gaussian, Exponential, Sersic, Moffat, Kolmogorov, Airy,
-Box / Pixel and InterpolatedImage.  The host code here mirrors the reference's Python API; every numerical
+Box / Pixel and InterpolatedImage, and the reference's Gaussian / Poisson / CCD noise applied
+on the device.  The host code here mirrors the reference's Python API; every numerical
 step of drawing (FP64 sizing and Sersic tables, k-space evaluation, Hermitian wrap, inverse
 FFT, crop and flux sum) runs in the hand-written CUDA kernels of libgsb.so, called through
 the C ABI declared in include/gsb.h.  There is no CPU fallback.
@@ -21,6 +22,7 @@ from .box import Box, Pixel
 from .interpolant import (Interpolant, Delta, Nearest, SincInterpolant, Linear, Cubic, Quintic,
                           Lanczos, convert_interpolant)
 from .interpolatedimage import InterpolatedImage
+from .noise import BaseDeviate, BaseNoise, GaussianNoise, PoissonNoise, CCDNoise
 from .compound import Convolve, Convolution, Add, Sum, Transform, Transformation, _Transform
 from .batch import draw_batch, plan_batch, run_batch, StampBatch
 from ._lib import set_device

@@ -51,6 +51,14 @@ class StampBatch(object):
     def __len__(self):
         return len(self.offsets)
 
+    def addNoise(self, noise, seeds, skips=None):
+        """Add noise to every stamp on the device, stamp i with its own stream
+        BaseDeviate(seeds[i]) (positioned skips[i] raw draws in): the noise each stamp would get
+        from ``image.addNoise(noise.copy(rng=galsim.BaseDeviate(seeds[i])))`` in the reference
+        (noise.py:31-39), as its config layer seeds each object.  Returns the draws used per
+        stamp (seeding included), to continue the streams."""
+        return noise._apply_batch(self, seeds, skips)
+
     def array(self, i):
         """Stamp i as a host numpy array (ny, nx)."""
         n = int(self.nx[i] * self.ny[i])

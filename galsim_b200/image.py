@@ -268,6 +268,10 @@ class Image(object):
     def copy(self):
         return _Image(self._array.copy(), self._bounds, self.wcs)
 
+    def addNoise(self, noise):
+        """Add noise to the image (image.py addNoise, noise.py:31-39); drawn on the GPU."""
+        noise.applyTo(self)
+
     def __iadd__(self, other):
         self._array += other.array if isinstance(other, Image) else other
         return self

@@ -1,0 +1,316 @@
+"""Random streams and noise: BaseDeviate, GaussianNoise, PoissonNoise, CCDNoise
+(galsim/random.py, galsim/noise.py).
+
+A BaseDeviate is the reference's random stream, named by its seed and the number of raw
+32-bit draws already taken from it; the draws themselves happen on the GPU
+(galsim_b200/csrc/gsb_noise.cu, `gsb_add_noise`), where the Mersenne Twister, its seeding and the
+Boost.Random 1.48 deviates the reference uses are restated, so a stamp gets the same noise as
+`image.addNoise(noise)` in the reference for the same seed.  Noise is applied to host Images
+(copied through the device) and, without leaving the device, to every stamp of a StampBatch
+with a seed per stamp (`StampBatch.addNoise`), as the reference's config layer seeds each
+object.
+"""
+import ctypes
+import math
+import os
+
+import numpy as np
+
+from . import _lib
+from .errors import GalSimError, GalSimNotImplementedError, GalSimRangeError, GalSimValueError
+
+
+class _Stream(object):
+    def __init__(self, seed):
+        self.seed = int(seed)
+        self.used = 0
+
+
+def _random_seed():
+    while True:
+        s = int.from_bytes(os.urandom(4), 'little')
+        if s:
+            return s
+
+
+class BaseDeviate(object):
+    """The reference's random-number stream (random.py BaseDeviate).  BaseDeviate(seed) with a
+    nonzero int is reproducible; None or 0 draws a seed from the operating system; another
+    BaseDeviate shares that stream (as the reference does)."""
+
+    def __init__(self, seed=None):
+        if isinstance(seed, BaseDeviate):
+            self._stream = seed._stream
+        elif seed is None or (not isinstance(seed, str) and int(seed) == 0):
+            self._stream = _Stream(_random_seed())
+        elif isinstance(seed, str):
+            raise GalSimNotImplementedError("BaseDeviate from a serialized state is not built")
+        else:
+            if int(seed) != seed:
+                raise TypeError("BaseDeviate must be initialized with an int or another BaseDeviate")
+            self._stream = _Stream(int(seed))
+
+    def seed(self, seed=0):
+        """Reseed this stream (seen by every object sharing it)."""
+        self._stream.seed = int(seed) if seed else _random_seed()
+        self._stream.used = 0
+
+    def reset(self, seed=None):
+        """Start an independent stream from seed."""
+        self._stream = BaseDeviate(seed)._stream
+
+    def duplicate(self):
+        """An independent copy at the same position."""
+        ret = BaseDeviate.__new__(BaseDeviate)
+        ret._stream = _Stream(self._stream.seed)
+        ret._stream.used = self._stream.used
+        return ret
+
+    def discard(self, n):
+        """Skip n raw draws."""
+        self._stream.used += int(n)
+
+    def __eq__(self, other):
+        return (isinstance(other, BaseDeviate) and self._stream.seed == other._stream.seed and
+                self._stream.used == other._stream.used)
+
+    def __ne__(self, other):
+        return not self.__eq__(other)
+
+    __hash__ = None
+
+    def __repr__(self):
+        return 'galsim.BaseDeviate(%r)' % self._stream.seed
+
+
+class NoiseParamsC(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ('sigma', 'sky_level', 'gain', 'read_noise',
+                                               'frac_sky', 'int_sky')] + \
+               [('int_sky_same_dtype', ctypes.c_int32), ('pad', ctypes.c_int32)]
+
+
+NOISE_STAMP_DTYPE = np.dtype({'names': ['offset', 'npix', 'pad', 'seed', 'skip'],
+                              'formats': ['i8', 'i4', 'i4', 'i8', 'i8'],
+                              'offsets': [0, 8, 12, 16, 24], 'itemsize': 32})
+
+GAUSSIAN, POISSON, CCD = 0, 1, 2
+
+
+def _sky_split(sky_level, dtype):
+    """frac_sky / int_sky of PoissonNoise / CCDNoise._applyTo with numpy's scalar rules
+    (noise.py:337-339): for float images frac_sky is 0 and int_sky is sky_level in the image
+    type."""
+    frac_sky = sky_level - np.dtype(dtype).type(sky_level)
+    int_sky = sky_level - frac_sky
+    same = np.dtype(type(int_sky)) == np.dtype(dtype)
+    return float(frac_sky), float(int_sky), bool(same)
+
+
+def _apply(kind, params, flat, offsets, npix, seeds, skips):
+    """Run gsb_add_noise on a device tensor `flat` (float32 / float64) with per-stamp records;
+    returns the per-stamp draw counts after the call."""
+    import torch
+    dev = _lib.Device.torch_device()
+    B = len(offsets)
+    rec = np.zeros(B, dtype=NOISE_STAMP_DTYPE)
+    rec['offset'] = offsets
+    rec['npix'] = npix
+    rec['seed'] = seeds
+    rec['skip'] = skips
+    d_rec = _lib.to_device(rec)
+    if flat.dtype == torch.float32:
+        dt = _lib.F32
+    elif flat.dtype == torch.float64:
+        dt = _lib.F64
+    else:
+        raise GalSimNotImplementedError("noise is applied to float32 / float64 images here")
+    scratch = torch.empty(flat.numel() if kind != GAUSSIAN else 1, dtype=torch.float64, device=dev)
+    used = torch.empty(B, dtype=torch.int64, device=dev)
+    _lib.check(_lib.lib().gsb_add_noise(kind, ctypes.byref(params), _lib.ptr(d_rec), B, _lib.ptr(flat),
+                                        dt, _lib.ptr(scratch), _lib.ptr(used), _lib.Device.stream()))
+    return used.cpu().numpy()
+
+
+class BaseNoise(object):
+    """noise.py BaseNoise: a noise model with its random stream."""
+
+    def __init__(self, rng=None):
+        if rng is None:
+            self._rng = BaseDeviate()
+        elif isinstance(rng, BaseDeviate):
+            self._rng = rng
+        else:
+            raise TypeError("rng must be a galsim.BaseDeviate")
+
+    @property
+    def rng(self):
+        return self._rng
+
+    def getVariance(self):
+        return self._getVariance()
+
+    def withVariance(self, variance):
+        if variance < 0.:
+            raise GalSimRangeError("variance must be >= 0", variance, 0.)
+        return self._withVariance(variance)
+
+    def withScaledVariance(self, variance_ratio):
+        if variance_ratio < 0.:
+            raise GalSimRangeError("variance_ratio must be >= 0", variance_ratio, 0.)
+        return self._withScaledVariance(variance_ratio)
+
+    def __mul__(self, variance_ratio):
+        return self.withScaledVariance(variance_ratio)
+
+    __rmul__ = __mul__
+
+    def __div__(self, variance_ratio):
+        return self.withScaledVariance(1. / variance_ratio)
+
+    __truediv__ = __div__
+
+    def __eq__(self, other):
+        return self is other or repr(self) == repr(other)
+
+    def __ne__(self, other):
+        return not self.__eq__(other)
+
+    __hash__ = None
+
+    def applyTo(self, image):
+        """Add this noise to an Image (on the GPU; the stream advances as in the reference)."""
+        from .image import Image
+        if not isinstance(image, Image):
+            raise TypeError("Provided image must be a galsim.Image")
+        self._applyTo(image)
+
+    def _applyTo(self, image):
+        import torch
+        arr = image.array
+        if arr.dtype not in (np.float32, np.float64):
+            raise GalSimNotImplementedError("noise is applied to float32 / float64 images here")
+        kind, params = self._params(arr.dtype)
+        host = np.ascontiguousarray(arr)
+        flat = torch.from_numpy(host.reshape(-1).copy()).to(_lib.Device.torch_device())
+        st = self._rng._stream
+        used = _apply(kind, params, flat, [0], [host.size], [st.seed], [st.used])
+        arr[...] = flat.cpu().numpy().reshape(arr.shape)
+        st.used = int(used[0])
+
+    def _apply_batch(self, sb, seeds, skips=None):
+        B = len(sb.offsets)
+        seeds = np.broadcast_to(np.asarray(seeds, dtype=np.int64), (B,))
+        if np.any(seeds == 0):
+            raise GalSimValueError("stamp seeds must be nonzero", seeds)
+        skips = np.zeros(B, np.int64) if skips is None else np.broadcast_to(np.asarray(skips, np.int64), (B,))
+        kind, params = self._params(np.float32 if sb.dtype == np.float32 else np.float64)
+        npix = (np.asarray(sb.nx) * np.asarray(sb.ny)).astype(np.int32)
+        return _apply(kind, params, sb.flat, np.asarray(sb.offsets, np.int64), npix, seeds, skips)
+
+
+class GaussianNoise(BaseNoise):
+    """Gaussian noise of standard deviation sigma (noise.py:227-291)."""
+
+    def __init__(self, rng=None, sigma=1.):
+        BaseNoise.__init__(self, rng)
+        self._sigma = sigma
+
+    sigma = property(lambda self: self._sigma)
+
+    def _params(self, dtype):
+        p = NoiseParamsC()
+        p.sigma = float(self._sigma)
+        return GAUSSIAN, p
+
+    def _getVariance(self):
+        return self.sigma ** 2
+
+    def _withVariance(self, variance):
+        return GaussianNoise(self.rng, math.sqrt(variance))
+
+    def _withScaledVariance(self, variance_ratio):
+        return GaussianNoise(self.rng, self.sigma * math.sqrt(variance_ratio))
+
+    def copy(self, rng=None):
+        return GaussianNoise(self.rng if rng is None else rng, self.sigma)
+
+    def __repr__(self):
+        return 'galsim.GaussianNoise(rng=%r, sigma=%r)' % (self.rng, self.sigma)
+
+
+class PoissonNoise(BaseNoise):
+    """Poisson noise of the image plus sky_level counts (noise.py:292-383)."""
+
+    def __init__(self, rng=None, sky_level=0.):
+        BaseNoise.__init__(self, rng)
+        self._sky_level = sky_level
+
+    sky_level = property(lambda self: self._sky_level)
+
+    def _params(self, dtype):
+        p = NoiseParamsC()
+        p.sky_level = float(self._sky_level)
+        p.frac_sky, p.int_sky, p.int_sky_same_dtype = _sky_split(self._sky_level, dtype)
+        return POISSON, p
+
+    def _getVariance(self):
+        return self.sky_level
+
+    def _withVariance(self, variance):
+        return PoissonNoise(self.rng, variance)
+
+    def _withScaledVariance(self, variance_ratio):
+        return PoissonNoise(self.rng, self.sky_level * variance_ratio)
+
+    def copy(self, rng=None):
+        return PoissonNoise(self.rng if rng is None else rng, self.sky_level)
+
+    def __repr__(self):
+        return 'galsim.PoissonNoise(rng=%r, sky_level=%r)' % (self.rng, self.sky_level)
+
+
+class CCDNoise(BaseNoise):
+    """Poisson noise in electrons (gain e- / ADU) plus Gaussian read noise (noise.py:384-550)."""
+
+    def __init__(self, rng=None, sky_level=0., gain=1., read_noise=0.):
+        BaseNoise.__init__(self, rng)
+        self._sky_level = float(sky_level)
+        self._gain = float(gain)
+        self._read_noise = float(read_noise)
+
+    sky_level = property(lambda self: self._sky_level)
+    gain = property(lambda self: self._gain)
+    read_noise = property(lambda self: self._read_noise)
+
+    def _params(self, dtype):
+        p = NoiseParamsC()
+        p.sky_level = self._sky_level
+        p.gain = self._gain
+        p.read_noise = self._read_noise
+        p.frac_sky, p.int_sky, p.int_sky_same_dtype = _sky_split(self._sky_level, dtype)
+        return CCD, p
+
+    def _getVariance(self):
+        if self.gain > 0.:
+            return self.sky_level / self.gain + (self.read_noise / self.gain) ** 2
+        return self.read_noise ** 2
+
+    def _withVariance(self, variance):
+        current = self._getVariance()
+        if current > 0.:
+            return self._withScaledVariance(variance / current)
+        return CCDNoise(self.rng, sky_level=variance)
+
+    def _withScaledVariance(self, variance_ratio):
+        return CCDNoise(self.rng, gain=self.gain, sky_level=self.sky_level * variance_ratio,
+                        read_noise=self.read_noise * math.sqrt(variance_ratio))
+
+    def copy(self, rng=None):
+        return CCDNoise(self.rng if rng is None else rng, self.sky_level, self.gain, self.read_noise)
+
+    def __repr__(self):
+        return 'galsim.CCDNoise(rng=%r, sky_level=%r, gain=%r, read_noise=%r)' % (
+            self.rng, self.sky_level, self.gain, self.read_noise)
+
+
+__all__ = ['BaseDeviate', 'BaseNoise', 'GaussianNoise', 'PoissonNoise', 'CCDNoise']

@@ -221,6 +221,42 @@ int gsb_images_build(gsb_tables* t, int count, const gsb_image_desc* h_desc, con
 /* Copy per image (R, maxk) back (2 doubles per image; 0 where not computed). */
 int gsb_images_info(const gsb_tables* t, double* h_out, int count, void* stream);
 
+/* Noise ---------------------------------------------------------------------------------- */
+/* GaussianNoise, PoissonNoise and CCDNoise applied to stamps in device memory with the
+ * reference's random streams (galsim/noise.py:259-263, 331-356, 463-486; src/Random.cpp).  Each
+ * stamp has its own BaseDeviate(seed) (Random.cpp:156-191: the seed passes through an mt11213b
+ * whose third draw seeds the mt19937), positioned `skip` raw 32-bit draws into its stream
+ * (0 for a fresh BaseDeviate); the deviates follow Boost.Random 1.48 as the reference vendors it
+ * (uniform_01, Box-Muller normal pairs, inversion / PTRD Poisson). */
+enum { GSB_NOISE_GAUSSIAN = 0, GSB_NOISE_POISSON = 1, GSB_NOISE_CCD = 2 };
+
+typedef struct gsb_noise_stamp {
+    int64_t offset;    /* first pixel of the stamp in the image buffer (elements) */
+    int32_t npix;      /* pixels, row-major and contiguous */
+    int32_t pad;
+    int64_t seed;      /* the BaseDeviate seed (nonzero) */
+    int64_t skip;      /* raw draws of that stream already consumed */
+} gsb_noise_stamp;
+
+typedef struct gsb_noise_params {
+    double sigma;          /* GaussianNoise sigma */
+    double sky_level;      /* Poisson / CCD: sky added before the draw */
+    double gain;           /* CCD gain (e- / ADU); ignored for Poisson */
+    double read_noise;     /* CCD read noise (e-) */
+    double frac_sky;       /* subtracted in FP64 before the cast to the image type */
+    double int_sky;        /* subtracted after the cast (the reference's numpy scalar rules
+                              decide the split; for float images frac_sky is 0) */
+    int32_t int_sky_same_dtype;   /* int_sky has the image's type: subtract in that type */
+    int32_t pad;
+} gsb_noise_params;
+
+/* Add noise of `kind` to n_stamps stamps of d_image (GSB_F32 or GSB_F64).  Poisson and CCD
+ * noise need d_scratch: one double per pixel, addressed like d_image.  d_used (may be NULL)
+ * receives, per stamp, the raw draws consumed since seeding (skip + this call's draws), so a
+ * caller can continue the stream.  One warp per stamp; no allocation. */
+int gsb_add_noise(int kind, const gsb_noise_params* p, const gsb_noise_stamp* d_stamps, int n_stamps,
+                  void* d_image, int dtype, double* d_scratch, long long* d_used, void* stream);
+
 /* Leaves -------------------------------------------------------------------------------- */
 /* Fill the derived values of every leaf and write its stepk and maxk (d_info[2*(s*L+l)]).
  * Reference: the leaf constructors and stepK()/maxK() (SBGaussian.cpp:55-89,

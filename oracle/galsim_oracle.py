@@ -1349,7 +1349,7 @@ def uniform01(rng):
     return rng() * (1. / 4294967296.)
 
 
-class OGaussian(object):
+class ONormal(object):
     """boost 1.48 normal_distribution: Box-Muller pairs, cos first (normal_distribution.hpp:153-175)."""
 
     def __init__(self, mean=0., sigma=1.):
@@ -1429,7 +1429,7 @@ class OPoissonDeviate(object):
             self.mean = mean
             if mean > float(1 << 30) or mean == 0.:
                 if self.gd is None:
-                    self.gd = OGaussian(mean, math.sqrt(mean))
+                    self.gd = ONormal(mean, math.sqrt(mean))
                 else:
                     self.gd.mean, self.gd.sigma = mean, math.sqrt(mean)
                 self.use_gd = True
@@ -1444,7 +1444,7 @@ class OPoissonDeviate(object):
 def gaussian_noise(image, rng, sigma):
     """GaussianNoise._applyTo (noise.py:259-263): N(0, sigma) per pixel in row-major order,
     cast to the image dtype and added."""
-    g = OGaussian(0., sigma)
+    g = ONormal(0., sigma)
     noise = np.array([g(rng) for _ in range(image.size)]).reshape(image.shape)
     image += noise.astype(image.dtype)
     return image
@@ -1501,7 +1501,7 @@ def ccd_noise(image, rng, sky_level=0., gain=1., read_noise=0.):
         _poisson_fill(noise, rng)
         noise /= gain
     if read_noise > 0.:
-        g = OGaussian(0., read_noise / gain if gain > 0. else read_noise)
+        g = ONormal(0., read_noise / gain if gain > 0. else read_noise)
         flat = noise.reshape(-1)
         for i in range(flat.size):
             flat[i] += g(rng)

@@ -25,6 +25,7 @@
 #include "SBGaussian.h"
 #include "SBInterpolatedImage.h"
 #include "Interpolant.h"
+#include "Random.h"
 #include "SBKolmogorov.h"
 #include "SBMoffat.h"
 #include "SBSersic.h"
@@ -134,6 +135,31 @@ int gsref_ii_draw_k(void* h, double* kimage, int xmin, int xmax, int ymin, int y
         if (jac) std::memcpy(j, jac, sizeof(j));
         ii->sb->drawK(view(reinterpret_cast<std::complex<double>*>(kimage), xmin, xmax, ymin, ymax),
                       dk, jac ? j : nullptr);
+        return 0;
+    } catch (std::exception& e) { g_err = e.what(); return -1; }
+}
+
+// CCDNoise._applyTo (galsim/noise.py:463-486) on a float64 image with the reference's
+// deviates: Poisson in electrons from a fresh BaseDeviate(seed), then the Gaussian read noise
+// from the same stream (for the CPU baseline of the noise stage).
+int gsref_ccd_noise(double* img, long long n, long seed, double sky, double gain, double read_noise)
+{
+    try {
+        BaseDeviate rng(seed);
+        PoissonDeviate pd(rng, 1.);
+        for (long long i = 0; i < n; ++i) {
+            double v = img[i] + sky;
+            v *= gain;
+            img[i] = v < 0. ? 0. : v;
+        }
+        pd.generateFromExpectation(n, img);
+        for (long long i = 0; i < n; ++i) img[i] /= gain;
+        if (read_noise > 0.) {
+            GaussianDeviate gd(rng, 0., read_noise / gain);
+            gd.clearCache();
+            gd.addGenerate(n, img);
+        }
+        for (long long i = 0; i < n; ++i) img[i] -= sky;
         return 0;
     } catch (std::exception& e) { g_err = e.what(); return -1; }
 }

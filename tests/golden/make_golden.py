@@ -328,6 +328,69 @@ def main_interp(ref_root):
     print('wrote', os.path.join(HERE, 'reference_interp.npz'), len(out), 'arrays')
 
 
+# Noise: the reference's addNoise on seeded images.  Inputs are drawn by the reference (a bright
+# sheared Sersic for Poisson means from 0 to a few thousand, covering the inversion and PTRD
+# branches) and stored with the outputs.
+NOISE_CASES = [
+    # (name, kind, image source, dtype, seed, params)
+    ('gauss_zero_f4', 'gauss', 'zero', 'f4', 5, dict(sigma=3.)),
+    ('gauss_gal_f8', 'gauss', 'gal', 'f8', 123, dict(sigma=0.7)),
+    ('poisson_gal_f4_sky', 'poisson', 'gal', 'f4', 77, dict(sky_level=12.3)),
+    ('poisson_gal_f8', 'poisson', 'gal', 'f8', 78, dict(sky_level=0.)),
+    ('ccd_gal_f4', 'ccd', 'gal', 'f4', 91, dict(sky_level=35.5, gain=1.7, read_noise=4.4)),
+    ('ccd_gal_f8_gain0', 'ccd', 'gal', 'f8', 92, dict(sky_level=20., gain=0., read_noise=3.)),
+    ('ccd_odd_f4', 'ccd', 'odd', 'f4', 93, dict(sky_level=5.25, gain=2.5, read_noise=0.)),
+]
+NOISE_BATCH_SEEDS = [1001, 1002, 1003, 1004]
+
+
+def noise_input(galsim, src, dtype):
+    if src == 'zero':
+        return galsim.Image(17, 13, dtype=dtype, init_value=0.)
+    if src == 'odd':
+        return galsim.Gaussian(sigma=0.4, flux=3e3).drawImage(nx=31, ny=27, scale=0.2, dtype=dtype)
+    gal = galsim.Convolve(galsim.Sersic(n=2.5, half_light_radius=0.6, flux=2e5).shear(g1=0.2, g2=-0.1),
+                          galsim.Moffat(beta=3., fwhm=0.7))
+    return gal.drawImage(nx=48, ny=40, scale=0.2, dtype=dtype)
+
+
+def make_noise(galsim, kind, seed, p):
+    rng = galsim.BaseDeviate(seed)
+    if kind == 'gauss':
+        return galsim.GaussianNoise(rng, **p)
+    if kind == 'poisson':
+        return galsim.PoissonNoise(rng, **p)
+    return galsim.CCDNoise(rng, **p)
+
+
+def main_noise(ref_root):
+    from ref_import import import_reference_galsim
+    galsim = import_reference_galsim(ref_root)
+    out = {}
+    for name, kind, src, dt, seed, p in NOISE_CASES:
+        im = noise_input(galsim, src, np.dtype(dt).type)
+        out['in_' + name] = im.array.copy()
+        im.addNoise(make_noise(galsim, kind, seed, p))
+        out['out_' + name] = im.array.copy()
+    # one stream used twice: the second image continues where the first ended
+    rng = galsim.BaseDeviate(4242)
+    a = galsim.ImageF(9, 7, init_value=0.)
+    b = galsim.ImageF(10, 5, init_value=0.)
+    a.addNoise(galsim.GaussianNoise(rng, sigma=1.))
+    b.addNoise(galsim.PoissonNoise(rng, sky_level=3.5))
+    out['stream_a'] = a.array.copy()
+    out['stream_b'] = b.array.copy()
+    # a stamp batch with one seed per stamp (the config layer's per-object seeding)
+    gal = galsim.Convolve(galsim.Exponential(half_light_radius=0.5, flux=5e3), galsim.Moffat(beta=3., fwhm=0.7))
+    for i, seed in enumerate(NOISE_BATCH_SEEDS):
+        im = gal.drawImage(nx=32, ny=32, scale=0.2)
+        out['batch_in_%d' % i] = im.array.copy()
+        im.addNoise(galsim.CCDNoise(galsim.BaseDeviate(seed), sky_level=50., gain=1.3, read_noise=5.))
+        out['batch_out_%d' % i] = im.array.copy()
+    np.savez_compressed(os.path.join(HERE, 'reference_noise.npz'), **out)
+    print('wrote', os.path.join(HERE, 'reference_noise.npz'), len(out), 'arrays')
+
+
 def main(ref_root):
     from ref_import import import_reference_galsim
     galsim = import_reference_galsim(ref_root)
@@ -381,6 +444,8 @@ if __name__ == '__main__':
         main_grad(root)
     elif '--interp-only' in sys.argv:
         main_interp(root)
+    elif '--noise-only' in sys.argv:
+        main_noise(root)
     elif '--config-only' in sys.argv:
         main_config(root)
     else:
@@ -390,3 +455,4 @@ if __name__ == '__main__':
         main_grad(root)
         main_config(root)
         main_interp(root)
+        main_noise(root)

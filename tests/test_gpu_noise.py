@@ -1,0 +1,88 @@
+"""GPU noise (gsb_add_noise through galsim_b200.Image.addNoise and StampBatch.addNoise) against
+fixtures made by the reference and against the oracle.
+
+The integer Poisson draws and the stream positions must agree exactly; the Gaussian deviates
+go through CUDA's FP64 log / cos / sin, which may differ from the host's in the last bit, so
+float64 results are held to 1e-13 relative and float32 results to one unit in the last place
+(in practice they are bit-identical)."""
+import numpy as np
+import pytest
+
+import galsim_b200 as galsim
+import galsim_oracle as O
+import make_golden as MG
+import specs
+
+pytestmark = pytest.mark.gpu
+GOLD = np.load(specs.HERE + '/reference_noise.npz')
+torch = pytest.importorskip('torch')
+
+
+def product_noise(kind, seed, p):
+    rng = galsim.BaseDeviate(seed)
+    if kind == 'gauss':
+        return galsim.GaussianNoise(rng, **p)
+    if kind == 'poisson':
+        return galsim.PoissonNoise(rng, **p)
+    return galsim.CCDNoise(rng, **p)
+
+
+def assert_close(got, ref):
+    assert got.dtype == ref.dtype
+    if ref.dtype == np.float32:
+        ulp = np.spacing(np.abs(ref).astype(np.float32))
+        assert np.all(np.abs(got.astype(np.float64) - ref) <= ulp), np.abs(got - ref).max()
+    else:
+        assert np.allclose(got, ref, rtol=1e-13, atol=1e-13), np.abs(got - ref).max()
+
+
+@pytest.mark.parametrize('case', MG.NOISE_CASES, ids=[c[0] for c in MG.NOISE_CASES])
+def test_image_add_noise_vs_reference(case):
+    name, kind, src, dt, seed, p = case
+    im = galsim.Image(GOLD['in_' + name].copy())
+    im.addNoise(product_noise(kind, seed, p))
+    assert_close(im.array, GOLD['out_' + name])
+
+
+def test_stream_continues_across_uses():
+    rng = galsim.BaseDeviate(4242)
+    a = galsim.ImageF(9, 7, init_value=0.)
+    b = galsim.ImageF(10, 5, init_value=0.)
+    a.addNoise(galsim.GaussianNoise(rng, sigma=1.))
+    assert rng._stream.used == 64            # 63 deviates use 32 pairs
+    b.addNoise(galsim.PoissonNoise(rng, sky_level=3.5))
+    assert_close(a.array, GOLD['stream_a'])
+    assert_close(b.array, GOLD['stream_b'])
+
+
+def test_stamp_batch_with_per_stamp_seeds_vs_reference():
+    from galsim_b200.batch import StampBatch
+    ins = [GOLD['batch_in_%d' % i] for i in range(len(MG.NOISE_BATCH_SEEDS))]
+    dev = galsim._lib.Device.torch_device()
+    flat = torch.as_tensor(np.concatenate([a.ravel() for a in ins]), device=dev)
+    n = np.array([a.size for a in ins])
+    offsets = np.concatenate([[0], np.cumsum(n)[:-1]])
+    ny = np.array([a.shape[0] for a in ins])
+    nx = np.array([a.shape[1] for a in ins])
+    sb = StampBatch(flat, offsets, nx, ny, None, None, None, None, None, np.float32, 0.2, None)
+    used = sb.addNoise(galsim.CCDNoise(sky_level=50., gain=1.3, read_noise=5.), seeds=MG.NOISE_BATCH_SEEDS)
+    assert np.all(used > 2 * n)
+    for i in range(len(ins)):
+        assert_close(sb.array(i), GOLD['batch_out_%d' % i])
+
+
+def test_many_blocks_and_odd_counts_vs_oracle():
+    """Streams crossing many 624-draw blocks, odd pixel counts (a pair split across blocks)
+    and a skipped start."""
+    for seed, shape, skip in ((31, (129, 127), 0), (32, (40, 33), 623), (33, (11, 7), 1247)):
+        ref = np.zeros(shape, np.float64)
+        rng = O.base_deviate(seed)
+        for _ in range(skip):
+            rng()
+        O.gaussian_noise(ref, rng, 2.5)
+        r = galsim.BaseDeviate(seed)
+        r.discard(skip)
+        im = galsim.ImageD(np.zeros(shape))
+        im.addNoise(galsim.GaussianNoise(r, sigma=2.5))
+        assert np.allclose(im.array, ref, rtol=1e-13, atol=1e-13), (seed, np.abs(im.array - ref).max())
+        assert r._stream.used == skip + 2 * ((ref.size + 1) // 2)
