@@ -88,7 +88,7 @@ def lib():
             'gsb_sersic_tables_info': (i, [vp, vp, i, vp]),
             'gsb_images_build': (i, [vp, i, vp, vp, ctypes.POINTER(GSParamsC), vp]),
             'gsb_images_info': (i, [vp, vp, i, vp]),
-            'gsb_add_noise': (i, [i, vp, vp, i, vp, i, vp, vp, vp]),
+            'gsb_add_noise': (i, [i, vp, vp, i, i, vp, i, vp, vp, vp]),
             'gsb_adjoint_grad_count': (i, [ctypes.POINTER(TemplateC)]),
             'gsb_adjoint_workspace_size': (sz, [i, i, i]),
             'gsb_adjoint_images': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp,

@@ -14,13 +14,17 @@
 //     of W. Hoermann (Insurance: Mathematics and Economics 12, 1993), one or more draws each;
 //     PoissonDeviate switches to a normal with sigma = sqrt(mean) above 2^30.
 //
-// One warp per stamp.  The warp holds the 624-word state in shared memory and regenerates it
+// One warp per stamp holds the 624-word state in shared memory and regenerates it
 // cooperatively (the twist in 32-word chunks, whose dependences span 227 and 397 words).
 // Gaussian pairs are independent once their two words are known, so the lanes take consecutive
-// pairs of each block; Poisson draws consume a data-dependent number of words, so the warp
-// runs them in lockstep (every lane computes the same draw) and only the twists are shared.
+// pairs of each block.  Poisson draws consume a data-dependent number of words; the warp draws
+// 32 pixels at a time speculatively and keeps the prefix whose stream positions were right
+// (pass 2, between a parallel pass for the expectations and a pass for the read noise and the
+// cast).
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <algorithm>
 
 #include "gsb_internal.cuh"
 
@@ -66,37 +70,39 @@ __device__ void mt_twist(uint32_t* x, int lane)
     __syncwarp();
 }
 
-// BaseDeviate(seed): mt11213b(seed), two draws discarded, the third seeds the mt19937
-// (lane 0 runs the sequential recurrences; the result is left in x with the position at the
-// end of the block, i.e. the first draw twists).
+// BaseDeviate(seed): mt11213b(seed), two draws discarded, the third seeds the mt19937; the
+// state is left at the end of its block, so the first draw twists.  Sequential, one thread.
+__device__ void mt_seed_body(uint32_t* x, long long seed)
+{
+    // mt11213b: w 32, n 351, m 175, r 19, a 0xccab8ee7, tempering (11, 7 0x31b6ab00,
+    // 15 0xffe50000, 17); the first 351 words of the buffer serve as its state
+    constexpr int n = 351, m = 175;
+    uint32_t* a = x;
+    a[0] = uint32_t(seed);
+    for (int i = 1; i < n; ++i) a[i] = 1812433253u * (a[i - 1] ^ (a[i - 1] >> 30)) + uint32_t(i);
+    uint32_t out = 0;
+    for (int k = 0; k < 3; ++k) {    // draws 0 and 1 are discarded
+        // only the first three words of the twisted state are needed: x'[k] = x[k+m] ^ mix(x[k], x[k+1])
+        const uint32_t y = (a[k] & 0xfff80000u) | (a[k + 1] & 0x0007ffffu);
+        uint32_t z = a[k + m] ^ (y >> 1) ^ ((a[k + 1] & 1u) * 0xccab8ee7u);
+        z ^= z >> 11;
+        z ^= (z << 7) & 0x31b6ab00u;
+        z ^= (z << 15) & 0xffe50000u;
+        z ^= z >> 17;
+        out = z;
+    }
+    x[0] = out;
+    for (int i = 1; i < kMtN; ++i) x[i] = 1812433253u * (x[i - 1] ^ (x[i - 1] >> 30)) + uint32_t(i);
+    if ((x[0] & 0x80000000u) == 0) {
+        bool zero = true;
+        for (int i = 1; i < kMtN && zero; ++i) zero = x[i] == 0;
+        if (zero) x[0] = 0x80000000u;
+    }
+}
+
 __device__ void mt_seed(uint32_t* x, long long seed, int lane)
 {
-    if (lane == 0) {
-        // mt11213b: w 32, n 351, m 175, r 19, a 0xccab8ee7, tempering (11, 7 0x31b6ab00,
-        // 15 0xffe50000, 17)
-        constexpr int n = 351, m = 175;
-        uint32_t* a = x;     // the first 351 words of the buffer serve as its state
-        a[0] = uint32_t(seed);
-        for (int i = 1; i < n; ++i) a[i] = 1812433253u * (a[i - 1] ^ (a[i - 1] >> 30)) + uint32_t(i);
-        uint32_t out = 0;
-        for (int k = 0; k < 3; ++k) {    // draws 0 and 1 are discarded
-            // only the first three words are needed after the twist: x'[k] = x[k+m] ^ mix(x[k], x[k+1])
-            const uint32_t y = (a[k] & 0xfff80000u) | (a[k + 1] & 0x0007ffffu);
-            uint32_t z = a[k + m] ^ (y >> 1) ^ ((a[k + 1] & 1u) * 0xccab8ee7u);
-            z ^= z >> 11;
-            z ^= (z << 7) & 0x31b6ab00u;
-            z ^= (z << 15) & 0xffe50000u;
-            z ^= z >> 17;
-            out = z;
-        }
-        x[0] = out;
-        for (int i = 1; i < kMtN; ++i) x[i] = 1812433253u * (x[i - 1] ^ (x[i - 1] >> 30)) + uint32_t(i);
-        if ((x[0] & 0x80000000u) == 0) {
-            bool zero = true;
-            for (int i = 1; i < kMtN && zero; ++i) zero = x[i] == 0;
-            if (zero) x[0] = 0x80000000u;
-        }
-    }
+    if (lane == 0) mt_seed_body(x, seed);
     __syncwarp();
 }
 
@@ -117,6 +123,7 @@ struct WarpStream {
         return w;
     }
     __device__ double uniform() { return double(next()) * (1. / 4294967296.); }
+    __device__ bool ok() const { return true; }
     __device__ void skip(long long n)
     {
         while (n > 0) {
@@ -200,8 +207,9 @@ __device__ __forceinline__ double log_factorial_small(int k)
     return r;
 }
 
-// One Poisson draw with the warp's stream (all lanes in lockstep).
-__device__ double poisson_draw(WarpStream& st, double mean)
+// One Poisson draw from the stream.
+template <typename Stream>
+__device__ double poisson_draw(Stream& st, double mean)
 {
     if (mean < 10.) {
         double p = exp(-mean);
@@ -209,7 +217,7 @@ __device__ double poisson_draw(WarpStream& st, double mean)
         double u = st.uniform();
         // ends once the cumulative probability reaches u <= 1 - 2^-32 (x well below 100 for
         // mean < 10); the bound only guards against a non-finite mean
-        while (u > p && x < 1000.) {
+        while (u > p && x < 1000. && st.ok()) {
             u = u - p;
             x += 1.;
             p = mean * p / x;
@@ -222,6 +230,7 @@ __device__ double poisson_draw(WarpStream& st, double mean)
     const double inv_alpha = 1.1239 + 1.1328 / (b - 3.4);
     const double v_r = 0.9277 - 3.6224 / (b - 2);
     for (int iter = 0; iter < (1 << 20); ++iter) {
+        if (!st.ok()) return 0.;
         double u;
         double v = st.uniform();
         if (v <= 0.86 * v_r) {
@@ -259,7 +268,7 @@ struct NoiseArgs {
     void* image;
     int dtype;
     double* scratch;       // FP64 value per pixel (Poisson / CCD), indexed like the image
-    long long* used;
+    long long* used;       // draws used per stamp (Poisson pass -> read-noise pass)
 };
 
 // The cast back into the image and the sky bookkeeping of PoissonNoise / CCDNoise._applyTo:
@@ -274,81 +283,9 @@ __device__ __forceinline__ T finish_pixel(double w, const gsb_noise_params& p)
     return out;
 }
 
+// GaussianNoise: one warp per stamp, the deviates added to the pixels in the image type.
 template <typename T>
-__device__ void noise_stamp(const NoiseArgs& a, const gsb_noise_stamp& sp, WarpStream& st)
-{
-    T* img = pix_ptr<T>(a.image, sp.offset);
-    const long long n = sp.npix;
-    const int lane = st.lane;
-    if (a.kind == GSB_NOISE_GAUSSIAN) {
-        gaussian_run(st, n, a.p.sigma, [&](long long j, double d) { img[j] = img[j] + T(d); });
-        return;
-    }
-    double* w = a.scratch + sp.offset;
-    const bool ccd = a.kind == GSB_NOISE_CCD;
-    const double gain = ccd ? a.p.gain : 1.;
-    // expectation per pixel (all lanes)
-    for (long long j = lane; j < n; j += 32) {
-        double v = double(img[j]);
-        if (a.p.sky_level != 0.) v += a.p.sky_level;
-        if (!ccd || gain > 0.) {
-            if (ccd) v *= gain;
-            if (v < 0.) v = 0.;
-        }
-        w[j] = v;
-    }
-    __syncwarp();
-    if (!ccd || gain > 0.) {
-        // the draws in pixel order, every lane computing the same value (PoissonDeviate
-        // generateFromExpectation with its mean switching; the normal branch above 2^30 keeps
-        // its pair cache while the mean is unchanged)
-        double cur_mean = 1.;
-        bool use_gd = false, gd_valid = false;
-        double gd_rho = 0., gd_r1 = 0.;
-        const double kMaxPoisson = double(1 << 30);
-        for (long long j = 0; j < n; ++j) {
-            double v = w[j];
-            if (v > 0.) {
-                if (v != cur_mean) {
-                    cur_mean = v;
-                    if (v > kMaxPoisson) {
-                        use_gd = true;
-                    } else {
-                        use_gd = false;
-                        gd_valid = false;
-                    }
-                }
-                if (use_gd) {
-                    const double sg = sqrt(v);
-                    if (!gd_valid) {
-                        gd_r1 = st.uniform();
-                        const double r2 = st.uniform();
-                        gd_rho = sqrt(-2. * log(1. - r2));
-                        gd_valid = true;
-                        v = gd_rho * cos(kPi2 * gd_r1) * sg + v;
-                    } else {
-                        gd_valid = false;
-                        v = gd_rho * sin(kPi2 * gd_r1) * sg + v;
-                    }
-                } else {
-                    v = poisson_draw(st, v);
-                }
-            }
-            if (ccd) v /= gain;
-            __syncwarp();
-            if (lane == 0) w[j] = v;
-            __syncwarp();
-        }
-    }
-    if (ccd && a.p.read_noise > 0.) {
-        const double sigma = gain > 0. ? a.p.read_noise / gain : a.p.read_noise;
-        gaussian_run(st, n, sigma, [&](long long j, double d) { w[j] += d; });
-    }
-    __syncwarp();
-    for (long long j = lane; j < n; j += 32) img[j] = finish_pixel<T>(w[j], a.p);
-}
-
-__global__ void __launch_bounds__(kNoiseWarps * 32) noise_kernel(const __grid_constant__ NoiseArgs a)
+__global__ void __launch_bounds__(kNoiseWarps * 32) gauss_kernel(const __grid_constant__ NoiseArgs a)
 {
     __shared__ uint32_t state[kNoiseWarps][kMtN];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -358,15 +295,318 @@ __global__ void __launch_bounds__(kNoiseWarps * 32) noise_kernel(const __grid_co
     WarpStream st{state[warp], kMtN, 0, lane};
     mt_seed(st.x, sp.seed, lane);
     st.skip(sp.skip);
-    if (a.dtype == GSB_F32) noise_stamp<float>(a, sp, st);
-    else noise_stamp<double>(a, sp, st);
-    if (lane == 0 && a.used) a.used[s] = st.used;     // words consumed since seeding
+    T* img = pix_ptr<T>(a.image, sp.offset);
+    gaussian_run(st, sp.npix, a.p.sigma, [&](long long j, double d) { img[j] = img[j] + T(d); });
+    if (lane == 0 && a.used) a.used[s] = st.used;      // draws consumed since seeding
+}
+
+// Poisson / CCD pass 1: the expectation of every pixel (image + sky, in electrons, clipped).
+// grid = (chunks, stamps).
+template <typename T>
+__global__ void expect_kernel(const __grid_constant__ NoiseArgs a)
+{
+    const gsb_noise_stamp sp = a.stamps[blockIdx.y];
+    const T* img = pix_ptr<T>(a.image, sp.offset);
+    double* w = a.scratch + sp.offset;
+    const bool ccd = a.kind == GSB_NOISE_CCD;
+    const double gain = ccd ? a.p.gain : 1.;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < sp.npix;
+         j += (long long)gridDim.x * blockDim.x) {
+        double v = double(img[j]);
+        if (a.p.sky_level != 0.) v += a.p.sky_level;
+        if (!ccd || gain > 0.) {
+            if (ccd) v *= gain;
+            if (v < 0.) v = 0.;
+        }
+        w[j] = v;
+    }
+}
+
+// Poisson / CCD pass 2: the draws in pixel order, as PoissonDeviate generateFromExpectation
+// (with its mean switching and the normal branch above 2^30, whose pair cache persists while
+// the mean is unchanged).  The stream is sequential -- a draw takes a data-dependent number of
+// words -- but most draws take exactly one (inversion always; PTRD when its first uniform
+// lands in the immediate-acceptance region), so the warp speculates: each lane draws one pixel
+// of the next 32 from the position it would have if every earlier nonzero pixel took one word,
+// and the pixels up to and including the first one that took a different count are committed
+// (their starting positions were right).  Words come from a shared window of two 624-word
+// blocks; a draw that would run past it, and the normal branch, are done by the whole warp in
+// order.  The result is the sequential stream exactly.
+struct Window {
+    uint32_t* x;        // mt19937 state of the last generated block
+    uint32_t* win;      // tempered words of blocks [wstart / 624, wstart / 624 + 2)
+    long long wstart;
+    int lane;
+
+    __device__ void gen(uint32_t* dst)
+    {
+        mt_twist(x, lane);
+        for (int j = lane; j < kMtN; j += 32) dst[j] = mt_temper(x[j]);
+        __syncwarp();
+    }
+    __device__ void advance()
+    {
+        for (int j = lane; j < kMtN; j += 32) win[j] = win[kMtN + j];
+        __syncwarp();
+        gen(win + kMtN);
+        wstart += kMtN;
+    }
+};
+
+// A lane's speculative reader of the window.
+struct LaneSource {
+    const uint32_t* win;
+    int pos, end;
+    int count;
+    bool overflow;
+    __device__ double uniform()
+    {
+        if (pos >= end) { overflow = true; return 0.5; }
+        ++count;
+        return double(win[pos++]) * (1. / 4294967296.);
+    }
+    __device__ bool ok() const { return !overflow; }
+};
+
+// The whole warp reading in order, advancing the window as needed (collective).
+struct WindowStream {
+    Window* w;
+    long long pos;
+    __device__ double uniform()
+    {
+        while (pos >= w->wstart + 2 * kMtN) w->advance();
+        const uint32_t v = w->win[pos - w->wstart];
+        ++pos;
+        return double(v) * (1. / 4294967296.);
+    }
+    __device__ bool ok() const { return true; }
+};
+
+// Exclusive prefix sum and total over the warp.
+__device__ __forceinline__ int warp_exclusive_sum(int v, int lane)
+{
+    int x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += y;
+    }
+    return x - v;
+}
+
+__device__ __forceinline__ int warp_sum(int v)
+{
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+    return v;
+}
+
+constexpr int kPoissonWarps = 4;      // 7.3 KB of state and window per warp
+
+__global__ void __launch_bounds__(kPoissonWarps * 32) poisson_kernel(const __grid_constant__ NoiseArgs a)
+{
+    __shared__ uint32_t state[kPoissonWarps][kMtN];
+    __shared__ uint32_t window[kPoissonWarps][2 * kMtN];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s = blockIdx.x * kPoissonWarps + warp;
+    if (s >= a.n_stamps) return;
+    const gsb_noise_stamp sp = a.stamps[s];
+    const bool ccd = a.kind == GSB_NOISE_CCD;
+    const double gain = ccd ? a.p.gain : 1.;
+    if (ccd && !(gain > 0.)) {
+        if (lane == 0) a.used[s] = sp.skip;
+        return;
+    }
+    mt_seed(state[warp], sp.seed, lane);
+    Window W{state[warp], window[warp], 0, lane};
+    const long long skip_blocks = sp.skip / kMtN;
+    for (long long b = 0; b < skip_blocks; ++b) mt_twist(W.x, lane);
+    W.wstart = skip_blocks * kMtN;
+    W.gen(W.win);
+    W.gen(W.win + kMtN);
+    double* w = a.scratch + sp.offset;
+    const long long n = sp.npix;
+    const double kMaxPoisson = double(1 << 30);
+    long long p0 = 0, base = sp.skip;
+    // normal-branch state (PoissonDeviate above 2^30)
+    double cur_mean = 1.;
+    bool gd_exists = false, gd_valid = false;
+    double gd_rho = 0., gd_r1 = 0.;
+    while (p0 < n) {
+        while (base >= W.wstart + kMtN) W.advance();
+        const long long j = p0 + lane;
+        const bool valid = j < n;
+        const double mean = valid ? w[j] : 0.;
+        const bool nz = valid && mean > 0.;
+        const bool special = nz && mean > kMaxPoisson;
+        // Assumed word counts: 1 for a draw whose first word lands in the immediate region
+        // (inversion always), 2 for the others (their common case), 0 for zero means.  The
+        // positions follow from the counts and the counts from the words at the positions, so
+        // a few rounds find the consistent assignment (the prefix that matters converges first).
+        int guess = nz ? 1 : 0;
+        int offs = 0;
+        bool imm = true;
+        double smu = 0., b = 0., v_r = 0., v0 = 0.;
+        if (nz && !special && !(mean < 10.)) {
+            smu = sqrt(mean);
+            b = 0.931 + 2.53 * smu;
+            v_r = 0.9277 - 3.6224 / (b - 2);
+        }
+        for (int round = 0; round < 6; ++round) {
+            offs = warp_exclusive_sum(guess, lane);
+            int g2 = 0;
+            if (nz) {
+                if (special) {
+                    g2 = 1;
+                } else {
+                    v0 = double(W.win[int(base - W.wstart) + offs]) * (1. / 4294967296.);
+                    imm = mean < 10. || v0 <= 0.86 * v_r;
+                    g2 = imm ? 1 : 2;
+                }
+            }
+            const bool same = __all_sync(0xffffffffu, g2 == guess);
+            guess = g2;
+            if (same) break;
+        }
+        offs = warp_exclusive_sum(guess, lane);
+        // every lane's draw at its assumed position (all in parallel)
+        double value = mean;
+        int count = 0;
+        bool bad = special;
+        if (nz && !special) {
+            const int wpos = int(base - W.wstart) + offs;
+            v0 = double(W.win[wpos]) * (1. / 4294967296.);
+            if (mean < 10.) {
+                double pp = exp(-mean), x = 0., u = v0;
+                while (u > pp && x < 1000.) {
+                    u = u - pp;
+                    x += 1.;
+                    pp = mean * pp / x;
+                }
+                value = x;
+                count = 1;
+            } else if (v0 <= 0.86 * v_r) {
+                const double a_ = -0.059 + 0.02483 * b;
+                const double u = v0 / v_r - 0.43;
+                value = floor((2 * a_ / (0.5 - fabs(u)) + b) * u + mean + 0.445);
+                count = 1;
+            } else {
+                LaneSource src{W.win, wpos, 2 * kMtN, 0, false};
+                value = poisson_draw(src, mean);
+                count = src.count;
+                bad = src.overflow;
+            }
+        }
+        // the prefix whose positions are right: up to the first lane whose count differs from
+        // its assumption (that lane's own start is right, so it is kept unless it must be
+        // redone in order: the normal branch, or a draw past the window)
+        const bool fail = valid && (bad || count != guess);
+        const unsigned fmask = __ballot_sync(0xffffffffu, fail);
+        const int nvalid = int(min((long long)32, n - p0));
+        const int f = fmask ? __ffs(fmask) - 1 : nvalid;
+        const bool f_bad = fmask ? bool(__shfl_sync(0xffffffffu, bad ? 1 : 0, f)) : false;
+        const int ncommit = f + ((fmask && !f_bad) ? 1 : 0);
+        const bool commit = lane < ncommit && valid;
+        if (commit && nz) w[j] = ccd ? value / gain : value;
+        long long used_words = warp_sum(lane < ncommit ? count : 0);
+        // a committed ordinary draw replaces the normal branch's deviate (its pair cache goes)
+        const unsigned pdmask = __ballot_sync(0xffffffffu, commit && nz);
+        if (pdmask) {
+            const int last = 31 - __clz(pdmask);
+            cur_mean = __shfl_sync(0xffffffffu, mean, last);
+            gd_exists = false;
+            gd_valid = false;
+        }
+        base += used_words;
+        p0 += ncommit;
+        __syncwarp();
+        if (fmask && f_bad) {
+            // the pixel at p0 in order by the whole warp: the normal branch, or a draw that ran
+            // past the window
+            const double m = w[p0];
+            WindowStream ws{&W, base};
+            double v;
+            if (m > kMaxPoisson) {
+                if (m != cur_mean) {
+                    cur_mean = m;
+                    if (!gd_exists) { gd_exists = true; gd_valid = false; }
+                }
+                const double sg = sqrt(m);
+                if (!gd_valid) {
+                    gd_r1 = ws.uniform();
+                    const double r2 = ws.uniform();
+                    gd_rho = sqrt(-2. * log(1. - r2));
+                    gd_valid = true;
+                    v = gd_rho * cos(kPi2 * gd_r1) * sg + m;
+                } else {
+                    gd_valid = false;
+                    v = gd_rho * sin(kPi2 * gd_r1) * sg + m;
+                }
+            } else {
+                v = poisson_draw(ws, m);
+                cur_mean = m;
+                gd_exists = false;
+                gd_valid = false;
+            }
+            __syncwarp();
+            if (lane == 0) w[p0] = ccd ? v / gain : v;
+            __syncwarp();
+            base = ws.pos;
+            ++p0;
+        }
+    }
+    if (lane == 0) a.used[s] = base;
+}
+
+// Poisson / CCD pass 3: the CCD read noise (a fresh Gaussian pair cache continuing the stream
+// where the draws ended) and the cast into the image.  One warp per stamp.
+template <typename T>
+__global__ void __launch_bounds__(kNoiseWarps * 32) finish_kernel(const __grid_constant__ NoiseArgs a)
+{
+    __shared__ uint32_t state[kNoiseWarps][kMtN];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s = blockIdx.x * kNoiseWarps + warp;
+    if (s >= a.n_stamps) return;
+    const gsb_noise_stamp sp = a.stamps[s];
+    double* w = a.scratch + sp.offset;
+    const bool ccd = a.kind == GSB_NOISE_CCD;
+    if (ccd && a.p.read_noise > 0.) {
+        WarpStream st{state[warp], kMtN, 0, lane};
+        mt_seed(st.x, sp.seed, lane);
+        st.skip(a.used[s]);
+        const double sigma = a.p.gain > 0. ? a.p.read_noise / a.p.gain : a.p.read_noise;
+        gaussian_run(st, sp.npix, sigma, [&](long long j, double d) { w[j] += d; });
+        if (lane == 0) a.used[s] = st.used;
+    }
+    __syncwarp();
+    T* img = pix_ptr<T>(a.image, sp.offset);
+    for (long long j = lane; j < sp.npix; j += 32) img[j] = finish_pixel<T>(w[j], a.p);
+}
+
+template <typename T>
+int launch_noise(const NoiseArgs& a, int max_npix, cudaStream_t stream)
+{
+    const int warp_grid = (a.n_stamps + kNoiseWarps - 1) / kNoiseWarps;
+    if (a.kind == GSB_NOISE_GAUSSIAN) {
+        gauss_kernel<T><<<warp_grid, kNoiseWarps * 32, 0, stream>>>(a);
+        GSB_CUDA_CHECK(cudaGetLastError());
+        return GSB_OK;
+    }
+    const int chunks = std::max(1, std::min(64, (max_npix + 255) / 256));
+    expect_kernel<T><<<dim3(chunks, a.n_stamps), 256, 0, stream>>>(a);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    poisson_kernel<<<(a.n_stamps + kPoissonWarps - 1) / kPoissonWarps, kPoissonWarps * 32, 0, stream>>>(a);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    finish_kernel<T><<<warp_grid, kNoiseWarps * 32, 0, stream>>>(a);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    return GSB_OK;
 }
 
 }  // namespace
 
 int add_noise(int kind, const gsb_noise_params* p, const gsb_noise_stamp* d_stamps, int n_stamps,
-              void* d_image, int dtype, double* d_scratch, long long* d_used, cudaStream_t stream)
+              int max_npix, void* d_image, int dtype, double* d_scratch, long long* d_used,
+              cudaStream_t stream)
 {
     if (n_stamps == 0) return GSB_OK;
     NoiseArgs a;
@@ -378,10 +618,7 @@ int add_noise(int kind, const gsb_noise_params* p, const gsb_noise_stamp* d_stam
     a.dtype = dtype;
     a.scratch = d_scratch;
     a.used = d_used;
-    const int grid = (n_stamps + kNoiseWarps - 1) / kNoiseWarps;
-    noise_kernel<<<grid, kNoiseWarps * 32, 0, stream>>>(a);
-    GSB_CUDA_CHECK(cudaGetLastError());
-    return GSB_OK;
+    return dtype == GSB_F32 ? launch_noise<float>(a, max_npix, stream) : launch_noise<double>(a, max_npix, stream);
 }
 
 }  // namespace gsb
@@ -389,7 +626,7 @@ int add_noise(int kind, const gsb_noise_params* p, const gsb_noise_stamp* d_stam
 using namespace gsb;
 
 extern "C" int gsb_add_noise(int kind, const gsb_noise_params* p, const gsb_noise_stamp* d_stamps,
-                             int n_stamps, void* d_image, int dtype, double* d_scratch,
+                             int n_stamps, int max_npix, void* d_image, int dtype, double* d_scratch,
                              long long* d_used, void* stream)
 {
     if (!p || n_stamps < 0 || (n_stamps > 0 && (!d_stamps || !d_image)))
@@ -397,8 +634,10 @@ extern "C" int gsb_add_noise(int kind, const gsb_noise_params* p, const gsb_nois
     if (kind < GSB_NOISE_GAUSSIAN || kind > GSB_NOISE_CCD)
         return set_error(GSB_ERR_INVALID, "unknown noise kind");
     if (dtype != GSB_F32 && dtype != GSB_F64) return set_error(GSB_ERR_INVALID, "image dtype must be F32 or F64");
-    if (kind != GSB_NOISE_GAUSSIAN && !d_scratch)
-        return set_error(GSB_ERR_INVALID, "Poisson and CCD noise need the FP64 scratch buffer");
+    if (kind != GSB_NOISE_GAUSSIAN && (!d_scratch || !d_used))
+        return set_error(GSB_ERR_INVALID, "Poisson and CCD noise need the FP64 scratch and the draw counts");
+    if (max_npix < 0) return set_error(GSB_ERR_INVALID, "negative pixel count");
     if (kind == GSB_NOISE_GAUSSIAN && !(p->sigma >= 0.)) return set_error(GSB_ERR_INVALID, "sigma must be >= 0");
-    return add_noise(kind, p, d_stamps, n_stamps, d_image, dtype, d_scratch, d_used, (cudaStream_t)stream);
+    return add_noise(kind, p, d_stamps, n_stamps, max_npix, d_image, dtype, d_scratch, d_used,
+                     (cudaStream_t)stream);
 }

@@ -126,8 +126,9 @@ def _apply(kind, params, flat, offsets, npix, seeds, skips):
         raise GalSimNotImplementedError("noise is applied to float32 / float64 images here")
     scratch = torch.empty(flat.numel() if kind != GAUSSIAN else 1, dtype=torch.float64, device=dev)
     used = torch.empty(B, dtype=torch.int64, device=dev)
-    _lib.check(_lib.lib().gsb_add_noise(kind, ctypes.byref(params), _lib.ptr(d_rec), B, _lib.ptr(flat),
-                                        dt, _lib.ptr(scratch), _lib.ptr(used), _lib.Device.stream()))
+    _lib.check(_lib.lib().gsb_add_noise(kind, ctypes.byref(params), _lib.ptr(d_rec), B,
+                                        int(np.max(npix)) if B else 0, _lib.ptr(flat), dt,
+                                        _lib.ptr(scratch), _lib.ptr(used), _lib.Device.stream()))
     return used.cpu().numpy()
 
 

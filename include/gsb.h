@@ -250,12 +250,16 @@ typedef struct gsb_noise_params {
     int32_t pad;
 } gsb_noise_params;
 
-/* Add noise of `kind` to n_stamps stamps of d_image (GSB_F32 or GSB_F64).  Poisson and CCD
- * noise need d_scratch: one double per pixel, addressed like d_image.  d_used (may be NULL)
- * receives, per stamp, the raw draws consumed since seeding (skip + this call's draws), so a
- * caller can continue the stream.  One warp per stamp; no allocation. */
+/* Add noise of `kind` to n_stamps stamps of d_image (GSB_F32 or GSB_F64); max_npix bounds the
+ * stamps' pixel counts.  Poisson and CCD noise need d_scratch (one double per pixel, addressed
+ * like d_image) and d_used.  d_used (may be NULL for Gaussian noise) receives, per stamp, the raw
+ * draws consumed since seeding (skip + this call's draws), so a caller can continue the stream.
+ * Gaussian: one warp per stamp.  Poisson / CCD: the expectations in parallel, the draws one
+ * thread per stamp (the stream is sequential), then the read noise and the cast one warp per
+ * stamp.  No allocation. */
 int gsb_add_noise(int kind, const gsb_noise_params* p, const gsb_noise_stamp* d_stamps, int n_stamps,
-                  void* d_image, int dtype, double* d_scratch, long long* d_used, void* stream);
+                  int max_npix, void* d_image, int dtype, double* d_scratch, long long* d_used,
+                  void* stream);
 
 /* Leaves -------------------------------------------------------------------------------- */
 /* Fill the derived values of every leaf and write its stepk and maxk (d_info[2*(s*L+l)]).
