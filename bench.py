@@ -231,6 +231,31 @@ def _ref_noise_worker(args):
 NOISE_SKY, NOISE_GAIN, NOISE_READ = 100., 1.5, 5.
 
 
+def run_fits(galsim, st, reps=3):
+    """FITS stage: the multi-extension file image of the main workload's 4096 stamps (one HDU
+    per stamp), assembled on the device by gsb_fits_pack and read back once, against the host
+    writer given the same stamps as host Images (formatting every header and byte-swapping every
+    pixel on the host).  Both end as the bytes of the file; the disk write is not timed."""
+    from galsim_b200 import fits
+    st.fits_bytes()                                    # warm (pinned buffer, header formats)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        dev_bytes = st.fits_bytes()
+    dev_ms = (time.perf_counter() - t0) / reps * 1e3
+    t0 = time.perf_counter()
+    ims = st.images()
+    hl = fits.HDUList()
+    for im in ims:
+        hl.append(fits._image_hdu(im, len(hl) == 0))
+    host_bytes = fits._file_bytes(hl)
+    host_ms = (time.perf_counter() - t0) * 1e3
+    return {'file_bytes': len(dev_bytes), 'device_ms': dev_ms, 'host_ms': host_ms,
+            'device_gb_per_s': len(dev_bytes) / (dev_ms * 1e-3) / 1e9,
+            'identical': dev_bytes == host_bytes,
+            'workload': 'writeMulti file image of the %d stamps (FP32), device pack + one read-back '
+                        'vs host formatting and byte swap from host Images' % len(st)}
+
+
 def run_noise(galsim, dev, st, steps, warmup, cpu=True):
     """Noise stage: CCDNoise(sky 100, gain 1.5 e-/ADU, read noise 5 e-) on every stamp of the
     main workload's batch, stamp i with its own BaseDeviate(1 + i) (the reference's Poisson and
@@ -428,6 +453,18 @@ def gpu_object(galsim, p):
 # Measured DRAM bytes per stamp of the fused draw kernel by FFT size (ncu, 600-stamp case of
 # this workload; profiles/draw_fused_kernel_dram_per_stamp.md).  Larger N scale as N^2.
 DRAM_BYTES_PER_STAMP = {128: 8732., 192: 110406., 256: 18898.}
+
+
+def table_build_launches(n_values, gsp_kvalue_accuracy=1e-5, table_spacing=1.):
+    """Kernel launches of one Sersic table build (gsb_sersic_tables_build): setup, scan init,
+    one (nodes, scan) pair per round of 32 ln k nodes over the table stride, and the finalize.
+    The stride is the node count of the largest n (sersic_stride in csrc/gsb_tables.cu)."""
+    nmax = float(np.max(n_values))
+    kderiv6 = math.exp(math.lgamma(8. * nmax) - math.lgamma(2. * nmax)) / 2304.
+    kmin = (gsp_kvalue_accuracy / kderiv6) ** (1. / 6.)
+    dlogk = table_spacing * math.sqrt(math.sqrt(gsp_kvalue_accuracy / 10.))
+    stride = int((math.log(500.) - (math.log(kmin) - 0.001)) / dlogk) + 4
+    return 3 + 2 * ((stride + 31) // 32)
 
 
 def measured_traffic(N):
@@ -629,8 +666,8 @@ def run_reference(args):
 # GPU arm
 # ---------------------------------------------------------------------------------------------
 def run_stage(args):
-    """Small single-stage runs for profiling (--stage draw | tables | fit | interp): no e2e /
-    CPU legs."""
+    """Small single-stage runs for profiling (--stage draw | tables | fit | interp | noise): no
+    e2e / CPU legs."""
     import torch
     import galsim_b200 as galsim
     from galsim_b200 import _lib
@@ -671,6 +708,13 @@ def run_stage(args):
         e1.record()
         torch.cuda.synchronize()
         print(json.dumps({'stage': 'tables', 'tables': len(n), 'ms_per_build': e0.elapsed_time(e1) / args.steps}))
+        return
+    if args.stage == 'noise':
+        dev = _lib.Device.torch_device()
+        st = galsim.draw_batch(obj, nx=args.nx, ny=args.nx, scale=SCALE, dtype=np.float32)
+        res = run_noise(galsim, dev, st, args.steps, args.warmup, cpu=False)
+        print(json.dumps({'stage': 'noise', 'stamps': len(st), 'ms_per_step': res['ms'],
+                          'mpix_per_s': res['mpix_per_s']}))
         return
     if args.stage == 'interp':
         psf = galsim.InterpolatedImage(galsim.Image(interp_psf_image(galsim), scale=SCALE))
@@ -816,6 +860,8 @@ def run_gpu(args):
                        cpu=(rank == 0 and world == 1 and not args.no_cpu))
              if not args.no_extra else None)
 
+    fits_stage = run_fits(galsim, st) if not args.no_extra else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference_rate(params, budget_s=15.)
@@ -843,7 +889,9 @@ def run_gpu(args):
                          'peak_kind': peak_kind,
                          'kernel': 'draw_fused_kernel, all FFT-size buckets concurrent (one draw-graph replay)',
                          'kernel_ms': k_ms},
-            'gpu_launches': int(args.steps * (nb + 5)),
+            # per step: the Sersic table build, one leaf-prepare launch and one fused draw per
+            # FFT-size bucket
+            'gpu_launches': int(args.steps * (table_build_launches(params[:, 0]) + 1 + nb)),
             'plain_one_stamp_per_launch': {'value': plain_rate, 'unit': 'stamps/s', 'sample': n_plain},
             'fp32_error_vs_fp64': fp32_err,
             'grad_evals': fit,
@@ -851,6 +899,7 @@ def run_gpu(args):
             'large_stamps': large,
             'interp_psf': interp,
             'noise': noise,
+            'fits': fits_stage,
             'clocks': clk.summary(),
         }
         if cpu is not None:
@@ -871,8 +920,8 @@ def main():
                     help='skip the mixed-batch and large-stamp measurements')
     ap.add_argument('--stamps', type=int, default=B_DEFAULT, help='stamps per GPU (leading subset)')
     ap.add_argument('--nx', type=int, default=None, help='fixed stamp size (default: automatic)')
-    ap.add_argument('--stage', default='all', choices=['all', 'draw', 'tables', 'fit', 'interp'],
-                    help="'draw' / 'tables' / 'fit' / 'interp': run only that stage (for profiling)")
+    ap.add_argument('--stage', default='all', choices=['all', 'draw', 'tables', 'fit', 'interp', 'noise'],
+                    help="'draw' / 'tables' / 'fit' / 'interp' / 'noise': run only that stage (for profiling)")
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)

@@ -2,8 +2,9 @@
 
 A drop-in for ``GSObject.drawImage(method='fft')`` and ``drawKImage`` on
 Convolve / Sum / Transform trees of Gaussian, Exponential, Sersic, Moffat, Kolmogorov, Airy,
-Box / Pixel and InterpolatedImage, and the reference's Gaussian / Poisson / CCD noise applied
-on the device.  The host code here mirrors the reference's Python API; every numerical
+Box / Pixel and InterpolatedImage, the reference's Gaussian / Poisson / CCD noise applied
+on the device, and FITS files of Images and stamp batches (galsim_b200.fits; a batch's file
+image is assembled on the device).  The host code here mirrors the reference's Python API; every numerical
 step of drawing (FP64 sizing and Sersic tables, k-space evaluation, Hermitian wrap, inverse
 FFT, crop and flux sum) runs in the hand-written CUDA kernels of libgsb.so, called through
 the C ABI declared in include/gsb.h.  There is no CPU fallback.
@@ -23,6 +24,8 @@ from .interpolant import (Interpolant, Delta, Nearest, SincInterpolant, Linear, 
                           Lanczos, convert_interpolant)
 from .interpolatedimage import InterpolatedImage
 from .noise import BaseDeviate, BaseNoise, GaussianNoise, PoissonNoise, CCDNoise
+from . import fits
+from .fits import FitsHeader
 from .compound import Convolve, Convolution, Add, Sum, Transform, Transformation, _Transform
 from .batch import draw_batch, plan_batch, run_batch, StampBatch
 from ._lib import set_device

@@ -60,6 +60,10 @@ IMAGE_DESC_DTYPE = np.dtype({'names': ['N', 'nx', 'ny', 'x0', 'y0', 'bx0', 'bx1'
                               'offsets': [0, 4, 8, 12, 16, 20, 24, 28, 32, 36, 40, 48, 56, 64, 72],
                               'itemsize': 80})
 
+# gsb_fits_hdu (include/gsb.h)
+FITS_HDU_DTYPE = np.dtype({'names': ['header_src', 'header_len', 'data_src', 'n_elem', 'dst'],
+                           'formats': ['i8'] * 5, 'offsets': [0, 8, 16, 24, 32], 'itemsize': 40})
+
 SERSIC_HEADER = 16
 SH_N, SH_NUSED, SH_FRONT, SH_DA, SH_KSQMIN, SH_KSQMAX, SH_KD2, SH_KD4, SH_HIGHA, SH_HIGHB, \
     SH_MAXK, SH_STEPK, SH_RE, SH_DLOGK, SH_NCAND, SH_STATUS = range(16)
@@ -89,6 +93,8 @@ def lib():
             'gsb_images_build': (i, [vp, i, vp, vp, ctypes.POINTER(GSParamsC), vp]),
             'gsb_images_info': (i, [vp, vp, i, vp]),
             'gsb_add_noise': (i, [i, vp, vp, i, i, vp, i, vp, vp, vp]),
+            'gsb_fits_pack': (i, [vp, i, vp, ctypes.c_longlong, vp, ctypes.c_longlong, i, vp,
+                                  ctypes.c_longlong, vp]),
             'gsb_adjoint_grad_count': (i, [ctypes.POINTER(TemplateC)]),
             'gsb_adjoint_workspace_size': (sz, [i, i, i]),
             'gsb_adjoint_images': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp,

@@ -92,6 +92,86 @@ class StampBatch(object):
         return self.flat[:len(self) * int(self.nx[0] * self.ny[0])].view(
             len(self), int(self.ny[0]), int(self.nx[0]))
 
+    def fits_bytes(self, cube=False):
+        """The FITS file image of every stamp, assembled on the device and read back once:
+        one HDU per stamp (writeMulti; the first is the primary HDU) or one data cube
+        (writeCube; the stamps must share a size).  Each header carries the stamp's BITPIX,
+        NAXISn, GS_XMIN / GS_YMIN and its PixelScale WCS, as fits.py writes them."""
+        import ctypes
+        import torch
+        from . import fits
+        from .bounds import _BoundsI
+        from .wcs import PixelScale
+        B = len(self)
+        if B == 0:
+            raise GalSimValueError("no stamps to write", B)
+        dt = np.dtype(np.float32) if self.flat.dtype == torch.float32 else np.dtype(np.float64)
+        esz = dt.itemsize
+        wcs = PixelScale(self.scale)
+        nx = np.asarray(self.nx, np.int64)
+        ny = np.asarray(self.ny, np.int64)
+        offsets = np.asarray(self.offsets, np.int64)
+        hdrs, index = [], {}
+
+        def header(shape, primary, b):
+            key = (shape, primary, b)
+            if key not in index:
+                cls = fits.PrimaryHDU if primary else fits.ImageHDU
+                hdu = cls(np.empty(shape, dt), fits.image_header_cards(_BoundsI(*b), wcs))
+                index[key] = (sum(len(h) for h in hdrs), len(hdrs))
+                hdrs.append(np.frombuffer(hdu.header_bytes(), np.uint8))
+            return index[key][0], len(hdrs[index[key][1]])
+
+        if cube:
+            if len(set(nx.tolist())) != 1 or len(set(ny.tolist())) != 1:
+                raise GalSimValueError("In writeCube: the stamps have different sizes",
+                                       (sorted(set(nx.tolist())), sorted(set(ny.tolist()))))
+            n1 = int(nx[0] * ny[0])
+            if not np.array_equal(offsets, np.arange(B, dtype=np.int64) * n1):
+                raise GalSimValueError("In writeCube: the stamps are not stored back to back", offsets)
+            b0 = tuple(int(v) for v in self.bounds[0])
+            hs, hl = header((B, int(ny[0]), int(nx[0])), True, b0)
+            recs = [(hs, hl, int(offsets[0]), B * n1)]
+        else:
+            recs = []
+            for i in range(B):
+                b = tuple(int(v) for v in self.bounds[i])
+                hs, hl = header((int(ny[i]), int(nx[i])), i == 0, b)
+                recs.append((hs, hl, int(offsets[i]), int(nx[i] * ny[i])))
+        rec = np.zeros(len(recs), dtype=_lib.FITS_HDU_DTYPE)
+        r = np.asarray(recs, np.int64)
+        rec['header_src'], rec['header_len'], rec['data_src'], rec['n_elem'] = r.T
+        dbytes = (r[:, 3] * esz + fits.BLOCK - 1) // fits.BLOCK * fits.BLOCK
+        sizes = r[:, 1] + dbytes
+        rec['dst'] = np.concatenate(([0], np.cumsum(sizes)[:-1]))
+        total = int(sizes.sum())
+        dev = self.flat.device
+        d_hdr = torch.from_numpy(np.concatenate(hdrs)).to(dev)
+        out = torch.empty(total, dtype=torch.uint8, device=dev)
+        _lib.check(_lib.lib().gsb_fits_pack(
+            rec.ctypes.data_as(ctypes.c_void_p), len(rec), _lib.ptr(d_hdr), d_hdr.numel(),
+            _lib.ptr(self.flat), self.flat.numel(), _lib.F32 if esz == 4 else _lib.F64,
+            _lib.ptr(out), total, _lib.Device.stream()))
+        host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+        host.copy_(out, non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+        return host.numpy().tobytes()
+
+    def writeMulti(self, file_name, dir=None, clobber=True, compression='auto'):
+        """galsim.fits.writeMulti of every stamp (fits.py:445-527), the file image made on the
+        device (fits_bytes)."""
+        from . import fits
+        file_compress, tile = fits._parse_compression(compression, file_name)
+        fits._no_tiles(tile)
+        fits._write_bytes(file_name, dir, self.fits_bytes(cube=False), clobber, file_compress)
+
+    def writeCube(self, file_name, dir=None, clobber=True, compression='auto'):
+        """galsim.fits.writeCube of the stamps (fits.py:529-648), made on the device."""
+        from . import fits
+        file_compress, tile = fits._parse_compression(compression, file_name)
+        fits._no_tiles(tile)
+        fits._write_bytes(file_name, dir, self.fits_bytes(cube=True), clobber, file_compress)
+
     def images(self):
         from .image import Image
         from .wcs import PixelScale

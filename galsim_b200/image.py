@@ -272,6 +272,11 @@ class Image(object):
         """Add noise to the image (image.py addNoise, noise.py:31-39); drawn on the GPU."""
         noise.applyTo(self)
 
+    def write(self, file_name=None, dir=None, hdu_list=None, clobber=True, compression='auto'):
+        """Write the image to a FITS file (galsim.fits.write, fits.py:378-443)."""
+        from . import fits
+        fits.write(self, file_name, dir, hdu_list, clobber, compression)
+
     def __iadd__(self, other):
         self._array += other.array if isinstance(other, Image) else other
         return self

@@ -254,11 +254,32 @@ typedef struct gsb_noise_params {
  * stamps' pixel counts.  Poisson and CCD noise need d_scratch (one double per pixel, addressed
  * like d_image) and d_used.  d_used (may be NULL for Gaussian noise) receives, per stamp, the raw
  * draws consumed since seeding (skip + this call's draws), so a caller can continue the stream.
- * Gaussian: one warp per stamp.  Poisson / CCD: the expectations in parallel, the draws one
- * thread per stamp (the stream is sequential), then the read noise and the cast one warp per
+ * Gaussian: one warp per stamp.  Poisson / CCD: the expectations in parallel, then one warp per
+ * stamp walks its sequential stream (speculative draws of 32 pixels at once, committed up to the
+ * first whose count of draws was mispredicted), then the read noise and the cast one warp per
  * stamp.  No allocation. */
 int gsb_add_noise(int kind, const gsb_noise_params* p, const gsb_noise_stamp* d_stamps, int n_stamps,
                   int max_npix, void* d_image, int dtype, double* d_scratch, long long* d_used,
+                  void* stream);
+
+/* FITS file images ---------------------------------------------------------------------- */
+/* One HDU of a FITS file assembled on the device (the layout galsim/fits.py writes through
+ * astropy: FITS Standard 4.0 header blocks and big-endian data padded to 2880 bytes). */
+typedef struct gsb_fits_hdu {
+    int64_t header_src;   /* byte offset of the HDU's header in d_headers (multiple of 16) */
+    int64_t header_len;   /* header bytes: formatted cards padded to a multiple of 2880 */
+    int64_t data_src;     /* element offset of the HDU's first pixel in d_src */
+    int64_t n_elem;       /* pixels, in the order they are stored (row-major, stamps in turn) */
+    int64_t dst;          /* byte offset of the HDU in d_out (multiple of 2880, ascending) */
+} gsb_fits_hdu;
+
+/* Write the file image of n_hdus HDUs (host records h_hdus, checked against the buffer sizes)
+ * into d_out: each header copied, the pixels of d_src (GSB_F32 / GSB_F64) byte-swapped to
+ * big-endian after it, and the data zero-padded to a 2880-byte block.  d_headers and d_out are
+ * 16-byte aligned.  Replaces astropy's HDUList.writeto as called by fits.py:378-701 for the
+ * pixels; the file itself is written by the caller from the copied-back buffer. */
+int gsb_fits_pack(const gsb_fits_hdu* h_hdus, int n_hdus, const void* d_headers, long long header_bytes,
+                  const void* d_src, long long src_elems, int dtype, void* d_out, long long out_bytes,
                   void* stream);
 
 /* Leaves -------------------------------------------------------------------------------- */

@@ -8,6 +8,7 @@ its own C++ sources (oracle/ref_import.py).  Everything drawn here goes through 
 reference's drawImage / drawKImage / wrap / irfft / stepk / maxk; the fixtures record the
 inputs next to the outputs.  These files are the pin for both the numpy oracle and the GPU
 kernels; the GPU tests read only these .npz files, never the reference checkout.
+(reference_fits.npz, from main_fits, holds the reference's FITS test files as bytes.)
 """
 import os
 import sys
@@ -391,6 +392,23 @@ def main_noise(ref_root):
     print('wrote', os.path.join(HERE, 'reference_noise.npz'), len(out), 'arrays')
 
 
+# FITS fixture files of the reference's test_image.py (test<T>.fits[.gz|.bz2] for T in S, I,
+# F, D, US, UI: the 5 x 7 ref_array in each type), kept as raw bytes so that the FITS reader is
+# checked against files astropy wrote, without the reference tree.
+FITS_FIXTURES = ['test%s.fits%s' % (t, e) for t in ('S', 'I', 'F', 'D', 'US', 'UI')
+                 for e in ('', '.gz', '.bz2')]
+
+
+def main_fits(ref_root):
+    src = os.path.join(ref_root, 'tests', 'Image_comparison_images')
+    out = {}
+    for name in FITS_FIXTURES:
+        with open(os.path.join(src, name), 'rb') as f:
+            out[name.replace('.', '_')] = np.frombuffer(f.read(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, 'reference_fits.npz'), **out)
+    print('wrote', os.path.join(HERE, 'reference_fits.npz'), len(out), 'files')
+
+
 def main(ref_root):
     from ref_import import import_reference_galsim
     galsim = import_reference_galsim(ref_root)
@@ -448,6 +466,8 @@ if __name__ == '__main__':
         main_noise(root)
     elif '--config-only' in sys.argv:
         main_config(root)
+    elif '--fits-only' in sys.argv:
+        main_fits(root)
     else:
         if '--large-only' not in sys.argv:
             main(root)
@@ -456,3 +476,4 @@ if __name__ == '__main__':
         main_config(root)
         main_interp(root)
         main_noise(root)
+        main_fits(root)
