@@ -17,7 +17,8 @@ from .gsparams import GSParams
 from .position import _PositionD
 
 
-_PINNED = {}
+_PINNED = {}          # page-locked read-back buffers: host() pixels
+_PINNED_FITS = {}     # and FITS file images
 
 
 class StampBatch(object):
@@ -97,6 +98,11 @@ class StampBatch(object):
         one HDU per stamp (writeMulti; the first is the primary HDU) or one data cube
         (writeCube; the stamps must share a size).  Each header carries the stamp's BITPIX,
         NAXISn, GS_XMIN / GS_YMIN and its PixelScale WCS, as fits.py writes them."""
+        return self._fits_image(cube).tobytes()
+
+    def _fits_image(self, cube=False):
+        """fits_bytes as a uint8 view of a reused page-locked buffer (valid until the next call
+        of the same size)."""
         import ctypes
         import torch
         from . import fits
@@ -111,39 +117,46 @@ class StampBatch(object):
         nx = np.asarray(self.nx, np.int64)
         ny = np.asarray(self.ny, np.int64)
         offsets = np.asarray(self.offsets, np.int64)
-        hdrs, index = [], {}
+        bnd = np.asarray(self.bounds, np.int64).reshape(B, 4)
+        hdrs = []
 
         def header(shape, primary, b):
-            key = (shape, primary, b)
-            if key not in index:
-                cls = fits.PrimaryHDU if primary else fits.ImageHDU
-                hdu = cls(np.empty(shape, dt), fits.image_header_cards(_BoundsI(*b), wcs))
-                index[key] = (sum(len(h) for h in hdrs), len(hdrs))
-                hdrs.append(np.frombuffer(hdu.header_bytes(), np.uint8))
-            return index[key][0], len(hdrs[index[key][1]])
+            cls = fits.PrimaryHDU if primary else fits.ImageHDU
+            hdu = cls(np.empty(shape, dt), fits.image_header_cards(_BoundsI(*(int(v) for v in b)), wcs))
+            off = sum(len(h) for h in hdrs)
+            hdrs.append(np.frombuffer(hdu.header_bytes(), np.uint8))
+            return off, len(hdrs[-1])
 
         if cube:
-            if len(set(nx.tolist())) != 1 or len(set(ny.tolist())) != 1:
+            if np.any(nx != nx[0]) or np.any(ny != ny[0]):
                 raise GalSimValueError("In writeCube: the stamps have different sizes",
                                        (sorted(set(nx.tolist())), sorted(set(ny.tolist()))))
             n1 = int(nx[0] * ny[0])
             if not np.array_equal(offsets, np.arange(B, dtype=np.int64) * n1):
                 raise GalSimValueError("In writeCube: the stamps are not stored back to back", offsets)
-            b0 = tuple(int(v) for v in self.bounds[0])
-            hs, hl = header((B, int(ny[0]), int(nx[0])), True, b0)
-            recs = [(hs, hl, int(offsets[0]), B * n1)]
+            hs, hl = header((B, int(ny[0]), int(nx[0])), True, bnd[0])
+            rec = np.zeros(1, dtype=_lib.FITS_HDU_DTYPE)
+            rec['header_src'], rec['header_len'], rec['data_src'], rec['n_elem'] = hs, hl, offsets[0], B * n1
         else:
-            recs = []
-            for i in range(B):
-                b = tuple(int(v) for v in self.bounds[i])
-                hs, hl = header((int(ny[i]), int(nx[i])), i == 0, b)
-                recs.append((hs, hl, int(offsets[i]), int(nx[i] * ny[i])))
-        rec = np.zeros(len(recs), dtype=_lib.FITS_HDU_DTYPE)
-        r = np.asarray(recs, np.int64)
-        rec['header_src'], rec['header_len'], rec['data_src'], rec['n_elem'] = r.T
-        dbytes = (r[:, 3] * esz + fits.BLOCK - 1) // fits.BLOCK * fits.BLOCK
-        sizes = r[:, 1] + dbytes
-        rec['dst'] = np.concatenate(([0], np.cumsum(sizes)[:-1]))
+            # one extension header per distinct (shape, origin); the first stamp's as the primary
+            keys = np.stack([ny, nx, bnd[:, 0], bnd[:, 2]], axis=1)
+            uniq, inv = np.unique(keys, axis=0, return_inverse=True)
+            inv = inv.reshape(-1)
+            hsrc = np.zeros(len(uniq), np.int64)
+            hlen = np.zeros(len(uniq), np.int64)
+            for u, k in enumerate(uniq):
+                b = (k[2], k[2] + k[1] - 1, k[3], k[3] + k[0] - 1)
+                hsrc[u], hlen[u] = header((int(k[0]), int(k[1])), False, b)
+            rec = np.zeros(B, dtype=_lib.FITS_HDU_DTYPE)
+            rec['header_src'] = hsrc[inv]
+            rec['header_len'] = hlen[inv]
+            p0, l0 = header((int(ny[0]), int(nx[0])), True, bnd[0])
+            rec['header_src'][0], rec['header_len'][0] = p0, l0
+            rec['data_src'] = offsets
+            rec['n_elem'] = nx * ny
+        dbytes = (rec['n_elem'] * esz + fits.BLOCK - 1) // fits.BLOCK * fits.BLOCK
+        sizes = rec['header_len'] + dbytes
+        rec['dst'][1:] = np.cumsum(sizes)[:-1]
         total = int(sizes.sum())
         dev = self.flat.device
         d_hdr = torch.from_numpy(np.concatenate(hdrs)).to(dev)
@@ -152,10 +165,14 @@ class StampBatch(object):
             rec.ctypes.data_as(ctypes.c_void_p), len(rec), _lib.ptr(d_hdr), d_hdr.numel(),
             _lib.ptr(self.flat), self.flat.numel(), _lib.F32 if esz == 4 else _lib.F64,
             _lib.ptr(out), total, _lib.Device.stream()))
-        host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
-        host.copy_(out, non_blocking=True)
+        buf = _PINNED_FITS.get(total)
+        if buf is None:
+            buf = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+            _PINNED_FITS.clear()
+            _PINNED_FITS[total] = buf
+        buf.copy_(out, non_blocking=True)
         torch.cuda.current_stream(dev).synchronize()
-        return host.numpy().tobytes()
+        return buf.numpy()
 
     def writeMulti(self, file_name, dir=None, clobber=True, compression='auto'):
         """galsim.fits.writeMulti of every stamp (fits.py:445-527), the file image made on the
@@ -163,14 +180,14 @@ class StampBatch(object):
         from . import fits
         file_compress, tile = fits._parse_compression(compression, file_name)
         fits._no_tiles(tile)
-        fits._write_bytes(file_name, dir, self.fits_bytes(cube=False), clobber, file_compress)
+        fits._write_bytes(file_name, dir, self._fits_image(cube=False), clobber, file_compress)
 
     def writeCube(self, file_name, dir=None, clobber=True, compression='auto'):
         """galsim.fits.writeCube of the stamps (fits.py:529-648), made on the device."""
         from . import fits
         file_compress, tile = fits._parse_compression(compression, file_name)
         fits._no_tiles(tile)
-        fits._write_bytes(file_name, dir, self.fits_bytes(cube=True), clobber, file_compress)
+        fits._write_bytes(file_name, dir, self._fits_image(cube=True), clobber, file_compress)
 
     def images(self):
         from .image import Image

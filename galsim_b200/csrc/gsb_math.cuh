@@ -76,12 +76,17 @@ __device__ const double kExp2Tab[32] = {
 __device__ __forceinline__ double exp_tab(double x)
 {
     if (x < -708.) return 0.;
-    const double t = rint(x * 46.16624130844683);           // 32 / ln2
+    // n = rint(x 32/ln2) without a rounding or conversion instruction: adding 1.5 * 2^52 to the
+    // (rounded) product leaves n, rounded to nearest-even as rint does, in the low mantissa bits
+    // (|n| < 2^31), and subtracting it back gives n as a double exactly.
+    const double kShift = 6755399441055744.0;               // 1.5 * 2^52
+    const double s = __dadd_rn(__dmul_rn(x, 46.16624130844683), kShift);   // 32 / ln2
+    const int n = __double2loint(s);
+    const double t = s - kShift;
     double r = fma(-t, 0.02166084939249829, x);              // ln2/32, leading double
     r = fma(-t, 7.247021293269686e-19, r);                   // ln2/32, remainder
-    const long long n = (long long)t;
-    const int j = int(n & 31);
-    const long long m = n >> 5;
+    const int j = n & 31;
+    const int m = n >> 5;
     double p = fma(r, 1. / 720., 1. / 120.);
     p = fma(p, r, 1. / 24.);
     p = fma(p, r, 1. / 6.);
@@ -89,7 +94,7 @@ __device__ __forceinline__ double exp_tab(double x)
     p = fma(p, r, 1.);
     p = fma(p, r, 1.);
     const double v = __ldg(&kExp2Tab[j]) * p;
-    return __longlong_as_double(__double_as_longlong(v) + (m << 52));
+    return __hiloint2double(__double2hiint(v) + (m << 20), __double2loint(v));
 }
 
 // ---------------------------------------------------------------------------------------

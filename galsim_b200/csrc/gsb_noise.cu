@@ -432,11 +432,16 @@ __global__ void __launch_bounds__(kPoissonWarps * 32) poisson_kernel(const __gri
     double cur_mean = 1.;
     bool gd_exists = false, gd_valid = false;
     double gd_rho = 0., gd_r1 = 0.;
+    // the means of this chunk (p0 + lane) and of the next (p0 + 32 + lane): the next chunk is
+    // loaded a round ahead, so the load is off the chain of dependent rounds
+    double m_cur = lane < n ? w[lane] : 0.;
+    double m_nxt = 32 + lane < n ? w[32 + lane] : 0.;
     while (p0 < n) {
         while (base >= W.wstart + kMtN) W.advance();
+        const long long p_start = p0;
         const long long j = p0 + lane;
         const bool valid = j < n;
-        const double mean = valid ? w[j] : 0.;
+        const double mean = valid ? m_cur : 0.;
         const bool nz = valid && mean > 0.;
         const bool special = nz && mean > kMaxPoisson;
         // Assumed word counts: 1 for a draw whose first word lands in the immediate region
@@ -554,6 +559,13 @@ __global__ void __launch_bounds__(kPoissonWarps * 32) poisson_kernel(const __gri
             base = ws.pos;
             ++p0;
         }
+        // advance the two chunks of means by the d pixels this round finished (1 <= d <= 32:
+        // at most 32 commits, or at most 31 and one pixel in order)
+        const int src = lane + int(p0 - p_start);
+        const double from_cur = __shfl_sync(0xffffffffu, m_cur, src & 31);
+        const double from_nxt = __shfl_sync(0xffffffffu, m_nxt, src & 31);
+        m_cur = p0 + lane < n ? (src < 32 ? from_cur : from_nxt) : 0.;
+        m_nxt = p0 + 32 + lane < n ? w[p0 + 32 + lane] : 0.;
     }
     if (lane == 0) a.used[s] = base;
 }

@@ -112,11 +112,14 @@ def _apply(kind, params, flat, offsets, npix, seeds, skips):
     import torch
     dev = _lib.Device.torch_device()
     B = len(offsets)
+    # the largest stamps first: each stamp's Poisson stream is one sequential chain, so the
+    # longest chains should start before all warps are busy
+    order = np.argsort(-np.asarray(npix, np.int64), kind='stable')
     rec = np.zeros(B, dtype=NOISE_STAMP_DTYPE)
-    rec['offset'] = offsets
-    rec['npix'] = npix
-    rec['seed'] = seeds
-    rec['skip'] = skips
+    rec['offset'] = np.asarray(offsets, np.int64)[order]
+    rec['npix'] = np.asarray(npix)[order]
+    rec['seed'] = np.broadcast_to(np.asarray(seeds, np.int64), (B,))[order]
+    rec['skip'] = np.broadcast_to(np.asarray(skips, np.int64), (B,))[order]
     d_rec = _lib.to_device(rec)
     if flat.dtype == torch.float32:
         dt = _lib.F32
@@ -129,7 +132,9 @@ def _apply(kind, params, flat, offsets, npix, seeds, skips):
     _lib.check(_lib.lib().gsb_add_noise(kind, ctypes.byref(params), _lib.ptr(d_rec), B,
                                         int(np.max(npix)) if B else 0, _lib.ptr(flat), dt,
                                         _lib.ptr(scratch), _lib.ptr(used), _lib.Device.stream()))
-    return used.cpu().numpy()
+    out = np.empty(B, np.int64)
+    out[order] = used.cpu().numpy()
+    return out
 
 
 class BaseNoise(object):
