@@ -107,23 +107,14 @@ __device__ void mt_seed(uint32_t* x, long long seed, int lane)
 }
 
 // A warp's position in its stream: the state x (shared), the index i of the next word in the
-// current block (kMtN = exhausted), and the count of words consumed since seeding.
+// current block (kMtN = exhausted), and the count of words consumed since seeding.  The words
+// themselves are read block by block (gaussian_run); skip moves the position.
 struct WarpStream {
     uint32_t* x;
     int i;
     long long used;
     int lane;
 
-    __device__ uint32_t next()           // every lane calls, all get the same word
-    {
-        if (i == kMtN) { mt_twist(x, lane); i = 0; }
-        const uint32_t w = mt_temper(x[i]);
-        ++i;
-        ++used;
-        return w;
-    }
-    __device__ double uniform() { return double(next()) * (1. / 4294967296.); }
-    __device__ bool ok() const { return true; }
     __device__ void skip(long long n)
     {
         while (n > 0) {
@@ -207,6 +198,25 @@ __device__ __forceinline__ double log_factorial_small(int k)
     return r;
 }
 
+// The constants of Hoermann's PTRD for one mean (Boost's poisson_distribution, mean >= 10)
+// that the speculative pass needs before the draw: sqrt(mean), b and v_r (a and 1/alpha follow
+// from b in the draw).
+struct PtrdSetup {
+    double smu, b, v_r;
+};
+
+__device__ __forceinline__ PtrdSetup ptrd_setup(double mean)
+{
+    PtrdSetup c;
+    c.smu = sqrt(mean);
+    c.b = 0.931 + 2.53 * c.smu;
+    c.v_r = 0.9277 - 3.6224 / (c.b - 2);
+    return c;
+}
+
+template <typename Stream>
+__device__ double ptrd_draw(Stream& st, double mean, const PtrdSetup& c);
+
 // One Poisson draw from the stream.
 template <typename Stream>
 __device__ double poisson_draw(Stream& st, double mean)
@@ -224,11 +234,16 @@ __device__ double poisson_draw(Stream& st, double mean)
         }
         return x;
     }
-    const double smu = sqrt(mean);
-    const double b = 0.931 + 2.53 * smu;
+    return ptrd_draw(st, mean, ptrd_setup(mean));
+}
+
+// The PTRD draw (mean >= 10) with its constants already formed.
+template <typename Stream>
+__device__ double ptrd_draw(Stream& st, double mean, const PtrdSetup& c)
+{
+    const double smu = c.smu, b = c.b, v_r = c.v_r;
     const double a = -0.059 + 0.02483 * b;
     const double inv_alpha = 1.1239 + 1.1328 / (b - 3.4);
-    const double v_r = 0.9277 - 3.6224 / (b - 2);
     for (int iter = 0; iter < (1 << 20); ++iter) {
         if (!st.ok()) return 0.;
         double u;
@@ -451,12 +466,10 @@ __global__ void __launch_bounds__(kPoissonWarps * 32) poisson_kernel(const __gri
         int guess = nz ? 1 : 0;
         int offs = 0;
         bool imm = true;
-        double smu = 0., b = 0., v_r = 0., v0 = 0.;
-        if (nz && !special && !(mean < 10.)) {
-            smu = sqrt(mean);
-            b = 0.931 + 2.53 * smu;
-            v_r = 0.9277 - 3.6224 / (b - 2);
-        }
+        double v0 = 0.;
+        PtrdSetup cs{0., 0., 0.};
+        if (nz && !special && !(mean < 10.)) cs = ptrd_setup(mean);
+        const double v_r = cs.v_r;
         for (int round = 0; round < 6; ++round) {
             offs = warp_exclusive_sum(guess, lane);
             int g2 = 0;
@@ -491,13 +504,13 @@ __global__ void __launch_bounds__(kPoissonWarps * 32) poisson_kernel(const __gri
                 value = x;
                 count = 1;
             } else if (v0 <= 0.86 * v_r) {
-                const double a_ = -0.059 + 0.02483 * b;
                 const double u = v0 / v_r - 0.43;
-                value = floor((2 * a_ / (0.5 - fabs(u)) + b) * u + mean + 0.445);
+                const double a_ = -0.059 + 0.02483 * cs.b;
+                value = floor((2 * a_ / (0.5 - fabs(u)) + cs.b) * u + mean + 0.445);
                 count = 1;
             } else {
                 LaneSource src{W.win, wpos, 2 * kMtN, 0, false};
-                value = poisson_draw(src, mean);
+                value = ptrd_draw(src, mean, cs);
                 count = src.count;
                 bad = src.overflow;
             }

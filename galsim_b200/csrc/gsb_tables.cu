@@ -376,8 +376,10 @@ __global__ void sersic_scan_kernel(const double* header, int count, int stride, 
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= count) return;
-    SersicScan& S = scan[s];
-    if (S.done) return;
+    if (scan[s].done) return;
+    // the state is advanced in a local copy (the node stores below may alias it as far as the
+    // compiler knows, which would send every field access to global memory) and written back
+    SersicScan S = scan[s];
     const double* H = header + (size_t)s * kSersicHeader;
     const double* v = vals + (size_t)s * stride;
     double4* nd = nodes + (size_t)s * stride;
@@ -402,7 +404,7 @@ __global__ void sersic_scan_kernel(const double* header, int count, int stride, 
             const double f0_pred = S.a + S.b / k;
             if (fabs(f0 - f0_pred) / ksq < gsp.kvalue_accuracy) ++S.n_correct;
             else S.n_correct = 0;
-            if (S.n_correct >= 5) { S.ksq_max = ksq; S.done = 1; return; }
+            if (S.n_correct >= 5) { S.ksq_max = ksq; S.done = 1; scan[s] = S; return; }
         }
         const double inv_k = 1. / k;
         if (S.fit_size == n_fit) {
@@ -424,6 +426,7 @@ __global__ void sersic_scan_kernel(const double* header, int count, int stride, 
         }
     }
     if (iend >= ncand) S.done = 1;
+    scan[s] = S;
 }
 
 // End of buildFT (SBSersic.cpp:510-537) and the natural spline (Table.cpp:634-686).
