@@ -671,8 +671,8 @@ def run_reference(args):
 # GPU arm
 # ---------------------------------------------------------------------------------------------
 def run_stage(args):
-    """Small single-stage runs for profiling (--stage draw | tables | fit | interp | noise): no
-    e2e / CPU legs."""
+    """Small single-stage runs for profiling (--stage draw | tables | fit | interp | noise |
+    fits): no e2e / CPU legs."""
     import torch
     import galsim_b200 as galsim
     from galsim_b200 import _lib
@@ -713,6 +713,16 @@ def run_stage(args):
         e1.record()
         torch.cuda.synchronize()
         print(json.dumps({'stage': 'tables', 'tables': len(n), 'ms_per_build': e0.elapsed_time(e1) / args.steps}))
+        return
+    if args.stage == 'fits':
+        st = galsim.draw_batch(obj, nx=args.nx, ny=args.nx, scale=SCALE, dtype=np.float32)
+        for _ in range(args.warmup):
+            st._fits_image()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            img = st._fits_image()
+        print(json.dumps({'stage': 'fits', 'stamps': len(st), 'file_bytes': int(img.size),
+                          'ms_per_step': (time.perf_counter() - t0) / args.steps * 1e3}))
         return
     if args.stage == 'noise':
         dev = _lib.Device.torch_device()
@@ -932,8 +942,8 @@ def main():
                     help='skip the mixed-batch and large-stamp measurements')
     ap.add_argument('--stamps', type=int, default=B_DEFAULT, help='stamps per GPU (leading subset)')
     ap.add_argument('--nx', type=int, default=None, help='fixed stamp size (default: automatic)')
-    ap.add_argument('--stage', default='all', choices=['all', 'draw', 'tables', 'fit', 'interp', 'noise'],
-                    help="'draw' / 'tables' / 'fit' / 'interp' / 'noise': run only that stage (for profiling)")
+    ap.add_argument('--stage', default='all', choices=['all', 'draw', 'tables', 'fit', 'interp', 'noise', 'fits'],
+                    help="'draw' / 'tables' / 'fit' / 'interp' / 'noise' / 'fits': run only that stage (for profiling)")
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)
