@@ -19,6 +19,33 @@ from .position import _PositionD
 
 _PINNED = {}          # page-locked read-back buffers: host() pixels
 _PINNED_FITS = {}     # and FITS file images
+_PINNED_ASYNC = {}    # host_async: two alternating buffers per size
+_COPY_STREAMS = {}
+
+
+def _copy_stream(dev):
+    import torch
+    s = _COPY_STREAMS.get(dev.index)
+    if s is None:
+        s = torch.cuda.Stream(device=dev)
+        _COPY_STREAMS[dev.index] = s
+    return s
+
+
+class HostRead(object):
+    """A read of a StampBatch's pixels to the host in flight on a copy stream
+    (StampBatch.host_async); result() waits for it and returns the flat host array."""
+
+    def __init__(self, buf, done):
+        self._buf = buf
+        self._done = done
+
+    def done(self):
+        return self._done.query()
+
+    def result(self):
+        self._done.synchronize()
+        return self._buf.numpy()
 
 
 class StampBatch(object):
@@ -80,6 +107,32 @@ class StampBatch(object):
         buf.copy_(self.flat, non_blocking=True)
         torch.cuda.current_stream(self.flat.device).synchronize()
         return buf.numpy().copy() if copy else buf.numpy()
+
+    def host_async(self):
+        """Start reading all pixels to the host on a copy stream, so that the read overlaps
+        whatever is launched next on the drawing stream (the next batch's tables and draws).
+        Returns a HostRead; its result() is a view of one of two page-locked buffers that
+        alternate between calls of the same size, valid until the call after next."""
+        import torch
+        dev = self.flat.device
+        key = (self.flat.numel(), self.flat.dtype)
+        slot = _PINNED_ASYNC.get(key)
+        if slot is None:
+            slot = [[torch.empty(key[0], dtype=key[1], pin_memory=True) for _ in range(2)], 0]
+            _PINNED_ASYNC.clear()
+            _PINNED_ASYNC[key] = slot
+        buf = slot[0][slot[1]]
+        slot[1] ^= 1
+        cs = _copy_stream(dev)
+        ready = torch.cuda.Event()
+        ready.record(torch.cuda.current_stream(dev))
+        cs.wait_event(ready)
+        with torch.cuda.stream(cs):
+            buf.copy_(self.flat, non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(cs)
+        self.flat.record_stream(cs)
+        return HostRead(buf, done)
 
     def arrays(self):
         host = self.host()

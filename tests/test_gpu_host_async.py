@@ -1,0 +1,28 @@
+"""StampBatch.host_async: the read-back on a copy stream returns the same pixels as host(),
+for reads in flight while the next batch is drawn (the pipelined catalog loop)."""
+import numpy as np
+import pytest
+
+import galsim_b200 as galsim
+
+pytestmark = pytest.mark.gpu
+
+
+def _obj(seed):
+    rng = np.random.default_rng(seed)
+    n = 16
+    gal = galsim.Sersic(n=rng.uniform(0.8, 3.5, n), half_light_radius=rng.uniform(0.3, 1.0, n),
+                        flux=1e3).shear(g1=rng.uniform(-0.2, 0.2, n), g2=0.05)
+    return galsim.Convolve(gal, galsim.Kolmogorov(fwhm=0.7), galsim.Pixel(0.2))
+
+
+def test_pipelined_reads_match_synchronous_reads():
+    pending, expected = [], []
+    for seed in range(4):
+        sb = galsim.draw_batch(_obj(seed), scale=0.2, dtype=np.float32)
+        expected.append(sb.host(copy=True))
+        pending.append(sb.host_async())
+        if len(pending) == 2:
+            got = pending.pop(0).result()
+            np.testing.assert_array_equal(got, expected[seed - 1])
+    np.testing.assert_array_equal(pending.pop(0).result(), expected[-1])
