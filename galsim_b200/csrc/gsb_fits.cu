@@ -4,11 +4,13 @@
 // order, zero-padded to a block.  One launch writes every HDU of the file into one buffer, which
 // then leaves the device with one copy.
 //
-// Layout of the work: grid.x walks the HDUs, grid.y the 4 KB chunks of one HDU (grid-stride), so
-// a file of thousands of small stamps and a data cube of one large HDU both fill the SMs.
+// Layout of the work: one block per chunk of 256 units (16-byte header words, pixels, padding
+// bytes) of one HDU, so a file of thousands of small stamps and a data cube of one large HDU
+// both fill the SMs with as many blocks as their bytes need.
 // Headers and padding move as 16-byte words (every HDU starts on a 2880-byte boundary, a
 // multiple of 16); pixels are read in the stamp buffer's own order and stored byte-swapped.
 #include <algorithm>
+#include <vector>
 
 #include "gsb_internal.cuh"
 
@@ -34,32 +36,34 @@ __device__ __forceinline__ unsigned long long bswap<unsigned long long>(unsigned
     return ((unsigned long long)bswap32(lo) << 32) | bswap32(hi);
 }
 
-// W: the pixel word (4 or 8 bytes).
+// W: the pixel word (4 or 8 bytes).  One block per chunk of kFitsThreads units of one HDU: the
+// blocks of HDU h are chunk_base[h] .. chunk_base[h + 1] - 1 (host prefix sums), found by a
+// binary search, so a small stamp costs as few blocks as its size needs.
 template <class W>
 __global__ void __launch_bounds__(kFitsThreads) fits_pack_kernel(const gsb_fits_hdu* hdus,
+                                                                 const long long* chunk_base, int n_hdus,
                                                                  const unsigned char* headers,
                                                                  const W* src, unsigned char* out)
 {
-    const gsb_fits_hdu h = hdus[blockIdx.x];
+    const long long blk = blockIdx.x;
+    int lo = 0, hi = n_hdus - 1;               // the last h with chunk_base[h] <= blk
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (chunk_base[mid] <= blk) lo = mid; else hi = mid - 1;
+    }
+    const gsb_fits_hdu h = hdus[lo];
+    const long long u = (blk - chunk_base[lo]) * kFitsThreads + threadIdx.x;   // unit index
     unsigned char* dst = out + h.dst;
     // header: 16-byte words
-    const uint4* hs = reinterpret_cast<const uint4*>(headers + h.header_src);
-    uint4* hd = reinterpret_cast<uint4*>(dst);
-    const long long hwords = h.header_len / 16;
-    const long long step = (long long)gridDim.y * kFitsThreads;
-    for (long long w = (long long)blockIdx.y * kFitsThreads + threadIdx.x; w < hwords; w += step)
-        hd[w] = hs[w];
+    if (u < h.header_len / 16)
+        reinterpret_cast<uint4*>(dst)[u] = reinterpret_cast<const uint4*>(headers + h.header_src)[u];
     // pixels
-    W* pd = reinterpret_cast<W*>(dst + h.header_len);
-    const W* ps = src + h.data_src;
-    for (long long e = (long long)blockIdx.y * kFitsThreads + threadIdx.x; e < h.n_elem; e += step)
-        pd[e] = bswap<W>(ps[e]);
+    if (u < h.n_elem)
+        reinterpret_cast<W*>(dst + h.header_len)[u] = bswap<W>(src[h.data_src + u]);
     // zero padding up to the next block, in bytes (at most 2879)
     const long long dbytes = h.n_elem * (long long)sizeof(W);
     const long long pad = (kFitsBlock - dbytes % kFitsBlock) % kFitsBlock;
-    unsigned char* pz = dst + h.header_len + dbytes;
-    for (long long b = (long long)blockIdx.y * kFitsThreads + threadIdx.x; b < pad; b += step)
-        pz[b] = 0;
+    if (u < pad) dst[h.header_len + dbytes + u] = 0;
 }
 
 }  // namespace
@@ -78,7 +82,7 @@ int fits_pack(const gsb_fits_hdu* h_hdus, int n_hdus, const void* d_headers, lon
     if (reinterpret_cast<uintptr_t>(d_src) % esz)
         return set_error(GSB_ERR_INVALID, "gsb_fits_pack: misaligned pixel buffer");
     // Every record must stay inside its buffers, start on a block, and not overlap the next HDU.
-    long long max_chunks = 1;
+    std::vector<long long> chunk_base(n_hdus + 1, 0);
     for (int i = 0; i < n_hdus; ++i) {
         const gsb_fits_hdu& h = h_hdus[i];
         const long long dbytes = h.n_elem * esz;
@@ -90,23 +94,28 @@ int fits_pack(const gsb_fits_hdu* h_hdus, int n_hdus, const void* d_headers, lon
         if (i + 1 < n_hdus && h_hdus[i + 1].dst < h.dst + total)
             return set_error(GSB_ERR_INVALID, "gsb_fits_pack: HDUs must follow one another without overlap");
         const long long units = std::max<long long>(h.header_len / 16, std::max<long long>(h.n_elem, kFitsBlock));
-        max_chunks = std::max<long long>(max_chunks, (units + kFitsThreads - 1) / kFitsThreads);
+        chunk_base[i + 1] = chunk_base[i] + (units + kFitsThreads - 1) / kFitsThreads;
     }
-    const unsigned gy = (unsigned)std::min<long long>(max_chunks, 1024);
+    const long long blocks = chunk_base[n_hdus];
+    if (blocks > 2147483647LL) return set_error(GSB_ERR_INVALID, "gsb_fits_pack: file image too large");
     gsb_fits_hdu* d_hdus = nullptr;
+    long long* d_base = nullptr;
     GSB_CUDA_CHECK(cudaMallocAsync(&d_hdus, sizeof(gsb_fits_hdu) * n_hdus, stream));
+    GSB_CUDA_CHECK(cudaMallocAsync(&d_base, sizeof(long long) * (n_hdus + 1), stream));
     GSB_CUDA_CHECK(cudaMemcpyAsync(d_hdus, h_hdus, sizeof(gsb_fits_hdu) * n_hdus, cudaMemcpyHostToDevice, stream));
-    const dim3 grid((unsigned)n_hdus, gy);
+    GSB_CUDA_CHECK(cudaMemcpyAsync(d_base, chunk_base.data(), sizeof(long long) * (n_hdus + 1),
+                                   cudaMemcpyHostToDevice, stream));
     if (dtype == GSB_F32)
-        fits_pack_kernel<unsigned int><<<grid, kFitsThreads, 0, stream>>>(
-            d_hdus, static_cast<const unsigned char*>(d_headers), static_cast<const unsigned int*>(d_src),
-            static_cast<unsigned char*>(d_out));
+        fits_pack_kernel<unsigned int><<<(unsigned)blocks, kFitsThreads, 0, stream>>>(
+            d_hdus, d_base, n_hdus, static_cast<const unsigned char*>(d_headers),
+            static_cast<const unsigned int*>(d_src), static_cast<unsigned char*>(d_out));
     else
-        fits_pack_kernel<unsigned long long><<<grid, kFitsThreads, 0, stream>>>(
-            d_hdus, static_cast<const unsigned char*>(d_headers), static_cast<const unsigned long long*>(d_src),
-            static_cast<unsigned char*>(d_out));
+        fits_pack_kernel<unsigned long long><<<(unsigned)blocks, kFitsThreads, 0, stream>>>(
+            d_hdus, d_base, n_hdus, static_cast<const unsigned char*>(d_headers),
+            static_cast<const unsigned long long*>(d_src), static_cast<unsigned char*>(d_out));
     GSB_CUDA_CHECK(cudaGetLastError());
     GSB_CUDA_CHECK(cudaFreeAsync(d_hdus, stream));
+    GSB_CUDA_CHECK(cudaFreeAsync(d_base, stream));
     return GSB_OK;
 }
 
