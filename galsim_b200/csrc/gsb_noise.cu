@@ -397,23 +397,18 @@ struct WindowStream {
     __device__ bool ok() const { return true; }
 };
 
-// Exclusive prefix sum and total over the warp.
-__device__ __forceinline__ int warp_exclusive_sum(int v, int lane)
-{
-    int x = v;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, d);
-        if (lane >= d) x += y;
-    }
-    return x - v;
-}
+// Exclusive prefix sum over the warp of per-lane word counts in {0, 1, 2}, and their total:
+// two ballots and population counts instead of a chain of shuffles.
+struct WarpCounts {
+    int excl, total;
+};
 
-__device__ __forceinline__ int warp_sum(int v)
+__device__ __forceinline__ WarpCounts warp_counts012(int g, int lane)
 {
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
-    return v;
+    const unsigned lt = (1u << lane) - 1u;
+    const unsigned b1 = __ballot_sync(0xffffffffu, g >= 1);
+    const unsigned b2 = __ballot_sync(0xffffffffu, g >= 2);
+    return WarpCounts{__popc(b1 & lt) + __popc(b2 & lt), __popc(b1) + __popc(b2)};
 }
 
 constexpr int kPoissonWarps = 4;      // 7.3 KB of state and window per warp
@@ -471,7 +466,7 @@ __global__ void __launch_bounds__(kPoissonWarps * 32) poisson_kernel(const __gri
         if (nz && !special && !(mean < 10.)) cs = ptrd_setup(mean);
         const double v_r = cs.v_r;
         for (int round = 0; round < 6; ++round) {
-            offs = warp_exclusive_sum(guess, lane);
+            offs = warp_counts012(guess, lane).excl;
             int g2 = 0;
             if (nz) {
                 if (special) {
@@ -486,7 +481,8 @@ __global__ void __launch_bounds__(kPoissonWarps * 32) poisson_kernel(const __gri
             guess = g2;
             if (same) break;
         }
-        offs = warp_exclusive_sum(guess, lane);
+        const WarpCounts wc = warp_counts012(guess, lane);
+        offs = wc.excl;
         // every lane's draw at its assumed position (all in parallel)
         double value = mean;
         int count = 0;
@@ -526,7 +522,9 @@ __global__ void __launch_bounds__(kPoissonWarps * 32) poisson_kernel(const __gri
         const int ncommit = f + ((fmask && !f_bad) ? 1 : 0);
         const bool commit = lane < ncommit && valid;
         if (commit && nz) w[j] = ccd ? value / gain : value;
-        long long used_words = warp_sum(lane < ncommit ? count : 0);
+        // the committed lanes before f used exactly their assumed counts (offs at f); f itself,
+        // when committed, its real count
+        long long used_words = fmask ? __shfl_sync(0xffffffffu, f_bad ? offs : offs + count, f) : wc.total;
         // a committed ordinary draw replaces the normal branch's deviate (its pair cache goes)
         const unsigned pdmask = __ballot_sync(0xffffffffu, commit && nz);
         if (pdmask) {
