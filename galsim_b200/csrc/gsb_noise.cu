@@ -237,42 +237,59 @@ __device__ double poisson_draw(Stream& st, double mean)
     return ptrd_draw(st, mean, ptrd_setup(mean));
 }
 
+// One attempt of the PTRD loop whose first uniform v missed the immediate region
+// (v > 0.86 v_r); w is the attempt's second uniform (the loop reads exactly one more word in
+// either branch).  Returns true, with *k the deviate, when the attempt is accepted; a rejected
+// attempt leaves nothing behind, the next one starts afresh at the following word.
+__device__ __forceinline__ bool ptrd_attempt2(double v, double w, double mean, const PtrdSetup& c, double a,
+                                              double inv_alpha, double* k_out)
+{
+    double u;
+    if (v >= c.v_r) {
+        u = w - 0.5;
+    } else {
+        u = v / c.v_r - 0.93;
+        u = ((u < 0) ? -0.5 : 0.5) - u;
+        v = w * c.v_r;
+    }
+    const double us = 0.5 - fabs(u);
+    if (us < 0.013 && v > us) return false;
+    const double k = floor((2 * a / us + c.b) * u + mean + 0.445);
+    v = v * inv_alpha / (a / (us * us) + c.b);
+    const double log_sqrt_2pi = 0.91893853320467267;
+    *k_out = k;
+    if (k >= 10) {
+        return log(v * c.smu) <= (k + 0.5) * log(mean / k) - mean - log_sqrt_2pi + k -
+                                     (1 / 12. - (1 / 360. - 1 / (1260. * k * k)) / (k * k)) / k;
+    }
+    if (k >= 0) return log(v) <= k * log(mean) - mean - log_factorial_small(int(k));
+    return false;
+}
+
+__device__ __forceinline__ double ptrd_a(const PtrdSetup& c) { return -0.059 + 0.02483 * c.b; }
+__device__ __forceinline__ double ptrd_inv_alpha(const PtrdSetup& c) { return 1.1239 + 1.1328 / (c.b - 3.4); }
+
+// At most this many PTRD attempts per deviate (the rejection loop accepts with probability
+// > 0.8 per attempt, so the bound is never reached; it keeps every loop finite).
+constexpr int kPtrdMaxAttempts = 1 << 20;
+
 // The PTRD draw (mean >= 10) with its constants already formed.
 template <typename Stream>
 __device__ double ptrd_draw(Stream& st, double mean, const PtrdSetup& c)
 {
-    const double smu = c.smu, b = c.b, v_r = c.v_r;
-    const double a = -0.059 + 0.02483 * b;
-    const double inv_alpha = 1.1239 + 1.1328 / (b - 3.4);
-    for (int iter = 0; iter < (1 << 20); ++iter) {
+    const double a = ptrd_a(c), inv_alpha = ptrd_inv_alpha(c);
+    for (int iter = 0; iter < kPtrdMaxAttempts; ++iter) {
         if (!st.ok()) return 0.;
-        double u;
-        double v = st.uniform();
-        if (v <= 0.86 * v_r) {
-            u = v / v_r - 0.43;
-            return floor((2 * a / (0.5 - fabs(u)) + b) * u + mean + 0.445);
+        const double v = st.uniform();
+        if (v <= 0.86 * c.v_r) {
+            const double u = v / c.v_r - 0.43;
+            return floor((2 * a / (0.5 - fabs(u)) + c.b) * u + mean + 0.445);
         }
-        if (v >= v_r) {
-            u = st.uniform() - 0.5;
-        } else {
-            u = v / v_r - 0.93;
-            u = ((u < 0) ? -0.5 : 0.5) - u;
-            v = st.uniform() * v_r;
-        }
-        const double us = 0.5 - fabs(u);
-        if (us < 0.013 && v > us) continue;
-        const double k = floor((2 * a / us + b) * u + mean + 0.445);
-        v = v * inv_alpha / (a / (us * us) + b);
-        const double log_sqrt_2pi = 0.91893853320467267;
-        if (k >= 10) {
-            if (log(v * smu) <= (k + 0.5) * log(mean / k) - mean - log_sqrt_2pi + k -
-                                    (1 / 12. - (1 / 360. - 1 / (1260. * k * k)) / (k * k)) / k)
-                return k;
-        } else if (k >= 0) {
-            if (log(v) <= k * log(mean) - mean - log_factorial_small(int(k))) return k;
-        }
+        const double w = st.uniform();
+        double k;
+        if (ptrd_attempt2(v, w, mean, c, a, inv_alpha, &k)) return k;
     }
-    return mean;   // unreachable in practice: the rejection loop accepts with probability > 0.8
+    return mean;   // unreachable in practice (see kPtrdMaxAttempts)
 }
 
 struct NoiseArgs {
@@ -368,21 +385,6 @@ struct Window {
     }
 };
 
-// A lane's speculative reader of the window.
-struct LaneSource {
-    const uint32_t* win;
-    int pos, end;
-    int count;
-    bool overflow;
-    __device__ double uniform()
-    {
-        if (pos >= end) { overflow = true; return 0.5; }
-        ++count;
-        return double(win[pos++]) * (1. / 4294967296.);
-    }
-    __device__ bool ok() const { return !overflow; }
-};
-
 // The whole warp reading in order, advancing the window as needed (collective).
 struct WindowStream {
     Window* w;
@@ -444,6 +446,7 @@ __global__ void __launch_bounds__(kPoissonWarps * 32) poisson_kernel(const __gri
     double gd_rho = 0., gd_r1 = 0.;
     // the means of this chunk (p0 + lane) and of the next (p0 + 32 + lane): the next chunk is
     // loaded a round ahead, so the load is off the chain of dependent rounds
+    int rejected = 0;          // rejected PTRD attempts on the unfinished pixel at p0
     double m_cur = lane < n ? w[lane] : 0.;
     double m_nxt = 32 + lane < n ? w[32 + lane] : 0.;
     while (p0 < n) {
@@ -483,10 +486,13 @@ __global__ void __launch_bounds__(kPoissonWarps * 32) poisson_kernel(const __gri
         }
         const WarpCounts wc = warp_counts012(guess, lane);
         offs = wc.excl;
-        // every lane's draw at its assumed position (all in parallel)
+        // every lane's draw at its assumed position (all in parallel): one PTRD attempt per lane;
+        // a rejected attempt (its two words consumed) leaves its pixel unfinished, to start
+        // afresh at the next word in the next round
         double value = mean;
         int count = 0;
         bool bad = special;
+        bool unfinished = false;
         if (nz && !special) {
             const int wpos = int(base - W.wstart) + offs;
             v0 = double(W.win[wpos]) * (1. / 4294967296.);
@@ -504,22 +510,27 @@ __global__ void __launch_bounds__(kPoissonWarps * 32) poisson_kernel(const __gri
                 const double a_ = -0.059 + 0.02483 * cs.b;
                 value = floor((2 * a_ / (0.5 - fabs(u)) + cs.b) * u + mean + 0.445);
                 count = 1;
+            } else if (wpos + 1 < 2 * kMtN) {
+                const double w2 = double(W.win[wpos + 1]) * (1. / 4294967296.);
+                double k;
+                unfinished = !ptrd_attempt2(v0, w2, mean, cs, ptrd_a(cs), ptrd_inv_alpha(cs), &k);
+                value = k;
+                count = 2;
             } else {
-                LaneSource src{W.win, wpos, 2 * kMtN, 0, false};
-                value = ptrd_draw(src, mean, cs);
-                count = src.count;
-                bad = src.overflow;
+                bad = true;            // the attempt's second word is past the window
             }
         }
         // the prefix whose positions are right: up to the first lane whose count differs from
-        // its assumption (that lane's own start is right, so it is kept unless it must be
-        // redone in order: the normal branch, or a draw past the window)
-        const bool fail = valid && (bad || count != guess);
+        // its assumption or whose pixel is unfinished (that lane's own start is right, so its
+        // draw is kept when finished, its consumed words when not, unless it must be redone in
+        // order: the normal branch, or a draw past the window)
+        const bool fail = valid && (bad || count != guess || unfinished);
         const unsigned fmask = __ballot_sync(0xffffffffu, fail);
         const int nvalid = int(min((long long)32, n - p0));
         const int f = fmask ? __ffs(fmask) - 1 : nvalid;
-        const bool f_bad = fmask ? bool(__shfl_sync(0xffffffffu, bad ? 1 : 0, f)) : false;
-        const int ncommit = f + ((fmask && !f_bad) ? 1 : 0);
+        const int f_state = fmask ? __shfl_sync(0xffffffffu, bad ? 2 : (unfinished ? 1 : 0), f) : 0;
+        const bool f_bad = f_state == 2, f_unf = f_state == 1;
+        const int ncommit = f + ((fmask && f_state == 0) ? 1 : 0);
         const bool commit = lane < ncommit && valid;
         if (commit && nz) w[j] = ccd ? value / gain : value;
         // the committed lanes before f used exactly their assumed counts (offs at f); f itself,
@@ -536,6 +547,18 @@ __global__ void __launch_bounds__(kPoissonWarps * 32) poisson_kernel(const __gri
         base += used_words;
         p0 += ncommit;
         __syncwarp();
+        if (f_unf) {
+            // rejected attempts on the pixel now at p0 (the PTRD loop's bound, never reached)
+            rejected = (ncommit == 0) ? rejected + 1 : 1;
+            if (rejected >= kPtrdMaxAttempts) {
+                if (lane == 0) w[p0] = ccd ? w[p0] / gain : w[p0];
+                __syncwarp();
+                ++p0;
+                rejected = 0;
+            }
+        } else {
+            rejected = 0;
+        }
         if (fmask && f_bad) {
             // the pixel at p0 in order by the whole warp: the normal branch, or a draw that ran
             // past the window
@@ -570,8 +593,9 @@ __global__ void __launch_bounds__(kPoissonWarps * 32) poisson_kernel(const __gri
             base = ws.pos;
             ++p0;
         }
-        // advance the two chunks of means by the d pixels this round finished (1 <= d <= 32:
-        // at most 32 commits, or at most 31 and one pixel in order)
+        // advance the two chunks of means by the d pixels this round finished (0 <= d <= 32:
+        // at most 32 commits, or at most 31 and one pixel in order; 0 when the first pixel's
+        // attempt was rejected)
         const int src = lane + int(p0 - p_start);
         const double from_cur = __shfl_sync(0xffffffffu, m_cur, src & 31);
         const double from_nxt = __shfl_sync(0xffffffffu, m_nxt, src & 31);
