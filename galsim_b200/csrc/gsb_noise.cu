@@ -414,6 +414,9 @@ __device__ __forceinline__ WarpCounts warp_counts012(int g, int lane)
 }
 
 constexpr int kPoissonWarps = 4;      // 7.3 KB of state and window per warp
+// Rounds of the fixed point of assumed word counts; each round extends the settled prefix past
+// one more two-word pixel, and the commit is bounded by the first rejected attempt anyway.
+constexpr int kFixedPointRounds = 4;
 
 __global__ void __launch_bounds__(kPoissonWarps * 32) poisson_kernel(const __grid_constant__ NoiseArgs a)
 {
@@ -463,23 +466,17 @@ __global__ void __launch_bounds__(kPoissonWarps * 32) poisson_kernel(const __gri
         // a few rounds find the consistent assignment (the prefix that matters converges first).
         int guess = nz ? 1 : 0;
         int offs = 0;
-        bool imm = true;
         double v0 = 0.;
         PtrdSetup cs{0., 0., 0.};
         if (nz && !special && !(mean < 10.)) cs = ptrd_setup(mean);
         const double v_r = cs.v_r;
-        for (int round = 0; round < 6; ++round) {
+        // the immediate region as a bound on the raw word: word * 2^-32 <= 0.86 v_r exactly when
+        // word <= floor(0.86 v_r 2^32) (0.4 < v_r < 1 for mean >= 10); every word for inversion
+        const uint32_t imm_max = (mean < 10. || special) ? 0xffffffffu
+                                                          : uint32_t(floor(0.86 * v_r * 4294967296.));
+        for (int round = 0; round < kFixedPointRounds; ++round) {
             offs = warp_counts012(guess, lane).excl;
-            int g2 = 0;
-            if (nz) {
-                if (special) {
-                    g2 = 1;
-                } else {
-                    v0 = double(W.win[int(base - W.wstart) + offs]) * (1. / 4294967296.);
-                    imm = mean < 10. || v0 <= 0.86 * v_r;
-                    g2 = imm ? 1 : 2;
-                }
-            }
+            const int g2 = nz ? (W.win[int(base - W.wstart) + offs] <= imm_max ? 1 : 2) : 0;
             const bool same = __all_sync(0xffffffffu, g2 == guess);
             guess = g2;
             if (same) break;
