@@ -502,19 +502,27 @@ __global__ void __launch_bounds__(kPoissonWarps * 32) poisson_kernel(const __gri
                 }
                 value = x;
                 count = 1;
-            } else if (v0 <= 0.86 * v_r) {
-                const double u = v0 / v_r - 0.43;
-                const double a_ = -0.059 + 0.02483 * cs.b;
-                value = floor((2 * a_ / (0.5 - fabs(u)) + cs.b) * u + mean + 0.445);
-                count = 1;
-            } else if (wpos + 1 < 2 * kMtN) {
-                const double w2 = double(W.win[wpos + 1]) * (1. / 4294967296.);
-                double k;
-                unfinished = !ptrd_attempt2(v0, w2, mean, cs, ptrd_a(cs), ptrd_inv_alpha(cs), &k);
-                value = k;
-                count = 2;
             } else {
-                bad = true;            // the attempt's second word is past the window
+                // mean >= 10: the immediate formula and the two-word attempt are both evaluated
+                // (straight-line, so their latencies overlap instead of running as two divergent
+                // paths); the lane keeps the one its first word selects
+                const double a_ = ptrd_a(cs);
+                const double u = v0 / v_r - 0.43;
+                const double val_imm = floor((2 * a_ / (0.5 - fabs(u)) + cs.b) * u + mean + 0.445);
+                const bool in_window = wpos + 1 < 2 * kMtN;
+                const double w2 = double(W.win[in_window ? wpos + 1 : wpos]) * (1. / 4294967296.);
+                double k = 0.;
+                const bool accepted = ptrd_attempt2(v0, w2, mean, cs, a_, ptrd_inv_alpha(cs), &k);
+                if (v0 <= 0.86 * v_r) {
+                    value = val_imm;
+                    count = 1;
+                } else if (in_window) {
+                    unfinished = !accepted;
+                    value = k;
+                    count = 2;
+                } else {
+                    bad = true;        // the attempt's second word is past the window
+                }
             }
         }
         // the prefix whose positions are right: up to the first lane whose count differs from
