@@ -845,12 +845,11 @@ def run_gpu(args):
     pending = None
     for _ in range(args.steps):
         sb = galsim.draw_batch(gpu_object(galsim, params), scale=SCALE, dtype=np.float32)
-        read = sb.host_async()
-        flux = sb.added_flux
+        read = sb.host_async()          # pixels and fluxes, on the copy stream
         if pending is not None:
-            pix = pending.result()
+            pix, flux = pending.result(), pending.added_flux()
         pending = read
-    pix = pending.result()
+    pix, flux = pending.result(), pending.added_flux()
     ee.record()
     barrier()
     e2e_ms = replicas.max_over_ranks(es.elapsed_time(ee) / args.steps)

@@ -33,12 +33,15 @@ def _copy_stream(dev):
 
 
 class HostRead(object):
-    """A read of a StampBatch's pixels to the host in flight on a copy stream
-    (StampBatch.host_async); result() waits for it and returns the flat host array."""
+    """A read of a StampBatch's pixels and drawn fluxes to the host in flight on a copy stream
+    (StampBatch.host_async); result() waits for it and returns the flat host array,
+    added_flux() the per-stamp fluxes."""
 
-    def __init__(self, buf, done):
+    def __init__(self, buf, fbuf, done, flux_scale):
         self._buf = buf
+        self._fbuf = fbuf
         self._done = done
+        self._flux_scale = flux_scale
 
     def done(self):
         return self._done.query()
@@ -46,6 +49,10 @@ class HostRead(object):
     def result(self):
         self._done.synchronize()
         return self._buf.numpy()
+
+    def added_flux(self):
+        self._done.synchronize()
+        return self._fbuf.numpy() / self._flux_scale
 
 
 class StampBatch(object):
@@ -109,19 +116,22 @@ class StampBatch(object):
         return buf.numpy().copy() if copy else buf.numpy()
 
     def host_async(self):
-        """Start reading all pixels to the host on a copy stream, so that the read overlaps
-        whatever is launched next on the drawing stream (the next batch's tables and draws).
-        Returns a HostRead; its result() is a view of one of two page-locked buffers that
-        alternate between calls of the same size, valid until the call after next."""
+        """Start reading all pixels and the drawn fluxes to the host on a copy stream, so that
+        the read overlaps whatever is launched next on the drawing stream (the next batch's
+        tables and draws) and the host need not wait for this batch's draws before preparing
+        the next.  Returns a HostRead; its result() is a view of one of two page-locked buffers
+        that alternate between calls of the same size, valid until the call after next."""
         import torch
         dev = self.flat.device
-        key = (self.flat.numel(), self.flat.dtype)
+        key = (self.flat.numel(), self.flat.dtype, self._flux_dev.numel())
         slot = _PINNED_ASYNC.get(key)
         if slot is None:
-            slot = [[torch.empty(key[0], dtype=key[1], pin_memory=True) for _ in range(2)], 0]
+            slot = [[(torch.empty(key[0], dtype=key[1], pin_memory=True),
+                      torch.empty(key[2], dtype=self._flux_dev.dtype, pin_memory=True))
+                     for _ in range(2)], 0]
             _PINNED_ASYNC.clear()
             _PINNED_ASYNC[key] = slot
-        buf = slot[0][slot[1]]
+        buf, fbuf = slot[0][slot[1]]
         slot[1] ^= 1
         cs = _copy_stream(dev)
         ready = torch.cuda.Event()
@@ -129,10 +139,12 @@ class StampBatch(object):
         cs.wait_event(ready)
         with torch.cuda.stream(cs):
             buf.copy_(self.flat, non_blocking=True)
+            fbuf.copy_(self._flux_dev, non_blocking=True)
             done = torch.cuda.Event()
             done.record(cs)
         self.flat.record_stream(cs)
-        return HostRead(buf, done)
+        self._flux_dev.record_stream(cs)
+        return HostRead(buf, fbuf, done, self._flux_scale)
 
     def arrays(self):
         host = self.host()

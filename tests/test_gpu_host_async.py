@@ -17,12 +17,16 @@ def _obj(seed):
 
 
 def test_pipelined_reads_match_synchronous_reads():
-    pending, expected = [], []
+    pending, expected, fluxes = [], [], []
     for seed in range(4):
         sb = galsim.draw_batch(_obj(seed), scale=0.2, dtype=np.float32)
         expected.append(sb.host(copy=True))
+        fluxes.append(sb.added_flux)
         pending.append(sb.host_async())
         if len(pending) == 2:
-            got = pending.pop(0).result()
-            np.testing.assert_array_equal(got, expected[seed - 1])
-    np.testing.assert_array_equal(pending.pop(0).result(), expected[-1])
+            r = pending.pop(0)
+            np.testing.assert_array_equal(r.result(), expected[seed - 1])
+            np.testing.assert_array_equal(r.added_flux(), fluxes[seed - 1])
+    r = pending.pop(0)
+    np.testing.assert_array_equal(r.result(), expected[-1])
+    np.testing.assert_array_equal(r.added_flux(), fluxes[-1])
