@@ -896,11 +896,12 @@ def run_gpu(args):
     interp = (run_interp(galsim, dev, params, max(args.steps, 3), max(args.warmup, 2),
                          cpu=(rank == 0 and world == 1 and not args.no_cpu))
               if not args.no_extra else None)
+    # the FITS stage times host-side work too, so it runs before the noise stage's CPU baseline
+    # (a pool of one process per core) rather than after it
+    fits_stage = run_fits(galsim, st) if not args.no_extra else None
     noise = (run_noise(galsim, dev, st, max(args.steps, 3), max(args.warmup, 2),
                        cpu=(rank == 0 and world == 1 and not args.no_cpu))
              if not args.no_extra else None)
-
-    fits_stage = run_fits(galsim, st) if not args.no_extra else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
