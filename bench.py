@@ -701,6 +701,16 @@ def run_stage(args):
         torch.cuda.synchronize()
         print(json.dumps({'stage': 'fit', 'stamps': len(pert), 'ms_per_step': e0.elapsed_time(e1) / args.steps}))
         return
+    if args.stage == 'large':
+        dev = _lib.Device.torch_device()
+        res = run_large(galsim, dev)
+        print(json.dumps({'stage': 'large', 'stamps_per_s': res['value'],
+                          'fp64_stamps_per_s': res['fp64_stamps_per_s'],
+                          'fp32_flux_rel_err_max': max(res['fp32_flux_rel_err']),
+                          'fp32_max_abs_err_over_peak_max': max(res['fp32_max_abs_err_over_peak']),
+                          'per_stamp': {k: res[k] for k in ('fft_sizes', 'fp32_flux_rel_err',
+                                                             'fp32_max_abs_err_over_peak')}}))
+        return
     if args.stage == 'tables':
         t = _lib.Tables()
         n = params[:, 0]
@@ -964,7 +974,7 @@ def main():
                     help='skip the mixed-batch and large-stamp measurements')
     ap.add_argument('--stamps', type=int, default=B_DEFAULT, help='stamps per GPU (leading subset)')
     ap.add_argument('--nx', type=int, default=None, help='fixed stamp size (default: automatic)')
-    ap.add_argument('--stage', default='all', choices=['all', 'draw', 'tables', 'fit', 'interp', 'noise', 'fits'],
+    ap.add_argument('--stage', default='all', choices=['all', 'draw', 'tables', 'fit', 'interp', 'noise', 'fits', 'large'],
                     help="'draw' / 'tables' / 'fit' / 'interp' / 'noise' / 'fits': run only that stage (for profiling)")
     args = ap.parse_args()
     if args.impl == 'reference':
