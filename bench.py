@@ -450,6 +450,51 @@ def run_large(galsim, dev):
             'reference_check': 'FP64 renders match the reference C++ to 1e-9 x peak on tests/golden/reference_large.npz'}
 
 
+def fp32_error_vs_reference(st):
+    """Max |diff| / peak and flux error of the leading stamps of a drawn batch against the
+    reference's drawImage of the same stamps (tests/golden/reference_configs.npz: its centred
+    blocks and strided grids, made by tests/golden/make_golden.py --configs-only)."""
+    path = os.path.join(ROOT, 'tests', 'golden', 'reference_configs.npz')
+    if not os.path.exists(path):
+        return None
+    ref = np.load(path)
+    shapes = ref['c2_shape']
+    block, stride = int(ref['cfg_block']), int(ref['cfg_stride'])
+    bo = go = 0
+    errs, ferrs = [], []
+    for i in range(min(len(shapes), len(st))):
+        a = st.array(i)
+        if a.shape != tuple(shapes[i]):
+            return {'error': 'stamp %d shape %s differs from the reference %s' % (i, a.shape, tuple(shapes[i]))}
+        b = min(block, *a.shape)
+        y0, x0 = (a.shape[0] - b) // 2, (a.shape[1] - b) // 2
+        blk, grd = a[y0:y0 + b, x0:x0 + b].ravel(), a[::stride, ::stride].ravel()
+        rb, rg = ref['c2_block'][bo:bo + blk.size], ref['c2_grid'][go:go + grd.size]
+        bo += blk.size
+        go += grd.size
+        pk = float(ref['c2_peak'][i])
+        errs.append(max(np.abs(blk.astype(float) - rb).max(), np.abs(grd.astype(float) - rg).max()) / pk)
+        fr = float(ref['c2_flux'][i])
+        ferrs.append(abs(float(st.added_flux[i]) - fr) / abs(fr))
+    return {'stamps': len(errs), 'max_abs_over_peak_median': float(np.median(errs)),
+            'max_abs_over_peak_max': float(np.max(errs)), 'flux_rel_median': float(np.median(ferrs)),
+            'flux_rel_max': float(np.max(ferrs)),
+            'against': "the reference's drawImage of the same stamps (centred 24x24 block and every "
+                       "7th pixel of each stamp, tests/golden/reference_configs.npz)"}
+
+
+def write_detail(detail):
+    """Per-stamp lists beside the JSON line (gpurun_out/bench_detail.json when that folder
+    exists, else bench_detail.json in the working directory)."""
+    d = os.path.join(os.getcwd(), 'gpurun_out')
+    path = os.path.join(d if os.path.isdir(d) else os.getcwd(), 'bench_detail.json')
+    try:
+        with open(path, 'w') as f:
+            json.dump(detail, f)
+    except OSError:
+        pass
+
+
 def gpu_object(galsim, p):
     gal = galsim.Sersic(n=p[:, 0], half_light_radius=p[:, 1], flux=p[:, 2]).shear(g1=p[:, 3], g2=p[:, 4])
     return galsim.Convolve(gal, galsim.Kolmogorov(fwhm=p[:, 5]), galsim.Pixel(SCALE))
@@ -564,45 +609,114 @@ def measured_peak_hbm():
 # ---------------------------------------------------------------------------------------------
 # CPU reference arm: the reference's C++ drawing arithmetic (oracle/_ref/libgsref.so)
 # ---------------------------------------------------------------------------------------------
-def _ref_worker(rows):
+def _ref_worker(rows, repeat=1):
+    """Draw rows with the reference C++ (oracle/_ref/libgsref.so) in this process; with
+    repeat=2 the rows are drawn twice and only the second pass is timed (the reference's
+    SersicInfo LRU cache then holds every table: the warm-table case)."""
     sys.path.insert(0, os.path.join(ROOT, 'oracle'))
     import ref_draw as R
-    out = []
-    for p in rows:
-        n, hlr, flux, g1, g2, fwhm = p
-        prof = R.c2_profile(n, hlr, flux, g1, g2, fwhm, SCALE)
+    t = 0.
+    for rep in range(repeat):
+        t0 = time.perf_counter()
+        for p in rows:
+            n, hlr, flux, g1, g2, fwhm = p
+            R.draw_image(R.c2_profile(n, hlr, flux, g1, g2, fwhm, SCALE), None, None, SCALE)
+        t = time.perf_counter() - t0
+    return t
+
+
+def _ref_warm_worker(rows):
+    return _ref_worker(rows, repeat=2)
+
+
+REF_STEP_STAMPS = 512
+
+
+def cpu_model():
+    try:
+        with open('/proc/cpuinfo') as f:
+            for line in f:
+                if line.startswith('model name'):
+                    return line.split(':', 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+class RefPool(object):
+    """The reference's C++ drawing path on every host core: one spawn-started process per
+    core (the reference's own pattern, galsim/config/util.py MultiProcess), persistent across
+    steps.  A step draws REF_STEP_STAMPS consecutive stamps of the batch, split over the
+    processes; consecutive steps continue through the batch and wrap around, so eight steps
+    cover the 4096 stamps once.  Tables are cold: every stamp has its own Sersic n and a
+    process meets each n again only after ~256 other ones (the reference's cache holds 100)."""
+
+    def __init__(self, params):
+        import multiprocessing as mp
+        sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+        import ref_draw as R
+        self.available = R.available()
+        self.params = params
+        self.cores = len(os.sched_getaffinity(0)) if hasattr(os, 'sched_getaffinity') else (os.cpu_count() or 1)
+        self.next = 0
+        self.pool = mp.get_context('spawn').Pool(self.cores) if self.available else None
+
+    def step(self, S=REF_STEP_STAMPS):
+        B = len(self.params)
+        idx = (self.next + np.arange(S)) % B
+        self.next = int((self.next + S) % B)
+        rows = self.params[idx]
         t = time.perf_counter()
-        a, f, N, Nk = R.draw_image(prof, None, None, SCALE)
-        out.append(time.perf_counter() - t)
-    return out
+        self.pool.map(_ref_worker, [rows[i::self.cores] for i in range(self.cores)])
+        return S, time.perf_counter() - t
+
+    def run(self, steps, warmup):
+        for _ in range(warmup):
+            self.step()
+        tot_s, tot_t, per = 0, 0., []
+        for _ in range(steps):
+            n, t = self.step()
+            tot_s += n
+            tot_t += t
+            per.append(t)
+        return tot_s, tot_t, per
+
+    def extras(self):
+        """Single-core and warm-table rates and the host CPU, beside the all-core cold rate."""
+        one = self.params[:32]
+        t1 = self.pool.apply(_ref_worker, (one,))
+        rows = self.params[:REF_STEP_STAMPS]
+        tw = max(self.pool.map(_ref_warm_worker, [rows[i::self.cores] for i in range(self.cores)]))
+        return {'single_core': {'value': len(one) / t1, 'unit': 'stamps/s', 'sample': '32 leading stamps, cold tables, one process'},
+                'warm_tables': {'value': len(rows) / tw, 'unit': 'stamps/s', 'cores': self.cores,
+                                'sample': '%d leading stamps, each process redrawing its share with '
+                                          'the Sersic tables already in the reference\'s cache' % len(rows)},
+                'cpu_model': cpu_model(), 'cores_available': os.cpu_count()}
+
+    def close(self):
+        if self.pool is not None:
+            self.pool.close()
+            self.pool.join()
 
 
-def cpu_reference_rate(params, budget_s=20., max_stamps=None):
-    """stamps/s of the reference's C++ path on all host cores (one process per core), over a
-    bounded leading sample of the workload sized to ~budget_s of CPU work."""
-    import multiprocessing as mp
-    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
-    import ref_draw as R
-    if not R.available():
+def cpu_reference_rate(params, steps=3, warmup=1, extras=False):
+    """stamps/s of the reference's C++ path on all host cores, over `steps` stepped samples of
+    REF_STEP_STAMPS stamps of the workload (after `warmup` untimed ones)."""
+    rp = RefPool(params)
+    if not rp.available:
         return None
-    cores = os.cpu_count() or 1
-    # estimate per-stamp cost on one core with a few stamps
-    t0 = time.perf_counter()
-    per = _ref_worker(params[:4])
-    est = max(np.mean(per), 1e-3)
-    n = int(min(len(params), max(cores, budget_s * cores / est)))
-    if max_stamps:
-        n = min(n, max_stamps)
-    sample = params[:n]
-    chunks = [sample[i::cores] for i in range(cores)]
-    ctx = mp.get_context('spawn')
-    with ctx.Pool(cores) as pool:
-        t = time.perf_counter()
-        pool.map(_ref_worker, chunks)
-        wall = time.perf_counter() - t
-    return {'value': n / wall, 'unit': 'stamps/s', 'cores': cores, 'kind': 'reference',
-            'sample': '%d leading stamps of the 4096-stamp batch (cold Sersic tables, one process '
-                      'per core, reference C++ with an FP64 shim in place of FFTW)' % n}
+    try:
+        n, t, per = rp.run(steps, warmup)
+        out = {'value': n / t, 'unit': 'stamps/s', 'cores': rp.cores, 'kind': 'reference',
+               'sample': '%d steps of %d consecutive stamps of the 4096-stamp batch (cold Sersic tables, '
+                         'one process per core, reference C++ with an FP64 Stockham FFT in place of FFTW)'
+                         % (steps, REF_STEP_STAMPS),
+               'step_ms': [1e3 * v for v in per]}
+        if extras:
+            out.update(rp.extras())
+        return out
+    finally:
+        rp.close()
 
 
 def _ref_interp_worker(args):
@@ -646,24 +760,42 @@ def cpu_interp_rate(params, psf, budget_s=8.):
                       'SBInterpolatedImage and SBSersic, one process per core)' % n}
 
 
+def workload_config(stamps=B_DEFAULT):
+    """The workload both arms are quoted on."""
+    return {'workload': 'sersic_kolmogorov_pixel_4096_seed1234', 'stamps_per_gpu': stamps,
+            'scale': SCALE, 'gsparams': 'default', 'image_dtype': 'float32', 'sizes': 'automatic'}
+
+
 def run_reference(args):
+    """The reference's own CPU implementation of the path (its C++ from oracle/_ref, built
+    from the reference sources) on all host cores: W warm-up and K timed steps of
+    REF_STEP_STAMPS stamps each, consecutive through the batch."""
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
         return
     params = workload_params()
-    res = cpu_reference_rate(params, budget_s=max(5., 20. / max(args.steps, 1)))
-    if res is None:
+    rp = RefPool(params)
+    if not rp.available:
         print(json.dumps({'impl': 'reference', 'unavailable': 'oracle/_ref/libgsref.so is not built'}))
         return
-    line = {'metric': 'stamps/s', 'value': res['value'], 'unit': 'stamps/s', 'n_gpus': args.gpus,
-            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * B_DEFAULT / res['value'],
+    try:
+        n, t, per = rp.run(args.steps, args.warmup)
+        ext = rp.extras()
+    finally:
+        rp.close()
+    value = n / t
+    cb = {'value': value, 'unit': 'stamps/s', 'cores': rp.cores, 'kind': 'reference',
+          'sample': 'each step %d consecutive stamps of the 4096-stamp batch, cycling (cold Sersic '
+                    'tables, one process per core, reference C++ with an FP64 Stockham FFT in place '
+                    'of FFTW)' % REF_STEP_STAMPS}
+    cb.update(ext)
+    line = {'metric': 'stamps/s', 'value': value, 'unit': 'stamps/s', 'n_gpus': args.gpus,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * t / args.steps,
+            'stamps_per_step': REF_STEP_STAMPS,
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
-            'data': 'synthetic', 'impl': 'reference',
-            'config': {'workload': 'sersic_kolmogorov_pixel_4096_seed1234', 'stamps': B_DEFAULT,
-                       'scale': SCALE, 'gsparams': 'default'},
-            'cpu_baseline': res,
-            'e2e': {'value': res['value'], 'unit': 'stamps/s', 'h2d_bytes_per_step': 0,
-                    'd2h_bytes_per_step': 0}}
+            'data': 'synthetic', 'impl': 'reference', 'config': workload_config(),
+            'cpu_baseline': cb,
+            'e2e': {'value': value, 'unit': 'stamps/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(line))
 
 
@@ -884,21 +1016,10 @@ def run_gpu(args):
     torch.cuda.synchronize(dev)
     plain_rate = n_plain / (tp0.elapsed_time(tp1) * 1e-3)
 
-    # FP32 error of the measured path against the FP64 kernels (which match the reference to
-    # 1e-9 x peak on its fixtures), on a leading sample of the batch
-    ns = min(256, B)
-    sub = gpu_object(galsim, params[:ns])
-    a32 = galsim.draw_batch(sub, scale=SCALE, dtype=np.float32)
-    a64 = galsim.draw_batch(sub, scale=SCALE, dtype=np.float64, precision='fp64')
-    errs = []
-    for i in range(ns):
-        o, m = int(a32.offsets[i]), int(a32.nx[i] * a32.ny[i])
-        d = (a32.flat[o:o + m].double() - a64.flat[o:o + m]).abs().max().item()
-        errs.append(d / a64.flat[o:o + m].abs().max().item())
-    ferr = np.abs(a32.added_flux - a64.added_flux) / np.abs(a64.added_flux)
-    fp32_err = {'stamps': ns, 'max_abs_over_peak_median': float(np.median(errs)),
-                'max_abs_over_peak_max': float(np.max(errs)), 'flux_rel_median': float(np.median(ferr)),
-                'flux_rel_max': float(np.max(ferr)), 'against': 'FP64 kernels of this library'}
+    # FP32 error of the measured path against the reference: the last timed step's first
+    # stamps against the same stamps drawn one by one by the reference's own drawImage
+    # (tests/golden/reference_configs.npz, the leading 256 stamps of this workload)
+    fp32_err = fp32_error_vs_reference(st)
 
     fit = run_fit_step(args, galsim, dev, max(args.steps, 3), max(args.warmup, 2))
     mixed = run_mixed(galsim, dev, max(args.steps, 3), max(args.warmup, 2)) if not args.no_extra else None
@@ -915,22 +1036,32 @@ def run_gpu(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_reference_rate(params, budget_s=15.)
+        cpu = cpu_reference_rate(params, steps=3, warmup=1, extras=True)
 
     if rank == 0:
+        # per-stamp lists go to a side file; the JSON line keeps their summaries
+        detail = {'large_stamps': large, 'step_fft_sizes': [int(v) for v in N]}
+        if large is not None:
+            large = {k: v for k, v in large.items() if not isinstance(v, list)}
+            ls = detail['large_stamps']
+            large.update({'fft_sizes': sorted(set(ls['fft_sizes'])),
+                          'fp32_max_abs_err_over_peak_max': max(ls['fp32_max_abs_err_over_peak']),
+                          'fp32_flux_rel_err_max': max(ls['fp32_flux_rel_err']),
+                          'per_stamp': 'bench_detail.json'})
+        write_detail(detail)
         line = {
             'metric': 'stamps/s', 'value': value, 'unit': 'stamps/s', 'n_gpus': world,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms,
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
             'data': 'synthetic',
-            'config': {'workload': 'sersic_kolmogorov_pixel_4096_seed1234', 'stamps_per_gpu': B,
-                       'scale': SCALE, 'gsparams': 'default', 'fft_sizes': sorted(set(int(v) for v in N)),
-                       'parallelism': 'replicas x%d' % world,
-                       'draw_stage': ('one CUDA graph replay per step (FFT-size buckets on forked streams)'
-                                      if getattr(prog, '_graph_state', None) and prog._graph_state.get('graph')
-                                      else 'eager launches'),
-                       'autotuned_variants': _lib.tune_report().splitlines(),
-                       'l2': 'no flush; per-step table build and stamp outputs exceed L2 reuse'},
+            'config': workload_config(B),
+            'path': {'fft_sizes': sorted(set(int(v) for v in N)),
+                     'parallelism': 'replicas x%d' % world,
+                     'draw_stage': ('one CUDA graph replay per step (FFT-size buckets on forked streams)'
+                                    if getattr(prog, '_graph_state', None) and prog._graph_state.get('graph')
+                                    else 'eager launches'),
+                     'autotuned_variants': _lib.tune_report().splitlines(),
+                     'l2': 'no flush; per-step table build and stamp outputs exceed L2 reuse'},
             'e2e': {'value': world * B / (e2e_ms * 1e-3), 'unit': 'stamps/s',
                     'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': d2h,
                     'mode': 'host parameters -> draw_batch -> host pixels and fluxes; step k read '
@@ -946,9 +1077,7 @@ def run_gpu(args):
             # per step: the Sersic table build, one leaf-prepare launch and one fused draw per
             # FFT-size bucket
             'gpu_launches': int(args.steps * (table_build_launches(params[:, 0]) + 1 + nb)),
-            'plain_one_stamp_per_launch': {'value': plain_rate, 'unit': 'stamps/s', 'sample': n_plain},
-            'fp32_error_vs_fp64': fp32_err,
-            'grad_evals': fit,
+            'fp32_error_vs_reference': fp32_err,
             'mixed_batch': mixed,
             'large_stamps': large,
             'interp_psf': interp,
@@ -958,6 +1087,9 @@ def run_gpu(args):
         }
         if cpu is not None:
             line['cpu_baseline'] = cpu
+        # the headline's second half last, so that a cut-off tail still shows it
+        line['plain_one_stamp_per_launch'] = {'value': plain_rate, 'unit': 'stamps/s', 'sample': n_plain}
+        line['grad_evals'] = fit
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()

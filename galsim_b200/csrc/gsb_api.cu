@@ -38,6 +38,7 @@ namespace {
 thread_local std::string g_err;
 std::mutex g_mu;
 DeviceState g_state[64];
+}  // namespace
 
 int validate_template(const gsb_template* tpl)
 {
@@ -83,7 +84,6 @@ bool good_fft_size_ok(int n)
     while (n % 2 == 0) n /= 2;
     return n == 1 || n == 3;
 }
-}  // namespace
 
 int set_error(int code, const std::string& msg)
 {

@@ -14,6 +14,11 @@ namespace gsb {
 // Records the message for gsb_last_error() and returns the code.
 int set_error(int code, const std::string& msg);
 
+// Host-side checks shared by the entry points: a template's sizes, program (stack discipline,
+// indices) and leaf types; an FFT size of the form 2^a or 3 * 2^a.
+int validate_template(const gsb_template* tpl);
+bool good_fft_size_ok(int n);
+
 #define GSB_CUDA_CHECK(expr)                                                              \
     do {                                                                                  \
         cudaError_t e_ = (expr);                                                          \

@@ -15,12 +15,20 @@
 //   * FFT sizes up to 1024 are accepted; larger sizes (the two-kernel large-FFT path) are
 //     rejected with GSB_ERR_UNSUPPORTED.  When the slabs of a full grid do not fit, the grid is
 //     reduced to the number of slabs that do, so large N runs with fewer CTAs.
-//   * The first call on a device looks up the array's device address (cudaGetSymbolAddress)
-//     with that device current; make that first call before any stream capture.
+//   * Every stamp's FFT size must equal the N argument.  A small check kernel compares them
+//     first and records a mismatch in a status word that is also static device memory; the
+//     call reads that word back (so it returns once the stream has reached the check) and
+//     refuses the draw with GSB_ERR_INVALID.
+//   * Programs with InterpolatedImage leaves are accepted as in gsb_draw_images; programs
+//     without them run the kernel instance compiled without the image-leaf code, as there.
+//   * The first call on a device looks up the device addresses of the array and of the
+//     status word (cudaGetSymbolAddress) with that device current; make that first call
+//     before any stream capture.  The addresses are kept for the life of the process, so the
+//     library must not be used on a device after cudaDeviceReset.
 //   * Every call shares the one array and nothing in it needs to start at zero (each slab
-//     region is fully written before it is read).  Calls whose kernels overlap on the GPU --
-//     on different streams, or from different host threads -- race on the array; serialise
-//     them on one stream.
+//     region is fully written before it is read; the status word is cleared by each call).
+//     Calls whose kernels overlap on the GPU -- on different streams, or from different host
+//     threads -- race on the array; serialise them on one stream.
 #include <mutex>
 
 #include "gsb_draw.cuh"
@@ -34,15 +42,18 @@ constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
 // Device-side scratch.  In host code this name is only a handle for cudaGetSymbolAddress,
 // never a device address: the address is looked up per device below.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+// Stamp-geometry check result of the current call (nonzero: a stamp's N differs from N).
+static __device__ int g_noalloc_status;
 
 struct NoAllocDevice {
     bool ready = false;
     void* ptr = nullptr;
+    int* status = nullptr;
 };
 NoAllocDevice g_noalloc_dev[64];
 std::mutex g_noalloc_mu;
 
-int noalloc_scratch(void** out)
+int noalloc_scratch(void** out, int** status)
 {
     int dev = 0;
     GSB_CUDA_CHECK(cudaGetDevice(&dev));
@@ -55,10 +66,49 @@ int noalloc_scratch(void** out)
         if (e != cudaSuccess)
             return set_error(GSB_ERR_CUDA, std::string("cudaGetSymbolAddress(no-alloc scratch): ") +
                                            cudaGetErrorString(e));
+        void* q = nullptr;
+        const cudaError_t e2 = cudaGetSymbolAddress(&q, g_noalloc_status);
+        if (e2 != cudaSuccess)
+            return set_error(GSB_ERR_CUDA, std::string("cudaGetSymbolAddress(no-alloc status): ") +
+                                           cudaGetErrorString(e2));
         d.ptr = p;
+        d.status = static_cast<int*>(q);
         d.ready = true;
     }
     *out = d.ptr;
+    if (status) *status = d.status;
+    return GSB_OK;
+}
+
+__global__ void noalloc_check_kernel(const gsb_stamp* stamps, int n_stamps, int N, int* status)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n_stamps && stamps[s].N != N) atomicOr(status, 1);
+}
+
+// Every stamp's N against the call's N, on the device; the answer is read back before drawing.
+int noalloc_check_stamps(const gsb_stamp* d_stamps, int n_stamps, int N, int* d_status, cudaStream_t stream)
+{
+    GSB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), stream));
+    noalloc_check_kernel<<<(n_stamps + 255) / 256, 256, 0, stream>>>(d_stamps, n_stamps, N, d_status);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    int h = 0;
+    GSB_CUDA_CHECK(cudaMemcpyAsync(&h, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    GSB_CUDA_CHECK(cudaStreamSynchronize(stream));
+    if (h) return set_error(GSB_ERR_INVALID, "gsb_draw_images_noalloc: a stamp's FFT size differs from N = " +
+                                             std::to_string(N));
+    return GSB_OK;
+}
+
+template <typename T, int N, bool II>
+int launch_noalloc_ii(const DrawArgs& args, int grid, cudaStream_t stream)
+{
+    constexpr bool wsmem = w_fits_smem<T, N>();
+    constexpr size_t sm = smem_bytes<T, N>(wsmem);
+    GSB_CUDA_CHECK(cudaFuncSetAttribute(draw_fused_kernel<T, N, wsmem, II>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    draw_fused_kernel<T, N, wsmem, II><<<grid, fused_warps<T, N>() * 32, sm, stream>>>(args);
+    GSB_CUDA_CHECK(cudaGetLastError());
     return GSB_OK;
 }
 
@@ -66,25 +116,25 @@ template <typename T, int N>
 int launch_noalloc(DrawArgs args, cudaStream_t stream)
 {
     constexpr bool wsmem = w_fits_smem<T, N>();
-    constexpr size_t sm = smem_bytes<T, N>(wsmem);
     int grid = draw_grid<T, N>(args.n_stamps);
+    void* p = nullptr;
+    int* status = nullptr;
+    int rc = noalloc_scratch(&p, &status);
+    if (rc) return rc;
+    rc = noalloc_check_stamps(args.stamps, args.n_stamps, N, status, stream);
+    if (rc) return rc;
     if (!wsmem) {
         constexpr size_t slab = sizeof(Cx<T>) * (size_t)(N / 2 + 1) * (N + 1);
         static_assert(slab <= kNoAllocScratchBytes, "one slab must fit the no-alloc scratch");
         const int fit = int(kNoAllocScratchBytes / slab);
         if (grid > fit) grid = fit;
-        void* p = nullptr;
-        const int rc = noalloc_scratch(&p);
-        if (rc) return rc;
         args.work = p;
     } else {
         args.work = nullptr;
     }
-    GSB_CUDA_CHECK(cudaFuncSetAttribute(draw_fused_kernel<T, N, wsmem>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-    draw_fused_kernel<T, N, wsmem><<<grid, fused_warps<T, N>() * 32, sm, stream>>>(args);
-    GSB_CUDA_CHECK(cudaGetLastError());
-    return GSB_OK;
+    // programs without image leaves run the instance compiled without their code
+    return has_image_leaves(args.tpl) ? launch_noalloc_ii<T, N, true>(args, grid, stream)
+                                      : launch_noalloc_ii<T, N, false>(args, grid, stream);
 }
 
 template <typename T>
@@ -107,36 +157,6 @@ int dispatch_noalloc(int N, const DrawArgs& args, cudaStream_t stream)
                                           "from 32 to 1024; got " + std::to_string(N));
 }
 
-int validate_noalloc_template(const gsb_template* tpl)
-{
-    if (!tpl || tpl->n_ops < 1 || tpl->n_ops > GSB_MAX_OPS || tpl->n_leaves < 1 ||
-        tpl->n_leaves > GSB_MAX_LEAVES || tpl->n_phases < 0 || tpl->n_phases > GSB_MAX_PHASES ||
-        tpl->n_scales < 0 || tpl->n_scales > GSB_MAX_SCALES)
-        return set_error(GSB_ERR_INVALID, "template sizes out of range");
-    int depth = 0;
-    for (int o = 0; o < tpl->n_ops; ++o) {
-        const int c = tpl->op_code[o], a = tpl->op_arg[o];
-        if (c == GSB_OP_LEAF) {
-            if (a < 0 || a >= tpl->n_leaves) return set_error(GSB_ERR_INVALID, "leaf index out of range");
-            ++depth;
-        } else if (c == GSB_OP_MUL || c == GSB_OP_ADD) {
-            if (depth < 2) return set_error(GSB_ERR_INVALID, "program stack underflow");
-            --depth;
-        } else if (c == GSB_OP_PHASE) {
-            if (a < 0 || a >= tpl->n_phases || depth < 1) return set_error(GSB_ERR_INVALID, "bad PHASE op");
-        } else if (c == GSB_OP_SCALE) {
-            if (a < 0 || a >= tpl->n_scales || depth < 1) return set_error(GSB_ERR_INVALID, "bad SCALE op");
-        } else {
-            return set_error(GSB_ERR_INVALID, "unknown opcode");
-        }
-    }
-    if (depth != 1) return set_error(GSB_ERR_INVALID, "program must leave exactly one value");
-    for (int l = 0; l < tpl->n_leaves; ++l)
-        if (tpl->leaf_type[l] < GSB_GAUSSIAN || tpl->leaf_type[l] > GSB_BOX)
-            return set_error(GSB_ERR_INVALID, "unknown leaf type");
-    return GSB_OK;
-}
-
 }  // namespace
 
 }  // namespace gsb
@@ -150,7 +170,7 @@ extern "C" int gsb_draw_images_noalloc(const gsb_template* tpl, int n_stamps, co
                                        int add_to_image, double* d_added_flux, int precision,
                                        void* stream)
 {
-    int rc = validate_noalloc_template(tpl);
+    int rc = validate_template(tpl);
     if (rc) return rc;
     if (!gsp) return set_error(GSB_ERR_INVALID, "null gsparams");
     if (n_stamps < 0) return set_error(GSB_ERR_INVALID, "negative stamp count");

@@ -349,12 +349,17 @@ int gsb_draw_kimages(const gsb_template* tpl, int n_stamps, const gsb_gsparams* 
 /* gsb_draw_images without any device allocation.  This entry point has no counterpart in
  * the reference; it exists for callers that cannot allocate device memory while they draw
  * (an application that owns a fixed GPU memory budget, or a plugin inside another program's
- * memory pool).  Same inputs and outputs as gsb_draw_images for one FFT-size bucket, with the
- * bucket's FFT size N passed explicitly (32 <= N <= 1024, 2^a or 3*2^a).  The scratch that
- * gsb_draw_images takes from the caller comes instead from a 32 MiB array compiled into the
- * library (held by every GPU that loads it until exit).  The first call on a device looks up
- * that array's address and should come before any stream capture.  All calls share the array:
- * calls that overlap on the GPU race, so serialise them on one stream. */
+ * memory pool).  Same inputs and outputs as gsb_draw_images for one FFT-size bucket
+ * (InterpolatedImage leaves included), with the bucket's FFT size N passed explicitly
+ * (32 <= N <= 1024, 2^a or 3*2^a; larger N returns GSB_ERR_UNSUPPORTED).  Every stamp's N
+ * must equal N: a check on the device compares them before the draw and a mismatch returns
+ * GSB_ERR_INVALID (the call reads that check back, so it returns once the stream has reached
+ * it).  The scratch that gsb_draw_images takes from the caller comes instead from a 32 MiB
+ * array compiled into the library (held by every GPU that loads it until exit).  The first
+ * call on a device looks up that array's address and should come before any stream capture;
+ * the address is kept, so do not use the library on a device after cudaDeviceReset.  All
+ * calls share the array: calls that overlap on the GPU race, so serialise them on one
+ * stream. */
 int gsb_draw_images_noalloc(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp,
                             const gsb_leaf* d_leaves, const gsb_phase* d_phases,
                             const double* d_scales, const gsb_stamp* d_stamps,

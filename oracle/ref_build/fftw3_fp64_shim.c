@@ -2,13 +2,14 @@
  * FP64 stand-in for the subset of the FFTW3 API that the reference's image code calls
  * (src/Image.cpp: rfft, irfft, cfft; src/hsm/PSFCorr.cpp is not built).
  *
- * ORACLE-ONLY test infrastructure.  libfftw3 is not installed on this machine, so the
- * reference C++ is linked against this file to be able to run its drawImage path on the
- * CPU.  The transform is a plain recursive mixed-radix Cooley-Tukey FFT in double
- * precision (radix 2 and 3 butterflies, an O(n*p) DFT for any other prime factor p), with
- * FFTW's sign and normalisation conventions:
+ * ORACLE-ONLY test infrastructure.  libfftw3 is not installed where the oracle is built,
+ * so the reference C++ is linked against this file to run its drawImage path on the CPU.
+ * The transform is an iterative mixed-radix Stockham FFT in double precision: radix-4 and
+ * radix-2 passes first, then 3, then a direct pass for any other prime factor, with the
+ * twiddles exp(2 pi i m / n) tabulated once per length (per thread) and exact integer
+ * exponents (m = r k n / (ns p) < n).  Conventions are FFTW's:
  *   out[k] = sum_j in[j] exp(sign * 2 pi i j k / n),  unnormalised,
- * and FFTW's half-complex array layouts for r2c / c2r, including the padded in-place
+ * with FFTW's half-complex array layouts for r2c / c2r, including the padded in-place
  * layout (real rows of stride 2*(n1/2+1) when in == out).
  * It is checked against numpy.fft (pocketfft, FP64) in tests/test_oracle_fft_shim.py.
  */
@@ -31,65 +32,104 @@ struct fftw_plan_s {
     void *out;
 };
 
-static void dft_rec(const double complex *x, double complex *y, int n, int stride, int sign,
-                    double complex *scratch)
+/* exp(+2 pi i m / n) for m < n, cached per length (a few lengths per thread). */
+#define TW_SLOTS 8
+static __thread int tw_len[TW_SLOTS];
+static __thread double complex *tw_tab[TW_SLOTS];
+static __thread int tw_next;
+
+static const double complex *twiddles(int n)
 {
-    if (n == 1) { y[0] = x[0]; return; }
-    int p = 0;
-    if (n % 2 == 0) p = 2;
-    else if (n % 3 == 0) p = 3;
-    else {
-        for (int q = 5; q * q <= n; q += 2) if (n % q == 0) { p = q; break; }
-        if (p == 0) p = n;
+    for (int i = 0; i < TW_SLOTS; ++i)
+        if (tw_len[i] == n && tw_tab[i]) return tw_tab[i];
+    const int slot = tw_next;
+    tw_next = (tw_next + 1) % TW_SLOTS;
+    free(tw_tab[slot]);
+    double complex *t = (double complex *)malloc(sizeof(double complex) * (size_t)n);
+    for (int m = 0; m < n; ++m) {
+        const double a = 2.0 * M_PI * (double)m / (double)n;
+        t[m] = cos(a) + I * sin(a);
     }
-    const int m = n / p;
-    if (m == 1) {
-        /* direct DFT of a prime length */
-        for (int k = 0; k < n; ++k) {
-            double complex acc = 0;
-            for (int j = 0; j < n; ++j) {
-                double ang = sign * 2.0 * M_PI * (double)((long)j * k % n) / n;
-                acc += x[j * stride] * (cos(ang) + I * sin(ang));
+    /* the quarter turns exactly */
+    if (n % 4 == 0) { t[n / 4] = I; t[3 * n / 4] = -I; }
+    if (n % 2 == 0) t[n / 2] = -1.0;
+    t[0] = 1.0;
+    tw_tab[slot] = t;
+    tw_len[slot] = n;
+    return t;
+}
+
+static int smallest_factor(int m)
+{
+    if (m % 4 == 0) return 4;
+    if (m % 2 == 0) return 2;
+    if (m % 3 == 0) return 3;
+    for (int q = 5; q * q <= m; q += 2) if (m % q == 0) return q;
+    return m;
+}
+
+/* In-place length-n DFT of x (contiguous) with scratch y (n values). */
+static void fft_inplace(double complex *x, double complex *y, int n, int sign)
+{
+    if (n <= 1) return;
+    const double complex *tw = twiddles(n);
+    double complex *src = x, *dst = y;
+    double complex vbuf[64], obuf[64];
+    int ns = 1;
+    while (ns < n) {
+        const int p = smallest_factor(n / ns);
+        const int nb = n / p;
+        const int tstep = n / (ns * p);
+        double complex *v = p <= 64 ? vbuf : (double complex *)malloc(sizeof(double complex) * p);
+        double complex *o = p <= 64 ? obuf : (double complex *)malloc(sizeof(double complex) * p);
+        for (int b = 0; b < nb; ++b) {
+            const int k = b % ns;
+            v[0] = src[b];
+            for (int r = 1; r < p; ++r) {
+                const double complex w = tw[(long)r * k * tstep % n];
+                v[r] = src[b + r * nb] * (sign > 0 ? w : conj(w));
             }
-            scratch[k] = acc;
-        }
-        memcpy(y, scratch, sizeof(double complex) * n);
-        return;
-    }
-    /* sub-transforms of the p decimated sequences, stored contiguously in y */
-    for (int r = 0; r < p; ++r)
-        dft_rec(x + r * stride, y + r * m, m, stride * p, sign, scratch);
-    /* combine: Y[k + q m] = sum_r W_n^{r (k + q m)} Y_r[k] */
-    double complex tmp[64];
-    double complex *t = (p <= 64) ? tmp : (double complex *)malloc(sizeof(double complex) * p);
-    for (int k = 0; k < m; ++k) {
-        for (int r = 0; r < p; ++r) {
-            double ang = sign * 2.0 * M_PI * (double)r * k / n;
-            t[r] = y[r * m + k] * (cos(ang) + I * sin(ang));
-        }
-        for (int q = 0; q < p; ++q) {
-            double complex acc = 0;
-            for (int r = 0; r < p; ++r) {
-                double ang = sign * 2.0 * M_PI * (double)((long)r * q % p) / p;
-                acc += t[r] * (cos(ang) + I * sin(ang));
+            if (p == 2) {
+                o[0] = v[0] + v[1];
+                o[1] = v[0] - v[1];
+            } else if (p == 4) {
+                const double complex s0 = v[0] + v[2], s1 = v[0] - v[2];
+                const double complex s2 = v[1] + v[3];
+                const double complex d = v[1] - v[3];
+                const double complex s3 = sign > 0 ? I * d : -I * d;
+                o[0] = s0 + s2; o[1] = s1 + s3; o[2] = s0 - s2; o[3] = s1 - s3;
+            } else {
+                /* direct p-point DFT; exp(2 pi i m / p) = tw[m n / p] */
+                const int step = n / p;
+                for (int q = 0; q < p; ++q) {
+                    double complex acc = 0;
+                    for (int r = 0; r < p; ++r) {
+                        const double complex w = tw[(long)((long)r * q % p) * step];
+                        acc += v[r] * (sign > 0 ? w : conj(w));
+                    }
+                    o[q] = acc;
+                }
             }
-            scratch[k + q * m] = acc;
+            const int base = (b / ns) * ns * p + k;
+            for (int q = 0; q < p; ++q) dst[base + q * ns] = o[q];
         }
+        if (v != vbuf) free(v);
+        if (o != obuf) free(o);
+        double complex *t = src; src = dst; dst = t;
+        ns *= p;
     }
-    memcpy(y, scratch, sizeof(double complex) * n);
-    if (t != tmp) free(t);
+    if (src != x) memcpy(x, src, sizeof(double complex) * (size_t)n);
 }
 
 /* One 1-d transform of n points read with stride `is` and written with stride `os`. */
 static void fft1(const double complex *in, int is, double complex *out, int os, int n, int sign)
 {
-    double complex *x = (double complex *)malloc(sizeof(double complex) * n);
-    double complex *y = (double complex *)malloc(sizeof(double complex) * n);
-    double complex *s = (double complex *)malloc(sizeof(double complex) * n);
+    double complex *x = (double complex *)malloc(sizeof(double complex) * (size_t)n * 2);
+    double complex *y = x + n;
     for (int j = 0; j < n; ++j) x[j] = in[(long)j * is];
-    dft_rec(x, y, n, 1, sign, s);
-    for (int j = 0; j < n; ++j) out[(long)j * os] = y[j];
-    free(x); free(y); free(s);
+    fft_inplace(x, y, n, sign);
+    for (int j = 0; j < n; ++j) out[(long)j * os] = x[j];
+    free(x);
 }
 
 static fftw_plan make_plan(int kind, int rank, int n0, int n1, int sign, void *in, void *out)

@@ -1,4 +1,4 @@
-"""ORACLE-ONLY: import the reference GalSim Python package in this container.
+"""ORACLE-ONLY: import the reference GalSim Python package from its checkout.
 
 The reference package (``galsim/`` under the reference checkout) is loaded unmodified from
 its own directory; its compiled extension ``_galsim`` comes from ``oracle/_ref`` (built by

@@ -1,7 +1,7 @@
 """Make the golden fixtures in tests/golden/ by running the reference GalSim itself.
 
-    make -C oracle ref               # build the reference C++ into oracle/_ref (once)
-    python tests/golden/make_golden.py /path/to/reference
+    make -C oracle ref REF=/path/to/reference    # build the reference C++ into oracle/_ref
+    python tests/golden/make_golden.py /path/to/reference [--configs-only | --grad-only | ...]
 
 The reference Python package is imported from its checkout with the extension built from
 its own C++ sources (oracle/ref_import.py).  Everything drawn here goes through the
@@ -409,6 +409,108 @@ def main_fits(ref_root):
     print('wrote', os.path.join(HERE, 'reference_fits.npz'), len(out), 'files')
 
 
+# The batched configurations at their own settings: stamps of bench.py's seeded generators
+# drawn one by one by the reference's drawImage.  Per stamp: its shape, the centred
+# CFG_BLOCK x CFG_BLOCK block, a CFG_STRIDE-strided pixel grid, the added flux, the peak and
+# the (N, Nk) that the reference's drawFFT_makeKImage chose (recorded by wrapping it).
+#   batched forward: the leading CFG_C2_STAMPS stamps of the 4096-stamp workload (seed 1234),
+#     default GSParams, automatically sized float32 images at scale 0.2;
+#   mixed bulge+disk: GSParams(minimum_fft_size=32), the leading CFG_C4_LEADING stamps of the
+#     16384-stamp workload (seed 2468) and up to CFG_C4_PER_N more per FFT size among the first
+#     CFG_C4_POOL stamps, so that every size of the batch is covered.
+CFG_BLOCK = 24
+CFG_STRIDE = 7
+CFG_C2_STAMPS = 256
+CFG_C4_LEADING = 16
+CFG_C4_PER_N = 3
+CFG_C4_POOL = 4096
+
+
+def bench_module():
+    sys.path.insert(0, ROOT)
+    import bench
+    return bench
+
+
+def config_sample(a):
+    """The centred block and the strided grid of a stamp (shared with the tests)."""
+    ny, nx = a.shape
+    b = min(CFG_BLOCK, nx, ny)
+    y0, x0 = (ny - b) // 2, (nx - b) // 2
+    return a[y0:y0 + b, x0:x0 + b], a[::CFG_STRIDE, ::CFG_STRIDE]
+
+
+def c2_object(galsim, p):
+    n, hlr, flux, g1, g2, fwhm = p
+    gal = galsim.Sersic(n=n, half_light_radius=hlr, flux=flux).shear(g1=g1, g2=g2)
+    return galsim.Convolve(gal, galsim.Kolmogorov(fwhm=fwhm), galsim.Pixel(0.2))
+
+
+def c4_object(galsim, m, i, gsp):
+    bulge = galsim.Sersic(n=4., half_light_radius=m['bh'][i], flux=m['flux'][i] * m['bf'][i],
+                          gsparams=gsp).shear(g1=m['g_b'][i, 0], g2=m['g_b'][i, 1])
+    disk = galsim.Exponential(half_light_radius=m['dh'][i], flux=m['flux'][i] * (1. - m['bf'][i]),
+                              gsparams=gsp).shear(g1=m['g_d'][i, 0], g2=m['g_d'][i, 1])
+    psf = galsim.Moffat(beta=m['beta'][i], fwhm=m['fwhm'][i], gsparams=gsp)
+    return galsim.Convolve(galsim.Add(bulge, disk), psf, galsim.Pixel(0.2, gsparams=gsp))
+
+
+def _record_sizes(galsim):
+    """Wrap the reference's drawFFT_makeKImage so that each draw leaves its (N, Nk)."""
+    rec = []
+    orig = galsim.GSObject.drawFFT_makeKImage
+
+    def wrapped(self, image):
+        kimage, N = orig(self, image)
+        rec.append((int(N), int(kimage.bounds.xmax * 2)))
+        return kimage, N
+    galsim.GSObject.drawFFT_makeKImage = wrapped
+    return rec
+
+
+def main_configs(ref_root):
+    from ref_import import import_reference_galsim
+    galsim = import_reference_galsim(ref_root)
+    bench = bench_module()
+    sizes = _record_sizes(galsim)
+    out = {}
+
+    def store(prefix, ims):
+        out[prefix + '_shape'] = np.array([im.array.shape for im in ims])
+        out[prefix + '_flux'] = np.array([im.added_flux for im in ims])
+        out[prefix + '_peak'] = np.array([np.abs(im.array).max() for im in ims])
+        out[prefix + '_N_Nk'] = np.array(sizes[-len(ims):])
+        blocks, grids = zip(*[config_sample(im.array) for im in ims])
+        out[prefix + '_block'] = np.concatenate([b.ravel() for b in blocks])
+        out[prefix + '_grid'] = np.concatenate([g.ravel() for g in grids])
+
+    p2 = bench.workload_params(CFG_C2_STAMPS)
+    ims = [c2_object(galsim, p).drawImage(scale=0.2, dtype=np.float32, method='fft') for p in p2]
+    store('c2', ims)
+    out['c2_params'] = p2
+
+    gsp = galsim.GSParams(minimum_fft_size=32)
+    m = bench.mixed_params()
+    # the FFT size of each pool stamp, from the reference's own sizing (a draw of the stamp)
+    pool_N = []
+    for i in range(CFG_C4_POOL):
+        c4_object(galsim, m, i, gsp).drawImage(scale=0.2, dtype=np.float32, method='fft')
+        pool_N.append(sizes[-1][0])
+    pick = list(range(CFG_C4_LEADING))
+    for N in sorted(set(pool_N)):
+        cand = [i for i in range(CFG_C4_POOL) if pool_N[i] == N and i not in pick]
+        pick += cand[:CFG_C4_PER_N]
+    ims = [c4_object(galsim, m, i, gsp).drawImage(scale=0.2, dtype=np.float32, method='fft') for i in pick]
+    store('c4', ims)
+    out['c4_index'] = np.array(pick)
+    out['c4_pool_N'] = np.array(pool_N)
+    out['cfg_block'] = np.array(CFG_BLOCK)
+    out['cfg_stride'] = np.array(CFG_STRIDE)
+    np.savez_compressed(os.path.join(HERE, 'reference_configs.npz'), **out)
+    print('wrote', os.path.join(HERE, 'reference_configs.npz'), len(out), 'arrays;',
+          'C4 sizes', dict(zip(*np.unique(out['c4_N_Nk'][:, 0], return_counts=True))))
+
+
 def main(ref_root):
     from ref_import import import_reference_galsim
     galsim = import_reference_galsim(ref_root)
@@ -457,7 +559,9 @@ def main(ref_root):
 
 if __name__ == '__main__':
     args = [a for a in sys.argv[1:] if not a.startswith('--')]
-    root = args[0] if args else '/root/reference'
+    root = args[0] if args else os.environ.get('GSB_REFERENCE')
+    if not root:
+        sys.exit('usage: make_golden.py REFERENCE_CHECKOUT [--<part>-only] (or set GSB_REFERENCE)')
     if '--grad-only' in sys.argv:
         main_grad(root)
     elif '--interp-only' in sys.argv:
@@ -468,6 +572,8 @@ if __name__ == '__main__':
         main_config(root)
     elif '--fits-only' in sys.argv:
         main_fits(root)
+    elif '--configs-only' in sys.argv:
+        main_configs(root)
     else:
         if '--large-only' not in sys.argv:
             main(root)
@@ -477,3 +583,4 @@ if __name__ == '__main__':
         main_interp(root)
         main_noise(root)
         main_fits(root)
+        main_configs(root)

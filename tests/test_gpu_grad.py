@@ -55,6 +55,15 @@ def _trees():
         galsim.Moffat(beta=1.5, scale_radius=0.3) * 1.7,
         galsim.Moffat(beta=3.5, fwhm=0.5),
         galsim.Box(0.3, 0.2))
+    # the mixed bulge+disk configuration at its own GSParams: Sersic(n=4) + Exponential with
+    # independent shears, general-beta Moffat, minimum_fft_size=32
+    gsp = galsim.GSParams(minimum_fft_size=32)
+    yield 'bulge_disk_moffat_gen_min32', galsim.Convolve(
+        galsim.Add(galsim.Sersic(n=4., half_light_radius=u(0.3, 0.5), flux=u(1e3, 3e3), gsparams=gsp)
+                   .shear(g1=u(-0.3, 0.3), g2=u(-0.3, 0.3)),
+                   galsim.Exponential(half_light_radius=u(0.6, 1.0), flux=u(2e3, 5e3), gsparams=gsp)
+                   .shear(g1=u(-0.3, 0.3), g2=u(-0.3, 0.3))),
+        galsim.Moffat(beta=u(2.6, 4.4), fwhm=u(0.5, 1.0), gsparams=gsp), galsim.Pixel(0.2, gsparams=gsp))
     yield 'gauss_diag_airy_unobscured', galsim.Convolve(
         galsim.Gaussian(sigma=u(0.3, 0.5), flux=u(1e3, 2e3)).dilate(u(0.9, 1.2)),
         galsim.Airy(lam_over_diam=0.15), galsim.Kolmogorov(fwhm=0.7), pix)

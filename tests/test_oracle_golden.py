@@ -60,3 +60,51 @@ def test_wrap_and_irfft(Nk, N):
     assert np.abs(w - GOLD['wrap_out_%d_%d' % (Nk, N)]).max() < 1e-12
     real = O.irfft_shifted(np.array(w), N)
     assert np.abs(real - GOLD['irfft_out_%d_%d' % (Nk, N)]).max() < 1e-12
+
+
+CFG = np.load(specs.HERE + '/reference_configs.npz')
+
+
+def _cfg_stamp(prefix, i):
+    """Stamp i of a configuration sample: shape, (N, Nk), block, grid, flux, peak."""
+    shapes = CFG[prefix + '_shape']
+    bo = go = 0
+    for j in range(i):
+        b = min(MG.CFG_BLOCK, *shapes[j])
+        bo += b * b
+        go += len(range(0, shapes[j][0], MG.CFG_STRIDE)) * len(range(0, shapes[j][1], MG.CFG_STRIDE))
+    b = min(MG.CFG_BLOCK, *shapes[i])
+    ng = len(range(0, shapes[i][0], MG.CFG_STRIDE)) * len(range(0, shapes[i][1], MG.CFG_STRIDE))
+    return (tuple(shapes[i]), tuple(CFG[prefix + '_N_Nk'][i]), CFG[prefix + '_block'][bo:bo + b * b],
+            CFG[prefix + '_grid'][go:go + ng], float(CFG[prefix + '_flux'][i]), float(CFG[prefix + '_peak'][i]))
+
+
+def _check_oracle_stamp(prefix, i, o, gsp):
+    shape, sizes, block, grid, flux, peak = _cfg_stamp(prefix, i)
+    arr, f, N, Nk = O.draw_image(o, shape[1], shape[0], 0.2, gsp=gsp)
+    assert (N, Nk) == sizes
+    b, g = MG.config_sample(arr)
+    # float32 reference images (complex64 k-images)
+    assert np.abs(b.ravel() - block).max() <= 2e-7 * peak
+    assert np.abs(g.ravel() - grid).max() <= 2e-7 * peak
+    assert abs(f - flux) <= 1e-6 * abs(flux)
+
+
+@pytest.mark.parametrize('i', [0, 1, 2])
+def test_batched_forward_sample_stamps(i):
+    n, hlr, flux, g1, g2, fwhm = CFG['c2_params'][i]
+    o = O.OConvolve(O.OSersic(n, hlr=hlr, flux=flux).shear(g1, g2), O.OKolmogorov(fwhm=fwhm), O.OBox(0.2))
+    _check_oracle_stamp('c2', i, o, O.DEFAULT)
+
+
+def test_mixed_sample_stamp_minimum_fft_size_32():
+    """A bulge+disk stamp with GSParams(minimum_fft_size=32): the sizing rule below the default
+    minimum (the smallest FFT size in the sample)."""
+    m = MG.bench_module().mixed_params()
+    sizes = CFG['c4_N_Nk'][:, 0]
+    j = int(np.argmin(sizes))
+    i = int(CFG['c4_index'][j])
+    bulge = O.OSersic(4., hlr=m['bh'][i], flux=m['flux'][i] * m['bf'][i]).shear(*m['g_b'][i])
+    disk = O.OExponential(m['dh'][i] / 1.6783469900166605, m['flux'][i] * (1. - m['bf'][i])).shear(*m['g_d'][i])
+    o = O.OConvolve(O.OSum(bulge, disk), O.OMoffat(m['beta'][i], fwhm=m['fwhm'][i]), O.OBox(0.2))
+    _check_oracle_stamp('c4', j, o, O.OGSParams(minimum_fft_size=32))
