@@ -20,6 +20,7 @@ namespace gsb {
 namespace {
 
 constexpr int kLevMin = 5;
+constexpr int kMaxRounds = 128;      // rounds of ln k nodes per table build (status flags)
 constexpr int kLevMax = 20;
 constexpr long long kNroot = 1000000;
 
@@ -197,6 +198,112 @@ struct SersicRadialDn {
     }
 };
 
+// Two adjacent ln k nodes of one Sersic table in one warp (k0 < k1 = k0 e^dlogk): the terms
+// of both sums at one level share the node load (log x_i, w_i) and the inner exponential,
+//   u0 = (x_i / k0)^(1/n) = exp((log x_i - log k0) / n),   u1 = u0 * exp((log k0 - log k1) / n),
+// so a pair of terms costs three exponentials instead of four, and each lane carries two
+// independent outer exponentials.  Each sum keeps warp_ogata_sum's stopping rule on its own
+// running total (the loop runs until both have stopped; a stopped or inactive sum skips its
+// outer exponential, a warp-uniform branch).  Node 0's terms are warp_ogata_sum's; node 1's
+// u differs from a direct exponential by the rounding of one product (~1e-16 relative), the
+// size of the exponential's own rounding.  The inner argument is bounded (|log x_i - log k|
+// / n < 100 for the tabulated nodes and the tables' k range), so it takes no range test.
+// (Groups of four nodes per warp share more, but their state no longer fits the 64 registers
+// that four 256-thread blocks per SM allow, and they measured slower.)
+template <bool TAB>
+__device__ __forceinline__ double2 warp_ogata_sum_pair(const OgataTables& og, double invn, double c1,
+                                                       double logk0, double logk1, int lev, bool act0,
+                                                       bool act1)
+{
+    const int lane = threadIdx.x & 31;
+    const double h = ldexp(1.0, -lev);
+    const int nmax = (int)fmin(kPi / h, 1e6);
+    const double2* xw = TAB ? og.xw + og.off[lev - og.lev_min] : nullptr;
+    double acc0 = 0., acc1 = 0., th0 = 0., th1 = 0.;
+    int chunk = 0;
+    for (int base = 0; base < nmax; base += 32, ++chunk) {
+        const int i = base + lane;
+        const bool valid = i < nmax;
+        double s0 = 0., s1 = 0.;
+        if (valid) {
+            const double2 n = TAB ? xw[i] : ogata_node(og.root, h, i);
+            const double u0 = exp_tab_core((n.x - logk0) * invn);
+            if (act0) s0 = n.y * exp_tab_neg(-u0);
+            if (act1) s1 = n.y * exp_tab_neg(-(u0 * c1));
+        }
+        if (act0) {
+            const unsigned m0 = __ballot_sync(0xffffffffu, valid && fabs(s0) < th0);
+            if (m0) {
+                acc0 = warp_total(acc0 + (lane <= __ffs(m0) - 1 ? s0 : 0.));
+                act0 = false;
+            } else {
+                acc0 += s0;
+            }
+        }
+        if (act1) {
+            const unsigned m1 = __ballot_sync(0xffffffffu, valid && fabs(s1) < th1);
+            if (m1) {
+                acc1 = warp_total(acc1 + (lane <= __ffs(m1) - 1 ? s1 : 0.));
+                act1 = false;
+            } else {
+                acc1 += s1;
+            }
+        }
+        if (!(act0 || act1)) break;
+        if (chunk < kEagerChunks || (chunk % kLazyChunks) == kLazyChunks - 1) {
+            if (act0) th0 = 1e-15 * fabs(warp_total(acc0));
+            if (act1) th1 = 1e-15 * fabs(warp_total(acc1));
+        }
+    }
+    // sums that ran to nmax without stopping
+    if (act0) acc0 = warp_total(acc0);
+    if (act1) acc1 = warp_total(acc1);
+    const double k0 = exp(logk0), k1 = exp(logk1);
+    return make_double2(acc0 / (k0 * k0), acc1 / (k1 * k1));
+}
+
+// The reference's halving and stopping rule (AdaptiveHankelIntegrator::integrate,
+// Hankel.cpp:179-219) for both nodes of the pair, advanced over one common level index L:
+// node j starts at its own level s_j (h0 = 1/32 halved while h0 > 100 k_j; s_1 <= s_0 since
+// k_1 > k_0), takes the sum at every level from s_j on (ans0 <- ans1, ans1 <- sum(L)) and
+// stops at the first level where the reference's test passes; a node that has stopped, or has
+// not started, does not contribute to the level's sums.  The running answers live in this
+// warp's shared-memory slot `a` (ans0, ans1 of node 0, then of node 1) rather than in
+// registers across the term loop.  has1 = false integrates node 0 alone.
+__device__ double2 warp_hankel_pair(const OgataTables& og, double invn, double logk0, double logk1,
+                                    bool has1, double relerr, double abserr, int* status, double* a)
+{
+    const int lane = threadIdx.x & 31;
+    const double k0 = exp(logk0), k1 = exp(logk1);
+    int s0 = 5, s1 = 5;
+    for (double h0 = 1. / 32.; h0 > 100. * k0 && s0 < 60; h0 *= 0.5) ++s0;
+    for (double h0 = 1. / 32.; h0 > 100. * k1 && s1 < 60; h0 *= 0.5) ++s1;
+    const double c1 = exp((logk0 - logk1) * invn);
+    auto more = [&](double x0, double x1) {
+        const double err = fabs(x1 - x0);
+        return (err > relerr * x1 && (err > abserr || fabs(x1) > 2. * fabs(x0))) || x1 == 0.;
+    };
+    bool run0 = true, run1 = has1;
+    for (int L = has1 ? min(s0, s1) : s0; run0 || run1; ++L) {
+        // the reference halves until its level counter passes 60: the last sum is at 61
+        if (L > 61) { if (status) *status = 1; break; }
+        const bool g0 = run0 && L >= s0, g1 = run1 && L >= s1;
+        const double2 r = (L >= og.lev_min && L <= og.lev_max)
+                              ? warp_ogata_sum_pair<true>(og, invn, c1, logk0, logk1, L, g0, g1)
+                              : warp_ogata_sum_pair<false>(og, invn, c1, logk0, logk1, L, g0, g1);
+        __syncwarp();
+        if (lane == 0) {
+            if (g0) { a[0] = a[1]; a[1] = r.x; }
+            if (g1) { a[2] = a[3]; a[3] = r.y; }
+        }
+        __syncwarp();
+        if (g0 && L > s0) run0 = more(a[0], a[1]);
+        if (g1 && L > s1) run1 = more(a[2], a[3]);
+    }
+    __syncwarp();
+    return make_double2(a[1], a[3]);
+}
+
 struct KolmKValue {
     __device__ double operator()(double logk) const { return exp_tab(-exp_tab(logk * (5. / 3.))); }
 };
@@ -369,11 +476,48 @@ __global__ void __launch_bounds__(256, 4) sersic_nodes_kernel(const double* head
     }
 }
 
-// Advance each table's scan over this round's nodes (SBSersic.cpp:436-509).
+// One warp per pair of adjacent nodes (i, i + 1) of this round: the values of
+// sersic_nodes_kernel<false>, through warp_hankel_pair.  prev_live (the previous round's scan
+// flag) is zero once every table has stopped: the launch then returns at once.
+__global__ void __launch_bounds__(256, 4) sersic_nodes_pair_kernel(const double* header, int count, int i0,
+                                    int nround, gsb_gsparams gsp, const __grid_constant__ OgataTables og,
+                                    const SersicScan* scan, double* vals, int stride,
+                                    const int* prev_live, int* status_out)
+{
+    if (prev_live && *prev_live == 0) return;
+    const int npair = (nround + 1) / 2;
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long s = count - 1 - warp / npair;
+    const int i = i0 + 2 * int(warp % npair);
+    if (s < 0) return;
+    if (scan[s].done) return;
+    const double* H = header + s * kSersicHeader;
+    const int ncand = int(H[kSH_NCAND]);
+    if (i >= ncand) return;
+    const bool has1 = i + 1 < ncand && i + 1 < i0 + nround;
+    const double n = H[kSH_N];
+    const double logk0 = H[kSH_FRONT] + i * H[kSH_DLOGK];
+    const double logk1 = H[kSH_FRONT] + (i + 1) * H[kSH_DLOGK];
+    const double hankel_norm = n * tgamma(2. * n);
+    __shared__ double ans[8][4];           // the running answers of each warp's pair
+    int st = 0;
+    const double2 v = warp_hankel_pair(og, 1. / n, logk0, logk1, has1, gsp.integration_relerr,
+                                       gsp.integration_abserr * hankel_norm, &st, ans[(threadIdx.x >> 5) & 7]);
+    if ((threadIdx.x & 31) == 0) {
+        vals[s * stride + i] = v.x / hankel_norm;
+        if (has1) vals[s * stride + i + 1] = v.y / hankel_norm;
+        if (st) atomicOr(status_out, 1);
+    }
+}
+
+// live_out is set when a table still needs nodes after this round; a zero prev_live (the
+// previous round's flag) means every table has stopped and the launch returns at once.
 __global__ void sersic_scan_kernel(const double* header, int count, int stride, int i0, int nround,
                                    gsb_gsparams gsp, const double* vals, double4* nodes,
-                                   SersicScan* scan, const double* dvals, double4* dnodes)
+                                   SersicScan* scan, const double* dvals, double4* dnodes,
+                                   const int* prev_live, int* live_out)
 {
+    if (prev_live && *prev_live == 0) return;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= count) return;
     if (scan[s].done) return;
@@ -427,6 +571,7 @@ __global__ void sersic_scan_kernel(const double* header, int count, int stride, 
     }
     if (iend >= ncand) S.done = 1;
     scan[s] = S;
+    if (!S.done && live_out) *live_out = 1;
 }
 
 // End of buildFT (SBSersic.cpp:510-537) and the natural spline (Table.cpp:634-686).
@@ -849,7 +994,7 @@ int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc,
         GSB_CUDA_CHECK(cudaMalloc(&t->d_val, sizeof(double) * t->cap_nodes));
         GSB_CUDA_CHECK(cudaMalloc(&t->d_scan, sizeof(SersicScan) * t->cap_slots));
         GSB_CUDA_CHECK(cudaMalloc(&t->d_n, sizeof(double) * t->cap_slots));
-        GSB_CUDA_CHECK(cudaMalloc(&t->d_status, sizeof(int)));
+        GSB_CUDA_CHECK(cudaMalloc(&t->d_status, sizeof(int) * (1 + kMaxRounds)));
     }
     if (with_dn && ((size_t)count > t->cap_dn_slots || (size_t)count * stride > t->cap_dn_nodes)) {
         cudaFree(t->d_dheader); cudaFree(t->d_dnode); cudaFree(t->d_dval);
@@ -869,7 +1014,8 @@ int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc,
     double* d_n = t->d_n;
     int* d_status = t->d_status;
     GSB_CUDA_CHECK(cudaMemcpyAsync(d_n, h_n, sizeof(double) * count, cudaMemcpyHostToDevice, stream));
-    GSB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), stream));
+    // d_status[0]: convergence status; d_status[1 + r]: some table still needs nodes after round r
+    GSB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int) * (1 + kMaxRounds), stream));
     sersic_setup_kernel<<<(count + 127) / 128, 128, 0, stream>>>(d_n, count, *gsp, t->d_header, stride, dheader);
     GSB_CUDA_CHECK(cudaGetLastError());
     sersic_scan_init_kernel<<<(count + 127) / 128, 128, 0, stream>>>(t->d_header, count, static_cast<SersicScan*>(t->d_scan));
@@ -877,21 +1023,26 @@ int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc,
     // Rounds of kRound ln k nodes: integrate, then advance each table's stopping scan.
     constexpr int kRound = 32;
     const int threads = 256;
-    for (int i0 = 0; i0 < stride; i0 += kRound) {
-        const long long nwarps = (long long)count * kRound;
-        const long long blocks = (nwarps * 32 + threads - 1) / threads;
-        if (with_dn)
+    if ((stride + kRound - 1) / kRound > kMaxRounds) return set_error(GSB_ERR_UNSUPPORTED, "Sersic table too long");
+    for (int i0 = 0, r = 0; i0 < stride; i0 += kRound, ++r) {
+        const int* prev_live = r > 0 ? d_status + r : nullptr;
+        if (with_dn) {
+            const long long nwarps = (long long)count * kRound;
+            const long long blocks = (nwarps * 32 + threads - 1) / threads;
             sersic_nodes_kernel<true><<<(unsigned)blocks, threads, 0, stream>>>(
                 t->d_header, count, stride, i0, kRound, *gsp, st->og,
                 static_cast<const SersicScan*>(t->d_scan), t->d_val, dheader, dval, d_status);
-        else
-            sersic_nodes_kernel<false><<<(unsigned)blocks, threads, 0, stream>>>(
-                t->d_header, count, stride, i0, kRound, *gsp, st->og,
-                static_cast<const SersicScan*>(t->d_scan), t->d_val, nullptr, nullptr, d_status);
+        } else {
+            const long long nwarps = (long long)count * ((kRound + 1) / 2);
+            const long long blocks = (nwarps * 32 + threads - 1) / threads;
+            sersic_nodes_pair_kernel<<<(unsigned)blocks, threads, 0, stream>>>(
+                t->d_header, count, i0, kRound, *gsp, st->og, static_cast<const SersicScan*>(t->d_scan),
+                t->d_val, stride, prev_live, d_status);
+        }
         GSB_CUDA_CHECK(cudaGetLastError());
         sersic_scan_kernel<<<(count + 63) / 64, 64, 0, stream>>>(t->d_header, count, stride, i0, kRound,
                                                                  *gsp, t->d_val, t->d_node, static_cast<SersicScan*>(t->d_scan),
-                                                                 dval, dnode);
+                                                                 dval, dnode, prev_live, d_status + 1 + r);
         GSB_CUDA_CHECK(cudaGetLastError());
     }
     const size_t fsm = sizeof(double) * 4 * (size_t)stride;
