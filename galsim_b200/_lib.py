@@ -111,6 +111,14 @@ def lib():
             'gsb_draw_tune_report': (i, [ctypes.c_char_p, sz]),
             'gsb_draw_kimages': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp,
                                      vp, vp, d, i, i, i, i, vp, i, vp]),
+            # the reference's hot-path steps one at a time (gsb_standalone.cu)
+            'gsb_draw_k': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp, vp, vp, d,
+                               vp, i, i, i, i, vp, i, vp]),
+            'gsb_apply_kimage_phases': (i, [vp, i, i, i, i, i, ctypes.c_longlong, d, vp, d, d, d, vp]),
+            'gsb_wrap_image': (i, [vp, i, i, i, i, i, i, ctypes.c_longlong, i, i, i, i, i, i, vp,
+                                   ctypes.c_longlong, vp]),
+            'gsb_irfft': (i, [vp, i, i, i, ctypes.c_longlong, vp, ctypes.c_longlong, i, i, vp, sz, vp]),
+            'gsb_irfft_workspace_size': (sz, [i, i]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

@@ -10,57 +10,50 @@
 // The slab W is the only HBM round trip; the chunk size keeps it inside the workspace.
 #include <algorithm>
 #include <map>
+#include <mutex>
 
 #include "gsb_draw.cuh"
 
 namespace gsb {
 
+static __global__ void twiddle_kernel(double2* tw, int N)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= N) return;
+    double s, c;
+    sincospi(2.0 * m / N, &s, &c);
+    tw[m] = make_double2(c, s);
+}
+
+static std::map<int, double2*>& twiddle_cache()
+{
+    static std::map<int, double2*> cache[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return cache[dev & 63];
+}
+
+// exp(+2 pi i m / N), m < N, in FP64: built once per (device, N) and kept for the process.
+int fft_twiddles(int N, cudaStream_t stream, const double2** out)
+{
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    auto& c = twiddle_cache();
+    auto it = c.find(N);
+    if (it != c.end()) { *out = it->second; return GSB_OK; }
+    double2* tw = nullptr;
+    GSB_CUDA_CHECK(cudaMalloc(&tw, sizeof(double2) * N));
+    twiddle_kernel<<<(N + 255) / 256, 256, 0, stream>>>(tw, N);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    GSB_CUDA_CHECK(cudaStreamSynchronize(stream));
+    c[N] = tw;
+    *out = tw;
+    return GSB_OK;
+}
+
 namespace {
 
 constexpr int kLargeThreads = 1024;
-constexpr int kMaxPerThread = 4;     // supports N / R <= 4096 butterflies per pass, N <= 16384
-
-// Block-wide in-place Stockham FFT of length N (2^a or 3 * 2^a) in shared memory.
-// tw: exp(+2 pi i m / N) for m < N (global, FP64).
-template <typename T, int SIGN>
-__device__ void block_fft(Cx<T>* buf, int N, const double2* __restrict__ tw)
-{
-    int NS = 1;
-    while (NS < N) {
-        const int rem = N / NS;
-        const int R = (NS == 1 && N % 3 == 0) ? 3 : ((rem % 4) == 0 ? 4 : 2);
-        const int NB = N / R;
-        const int tstep = N / (NS * R);
-        Cx<T> v[kMaxPerThread][4];
-#pragma unroll
-        for (int t = 0; t < kMaxPerThread; ++t) {
-            const int b = threadIdx.x + t * blockDim.x;
-            if (b < NB) {
-                const int k = b % NS;
-                for (int r = 0; r < R; ++r) v[t][r] = buf[b + r * NB];
-                for (int r = 1; r < R; ++r) {
-                    const double2 w = __ldg(&tw[(long long)(r * k) * tstep % N]);
-                    v[t][r] = cmul<T>(v[t][r], cx<T>(T(w.x), SIGN > 0 ? T(w.y) : T(-w.y)));
-                }
-                if (R == 4) dft_small<T, 4, SIGN>(v[t]);
-                else if (R == 3) dft_small<T, 3, SIGN>(v[t]);
-                else dft_small<T, 2, SIGN>(v[t]);
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int t = 0; t < kMaxPerThread; ++t) {
-            const int b = threadIdx.x + t * blockDim.x;
-            if (b < NB) {
-                const int k = b % NS;
-                const int base = (b / NS) * NS * R + k;
-                for (int r = 0; r < R; ++r) buf[base + r * NS] = v[t][r];
-            }
-        }
-        __syncthreads();
-        NS *= R;
-    }
-}
 
 struct LargeArgs {
     DrawArgs a;          // leaves/phases/scales/stamps already offset to the chunk
@@ -185,38 +178,6 @@ __global__ void __launch_bounds__(THREADS) large_row_kernel(const __grid_constan
     }
 }
 
-__global__ void twiddle_kernel(double2* tw, int N)
-{
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= N) return;
-    double s, c;
-    sincospi(2.0 * m / N, &s, &c);
-    tw[m] = make_double2(c, s);
-}
-
-std::map<int, double2*>& twiddle_cache()
-{
-    static std::map<int, double2*> cache[64];
-    int dev = 0;
-    cudaGetDevice(&dev);
-    return cache[dev & 63];
-}
-
-int twiddles(int N, cudaStream_t stream, const double2** out)
-{
-    auto& c = twiddle_cache();
-    auto it = c.find(N);
-    if (it != c.end()) { *out = it->second; return GSB_OK; }
-    double2* tw = nullptr;
-    GSB_CUDA_CHECK(cudaMalloc(&tw, sizeof(double2) * N));
-    twiddle_kernel<<<(N + 255) / 256, 256, 0, stream>>>(tw, N);
-    GSB_CUDA_CHECK(cudaGetLastError());
-    GSB_CUDA_CHECK(cudaStreamSynchronize(stream));
-    c[N] = tw;
-    *out = tw;
-    return GSB_OK;
-}
-
 template <typename T>
 size_t slab_bytes(int N) { return sizeof(Cx<T>) * (size_t)(N / 2 + 1) * N; }
 
@@ -235,7 +196,7 @@ int launch_large_t(const DrawArgs& args, int N, void* work, size_t work_bytes, c
     const int cache_bytes = int(std::min<size_t>(room, 192 * 1024) & ~size_t(15));
     const size_t sm = base + cache_bytes;
     const double2* tw = nullptr;
-    int rc = twiddles(N, stream, &tw);
+    int rc = fft_twiddles(N, stream, &tw);
     if (rc) return rc;
     // programs without image leaves run the column kernel compiled without their code
     const bool ii = has_image_leaves(args.tpl);

@@ -122,4 +122,49 @@ __device__ inline void fill_twiddles(Cx<T>* tw, int N)
     }
 }
 
+constexpr int kBlockFftMaxPerThread = 4;   // N / R <= 4096 butterflies per pass at 1024 threads
+
+// Block-wide in-place Stockham FFT of length N (2^a or 3 * 2^a, N / R <= blockDim.x *
+// kBlockFftMaxPerThread) in shared memory, the same radix plan as warp_fft; all threads of the
+// block must call.  tw: exp(+2 pi i m / N) for m < N (global, FP64).
+template <typename T, int SIGN>
+__device__ void block_fft(Cx<T>* buf, int N, const double2* __restrict__ tw)
+{
+    int NS = 1;
+    while (NS < N) {
+        const int rem = N / NS;
+        const int R = (NS == 1 && N % 3 == 0) ? 3 : ((rem % 4) == 0 ? 4 : 2);
+        const int NB = N / R;
+        const int tstep = N / (NS * R);
+        Cx<T> v[kBlockFftMaxPerThread][4];
+#pragma unroll
+        for (int t = 0; t < kBlockFftMaxPerThread; ++t) {
+            const int b = threadIdx.x + t * blockDim.x;
+            if (b < NB) {
+                const int k = b % NS;
+                for (int r = 0; r < R; ++r) v[t][r] = buf[b + r * NB];
+                for (int r = 1; r < R; ++r) {
+                    const double2 w = __ldg(&tw[(long long)(r * k) * tstep % N]);
+                    v[t][r] = cmul<T>(v[t][r], cx<T>(T(w.x), SIGN > 0 ? T(w.y) : T(-w.y)));
+                }
+                if (R == 4) dft_small<T, 4, SIGN>(v[t]);
+                else if (R == 3) dft_small<T, 3, SIGN>(v[t]);
+                else dft_small<T, 2, SIGN>(v[t]);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int t = 0; t < kBlockFftMaxPerThread; ++t) {
+            const int b = threadIdx.x + t * blockDim.x;
+            if (b < NB) {
+                const int k = b % NS;
+                const int base = (b / NS) * NS * R + k;
+                for (int r = 0; r < R; ++r) buf[base + r * NS] = v[t][r];
+            }
+        }
+        __syncthreads();
+        NS *= R;
+    }
+}
+
 }  // namespace gsb

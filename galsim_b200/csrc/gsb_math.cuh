@@ -73,8 +73,9 @@ __device__ const double kExp2Tab[32] = {
     1.718619298122478, 1.7562521603732995, 1.7947090750031072, 1.8340080864093424,
     1.8741676341103, 1.9152065613971474, 1.9571441241754002};
 
-// The exponential's body for -708 <= x <= 709 (no range test).
-__device__ __forceinline__ double exp_tab_core(double x)
+// The exponential's body for -708 <= x <= 709 (no range test); `tab` is kExp2Tab or a copy of
+// it (in shared memory, for kernels that evaluate many exponentials per thread).
+__device__ __forceinline__ double exp_tab_core(double x, const double* tab = kExp2Tab)
 {
     // n = rint(x 32/ln2) without a rounding or conversion instruction: adding 1.5 * 2^52 to the
     // (rounded) product leaves n, rounded to nearest-even as rint does, in the low mantissa bits
@@ -93,7 +94,7 @@ __device__ __forceinline__ double exp_tab_core(double x)
     p = fma(p, r, 0.5);
     p = fma(p, r, 1.);
     p = fma(p, r, 1.);
-    const double v = __ldg(&kExp2Tab[j]) * p;
+    const double v = tab[j] * p;
     return __hiloint2double(__double2hiint(v) + (m << 20), __double2loint(v));
 }
 
@@ -105,9 +106,9 @@ __device__ __forceinline__ double exp_tab(double x)
 
 // exp(x) for x <= 0 without a branch: arguments below -708 give exp(-708) ~ 3e-308 instead
 // of 0 (the quadrature's terms that reach them are far below its stopping threshold).
-__device__ __forceinline__ double exp_tab_neg(double x)
+__device__ __forceinline__ double exp_tab_neg(double x, const double* tab = kExp2Tab)
 {
-    return exp_tab_core(fmax(x, -708.));
+    return exp_tab_core(fmax(x, -708.), tab);
 }
 
 // ---------------------------------------------------------------------------------------

@@ -213,7 +213,7 @@ struct SersicRadialDn {
 template <bool TAB>
 __device__ __forceinline__ double2 warp_ogata_sum_pair(const OgataTables& og, double invn, double c1,
                                                        double logk0, double logk1, int lev, bool act0,
-                                                       bool act1)
+                                                       bool act1, const double* etab)
 {
     const int lane = threadIdx.x & 31;
     const double h = ldexp(1.0, -lev);
@@ -227,9 +227,9 @@ __device__ __forceinline__ double2 warp_ogata_sum_pair(const OgataTables& og, do
         double s0 = 0., s1 = 0.;
         if (valid) {
             const double2 n = TAB ? xw[i] : ogata_node(og.root, h, i);
-            const double u0 = exp_tab_core((n.x - logk0) * invn);
-            if (act0) s0 = n.y * exp_tab_neg(-u0);
-            if (act1) s1 = n.y * exp_tab_neg(-(u0 * c1));
+            const double u0 = exp_tab_core((n.x - logk0) * invn, etab);
+            if (act0) s0 = n.y * exp_tab_neg(-u0, etab);
+            if (act1) s1 = n.y * exp_tab_neg(-(u0 * c1), etab);
         }
         if (act0) {
             const unsigned m0 = __ballot_sync(0xffffffffu, valid && fabs(s0) < th0);
@@ -271,7 +271,8 @@ __device__ __forceinline__ double2 warp_ogata_sum_pair(const OgataTables& og, do
 // warp's shared-memory slot `a` (ans0, ans1 of node 0, then of node 1) rather than in
 // registers across the term loop.  has1 = false integrates node 0 alone.
 __device__ double2 warp_hankel_pair(const OgataTables& og, double invn, double logk0, double logk1,
-                                    bool has1, double relerr, double abserr, int* status, double* a)
+                                    bool has1, double relerr, double abserr, int* status, double* a,
+                                    const double* etab)
 {
     const int lane = threadIdx.x & 31;
     const double k0 = exp(logk0), k1 = exp(logk1);
@@ -289,8 +290,8 @@ __device__ double2 warp_hankel_pair(const OgataTables& og, double invn, double l
         if (L > 61) { if (status) *status = 1; break; }
         const bool g0 = run0 && L >= s0, g1 = run1 && L >= s1;
         const double2 r = (L >= og.lev_min && L <= og.lev_max)
-                              ? warp_ogata_sum_pair<true>(og, invn, c1, logk0, logk1, L, g0, g1)
-                              : warp_ogata_sum_pair<false>(og, invn, c1, logk0, logk1, L, g0, g1);
+                              ? warp_ogata_sum_pair<true>(og, invn, c1, logk0, logk1, L, g0, g1, etab)
+                              : warp_ogata_sum_pair<false>(og, invn, c1, logk0, logk1, L, g0, g1, etab);
         __syncwarp();
         if (lane == 0) {
             if (g0) { a[0] = a[1]; a[1] = r.x; }
@@ -485,6 +486,10 @@ __global__ void __launch_bounds__(256, 4) sersic_nodes_pair_kernel(const double*
                                     const int* prev_live, int* status_out)
 {
     if (prev_live && *prev_live == 0) return;
+    // the exponential's 2^(j/32) table, read three times per pair of terms, from shared memory
+    __shared__ double etab[32];
+    if (threadIdx.x < 32) etab[threadIdx.x] = kExp2Tab[threadIdx.x];
+    __syncthreads();
     const int npair = (nround + 1) / 2;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long s = count - 1 - warp / npair;
@@ -502,7 +507,7 @@ __global__ void __launch_bounds__(256, 4) sersic_nodes_pair_kernel(const double*
     __shared__ double ans[8][4];           // the running answers of each warp's pair
     int st = 0;
     const double2 v = warp_hankel_pair(og, 1. / n, logk0, logk1, has1, gsp.integration_relerr,
-                                       gsp.integration_abserr * hankel_norm, &st, ans[(threadIdx.x >> 5) & 7]);
+                                       gsp.integration_abserr * hankel_norm, &st, ans[(threadIdx.x >> 5) & 7], etab);
     if ((threadIdx.x & 31) == 0) {
         vals[s * stride + i] = v.x / hankel_norm;
         if (has1) vals[s * stride + i + 1] = v.y / hankel_norm;

@@ -346,6 +346,62 @@ int gsb_draw_kimages(const gsb_template* tpl, int n_stamps, const gsb_gsparams* 
                      const gsb_tables* t, double dk, int kxmin, int kymin, int nkx, int nky,
                      void* d_out, int out_dtype, void* stream);
 
+/* The reference's compiled hot-path steps one by one --------------------------------------
+ * For callers that keep the reference's Python orchestration (GSObject.drawFFT,
+ * galsim/gsobject.py:2014-2045, and the _drawKImage tree walk) and replace only what it calls
+ * in _galsim.  Each acts on one image in device memory; gsb_draw_images fuses all four. */
+
+/* SBProfile.drawK (pysrc/SBProfile.cpp:35-40, src/SBProfile.cpp:383-425): the profile's
+ * k-values on the grid kx = i dk, ky = j dk for the image bounds i = xmin .. xmin+nx-1,
+ * j = ymin .. ymin+ny-1, written as complex (re, im) rows of nx values, FP32 or FP64 per
+ * out_dtype; n_stamps images one after the other.  jac (a host array of 4 doubles, row-major
+ * [A, B, C, D], or NULL) is the drawK Jacobian: as in Transformation._drawKImage
+ * (transform.py:592) it multiplies every leaf's and phase's composed Jacobian from the left,
+ * and the 1-d / 2-d fill rules follow the product.  The records are the batch records of
+ * gsb_draw_kimages (prepared by gsb_prepare_leaves). */
+int gsb_draw_k(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp, const gsb_leaf* d_leaves,
+               const gsb_phase* d_phases, const double* d_scales, const gsb_tables* t, double dk,
+               const double* jac, int xmin, int ymin, int nx, int ny, void* d_out, int out_dtype,
+               void* stream);
+
+/* ApplyKImagePhases (pysrc/SBTransform.cpp:27-40, src/SBTransform.cpp:740-883): multiply the
+ * complex k-image (bounds xmin.., ymin.., nx x ny, row stride `stride` complex elements,
+ * complex64 for GSB_F32 or complex128 for GSB_F64) in place by
+ * flux_scaling * exp(-i (kx' cenx + ky' ceny)), kx = i dk, ky = j dk, (kx', ky') =
+ * (A kx + C ky, B kx + D ky) from jac (host, 4 doubles, or NULL for the identity).  The phase
+ * is formed in FP64 turns. */
+int gsb_apply_kimage_phases(void* d_image, int dtype, int xmin, int ymin, int nx, int ny, long long stride,
+                            double dk, const double* jac, double cenx, double ceny, double flux_scaling,
+                            void* stream);
+
+/* wrapImage (pysrc/Image.cpp:60-61, src/Image.cpp:578-727, Image.wrap in image.py:711-796):
+ * fold the image with bounds (xmin..xmax, ymin..ymax) (row stride in_stride elements) onto
+ * the bounds b = (bxmin..bxmax, bymin..bymax): every cell of b receives the sum of its aliases
+ * (periods of b's widths).  hermx: the image holds x >= 0 only and is Hermitian
+ * (X(-x, -y) = conj X(x, y)); the x period is 2 bxmax; the reference's conditions apply
+ * (xmin = bxmin = 0, symmetric y bounds, b missing its most negative row).  Real (is_complex
+ * = 0) or complex images, FP32 or FP64 per dtype.  Unlike the reference, which wraps in place
+ * and returns the subimage, the result is written to d_out (b's cells, row stride
+ * out_stride), which must not overlap d_in.  hermy returns GSB_ERR_UNSUPPORTED. */
+int gsb_wrap_image(const void* d_in, int dtype, int is_complex, int xmin, int xmax, int ymin, int ymax,
+                   long long in_stride, int bxmin, int bxmax, int bymin, int bymax, int hermx, int hermy,
+                   void* d_out, long long out_stride, void* stream);
+
+/* irfft (pysrc/Image.cpp:53-57, src/Image.cpp:815-912): inverse real FFT of the Hermitian
+ * half plane with bounds (0..Nx/2, -Ny/2..Ny/2-1) (complex64 or complex128 per in_dtype, row
+ * stride in_stride complex elements) into FP64 rows of the output bounds
+ * (-Nx/2..Nx/2+1, -Ny/2..Ny/2-1), row stride out_stride >= Nx + 2 doubles (the last two columns
+ * of each row are not written).  Scaled by 1/(Nx Ny); shift_in swaps the ky halves into FFT
+ * order, shift_out multiplies by (-1)^(i+j) so that x = y = 0 lands at the centre, as the
+ * reference's flags do.  As in a c2r transform, the imaginary parts left in the kx = 0 and
+ * kx = Nx/2 columns after the y transform are ignored.  Nx, Ny: 2^a or 3*2^a up to 12288
+ * (others return GSB_ERR_UNSUPPORTED).  d_work: gsb_irfft_workspace_size(Nx, Ny) bytes of
+ * device scratch. */
+int gsb_irfft(const void* d_in, int in_dtype, int Nx, int Ny, long long in_stride, double* d_out,
+              long long out_stride, int shift_in, int shift_out, void* d_work, size_t work_bytes,
+              void* stream);
+size_t gsb_irfft_workspace_size(int Nx, int Ny);
+
 /* gsb_draw_images without any device allocation.  This entry point has no counterpart in
  * the reference; it exists for callers that cannot allocate device memory while they draw
  * (an application that owns a fixed GPU memory budget, or a plugin inside another program's

@@ -511,6 +511,65 @@ def main_configs(ref_root):
           'C4 sizes', dict(zip(*np.unique(out['c4_N_Nk'][:, 0], return_counts=True))))
 
 
+# The reference's compiled hot-path steps one at a time (for the standalone C-ABI entry points):
+# SBProfile.drawK through _drawKImage(image, jac) (the Jacobian composition of
+# Transformation._drawKImage included), ApplyKImagePhases, Image.wrap on real and complex
+# non-Hermitian images, and irfft with each combination of its shift flags, Nx != Ny.
+STANDALONE_DRAWK = [
+    # (name, spec, dk, bounds (xmin, xmax, ymin, ymax), jac (row-major) or None, dtype)
+    ('exp_jac_general', ('exp', 0.8, 3.), 0.35, (0, 20, -20, 20), (1.1, 0.2, -0.1, 0.9), 'c16'),
+    ('conv_shift_jac_diag', ('conv', [('shift', 0.15, -0.1, ('shear', 0.1, 0.05, ('gauss', 0.5, 2.))),
+                                      ('moffat', 3.0, 0.7, 1.)]), 0.4, (-10, 10, -12, 12), (0.8, 0., 0., 1.3), 'c16'),
+    ('sum_sersic_exp_jac', ('sum', [('sersic', 2.2, 0.6, 5.), ('rotate', 20., ('exp', 0.9, 2.))]), 0.3,
+     (0, 16, -16, 16), (0.9, -0.15, 0.2, 1.05), 'c8'),
+    ('conv_nojac', ('conv', [('exp', 0.5, 1.), ('kolmogorov', 0.7, 1.), ('pixel', 0.2)]), 0.5,
+     (-8, 8, -8, 8), None, 'c16'),
+]
+STANDALONE_IRFFT = [(8, 12), (16, 8), (12, 12)]
+
+
+def main_standalone(ref_root):
+    from ref_import import import_reference_galsim
+    galsim = import_reference_galsim(ref_root)
+    out = {}
+    for name, spec, dk, b, jac, dt in STANDALONE_DRAWK:
+        im = galsim.Image(galsim.BoundsI(*b), dtype=np.complex128 if dt == 'c16' else np.complex64, scale=dk)
+        j = None if jac is None else np.array(jac, dtype=float).reshape(2, 2)
+        profile(galsim, spec)._drawKImage(im, j)
+        out['drawk_' + name] = im.array.copy()
+    rng = np.random.default_rng(31)
+    # ApplyKImagePhases on a random complex image, general Jacobian and none
+    for tag, jac in (('jac', (0.9, 0.3, -0.2, 1.1)), ('nojac', None)):
+        a = rng.normal(size=(21, 13)) + 1j * rng.normal(size=(21, 13))
+        im = galsim.ImageCD(a.copy(), xmin=0, ymin=-10, scale=0.3)
+        j = None if jac is None else np.array(jac, dtype=float).reshape(2, 2)
+        galsim._galsim.ApplyKImagePhases(im._image, im.scale, 0 if j is None else j.__array_interface__['data'][0],
+                                         0.37, -0.61, 1.7)
+        out['phase_in_' + tag] = a
+        out['phase_out_' + tag] = im.array.copy()
+    # wrap: non-Hermitian real and complex images
+    a = rng.normal(size=(18, 17))
+    im = galsim.ImageD(a.copy(), xmin=-7, ymin=-5)
+    out['wrapr_in'] = a
+    out['wrapr_out'] = im.wrap(galsim.BoundsI(-2, 3, -1, 4)).array.copy()
+    a = rng.normal(size=(15, 12)) + 1j * rng.normal(size=(15, 12))
+    im = galsim.ImageCD(a.copy(), xmin=-4, ymin=-6)
+    out['wrapc_in'] = a
+    out['wrapc_out'] = im.wrap(galsim.BoundsI(-1, 4, -3, 2)).array.copy()
+    # irfft with each flag combination
+    for Nx, Ny in STANDALONE_IRFFT:
+        k = rng.normal(size=(Ny, Nx // 2 + 1)) + 1j * rng.normal(size=(Ny, Nx // 2 + 1))
+        kim = galsim.ImageCD(k.copy(), xmin=0, ymin=-Ny // 2)
+        out['irfft_in_%d_%d' % (Nx, Ny)] = k
+        for si in (0, 1):
+            for so in (0, 1):
+                real = galsim.Image(galsim.BoundsI(-Nx // 2, Nx // 2 + 1, -Ny // 2, Ny // 2 - 1), dtype=float)
+                galsim._galsim.irfft(kim._image, real._image, bool(si), bool(so))
+                out['irfft_out_%d_%d_%d%d' % (Nx, Ny, si, so)] = real.array[:, :Nx].copy()
+    np.savez_compressed(os.path.join(HERE, 'reference_standalone.npz'), **out)
+    print('wrote', os.path.join(HERE, 'reference_standalone.npz'), len(out), 'arrays')
+
+
 def main(ref_root):
     from ref_import import import_reference_galsim
     galsim = import_reference_galsim(ref_root)
@@ -574,6 +633,8 @@ if __name__ == '__main__':
         main_fits(root)
     elif '--configs-only' in sys.argv:
         main_configs(root)
+    elif '--standalone-only' in sys.argv:
+        main_standalone(root)
     else:
         if '--large-only' not in sys.argv:
             main(root)
@@ -584,3 +645,4 @@ if __name__ == '__main__':
         main_noise(root)
         main_fits(root)
         main_configs(root)
+        main_standalone(root)

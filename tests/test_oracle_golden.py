@@ -108,3 +108,45 @@ def test_mixed_sample_stamp_minimum_fft_size_32():
     disk = O.OExponential(m['dh'][i] / 1.6783469900166605, m['flux'][i] * (1. - m['bf'][i])).shear(*m['g_d'][i])
     o = O.OConvolve(O.OSum(bulge, disk), O.OMoffat(m['beta'][i], fwhm=m['fwhm'][i]), O.OBox(0.2))
     _check_oracle_stamp('c4', j, o, O.OGSParams(minimum_fft_size=32))
+
+
+STD = np.load(specs.HERE + '/reference_standalone.npz')
+
+
+@pytest.mark.parametrize('case', MG.STANDALONE_DRAWK, ids=[c[0] for c in MG.STANDALONE_DRAWK])
+def test_drawk_with_jacobian_matches_reference(case):
+    """SBProfile.drawK through the tree's _drawKImage(image, jac): the oracle's drawK with the
+    same Jacobian composed as Transformation._drawKImage does."""
+    name, spec, dk, b, jac, dt = case
+    kim = np.zeros((b[3] - b[2] + 1, b[1] - b[0] + 1), complex)
+    j = None if jac is None else np.array(jac, dtype=float).reshape(2, 2)
+    specs.oracle_profile(spec).drawK(kim, b[0], b[2], dk, j)
+    ref = STD['drawk_' + name]
+    tol = 1e-12 if dt == 'c16' else 2e-7
+    assert np.abs(kim - ref).max() <= tol * np.abs(ref).max()
+
+
+@pytest.mark.parametrize('tag', ['jac', 'nojac'])
+def test_apply_phases_matches_reference(tag):
+    a = STD['phase_in_' + tag].copy()
+    jac = None if tag == 'nojac' else np.array((0.9, 0.3, -0.2, 1.1)).reshape(2, 2)
+    O.apply_phases(a, 0, -10, 0.3, jac, 0.37, -0.61, 1.7)
+    assert np.abs(a - STD['phase_out_' + tag]).max() <= 1e-12 * np.abs(a).max()
+
+
+@pytest.mark.parametrize('Nx,Ny', MG.STANDALONE_IRFFT)
+@pytest.mark.parametrize('si', [0, 1])
+@pytest.mark.parametrize('so', [0, 1])
+def test_irfft_flags_match_reference(Nx, Ny, si, so):
+    """irfft's shift_in / shift_out (Image.cpp:848-898) restated with numpy: the rows taken in
+    FFT order, the (-1)^(i+j) factor, then a c2r transform (which ignores the imaginary parts of
+    the kx = 0 and Nx/2 columns after the y transform)."""
+    k = STD['irfft_in_%d_%d' % (Nx, Ny)]
+    K = np.concatenate([k[Ny // 2:], k[:Ny // 2]], axis=0) if si else k.copy()
+    if so:
+        r = np.arange(Ny)[:, None]
+        c = np.arange(Nx // 2 + 1)[None, :]
+        K = K * np.where((r + c) % 2 == 0, 1., -1.)
+    out = np.fft.irfft2(K, s=(Ny, Nx))
+    ref = STD['irfft_out_%d_%d_%d%d' % (Nx, Ny, si, so)]
+    assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max()
