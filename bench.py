@@ -500,9 +500,16 @@ def gpu_object(galsim, p):
     return galsim.Convolve(gal, galsim.Kolmogorov(fwhm=p[:, 5]), galsim.Pixel(SCALE))
 
 
-# Measured DRAM bytes per stamp of the fused draw kernel by FFT size (ncu, 600-stamp case of
-# this workload; profiles/draw_fused_kernel_dram_per_stamp.md).  Larger N scale as N^2.
-DRAM_BYTES_PER_STAMP = {128: 8732., 192: 110406., 256: 18898.}
+# DRAM bytes of one step's draw kernels (ncu, one-pass metrics, this workload at its own
+# automatic sizes; profiles/draw_fused_kernel_dram_bench_step_4096.md): reads, writes, and the
+# global stores the SMs issue (stamps plus the N >= 256 buckets' W slabs, which stay in L2).
+DRAW_STEP_DRAM_READ = 37439488
+DRAW_STEP_DRAM_WRITE = 63917824
+DRAW_STEP_STORES = 285221408
+# FP64 pipe and issue utilisation of the Sersic table kernel (ncu --set full, round 5 of a
+# 4096-table build; profiles/sersic_nodes_pair_kernel_4096_tables.md)
+TABLES_FP64_PIPE = 0.446
+TABLES_ISSUE_ACTIVE = 0.747
 
 
 def table_build_launches(n_values, gsp_kvalue_accuracy=1e-5, table_spacing=1.):
@@ -515,15 +522,6 @@ def table_build_launches(n_values, gsp_kvalue_accuracy=1e-5, table_spacing=1.):
     dlogk = table_spacing * math.sqrt(math.sqrt(gsp_kvalue_accuracy / 10.))
     stride = int((math.log(500.) - (math.log(kmin) - 0.001)) / dlogk) + 4
     return 3 + 2 * ((stride + 31) // 32)
-
-
-def measured_traffic(N):
-    N = np.asarray(N)
-    tot = 0.
-    for n in N:
-        n = int(n)
-        tot += DRAM_BYTES_PER_STAMP.get(n, DRAM_BYTES_PER_STAMP[256] * (n / 256.) ** 2)
-    return tot
 
 
 def algorithmic_bytes(N, nx, ny):
@@ -957,6 +955,27 @@ def run_gpu(args):
     peak, peak_kind = measured_peak_hbm()
     achieved = alg / (k_ms * 1e-3) / 1e9
 
+    # the Sersic table stage alone (one FP64 table per stamp), CUDA events on its stream
+    tables_roof = None
+    if prog.tables is not None and prog.sersic_n is not None:
+        for _ in range(2):
+            prog.tables.build_sersic(prog.sersic_n, prog.gsparams)
+        torch.cuda.synchronize(dev)
+        ts, te = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ts.record()
+        for _ in range(reps):
+            prog.tables.build_sersic(prog.sersic_n, prog.gsparams)
+        te.record()
+        torch.cuda.synchronize(dev)
+        t_ms = ts.elapsed_time(te) / reps
+        tables_roof = {'bound': 'fp64 issue', 'unit': 'fraction of the FP64 pipe',
+                       'kernel': 'sersic_nodes_pair_kernel (+ scan, setup, finalize): %d FP64 Sersic FT tables'
+                                 % len(prog.sersic_n),
+                       'kernel_ms': t_ms, 'step_share': t_ms / ms,
+                       'frac': TABLES_FP64_PIPE, 'issue_active': TABLES_ISSUE_ACTIVE,
+                       'frac_source': 'ncu --set full, round 5 of a 4096-table build '
+                                      '(profiles/sersic_nodes_pair_kernel_4096_tables.md)'}
+
     # e2e through the public API: host parameters -> draw_batch -> host pixels.  The warm-up
     # steps make the one-time allocations (the page-locked read-back buffer) before timing.
     def e2e_step():
@@ -1068,12 +1087,18 @@ def run_gpu(args):
                             'back on a copy stream while step k+1 runs (StampBatch.host_async)',
                     'serial_value': world * B / (e2e_serial_ms * 1e-3)},
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
-                         'frac': achieved / peak, 'traffic': measured_traffic(N),
-                         'traffic_note': 'ncu DRAM read+write bytes per stamp by N (600-stamp capture) '
-                                         'scaled to this step; algorithmic bytes %.0f' % alg,
+                         'frac': achieved / peak, 'traffic': DRAW_STEP_DRAM_READ + DRAW_STEP_DRAM_WRITE,
+                         'traffic_with_stamp_writeback': DRAW_STEP_DRAM_READ + int(pix.size * 4),
+                         'traffic_note': 'ncu dram read+write of the step\'s draw kernels at this workload '
+                                         '(profiles/draw_fused_kernel_dram_bench_step_4096.md); most stamp '
+                                         'writes are still in L2 when each kernel exits, so their write-back '
+                                         'is counted in traffic_with_stamp_writeback; the SMs store %d B '
+                                         '(stamps + W slabs); algorithmic bytes of the staged path %.0f'
+                                         % (DRAW_STEP_STORES, alg),
                          'peak_kind': peak_kind,
                          'kernel': 'draw_fused_kernel, all FFT-size buckets concurrent (one draw-graph replay)',
                          'kernel_ms': k_ms},
+            'roofline_tables': tables_roof,
             # per step: the Sersic table build, one leaf-prepare launch and one fused draw per
             # FFT-size bucket
             'gpu_launches': int(args.steps * (table_build_launches(params[:, 0]) + 1 + nb)),
