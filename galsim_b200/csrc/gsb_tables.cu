@@ -119,84 +119,11 @@ __device__ double warp_hankel(const OgataTables& og, const F& f, double k, doubl
     return ans1;
 }
 
-// The same quadrature for a pair of integrands (f, df/dn) evaluated together: the stopping
-// rules and the level halving follow the first component only, so the first component is
-// bit-identical to warp_ogata_sum / warp_hankel and the second is integrated on the same nodes.
-// (Same lane-local accumulation and lagged stopping test as warp_ogata_sum.)
-template <class F>
-__device__ double2 warp_ogata_sum2(const OgataTables& og, const F& f, double k, int lev)
-{
-    const int lane = threadIdx.x & 31;
-    const double h = ldexp(1.0, -lev);
-    const long long nmax = (long long)fmin(kPi / h, 1e6);
-    const bool tab = lev >= og.lev_min && lev <= og.lev_max;
-    const double2* xw = tab ? og.xw + og.off[lev - og.lev_min] : nullptr;
-    const double logk = log(k);
-    double acc = 0., dacc = 0., thresh = 0.;
-    int chunk = 0;
-    for (long long base = 0; base < nmax; base += 32, ++chunk) {
-        const long long i = base + lane;
-        const bool valid = i < nmax;
-        double step = 0., dstep = 0.;
-        if (valid) {
-            const double2 n = tab ? xw[i] : ogata_node(og.root, h, i);
-            const double2 v = f(n.x - logk);
-            step = n.y * v.x;
-            dstep = n.y * v.y;
-        }
-        const unsigned mask = __ballot_sync(0xffffffffu, valid && fabs(step) < thresh);
-        if (mask) {
-            const int last = __ffs(mask) - 1;
-            const bool in = lane <= last;
-            return make_double2(warp_total(acc + (in ? step : 0.)) / (k * k),
-                                warp_total(dacc + (in ? dstep : 0.)) / (k * k));
-        }
-        acc += step;
-        dacc += dstep;
-        if (chunk < kEagerChunks || (chunk % kLazyChunks) == kLazyChunks - 1)
-            thresh = 1e-15 * fabs(warp_total(acc));
-    }
-    return make_double2(warp_total(acc) / (k * k), warp_total(dacc) / (k * k));
-}
-
-template <class F>
-__device__ double2 warp_hankel2(const OgataTables& og, const F& f, double k, double relerr,
-                                double abserr, int* status)
-{
-    int lev = 5;
-    double h0 = 1. / 32.;
-    while (h0 > 100. * k && lev < 60) { h0 *= 0.5; ++lev; }
-    double2 ans0 = warp_ogata_sum2(og, f, k, lev);
-    double2 ans1 = warp_ogata_sum2(og, f, k, lev + 1);
-    double err = fabs(ans1.x - ans0.x);
-    while ((err > relerr * ans1.x && (err > abserr || fabs(ans1.x) > 2. * fabs(ans0.x))) || ans1.x == 0.) {
-        ++lev;
-        if (lev > 60) { if (status) *status = 1; break; }
-        ans0 = ans1;
-        ans1 = warp_ogata_sum2(og, f, k, lev + 1);
-        err = fabs(ans1.x - ans0.x);
-    }
-    return ans1;
-}
-
-// Integrands as functions of log r: exp(-r^(1/n)) and exp(-k^(5/3)).
-struct SersicRadial {
-    double invn;
-    __device__ double operator()(double logr) const { return exp_tab(-exp_tab(logr * invn)); }
-};
-
-// (f, g) with f = exp(-r^(1/n)) and g = df/dn + c r df/dr:  the quadrature sum
-// T(k) = sum_j w_j f(x_j / k) has dT/dn along k = k(n) with d ln k / dn = c equal to
-// sum_j w_j [df/dn - c r df/dr](x_j / k); df/dn = f u ln r / n^2, r df/dr = -f u / n, u = r^(1/n).
-struct SersicRadialDn {
-    double invn, c;
-    __device__ double2 operator()(double logr) const
-    {
-        const double u = exp_tab(logr * invn);
-        const double f = exp_tab(-u);
-        return make_double2(f, f * u * invn * (logr * invn + c));
-    }
-};
+// The Sersic integrand exp(-r^(1/n)) is evaluated inline by the node-pair quadrature below, with
+// log r = log x_i - log k; its n-derivative along the table's moving grid (GSB_TABLES_DN): the
+// quadrature sum T(k) = sum_j w_j f(x_j / k) has dT/dn along k = k(n) with d ln k / dn = c equal
+// to sum_j w_j [df/dn - c r df/dr](x_j / k); df/dn = f u ln r / n^2, r df/dr = -f u / n,
+// u = r^(1/n).
 
 // Two adjacent ln k nodes of one Sersic table in one warp (k0 < k1 = k0 e^dlogk): the terms
 // of both sums at one level share the node load (log x_i, w_i) and the inner exponential,
@@ -210,43 +137,63 @@ struct SersicRadialDn {
 // / n < 100 for the tabulated nodes and the tables' k range), so it takes no range test.
 // (Groups of four nodes per warp share more, but their state no longer fits the 64 registers
 // that four 256-thread blocks per SM allow, and they measured slower.)
-template <bool TAB>
+// DN: also the d/dn integrand on the same nodes, f u / n (log r / n + c) with c = dfront/dn (its
+// sums stop where the value sums stop, the halving follows the values), returned through dout.
+template <bool TAB, bool DN = false>
 __device__ __forceinline__ double2 warp_ogata_sum_pair(const OgataTables& og, double invn, double c1,
                                                        double logk0, double logk1, int lev, bool act0,
-                                                       bool act1, const double* etab)
+                                                       bool act1, const double* etab, double dnc = 0.,
+                                                       double2* dout = nullptr)
 {
     const int lane = threadIdx.x & 31;
     const double h = ldexp(1.0, -lev);
     const int nmax = (int)fmin(kPi / h, 1e6);
     const double2* xw = TAB ? og.xw + og.off[lev - og.lev_min] : nullptr;
     double acc0 = 0., acc1 = 0., th0 = 0., th1 = 0.;
+    double dacc0 = 0., dacc1 = 0.;
     int chunk = 0;
     for (int base = 0; base < nmax; base += 32, ++chunk) {
         const int i = base + lane;
         const bool valid = i < nmax;
-        double s0 = 0., s1 = 0.;
+        double s0 = 0., s1 = 0., ds0 = 0., ds1 = 0.;
         if (valid) {
             const double2 n = TAB ? xw[i] : ogata_node(og.root, h, i);
-            const double u0 = exp_tab_core((n.x - logk0) * invn, etab);
-            if (act0) s0 = n.y * exp_tab_neg(-u0, etab);
-            if (act1) s1 = n.y * exp_tab_neg(-(u0 * c1), etab);
+            const double lr0 = n.x - logk0;
+            const double u0 = exp_tab_core(lr0 * invn, etab);
+            if (act0) {
+                const double f = exp_tab_neg(-u0, etab);
+                s0 = n.y * f;
+                if (DN) ds0 = s0 * u0 * invn * (lr0 * invn + dnc);
+            }
+            if (act1) {
+                const double u1 = u0 * c1;
+                const double f = exp_tab_neg(-u1, etab);
+                s1 = n.y * f;
+                if (DN) ds1 = s1 * u1 * invn * ((n.x - logk1) * invn + dnc);
+            }
         }
         if (act0) {
             const unsigned m0 = __ballot_sync(0xffffffffu, valid && fabs(s0) < th0);
             if (m0) {
-                acc0 = warp_total(acc0 + (lane <= __ffs(m0) - 1 ? s0 : 0.));
+                const bool in = lane <= __ffs(m0) - 1;
+                acc0 = warp_total(acc0 + (in ? s0 : 0.));
+                if (DN) dacc0 = warp_total(dacc0 + (in ? ds0 : 0.));
                 act0 = false;
             } else {
                 acc0 += s0;
+                if (DN) dacc0 += ds0;
             }
         }
         if (act1) {
             const unsigned m1 = __ballot_sync(0xffffffffu, valid && fabs(s1) < th1);
             if (m1) {
-                acc1 = warp_total(acc1 + (lane <= __ffs(m1) - 1 ? s1 : 0.));
+                const bool in = lane <= __ffs(m1) - 1;
+                acc1 = warp_total(acc1 + (in ? s1 : 0.));
+                if (DN) dacc1 = warp_total(dacc1 + (in ? ds1 : 0.));
                 act1 = false;
             } else {
                 acc1 += s1;
+                if (DN) dacc1 += ds1;
             }
         }
         if (!(act0 || act1)) break;
@@ -256,9 +203,10 @@ __device__ __forceinline__ double2 warp_ogata_sum_pair(const OgataTables& og, do
         }
     }
     // sums that ran to nmax without stopping
-    if (act0) acc0 = warp_total(acc0);
-    if (act1) acc1 = warp_total(acc1);
+    if (act0) { acc0 = warp_total(acc0); if (DN) dacc0 = warp_total(dacc0); }
+    if (act1) { acc1 = warp_total(acc1); if (DN) dacc1 = warp_total(dacc1); }
     const double k0 = exp(logk0), k1 = exp(logk1);
+    if (DN) *dout = make_double2(dacc0 / (k0 * k0), dacc1 / (k1 * k1));
     return make_double2(acc0 / (k0 * k0), acc1 / (k1 * k1));
 }
 
@@ -270,9 +218,10 @@ __device__ __forceinline__ double2 warp_ogata_sum_pair(const OgataTables& og, do
 // not started, does not contribute to the level's sums.  The running answers live in this
 // warp's shared-memory slot `a` (ans0, ans1 of node 0, then of node 1) rather than in
 // registers across the term loop.  has1 = false integrates node 0 alone.
+template <bool DN = false>
 __device__ double2 warp_hankel_pair(const OgataTables& og, double invn, double logk0, double logk1,
                                     bool has1, double relerr, double abserr, int* status, double* a,
-                                    const double* etab)
+                                    const double* etab, double dnc = 0.)
 {
     const int lane = threadIdx.x & 31;
     const double k0 = exp(logk0), k1 = exp(logk1);
@@ -289,13 +238,14 @@ __device__ double2 warp_hankel_pair(const OgataTables& og, double invn, double l
         // the reference halves until its level counter passes 60: the last sum is at 61
         if (L > 61) { if (status) *status = 1; break; }
         const bool g0 = run0 && L >= s0, g1 = run1 && L >= s1;
+        double2 d = make_double2(0., 0.);
         const double2 r = (L >= og.lev_min && L <= og.lev_max)
-                              ? warp_ogata_sum_pair<true>(og, invn, c1, logk0, logk1, L, g0, g1, etab)
-                              : warp_ogata_sum_pair<false>(og, invn, c1, logk0, logk1, L, g0, g1, etab);
+                              ? warp_ogata_sum_pair<true, DN>(og, invn, c1, logk0, logk1, L, g0, g1, etab, dnc, &d)
+                              : warp_ogata_sum_pair<false, DN>(og, invn, c1, logk0, logk1, L, g0, g1, etab, dnc, &d);
         __syncwarp();
         if (lane == 0) {
-            if (g0) { a[0] = a[1]; a[1] = r.x; }
-            if (g1) { a[2] = a[3]; a[3] = r.y; }
+            if (g0) { a[0] = a[1]; a[1] = r.x; if (DN) a[5] = d.x; }
+            if (g1) { a[2] = a[3]; a[3] = r.y; if (DN) a[7] = d.y; }
         }
         __syncwarp();
         if (g0 && L > s0) run0 = more(a[0], a[1]);
@@ -434,56 +384,16 @@ __global__ void sersic_scan_init_kernel(const double* header, int count, SersicS
     S.done = int(header[(size_t)s * kSersicHeader + kSH_NCAND]) < 2 ? 1 : 0;
 }
 
-// One warp per (slot, node) of this round: val = Hankel transform at k_i / hankel_norm.
+// One warp per pair of adjacent nodes (i, i + 1) of this round: Hankel transform / hankel_norm at
+// k_i, k_{i+1} through warp_hankel_pair; DN: with the d/dn values of the same nodes.
+// prev_live (the previous round's scan flag) is zero once every table has stopped: the launch
+// then returns at once.
 template <bool DN>
-__global__ void __launch_bounds__(256, 4) sersic_nodes_kernel(const double* header, int count, int stride, int i0, int nround,
-                                    gsb_gsparams gsp, const __grid_constant__ OgataTables og, const SersicScan* scan,
-                                    double* vals, const double* dheader, double* dvals, int* status_out)
-{
-    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-    // slots hold ascending n; the costly large-n tables are taken first so that they do not
-    // form the tail of the launch
-    const long long s = count - 1 - warp / nround;
-    const int i = i0 + int(warp % nround);
-    if (s < 0) return;
-    if (scan[s].done) return;
-    const double* H = header + s * kSersicHeader;
-    if (i >= int(H[kSH_NCAND])) return;
-    const double n = H[kSH_N];
-    const double logk = H[kSH_FRONT] + i * H[kSH_DLOGK];
-    const double k = exp(logk);
-    const double hankel_norm = n * tgamma(2. * n);
-    int st = 0;
-    if (DN) {
-        // node value y = v k^2 = T(k) / norm with norm = n Gamma(2n) and k = k_i(n):
-        // dy/dn = (dT/dn) / norm - y (1/n + 2 psi(2n)), dT/dn from the second integrand.
-        SersicRadialDn f{1. / n, dheader[s * kSersicDHeader + kSD_DFRONT]};
-        const double2 hv = warp_hankel2(og, f, k, gsp.integration_relerr,
-                                        gsp.integration_abserr * hankel_norm, &st);
-        const double v = hv.x / hankel_norm;
-        if ((threadIdx.x & 31) == 0) {
-            vals[s * stride + i] = v;
-            dvals[s * stride + i] = (hv.y / hankel_norm - v * (1. / n + 2. * digamma(2. * n))) * k * k;
-            if (st) atomicOr(status_out, 1);
-        }
-        return;
-    }
-    SersicRadial f{1. / n};
-    const double v = warp_hankel(og, f, k, gsp.integration_relerr,
-                                 gsp.integration_abserr * hankel_norm, &st) / hankel_norm;
-    if ((threadIdx.x & 31) == 0) {
-        vals[s * stride + i] = v;
-        if (st) atomicOr(status_out, 1);
-    }
-}
-
-// One warp per pair of adjacent nodes (i, i + 1) of this round: the values of
-// sersic_nodes_kernel<false>, through warp_hankel_pair.  prev_live (the previous round's scan
-// flag) is zero once every table has stopped: the launch then returns at once.
 __global__ void __launch_bounds__(256, 4) sersic_nodes_pair_kernel(const double* header, int count, int i0,
                                     int nround, gsb_gsparams gsp, const __grid_constant__ OgataTables og,
                                     const SersicScan* scan, double* vals, int stride,
-                                    const int* prev_live, int* status_out)
+                                    const int* prev_live, int* status_out, const double* dheader,
+                                    double* dvals)
 {
     if (prev_live && *prev_live == 0) return;
     // the exponential's 2^(j/32) table, read three times per pair of terms, from shared memory
@@ -492,6 +402,8 @@ __global__ void __launch_bounds__(256, 4) sersic_nodes_pair_kernel(const double*
     __syncthreads();
     const int npair = (nround + 1) / 2;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    // slots hold ascending n; the costly large-n tables are taken first so that they do not
+    // form the tail of the launch
     const long long s = count - 1 - warp / npair;
     const int i = i0 + 2 * int(warp % npair);
     if (s < 0) return;
@@ -504,13 +416,24 @@ __global__ void __launch_bounds__(256, 4) sersic_nodes_pair_kernel(const double*
     const double logk0 = H[kSH_FRONT] + i * H[kSH_DLOGK];
     const double logk1 = H[kSH_FRONT] + (i + 1) * H[kSH_DLOGK];
     const double hankel_norm = n * tgamma(2. * n);
-    __shared__ double ans[8][4];           // the running answers of each warp's pair
+    __shared__ double ans[8][DN ? 8 : 4];  // the running answers of each warp's pair
+    double* a = ans[(threadIdx.x >> 5) & 7];
     int st = 0;
-    const double2 v = warp_hankel_pair(og, 1. / n, logk0, logk1, has1, gsp.integration_relerr,
-                                       gsp.integration_abserr * hankel_norm, &st, ans[(threadIdx.x >> 5) & 7], etab);
+    const double dnc = DN ? dheader[s * kSersicDHeader + kSD_DFRONT] : 0.;
+    const double2 v = warp_hankel_pair<DN>(og, 1. / n, logk0, logk1, has1, gsp.integration_relerr,
+                                           gsp.integration_abserr * hankel_norm, &st, a, etab, dnc);
     if ((threadIdx.x & 31) == 0) {
-        vals[s * stride + i] = v.x / hankel_norm;
-        if (has1) vals[s * stride + i + 1] = v.y / hankel_norm;
+        const double v0 = v.x / hankel_norm, v1 = v.y / hankel_norm;
+        vals[s * stride + i] = v0;
+        if (has1) vals[s * stride + i + 1] = v1;
+        if (DN) {
+            // node value y = v k^2 = T(k) / norm with norm = n Gamma(2n) and k = k_i(n):
+            // dy/dn = (dT/dn) / norm - y (1/n + 2 psi(2n)), dT/dn from the second integrand.
+            const double q = 1. / n + 2. * digamma(2. * n);
+            const double k0 = exp(logk0), k1 = exp(logk1);
+            dvals[s * stride + i] = (a[5] / hankel_norm - v0 * q) * k0 * k0;
+            if (has1) dvals[s * stride + i + 1] = (a[7] / hankel_norm - v1 * q) * k1 * k1;
+        }
         if (st) atomicOr(status_out, 1);
     }
 }
@@ -1031,19 +954,16 @@ int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc,
     if ((stride + kRound - 1) / kRound > kMaxRounds) return set_error(GSB_ERR_UNSUPPORTED, "Sersic table too long");
     for (int i0 = 0, r = 0; i0 < stride; i0 += kRound, ++r) {
         const int* prev_live = r > 0 ? d_status + r : nullptr;
-        if (with_dn) {
-            const long long nwarps = (long long)count * kRound;
-            const long long blocks = (nwarps * 32 + threads - 1) / threads;
-            sersic_nodes_kernel<true><<<(unsigned)blocks, threads, 0, stream>>>(
-                t->d_header, count, stride, i0, kRound, *gsp, st->og,
-                static_cast<const SersicScan*>(t->d_scan), t->d_val, dheader, dval, d_status);
-        } else {
-            const long long nwarps = (long long)count * ((kRound + 1) / 2);
-            const long long blocks = (nwarps * 32 + threads - 1) / threads;
-            sersic_nodes_pair_kernel<<<(unsigned)blocks, threads, 0, stream>>>(
+        const long long nwarps = (long long)count * ((kRound + 1) / 2);
+        const long long blocks = (nwarps * 32 + threads - 1) / threads;
+        if (with_dn)
+            sersic_nodes_pair_kernel<true><<<(unsigned)blocks, threads, 0, stream>>>(
                 t->d_header, count, i0, kRound, *gsp, st->og, static_cast<const SersicScan*>(t->d_scan),
-                t->d_val, stride, prev_live, d_status);
-        }
+                t->d_val, stride, prev_live, d_status, dheader, dval);
+        else
+            sersic_nodes_pair_kernel<false><<<(unsigned)blocks, threads, 0, stream>>>(
+                t->d_header, count, i0, kRound, *gsp, st->og, static_cast<const SersicScan*>(t->d_scan),
+                t->d_val, stride, prev_live, d_status, nullptr, nullptr);
         GSB_CUDA_CHECK(cudaGetLastError());
         sersic_scan_kernel<<<(count + 63) / 64, 64, 0, stream>>>(t->d_header, count, stride, i0, kRound,
                                                                  *gsp, t->d_val, t->d_node, static_cast<SersicScan*>(t->d_scan),
