@@ -148,6 +148,7 @@ class RecordPlan(object):
         from .batch import run_batch
         sb = run_batch(self.batch_plan)
         self.last = sb
+        self.draw_count = getattr(self, 'draw_count', 0) + 1
         t = self.prog.tables
         self._tables_gen = (t, t.generation) if t is not None else None
         return sb.stack()
@@ -201,11 +202,19 @@ def _function():
             img = plan.draw()
             ctx.plan = plan
             ctx.dtypes = [t.dtype for t in tensors]
+            ctx.records = [t.detach() for t in tensors]
+            ctx.draw_id = plan.draw_count
             return img.clone()
 
         @staticmethod
         def backward(ctx, gout):
-            g = ctx.plan.adjoint(gout)
+            plan = ctx.plan
+            if plan.draw_count != ctx.draw_id:
+                # the plan drew other records since this forward (a reused plan): draw this
+                # forward's records again so that the adjoint sees its stamps and geometry
+                plan.set_records(dict(zip(RECORD_FIELDS, ctx.records)))
+                plan.draw()
+            g = plan.adjoint(gout)
             return (None,) + tuple(g[k].to(dt) for k, dt in zip(RECORD_FIELDS, ctx.dtypes))
 
     return RecordDraw
@@ -267,32 +276,40 @@ class GalaxyModel(object):
 
     def __call__(self, params):
         import torch
-        p = params.detach().to('cpu', torch.float64).numpy()
-        if self.tables is None:
-            self.tables = _lib.Tables()
-        plan = RecordPlan(self.build(p), self.nx, self.ny, self.scale, self.dtype, self.precision,
-                          tables=self.tables)
-        if plan.types[0] != _lib.SERSIC or plan.P < 1:
-            raise GalSimError("unexpected program layout for GalaxyModel")
-        plan.want = 1 | (1 << 8)          # the galaxy leaf and its shift
-        self.plan = plan
-        rec = plan.records()
-        B = plan.B
+        B = int(params.shape[0])
+        if self.plan is None or self.plan.B != B:
+            # The program's layout (galaxy leaf, its shift, the PSF's leaves) depends only on the
+            # batch size: built once, then every call overwrites the galaxy's records.
+            p = params.detach().to('cpu', torch.float64).numpy()
+            if self.tables is None:
+                self.tables = _lib.Tables()
+            plan = RecordPlan(self.build(p), self.nx, self.ny, self.scale, self.dtype, self.precision,
+                              tables=self.tables)
+            if plan.types[0] != _lib.SERSIC or plan.P < 1:
+                raise GalSimError("unexpected program layout for GalaxyModel")
+            plan.want = 1 | (1 << 8)          # the galaxy leaf and its shift
+            rec = plan.records()
+            g1, g2 = torch.as_tensor(p[:, 3], device=rec['leaf_jac'].device), \
+                torch.as_tensor(p[:, 4], device=rec['leaf_jac'].device)
+            S = shear_matrix(g1, g2)
+            # the galaxy leaf's Jacobian without its shear: the world-to-image transform
+            self._jpre = rec['leaf_jac'][:, 0].reshape(B, 2, 2) @ torch.linalg.inv(S)
+            self._rec0 = rec
+            self.plan = plan
+        plan, rec = self.plan, self._rec0
         pr = params.to(torch.float64)
         flux, hlr, n, g1, g2, dx, dy = pr.unbind(-1)
         S = shear_matrix(g1, g2)
-        J = rec['leaf_jac'][:, 0].reshape(B, 2, 2)
-        Jpre = J @ torch.linalg.inv(S.detach())
         leaf_flux = rec['leaf_flux'].clone()
         leaf_flux[:, 0] = flux
         leaf_jac = rec['leaf_jac'].clone()
-        leaf_jac[:, 0] = (Jpre @ S).reshape(B, 4)
+        leaf_jac[:, 0] = (self._jpre @ S).reshape(B, 4)
         leaf_size = rec['leaf_size'].clone()
         leaf_size[:, 0, 0] = hlr
         leaf_n = rec['leaf_n'].clone()
         leaf_n[:, 0] = n
         phase_cen = rec['phase_cen'].clone()
-        phase_cen[:, 0] = torch.stack([dx, dy], -1)
+        phase_cen[:, 0] = torch.stack([dx, dy], -1)     # the program keeps its shift op (see build)
         phase_fs = rec['phase_fs'].clone()
         phase_fs[:, 0] = torch.abs(torch.linalg.det(S))
         return draw_records(plan, leaf_flux, leaf_jac, leaf_size, leaf_n, phase_cen, phase_fs,
