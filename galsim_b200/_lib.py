@@ -64,9 +64,9 @@ IMAGE_DESC_DTYPE = np.dtype({'names': ['N', 'nx', 'ny', 'x0', 'y0', 'bx0', 'bx1'
 FITS_HDU_DTYPE = np.dtype({'names': ['header_src', 'header_len', 'data_src', 'n_elem', 'dst'],
                            'formats': ['i8'] * 5, 'offsets': [0, 8, 16, 24, 32], 'itemsize': 40})
 
-SERSIC_HEADER = 16
+SERSIC_HEADER = 18
 SH_N, SH_NUSED, SH_FRONT, SH_DA, SH_KSQMIN, SH_KSQMAX, SH_KD2, SH_KD4, SH_HIGHA, SH_HIGHB, \
-    SH_MAXK, SH_STEPK, SH_RE, SH_DLOGK, SH_NCAND, SH_STATUS = range(16)
+    SH_MAXK, SH_STEPK, SH_RE, SH_DLOGK, SH_NCAND, SH_STATUS, SH_TRUNC, SH_FLUXFRAC = range(18)
 
 _lib = None
 
@@ -90,6 +90,7 @@ def lib():
             'gsb_sersic_tables_build': (i, [vp, vp, vp, i, ctypes.POINTER(GSParamsC), vp]),
             'gsb_sersic_tables_build_ex': (i, [vp, vp, vp, i, ctypes.POINTER(GSParamsC), i, vp]),
             'gsb_sersic_tables_info': (i, [vp, vp, i, vp]),
+            'gsb_sersic_truncation': (i, [i, vp, vp, vp]),
             'gsb_images_build': (i, [vp, i, vp, vp, ctypes.POINTER(GSParamsC), vp]),
             'gsb_images_info': (i, [vp, vp, i, vp]),
             'gsb_add_noise': (i, [i, vp, vp, i, i, vp, i, vp, vp, vp]),
@@ -185,6 +186,21 @@ class Device(object):
         return lst[:n]
 
 
+def sersic_truncation(n, size, trunc, size_is_hlr, flux_untruncated):
+    """(r0, flux fraction) per truncated Sersic profile, by FP64 root finding on the device
+    (gsb_sersic_truncation)."""
+    n, size, trunc = np.broadcast_arrays(np.atleast_1d(np.asarray(n, float)), np.asarray(size, float),
+                                         np.asarray(trunc, float))
+    inp = np.stack([n, size, trunc, np.full(n.shape, (1 if size_is_hlr else 0) | (2 if flux_untruncated else 0),
+                                            dtype=float)], -1)
+    inp = np.ascontiguousarray(inp, dtype=np.float64)
+    out = np.zeros((len(n), 2))
+    Device.torch_device()
+    check(lib().gsb_sersic_truncation(len(n), inp.ctypes.data_as(ctypes.c_void_p),
+                                      out.ctypes.data_as(ctypes.c_void_p), Device.stream()))
+    return out[:, 0], out[:, 1]
+
+
 def set_draw_variant(variant):
     """0 automatic (autotuned), 1 fused kernel only, 2 split kernels where N >= 192."""
     check(lib().gsb_draw_set_variant(int(variant)))
@@ -226,11 +242,14 @@ class Tables(object):
         check(lib().gsb_tables_create(ctypes.byref(h)))
         self.handle = h
 
-    def build_sersic(self, n_values, gsp, with_dn=False):
-        """Build one table per Sersic index; with_dn also builds the d/dn tables that the
-        adjoint needs (the tables themselves are the same either way)."""
+    def build_sersic(self, n_values, gsp, with_dn=False, trunc_over_r0=None):
+        """Build one table per Sersic index (and truncation radius / r0, 0 = untruncated);
+        with_dn also builds the d/dn tables that the adjoint needs (the tables themselves are
+        the same either way)."""
         n = np.ascontiguousarray(n_values, dtype=np.float64)
-        check(lib().gsb_sersic_tables_build_ex(self.handle, n.ctypes.data_as(ctypes.c_void_p), None,
+        tr = None if trunc_over_r0 is None else np.ascontiguousarray(trunc_over_r0, dtype=np.float64)
+        check(lib().gsb_sersic_tables_build_ex(self.handle, n.ctypes.data_as(ctypes.c_void_p),
+                                               tr.ctypes.data_as(ctypes.c_void_p) if tr is not None else None,
                                                len(n), ctypes.byref(gsparams_c(gsp)),
                                                TABLES_DN if with_dn else 0, Device.stream()))
         self.count = len(n)

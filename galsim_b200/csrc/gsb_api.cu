@@ -10,6 +10,7 @@
 namespace gsb {
 
 int ogata_init(DeviceState* st);
+int sersic_truncation(int count, const double* h_in, double* h_out, cudaStream_t stream);
 int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc, int count,
                         const gsb_gsparams* gsp, bool with_dn, cudaStream_t stream);
 int adjoint_grad_count(const gsb_template* tpl);
@@ -154,6 +155,7 @@ int gsb_tables_destroy(gsb_tables* t)
     cudaFree(t->d_scan);
     cudaFree(t->d_n);
     cudaFree(t->d_status);
+    cudaFree(t->d_trunc);
     cudaFree(t->d_dheader);
     cudaFree(t->d_dnode);
     cudaFree(t->d_dval);
@@ -182,6 +184,19 @@ int gsb_sersic_tables_build_ex(gsb_tables* t, const double* h_n, const double* h
     if (flags & ~GSB_TABLES_DN) return set_error(GSB_ERR_INVALID, "unknown table flags");
     return sersic_tables_build(t, h_n, h_trunc_over_r0, count, gsp, (flags & GSB_TABLES_DN) != 0,
                                (cudaStream_t)stream);
+}
+
+int gsb_sersic_truncation(int count, const double* h_in, double* h_out, void* stream)
+{
+    if (count < 0 || (count > 0 && (!h_in || !h_out))) return set_error(GSB_ERR_INVALID, "bad arguments");
+    for (int i = 0; i < count; ++i) {
+        const double n = h_in[4 * i], size = h_in[4 * i + 1], trunc = h_in[4 * i + 2];
+        if (!(n >= 0.3 && n <= 6.2)) return set_error(GSB_ERR_INVALID, "Sersic index out of range [0.3, 6.2]");
+        if (!(size > 0.) || !(trunc > 0.)) return set_error(GSB_ERR_INVALID, "size and trunc must be > 0");
+        if ((int(h_in[4 * i + 3]) & 3) == 1 && !(trunc > 1.4142135623730951 * size))
+            return set_error(GSB_ERR_INVALID, "Sersic truncation must be larger than sqrt(2)*half_light_radius.");
+    }
+    return sersic_truncation(count, h_in, h_out, (cudaStream_t)stream);
 }
 
 int gsb_sersic_tables_info(const gsb_tables* t, double* h_out, int count, void* stream)

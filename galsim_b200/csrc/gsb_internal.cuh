@@ -51,7 +51,8 @@ struct SersicTableView {
 enum {
     kSH_N = 0, kSH_NUSED, kSH_FRONT, kSH_DA, kSH_KSQMIN, kSH_KSQMAX, kSH_KD2, kSH_KD4,
     kSH_HIGHA, kSH_HIGHB, kSH_MAXK, kSH_STEPK, kSH_RE, kSH_DLOGK, kSH_NCAND, kSH_STATUS,
-    kSersicHeader = 16
+    kSH_TRUNC, kSH_FLUXFRAC,    // truncation radius / r0 (0: untruncated) and the flux fraction within it
+    kSersicHeader = 18
 };
 
 // Per-slot derivative header (doubles) of tables built with n-derivatives: d/dn (at fixed
@@ -209,6 +210,8 @@ struct gsb_tables {
     double* d_val = nullptr;      // scratch: count * stride Hankel values
     void* d_scan = nullptr;       // scratch: per-slot state of the table's stopping scan
     double* d_n = nullptr;        // Sersic indices of the slots
+    double* d_trunc = nullptr;    // truncation radius / r0 of the slots (when any is truncated)
+    size_t cap_trunc = 0;
     int* d_status = nullptr;      // convergence status word
     size_t cap_slots = 0, cap_nodes = 0;
     // n-derivative tables (built on request)

@@ -255,6 +255,67 @@ __device__ double2 warp_hankel_pair(const OgataTables& og, double invn, double l
     return make_double2(a[1], a[3]);
 }
 
+// Truncated Hankel transform of the Sersic profile (math::hankel_trunc, src/math/Hankel.cpp:
+// 249-255, as SersicInfo::buildFT calls it for trunc > 0, src/SBSersic.cpp:453-457):
+//   I(k) = int_0^t r exp(-r^(1/n)) J0(k r) dr,   t = trunc / r0.
+// The reference integrates adaptively (Gauss-Kronrod-Patterson to relerr 1e-6); here the
+// integral is taken to near FP64 precision by 16-point Gauss-Legendre on panels between
+// consecutive zeros of J0(k r) (the first interval graded toward r = 0 in 48 halvings, where
+// r^(1/n) has its cusp), so the two agree to the reference's integration error.  One warp per
+// node: lanes 0-15 and 16-31 take two panels at a time, one Legendre node each.
+__device__ inline void gauss_legendre16(int q, double* x, double* w)
+{
+    // node q of P_16 by Newton's method from the Tricomi estimate, weight 2 / ((1 - x^2) P'^2)
+    double z = cos(kPi * (q + 0.75) / 16.5), dp = 1.;
+    for (int it = 0; it < 10; ++it) {
+        double p0 = 1., p1 = z;
+        for (int m = 2; m <= 16; ++m) {
+            const double p2 = ((2. * m - 1.) * z * p1 - (m - 1.) * p0) / m;
+            p0 = p1;
+            p1 = p2;
+        }
+        dp = 16. * (z * p1 - p0) / (z * z - 1.);
+        z -= p1 / dp;
+    }
+    *x = z;
+    *w = 2. / ((1. - z * z) * dp * dp);
+}
+
+__device__ double warp_hankel_trunc(const OgataTables& og, double invn, double k, double t, int* status)
+{
+    const int lane = threadIdx.x & 31, half = lane >> 4;
+    double xq, wq;
+    gauss_legendre16(lane & 15, &xq, &wq);
+    const double rfirst = fmin(og.root[0].x / k, t);
+    constexpr int M = 48;
+    double acc = 0.;
+    for (long long jp = 0;; jp += 2) {
+        // panel jp (lanes 0-15) and jp + 1 (lanes 16-31)
+        const long long j = jp + half;
+        double a, b;
+        bool live;
+        if (j < M) {
+            a = ldexp(rfirst, int(j - M));
+            b = ldexp(rfirst, int(j + 1 - M));
+            live = true;
+        } else {
+            const long long m = j - M;                      // panel between zeros m and m + 1 (1-based)
+            if (m + 1 >= og.nroot) { if (status) *status = 1; live = false; a = b = t; }
+            else {
+                a = m == 0 ? rfirst : og.root[m - 1].x / k;
+                b = fmin(og.root[m].x / k, t);
+                live = a < t;
+            }
+        }
+        if (!__any_sync(0xffffffffu, live)) break;
+        if (live) {
+            const double h = 0.5 * (b - a), r = a + h * (1. + xq);
+            acc += wq * h * r * exp(-pow(r, invn)) * j0(k * r);
+        }
+    }
+    return warp_total(acc);
+}
+
 struct KolmKValue {
     __device__ double operator()(double logk) const { return exp_tab(-exp_tab(logk * (5. / 3.))); }
 };
@@ -300,21 +361,73 @@ __device__ RootResult sersic_missing_flux_radius(double n, double gamma2n, doubl
     return {pow(z, n), true};
 }
 
-__global__ void sersic_setup_kernel(const double* n_arr, int count, gsb_gsparams gsp,
+// Truncated Sersic sizes (sersic.py:218-247 with SersicTruncatedScale / SersicIntegratedFlux,
+// src/SBSersic.cpp:332-336, 688-775): per profile (n, size, trunc, flags) with flags bit 0 = size
+// is a half-light radius, bit 1 = flux_untruncated:
+//   r0 = size                                 (scale radius given)
+//   r0 = hlr / b_untruncated(n)^n             (hlr given, flux_untruncated)
+//   r0 = hlr * CalculateTruncatedScale(n, b, trunc / hlr)   (hlr of the truncated profile)
+// and the flux fraction gamma_p(2n, (trunc / r0)^(1/n)) inside trunc.
+struct SersicTruncatedHLR {
+    double twon, x, gam;
+    __device__ double operator()(double b) const
+    { return (2. * gamma_p(twon, b) - gamma_p(twon, x * b)) * gam; }
+};
+
+__global__ void sersic_truncation_kernel(const double* in, int count, double* out, int* status)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const double n = in[4 * i], size = in[4 * i + 1], trunc = in[4 * i + 2];
+    const int flags = int(in[4 * i + 3]);
+    const double gamma2n = tgamma(2. * n);
+    double r0 = size;
+    if (flags & 1) {
+        const RootResult rb = sersic_b(n, gamma2n, 1.);
+        if (!rb.ok) { atomicOr(status, 1); return; }
+        if (flags & 2) {
+            r0 = size / pow(rb.x, n);
+        } else {
+            // b solves gamma_p(2n, b) = gamma_p(2n, x b) / 2, x = (trunc / hlr)^(1/n), bracketed
+            // by the asymptotic guess (or b / 2) and the untruncated b (SBSersic.cpp:688-768)
+            const double x = pow(trunc / size, 1. / n);
+            double b1 = (log(0.5) + (2. * n - 1.) * log(x)) / (x - 1.);
+            if (b1 < 1e-3 * rb.x) b1 = 0.5 * rb.x;
+            const RootResult rt = solve_bracket_lower_limit(SersicTruncatedHLR{2. * n, x, gamma2n}, b1, rb.x, 0.);
+            if (!rt.ok) { atomicOr(status, 1); return; }
+            r0 = size / pow(rt.x, n);
+        }
+    }
+    out[2 * i] = r0;
+    out[2 * i + 1] = gamma_p(2. * n, pow(trunc / r0, 1. / n));
+}
+
+__global__ void sersic_setup_kernel(const double* n_arr, const double* trunc_arr, int count, gsb_gsparams gsp,
                                     double* header, int stride, double* dheader)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= count) return;
     double* H = header + (size_t)s * kSersicHeader;
     const double n = n_arr[s];
+    const double trunc = trunc_arr ? trunc_arr[s] : 0.;      // in units of r0
     const double gamma2n = tgamma(2. * n);
-    const double gamma4n = tgamma(4. * n);
-    const double gamma6n = tgamma(6. * n);
-    const double gamma8n = tgamma(8. * n);
-    // buildFT low-k series (SBSersic.cpp:386-424); untruncated, flux fraction 1
-    const double kderiv2 = -gamma4n / (4. * gamma2n);
-    const double kderiv4 = gamma6n / (64. * gamma2n);
-    const double kderiv6 = gamma8n / (2304. * gamma2n);
+    double gamma4n = tgamma(4. * n);
+    double gamma6n = tgamma(6. * n);
+    double gamma8n = tgamma(8. * n);
+    // truncated profiles (SBSersic.cpp:332-352, 393-424): the flux fraction inside trunc and the
+    // moments of the truncated profile
+    double ff = 1.;
+    if (trunc > 0.) {
+        const double z = pow(trunc, 1. / n);
+        ff = gamma_p(2. * n, z);
+        gamma4n *= gamma_p(4. * n, z);
+        gamma6n *= gamma_p(6. * n, z);
+        gamma8n *= gamma_p(8. * n, z);
+    }
+    // buildFT low-k series (SBSersic.cpp:386-424)
+    const double kderiv2 = -gamma4n / (4. * gamma2n) / ff;
+    const double kderiv4 = gamma6n / (64. * gamma2n) / ff;
+    const double kderiv6 = gamma8n / (2304. * gamma2n) / ff;
     const double kmin = pow(gsp.kvalue_accuracy / kderiv6, 1. / 6.);
     const double dlogk = gsp.table_spacing * sqrt(sqrt(gsp.kvalue_accuracy / 10.));
     int ncand = 0;
@@ -322,12 +435,15 @@ __global__ void sersic_setup_kernel(const double* n_arr, int count, gsb_gsparams
     for (double logk = log(kmin) - 0.001; logk < logk_end && ncand < stride; logk += dlogk)
         ++ncand;
     int status = 0;
-    RootResult rb = sersic_b(n, gamma2n, 1.);
+    RootResult rb = sersic_b(n, gamma2n, ff);
     if (!rb.ok) status = 2;
     const double b = rb.x;
+    // stepK (SBSersic.cpp:304-318): the untruncated missing-flux radius (its lower bracket falls
+    // back to the profile's own b, :589-592), capped at trunc
     RootResult rr = sersic_missing_flux_radius(n, gamma2n, b, gsp.folding_threshold);
     if (!rr.ok) status = 3;
     double R = rr.x;
+    if (trunc > 0. && trunc < R) R = trunc;
     R = fmax(R, gsp.stepk_minimum_hlr);
     H[kSH_N] = n;
     H[kSH_NUSED] = 0;
@@ -345,6 +461,8 @@ __global__ void sersic_setup_kernel(const double* n_arr, int count, gsb_gsparams
     H[kSH_DLOGK] = dlogk;
     H[kSH_NCAND] = ncand;
     H[kSH_STATUS] = status;
+    H[kSH_TRUNC] = trunc;
+    H[kSH_FLUXFRAC] = ff;
     if (dheader) {
         // d/dn of the low-k coefficients (ratios of Gamma functions) and of ln(r_e / r0) =
         // n ln b, with db/dn from P(2n, b) = 1/2 by implicit differentiation.
@@ -384,6 +502,31 @@ __global__ void sersic_scan_init_kernel(const double* header, int count, SersicS
     S.done = int(header[(size_t)s * kSersicHeader + kSH_NCAND]) < 2 ? 1 : 0;
 }
 
+// One warp per node of this round for the truncated tables (trunc > 0; the pair kernel skips
+// them): the truncated Hankel transform / hankel_norm, hankel_norm = flux fraction n Gamma(2n).
+__global__ void __launch_bounds__(256) sersic_trunc_nodes_kernel(const double* header, int count, int i0,
+                                    int nround, const __grid_constant__ OgataTables og, const SersicScan* scan,
+                                    double* vals, int stride, const int* prev_live, int* status_out)
+{
+    if (prev_live && *prev_live == 0) return;
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long s = warp / nround;
+    const int i = i0 + int(warp % nround);
+    if (s >= count) return;
+    const double* H = header + s * kSersicHeader;
+    if (H[kSH_TRUNC] <= 0. || scan[s].done) return;
+    if (i >= int(H[kSH_NCAND])) return;
+    const double n = H[kSH_N];
+    const double k = exp(H[kSH_FRONT] + i * H[kSH_DLOGK]);
+    const double hankel_norm = H[kSH_FLUXFRAC] * n * tgamma(2. * n);
+    int st = 0;
+    const double v = warp_hankel_trunc(og, 1. / n, k, H[kSH_TRUNC], &st) / hankel_norm;
+    if ((threadIdx.x & 31) == 0) {
+        vals[s * stride + i] = v;
+        if (st) atomicOr(status_out, 1);
+    }
+}
+
 // One warp per pair of adjacent nodes (i, i + 1) of this round: Hankel transform / hankel_norm at
 // k_i, k_{i+1} through warp_hankel_pair; DN: with the d/dn values of the same nodes.
 // prev_live (the previous round's scan flag) is zero once every table has stopped: the launch
@@ -409,6 +552,7 @@ __global__ void __launch_bounds__(256, 4) sersic_nodes_pair_kernel(const double*
     if (s < 0) return;
     if (scan[s].done) return;
     const double* H = header + s * kSersicHeader;
+    if (H[kSH_TRUNC] > 0.) return;          // sersic_trunc_nodes_kernel
     const int ncand = int(H[kSH_NCAND]);
     if (i >= ncand) return;
     const bool has1 = i + 1 < ncand && i + 1 < i0 + nround;
@@ -905,10 +1049,14 @@ int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc,
     for (int i = 0; i < count; ++i) {
         if (!(h_n[i] >= 0.3 && h_n[i] <= 6.2))
             return set_error(GSB_ERR_INVALID, "Sersic index out of range [0.3, 6.2]");
-        if (h_trunc && h_trunc[i] != 0.)
-            return set_error(GSB_ERR_UNSUPPORTED, "truncated Sersic profiles are not built");
+        if (h_trunc && !(h_trunc[i] >= 0.))
+            return set_error(GSB_ERR_INVALID, "Sersic truncation radius must be >= 0");
     }
     if (count <= 0) { t->count = 0; return GSB_OK; }
+    bool has_trunc = false;
+    for (int i = 0; h_trunc && i < count; ++i) has_trunc |= h_trunc[i] > 0.;
+    if (has_trunc && with_dn)
+        return set_error(GSB_ERR_UNSUPPORTED, "n-derivative tables of truncated Sersic profiles are not built");
     const int stride = sersic_stride(h_n, count, gsp);
     if ((size_t)count > t->cap_slots || (size_t)count * stride > t->cap_nodes) {
         cudaFree(t->d_header); cudaFree(t->d_node); cudaFree(t->d_val); cudaFree(t->d_scan);
@@ -942,9 +1090,21 @@ int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc,
     double* d_n = t->d_n;
     int* d_status = t->d_status;
     GSB_CUDA_CHECK(cudaMemcpyAsync(d_n, h_n, sizeof(double) * count, cudaMemcpyHostToDevice, stream));
+    double* d_trunc = nullptr;
+    if (has_trunc) {
+        if ((size_t)count > t->cap_trunc) {
+            cudaFree(t->d_trunc);
+            t->d_trunc = nullptr;
+            t->cap_trunc = count;
+            GSB_CUDA_CHECK(cudaMalloc(&t->d_trunc, sizeof(double) * t->cap_trunc));
+        }
+        d_trunc = t->d_trunc;
+        GSB_CUDA_CHECK(cudaMemcpyAsync(d_trunc, h_trunc, sizeof(double) * count, cudaMemcpyHostToDevice, stream));
+    }
     // d_status[0]: convergence status; d_status[1 + r]: some table still needs nodes after round r
     GSB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int) * (1 + kMaxRounds), stream));
-    sersic_setup_kernel<<<(count + 127) / 128, 128, 0, stream>>>(d_n, count, *gsp, t->d_header, stride, dheader);
+    sersic_setup_kernel<<<(count + 127) / 128, 128, 0, stream>>>(d_n, d_trunc, count, *gsp, t->d_header, stride,
+                                                                 dheader);
     GSB_CUDA_CHECK(cudaGetLastError());
     sersic_scan_init_kernel<<<(count + 127) / 128, 128, 0, stream>>>(t->d_header, count, static_cast<SersicScan*>(t->d_scan));
     GSB_CUDA_CHECK(cudaGetLastError());
@@ -965,6 +1125,13 @@ int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc,
                 t->d_header, count, i0, kRound, *gsp, st->og, static_cast<const SersicScan*>(t->d_scan),
                 t->d_val, stride, prev_live, d_status, nullptr, nullptr);
         GSB_CUDA_CHECK(cudaGetLastError());
+        if (has_trunc) {
+            const long long tw = (long long)count * kRound;
+            sersic_trunc_nodes_kernel<<<(unsigned)((tw * 32 + threads - 1) / threads), threads, 0, stream>>>(
+                t->d_header, count, i0, kRound, st->og, static_cast<const SersicScan*>(t->d_scan), t->d_val, stride,
+                prev_live, d_status);
+            GSB_CUDA_CHECK(cudaGetLastError());
+        }
         sersic_scan_kernel<<<(count + 63) / 64, 64, 0, stream>>>(t->d_header, count, stride, i0, kRound,
                                                                  *gsp, t->d_val, t->d_node, static_cast<SersicScan*>(t->d_scan),
                                                                  dval, dnode, prev_live, d_status + 1 + r);
@@ -983,6 +1150,29 @@ int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc,
     GSB_CUDA_CHECK(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
     GSB_CUDA_CHECK(cudaStreamSynchronize(stream));
     if (h_status) return set_error(GSB_ERR_NUMERIC, "Sersic Hankel transform did not converge");
+    return GSB_OK;
+}
+
+int sersic_truncation(int count, const double* h_in, double* h_out, cudaStream_t stream)
+{
+    if (count <= 0) return GSB_OK;
+    double *d_in = nullptr, *d_out = nullptr;
+    int* d_status = nullptr;
+    GSB_CUDA_CHECK(cudaMallocAsync(&d_in, sizeof(double) * 4 * count, stream));
+    GSB_CUDA_CHECK(cudaMallocAsync(&d_out, sizeof(double) * 2 * count, stream));
+    GSB_CUDA_CHECK(cudaMallocAsync(&d_status, sizeof(int), stream));
+    GSB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), stream));
+    GSB_CUDA_CHECK(cudaMemcpyAsync(d_in, h_in, sizeof(double) * 4 * count, cudaMemcpyHostToDevice, stream));
+    sersic_truncation_kernel<<<(count + 127) / 128, 128, 0, stream>>>(d_in, count, d_out, d_status);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    int h_status = 0;
+    GSB_CUDA_CHECK(cudaMemcpyAsync(h_out, d_out, sizeof(double) * 2 * count, cudaMemcpyDeviceToHost, stream));
+    GSB_CUDA_CHECK(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    GSB_CUDA_CHECK(cudaStreamSynchronize(stream));
+    cudaFreeAsync(d_in, stream);
+    cudaFreeAsync(d_out, stream);
+    cudaFreeAsync(d_status, stream);
+    if (h_status) return set_error(GSB_ERR_NUMERIC, "truncated Sersic scale radius root find did not converge");
     return GSB_OK;
 }
 

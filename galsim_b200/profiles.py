@@ -139,7 +139,12 @@ class Exponential(_Leaf):
 
 class Sersic(_Leaf):
     """exp(-(r/r0)^(1/n)) (sersic.py:196-373).  The FT is a per-n FP64 Hankel table built on
-    the GPU; half_light_radius -> scale_radius uses the same table build (Brent in FP64)."""
+    the GPU; half_light_radius -> scale_radius uses the same table build (Brent in FP64).
+    trunc > 0 truncates the profile there: without flux_untruncated, flux and half_light_radius
+    refer to the truncated profile (its scale radius from SersicTruncatedScale), with it to the
+    untruncated one (the flux then scaled by the fraction inside trunc), sersic.py:218-247; the
+    sizes come from an FP64 root find on the GPU and the table from the truncated Hankel
+    transform."""
     _minimum_n = 0.3
     _maximum_n = 6.2
     _is_axisymmetric = True
@@ -149,7 +154,8 @@ class Sersic(_Leaf):
                  flux=1., trunc=0., flux_untruncated=False, gsparams=None):
         self._n = _as_param(n)
         self._flux = _as_param(flux)
-        self._trunc = float(trunc)
+        self._trunc = _as_param(trunc)
+        self._flux_untruncated = bool(flux_untruncated)
         self._gsparams = GSParams.check(gsparams)
         if np.any(np.asarray(self._n) < Sersic._minimum_n):
             raise GalSimRangeError("Requested Sersic index is too small",
@@ -157,11 +163,8 @@ class Sersic(_Leaf):
         if np.any(np.asarray(self._n) > Sersic._maximum_n):
             raise GalSimRangeError("Requested Sersic index is too large",
                                    self._n, Sersic._minimum_n, Sersic._maximum_n)
-        if self._trunc < 0:
+        if np.any(np.asarray(self._trunc) < 0):
             raise GalSimRangeError("Sersic trunc must be > 0", self._trunc, 0.)
-        if self._trunc > 0:
-            from .errors import GalSimNotImplementedError
-            raise GalSimNotImplementedError("truncated Sersic profiles are not built")
         if half_light_radius is not None:
             if scale_radius is not None:
                 raise GalSimIncompatibleValuesError(
@@ -177,20 +180,42 @@ class Sersic(_Leaf):
                 "Either scale_radius or half_light_radius must be specified for Spergel",
                 half_light_radius=half_light_radius, scale_radius=scale_radius)
         self._flux_fraction = 1.
-        self._batch = _plen(self._n, self._flux, self._hlr if self._hlr is not None else self._r0)
+        truncated = np.any(np.asarray(self._trunc) > 0)
+        if truncated:
+            if not np.all(np.asarray(self._trunc) > 0):
+                raise GalSimIncompatibleValuesError("a batch of Sersic profiles is either truncated "
+                                                    "or not", trunc=self._trunc)
+            if self._hlr is not None and not self._flux_untruncated and \
+                    np.any(np.asarray(self._trunc) <= math.sqrt(2.) * np.asarray(self._hlr)):
+                raise GalSimRangeError("Sersic trunc must be > sqrt(2) * half_light_radius",
+                                       self._trunc, math.sqrt(2.) * np.asarray(self._hlr))
+            size = self._hlr if self._hlr is not None else self._r0
+            r0, ff = _lib.sersic_truncation(self._n, size, self._trunc, self._hlr is not None,
+                                            self._flux_untruncated)
+            scalar = np.ndim(self._n) == 0 and np.ndim(size) == 0 and np.ndim(self._trunc) == 0
+            self._r0 = float(r0[0]) if scalar else r0
+            self._flux_fraction = float(ff[0]) if scalar else ff
+            if self._flux_untruncated:
+                self._flux = self._flux * self._flux_fraction
+                self._hlr = None          # the truncated profile's, computed when asked for
+        self._batch = _plen(self._n, self._flux, self._hlr if self._hlr is not None else self._r0,
+                            self._trunc)
 
     n = property(lambda self: self._n)
     trunc = property(lambda self: self._trunc)
 
     def calculateHLRFactor(self):
         """Half-light radius in units of the scale radius (SersicHLR, SBSersic.cpp:660-667),
-        computed on the GPU."""
+        computed on the GPU (of the truncated profile when truncated)."""
         n = np.atleast_1d(self._n)
-        uniq, inv = np.unique(n, return_inverse=True)
-        t = _lib.Tables()
-        t.build_sersic(uniq, self.gsparams)
-        re = t.sersic_info()[:, _lib.SH_RE][inv]
-        return float(re[0]) if np.ndim(self._n) == 0 else re
+        t = np.broadcast_to(np.atleast_1d(np.asarray(self._trunc, float)), n.shape)
+        r0 = np.broadcast_to(np.atleast_1d(np.asarray(self._r0, float)), n.shape) if self._r0 is not None else None
+        tr = (t / r0) if (r0 is not None and np.any(t > 0)) else np.zeros_like(n)
+        uniq, inv = np.unique(np.stack([n, tr], -1), axis=0, return_inverse=True)
+        tabs = _lib.Tables()
+        tabs.build_sersic(uniq[:, 0], self.gsparams, trunc_over_r0=uniq[:, 1] if np.any(uniq[:, 1] > 0) else None)
+        re = tabs.sersic_info()[:, _lib.SH_RE][np.asarray(inv).reshape(-1)]
+        return float(re[0]) if np.ndim(self._n) == 0 and re.size == 1 else re
 
     @property
     def scale_radius(self):
@@ -207,12 +232,14 @@ class Sersic(_Leaf):
     def _params(self):
         if self._hlr is not None and self._r0 is None:
             return (self._n, self._hlr, 0.)
-        return (self._n, self._r0, 0.)
+        return (self._n, self._r0, self._trunc)
 
     def _leaf_flags(self):
         return _lib.LEAF_SIZE_IS_HLR if (self._hlr is not None and self._r0 is None) else 0
 
     def withFlux(self, flux):
+        if np.any(np.asarray(self._trunc) > 0):
+            return Sersic(n=self.n, scale_radius=self._r0, flux=flux, trunc=self._trunc, gsparams=self.gsparams)
         if self._r0 is None:
             return Sersic(n=self.n, half_light_radius=self._hlr, flux=flux, gsparams=self.gsparams)
         return Sersic(n=self.n, scale_radius=self._r0, flux=flux, gsparams=self.gsparams)

@@ -129,12 +129,18 @@ class Program(object):
         B, L = self.B, self.L
         leaves = np.stack(self.bld.leaves, axis=1)            # (B, L)
         self.sersic_n = None
+        self.sersic_trunc = None
         sersic = [l for l in range(L) if self.bld.leaf_types[l] == _lib.SERSIC]
         if sersic:
+            # one table per distinct (n, trunc / r0); truncated leaves carry r0 in p[1]
             nvals = np.concatenate([leaves[:, l]['p'][:, 0] for l in sersic])
-            uniq, inv = np.unique(nvals, return_inverse=True)
-            self.sersic_n = uniq
-            inv = inv.reshape(len(sersic), B)
+            tvals = np.concatenate([np.where(leaves[:, l]['p'][:, 2] > 0.,
+                                             leaves[:, l]['p'][:, 2] / leaves[:, l]['p'][:, 1], 0.)
+                                    for l in sersic])
+            uniq, inv = np.unique(np.stack([nvals, tvals], -1), axis=0, return_inverse=True)
+            self.sersic_n = np.ascontiguousarray(uniq[:, 0])
+            self.sersic_trunc = np.ascontiguousarray(uniq[:, 1]) if np.any(uniq[:, 1] > 0.) else None
+            inv = np.asarray(inv).reshape(len(sersic), B)
             for k, l in enumerate(sersic):
                 leaves['table'][:, l] = inv[k]
         self.image_order = []
@@ -163,7 +169,8 @@ class Program(object):
         self.upload()
         B, L = self.B, self.L
         if self.tables is not None and self.sersic_n is not None:
-            self.tables.build_sersic(self.sersic_n, self.gsparams, with_dn=self.need_dn)
+            self.tables.build_sersic(self.sersic_n, self.gsparams, with_dn=self.need_dn,
+                                     trunc_over_r0=self.sersic_trunc)
         if self.image_order:
             self._build_images()
         _lib.check(_lib.lib().gsb_prepare_leaves(
@@ -318,7 +325,8 @@ class Program(object):
         if graph and add_to is None:
             # the captured launches hold the table pointers: the same Sersic indices keep them
             key = tuple(np.asarray(v, np.int64).tobytes() for v in (N, Nk, xmin, ymin, nx, ny)) + \
-                (dtype, precision, b'' if self.sersic_n is None else self.sersic_n.tobytes())
+                (dtype, precision, b'' if self.sersic_n is None else self.sersic_n.tobytes(),
+                 b'' if self.sersic_trunc is None else self.sersic_trunc.tobytes())
             gs = getattr(self, '_graph_state', None)
             if gs is not None and gs['key'] == key:
                 g = gs['geom']

@@ -163,7 +163,10 @@ int gsb_tables_destroy(gsb_tables* t);
  * natural-spline coefficients, the low-k quartic and high-k asymptote, maxk, stepk and the
  * half-light radius in units of r0.  Reference: SersicInfo (src/SBSersic.cpp:301-667),
  * hankel_inf (src/math/Hankel.cpp:231-249), TSpline (src/Table.cpp:553-686).
- * h_n / h_trunc_over_r0 are host arrays.  Truncated profiles (trunc > 0) are not built. */
+ * h_n / h_trunc_over_r0 are host arrays (h_trunc_over_r0 may be NULL: untruncated).  A slot with
+ * trunc > 0 is the truncated profile's table: flux fraction, moments and the Hankel transform
+ * over 0 .. trunc (math::hankel_trunc, src/math/Hankel.cpp:249-255, src/SBSersic.cpp:393-457),
+ * stepk capped at trunc; its n-derivative tables (GSB_TABLES_DN) are not built. */
 int gsb_sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc_over_r0,
                             int count, const gsb_gsparams* gsp, void* stream);
 
@@ -177,7 +180,16 @@ int gsb_sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_tr
 int gsb_sersic_tables_build_ex(gsb_tables* t, const double* h_n, const double* h_trunc_over_r0,
                                int count, const gsb_gsparams* gsp, int flags, void* stream);
 
-/* Copy slot headers back (16 doubles per slot: see gsb_tables.cu) for inspection. */
+/* Scale radius and flux fraction of truncated Sersic profiles (sersic.py:218-247 with
+ * SersicTruncatedScale, SersicHLR and SersicIntegratedFlux, src/SBSersic.cpp:332-336, 627-775),
+ * by FP64 root finding on the device.  h_in: per profile 4 doubles (n, size, trunc, flags):
+ * flags bit 0 = size is a half-light radius (else the scale radius), bit 1 = flux_untruncated
+ * (the half-light radius refers to the untruncated profile).  h_out: per profile (r0, flux
+ * fraction inside trunc).  A half-light radius of the truncated profile needs
+ * trunc > sqrt(2) hlr (GSB_ERR_INVALID otherwise, as the reference). */
+int gsb_sersic_truncation(int count, const double* h_in, double* h_out, void* stream);
+
+/* Copy slot headers back (18 doubles per slot: see gsb_tables.cu) for inspection. */
 int gsb_sersic_tables_info(const gsb_tables* t, double* h_out, int count, void* stream);
 
 /* InterpolatedImage sources ------------------------------------------------------------ */

@@ -197,6 +197,30 @@ def hankel_inf(f, k, relerr, abserr):
     return ans1
 
 
+def hankel_trunc_exact(f, k, rmax):
+    """int_0^rmax r f(r) J0(k r) dr -- the quantity of math::hankel_trunc
+    (src/math/Hankel.cpp:249-255), computed to ~1e-13 relative: adaptive Gauss-Kronrod
+    (scipy.integrate.quad) on panels between consecutive zeros of J0(k r), with breakpoints
+    graded toward r = 0 where r f(r) has an integrable cusp.  The reference integrates the same
+    integral with its own adaptive Gauss-Kronrod-Patterson scheme to relerr 1e-6, so the two
+    agree to the reference's integration error (this value is the more accurate one)."""
+    from scipy import integrate
+    g = lambda r: r * f(r) * special.j0(k * r)
+    pts = [0.]
+    if k > 0.:
+        zs = _j0_zeros(max(16, int(k * rmax / PI) + 8))[0] / k
+        pts += [float(z) for z in zs if z < rmax]
+    pts.append(float(rmax))
+    first = pts[1]
+    grade = [first * 2. ** -j for j in range(1, 30)][::-1]
+    pts = [0.] + grade + pts[1:]
+    tot = 0.
+    for a, b in zip(pts[:-1], pts[1:]):
+        v, _ = integrate.quad(g, a, b, epsabs=0., epsrel=1e-13, limit=200)
+        tot += v
+    return tot
+
+
 # ---------------------------------------------------------------------------------------------
 # Natural cubic spline (src/Table.cpp:553-686)
 # ---------------------------------------------------------------------------------------------
@@ -247,13 +271,21 @@ _SERSIC = {}
 
 
 class SersicInfo(object):
-    def __init__(self, n, gsp):
+    """SersicInfo (src/SBSersic.cpp:288-667); trunc > 0 (in units of r0) for a truncated
+    profile: flux fraction gamma_p(2n, trunc^(1/n)) (:332-352), truncated low-k moments and Hankel
+    normalisation (:393-424), hankel_trunc values (:453-457), stepk capped at trunc (:304-318)."""
+
+    def __init__(self, n, gsp, trunc=0.):
         self.n = n
         self.gsp = gsp
+        self.trunc = float(trunc)
         self.gamma2n = special.gamma(2 * n)
+        self.flux_fraction = (special.gammainc(2. * n, self.trunc ** (1. / n)) if self.trunc > 0. else 1.)
         self.b = self._calc_b()
         self.re = self.b ** n
         R = self._missing_flux_radius(gsp.folding_threshold)
+        if self.trunc > 0. and self.trunc < R:
+            R = self.trunc
         R = max(R, gsp.stepk_minimum_hlr)
         self.stepk = PI / R
         self._build_ft()
@@ -263,11 +295,12 @@ class SersicInfo(object):
         return lambda z: (1. - special.gammainc(twon, z)) * gam - target
 
     def _calc_b(self):
+        """CalculateB (SBSersic.cpp:627-658) with the profile's flux fraction."""
         n = self.n
         invn = 1. / n
         b1 = 2. * n - 1. / 3.
         b2 = b1 + (8. / 405.) * invn + (46. / 25515.) * invn ** 2 + (131. / 1148175.) * invn ** 3
-        return solve_lower_limit(self._missing(0.5 * self.gamma2n), b1, b2, 0.)
+        return solve_lower_limit(self._missing((1. - 0.5 * self.flux_fraction) * self.gamma2n), b1, b2, 0.)
 
     def _missing_flux_radius(self, frac):
         n = self.n
@@ -290,13 +323,19 @@ class SersicInfo(object):
 
     def _build_ft(self):
         n, gsp = self.n, self.gsp
-        g2, g4, g6, g8 = (special.gamma(m * n) for m in (2, 4, 6, 8))
-        self.kd2 = -g4 / (4. * g2)
-        self.kd4 = g6 / (64. * g2)
-        kd6 = g8 / (2304. * g2)
+        g2 = special.gamma(2. * n)
+        if self.trunc > 0.:
+            z = self.trunc ** (1. / n)
+            g4, g6, g8 = (special.gammainc(m * n, z) * special.gamma(m * n) for m in (4, 6, 8))
+        else:
+            g4, g6, g8 = (special.gamma(m * n) for m in (4, 6, 8))
+        ff = self.flux_fraction
+        self.kd2 = -g4 / (4. * g2) / ff
+        self.kd4 = g6 / (64. * g2) / ff
+        kd6 = g8 / (2304. * g2) / ff
         kmin = (gsp.kvalue_accuracy / kd6) ** (1. / 6.)
         self.ksq_min = kmin * kmin
-        hankel_norm = n * g2
+        hankel_norm = ff * n * g2
         dlogk = gsp.table_spacing * math.sqrt(math.sqrt(gsp.kvalue_accuracy / 10.))
         f = lambda r: np.exp(-np.power(r, 1. / n))
         n_fit = 10
@@ -314,7 +353,10 @@ class SersicInfo(object):
             lk = math.log(kmin) - 0.001 + i * dlogk
             k = math.exp(lk)
             ksq = k * k
-            val = hankel_inf(f, k, gsp.integration_relerr, gsp.integration_abserr * hankel_norm) / hankel_norm
+            if self.trunc > 0.:
+                val = hankel_trunc_exact(f, k, self.trunc) / hankel_norm
+            else:
+                val = hankel_inf(f, k, gsp.integration_relerr, gsp.integration_abserr * hankel_norm) / hankel_norm
             f0 = val * ksq
             args.append(lk)
             vals.append(f0)
@@ -376,11 +418,31 @@ class SersicInfo(object):
         return out
 
 
-def sersic_info(n, gsp=DEFAULT):
-    key = (n, id(gsp))
+def sersic_info(n, gsp=DEFAULT, trunc=0.):
+    key = (n, id(gsp), float(trunc))
     if key not in _SERSIC:
-        _SERSIC[key] = SersicInfo(n, gsp)
+        _SERSIC[key] = SersicInfo(n, gsp, trunc)
     return _SERSIC[key]
+
+
+def sersic_truncated_scale(n, hlr, trunc):
+    """SersicTruncatedScale (SBSersic.cpp:700-775): the scale radius that gives a Sersic
+    truncated at trunc the half-light radius hlr: b solves gamma_p(2n, b) = gamma_p(2n, x b) / 2
+    with x = (trunc / hlr)^(1/n), bracketed between the untruncated b (upper) and an asymptotic
+    guess (lower, expanded toward 0); r0 = hlr / b^n."""
+    invn = 1. / n
+    b = sersic_info(n).b
+    t = trunc / hlr
+    if t <= math.sqrt(2.):
+        raise ValueError("Sersic truncation must be larger than sqrt(2)*half_light_radius.")
+    x = t ** invn
+    b1 = (math.log(0.5) + (2. * n - 1) * math.log(x)) / (x - 1.)
+    if b1 < 1e-3 * b:
+        b1 = b / 2.
+    twon, gam = 2. * n, special.gamma(2. * n)
+    fn = lambda bb: (2. * special.gammainc(twon, bb) - special.gammainc(twon, x * bb)) * gam
+    bb = solve_lower_limit(fn, b1, b, 0.)
+    return hlr / bb ** n
 
 
 # ---------------------------------------------------------------------------------------------
@@ -608,10 +670,20 @@ class OExponential(OLeaf):
 
 
 class OSersic(OLeaf):
-    def __init__(self, n, r0=None, hlr=None, flux=1.):
-        self.n, self.flux = float(n), float(flux)
-        self.info = sersic_info(self.n, self.gsp)
-        self.r0 = float(r0) if r0 is not None else float(hlr) / self.info.re
+    """Sersic (sersic.py:200-265): trunc > 0 truncates at that radius; without
+    flux_untruncated the flux and half-light radius are those of the truncated profile."""
+
+    def __init__(self, n, r0=None, hlr=None, flux=1., trunc=0., flux_untruncated=False):
+        self.n, self.flux, self.trunc = float(n), float(flux), float(trunc)
+        if r0 is not None:
+            self.r0 = float(r0)
+        elif self.trunc == 0. or flux_untruncated:
+            self.r0 = float(hlr) / sersic_info(self.n, self.gsp).re
+        else:
+            self.r0 = sersic_truncated_scale(self.n, float(hlr), self.trunc)
+        self.info = sersic_info(self.n, self.gsp, self.trunc / self.r0 if self.trunc > 0. else 0.)
+        if self.trunc > 0. and flux_untruncated:
+            self.flux *= self.info.flux_fraction
 
     def stepk_maxk(self):
         return self.info.stepk / self.r0, self.info.maxk / self.r0

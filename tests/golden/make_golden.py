@@ -29,6 +29,10 @@ def profile(galsim, spec):
         return galsim.Exponential(half_light_radius=spec[1], flux=spec[2])
     if kind == 'sersic':
         return galsim.Sersic(n=spec[1], half_light_radius=spec[2], flux=spec[3])
+    if kind == 'sersict':
+        # ('sersict', n, size, flux, trunc, flux_untruncated, 'hlr' | 'r0')
+        size = dict(half_light_radius=spec[2]) if spec[6] == 'hlr' else dict(scale_radius=spec[2])
+        return galsim.Sersic(n=spec[1], flux=spec[3], trunc=spec[4], flux_untruncated=spec[5], **size)
     if kind == 'moffat':
         return galsim.Moffat(beta=spec[1], fwhm=spec[2], flux=spec[3])
     if kind == 'kolmogorov':
@@ -570,6 +574,44 @@ def main_standalone(ref_root):
     print('wrote', os.path.join(HERE, 'reference_standalone.npz'), len(out), 'arrays')
 
 
+# Truncated Sersic profiles (sersic.py:196-265, SersicInfo with trunc > 0): drawImage through the
+# reference, and the leaves' stepk / maxk.
+TRUNC_CASES = [
+    # (name, spec, nx, ny, scale, dtype, offset)
+    ('t_n15_hlr_moffat', ('conv', [('sersict', 1.5, 0.5, 100., 2.0, False, 'hlr'), ('moffat', 3.0, 0.6, 1.),
+                                   ('pixel', 0.2)]), 48, 48, 0.2, 'f8', (0., 0.)),
+    ('t_n3_shear_kolm_f4', ('conv', [('shear', 0.1, -0.2, ('sersict', 3.0, 0.4, 1e3, 1.5, False, 'hlr')),
+                                     ('kolmogorov', 0.7, 1.), ('pixel', 0.2)]), 48, 48, 0.2, 'f4', (0., 0.)),
+    ('t_n4_fluxuntrunc', ('conv', [('sersict', 4.0, 0.5, 100., 3.0, True, 'hlr'), ('moffat', 3.0, 0.6, 1.),
+                                   ('pixel', 0.2)]), 48, 48, 0.2, 'f8', (0.2, -0.1)),
+    ('t_n25_r0_airy', ('conv', [('sersict', 2.5, 0.1, 50., 0.6, False, 'r0'), ('airy', 0.1, 0.3, 1.),
+                                ('pixel', 0.05)]), 40, 40, 0.05, 'f8', (0., 0.)),
+    ('t_n1_alone', ('sersict', 1.0, 0.6, 20., 1.2, False, 'hlr'), 32, 32, 0.2, 'f8', (0., 0.)),
+    ('t_bulge_disk_f4', ('conv', [('sum', [('sersict', 4.0, 0.3, 300., 1.5, False, 'hlr'),
+                                           ('shear', -0.2, 0.1, ('exp', 0.8, 700.))]),
+                                  ('moffat', 3.7, 0.7, 1.), ('pixel', 0.2)]), 48, 48, 0.2, 'f4', (0., 0.)),
+]
+TRUNC_SIZE_CASES = [('sersict', n, 0.5, 1., t, fu, kind) for n, t, fu, kind in
+                    ((0.7, 1.0, False, 'hlr'), (1.5, 2.0, False, 'hlr'), (3.0, 1.5, False, 'hlr'),
+                     (4.0, 3.0, True, 'hlr'), (5.5, 2.5, False, 'r0'), (2.0, 0.9, False, 'hlr'))]
+
+
+def main_trunc(ref_root):
+    from ref_import import import_reference_galsim
+    galsim = import_reference_galsim(ref_root)
+    out = {}
+    for name, spec, nx, ny, scale, dt, off in TRUNC_CASES:
+        im = profile(galsim, spec).drawImage(nx=nx, ny=ny, scale=scale, dtype=np.dtype(dt).type, method='fft',
+                                             offset=off)
+        out['draw_' + name] = im.array
+        out['draw_' + name + '_flux'] = np.array(im.added_flux)
+    out['sizes'] = np.array([(profile(galsim, sp).stepk, profile(galsim, sp).maxk) for sp in TRUNC_SIZE_CASES])
+    out['scale_radius'] = np.array([profile(galsim, sp).scale_radius for sp in TRUNC_SIZE_CASES])
+    out['flux'] = np.array([profile(galsim, sp).flux for sp in TRUNC_SIZE_CASES])
+    np.savez_compressed(os.path.join(HERE, 'reference_trunc.npz'), **out)
+    print('wrote', os.path.join(HERE, 'reference_trunc.npz'), len(out), 'arrays')
+
+
 def main(ref_root):
     from ref_import import import_reference_galsim
     galsim = import_reference_galsim(ref_root)
@@ -635,6 +677,8 @@ if __name__ == '__main__':
         main_configs(root)
     elif '--standalone-only' in sys.argv:
         main_standalone(root)
+    elif '--trunc-only' in sys.argv:
+        main_trunc(root)
     else:
         if '--large-only' not in sys.argv:
             main(root)
@@ -646,3 +690,4 @@ if __name__ == '__main__':
         main_fits(root)
         main_configs(root)
         main_standalone(root)
+        main_trunc(root)

@@ -16,6 +16,9 @@ def oracle_profile(spec):
         return O.OExponential(spec[1] / 1.6783469900166605, spec[2])
     if kind == 'sersic':
         return O.OSersic(spec[1], hlr=spec[2], flux=spec[3])
+    if kind == 'sersict':
+        size = dict(hlr=spec[2]) if spec[6] == 'hlr' else dict(r0=spec[2])
+        return O.OSersic(spec[1], flux=spec[3], trunc=spec[4], flux_untruncated=spec[5], **size)
     if kind == 'moffat':
         return O.OMoffat(spec[1], fwhm=spec[2], flux=spec[3])
     if kind == 'kolmogorov':

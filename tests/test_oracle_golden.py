@@ -150,3 +150,30 @@ def test_irfft_flags_match_reference(Nx, Ny, si, so):
     out = np.fft.irfft2(K, s=(Ny, Nx))
     ref = STD['irfft_out_%d_%d_%d%d' % (Nx, Ny, si, so)]
     assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+TRUNC = np.load(specs.HERE + '/reference_trunc.npz')
+
+
+@pytest.mark.parametrize('case', MG.TRUNC_CASES, ids=[c[0] for c in MG.TRUNC_CASES])
+def test_truncated_sersic_draw_matches_reference(case):
+    """Truncated Sersic profiles: the oracle's exact truncated Hankel transform against the
+    reference's adaptive Gauss-Kronrod-Patterson one (relerr 1e-6) -- they agree to the
+    reference's integration error, a few 1e-8 of the peak."""
+    name, spec, nx, ny, scale, dt, off = case
+    arr, flux, N, Nk = O.draw_image(specs.oracle_profile(spec), nx, ny, scale, off)
+    ref = TRUNC['draw_' + name]
+    peak = np.abs(ref).max()
+    assert np.abs(arr.astype(ref.dtype) - ref).max() <= 2e-7 * peak
+    assert abs(flux - float(TRUNC['draw_' + name + '_flux'])) <= 2e-7 * abs(flux)
+
+
+def test_truncated_sersic_sizes_match_reference():
+    for k, spec in enumerate(MG.TRUNC_SIZE_CASES):
+        o = specs.oracle_profile(spec)
+        s, m = o.stepk_maxk()
+        sk, mk = TRUNC['sizes'][k]
+        assert abs(s - sk) <= 1e-9 * sk, spec
+        assert abs(m - mk) <= 1e-6 * mk, spec
+        assert abs(o.r0 - TRUNC['scale_radius'][k]) <= 1e-9 * o.r0, spec
+        assert abs(o.flux - TRUNC['flux'][k]) <= 1e-10 * o.flux, spec
