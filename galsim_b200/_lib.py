@@ -91,6 +91,9 @@ def lib():
             'gsb_sersic_tables_build_ex': (i, [vp, vp, vp, i, ctypes.POINTER(GSParamsC), i, vp]),
             'gsb_sersic_tables_info': (i, [vp, vp, i, vp]),
             'gsb_sersic_truncation': (i, [i, vp, vp, vp]),
+            'gsb_moffat_tables_build': (i, [vp, vp, vp, i, vp, vp]),
+            'gsb_moffat_tables_info': (i, [vp, vp, i, vp]),
+            'gsb_moffat_scale_radius': (i, [i, vp, vp, vp]),
             'gsb_images_build': (i, [vp, i, vp, vp, ctypes.POINTER(GSParamsC), vp]),
             'gsb_images_info': (i, [vp, vp, i, vp]),
             'gsb_add_noise': (i, [i, vp, vp, i, i, vp, i, vp, vp, vp]),
@@ -201,6 +204,23 @@ def sersic_truncation(n, size, trunc, size_is_hlr, flux_untruncated):
     return out[:, 0], out[:, 1]
 
 
+MOFFAT_HEADER = 8
+(MH_BETA, MH_TRUNC, MH_FLUXFACTOR, MH_DK, MH_NUSED, MH_KSQMAX, MH_MAXK, MH_STATUS) = range(8)
+
+
+def moffat_scale_radius(beta, hlr, trunc):
+    """Scale radius per Moffat profile from its half-light radius (trunc 0: untruncated), by
+    FP64 root finding on the device for truncated profiles (gsb_moffat_scale_radius)."""
+    beta, hlr, trunc = np.broadcast_arrays(np.atleast_1d(np.asarray(beta, float)), np.asarray(hlr, float),
+                                           np.asarray(trunc, float))
+    inp = np.ascontiguousarray(np.stack([beta, hlr, trunc], -1), dtype=np.float64)
+    out = np.zeros(len(beta))
+    Device.torch_device()
+    check(lib().gsb_moffat_scale_radius(len(beta), inp.ctypes.data_as(ctypes.c_void_p),
+                                        out.ctypes.data_as(ctypes.c_void_p), Device.stream()))
+    return out
+
+
 def set_draw_variant(variant):
     """0 automatic (autotuned), 1 fused kernel only, 2 split kernels where N >= 192."""
     check(lib().gsb_draw_set_variant(int(variant)))
@@ -255,6 +275,23 @@ class Tables(object):
         self.count = len(n)
         self.with_dn = with_dn
         self.generation = getattr(self, 'generation', 0) + 1
+
+    def build_moffat(self, beta, trunc_over_rd, gsp):
+        """Build one truncated-Moffat table per (beta, trunc / scale radius) pair."""
+        b = np.ascontiguousarray(beta, dtype=np.float64)
+        t = np.ascontiguousarray(trunc_over_rd, dtype=np.float64)
+        check(lib().gsb_moffat_tables_build(self.handle, b.ctypes.data_as(ctypes.c_void_p),
+                                            t.ctypes.data_as(ctypes.c_void_p), len(b),
+                                            ctypes.byref(gsparams_c(gsp)), Device.stream()))
+        self.moffat_count = len(b)
+        self.generation = getattr(self, 'generation', 0) + 1
+
+    def moffat_info(self, count=None):
+        count = self.moffat_count if count is None else count
+        out = np.zeros((count, MOFFAT_HEADER))
+        check(lib().gsb_moffat_tables_info(self.handle, out.ctypes.data_as(ctypes.c_void_p), count,
+                                           Device.stream()))
+        return out
 
     def build_images(self, desc, pixels, gsp):
         """Build the k-images (and stepk / maxk scans) of the InterpolatedImage sources:

@@ -44,6 +44,12 @@ class RecordPlan(object):
                                      use_true_center=use_true_center, precision=precision,
                                      tables=tables)
         self.prog = self.batch_plan.prog
+        for l, t in enumerate(self.prog.bld.leaf_types):
+            if t == _lib.MOFFAT and np.any(self.prog.bld.leaves[l]['p'][:, 2] > 0.):
+                # its table depends on trunc / scale_radius, so the size derivative at fixed
+                # trunc is not the derivative at a fixed table that the adjoint computes
+                from .errors import GalSimNotImplementedError
+                raise GalSimNotImplementedError("gradients of truncated Moffat profiles are not built")
         self.prog.need_dn = True
         self.B = self.prog.B
         self.L = self.prog.L

@@ -11,6 +11,9 @@ namespace gsb {
 
 int ogata_init(DeviceState* st);
 int sersic_truncation(int count, const double* h_in, double* h_out, cudaStream_t stream);
+int moffat_tables_build(gsb_tables* t, const double* h_beta, const double* h_trunc, int count,
+                        const gsb_gsparams* gsp, cudaStream_t stream);
+int moffat_scale_radius(int count, const double* h_in, double* h_out, cudaStream_t stream);
 int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc, int count,
                         const gsb_gsparams* gsp, bool with_dn, cudaStream_t stream);
 int adjoint_grad_count(const gsb_template* tpl);
@@ -159,6 +162,11 @@ int gsb_tables_destroy(gsb_tables* t)
     cudaFree(t->d_dheader);
     cudaFree(t->d_dnode);
     cudaFree(t->d_dval);
+    cudaFree(t->d_mheader);
+    cudaFree(t->d_mnode);
+    cudaFree(t->d_mval);
+    cudaFree(t->d_mk);
+    cudaFree(t->d_mstatus);
     cudaFree(t->d_images);
     cudaFree(t->d_image_info);
     cudaFree(t->d_k64);
@@ -208,6 +216,38 @@ int gsb_sersic_tables_info(const gsb_tables* t, double* h_out, int count, void* 
                                    cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     GSB_CUDA_CHECK(cudaStreamSynchronize((cudaStream_t)stream));
     return GSB_OK;
+}
+
+int gsb_moffat_tables_build(gsb_tables* t, const double* h_beta, const double* h_trunc_over_rd, int count,
+                            const gsb_gsparams* gsp, void* stream)
+{
+    if (!t || !gsp || (count > 0 && (!h_beta || !h_trunc_over_rd))) return set_error(GSB_ERR_INVALID, "null argument");
+    if (count < 0) return set_error(GSB_ERR_INVALID, "negative count");
+    return moffat_tables_build(t, h_beta, h_trunc_over_rd, count, gsp, (cudaStream_t)stream);
+}
+
+int gsb_moffat_tables_info(const gsb_tables* t, double* h_out, int count, void* stream)
+{
+    if (!t || !h_out) return set_error(GSB_ERR_INVALID, "null argument");
+    if (count < 0 || count > t->moffat_count) return set_error(GSB_ERR_INVALID, "count exceeds built slots");
+    if (count == 0) return GSB_OK;
+    GSB_CUDA_CHECK(cudaMemcpyAsync(h_out, t->d_mheader, sizeof(double) * kMoffatHeader * count,
+                                   cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    GSB_CUDA_CHECK(cudaStreamSynchronize((cudaStream_t)stream));
+    return GSB_OK;
+}
+
+int gsb_moffat_scale_radius(int count, const double* h_in, double* h_out, void* stream)
+{
+    if (count < 0 || (count > 0 && (!h_in || !h_out))) return set_error(GSB_ERR_INVALID, "bad arguments");
+    for (int i = 0; i < count; ++i) {
+        const double beta = h_in[3 * i], hlr = h_in[3 * i + 1], trunc = h_in[3 * i + 2];
+        if (!(hlr > 0.) || !(trunc >= 0.) || !std::isfinite(beta))
+            return set_error(GSB_ERR_INVALID, "half_light_radius must be > 0 and trunc >= 0");
+        if (trunc > 0. && !(trunc > 1.4142135623730951 * hlr))
+            return set_error(GSB_ERR_INVALID, "Moffat truncation radius must be > sqrt(2) * half_light_radius.");
+    }
+    return moffat_scale_radius(count, h_in, h_out, (cudaStream_t)stream);
 }
 
 int gsb_prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gsp,

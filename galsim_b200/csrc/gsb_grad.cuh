@@ -175,7 +175,13 @@ __device__ inline LeafD<T> leaf_grad(const LeafParams& L, const SersicTableView*
         const T knorm = T(L.d[1]);
         T K, dKx;   // K(k) and K'(k) / k
         const T e = exp(-k);
-        if (mode == 1) { K = e; dKx = k > T(0) ? -e / k : T(0); }
+        if (mode == 4) {
+            // truncated: the spline in k^2, K'(k) / k = 2 dK / d(k^2) (the table held fixed)
+            const double4* nd = reinterpret_cast<const double4*>(__double_as_longlong(L.d[6]));
+            T dv;
+            K = moffat_trunc_kvalue<T>(nd, int(L.d[5]), T(L.d[3]), T(L.d[4]), q * rD * rD, &dv);
+            dKx = T(2) * dv;
+        } else if (mode == 1) { K = e; dKx = k > T(0) ? -e / k : T(0); }
         else if (mode == 2) { K = e * (T(1) + k); dKx = -e; }
         else if (mode == 3) { K = e * (T(3) + (T(3) + k) * k) * T(1. / 3.); dKx = -e * (T(1) + k) * T(1. / 3.); }
         else { K = moffat_kv<T>(T(L.d[3]), T(L.d[4]), k); dKx = moffat_dkv_over_x<T>(T(L.d[3]), T(L.d[4]), k); }

@@ -55,6 +55,14 @@ enum {
     kSersicHeader = 18
 };
 
+// Truncated Moffat FT table slot (SBMoffat::setupFT, src/SBMoffat.cpp:565-625): header plus
+// nodes (k^2, value, y2, 0) of a natural cubic spline in k^2 on the grid k = 0, dk, 2 dk, ...
+// (k in units of 1 / rD; the grid is the reference's running sum k += dk).
+enum {
+    kMH_BETA = 0, kMH_TRUNC, kMH_FLUXFACTOR, kMH_DK, kMH_NUSED, kMH_KSQMAX, kMH_MAXK, kMH_STATUS,
+    kMoffatHeader = 8
+};
+
 // Per-slot derivative header (doubles) of tables built with n-derivatives: d/dn (at fixed
 // r0) of the low-k coefficients and of the high-k fit, and d ln(r_e / r0) / dn.
 // The table's grid starts at front = ln k_min(n) - 0.001, so its nodes k_i move with n:
@@ -220,6 +228,15 @@ struct gsb_tables {
     double4* d_dnode = nullptr;   // count * stride
     double* d_dval = nullptr;     // scratch: count * stride d/dn Hankel values
     size_t cap_dn_slots = 0, cap_dn_nodes = 0;
+    // truncated Moffat slots (gsb_moffat_tables_build)
+    int moffat_count = 0;
+    int moffat_stride = 0;            // nodes per slot
+    double* d_mheader = nullptr;      // moffat_count * kMoffatHeader
+    double4* d_mnode = nullptr;       // moffat_count * moffat_stride
+    double* d_mval = nullptr;         // scratch: Hankel values
+    double* d_mk = nullptr;           // the k grid (moffat_stride)
+    int* d_mstatus = nullptr;
+    size_t cap_mslots = 0, cap_mnodes = 0, cap_mk = 0;
     // InterpolatedImage slots (gsb_images_build)
     int n_images = 0;
     gsb::ImageSlot* d_images = nullptr;   // n_images slot headers

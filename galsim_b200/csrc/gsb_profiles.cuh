@@ -124,6 +124,34 @@ __device__ inline T sersic_kvalue(const SersicTableView& tb, T ksq)
     }
 }
 
+// Truncated Moffat FT at ksq = (k rD)^2 (kV_trunc, src/SBMoffat.cpp:339-345): 0 beyond the
+// table's last argument, else its natural cubic spline in k^2 (TSpline, src/Table.cpp:553-686)
+// over nodes (k_i^2, v_i, y2_i), k_i = i dk up to rounding of the running sum.  The interval is
+// the one the reference's lookup finds (k_{i-1}^2 <= ksq <= k_i^2): first guessed from
+// sqrt(ksq) / dk, then moved to the node that brackets ksq.  The offsets from the nodes are
+// taken in k (x_i - ksq = (k_i - k)(k_i + k)), which keeps their FP32 rounding relative to
+// k rather than to k^2.  *dv (when given) receives the spline's derivative d v / d ksq.
+template <typename T>
+__device__ inline T moffat_trunc_kvalue(const double4* nd, int n, T dk, T ksq_max, T ksq, T* dv = nullptr)
+{
+    if (ksq > ksq_max) { if (dv) *dv = T(0); return T(0); }
+    const T k = sqrt(ksq);
+    int i = int(ceil(k / dk));
+    if (i > n - 1) i = n - 1;
+    if (i < 1) i = 1;
+    for (int it = 0; it < 2 && i < n - 1 && ksq > T(nd[i].x); ++it) ++i;
+    for (int it = 0; it < 2 && i > 1 && ksq < T(nd[i - 1].x); ++it) --i;
+    const double4 n0 = nd[i - 1];
+    const double4 n1 = nd[i];
+    const T h = T(n1.x - n0.x);
+    const T k0 = T(sqrt(n0.x)), k1 = T(sqrt(n1.x));
+    const T aa = (k1 - k) * (k1 + k) / h;      // (x_i - ksq) / h
+    const T bb = (k - k0) * (k + k0) / h;      // (ksq - x_{i-1}) / h
+    const T y0 = T(n0.y), y1 = T(n1.y), z0 = T(n0.z), z1 = T(n1.z);
+    if (dv) *dv = (y1 - y0) / h + (-(T(3) * aa * aa - T(1)) * z0 + (T(3) * bb * bb - T(1)) * z1) * h * T(1. / 6.);
+    return aa * y0 + bb * y1 + ((aa * aa * aa - aa) * z0 + (bb * bb * bb - bb) * z1) * (h * h) * T(1. / 6.);
+}
+
 // c_nu x^nu K_nu(x) normalised to 1 at x = 0, by the trapezoid rule on
 // K_nu(x) = int_0^inf exp(-x cosh t) cosh(nu t) dt (DLMF 10.32.9).
 template <typename T>
@@ -199,9 +227,14 @@ __device__ inline T leaf_kvalue(const LeafParams& L, const SersicTableView* tabl
       }
       case GSB_MOFFAT: {
         const T rD = T(L.d[0]);
-        const T k = sqrt(kxp * kxp + kyp * kyp) * rD;
         const int mode = int(L.d[2]);
         const T knorm = T(L.d[1]);
+        if (mode == 4) {
+            const double4* nd = reinterpret_cast<const double4*>(__double_as_longlong(L.d[6]));
+            return knorm * moffat_trunc_kvalue<T>(nd, int(L.d[5]), T(L.d[3]), T(L.d[4]),
+                                                  (kxp * kxp + kyp * kyp) * rD * rD);
+        }
+        const T k = sqrt(kxp * kxp + kyp * kyp) * rD;
         if (mode == 1) return knorm * exp(-k);
         if (mode == 2) return knorm * exp(-k) * (T(1) + k);
         if (mode == 3) return knorm * exp(-k) * (T(3) + (T(3) + k) * k) * T(1. / 3.);

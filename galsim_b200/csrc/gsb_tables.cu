@@ -255,14 +255,15 @@ __device__ double2 warp_hankel_pair(const OgataTables& og, double invn, double l
     return make_double2(a[1], a[3]);
 }
 
-// Truncated Hankel transform of the Sersic profile (math::hankel_trunc, src/math/Hankel.cpp:
-// 249-255, as SersicInfo::buildFT calls it for trunc > 0, src/SBSersic.cpp:453-457):
-//   I(k) = int_0^t r exp(-r^(1/n)) J0(k r) dr,   t = trunc / r0.
+// Truncated Hankel transform (math::hankel_trunc, src/math/Hankel.cpp:249-255) of a radial
+// profile f, as SersicInfo::buildFT (src/SBSersic.cpp:453-457) and SBMoffat::setupFT
+// (src/SBMoffat.cpp:587-592) call it:
+//   I(k) = int_0^t r f(r) J0(k r) dr,   f = exp(-r^(1/n)) (Sersic), (1 + r^2)^-beta (Moffat).
 // The reference integrates adaptively (Gauss-Kronrod-Patterson to relerr 1e-6); here the
 // integral is taken to near FP64 precision by 16-point Gauss-Legendre on panels between
 // consecutive zeros of J0(k r) (the first interval graded toward r = 0 in 48 halvings, where
-// r^(1/n) has its cusp), so the two agree to the reference's integration error.  One warp per
-// node: lanes 0-15 and 16-31 take two panels at a time, one Legendre node each.
+// the Sersic r^(1/n) has its cusp), so the two agree to the reference's integration error.
+// One warp per node: lanes 0-15 and 16-31 take two panels at a time, one Legendre node each.
 __device__ inline void gauss_legendre16(int q, double* x, double* w)
 {
     // node q of P_16 by Newton's method from the Tricomi estimate, weight 2 / ((1 - x^2) P'^2)
@@ -281,7 +282,17 @@ __device__ inline void gauss_legendre16(int q, double* x, double* w)
     *w = 2. / ((1. - z * z) * dp * dp);
 }
 
-__device__ double warp_hankel_trunc(const OgataTables& og, double invn, double k, double t, int* status)
+struct SersicRadial {
+    double invn;
+    __device__ double operator()(double r) const { return exp(-pow(r, invn)); }
+};
+struct MoffatRadial {
+    double beta;
+    __device__ double operator()(double r) const { return pow(1. + r * r, -beta); }
+};
+
+template <class F>
+__device__ double warp_hankel_trunc(const OgataTables& og, const F& f, double k, double t, int* status)
 {
     const int lane = threadIdx.x & 31, half = lane >> 4;
     double xq, wq;
@@ -310,7 +321,7 @@ __device__ double warp_hankel_trunc(const OgataTables& og, double invn, double k
         if (!__any_sync(0xffffffffu, live)) break;
         if (live) {
             const double h = 0.5 * (b - a), r = a + h * (1. + xq);
-            acc += wq * h * r * exp(-pow(r, invn)) * j0(k * r);
+            acc += wq * h * r * f(r) * j0(k * r);
         }
     }
     return warp_total(acc);
@@ -520,7 +531,7 @@ __global__ void __launch_bounds__(256) sersic_trunc_nodes_kernel(const double* h
     const double k = exp(H[kSH_FRONT] + i * H[kSH_DLOGK]);
     const double hankel_norm = H[kSH_FLUXFRAC] * n * tgamma(2. * n);
     int st = 0;
-    const double v = warp_hankel_trunc(og, 1. / n, k, H[kSH_TRUNC], &st) / hankel_norm;
+    const double v = warp_hankel_trunc(og, SersicRadial{1. / n}, k, H[kSH_TRUNC], &st) / hankel_norm;
     if ((threadIdx.x & 31) == 0) {
         vals[s * stride + i] = v;
         if (st) atomicOr(status_out, 1);
@@ -774,6 +785,120 @@ __global__ void __launch_bounds__(32) sersic_finalize_kernel(double* header, int
     H[kSH_MAXK] = maxk;
 }
 
+// Truncated Moffat FT tables (SBMoffat::setupFT, src/SBMoffat.cpp:565-625).  Per slot
+// (beta, t = trunc / rD): the values
+//     v(k) = 2 (beta - 1) / F  int_0^t r (1 + r^2)^-beta J0(k r) dr,  F = 1 - (1 + t^2)^(1 - beta)
+// on the reference's grid k = 0, dk, 2 dk, ... (its running sum, k < 50), one warp per node for
+// all candidate nodes at once; then, per slot, the reference's stopping rule (5 nodes in a row
+// with |v| <= kvalue_accuracy end the table), maxk (the last node with |v| > maxk_threshold,
+// refined linearly toward the next node) and the natural cubic spline in k^2.
+__global__ void moffat_setup_kernel(int count, double* header)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    double* H = header + (size_t)s * kMoffatHeader;
+    H[kMH_FLUXFACTOR] = 1. - pow(1. + H[kMH_TRUNC] * H[kMH_TRUNC], 1. - H[kMH_BETA]);
+}
+
+__global__ void __launch_bounds__(256) moffat_nodes_kernel(const double* header, int count, const double* kgrid,
+                                                           int ncand, const __grid_constant__ OgataTables og,
+                                                           double* vals, int* status_out)
+{
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long s = warp / ncand;
+    const int i = int(warp % ncand);
+    if (s >= count) return;
+    const double* H = header + s * kMoffatHeader;
+    const double b = H[kMH_BETA];
+    const double prefactor = 2. * (b - 1.) / H[kMH_FLUXFACTOR];
+    int st = 0;
+    const double v = prefactor * warp_hankel_trunc(og, MoffatRadial{b}, kgrid[i], H[kMH_TRUNC], &st);
+    if ((threadIdx.x & 31) == 0) {
+        vals[s * ncand + i] = v;
+        if (st) atomicOr(status_out, 1);
+    }
+}
+
+// One warp per slot; dynamic shared memory 4 * ncand doubles.
+__global__ void __launch_bounds__(32) moffat_finalize_kernel(double* header, int count, const double* kgrid,
+                                                             int ncand, gsb_gsparams gsp, const double* vals,
+                                                             double4* nodes)
+{
+    extern __shared__ double msm[];
+    const int s = blockIdx.x;
+    const int lane = threadIdx.x;
+    if (s >= count) return;
+    double* xs = msm;
+    double* ys = xs + ncand;
+    double* zs = ys + ncand;
+    double* cs = zs + ncand;
+    const double* v = vals + (size_t)s * ncand;
+    for (int i = lane; i < ncand; i += 32) {
+        xs[i] = kgrid[i] * kgrid[i];
+        ys[i] = v[i];
+    }
+    __syncwarp();
+    __shared__ int n_used;
+    if (lane == 0) {
+        double* H = header + (size_t)s * kMoffatHeader;
+        // the reference's loop over k: maxk bookkeeping and the stopping rule
+        int im = 0, nbelow = 0, N = ncand;
+        for (int i = 0; i < ncand; ++i) {
+            const double a = fabs(ys[i]);
+            if (a > gsp.maxk_threshold) im = i;
+            nbelow = a > gsp.kvalue_accuracy ? 0 : nbelow + 1;
+            if (nbelow == 5) { N = i + 1; break; }
+        }
+        double maxk = kgrid[im];
+        // the refinement between k1 = maxk and k2 = maxk + dk (both tabulated nodes when k2 < 50,
+        // where the spline returns the node values)
+        const double k2 = maxk + H[kMH_DK];
+        if (k2 < 50. && im + 1 < N) {
+            const double f1 = fabs(ys[im]), f2 = fabs(ys[im + 1]);
+            maxk = (maxk * (f2 - gsp.maxk_threshold) + k2 * (gsp.maxk_threshold - f1)) / (f2 - f1);
+        }
+        if (N >= 2) natural_spline(xs, ys, zs, cs, N);
+        H[kMH_NUSED] = N;
+        H[kMH_KSQMAX] = xs[N - 1];
+        H[kMH_MAXK] = maxk;
+        if (N < 2) H[kMH_STATUS] = 5;
+        n_used = N;
+    }
+    __syncwarp();
+    const int N = n_used;
+    double4* nd = nodes + (size_t)s * ncand;
+    for (int i = lane; i < N; i += 32) nd[i] = make_double4(xs[i], ys[i], zs[i], 0.);
+}
+
+// Scale radius of truncated Moffat profiles from the half-light radius
+// (MoffatCalculateScaleRadiusFromHLR, src/SBMoffat.cpp:103-160): Brent on
+//     2 f(re) - f(rm) = 0,   f(R) = 1 - (1 + R^2 / rd^2)^(1 - beta),
+// bracketed upward from the untruncated radius r1 and 2 r1.
+struct MoffatScaleRadiusFunc {
+    double re, rm, beta;
+    __device__ double operator()(double rd) const
+    {
+        const double fre = 1. - pow(1. + (re * re) / (rd * rd), 1. - beta);
+        const double frm = 1. - pow(1. + (rm * rm) / (rd * rd), 1. - beta);
+        return 2. * fre - frm;
+    }
+};
+
+__global__ void moffat_scale_radius_kernel(const double* in, int count, double* out, int* status)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const double beta = in[3 * i], re = in[3 * i + 1], rm = in[3 * i + 2];
+    const double r1 = re / sqrt(pow(0.5, 1. / (1. - beta)) - 1.);
+    // beta <= 1 has no finite untruncated radius to start from: the reference's bracketing
+    // fails there too
+    if (!(r1 > 0.) || !isfinite(r1)) { atomicOr(status, 1); out[i] = 0.; return; }
+    if (rm == 0.) { out[i] = r1; return; }
+    const RootResult r = solve_bracket_upper(MoffatScaleRadiusFunc{re, rm, beta}, r1, 2. * r1);
+    if (!r.ok) { atomicOr(status, 1); out[i] = 0.; return; }
+    out[i] = r.x;
+}
+
 // KolmogorovInfo: x-space radial profile by Hankel transform of exp(-k^{5/3}) at
 // r = exp(-3 + i dlogr); only the last tabulated point matters for stepk.
 __global__ void kolmogorov_nodes_kernel(int ncand, double dlogr, gsb_gsparams gsp, const __grid_constant__ OgataTables og,
@@ -826,6 +951,12 @@ struct MoffatKV2 {
     }
 };
 
+struct MoffatRefs {
+    const double* header;
+    const double4* node;
+    int count, stride;
+};
+
 struct ImageRefs {
     const ImageSlot* slots;
     const double* info;
@@ -835,7 +966,7 @@ struct ImageRefs {
 };
 
 __global__ void prepare_leaves_kernel(const __grid_constant__ gsb_template tpl, int n_stamps, gsb_gsparams gsp,
-                                      gsb_leaf* leaves, const double* sersic_header,
+                                      gsb_leaf* leaves, const double* sersic_header, MoffatRefs moffat,
                                       double kolm_stepk, ImageRefs images, double* info, int* status_out)
 {
     const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -884,34 +1015,55 @@ __global__ void prepare_leaves_kernel(const __grid_constant__ gsb_template tpl, 
         break;
       }
       case GSB_MOFFAT: {
-        // SBMoffat.cpp:163-244 (kV selection), :481-549 (maxK, stepK); untruncated
-        const double beta = L.p[0], rD = L.p[1];
-        const double kacc = gsp.kvalue_accuracy;
-        int mode = 0;
-        double nu = beta - 1., knorm = L.flux;
-        if (fabs(beta - 1.5) < kacc) { mode = 1; }
-        else if (fabs(beta - 2.) < kacc) { nu = 1.; }
-        else if (fabs(beta - 2.5) < kacc) { mode = 2; }
-        else if (fabs(beta - 3.) < kacc) { nu = 2.; }
-        else if (fabs(beta - 3.5) < kacc) { mode = 3; }
-        else if (fabs(beta - 4.) < kacc) { nu = 3.; }
+        // SBMoffat.cpp:163-244 (kV selection), :481-549 (maxK, stepK)
+        const double beta = L.p[0], rD = L.p[1], trunc = L.p[2];
+        double maxRrD, flux_factor = 1.;
         L.d[0] = rD;
-        L.d[1] = knorm;
-        L.d[2] = mode;
-        L.d[3] = nu;
-        L.d[4] = (1. - nu) * log(2.) - lgamma(nu);
-        MoffatKV2 f{mode, nu, gsp.maxk_threshold};
-        RootResult r = solve_bracket_upper(f, 0., 100.);
-        if (!r.ok) atomicOr(status_out, 4);
-        maxk = sqrt(r.x) / rD;
-        const double maxRrD = sqrt(pow(gsp.xvalue_accuracy, 1. / (1. - beta)) - 1.);
+        L.d[1] = L.flux;
+        if (trunc > 0.) {
+            // the FT from the slot's spline in k^2 (kV_trunc, SBMoffat.cpp:339-345); the slot
+            // must have been built for this (beta, trunc / rD)
+            const int slot = L.table;
+            if (slot < 0 || slot >= moffat.count) { atomicOr(status_out, 64); break; }
+            const double* H = moffat.header + (size_t)slot * kMoffatHeader;
+            if (fabs(H[kMH_BETA] - beta) > 1e-12 * fabs(beta) ||
+                fabs(H[kMH_TRUNC] - trunc / rD) > 1e-12 * (trunc / rD)) { atomicOr(status_out, 128); break; }
+            if (H[kMH_STATUS] != 0.) atomicOr(status_out, 256);
+            maxRrD = trunc / rD;
+            flux_factor = H[kMH_FLUXFACTOR];
+            L.d[2] = 4;
+            L.d[3] = H[kMH_DK];
+            L.d[4] = H[kMH_KSQMAX];
+            L.d[5] = H[kMH_NUSED];
+            L.d[6] = __longlong_as_double((long long)(moffat.node + (size_t)slot * moffat.stride));
+            maxk = H[kMH_MAXK] / rD;
+        } else {
+            const double kacc = gsp.kvalue_accuracy;
+            int mode = 0;
+            double nu = beta - 1.;
+            if (fabs(beta - 1.5) < kacc) { mode = 1; }
+            else if (fabs(beta - 2.) < kacc) { nu = 1.; }
+            else if (fabs(beta - 2.5) < kacc) { mode = 2; }
+            else if (fabs(beta - 3.) < kacc) { nu = 2.; }
+            else if (fabs(beta - 3.5) < kacc) { mode = 3; }
+            else if (fabs(beta - 4.) < kacc) { nu = 3.; }
+            L.d[2] = mode;
+            L.d[3] = nu;
+            L.d[4] = (1. - nu) * log(2.) - lgamma(nu);
+            MoffatKV2 f{mode, nu, gsp.maxk_threshold};
+            RootResult r = solve_bracket_upper(f, 0., 100.);
+            if (!r.ok) atomicOr(status_out, 4);
+            maxk = sqrt(r.x) / rD;
+            maxRrD = sqrt(pow(gsp.xvalue_accuracy, 1. / (1. - beta)) - 1.);
+        }
         const double maxR = maxRrD * rD;
         if (beta <= 1.1) {
             stepk = kPi / maxR;
         } else {
             double R = pow(gsp.folding_threshold, 0.5 / (1. - beta)) * rD;
             if (R > maxR) R = maxR;
-            const double hlr = rD * sqrt(pow(1. - 0.5, 1. / (1. - beta)) - 1.);
+            // getHalfLightRadius (SBMoffat.cpp:247-258), of the truncated profile when truncated
+            const double hlr = rD * sqrt(pow(1. - 0.5 * flux_factor, 1. / (1. - beta)) - 1.);
             R = fmax(R, gsp.stepk_minimum_hlr * hlr);
             stepk = kPi / R;
         }
@@ -1176,6 +1328,104 @@ int sersic_truncation(int count, const double* h_in, double* h_out, cudaStream_t
     return GSB_OK;
 }
 
+// The reference's k grid of SBMoffat::setupFT: k = 0, dk, 2 dk, ... as a running sum, k < 50.
+static std::vector<double> moffat_kgrid(const gsb_gsparams* gsp)
+{
+    const double dk = gsp->table_spacing * std::sqrt(std::sqrt(gsp->kvalue_accuracy / 10.));
+    std::vector<double> k;
+    for (double x = 0.; x < 50.; x += dk) k.push_back(x);
+    return k;
+}
+
+int moffat_tables_build(gsb_tables* t, const double* h_beta, const double* h_trunc, int count,
+                        const gsb_gsparams* gsp, cudaStream_t stream)
+{
+    DeviceState* st = device_state();
+    if (!st->ready) return set_error(GSB_ERR_INVALID, "gsb_init has not been called");
+    for (int i = 0; i < count; ++i) {
+        if (!(h_trunc[i] > 0.) || !std::isfinite(h_trunc[i]))
+            return set_error(GSB_ERR_INVALID, "Moffat table needs trunc / scale_radius > 0");
+        if (!(h_beta[i] > 0.) || h_beta[i] == 1. || !std::isfinite(h_beta[i]))
+            return set_error(GSB_ERR_INVALID, "truncated Moffat beta must be > 0 and != 1 (at beta = 1 the "
+                                              "flux normalisation 2 (beta - 1) / (1 - (1 + t^2)^(1 - beta)) is 0/0)");
+    }
+    if (count <= 0) { t->moffat_count = 0; return GSB_OK; }
+    if (!(gsp->kvalue_accuracy > 0.) || !(gsp->table_spacing > 0.))
+        return set_error(GSB_ERR_INVALID, "kvalue_accuracy and table_spacing must be > 0");
+    const std::vector<double> kg = moffat_kgrid(gsp);
+    const int ncand = int(kg.size());
+    const size_t fsm = sizeof(double) * 4 * (size_t)ncand;
+    if (fsm > 227 * 1024)
+        return set_error(GSB_ERR_UNSUPPORTED, "truncated Moffat table too long for this kvalue_accuracy / "
+                                              "table_spacing (more than 7264 nodes)");
+    if ((size_t)count > t->cap_mslots || (size_t)count * ncand > t->cap_mnodes || (size_t)ncand > t->cap_mk) {
+        cudaFree(t->d_mheader); cudaFree(t->d_mnode); cudaFree(t->d_mval); cudaFree(t->d_mk); cudaFree(t->d_mstatus);
+        t->d_mheader = nullptr; t->d_mnode = nullptr; t->d_mval = nullptr; t->d_mk = nullptr; t->d_mstatus = nullptr;
+        t->cap_mslots = std::max<size_t>(count, t->cap_mslots);
+        t->cap_mnodes = std::max<size_t>((size_t)count * ncand, t->cap_mnodes);
+        t->cap_mk = std::max<size_t>(ncand, t->cap_mk);
+        GSB_CUDA_CHECK(cudaMalloc(&t->d_mheader, sizeof(double) * kMoffatHeader * t->cap_mslots));
+        GSB_CUDA_CHECK(cudaMalloc(&t->d_mnode, sizeof(double4) * t->cap_mnodes));
+        GSB_CUDA_CHECK(cudaMalloc(&t->d_mval, sizeof(double) * t->cap_mnodes));
+        GSB_CUDA_CHECK(cudaMalloc(&t->d_mk, sizeof(double) * t->cap_mk));
+        GSB_CUDA_CHECK(cudaMalloc(&t->d_mstatus, sizeof(int)));
+    }
+    t->moffat_count = count;
+    t->moffat_stride = ncand;
+    // slot headers: (beta, trunc / rD, dk) from the host, the rest written on the device
+    std::vector<double> hh((size_t)kMoffatHeader * count, 0.);
+    for (int i = 0; i < count; ++i) {
+        hh[(size_t)i * kMoffatHeader + kMH_BETA] = h_beta[i];
+        hh[(size_t)i * kMoffatHeader + kMH_TRUNC] = h_trunc[i];
+        hh[(size_t)i * kMoffatHeader + kMH_DK] = ncand > 1 ? kg[1] : 0.;
+    }
+    GSB_CUDA_CHECK(cudaMemcpyAsync(t->d_mheader, hh.data(), sizeof(double) * hh.size(), cudaMemcpyHostToDevice,
+                                   stream));
+    GSB_CUDA_CHECK(cudaMemcpyAsync(t->d_mk, kg.data(), sizeof(double) * ncand, cudaMemcpyHostToDevice, stream));
+    GSB_CUDA_CHECK(cudaMemsetAsync(t->d_mstatus, 0, sizeof(int), stream));
+    moffat_setup_kernel<<<(count + 127) / 128, 128, 0, stream>>>(count, t->d_mheader);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    const int threads = 256;
+    const long long nwarps = (long long)count * ncand;
+    moffat_nodes_kernel<<<(unsigned)((nwarps * 32 + threads - 1) / threads), threads, 0, stream>>>(
+        t->d_mheader, count, t->d_mk, ncand, st->og, t->d_mval, t->d_mstatus);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    if (fsm > 48 * 1024)
+        GSB_CUDA_CHECK(cudaFuncSetAttribute(moffat_finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            int(fsm)));
+    moffat_finalize_kernel<<<count, 32, fsm, stream>>>(t->d_mheader, count, t->d_mk, ncand, *gsp, t->d_mval,
+                                                       t->d_mnode);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    int h_status = 0;
+    GSB_CUDA_CHECK(cudaMemcpyAsync(&h_status, t->d_mstatus, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    GSB_CUDA_CHECK(cudaStreamSynchronize(stream));
+    if (h_status) return set_error(GSB_ERR_NUMERIC, "truncated Moffat Hankel transform ran out of J0 zeros");
+    return GSB_OK;
+}
+
+int moffat_scale_radius(int count, const double* h_in, double* h_out, cudaStream_t stream)
+{
+    if (count <= 0) return GSB_OK;
+    double *d_in = nullptr, *d_out = nullptr;
+    int* d_status = nullptr;
+    GSB_CUDA_CHECK(cudaMallocAsync(&d_in, sizeof(double) * 3 * count, stream));
+    GSB_CUDA_CHECK(cudaMallocAsync(&d_out, sizeof(double) * count, stream));
+    GSB_CUDA_CHECK(cudaMallocAsync(&d_status, sizeof(int), stream));
+    GSB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), stream));
+    GSB_CUDA_CHECK(cudaMemcpyAsync(d_in, h_in, sizeof(double) * 3 * count, cudaMemcpyHostToDevice, stream));
+    moffat_scale_radius_kernel<<<(count + 127) / 128, 128, 0, stream>>>(d_in, count, d_out, d_status);
+    GSB_CUDA_CHECK(cudaGetLastError());
+    int h_status = 0;
+    GSB_CUDA_CHECK(cudaMemcpyAsync(h_out, d_out, sizeof(double) * count, cudaMemcpyDeviceToHost, stream));
+    GSB_CUDA_CHECK(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    GSB_CUDA_CHECK(cudaStreamSynchronize(stream));
+    cudaFreeAsync(d_in, stream);
+    cudaFreeAsync(d_out, stream);
+    cudaFreeAsync(d_status, stream);
+    if (h_status) return set_error(GSB_ERR_NUMERIC, "Solve error: Moffat scale radius root find did not converge");
+    return GSB_OK;
+}
+
 int kolmogorov_stepk(const gsb_gsparams* gsp, cudaStream_t stream, double* out)
 {
     DeviceState* st = device_state();
@@ -1233,6 +1483,8 @@ int prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gs
         return set_error(GSB_ERR_INVALID, "InterpolatedImage leaves need built image slots");
     ImageRefs images{};
     if (t) images = ImageRefs{t->d_images, t->d_image_info, t->d_k64, t->d_k32, t->n_images};
+    MoffatRefs moffat{};
+    if (t) moffat = MoffatRefs{t->d_mheader, t->d_mnode, t->moffat_count, t->moffat_stride};
     double kolm = 0.;
     if (need_kolm) {
         const int rc = kolmogorov_stepk(gsp, stream, &kolm);
@@ -1243,7 +1495,7 @@ int prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gs
     const long long n = (long long)n_stamps * tpl->n_leaves;
     if (n > 0) {
         prepare_leaves_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(
-            *tpl, n_stamps, *gsp, d_leaves, t ? t->d_header : nullptr, kolm, images, d_info, d_status);
+            *tpl, n_stamps, *gsp, d_leaves, t ? t->d_header : nullptr, moffat, kolm, images, d_info, d_status);
         GSB_CUDA_CHECK(cudaGetLastError());
     }
     int h_status = 0;
@@ -1255,6 +1507,10 @@ int prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gs
                                                              "Linear, Cubic, Quintic; k: the same but Delta)");
     if (h_status & 2) return set_error(GSB_ERR_NUMERIC, "Sersic radius root finding failed");
     if (h_status & 4) return set_error(GSB_ERR_NUMERIC, "Moffat maxk root finding failed");
+    if (h_status & 64) return set_error(GSB_ERR_INVALID, "truncated Moffat leaf names no built Moffat table slot");
+    if (h_status & 128) return set_error(GSB_ERR_INVALID, "truncated Moffat leaf's table slot was built for "
+                                                          "another (beta, trunc / scale_radius)");
+    if (h_status & 256) return set_error(GSB_ERR_NUMERIC, "truncated Moffat table is empty");
     return GSB_OK;
 }
 

@@ -203,6 +203,8 @@ class Sersic(_Leaf):
 
     n = property(lambda self: self._n)
     trunc = property(lambda self: self._trunc)
+    # a truncated profile has a hard edge (sersic.py:338-340)
+    _has_hard_edges = property(lambda self: bool(np.any(np.asarray(self._trunc) > 0.)))
 
     def calculateHLRFactor(self):
         """Half-light radius in units of the scale radius (SersicHLR, SBSersic.cpp:660-667),
@@ -247,7 +249,7 @@ class Sersic(_Leaf):
     def __eq__(self, other):
         return self is other or (isinstance(other, Sersic) and _eq(self.n, other.n) and
                                  _eq(self.scale_radius, other.scale_radius) and
-                                 self.trunc == other.trunc and _eq(self.flux, other.flux) and
+                                 _eq(self.trunc, other.trunc) and _eq(self.flux, other.flux) and
                                  self.gsparams == other.gsparams)
 
     def __hash__(self):
@@ -270,34 +272,47 @@ class DeVaucouleurs(Sersic):
 
 
 class Moffat(_Leaf):
-    """(1 + (r/r0)^2)^-beta (moffat.py:76-231).  Untruncated profiles only."""
+    """(1 + (r/r0)^2)^-beta (moffat.py:76-231).  trunc > 0 truncates the profile there
+    (beta <= 1.1 needs it): the FT then comes from an FP64 table of the truncated Hankel
+    transform built on the GPU per (beta, trunc / scale_radius), and a half_light_radius of a
+    truncated profile gives the scale radius by an FP64 root find on the GPU.  A batch may mix
+    truncated and untruncated profiles."""
     _is_axisymmetric = True
     _type = _lib.MOFFAT
 
     def __init__(self, beta, scale_radius=None, half_light_radius=None, fwhm=None, trunc=0.,
                  flux=1., gsparams=None):
         self._beta = _as_param(beta)
-        self._trunc = float(trunc)
+        self._trunc = _as_param(trunc)
         self._flux = _as_param(flux)
         self._gsparams = GSParams.check(gsparams)
-        beta = np.asarray(self._beta)
-        if self._trunc == 0. and np.any(beta <= 1.1):
+        beta = np.asarray(self._beta, float)
+        trunc = np.asarray(self._trunc, float)
+        bb, tt = np.broadcast_arrays(beta, trunc)
+        if np.any((bb <= 1.1) & (tt == 0.)):
             raise GalSimRangeError("Moffat profiles with beta <= 1.1 must be truncated", self._beta, 1.1)
-        if self._trunc < 0.:
+        if np.any(trunc < 0.):
             raise GalSimRangeError("Moffat trunc must be >= 0", self._trunc, 0.)
-        if self._trunc > 0.:
-            from .errors import GalSimNotImplementedError
-            raise GalSimNotImplementedError("truncated Moffat profiles are not built")
         if half_light_radius is not None:
             if scale_radius is not None or fwhm is not None:
                 raise GalSimIncompatibleValuesError(
                     "Only one of scale_radius, half_light_radius, or fwhm may be specified",
                     half_light_radius=half_light_radius, scale_radius=scale_radius, fwhm=fwhm)
             self._hlr = _as_param(half_light_radius)
-            # MoffatCalculateScaleRadiusFromHLR, untruncated (SBMoffat.cpp:103-127)
-            self._r0 = self._hlr / np.sqrt(np.power(0.5, 1. / (1. - self._beta)) - 1.)
-            if np.ndim(self._r0) == 0:
-                self._r0 = float(self._r0)
+            hlr = np.asarray(self._hlr, float)
+            if np.any((trunc > 0.) & (trunc <= math.sqrt(2.) * hlr)):
+                raise GalSimRangeError("Moffat trunc must be > sqrt(2) * half_light_radius.",
+                                       self._trunc, math.sqrt(2.) * hlr)
+            if np.any(trunc > 0.):
+                # MoffatCalculateScaleRadiusFromHLR with rm = trunc (SBMoffat.cpp:128-160)
+                r0 = _lib.moffat_scale_radius(self._beta, self._hlr, self._trunc)
+                scalar = np.ndim(self._beta) == 0 and np.ndim(self._hlr) == 0 and np.ndim(self._trunc) == 0
+                self._r0 = float(r0[0]) if scalar else r0
+            else:
+                # the untruncated case is analytic (SBMoffat.cpp:103-127)
+                self._r0 = self._hlr / np.sqrt(np.power(0.5, 1. / (1. - self._beta)) - 1.)
+                if np.ndim(self._r0) == 0:
+                    self._r0 = float(self._r0)
             self._fwhm = 0.
         elif fwhm is not None:
             if scale_radius is not None:
@@ -318,22 +333,35 @@ class Moffat(_Leaf):
             raise GalSimIncompatibleValuesError(
                 "One of scale_radius, half_light_radius, or fwhm must be specified",
                 half_light_radius=half_light_radius, scale_radius=scale_radius, fwhm=fwhm)
-        self._batch = _plen(self._beta, self._r0, self._flux)
+        self._batch = _plen(self._beta, self._r0, self._flux, self._trunc)
 
     beta = property(lambda self: self._beta)
     scale_radius = property(lambda self: self._r0)
     trunc = property(lambda self: self._trunc)
+    # a truncated profile has a hard edge (moffat.py:202-204)
+    _has_hard_edges = property(lambda self: bool(np.any(np.asarray(self._trunc) > 0.)))
 
     @property
     def half_light_radius(self):
-        return self._r0 * np.sqrt(np.power(0.5, 1. / (1. - np.asarray(self._beta))) - 1.)
+        """getHalfLightRadius (SBMoffat.cpp:246-249): rD sqrt((1 - F/2)^(1/(1-beta)) - 1) with
+        F the flux fraction factor 1 - (1 + (trunc/rD)^2)^(1-beta) (1 untruncated); the given
+        value when the profile was made from its half-light radius (moffat.py:144-150)."""
+        if not (np.ndim(self._hlr) == 0 and self._hlr == 0.):
+            return self._hlr
+        beta = np.asarray(self._beta, float)
+        rd = np.asarray(self._r0, float)
+        t = np.asarray(self._trunc, float)
+        with np.errstate(divide='ignore', invalid='ignore'):
+            ff = np.where(t > 0., 1. - np.power(1. + (t / rd) ** 2, 1. - beta), 1.)
+            hlr = rd * np.sqrt(np.power(1. - 0.5 * ff, 1. / (1. - beta)) - 1.)
+        return float(hlr) if np.ndim(hlr) == 0 else hlr
 
     @property
     def fwhm(self):
         return self._r0 * (2. * np.sqrt(2. ** (1. / np.asarray(self._beta)) - 1.))
 
     def _params(self):
-        return (self._beta, self._r0, 0.)
+        return (self._beta, self._r0, self._trunc)
 
     def withFlux(self, flux):
         return Moffat(beta=self.beta, scale_radius=self.scale_radius, trunc=self.trunc, flux=flux,
@@ -342,11 +370,11 @@ class Moffat(_Leaf):
     def __eq__(self, other):
         return self is other or (isinstance(other, Moffat) and _eq(self.beta, other.beta) and
                                  _eq(self.scale_radius, other.scale_radius) and
-                                 self.trunc == other.trunc and _eq(self.flux, other.flux) and
+                                 _eq(self.trunc, other.trunc) and _eq(self.flux, other.flux) and
                                  self.gsparams == other.gsparams)
 
     def __hash__(self):
-        return hash(("galsim.Moffat", str(self.beta), str(self.scale_radius), str(self.flux),
+        return hash(("galsim.Moffat", str(self.beta), str(self.scale_radius), str(self.trunc), str(self.flux),
                      self.gsparams))
 
     def __repr__(self):

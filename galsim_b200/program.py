@@ -143,6 +143,23 @@ class Program(object):
             inv = np.asarray(inv).reshape(len(sersic), B)
             for k, l in enumerate(sersic):
                 leaves['table'][:, l] = inv[k]
+        self.moffat_beta = None
+        self.moffat_trunc = None
+        moffat = [l for l in range(L) if self.bld.leaf_types[l] == _lib.MOFFAT]
+        if moffat:
+            # one table per distinct (beta, trunc / rD) of the truncated Moffat leaves
+            bvals = np.concatenate([leaves[:, l]['p'][:, 0] for l in moffat])
+            tvals = np.concatenate([leaves[:, l]['p'][:, 2] / leaves[:, l]['p'][:, 1] for l in moffat])
+            cut = tvals > 0.
+            if np.any(cut):
+                uniq, inv = np.unique(np.stack([bvals[cut], tvals[cut]], -1), axis=0, return_inverse=True)
+                slot = np.full(len(bvals), -1, dtype=np.int32)
+                slot[cut] = np.asarray(inv).reshape(-1)
+                slot = slot.reshape(len(moffat), B)
+                for k, l in enumerate(moffat):
+                    leaves['table'][:, l] = slot[k]
+                self.moffat_beta = np.ascontiguousarray(uniq[:, 0])
+                self.moffat_trunc = np.ascontiguousarray(uniq[:, 1])
         self.image_order = []
         image_leaves = [l for l in range(L) if self.bld.leaf_types[l] == _lib.INTERPOLATED]
         if image_leaves:
@@ -157,20 +174,22 @@ class Program(object):
                 leaves['table'][:, l] = np.broadcast_to(np.array(slots, dtype=np.int32), (B,))
         self.d_leaves = _lib.to_device(leaves)
         self.d_info = torch.empty(B * L * 2, dtype=torch.float64, device=_lib.Device.torch_device())
-        if self.sersic_n is None and not self.image_order:
+        if self.sersic_n is None and not self.image_order and self.moffat_beta is None:
             self.tables = None
         elif getattr(self, 'tables', None) is None:
             self.tables = _lib.TablePool.acquire()
             self._pooled_tables = True
 
     def compute_leaves(self):
-        """FP64 on the GPU: build the Sersic FT tables, then every leaf's derived constants,
-        stepk and maxk; copy stepk / maxk back for the host-side composition."""
+        """FP64 on the GPU: build the Sersic and truncated-Moffat FT tables, then every leaf's
+        derived constants, stepk and maxk; copy stepk / maxk back for the host-side composition."""
         self.upload()
         B, L = self.B, self.L
         if self.tables is not None and self.sersic_n is not None:
             self.tables.build_sersic(self.sersic_n, self.gsparams, with_dn=self.need_dn,
                                      trunc_over_r0=self.sersic_trunc)
+        if self.tables is not None and self.moffat_beta is not None:
+            self.tables.build_moffat(self.moffat_beta, self.moffat_trunc, self.gsparams)
         if self.image_order:
             self._build_images()
         _lib.check(_lib.lib().gsb_prepare_leaves(
@@ -326,7 +345,8 @@ class Program(object):
             # the captured launches hold the table pointers: the same Sersic indices keep them
             key = tuple(np.asarray(v, np.int64).tobytes() for v in (N, Nk, xmin, ymin, nx, ny)) + \
                 (dtype, precision, b'' if self.sersic_n is None else self.sersic_n.tobytes(),
-                 b'' if self.sersic_trunc is None else self.sersic_trunc.tobytes())
+                 b'' if self.sersic_trunc is None else self.sersic_trunc.tobytes(),
+                 b'' if self.moffat_beta is None else self.moffat_beta.tobytes() + self.moffat_trunc.tobytes())
             gs = getattr(self, '_graph_state', None)
             if gs is not None and gs['key'] == key:
                 g = gs['geom']

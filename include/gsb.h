@@ -42,7 +42,8 @@ enum {
     GSB_GAUSSIAN    = 0,   /* p = {sigma}                                  */
     GSB_EXPONENTIAL = 1,   /* p = {r0}                                     */
     GSB_SERSIC      = 2,   /* p = {n, r0 or hlr (GSB_LEAF_SIZE_IS_HLR), trunc} */
-    GSB_MOFFAT      = 3,   /* p = {beta, r0, trunc}                        */
+    GSB_MOFFAT      = 3,   /* p = {beta, r0, trunc}; trunc > 0: `table` names a Moffat slot
+                              built by gsb_moffat_tables_build for (beta, trunc / r0) */
     GSB_KOLMOGOROV  = 4,   /* p = {lam_over_r0}                            */
     GSB_AIRY        = 5,   /* p = {lam_over_diam, obscuration}             */
     GSB_BOX         = 6,   /* p = {width, height}                          */
@@ -111,11 +112,13 @@ typedef struct gsb_leaf {
     double jac[4];     /* composed Jacobian [A, B, C, D] (row-major 2x2, transform.py:593) */
     double flux;
     double p[3];       /* profile parameters, see the type enum */
-    double d[8];       /* derived values, written by gsb_prepare_leaves (GSB_INTERPOLATED:
-                          the slot's k-image device addresses are kept in d[6] and d[7], so
-                          the leaves must be prepared again after gsb_images_build) */
+    double d[8];       /* derived values, written by gsb_prepare_leaves (GSB_INTERPOLATED and
+                          truncated GSB_MOFFAT: the slot's device addresses are kept in d[6]
+                          and d[7], so the leaves must be prepared again after
+                          gsb_images_build / gsb_moffat_tables_build) */
     int32_t flags;     /* GSB_LEAF_* */
-    int32_t table;     /* FT table slot (Sersic) or image slot (GSB_INTERPOLATED), set by the caller */
+    int32_t table;     /* FT table slot (Sersic, truncated Moffat) or image slot (GSB_INTERPOLATED),
+                          set by the caller */
 } gsb_leaf;
 
 /* One phase / flux factor of one stamp (stamp-major: phases[s * n_phases + i]). */
@@ -191,6 +194,30 @@ int gsb_sersic_truncation(int count, const double* h_in, double* h_out, void* st
 
 /* Copy slot headers back (18 doubles per slot: see gsb_tables.cu) for inspection. */
 int gsb_sersic_tables_info(const gsb_tables* t, double* h_out, int count, void* stream);
+
+/* Build `count` truncated-Moffat FT tables in FP64 on the device, Moffat slots 0..count-1
+ * (replacing earlier Moffat slots; Sersic and image slots are kept).  Per slot (h_beta[i],
+ * h_trunc_over_rd[i] = trunc / scale radius): the truncated Hankel transform
+ *     v(k) = 2 (beta - 1) / F  int_0^t r (1 + r^2)^-beta J0(k r) dr,  F = 1 - (1 + t^2)^(1 - beta)
+ * on the grid k = 0, dk, 2 dk, ... (k < 50, dk = table_spacing (kvalue_accuracy / 10)^(1/4)),
+ * ended after 5 values in a row at or below kvalue_accuracy, with its natural cubic spline in
+ * k^2 and maxk (in units of 1 / scale radius).  Reference: SBMoffat::setupFT
+ * (src/SBMoffat.cpp:565-625), math::hankel_trunc (src/math/Hankel.cpp:249-255).  beta must be
+ * > 0 and != 1 (at beta = 1 the reference's normalisation is 0 / 0); tables longer than 7264
+ * nodes (kvalue_accuracy below ~2e-8 at table_spacing 1) return GSB_ERR_UNSUPPORTED. */
+int gsb_moffat_tables_build(gsb_tables* t, const double* h_beta, const double* h_trunc_over_rd, int count,
+                            const gsb_gsparams* gsp, void* stream);
+
+/* Copy Moffat slot headers back, 8 doubles per slot: beta, trunc / rD, flux fraction factor F,
+ * dk, nodes used, last k^2, maxk (units of 1 / rD), status. */
+int gsb_moffat_tables_info(const gsb_tables* t, double* h_out, int count, void* stream);
+
+/* Scale radius of Moffat profiles from the half-light radius (moffat.py:97-104,
+ * MoffatCalculateScaleRadiusFromHLR, src/SBMoffat.cpp:103-160): h_in per profile (beta, hlr,
+ * trunc), h_out the scale radius; analytic for trunc = 0, else FP64 Brent on the device.
+ * trunc > 0 needs trunc > sqrt(2) hlr (GSB_ERR_INVALID); beta <= 1 has no bracket
+ * (GSB_ERR_NUMERIC, as the reference's "Solve error"). */
+int gsb_moffat_scale_radius(int count, const double* h_in, double* h_out, void* stream);
 
 /* InterpolatedImage sources ------------------------------------------------------------ */
 /* One image of an InterpolatedImage, placed in its zero-padded N x N frame (the reference's

@@ -197,28 +197,33 @@ def hankel_inf(f, k, relerr, abserr):
     return ans1
 
 
-def hankel_trunc_exact(f, k, rmax):
+_GL = {}
+
+
+def hankel_trunc_exact(f, k, rmax, order=24):
     """int_0^rmax r f(r) J0(k r) dr -- the quantity of math::hankel_trunc
-    (src/math/Hankel.cpp:249-255), computed to ~1e-13 relative: adaptive Gauss-Kronrod
-    (scipy.integrate.quad) on panels between consecutive zeros of J0(k r), with breakpoints
-    graded toward r = 0 where r f(r) has an integrable cusp.  The reference integrates the same
-    integral with its own adaptive Gauss-Kronrod-Patterson scheme to relerr 1e-6, so the two
-    agree to the reference's integration error (this value is the more accurate one)."""
-    from scipy import integrate
-    g = lambda r: r * f(r) * special.j0(k * r)
-    pts = [0.]
+    (src/math/Hankel.cpp:249-255), computed to ~1e-13 relative: Gauss-Legendre (`order` points)
+    on the panels between consecutive zeros of J0(k r), the first one graded toward r = 0 in 48
+    halvings (where r f(r) may have an integrable cusp, r^(1/n) for a Sersic).  The reference
+    integrates the same integral with its own adaptive Gauss-Kronrod-Patterson scheme to relerr
+    1e-6, so the two agree to the reference's integration error (this value is the more
+    accurate one)."""
+    if order not in _GL:
+        _GL[order] = np.polynomial.legendre.leggauss(order)
+    x, w = _GL[order]
     if k > 0.:
         zs = _j0_zeros(max(16, int(k * rmax / PI) + 8))[0] / k
-        pts += [float(z) for z in zs if z < rmax]
-    pts.append(float(rmax))
-    first = pts[1]
-    grade = [first * 2. ** -j for j in range(1, 30)][::-1]
-    pts = [0.] + grade + pts[1:]
-    tot = 0.
-    for a, b in zip(pts[:-1], pts[1:]):
-        v, _ = integrate.quad(g, a, b, epsabs=0., epsrel=1e-13, limit=200)
-        tot += v
-    return tot
+        zs = zs[zs < rmax]
+    else:
+        zs = np.zeros(0)
+    first = float(zs[0]) if len(zs) else float(rmax)
+    grade = first * 2. ** -np.arange(48, 0, -1)
+    edges = np.concatenate([grade, [first], zs[1:], [rmax]]) if len(zs) else np.concatenate([grade, [rmax]])
+    a, b = edges[:-1], edges[1:]
+    h = 0.5 * (b - a)
+    r = (a + h)[:, None] + h[:, None] * x[None, :]
+    g = r * f(r) * special.j0(k * r)
+    return float(np.sum(h[:, None] * w[None, :] * g))
 
 
 # ---------------------------------------------------------------------------------------------
@@ -251,11 +256,17 @@ class Spline(object):
                 y2[i] -= c[i - 1] * y2[i + 1]
         self.y2 = y2
         self.da = (self.x[-1] - self.x[0]) / (n - 1)
+        # ArgVec (Table.cpp:64-130): equal spacing to 1% of a step gives the direct index,
+        # otherwise the first argument above a (std::upper_bound)
+        self.equal = bool(np.all(np.abs((self.x - self.x[0]) / self.da - np.arange(n)) <= 0.01))
 
     def __call__(self, a):
         a = np.asarray(a, float)
         n = len(self.x)
-        i = np.ceil((a - self.x[0]) / self.da).astype(int)
+        if self.equal:
+            i = np.ceil((a - self.x[0]) / self.da).astype(int)
+        else:
+            i = np.searchsorted(self.x, a, side='right')
         i = np.clip(i, 1, n - 1)
         h = self.x[i] - self.x[i - 1]
         aa = self.x[i] - a
@@ -693,14 +704,32 @@ class OSersic(OLeaf):
         return self.flux * self.info.kvalue(ksq)
 
 
+def moffat_scale_radius_from_hlr(hlr, trunc, beta):
+    """MoffatCalculateScaleRadiusFromHLR (SBMoffat.cpp:95-160): analytic without truncation,
+    else Brent on 2 f(re) - f(rm) = 0, f(R) = 1 - (1 + R^2/rd^2)^(1-beta), from the untruncated
+    value with the upper bracket expanded."""
+    r1 = hlr / math.sqrt(0.5 ** (1. / (1. - beta)) - 1.)
+    if trunc == 0.:
+        return r1
+    fn = lambda rd: 2. * (1. - (1. + hlr * hlr / (rd * rd)) ** (1. - beta)) - \
+        (1. - (1. + trunc * trunc / (rd * rd)) ** (1. - beta))
+    return solve_upper(fn, r1, 2. * r1)
+
+
 class OMoffat(OLeaf):
-    def __init__(self, beta, r0=None, fwhm=None, hlr=None, flux=1.):
-        self.beta, self.flux = float(beta), float(flux)
+    """Moffat (moffat.py:79-125, SBMoffat.cpp:163-345, 498-625); trunc > 0: the FT from a spline
+    in k^2 of the truncated Hankel transform (setupFT, :565-625)."""
+
+    def __init__(self, beta, r0=None, fwhm=None, hlr=None, flux=1., trunc=0.):
+        self.beta, self.flux, self.trunc = float(beta), float(flux), float(trunc)
         if fwhm is not None:
             r0 = fwhm / (2. * math.sqrt(2. ** (1. / self.beta) - 1.))
         elif hlr is not None:
-            r0 = hlr / math.sqrt(0.5 ** (1. / (1. - self.beta)) - 1.)
+            r0 = moffat_scale_radius_from_hlr(float(hlr), self.trunc, self.beta)
         self.r0 = float(r0)
+        if self.trunc > 0.:
+            self._setup_ft()
+            return
         kacc = self.gsp.kvalue_accuracy
         b = self.beta
         self.mode, self.nu = 0, b - 1.
@@ -711,6 +740,34 @@ class OMoffat(OLeaf):
                 if nu is not None:
                     self.nu = nu
                 break
+
+    def _setup_ft(self):
+        gsp, b = self.gsp, self.beta
+        self.maxRrD = self.trunc / self.r0
+        self.flux_factor = 1. - (1. + self.maxRrD ** 2) ** (1. - b)
+        prefactor = 2. * (b - 1.) / self.flux_factor
+        dk = gsp.table_spacing * math.sqrt(math.sqrt(gsp.kvalue_accuracy / 10.))
+        f = lambda r: (1. + r * r) ** (-b)
+        args, vals = [], []
+        maxk = 0.
+        nbelow = 0
+        k = 0.
+        while k < 50:
+            v = prefactor * hankel_trunc_exact(f, k, self.maxRrD)
+            args.append(k * k)
+            vals.append(v)
+            if abs(v) > gsp.maxk_threshold:
+                maxk = k
+            nbelow = 0 if abs(v) > gsp.kvalue_accuracy else nbelow + 1
+            if nbelow == 5:
+                break
+            k += dk
+        self.ft = Spline(args, vals)
+        k1, k2 = maxk, maxk + dk
+        if k2 < 50:
+            f1, f2 = abs(float(self.ft(k1 * k1))), abs(float(self.ft(k2 * k2)))
+            maxk = (k1 * (f2 - gsp.maxk_threshold) + k2 * (gsp.maxk_threshold - f1)) / (f2 - f1)
+        self.maxk_rd = maxk
 
     def kv2(self, k):
         """kV normalised to 1 at k = 0 (SBMoffat.cpp:274-345)."""
@@ -729,17 +786,28 @@ class OMoffat(OLeaf):
     def stepk_maxk(self):
         gsp = self.gsp
         b, rD = self.beta, self.r0
-        ksq = solve_upper(lambda q: float(self.kv2(math.sqrt(q))) - gsp.maxk_threshold, 0., 100.)
-        maxk = math.sqrt(ksq) / rD
-        maxR = math.sqrt(gsp.xvalue_accuracy ** (1. / (1. - b)) - 1.) * rD
+        if self.trunc > 0.:
+            maxk = self.maxk_rd / rD
+            maxR = self.maxRrD * rD
+            ff = self.flux_factor
+        else:
+            ksq = solve_upper(lambda q: float(self.kv2(math.sqrt(q))) - gsp.maxk_threshold, 0., 100.)
+            maxk = math.sqrt(ksq) / rD
+            maxR = math.sqrt(gsp.xvalue_accuracy ** (1. / (1. - b)) - 1.) * rD
+            ff = 1.
+        if b <= 1.1:
+            return PI / maxR, maxk
         R = gsp.folding_threshold ** (0.5 / (1. - b)) * rD
         if R > maxR:
             R = maxR
-        hlr = rD * math.sqrt(0.5 ** (1. / (1. - b)) - 1.)
+        hlr = rD * math.sqrt((1. - 0.5 * ff) ** (1. / (1. - b)) - 1.)
         R = max(R, gsp.stepk_minimum_hlr * hlr)
         return PI / R, maxk
 
     def kvalue(self, kx, ky):
+        if self.trunc > 0.:
+            ksq = (kx ** 2 + ky ** 2) * self.r0 ** 2
+            return self.flux * np.where(ksq > self.ft.x[-1], 0., self.ft(ksq))
         k = np.sqrt(kx ** 2 + ky ** 2) * self.r0
         return self.flux * self.kv2(k)
 

@@ -35,6 +35,10 @@ def profile(galsim, spec):
         return galsim.Sersic(n=spec[1], flux=spec[3], trunc=spec[4], flux_untruncated=spec[5], **size)
     if kind == 'moffat':
         return galsim.Moffat(beta=spec[1], fwhm=spec[2], flux=spec[3])
+    if kind == 'moffatt':
+        # ('moffatt', beta, size, flux, trunc, 'fwhm' | 'hlr' | 'r0')
+        key = {'fwhm': 'fwhm', 'hlr': 'half_light_radius', 'r0': 'scale_radius'}[spec[5]]
+        return galsim.Moffat(beta=spec[1], flux=spec[3], trunc=spec[4], **{key: spec[2]})
     if kind == 'kolmogorov':
         return galsim.Kolmogorov(fwhm=spec[1], flux=spec[2])
     if kind == 'airy':
@@ -596,6 +600,32 @@ TRUNC_SIZE_CASES = [('sersict', n, 0.5, 1., t, fu, kind) for n, t, fu, kind in
                      (4.0, 3.0, True, 'hlr'), (5.5, 2.5, False, 'r0'), (2.0, 0.9, False, 'hlr'))]
 
 
+# Truncated Moffat profiles (moffat.py:79-125, SBMoffat with trunc > 0: the FT from a spline of
+# the truncated Hankel transform): drawImage through the reference, and the profiles' sizes.
+TRUNC_MOFFAT_CASES = [
+    ('tm_b25_fwhm_gauss', ('conv', [('gauss', 0.4, 100.), ('moffatt', 2.5, 0.7, 1., 2.0, 'fwhm'),
+                                    ('pixel', 0.2)]), 48, 48, 0.2, 'f8', (0., 0.)),
+    ('tm_b105_hlr_alone', ('moffatt', 1.05, 0.4, 30., 1.5, 'hlr'), 40, 40, 0.2, 'f8', (0.1, 0.3)),
+    ('tm_b3_r0_shear_f4', ('conv', [('shear', 0.15, 0.05, ('exp', 0.5, 1e3)),
+                                    ('moffatt', 3.0, 0.5, 1., 1.6, 'r0'), ('pixel', 0.2)]), 48, 48, 0.2, 'f4',
+                           (0., 0.)),
+    ('tm_b45_hlr_sersic', ('conv', [('sersic', 2.0, 0.3, 50.), ('moffatt', 4.5, 0.35, 1., 0.9, 'hlr'),
+                                    ('pixel', 0.1)]), 40, 40, 0.1, 'f8', (0., 0.)),
+    ('tm_b08_r0_sum', ('sum', [('moffatt', 0.8, 0.3, 10., 1.2, 'r0'), ('gauss', 0.5, 5.)]), 32, 32, 0.2, 'f8',
+                      (0., 0.)),
+]
+TRUNC_MOFFAT_SIZE_CASES = [('moffatt', b, sz, 1., t, kind) for b, sz, t, kind in
+                           ((2.5, 0.7, 2.0, 'fwhm'), (1.05, 0.4, 1.5, 'hlr'), (3.0, 0.5, 1.6, 'r0'),
+                            (4.5, 0.35, 0.9, 'hlr'), (0.8, 0.3, 1.2, 'r0'), (1.5, 0.6, 3.0, 'hlr'),
+                            (6.0, 1.0, 2.0, 'fwhm'), (2.0, 0.5, 0.8, 'hlr'))]
+TRUNC_MOFFAT_KIMAGE_CASES = [
+    # (name, spec, dk, n): drawKImage on an n x n grid centred on k = 0
+    ('tmk_b25', ('moffatt', 2.5, 0.7, 3., 2.0, 'fwhm'), 0.3, 41),
+    ('tmk_b08_shear', ('shear', 0.1, 0.2, ('moffatt', 0.8, 0.3, 2., 1.2, 'r0')), 0.5, 51),
+    ('tmk_b45_far', ('moffatt', 4.5, 0.35, 1., 0.9, 'hlr'), 2.0, 61),
+]
+
+
 def main_trunc(ref_root):
     from ref_import import import_reference_galsim
     galsim = import_reference_galsim(ref_root)
@@ -608,6 +638,17 @@ def main_trunc(ref_root):
     out['sizes'] = np.array([(profile(galsim, sp).stepk, profile(galsim, sp).maxk) for sp in TRUNC_SIZE_CASES])
     out['scale_radius'] = np.array([profile(galsim, sp).scale_radius for sp in TRUNC_SIZE_CASES])
     out['flux'] = np.array([profile(galsim, sp).flux for sp in TRUNC_SIZE_CASES])
+    for name, spec, nx, ny, scale, dt, off in TRUNC_MOFFAT_CASES:
+        im = profile(galsim, spec).drawImage(nx=nx, ny=ny, scale=scale, dtype=np.dtype(dt).type, method='fft',
+                                             offset=off)
+        out['draw_' + name] = im.array
+        out['draw_' + name + '_flux'] = np.array(im.added_flux)
+    objs = [profile(galsim, sp) for sp in TRUNC_MOFFAT_SIZE_CASES]
+    out['moffat_sizes'] = np.array([(o.stepk, o.maxk) for o in objs])
+    out['moffat_scale_radius'] = np.array([o.scale_radius for o in objs])
+    out['moffat_hlr'] = np.array([o.half_light_radius for o in objs])
+    for name, spec, dk, n in TRUNC_MOFFAT_KIMAGE_CASES:
+        out['kimg_' + name] = profile(galsim, spec).drawKImage(nx=n, ny=n, scale=dk).array
     np.savez_compressed(os.path.join(HERE, 'reference_trunc.npz'), **out)
     print('wrote', os.path.join(HERE, 'reference_trunc.npz'), len(out), 'arrays')
 

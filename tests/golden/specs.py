@@ -21,6 +21,9 @@ def oracle_profile(spec):
         return O.OSersic(spec[1], flux=spec[3], trunc=spec[4], flux_untruncated=spec[5], **size)
     if kind == 'moffat':
         return O.OMoffat(spec[1], fwhm=spec[2], flux=spec[3])
+    if kind == 'moffatt':
+        key = {'fwhm': 'fwhm', 'hlr': 'hlr', 'r0': 'r0'}[spec[5]]
+        return O.OMoffat(spec[1], flux=spec[3], trunc=spec[4], **{key: spec[2]})
     if kind == 'kolmogorov':
         return O.OKolmogorov(fwhm=spec[1], flux=spec[2])
     if kind == 'airy':

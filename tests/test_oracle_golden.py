@@ -177,3 +177,35 @@ def test_truncated_sersic_sizes_match_reference():
         assert abs(m - mk) <= 1e-6 * mk, spec
         assert abs(o.r0 - TRUNC['scale_radius'][k]) <= 1e-9 * o.r0, spec
         assert abs(o.flux - TRUNC['flux'][k]) <= 1e-10 * o.flux, spec
+
+
+@pytest.mark.parametrize('case', MG.TRUNC_MOFFAT_CASES, ids=[c[0] for c in MG.TRUNC_MOFFAT_CASES])
+def test_truncated_moffat_draw_matches_reference(case):
+    """Truncated Moffat profiles: the oracle's spline over k^2 of the exact truncated Hankel
+    transform against the reference's spline of its adaptive one (relerr 1e-6)."""
+    name, spec, nx, ny, scale, dt, off = case
+    arr, flux, N, Nk = O.draw_image(specs.oracle_profile(spec), nx, ny, scale, off)
+    ref = TRUNC['draw_' + name]
+    peak = np.abs(ref).max()
+    assert np.abs(arr.astype(ref.dtype) - ref).max() <= 2e-7 * peak
+    assert abs(flux - float(TRUNC['draw_' + name + '_flux'])) <= 2e-7 * abs(flux)
+
+
+def test_truncated_moffat_sizes_match_reference():
+    for k, spec in enumerate(MG.TRUNC_MOFFAT_SIZE_CASES):
+        o = specs.oracle_profile(spec)
+        s, m = o.stepk_maxk()
+        sk, mk = TRUNC['moffat_sizes'][k]
+        assert abs(s - sk) <= 1e-9 * sk, spec
+        assert abs(m - mk) <= 1e-6 * mk, spec
+        assert abs(o.r0 - TRUNC['moffat_scale_radius'][k]) <= 1e-9 * o.r0, spec
+
+
+@pytest.mark.parametrize('case', MG.TRUNC_MOFFAT_KIMAGE_CASES, ids=[c[0] for c in MG.TRUNC_MOFFAT_KIMAGE_CASES])
+def test_truncated_moffat_kimage_matches_reference(case):
+    """k-values of truncated Moffat profiles on odd grids centred on k = 0, out to beyond the
+    table's last argument (where the reference returns 0)."""
+    name, spec, dk, n = case
+    kim = O.draw_kimage(specs.oracle_profile(spec), n, n, -(n // 2), -(n // 2), dk)
+    ref = TRUNC['kimg_' + name]
+    assert np.abs(kim - ref).max() <= 1e-12 * np.abs(ref).max()
