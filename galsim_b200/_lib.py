@@ -112,6 +112,7 @@ def lib():
                                     vp, vp, i, vp, i, i, vp, i, vp, sz, vp]),
             'gsb_draw_set_variant': (i, [i]),
             'gsb_exp_fp64': (i, [vp, vp, i, vp]),
+            'gsb_exp_fp64_ex': (i, [vp, vp, i, i, vp]),
             'gsb_draw_tune_report': (i, [ctypes.c_char_p, sz]),
             'gsb_draw_kimages': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp,
                                      vp, vp, d, i, i, i, i, vp, i, vp]),

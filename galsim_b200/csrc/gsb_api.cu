@@ -26,7 +26,7 @@ int prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gs
                    const gsb_tables* t, double* d_info, cudaStream_t stream);
 size_t draw_workspace_size(int N, int n_stamps, int precision);
 int draw_set_variant(int v);
-int exp_fp64(const double* d_x, double* d_y, int n, cudaStream_t stream);
+int exp_fp64(const double* d_x, double* d_y, int n, int table_size, cudaStream_t stream);
 int draw_tune_report(char* buf, size_t len);
 int draw_images(const gsb_template* tpl, int n_stamps, const gsb_leaf* d_leaves,
                 const gsb_phase* d_phases, const double* d_scales, const gsb_stamp* d_stamps,
@@ -335,7 +335,15 @@ int gsb_draw_set_variant(int variant) { return draw_set_variant(variant); }
 int gsb_exp_fp64(const double* d_x, double* d_y, int n, void* stream)
 {
     if (n < 0 || (n > 0 && (!d_x || !d_y))) return set_error(GSB_ERR_INVALID, "bad argument");
-    return exp_fp64(d_x, d_y, n, (cudaStream_t)stream);
+    return exp_fp64(d_x, d_y, n, 32, (cudaStream_t)stream);
+}
+
+int gsb_exp_fp64_ex(const double* d_x, double* d_y, int n, int table_size, void* stream)
+{
+    if (n < 0 || (n > 0 && (!d_x || !d_y))) return set_error(GSB_ERR_INVALID, "bad arguments");
+    if (table_size != 32 && table_size != 256) return set_error(GSB_ERR_INVALID, "table_size must be 32 or 256");
+    if (!device_state()->ready) return set_error(GSB_ERR_INVALID, "gsb_init has not been called");
+    return exp_fp64(d_x, d_y, n, table_size, (cudaStream_t)stream);
 }
 
 int gsb_draw_tune_report(char* buf, size_t len) { return draw_tune_report(buf, len); }

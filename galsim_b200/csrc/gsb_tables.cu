@@ -24,6 +24,37 @@ constexpr int kMaxRounds = 128;      // rounds of ln k nodes per table build (st
 constexpr int kLevMax = 20;
 constexpr long long kNroot = 1000000;
 
+// 2^(j/256), j = 0..255, correctly rounded (computed on the host in extended precision by
+// ogata_init): the exponential table of the quadrature kernels' exp_tab256_core.
+__device__ double g_exp2_256[256];
+
+// The same method with a 256-entry table 2^(j/256) (`tab`, correctly rounded, filled by the
+// caller): |r| <= ln2/512, so the degree-4 Taylor polynomial of e^r suffices (truncation
+// < 4e-17 relative), two fused multiply-adds fewer than exp_tab_core.  For the quadrature
+// kernels, which evaluate billions of exponentials per table build.
+__device__ __forceinline__ double exp_tab256_core(double x, const double* tab)
+{
+    const double kShift = 6755399441055744.0;               // 1.5 * 2^52
+    const double s = __dadd_rn(__dmul_rn(x, 369.3299304675746), kShift);   // 256 / ln2
+    const int n = __double2loint(s);
+    const double t = s - kShift;
+    double r = fma(-t, 0.0027076061740622863, x);            // ln2/256, leading double
+    r = fma(-t, 9.058776616587108e-20, r);                   // ln2/256, remainder
+    const int j = n & 255;
+    const int m = n >> 8;
+    double p = fma(r, 1. / 24., 1. / 6.);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.);
+    p = fma(p, r, 1.);
+    const double v = tab[j] * p;
+    return __hiloint2double(__double2hiint(v) + (m << 20), __double2loint(v));
+}
+
+__device__ __forceinline__ double exp_tab256_neg(double x, const double* tab)
+{
+    return exp_tab256_core(fmax(x, -708.), tab);
+}
+
 __global__ void ogata_root_kernel(double2* root, long long nroot)
 {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -159,15 +190,15 @@ __device__ __forceinline__ double2 warp_ogata_sum_pair(const OgataTables& og, do
         if (valid) {
             const double2 n = TAB ? xw[i] : ogata_node(og.root, h, i);
             const double lr0 = n.x - logk0;
-            const double u0 = exp_tab_core(lr0 * invn, etab);
+            const double u0 = exp_tab256_core(lr0 * invn, etab);
             if (act0) {
-                const double f = exp_tab_neg(-u0, etab);
+                const double f = exp_tab256_neg(-u0, etab);
                 s0 = n.y * f;
                 if (DN) ds0 = s0 * u0 * invn * (lr0 * invn + dnc);
             }
             if (act1) {
                 const double u1 = u0 * c1;
-                const double f = exp_tab_neg(-u1, etab);
+                const double f = exp_tab256_neg(-u1, etab);
                 s1 = n.y * f;
                 if (DN) ds1 = s1 * u1 * invn * ((n.x - logk1) * invn + dnc);
             }
@@ -550,9 +581,9 @@ __global__ void __launch_bounds__(256, 4) sersic_nodes_pair_kernel(const double*
                                     double* dvals)
 {
     if (prev_live && *prev_live == 0) return;
-    // the exponential's 2^(j/32) table, read three times per pair of terms, from shared memory
-    __shared__ double etab[32];
-    if (threadIdx.x < 32) etab[threadIdx.x] = kExp2Tab[threadIdx.x];
+    // the exponential's 2^(j/256) table, read three times per pair of terms, from shared memory
+    __shared__ double etab[256];
+    etab[threadIdx.x] = g_exp2_256[threadIdx.x];
     __syncthreads();
     const int npair = (nround + 1) / 2;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
@@ -1139,18 +1170,35 @@ __global__ void exp_tab_kernel(const double* x, double* y, int n)
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) y[i] = exp_tab(x[i]);
 }
+
+__global__ void exp_tab256_kernel(const double* x, double* y, int n)
+{
+    __shared__ double etab[256];
+    etab[threadIdx.x] = g_exp2_256[threadIdx.x];
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = x[i] < -708. ? 0. : exp_tab256_core(x[i], etab);
+}
 }  // namespace
 
-int exp_fp64(const double* d_x, double* d_y, int n, cudaStream_t stream)
+int exp_fp64(const double* d_x, double* d_y, int n, int table_size, cudaStream_t stream)
 {
     if (n <= 0) return GSB_OK;
-    exp_tab_kernel<<<(n + 255) / 256, 256, 0, stream>>>(d_x, d_y, n);
+    if (table_size == 256)
+        exp_tab256_kernel<<<(n + 255) / 256, 256, 0, stream>>>(d_x, d_y, n);
+    else
+        exp_tab_kernel<<<(n + 255) / 256, 256, 0, stream>>>(d_x, d_y, n);
     GSB_CUDA_CHECK(cudaGetLastError());
     return GSB_OK;
 }
 
 int ogata_init(DeviceState* st)
 {
+    {
+        double tab[256];
+        for (int j = 0; j < 256; ++j) tab[j] = (double)exp2l((long double)j / 256.L);
+        GSB_CUDA_CHECK(cudaMemcpyToSymbol(g_exp2_256, tab, sizeof(tab)));
+    }
     GSB_CUDA_CHECK(cudaMalloc(&st->d_status, sizeof(int)));
     GSB_CUDA_CHECK(cudaMalloc(&st->d_root, sizeof(double2) * kNroot));
     ogata_root_kernel<<<(unsigned)((kNroot + 255) / 256), 256>>>(st->d_root, kNroot);

@@ -372,6 +372,10 @@ int gsb_draw_set_variant(int variant);
  * its accuracy can be checked against the CUDA math library.  No reference counterpart. */
 int gsb_exp_fp64(const double* d_x, double* d_y, int n, void* stream);
 
+/* The same with the table size chosen: 32 (gsb_exp_fp64) or 256, the variant with a degree-4
+ * polynomial that the Sersic quadrature kernel uses. */
+int gsb_exp_fp64_ex(const double* d_x, double* d_y, int n, int table_size, void* stream);
+
 /* Text report of the tuned classes, one line each; returns its length (writes at most len-1
  * characters and a terminating zero to buf when buf is not NULL). */
 int gsb_draw_tune_report(char* buf, size_t len);
