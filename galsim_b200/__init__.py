@@ -28,6 +28,12 @@ from . import fits
 from .fits import FitsHeader
 from .compound import Convolve, Convolution, Add, Sum, Transform, Transformation, _Transform
 from .batch import draw_batch, plan_batch, run_batch, StampBatch
+from .table import LookupTable, _LookupTable, trapz
+from .sed import SED
+from .bandpass import Bandpass
+from . import integ, dcr
+from .chromatic import (ChromaticObject, ChromaticTransformation, SimpleChromaticTransformation,
+                        ChromaticAtmosphere, ChromaticSum, ChromaticConvolution)
 from ._lib import set_device
 from . import autodiff
 from . import config

@@ -53,6 +53,11 @@ STAMP_DTYPE = np.dtype({'names': ['N', 'Nk', 'xmin', 'ymin', 'nx', 'ny', 'out_of
                         'formats': ['i4', 'i4', 'i4', 'i4', 'i4', 'i4', 'i8'],
                         'offsets': [0, 4, 8, 12, 16, 20, 24], 'itemsize': 32})
 
+XLEAF_DTYPE = np.dtype({'names': ['jac', 'xoff', 'yoff', 'flux_ratio', 'flux', 'p', 'type', 'flags'],
+                        'formats': [('f8', 4), 'f8', 'f8', 'f8', 'f8', ('f8', 3), 'i4', 'i4'],
+                        'offsets': [0, 32, 40, 48, 56, 64, 88, 92], 'itemsize': 96})
+XLEAF_JAC = 1
+
 IMAGE_DESC_DTYPE = np.dtype({'names': ['N', 'nx', 'ny', 'x0', 'y0', 'bx0', 'bx1', 'by0', 'by1',
                                          'x_interp', 'flags', 'pix_offset', 'flux', 'stepk_target',
                                          'maxk_limit'],
@@ -94,6 +99,8 @@ def lib():
             'gsb_moffat_tables_build': (i, [vp, vp, vp, i, vp, vp]),
             'gsb_moffat_tables_info': (i, [vp, vp, i, vp]),
             'gsb_moffat_scale_radius': (i, [i, vp, vp, vp]),
+            'gsb_weighted_stamp_sum': (i, [vp, i, vp, vp, i, ctypes.c_int64, vp, i, vp]),
+            'gsb_draw_real': (i, [i, i, vp, vp, vp, vp, i, i, vp, vp]),
             'gsb_images_build': (i, [vp, i, vp, vp, ctypes.POINTER(GSParamsC), vp]),
             'gsb_images_info': (i, [vp, vp, i, vp]),
             'gsb_add_noise': (i, [i, vp, vp, i, i, vp, i, vp, vp, vp]),

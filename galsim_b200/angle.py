@@ -84,6 +84,9 @@ class Angle(object):
     def sincos(self):
         return math.sin(self._rad), math.cos(self._rad)
 
+    def tan(self):
+        return math.tan(self._rad)
+
     def __repr__(self):
         return 'galsim.Angle(%r, galsim.radians)' % self._rad
 

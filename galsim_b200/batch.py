@@ -318,7 +318,12 @@ def plan_batch(obj, nx=None, ny=None, scale=None, dtype=np.float32, method='fft'
                                  real_space=False, gsparams=obj.gsparams)
     prog = Program(prof, tables=tables)
     prog.upload()
-    return BatchPlan(prog, nx, ny, nx is not None, flux_scale, dtype, scale, precision)
+    plan = BatchPlan(prog, nx, ny, nx is not None, flux_scale, dtype, scale, precision)
+    # 'no_pixel' / 'sb' on a profile analytic in real space is drawn in real space, as
+    # drawImage does (gsobject.py:1810-1811)
+    plan.real = method in ('no_pixel', 'sb') and prof.is_analytic_x
+    plan.prof = prof
+    return plan
 
 
 def run_batch(plan, recompute=True, graph=True):
@@ -329,6 +334,8 @@ def run_batch(plan, recompute=True, graph=True):
     from .program import fft_sizes, good_image_size
     prog = plan.prog
     B = prog.B
+    if getattr(plan, 'real', False):
+        return _run_real(plan)
     if recompute or not prog._prepared:
         prog.compute_leaves()
     stepk, maxk = prog.stepk_maxk()
@@ -347,6 +354,30 @@ def run_batch(plan, recompute=True, graph=True):
     flat, offsets, flux = prog.draw_stamps(N, Nk, xmin, ymin, nxs, nys, dt, precision=prec, graph=graph)
     bounds = [(1, int(x), 1, int(y)) for x, y in zip(nxs, nys)]
     return StampBatch(flat, offsets, nxs, nys, xmin, ymin, N, Nk, flux, plan.dtype, plan.scale,
+                      bounds, plan.flux_scale)
+
+
+def _run_real(plan):
+    """run_batch for a real-space plan: GalSim's automatic image size where needed (from the
+    FP64 stepk), then one gsb_draw_real over all stamps."""
+    from .program import good_image_size
+    from .realspace import draw_real_stamps
+    prog = plan.prog
+    B = prog.B
+    if plan.fixed:
+        nxs = np.full(B, int(plan.nx), np.int64)
+        nys = np.full(B, int(plan.ny), np.int64)
+    else:
+        prog.compute_leaves()
+        stepk, _ = prog.stepk_maxk()
+        nxs = good_image_size(stepk, 1.0)
+        nys = nxs.copy()
+    xmin = -(nxs // 2)
+    ymin = -(nys // 2)
+    flat, offsets, flux = draw_real_stamps(plan.prof, B, prog.gsparams, xmin, ymin, nxs, nys, plan.dtype)
+    bounds = [(1, int(x), 1, int(y)) for x, y in zip(nxs, nys)]
+    zero = np.zeros(B, np.int64)
+    return StampBatch(flat, offsets, nxs, nys, xmin, ymin, zero, zero, flux, plan.dtype, plan.scale,
                       bounds, plan.flux_scale)
 
 

@@ -17,7 +17,7 @@ SOURCES = ['gsb_api.cu', 'gsb_tables.cu', 'gsb_draw.cu', 'gsb_draw_f32_small.cu'
            'gsb_draw_f32_large.cu', 'gsb_draw_f64_small.cu', 'gsb_draw_f64_large.cu', 'gsb_draw_large.cu',
            'gsb_noalloc.cu', 'gsb_adjoint.cu', 'gsb_adjoint_f32_small.cu', 'gsb_adjoint_f32_large.cu',
            'gsb_adjoint_f64_small.cu', 'gsb_adjoint_f64_large.cu', 'gsb_images.cu', 'gsb_noise.cu',
-           'gsb_fits.cu', 'gsb_standalone.cu']
+           'gsb_fits.cu', 'gsb_standalone.cu', 'gsb_chromatic.cu', 'gsb_real.cu']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
 

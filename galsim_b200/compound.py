@@ -40,13 +40,17 @@ def Convolve(*args, **kwargs):
     if len(args) == 0:
         raise TypeError("At least one ChromaticObject or GSObject must be provided.")
     elif len(args) == 1:
-        if isinstance(args[0], GSObject):
+        from .chromatic import ChromaticObject
+        if isinstance(args[0], (GSObject, ChromaticObject)):
             args = [args[0]]
         elif isinstance(args[0], (list, tuple)):
             args = args[0]
         else:
             raise TypeError("Single input argument must be a GSObject, ChromaticObject, "
                             "or a (possibly mixed) list of them.")
+    from .chromatic import ChromaticObject, ChromaticConvolution
+    if any(isinstance(a, ChromaticObject) for a in args):
+        return ChromaticConvolution(*args, **kwargs)
     return Convolution(*args, **kwargs)
 
 
@@ -178,12 +182,16 @@ def Add(*args, **kwargs):
     if len(args) == 0:
         raise TypeError("At least one ChromaticObject or GSObject must be provided.")
     elif len(args) == 1:
-        if isinstance(args[0], GSObject):
+        from .chromatic import ChromaticObject
+        if isinstance(args[0], (GSObject, ChromaticObject)):
             args = [args[0]]
         elif isinstance(args[0], (list, tuple)):
             args = args[0]
         else:
             raise TypeError("Single input argument must be a GSObject or a list of them.")
+    from .chromatic import ChromaticObject, ChromaticSum
+    if any(isinstance(a, ChromaticObject) for a in args):
+        return ChromaticSum(*args, **kwargs)
     return Sum(*args, **kwargs)
 
 
@@ -284,6 +292,11 @@ def _as_jac(jac):
 
 def Transform(obj, jac=None, offset=(0., 0.), flux_ratio=1., gsparams=None, propagate_gsparams=True):
     """An affine transformation of a GSObject (transform.py:40-80)."""
+    from .chromatic import ChromaticObject, _Transform as _chromatic_transform
+    from .sed import SED
+    if isinstance(obj, ChromaticObject) or hasattr(jac, '__call__') or hasattr(offset, '__call__') or \
+            isinstance(flux_ratio, SED) or hasattr(flux_ratio, '__call__'):
+        return _chromatic_transform(obj, jac, offset, flux_ratio, gsparams, propagate_gsparams)
     if not isinstance(obj, GSObject):
         raise TypeError("Argument to Transform must be a GSObject.")
     return Transformation(obj, jac, offset, flux_ratio, gsparams, propagate_gsparams)

@@ -949,13 +949,17 @@ __global__ void kolmogorov_nodes_kernel(int ncand, double dlogr, gsb_gsparams gs
 }
 
 __global__ void kolmogorov_finalize_kernel(int ncand, double dlogr, gsb_gsparams gsp,
-                                           const double* vals, double* out)
+                                           const double* vals, double* out, double4* nodes, double* scratch)
 {
+    // the reference's loop: entries (r, f(r)) from r = e^-3 until f r^2 / 1.67 < thresh (that
+    // entry included), after the analytic f(0) = XVAL_ZERO (SBKolmogorov.cpp:352-384)
     const double thresh = gsp.shoot_accuracy / (2. * kPi);
     double r1 = 0., F1 = 0.;
+    int nused = 0;
     for (int i = 0; i < ncand; ++i) {
         const double r = exp(-3. + i * dlogr);
         r1 = r; F1 = vals[i];
+        nused = i + 1;
         if (vals[i] * r * r / 1.67 < thresh) break;
     }
     const double n = 11. / 3.;
@@ -963,6 +967,19 @@ __global__ void kolmogorov_finalize_kernel(int ncand, double dlogr, gsb_gsparams
     const double hlr = 2.992939911888651 * 0.5548101137;
     R = fmax(R, gsp.stepk_minimum_hlr * hlr);
     out[0] = kPi / R;
+    // the radial table's natural spline in r (Table::spline, src/Table.cpp:634-686), for the
+    // real-space drawing of Kolmogorov leaves
+    const int N = nused + 1;
+    double* xs = scratch;
+    double* ys = xs + N;
+    double* zs = ys + N;
+    double* cs = zs + N;
+    xs[0] = 0.;
+    ys[0] = 0.0876786563672346;     // XVAL_ZERO = (3/5) Gamma(6/5) / (2 pi)
+    for (int i = 0; i < nused; ++i) { xs[i + 1] = exp(-3. + i * dlogr); ys[i + 1] = vals[i]; }
+    natural_spline(xs, ys, zs, cs, N);
+    for (int i = 0; i < N; ++i) nodes[i] = make_double4(xs[i], ys[i], zs[i], 0.);
+    out[1] = N;
 }
 
 // kV2 for the Moffat maxk solve (MoffatMaxKSolver, SBMoffat.cpp:481-520), normalised to 1
@@ -1474,43 +1491,86 @@ int moffat_scale_radius(int count, const double* h_in, double* h_out, cudaStream
     return GSB_OK;
 }
 
-int kolmogorov_stepk(const gsb_gsparams* gsp, cudaStream_t stream, double* out)
+// The Kolmogorov radial spline of each device (its GSParams are those of the stepk cached in
+// the device state).
+namespace {
+struct KolmRadial {
+    double4* nodes = nullptr;
+    int n = 0, cap = 0;
+};
+KolmRadial g_kolm_radial[64];
+}  // namespace
+
+static int kolmogorov_build(const gsb_gsparams* gsp, cudaStream_t stream)
 {
     DeviceState* st = device_state();
+    int dev = 0;
+    cudaGetDevice(&dev);
+    KolmRadial& kr = g_kolm_radial[dev & 63];
     const double key[13] = {double(gsp->minimum_fft_size), double(gsp->maximum_fft_size),
                             gsp->folding_threshold, gsp->stepk_minimum_hlr, gsp->maxk_threshold,
                             gsp->kvalue_accuracy, gsp->xvalue_accuracy, gsp->table_spacing,
                             gsp->realspace_relerr, gsp->realspace_abserr, gsp->integration_relerr,
                             gsp->integration_abserr, gsp->shoot_accuracy};
-    if (st->kolm_valid && std::equal(key, key + 13, st->kolm_key)) { *out = st->kolm_stepk; return GSB_OK; }
+    if (st->kolm_valid && std::equal(key, key + 13, st->kolm_key)) return GSB_OK;
     const double dlogr = gsp->table_spacing * std::sqrt(std::sqrt(gsp->xvalue_accuracy / 10.));
     int ncand = 0;
     for (double logr = -3.; logr < std::log(1.e4); logr += dlogr) ++ncand;
+    if (ncand + 1 > kr.cap) {
+        cudaFree(kr.nodes);
+        kr.nodes = nullptr;
+        kr.cap = 0;
+        GSB_CUDA_CHECK(cudaMalloc(&kr.nodes, sizeof(double4) * (ncand + 1)));
+        kr.cap = ncand + 1;
+    }
     double* d_vals = nullptr;
     int* d_status = nullptr;
     double* d_out = nullptr;
+    double* d_scratch = nullptr;
     GSB_CUDA_CHECK(cudaMallocAsync(&d_vals, sizeof(double) * ncand, stream));
     GSB_CUDA_CHECK(cudaMallocAsync(&d_status, sizeof(int), stream));
-    GSB_CUDA_CHECK(cudaMallocAsync(&d_out, sizeof(double), stream));
+    GSB_CUDA_CHECK(cudaMallocAsync(&d_out, sizeof(double) * 2, stream));
+    GSB_CUDA_CHECK(cudaMallocAsync(&d_scratch, sizeof(double) * 4 * (ncand + 1), stream));
     GSB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), stream));
     kolmogorov_nodes_kernel<<<(ncand * 32 + 255) / 256, 256, 0, stream>>>(ncand, dlogr, *gsp, st->og,
                                                                           d_vals, d_status);
     GSB_CUDA_CHECK(cudaGetLastError());
-    kolmogorov_finalize_kernel<<<1, 1, 0, stream>>>(ncand, dlogr, *gsp, d_vals, d_out);
+    kolmogorov_finalize_kernel<<<1, 1, 0, stream>>>(ncand, dlogr, *gsp, d_vals, d_out, kr.nodes, d_scratch);
     GSB_CUDA_CHECK(cudaGetLastError());
-    double h_out = 0.;
+    double h_out[2] = {0., 0.};
     int h_status = 0;
-    GSB_CUDA_CHECK(cudaMemcpyAsync(&h_out, d_out, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    GSB_CUDA_CHECK(cudaMemcpyAsync(h_out, d_out, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
     GSB_CUDA_CHECK(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
     GSB_CUDA_CHECK(cudaFreeAsync(d_vals, stream));
     GSB_CUDA_CHECK(cudaFreeAsync(d_status, stream));
     GSB_CUDA_CHECK(cudaFreeAsync(d_out, stream));
+    GSB_CUDA_CHECK(cudaFreeAsync(d_scratch, stream));
     GSB_CUDA_CHECK(cudaStreamSynchronize(stream));
     if (h_status) return set_error(GSB_ERR_NUMERIC, "Kolmogorov Hankel transform did not converge");
     std::copy(key, key + 13, st->kolm_key);
-    st->kolm_stepk = h_out;
+    st->kolm_stepk = h_out[0];
+    kr.n = int(h_out[1]);
     st->kolm_valid = true;
-    *out = h_out;
+    return GSB_OK;
+}
+
+int kolmogorov_stepk(const gsb_gsparams* gsp, cudaStream_t stream, double* out)
+{
+    const int rc = kolmogorov_build(gsp, stream);
+    if (rc) return rc;
+    *out = device_state()->kolm_stepk;
+    return GSB_OK;
+}
+
+// The radial spline nodes (r, f, y2, 0) of KolmogorovInfo for these GSParams (gsb_real.cu).
+int kolmogorov_radial(const gsb_gsparams* gsp, cudaStream_t stream, const double4** nodes, int* n)
+{
+    const int rc = kolmogorov_build(gsp, stream);
+    if (rc) return rc;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    *nodes = g_kolm_radial[dev & 63].nodes;
+    *n = g_kolm_radial[dev & 63].n;
     return GSB_OK;
 }
 

@@ -137,9 +137,38 @@ class GSObject(object):
 
     def withScaledFlux(self, flux_ratio):
         from .compound import Transform
+        from .sed import SED
+        if isinstance(flux_ratio, SED):
+            # obj * SED: a separable chromatic object (gsobject.py:799-838, transform.py:76-83)
+            from .chromatic import SimpleChromaticTransformation
+            return SimpleChromaticTransformation(self, flux_ratio)
+        if hasattr(flux_ratio, '__call__'):
+            raise TypeError('callable flux_ratio must be an SED.')
         if np.ndim(flux_ratio) == 0 and flux_ratio == 1:
             return self
         return Transform(self, flux_ratio=flux_ratio)
+
+    # -- duck typing as a ChromaticObject (gsobject.py:427-454) --------------------------------
+    separable = property(lambda self: True)
+    interpolated = property(lambda self: False)
+    deinterpolated = property(lambda self: self)
+    spectral = property(lambda self: False)
+    dimensionless = property(lambda self: True)
+    wave_list = property(lambda self: np.array([], dtype=float))
+
+    @property
+    def sed(self):
+        from .sed import SED
+        return SED(float(self.flux), 'nm', '1')
+
+    def _fiducial_profile(self, bandpass):
+        return bandpass.effective_wavelength, self
+
+    def evaluateAtWavelength(self, wave):
+        return self
+
+    def _approxWavelength(self, wave):
+        return wave, self
 
     def expand(self, scale):
         from .compound import Transform
@@ -415,10 +444,40 @@ class GSObject(object):
         imview._shift(-image.center)
         imview.wcs = PixelScale(1.0)
         if prof.is_analytic_x:
-            raise GalSimNotImplementedError("real-space drawing (drawReal) is not part of the FFT path")
-        added_photons = prof.drawFFT(imview, add_to_image, precision=precision)
+            # method 'no_pixel' / 'sb' on a profile analytic in real space (gsobject.py:1810-1811)
+            added_photons = prof.drawReal(imview, add_to_image)
+        else:
+            added_photons = prof.drawFFT(imview, add_to_image, precision=precision)
         image.added_flux = added_photons / flux_scale
         return image
+
+    def drawReal(self, image, add_to_image=False):
+        """The profile sampled at the pixel centres of an image with a PixelScale wcs, times the
+        pixel area (gsobject.py:1846-1889), drawn on the GPU (gsb_draw_real).  Returns the total
+        flux drawn."""
+        import torch
+        from .compound import _Transform
+        from .realspace import draw_real_stamps
+        if image.wcs is None or not image.wcs._isPixelScale:
+            raise GalSimValueError("drawReal requires an image with a PixelScale wcs", image)
+        if self._batch != 1:
+            raise GalSimIncompatibleValuesError(
+                "drawReal draws one profile; use galsim_b200.draw_batch for batched parameters")
+        if image.dtype not in (np.float32, np.float64):
+            raise GalSimNotImplementedError("drawReal into an image of dtype %s" % image.dtype)
+        scale = image.scale
+        prof = self if scale == 1. else _Transform(self, jac=np.array([[1. / scale, 0.], [0., 1. / scale]]),
+                                                    flux_ratio=scale ** 2)
+        b = image.bounds
+        nx, ny = b.xmax - b.xmin + 1, b.ymax - b.ymin + 1
+        init = None
+        if add_to_image:
+            init = torch.from_numpy(np.ascontiguousarray(image.array).reshape(-1).copy()).to(
+                _lib.Device.torch_device())
+        out, _, flux = draw_real_stamps(prof, 1, self.gsparams, [b.xmin], [b.ymin], [nx], [ny], image.dtype,
+                                        init=init)
+        image.array[...] = out.cpu().numpy().reshape(image.array.shape)
+        return float(flux[0].item())
 
     def drawFFT(self, image, add_to_image=False, precision='fp32'):
         """Draw by k-space evaluation and FFT into an image with a PixelScale wcs, centred on

@@ -260,6 +260,48 @@ int gsb_images_build(gsb_tables* t, int count, const gsb_image_desc* h_desc, con
 /* Copy per image (R, maxk) back (2 doubles per image; 0 where not computed). */
 int gsb_images_info(const gsb_tables* t, double* h_out, int count, void* stream);
 
+/* Real-space drawing ----------------------------------------------------------------------- */
+/* One leaf of a profile drawn in real space (drawReal: method 'no_pixel' or 'sb' on a profile
+ * that is analytic in real space, gsobject.py:1810-1811, 1846-1889).  The reference walks the
+ * tree with _drawReal (transform.py:571-583, sum.py:304-310), composing each Transformation's
+ * Jacobian, offset and flux scaling, and draws every leaf with SBProfile::draw
+ * (src/SBProfile.cpp:305-383); a gsb_xleaf holds one leaf with that composition. */
+typedef struct gsb_xleaf {
+    double jac[4];       /* composed Jacobian [A, B, C, D] (image = jac . profile), used when
+                            flags & GSB_XLEAF_JAC */
+    double xoff, yoff;   /* composed offset of the profile centre (image pixels) */
+    double flux_ratio;   /* composed flux scaling |det| x flux_ratio (SBProfile::draw's flux_ratio) */
+    double flux;         /* the leaf's flux */
+    double p[3];         /* as gsb_leaf.p (Sersic: p[1] the scale radius; a truncated Sersic's
+                            flux is that of the truncated profile) */
+    int32_t type;        /* GSB_GAUSSIAN .. GSB_BOX (not GSB_INTERPOLATED) */
+    int32_t flags;
+} gsb_xleaf;
+
+#define GSB_XLEAF_JAC 1
+
+/* Draw n_stamps stamps of n_leaves real-space leaves each (d_leaves stamp-major): pixel (i, j)
+ * of stamp s samples the sum of the leaves at image position (xmin + i, ymin + j) (the
+ * stamp's bounds relative to its centre, as gsb_draw_images), each leaf's value being
+ * flux_ratio x its xValue at jac^-1 ((x, y) - (xoff, yoff)) (SBGaussian.cpp:99-103,
+ * SBExponential.cpp:99-103, SBSersic.cpp:92-96 and 357-361, SBMoffat.cpp:256-261,
+ * SBKolmogorov.cpp:108-115 with KolmogorovInfo's radial spline, SBAiry.cpp:88-117 and
+ * 410-428, SBBox.cpp:79-150), in FP64, stored as out_dtype; add_to_image adds to the output.
+ * d_added_flux (optional) receives per stamp the FP64 sum of the drawn (rounded) values. */
+int gsb_draw_real(int n_leaves, int n_stamps, const gsb_gsparams* gsp, const gsb_xleaf* d_leaves,
+                  const gsb_stamp* d_stamps, void* d_out, int out_dtype, int add_to_image,
+                  double* d_added_flux, void* stream);
+
+/* Chromatic drawing ---------------------------------------------------------------------- */
+/* The wavelength integral of chromatic drawing (the integrators' IntegrationRule.__call__,
+ * galsim/integ.py:134-146): out[p] = sum_s w[s] * stamp_s[p] over n_stamps stamps of npix
+ * pixels each, stamp s starting at element d_offsets[s] of d_flat (the monochromatic images
+ * drawn at the integration wavelengths, e.g. one gsb_draw_images batch); FP64 accumulation,
+ * in / out dtypes GSB_F32 or GSB_F64.  All pointers are device memory. */
+int gsb_weighted_stamp_sum(const void* d_flat, int in_dtype, const int64_t* d_offsets,
+                           const double* d_weights, int n_stamps, int64_t npix, void* d_out,
+                           int out_dtype, void* stream);
+
 /* Noise ---------------------------------------------------------------------------------- */
 /* GaussianNoise, PoissonNoise and CCDNoise applied to stamps in device memory with the
  * reference's random streams (galsim/noise.py:259-263, 331-356, 463-486; src/Random.cpp).  Each

@@ -462,7 +462,10 @@ def sersic_truncated_scale(n, hlr, trunc):
 _KOLM = {}
 
 
-def kolmogorov_stepk_factor(gsp=DEFAULT):
+def _kolmogorov_info(gsp):
+    """KolmogorovInfo (SBKolmogorov.cpp:338-420): the radial table f(r) = hankel(exp(-k^5/3), r)
+    / 2 pi at r = 0 (XVAL_ZERO) and r = exp(-3 + i dlogr) until f r^2 / 1.67 < shoot_accuracy / 2 pi,
+    its natural spline, and stepk in units of k0."""
     if id(gsp) in _KOLM:
         return _KOLM[id(gsp)]
     dlogr = gsp.table_spacing * math.sqrt(math.sqrt(gsp.xvalue_accuracy / 10.))
@@ -470,9 +473,12 @@ def kolmogorov_stepk_factor(gsp=DEFAULT):
     f = lambda k: np.exp(-np.power(k, 5. / 3.))
     i = 0
     r1 = F1 = 0.
+    rs, vs = [0.], [0.0876786563672346]
     while -3. + i * dlogr < math.log(1.e4):
         r = math.exp(-3. + i * dlogr)
         val = hankel_inf(f, r, gsp.integration_relerr, gsp.integration_abserr) / (2. * PI)
+        rs.append(r)
+        vs.append(val)
         r1, F1 = r, val
         if val * r * r / 1.67 < thresh:
             break
@@ -480,8 +486,19 @@ def kolmogorov_stepk_factor(gsp=DEFAULT):
     nn = 11. / 3.
     R = (2. * PI * F1 * r1 ** nn / ((nn - 2.) * gsp.folding_threshold)) ** (1. / (nn - 2.))
     R = max(R, gsp.stepk_minimum_hlr * 2.992939911888651 * 0.5548101137)
-    _KOLM[id(gsp)] = PI / R
-    return PI / R
+    _KOLM[id(gsp)] = (PI / R, Spline(rs, vs))
+    return _KOLM[id(gsp)]
+
+
+def kolmogorov_stepk_factor(gsp=DEFAULT):
+    return _kolmogorov_info(gsp)[0]
+
+
+def kolmogorov_radial(r, gsp=DEFAULT):
+    """KolmogorovInfo::xValue (SBKolmogorov.cpp:114-115): the radial spline, 0 beyond its last node."""
+    sp = _kolmogorov_info(gsp)[1]
+    r = np.asarray(r, float)
+    return np.where(r < sp.x[-1], sp(np.minimum(r, sp.x[-1])), 0.)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -1414,6 +1431,134 @@ def draw_image(prof, nx, ny, scale, offset=(0., 0.), method='fft', use_true_cent
     cy = 1 + ny // 2
     bounds = (1 - cx, nx - cx, 1 - cy, ny - cy)
     return draw_fft(img_prof, bounds, gsp)
+
+
+# ---------------------------------------------------------------------------------------------
+# Real-space drawing (drawReal: gsobject.py:1846-1898; transform.py:571-583; sum.py:304-310;
+# SBProfile::draw, SBProfile.cpp:305-383; the profiles' xValue / fillXImage)
+# ---------------------------------------------------------------------------------------------
+def _leaf_xvalue(leaf, u, v):
+    gsp = leaf.gsp
+    if isinstance(leaf, OGaussian):                       # SBGaussian.cpp:57-69, 99-103
+        iss = (1. / leaf.sigma) ** 2
+        return leaf.flux * iss / (2. * PI) * np.exp(-0.5 * (u * u + v * v) * iss)
+    if isinstance(leaf, OExponential):                    # SBExponential.cpp:67-82, 99-103
+        ir = 1. / leaf.r0
+        return (leaf.flux / (2. * PI)) * (ir * ir) * np.exp(-np.sqrt(u * u + v * v) * ir)
+    if isinstance(leaf, OSersic):                         # SBSersic.cpp:71-96, 354-361
+        n, r0 = leaf.n, leaf.r0
+        ff = leaf.info.flux_fraction if leaf.trunc > 0. else 1.
+        ir2 = (1. / r0) ** 2
+        xnorm = leaf.flux * (1. / (2. * PI * n * math.gamma(2. * n) * ff)) * ir2
+        rsq = (u * u + v * v) * ir2
+        val = xnorm * np.exp(-np.power(rsq, 1. / (2. * n)))
+        if leaf.trunc > 0.:
+            val = np.where(rsq > (leaf.trunc / r0) ** 2, 0., val)
+        return val
+    if isinstance(leaf, OMoffat):                         # SBMoffat.cpp:163-203, 256-261
+        b, rD = leaf.beta, leaf.r0
+        if leaf.trunc > 0.:
+            maxRrD = leaf.trunc / rD
+            ff = 1. - (1. + maxRrD * maxRrD) ** (1. - b)
+        else:
+            ff = 1.
+            maxRrD = math.sqrt(gsp.xvalue_accuracy ** (1. / (1. - b)) - 1.)
+        norm = leaf.flux * (b - 1.) / (PI * ff * rD * rD)
+        rsq = (u * u + v * v) / (rD * rD)
+        return np.where(rsq > maxRrD * maxRrD, 0., norm * np.power(1. + rsq, -b))
+    if isinstance(leaf, OKolmogorov):                     # SBKolmogorov.cpp:85-115
+        k0 = leaf.k0
+        return leaf.flux * k0 * k0 * kolmogorov_radial(np.sqrt(u * u + v * v) * k0, gsp)
+    if isinstance(leaf, OAiry):                           # SBAiry.cpp:66-117, 392-428
+        D = 1. / leaf.lod
+        obs = leaf.obs
+        nu = np.sqrt(u * u + v * v) * D * PI
+        thresh = math.sqrt(8. * gsp.xvalue_accuracy)
+        with np.errstate(invalid='ignore', divide='ignore'):
+            if obs == 0.:
+                x = np.where(nu < thresh, 0.5, special.j1(nu) / nu)
+                norm = PI
+            else:
+                x = np.where(nu < thresh, 0.5 * (1. - obs * obs),
+                             (special.j1(nu) - obs * special.j1(obs * nu)) / nu)
+                norm = PI / (1. - obs * obs)
+        return leaf.flux * D * D * (x * x * norm)
+    raise NotImplementedError(type(leaf).__name__)
+
+
+def draw_real_leaf(leaf, nx, ny, xmin, ymin, jac, xoff, yoff, flux_ratio):
+    """SBProfile::draw with imscale 1 for one leaf: the image positions xmin + i, ymin + j."""
+    x0, y0 = xmin - xoff, ymin - yoff
+    i = np.arange(nx)[None, :].astype(float)
+    j = np.arange(ny)[:, None].astype(float)
+    amp = flux_ratio
+    if jac is None:
+        mode, u0, du, duy, v0, dv, dvx = 0, x0, 1., 0., y0, 1., 0.
+    elif jac[0, 1] == 0. and jac[1, 0] == 0.:
+        xs, ys = 1. / jac[0, 0], 1. / jac[1, 1]
+        mode, u0, du, duy, v0, dv, dvx = 1, x0 * xs, xs, 0., y0 * ys, ys, 0.
+        amp *= abs(xs * ys)
+    else:
+        A, B, C, D = jac[0, 0], jac[0, 1], jac[1, 0], jac[1, 1]
+        invdet = 1. / (A * D - B * C)
+        mode = 2
+        u0, v0 = (D * x0 - B * y0) * invdet, (-C * x0 + A * y0) * invdet
+        du, duy, dv, dvx = D * invdet, -B * invdet, A * invdet, -C * invdet
+        amp *= abs(invdet)
+    if isinstance(leaf, OBox):                            # SBBox.cpp:79-150
+        norm = leaf.flux / (leaf.w * leaf.h)
+        if mode <= 1:
+            bx0, by0 = u0 / du, v0 / dv
+            wo2, ho2 = 0.5 * leaf.w / abs(du), 0.5 * leaf.h / abs(dv)
+            inside = ((i >= np.ceil(-wo2 - bx0)) & (i < np.ceil(wo2 - bx0)) &
+                      (j >= np.ceil(-ho2 - by0)) & (j < np.ceil(ho2 - by0)))
+        else:
+            x = u0 + i * du + j * duy
+            y = v0 + j * dv + i * dvx
+            inside = (np.abs(x) < 0.5 * leaf.w) & (np.abs(y) < 0.5 * leaf.h)
+        return amp * np.where(inside, norm, 0.)
+    u = u0 + i * du + j * duy
+    v = v0 + j * dv + i * dvx
+    return amp * _leaf_xvalue(leaf, u, v)
+
+
+def draw_real(obj, nx, ny, xmin, ymin, jac=None, offset=(0., 0.), flux_scaling=1.):
+    """The _drawReal walk (transform.py:571-583, sum.py:304-310) summed in FP64."""
+    if isinstance(obj, OTransform):
+        dx, dy = offset
+        if obj.dx != 0. or obj.dy != 0.:
+            if jac is not None:
+                x1 = jac[0, 0] * obj.dx + jac[0, 1] * obj.dy
+                y1 = jac[1, 0] * obj.dx + jac[1, 1] * obj.dy
+            else:
+                x1, y1 = obj.dx, obj.dy
+            dx += x1
+            dy += y1
+        flux_scaling *= abs(obj.det()) * obj.flux_ratio
+        jac = obj.jac if jac is None else jac if obj.jac is None else jac.dot(obj.jac)
+        return draw_real(obj.original, nx, ny, xmin, ymin, jac, (dx, dy), flux_scaling)
+    if isinstance(obj, OSum):
+        return sum(draw_real(o, nx, ny, xmin, ymin, jac, offset, flux_scaling) for o in obj.objs)
+    return draw_real_leaf(obj, nx, ny, xmin, ymin, jac, offset[0], offset[1], flux_scaling)
+
+
+def draw_image_real(prof, nx, ny, scale, offset=(0., 0.), method='no_pixel', use_true_center=True):
+    """drawImage(method='no_pixel' | 'sb') of a profile analytic in real space (gsobject.py:
+    1647-1811 with drawReal).  Returns (array, added_flux)."""
+    dx, dy = float(offset[0]), float(offset[1])
+    if use_true_center:
+        if nx % 2 == 0:
+            dx -= 0.5
+        if ny % 2 == 0:
+            dy -= 0.5
+    inv = 1. / scale
+    jac = None if scale == 1. else np.array([[inv, 0.], [0., inv]])
+    fr = scale ** 2 / (scale * scale if method == 'sb' else 1.)
+    img_prof = OTransform(prof, jac=jac, offset=(dx, dy), flux_ratio=fr)
+    xmin, ymin = -(nx // 2), -(ny // 2)
+    arr = draw_real(img_prof, nx, ny, xmin, ymin)
+    flux_scale = 1. / (scale * scale) if method == 'sb' else 1.
+    return arr, float(arr.sum()) / flux_scale
 
 
 def draw_kimage(obj, nkx, nky, kxmin, kymin, dk):

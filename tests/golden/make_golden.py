@@ -653,6 +653,67 @@ def main_trunc(ref_root):
     print('wrote', os.path.join(HERE, 'reference_trunc.npz'), len(out), 'arrays')
 
 
+# Real-space drawing (drawImage with method 'no_pixel' / 'sb' on profiles analytic in real
+# space: GSObject.drawReal, gsobject.py:1846-1898, SBProfile::draw).
+REAL_CASES = [
+    # (name, spec, nx, ny, scale, dtype, method, offset)
+    ('r_gauss_f8', ('gauss', 0.7, 10.), 32, 32, 0.2, 'f8', 'no_pixel', (0., 0.)),
+    ('r_exp_shear_f4', ('shear', 0.2, -0.1, ('exp', 0.6, 50.)), 33, 31, 0.2, 'f4', 'no_pixel', (0.3, -0.2)),
+    ('r_sersic_f8', ('sersic', 2.5, 0.5, 20.), 40, 40, 0.1, 'f8', 'no_pixel', (0., 0.)),
+    ('r_sersict_f8', ('sersict', 3.0, 0.4, 8., 1.5, False, 'hlr'), 40, 40, 0.1, 'f8', 'sb', (0.1, 0.)),
+    ('r_moffat_f8', ('moffat', 3.5, 0.8, 5.), 32, 32, 0.2, 'f8', 'no_pixel', (0., 0.25)),
+    ('r_moffatt_f4', ('moffatt', 2.0, 0.5, 3., 1.2, 'r0'), 32, 32, 0.1, 'f4', 'no_pixel', (0., 0.)),
+    ('r_kolm_f8', ('kolmogorov', 0.7, 4.), 48, 48, 0.1, 'f8', 'no_pixel', (0., 0.)),
+    ('r_kolm_dilate_shift_f4', ('shift', 0.05, -0.03, ('dilate', 1.1, ('kolmogorov', 0.6, 2.))), 40, 40, 0.08,
+     'f4', 'no_pixel', (0., 0.)),
+    ('r_airy_obs_f8', ('airy', 0.2, 0.3, 1.), 40, 40, 0.05, 'f8', 'no_pixel', (0., 0.)),
+    ('r_airy_f8', ('rotate', 20., ('airy', 0.25, 0.0, 2.)), 40, 40, 0.05, 'f8', 'no_pixel', (0.2, 0.)),
+    ('r_box_f8', ('box', 1.05, 0.7, 3.), 16, 16, 0.2, 'f8', 'no_pixel', (0., 0.)),
+    ('r_box_rot_f8', ('rotate', 30., ('box', 1.3, 0.9, 3.)), 16, 16, 0.2, 'f8', 'no_pixel', (0.1, 0.1)),
+    ('r_sum_f8', ('sum', [('gauss', 0.5, 3.), ('shift', 0.3, 0.2, ('exp', 0.4, 2.)),
+                          ('shear', 0.1, 0.3, ('moffat', 2.5, 0.6, 1.))]), 36, 36, 0.15, 'f8', 'no_pixel', (0., 0.)),
+]
+
+
+def main_real(ref_root):
+    from ref_import import import_reference_galsim
+    galsim = import_reference_galsim(ref_root)
+    out = {}
+    for name, spec, nx, ny, scale, dt, method, off in REAL_CASES:
+        im = profile(galsim, spec).drawImage(nx=nx, ny=ny, scale=scale, dtype=np.dtype(dt).type, method=method,
+                                             offset=off)
+        out['draw_' + name] = im.array
+        out['draw_' + name + '_flux'] = np.array(im.added_flux)
+    np.savez_compressed(os.path.join(HERE, 'reference_real.npz'), **out)
+    print('wrote', os.path.join(HERE, 'reference_real.npz'), len(out), 'arrays')
+
+
+def main_chromatic(ref_root):
+    """Chromatic drawing through bandpasses (chromatic.py) and the host-side numbers it uses."""
+    import chromatic_cases as CC
+    from ref_import import import_reference_galsim
+    galsim = import_reference_galsim(ref_root)
+    out = {}
+    for name in CC.CASES:
+        im = CC.draw(galsim, name)
+        out['draw_' + name] = im.array
+        out['draw_' + name + '_flux'] = np.array(getattr(im, 'added_flux', np.nan))
+    s1, s2 = CC.seds(galsim)
+    b1, b2 = CC.bandpasses(galsim)
+    out['effective_wavelength'] = np.array([b1.effective_wavelength, b2.effective_wavelength])
+    out['sed_flux'] = np.array([s1.calculateFlux(b1), s2.calculateFlux(b2), s1.atRedshift(0.3).calculateFlux(b1),
+                                s2.atRedshift(0.3).calculateFlux(b2), (s1 * 2.5).calculateFlux(b2)])
+    waves = np.linspace(400., 600., 37)
+    out['sed_values'] = np.array([s1(waves), s2(waves), s1.atRedshift(0.3)(waves)])
+    out['bp_values'] = np.array([b1(waves), b2(np.linspace(540., 720., 37))])
+    w = np.array(CC.REFRACTION_WAVES)
+    out['refraction'] = np.array([galsim.dcr.get_refraction(w, 30. * galsim.degrees),
+                                  galsim.dcr.get_refraction(w, 45. * galsim.degrees, temperature=280.,
+                                                            pressure=75.)])
+    np.savez_compressed(os.path.join(HERE, 'reference_chromatic.npz'), **out)
+    print('wrote', os.path.join(HERE, 'reference_chromatic.npz'), len(out), 'arrays')
+
+
 def main(ref_root):
     from ref_import import import_reference_galsim
     galsim = import_reference_galsim(ref_root)
@@ -720,6 +781,10 @@ if __name__ == '__main__':
         main_standalone(root)
     elif '--trunc-only' in sys.argv:
         main_trunc(root)
+    elif '--chromatic-only' in sys.argv:
+        main_chromatic(root)
+    elif '--real-only' in sys.argv:
+        main_real(root)
     else:
         if '--large-only' not in sys.argv:
             main(root)
@@ -732,3 +797,5 @@ if __name__ == '__main__':
         main_configs(root)
         main_standalone(root)
         main_trunc(root)
+        main_chromatic(root)
+        main_real(root)

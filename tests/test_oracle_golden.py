@@ -209,3 +209,18 @@ def test_truncated_moffat_kimage_matches_reference(case):
     kim = O.draw_kimage(specs.oracle_profile(spec), n, n, -(n // 2), -(n // 2), dk)
     ref = TRUNC['kimg_' + name]
     assert np.abs(kim - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+REAL = np.load(specs.HERE + '/reference_real.npz')
+
+
+@pytest.mark.parametrize('case', MG.REAL_CASES, ids=[c[0] for c in MG.REAL_CASES])
+def test_real_space_draw_matches_reference(case):
+    """drawImage with method 'no_pixel' / 'sb' on analytic profiles (drawReal): the oracle's
+    restatement of the _drawReal walk and the profiles' xValues against the reference."""
+    name, spec, nx, ny, scale, dt, method, off = case
+    arr, flux = O.draw_image_real(specs.oracle_profile(spec), nx, ny, scale, off, method)
+    ref = REAL['draw_' + name]
+    tol = 2e-7 if dt == 'f4' else (1e-10 if 'kolm' in name else 1e-12)
+    assert np.abs(arr.astype(ref.dtype).astype(float) - ref).max() <= tol * np.abs(ref).max(), name
+    assert abs(flux - float(REAL['draw_' + name + '_flux'])) <= max(tol, 1e-7 if dt == 'f4' else 0) * abs(flux)
