@@ -1,13 +1,16 @@
 """galsim_b200: GalSim's FFT drawing path on NVIDIA B200 (sm_100a).
 
 A drop-in for ``GSObject.drawImage(method='fft')`` and ``drawKImage`` on
-Convolve / Sum / Transform trees of Gaussian, Exponential, Sersic, Moffat, Kolmogorov, Airy,
-Box / Pixel and InterpolatedImage, the reference's Gaussian / Poisson / CCD noise applied
-on the device, and FITS files of Images and stamp batches (galsim_b200.fits; a batch's file
-image is assembled on the device).  The host code here mirrors the reference's Python API; every numerical
-step of drawing (FP64 sizing and Sersic tables, k-space evaluation, Hermitian wrap, inverse
-FFT, crop and flux sum) runs in the hand-written CUDA kernels of libgsb.so, called through
-the C ABI declared in include/gsb.h.  There is no CPU fallback.
+Convolve / Sum / Transform trees of Gaussian, Exponential, Sersic, Moffat (both also
+truncated), Kolmogorov, Airy, Box / Pixel and InterpolatedImage, real-space drawing of analytic
+profiles ('no_pixel' / 'sb'), chromatic objects drawn through bandpasses (SED, Bandpass,
+ChromaticAtmosphere, chromatic sums and convolutions), the reference's Gaussian / Poisson / CCD
+noise applied on the device, and FITS files of Images and stamp batches (galsim_b200.fits; a
+batch's file image is assembled on the device).  The host code here mirrors the reference's
+Python API; every numerical step of drawing (FP64 sizing and FT tables, k-space evaluation,
+Hermitian wrap, inverse FFT, crop and flux sum, real-space evaluation, wavelength integrals of
+images) runs in the hand-written CUDA kernels of libgsb.so, called through the C ABI declared in
+include/gsb.h.  There is no CPU fallback.
 """
 from .errors import *
 from .gsparams import GSParams

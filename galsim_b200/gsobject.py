@@ -1,9 +1,11 @@
 """GSObject: the base class of every surface-brightness profile (galsim/gsobject.py).
 
-Drawing goes through the GPU: ``drawImage(method='fft')`` (also 'auto' and, for profiles
-that are not analytic in real space, 'no_pixel' / 'sb') and ``drawKImage``.  Real-space
-drawing and photon shooting are not part of this package and raise
-GalSimNotImplementedError.
+Drawing goes through the GPU: ``drawImage(method='fft')`` (also 'auto'), 'no_pixel' / 'sb'
+(by FFT for profiles that are not analytic in real space, by real-space evaluation --
+``drawReal`` -- for sums and transformations of analytic leaves, as the reference chooses) and
+``drawKImage``.  Real-space convolution and photon shooting are not part of this package and
+raise GalSimNotImplementedError.  Multiplying by an SED makes a chromatic object
+(galsim_b200.chromatic).
 
 Parameters of the leaf profiles may be numpy arrays: such an object stands for a batch of
 profiles (one per array element) with the same tree structure, and is drawn with
