@@ -212,6 +212,61 @@ def run_mixed(galsim, dev, steps, warmup):
             'gsparams': 'minimum_fft_size=32', 'fft_sizes': dict(zip(map(int, u), map(int, c)))}
 
 
+# Chromatic stage: a bulge + disk batch with one SED per component (tabulated, photons/nm),
+# convolved with an atmospheric PSF whose size and centroid depend on wavelength, drawn through a
+# tabulated bandpass.  Synthetic spectra and throughput stand in for the reference's share/ files.
+CHROM_B = 4096
+CHROM_SED_BULGE = ([300., 400., 500., 600., 700., 800., 900., 1100.], [0.3, 0.6, 1.0, 1.4, 1.6, 1.7, 1.7, 1.6])
+CHROM_SED_DISK = ([300., 400., 500., 600., 700., 800., 900., 1100.], [2.0, 1.8, 1.4, 1.1, 0.9, 0.8, 0.7, 0.6])
+CHROM_BP = ([400., 420., 440., 460., 480., 500., 520., 540., 560., 580., 600.],
+            [0.0, 0.35, 0.62, 0.71, 0.74, 0.76, 0.75, 0.70, 0.52, 0.2, 0.0])
+
+
+def chromatic_object(galsim, m):
+    sb = galsim.SED(galsim.LookupTable(*CHROM_SED_BULGE, interpolant='linear'), 'nm', 'fphotons')
+    sd = galsim.SED(galsim.LookupTable(*CHROM_SED_DISK, interpolant='linear'), 'nm', 'fphotons')
+    bulge = galsim.Sersic(n=4., half_light_radius=m['bh'], flux=m['flux'] * m['bf'] * 1e-2) \
+        .shear(g1=m['g_b'][:, 0], g2=m['g_b'][:, 1]) * sb
+    disk = galsim.Exponential(half_light_radius=m['dh'], flux=m['flux'] * (1. - m['bf']) * 1e-2) \
+        .shear(g1=m['g_d'][:, 0], g2=m['g_d'][:, 1]) * sd
+    psf = galsim.ChromaticAtmosphere(galsim.Kolmogorov(fwhm=0.7), 500., zenith_angle=30. * galsim.degrees,
+                                     parallactic_angle=20. * galsim.degrees)
+    bp = galsim.Bandpass(galsim.LookupTable(*CHROM_BP, interpolant='linear'), 'nm')
+    return galsim.Convolve(galsim.Add(bulge, disk), psf), bp
+
+
+def run_chromatic(galsim, dev, steps, warmup):
+    """Chromatic batch: 4096 bulge + disk galaxies (two SEDs) through ChromaticAtmosphere and a
+    bandpass, 32 x 32 stamps.  One step = both terms' effective PSFs (their wavelengths drawn in
+    real space as one batch each, integrated on the device, turned into InterpolatedImages) and
+    the two batched galaxy draws, summed on the device."""
+    import torch
+    m = mixed_params(CHROM_B, seed=1357)
+    obj, bp = chromatic_object(galsim, m)
+
+    def step():
+        return galsim.draw_batch(obj, nx=32, ny=32, scale=SCALE, bandpass=bp)
+
+    for _ in range(warmup):
+        st = step()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        st = step()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    from galsim_b200.sed import combine_wave_list
+    return {'value': CHROM_B / (ms * 1e-3), 'unit': 'stamps/s', 'ms_per_step': ms, 'stamps': CHROM_B,
+            'wavelengths_per_integral': int(len(combine_wave_list(obj.obj_list[1] * obj.obj_list[0].obj_list[0].sed,
+                                                                  bp)[0])),
+            'workload': 'bulge_disk_2sed_chromatic_atmosphere_kolmogorov_32x32_4096_seed1357',
+            'timed': 'galsim_b200.draw_batch(chromatic object, bandpass): effective PSFs + batched draws '
+                     '(host orchestration included)',
+            'flux_check': float(np.median(st.added_flux))}
+
+
 def _ref_noise_worker(args):
     stamps, seeds = args
     sys.path.insert(0, os.path.join(ROOT, 'oracle'))
@@ -809,6 +864,10 @@ def run_stage(args):
     params = workload_params(args.stamps)
     obj = gpu_object(galsim, params)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.stage == 'chromatic':
+        print(json.dumps({'stage': 'chromatic', **run_chromatic(galsim, _lib.Device.torch_device(), args.steps,
+                                                                  max(args.warmup, 1))}))
+        return
     if args.stage == 'fit':
         from galsim_b200 import autodiff
         psf = galsim.Convolve(galsim.Moffat(beta=2.5, fwhm=0.8), galsim.Pixel(SCALE))
@@ -1043,6 +1102,7 @@ def run_gpu(args):
     fit = run_fit_step(args, galsim, dev, max(args.steps, 3), max(args.warmup, 2))
     mixed = run_mixed(galsim, dev, max(args.steps, 3), max(args.warmup, 2)) if not args.no_extra else None
     large = run_large(galsim, dev) if not args.no_extra else None
+    chrom = run_chromatic(galsim, dev, max(args.steps, 3), max(args.warmup, 2)) if not args.no_extra else None
     interp = (run_interp(galsim, dev, params, max(args.steps, 3), max(args.warmup, 2),
                          cpu=(rank == 0 and world == 1 and not args.no_cpu))
               if not args.no_extra else None)
@@ -1106,6 +1166,7 @@ def run_gpu(args):
             'mixed_batch': mixed,
             'large_stamps': large,
             'interp_psf': interp,
+            'chromatic': chrom,
             'noise': noise,
             'fits': fits_stage,
             'clocks': clk.summary(),
@@ -1131,7 +1192,8 @@ def main():
                     help='skip the mixed-batch and large-stamp measurements')
     ap.add_argument('--stamps', type=int, default=B_DEFAULT, help='stamps per GPU (leading subset)')
     ap.add_argument('--nx', type=int, default=None, help='fixed stamp size (default: automatic)')
-    ap.add_argument('--stage', default='all', choices=['all', 'draw', 'tables', 'fit', 'interp', 'noise', 'fits', 'large'],
+    ap.add_argument('--stage', default='all', choices=['all', 'draw', 'tables', 'fit', 'interp', 'noise', 'fits', 'large',
+                                                       'chromatic'],
                     help="'draw' / 'tables' / 'fit' / 'interp' / 'noise' / 'fits': run only that stage (for profiling)")
     args = ap.parse_args()
     if args.impl == 'reference':

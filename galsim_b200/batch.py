@@ -382,15 +382,29 @@ def _run_real(plan):
 
 
 def draw_batch(obj, nx=None, ny=None, scale=None, dtype=np.float32, method='fft', area=1.,
-               exptime=1., gain=1., offset=None, use_true_center=True, precision='fp32'):
+               exptime=1., gain=1., offset=None, use_true_center=True, precision='fp32',
+               bandpass=None, integrator='quadratic'):
     """Draw every stamp of a batched GSObject.
 
     Each stamp is drawn like ``obj_i.drawImage(nx=nx, ny=ny, scale=scale, dtype=dtype,
     method=method, ...)``; without nx, ny every stamp gets its automatic size
     (getGoodImageSize).  ``offset`` may be a (B, 2) array.  Returns a StampBatch whose pixels
-    stay on the device until read."""
+    stay on the device until read.
+
+    A chromatic object (a batched GSObject times an SED, convolved with chromatic or achromatic
+    PSFs, and sums of such terms) is drawn through ``bandpass`` like
+    ``obj_i.drawImage(bandpass, nx=nx, ny=ny, ...)``; fixed nx, ny are then required, and each
+    term's effective PSF is integrated once for the whole batch (see
+    galsim_b200.chromatic.draw_batch_chromatic)."""
+    from .chromatic import ChromaticObject, draw_batch_chromatic
     if isinstance(obj, (list, tuple)):
         obj = stack_objects(obj)
+    if isinstance(obj, ChromaticObject):
+        if bandpass is None:
+            raise GalSimIncompatibleValuesError("a chromatic object is drawn through a bandpass",
+                                                bandpass=bandpass)
+        return draw_batch_chromatic(obj, bandpass, nx, ny, scale, dtype, method, area, exptime, gain,
+                                    offset, use_true_center, precision, integrator)
     return run_batch(plan_batch(obj, nx, ny, scale, dtype, method, area, exptime, gain, offset,
                                 use_true_center, precision))
 

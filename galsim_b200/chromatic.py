@@ -41,7 +41,7 @@ from .errors import (GalSimError, GalSimSEDError, GalSimValueError, GalSimIncomp
                      GalSimNotImplementedError)
 
 __all__ = ['ChromaticObject', 'ChromaticTransformation', 'SimpleChromaticTransformation',
-           'ChromaticAtmosphere', 'ChromaticSum', 'ChromaticConvolution']
+           'ChromaticAtmosphere', 'ChromaticSum', 'ChromaticConvolution', 'draw_batch_chromatic']
 
 
 def _remove_setup_kwargs(kwargs):
@@ -169,7 +169,7 @@ class ChromaticObject(object):
         """chromatic.py:226-259."""
         bpwave = bandpass.effective_wavelength
         bpwave, prof0 = self._approxWavelength(bpwave)
-        if prof0.flux != 0:
+        if np.all(np.asarray(prof0.flux) != 0):
             return bpwave, prof0
         candidate_waves = np.concatenate([np.array([0.5 * (bandpass.blue_limit + bandpass.red_limit)]),
                                           bandpass.wave_list, self.wave_list])
@@ -177,7 +177,7 @@ class ChromaticObject(object):
         for w in candidate_waves:
             if bandpass.blue_limit <= w <= bandpass.red_limit:
                 prof0 = self.evaluateAtWavelength(w)
-                if prof0.flux != 0:
+                if np.all(np.asarray(prof0.flux) != 0):
                     return w, prof0
         raise GalSimError("Could not locate fiducial wavelength where SED * Bandpass is nonzero.")
 
@@ -478,7 +478,11 @@ class SimpleChromaticTransformation(ChromaticTransformation):
 
     @property
     def sed(self):
-        return self._flux_ratio * float(self._original.flux)
+        flux = self._original.flux
+        if np.ndim(flux) > 0:
+            # a batch of galaxies sharing the SED: the flux stays with the batched profile
+            return self._flux_ratio
+        return self._flux_ratio * float(flux)
 
     def _getTransformations(self, wave):
         return self._jac, self._offset, self._flux_ratio(wave)
@@ -797,3 +801,84 @@ class ChromaticConvolution(ChromaticObject):
         sep_profs.append(effective_prof)
         final_prof = Convolve(sep_profs, gsparams=self._gsparams, propagate_gsparams=self._propagate_gsparams)
         return final_prof.drawImage(image=image, precision=precision, **kwargs)
+
+
+def _batch_terms(obj):
+    """The terms of a chromatic batch: ChromaticSums distributed over the convolution, as
+    ChromaticConvolution.drawImage distributes them (chromatic.py:2935-2975)."""
+    if isinstance(obj, ChromaticSum):
+        out = []
+        for o in obj.obj_list:
+            out.extend(_batch_terms(o))
+        return out
+    if isinstance(obj, ChromaticConvolution):
+        for i, o in enumerate(obj.obj_list):
+            if isinstance(o, ChromaticSum):
+                out = []
+                for summand in o.obj_list:
+                    tmp = list(obj.obj_list)
+                    del tmp[i]
+                    tmp.append(summand)
+                    out.extend(_batch_terms(ChromaticConvolution(tmp)))
+                return out
+    return [obj]
+
+
+def _batch_term_profile(term, bandpass, integrator, precision):
+    """The achromatic (batched) profile whose draw is the term's chromatic draw: the fiducial
+    profile scaled by the SED x throughput integral for a separable term (chromatic.py:483-487),
+    the separable factors convolved with the effective PSF for a convolution with inseparable
+    factors (chromatic.py:2999-3030).  The effective PSF, which depends only on the PSF, the
+    galaxy SED and the bandpass, is integrated once for the whole batch."""
+    from .compound import Convolve
+    if term.sed.dimensionless:
+        raise GalSimSEDError("Can only draw ChromaticObjects with spectral SEDs.", term.sed)
+    if term.separable:
+        wave0, prof0 = term._fiducial_profile(bandpass)
+        wave_list, _, _ = combine_wave_list(term, bandpass)
+        return prof0 * (_get_multiplier(term.sed, bandpass, tuple(wave_list)) / term.sed(wave0))
+    if not isinstance(term, ChromaticConvolution):
+        raise GalSimNotImplementedError("batched drawing of a chromatic %s that is not a convolution with "
+                                        "separable galaxy terms is not built" % type(term).__name__)
+    insep = [o for o in term.obj_list if not o.separable]
+    insep_obj = insep[0] if len(insep) == 1 else ChromaticConvolution(
+        insep, gsparams=term._gsparams, propagate_gsparams=term._propagate_gsparams)
+    sep = []
+    for o in term.obj_list:
+        if o.separable:
+            wave0, p0 = o._fiducial_profile(bandpass)
+            sep.append(p0 / o.sed(wave0))
+            insep_obj = insep_obj * o.sed
+    eff = ChromaticConvolution._get_effective_prof(insep_obj, bandpass, None, integrator, term._gsparams,
+                                                   precision)
+    return Convolve(sep + [eff], gsparams=term._gsparams, propagate_gsparams=term._propagate_gsparams)
+
+
+def draw_batch_chromatic(obj, bandpass, nx, ny, scale, dtype=np.float32, method='auto', area=1., exptime=1.,
+                         gain=1., offset=None, use_true_center=True, precision='fp32', integrator='quadratic'):
+    """A batch of chromatic objects drawn through a bandpass: galaxies whose spatial profiles
+    are batched GSObjects times one SED per term, convolved with chromatic (or achromatic)
+    PSFs shared by the batch.  Stamp i is what ``obj_i.drawImage(bandpass, nx=nx, ny=ny,
+    scale=scale, ...)`` draws: each term's effective PSF is integrated once (one batched draw
+    of its wavelengths) and the terms' batched profiles are drawn with draw_batch, their stamps
+    summed on the device.  added_flux is the sum over the terms."""
+    from .batch import draw_batch
+    if nx is None or ny is None:
+        raise GalSimIncompatibleValuesError("batched chromatic drawing needs fixed nx, ny", nx=nx, ny=ny)
+    out = None
+    flux = None
+    for term in _batch_terms(obj):
+        prof = _batch_term_profile(term, bandpass, integrator, precision)
+        st = draw_batch(prof, nx=nx, ny=ny, scale=scale, dtype=dtype, method=method, area=area,
+                        exptime=exptime, gain=gain, offset=offset, use_true_center=use_true_center,
+                        precision=precision)
+        if out is None:
+            out = st
+            flux = st._flux_dev.clone()
+        else:
+            if len(st) != len(out) and len(out) == 1:
+                raise GalSimIncompatibleValuesError("the terms of a chromatic batch have different batch sizes")
+            out.flat += st.flat
+            flux += st._flux_dev
+    out._flux_dev = flux
+    return out

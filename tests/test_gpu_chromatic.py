@@ -60,3 +60,22 @@ def test_integrand_batch_is_one_draw_per_wavelength():
     img = insep.drawImage(bp, scale=0.05, method='no_pixel')
     assert insep._last_n_eval == 12
     assert np.isfinite(img.array).all() and img.array.sum() > 0.
+
+
+def test_chromatic_batch_matches_single_draws():
+    """draw_batch of a batched bulge + disk through a ChromaticAtmosphere (two effective PSFs,
+    each integrated once for the batch) draws what drawImage draws galaxy by galaxy."""
+    s1, s2 = CC.seds(galsim)
+    b1, _ = CC.bandpasses(galsim)
+    psf = galsim.ChromaticAtmosphere(galsim.Kolmogorov(fwhm=0.7), 500., zenith_angle=30. * galsim.degrees)
+    hlr = np.array([0.3, 0.5, 0.8])
+    g1 = np.array([0.1, -0.2, 0.05])
+
+    def gal(h, g):
+        return (galsim.DeVaucouleurs(half_light_radius=h * 0.5, flux=0.3) * s1 +
+                galsim.Exponential(half_light_radius=h, flux=0.7).shear(g1=g, g2=0.1) * s2)
+    st = galsim.draw_batch(galsim.Convolve(gal(hlr, g1), psf), nx=32, ny=32, scale=0.2, bandpass=b1)
+    for i in range(3):
+        im = galsim.Convolve(gal(hlr[i], g1[i]), psf).drawImage(b1, nx=32, ny=32, scale=0.2)
+        a = st.array(i)
+        assert np.abs(a - im.array).max() <= 1e-5 * np.abs(im.array).max(), i
