@@ -22,6 +22,22 @@ from . import _lib
 from .errors import GalSimError, galsim_warn_fft
 
 
+def unique_pairs(a, b):
+    """np.unique of the rows (a_i, b_i) with return_inverse (lexicographic order), through a
+    complex key: numpy's row-wise unique (axis=0) is ~10x slower on thousands of rows."""
+    u, inv = np.unique(np.asarray(a, np.float64) + 1j * np.asarray(b, np.float64), return_inverse=True)
+    return u.real.copy(), u.imag.copy(), np.asarray(inv).reshape(-1)
+
+
+def stack_records(recs):
+    """np.stack(recs, axis=1) of equal-length 1-d structured record arrays, copied as raw
+    bytes (numpy's structured stack copies record by record)."""
+    B = len(recs[0])
+    dt = recs[0].dtype
+    raw = np.stack([np.ascontiguousarray(r).view(np.uint8).reshape(B, dt.itemsize) for r in recs], axis=1)
+    return raw.view(dt).reshape(B, len(recs))
+
+
 class Builder(object):
     def __init__(self, B, gsparams):
         self.B = B
@@ -46,18 +62,31 @@ class Builder(object):
     def add_leaf(self, ltype, jac, flux, params, flags=0):
         if len(self.leaves) >= _lib.MAX_LEAVES:
             raise GalSimError("profile tree has more than %d leaves" % _lib.MAX_LEAVES)
-        rec = np.zeros(self.B, dtype=_lib.LEAF_DTYPE)
-        j = self._bjac(jac)
-        if j is None:
-            rec['jac'][:] = (1., 0., 0., 1.)
-            general = np.zeros(self.B, bool)
+        # the record as 17 float64 words (jac 0-3, flux 4, p 5-7, d 8-15, flags / table in 16),
+        # filled column by column with broadcasting, then viewed as LEAF_DTYPE
+        B = self.B
+        w = np.empty((B, 17), dtype=np.float64)
+        iw = w.view(np.int32)                      # (B, 34): flags at 32, table at 33
+        if jac is None:
+            w[:, 0:4] = (1., 0., 0., 1.)
+            general = 0
         else:
-            rec['jac'] = j.reshape(self.B, 4)
-            general = (j[:, 0, 1] != 0.) | (j[:, 1, 0] != 0.)
-        rec['flux'] = self._bcast(flux)
+            j = np.asarray(jac, dtype=np.float64)
+            if j.ndim == 2:
+                w[:, 0:4] = j.reshape(4)
+                general = _lib.LEAF_JAC_GENERAL if (j[0, 1] != 0. or j[1, 0] != 0.) else 0
+            else:
+                j = j.reshape(B, 4)
+                w[:, 0:4] = j
+                general = np.where((j[:, 1] != 0.) | (j[:, 2] != 0.), _lib.LEAF_JAC_GENERAL, 0)
+        w[:, 4] = flux
+        w[:, 5:8] = 0.
         for i, p in enumerate(params):
-            rec['p'][:, i] = self._bcast(p)
-        rec['flags'] = np.where(general, _lib.LEAF_JAC_GENERAL, 0) | flags
+            w[:, 5 + i] = np.asarray(p, dtype=np.float64).reshape(-1) if np.ndim(p) else p
+        w[:, 8:16] = 0.
+        iw[:, 32] = np.bitwise_or(general, flags)
+        iw[:, 33] = 0
+        rec = w.view(_lib.LEAF_DTYPE).reshape(B)
         self.ops.append((_lib.OP_LEAF, len(self.leaves)))
         self.leaf_types.append(ltype)
         self.leaves.append(rec)
@@ -127,7 +156,7 @@ class Program(object):
             return
         import torch
         B, L = self.B, self.L
-        leaves = np.stack(self.bld.leaves, axis=1)            # (B, L)
+        leaves = stack_records(self.bld.leaves)               # (B, L)
         self.sersic_n = None
         self.sersic_trunc = None
         sersic = [l for l in range(L) if self.bld.leaf_types[l] == _lib.SERSIC]
@@ -137,9 +166,9 @@ class Program(object):
             tvals = np.concatenate([np.where(leaves[:, l]['p'][:, 2] > 0.,
                                              leaves[:, l]['p'][:, 2] / leaves[:, l]['p'][:, 1], 0.)
                                     for l in sersic])
-            uniq, inv = np.unique(np.stack([nvals, tvals], -1), axis=0, return_inverse=True)
-            self.sersic_n = np.ascontiguousarray(uniq[:, 0])
-            self.sersic_trunc = np.ascontiguousarray(uniq[:, 1]) if np.any(uniq[:, 1] > 0.) else None
+            un, ut, inv = unique_pairs(nvals, tvals)
+            self.sersic_n = np.ascontiguousarray(un)
+            self.sersic_trunc = np.ascontiguousarray(ut) if np.any(ut > 0.) else None
             inv = np.asarray(inv).reshape(len(sersic), B)
             for k, l in enumerate(sersic):
                 leaves['table'][:, l] = inv[k]
@@ -152,9 +181,10 @@ class Program(object):
             tvals = np.concatenate([leaves[:, l]['p'][:, 2] / leaves[:, l]['p'][:, 1] for l in moffat])
             cut = tvals > 0.
             if np.any(cut):
-                uniq, inv = np.unique(np.stack([bvals[cut], tvals[cut]], -1), axis=0, return_inverse=True)
+                ub, ut, inv = unique_pairs(bvals[cut], tvals[cut])
+                uniq = np.stack([ub, ut], -1)
                 slot = np.full(len(bvals), -1, dtype=np.int32)
-                slot[cut] = np.asarray(inv).reshape(-1)
+                slot[cut] = inv
                 slot = slot.reshape(len(moffat), B)
                 for k, l in enumerate(moffat):
                     leaves['table'][:, l] = slot[k]
@@ -274,7 +304,7 @@ class Program(object):
         stamps['out_offset'] = offsets
         perm = torch.from_numpy(order).to(dev)
         lv = self.d_leaves.view(B, L * _lib.LEAF_DTYPE.itemsize).index_select(0, perm).contiguous()
-        ph = (_lib.to_device(np.stack(self.bld.phases, axis=1)[order]) if self.bld.phases else None)
+        ph = (_lib.to_device(stack_records(self.bld.phases)[order]) if self.bld.phases else None)
         sc = (_lib.to_device(np.stack(self.bld.scales, axis=1)[order]) if self.bld.scales else None)
         st = _lib.to_device(stamps[order])
         Ns = N[order]
@@ -354,7 +384,7 @@ class Program(object):
                 torch.index_select(self.d_leaves.view(B, self.L * _lib.LEAF_DTYPE.itemsize), 0, g['perm'],
                                    out=g['lv'])
                 if g['ph'] is not None:
-                    g['ph'].copy_(_lib.to_device(np.stack(self.bld.phases, axis=1)[g['order']]))
+                    g['ph'].copy_(_lib.to_device(stack_records(self.bld.phases)[g['order']]))
                 if g['sc'] is not None:
                     g['sc'].copy_(_lib.to_device(np.stack(self.bld.scales, axis=1)[g['order']]))
                 if gs['graph'] is None:
@@ -420,7 +450,7 @@ class Program(object):
         dev = _lib.Device.torch_device()
         tdt = torch.float32 if dtype == _lib.F32 else torch.float64
         out = torch.empty(self.B * nkx * nky * 2, dtype=tdt, device=dev)
-        ph = _lib.to_device(np.stack(self.bld.phases, axis=1)) if self.bld.phases else None
+        ph = _lib.to_device(stack_records(self.bld.phases)) if self.bld.phases else None
         sc = _lib.to_device(np.stack(self.bld.scales, axis=1)) if self.bld.scales else None
         _lib.check(_lib.lib().gsb_draw_kimages(
             ctypes.byref(self.tpl), self.B, ctypes.byref(self.gsp_c), _lib.ptr(self.d_leaves),
