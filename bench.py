@@ -1055,23 +1055,22 @@ def run_gpu(args):
     ee.record()
     barrier()
     e2e_serial_ms = replicas.max_over_ranks(es.elapsed_time(ee) / args.steps)
-    # the same steps pipelined as a catalog run would be: step k's pixels are read on a copy
-    # stream (StampBatch.host_async) while step k+1's tables and draws run; every step's
-    # read-back is still inside the timed region (the last one is waited for before the stop)
-    for _ in range(args.warmup):
-        galsim.draw_batch(gpu_object(galsim, params), scale=SCALE, dtype=np.float32).host_async().result()
+    # the same steps pipelined as a catalog run is (galsim_b200.draw_batches): a worker thread
+    # builds and uploads step k+1's records while step k's tables and draws run, and step k's
+    # pixels are read on a copy stream while step k+1 draws; every step's read-back is inside
+    # the timed region (the generator yields each step's host pixels and fluxes)
+    for _ in galsim.draw_batches((gpu_object(galsim, params) for _ in range(max(args.warmup, 2))),
+                                 scale=SCALE, dtype=np.float32):
+        pass
     barrier()
     es.record()
-    pending = None
-    for _ in range(args.steps):
-        sb = galsim.draw_batch(gpu_object(galsim, params), scale=SCALE, dtype=np.float32)
-        read = sb.host_async()          # pixels and fluxes, on the copy stream
-        if pending is not None:
-            pix, flux = pending.result(), pending.added_flux()
-        pending = read
-    pix, flux = pending.result(), pending.added_flux()
+    n_done = 0
+    for sb, pix, flux in galsim.draw_batches((gpu_object(galsim, params) for _ in range(args.steps)),
+                                             scale=SCALE, dtype=np.float32):
+        n_done += 1
     ee.record()
     barrier()
+    assert n_done == args.steps
     e2e_ms = replicas.max_over_ranks(es.elapsed_time(ee) / args.steps)
     clk.__exit__(None, None, None)
     L = prog.L
@@ -1143,8 +1142,9 @@ def run_gpu(args):
                      'l2': 'no flush; per-step table build and stamp outputs exceed L2 reuse'},
             'e2e': {'value': world * B / (e2e_ms * 1e-3), 'unit': 'stamps/s',
                     'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': d2h,
-                    'mode': 'host parameters -> draw_batch -> host pixels and fluxes; step k read '
-                            'back on a copy stream while step k+1 runs (StampBatch.host_async)',
+                    'mode': 'host parameters -> draw_batches -> host pixels and fluxes; step k+1 built and '
+                            'uploaded on a worker thread while step k runs, step k read back on a copy '
+                            'stream while step k+1 draws',
                     'serial_value': world * B / (e2e_serial_ms * 1e-3)},
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                          'frac': achieved / peak, 'traffic': DRAW_STEP_DRAM_READ + DRAW_STEP_DRAM_WRITE,

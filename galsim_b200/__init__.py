@@ -30,7 +30,7 @@ from .noise import BaseDeviate, BaseNoise, GaussianNoise, PoissonNoise, CCDNoise
 from . import fits
 from .fits import FitsHeader
 from .compound import Convolve, Convolution, Add, Sum, Transform, Transformation, _Transform
-from .batch import draw_batch, plan_batch, run_batch, StampBatch
+from .batch import draw_batch, draw_batches, plan_batch, run_batch, StampBatch
 from .table import LookupTable, _LookupTable, trapz
 from .sed import SED
 from .bandpass import Bandpass

@@ -409,6 +409,52 @@ def draw_batch(obj, nx=None, ny=None, scale=None, dtype=np.float32, method='fft'
                                 use_true_center, precision))
 
 
+def draw_batches(objects, nx=None, ny=None, scale=None, dtype=np.float32, method='fft', area=1.,
+                 exptime=1., gain=1., offset=None, use_true_center=True, precision='fp32'):
+    """Draw a sequence of batched GSObjects (a catalog in chunks), yielding per batch
+    ``(stamps, pixels, fluxes)``: the StampBatch (its geometry; pixels still on the device),
+    the flat host pixels and the per-stamp added fluxes.  Three stages overlap: a worker thread
+    takes the next object from `objects` and builds and uploads its records (plan_batch) while
+    the current batch's tables and draws run, and each batch's pixels are read back on a copy
+    stream while the next batch draws.  The host arrays are views of page-locked buffers that
+    alternate between batches of the same size: copy them to keep them past the next
+    iteration.  The other arguments are draw_batch's."""
+    from concurrent.futures import ThreadPoolExecutor
+    it = iter(objects)
+    kw = dict(nx=nx, ny=ny, scale=scale, dtype=dtype, method=method, area=area, exptime=exptime, gain=gain,
+              offset=offset, use_true_center=use_true_center, precision=precision)
+    import torch
+    dev = _lib.Device.torch_device()
+
+    def prepare():
+        torch.cuda.set_device(dev)           # the worker thread's current device is its own
+        try:
+            obj = next(it)
+        except StopIteration:
+            return None
+        if isinstance(obj, (list, tuple)):
+            obj = stack_objects(obj)
+        return plan_batch(obj, **kw)
+
+    with ThreadPoolExecutor(max_workers=1) as pool:
+        nxt = pool.submit(prepare)
+        pending = None
+        while True:
+            plan = nxt.result()
+            if plan is None:
+                break
+            nxt = pool.submit(prepare)          # the next batch's host set-up overlaps this one
+            sb = run_batch(plan)
+            read = sb.host_async()
+            if pending is not None:
+                psb, pread = pending
+                yield psb, pread.result(), pread.added_flux()
+            pending = (sb, read)
+        if pending is not None:
+            psb, pread = pending
+            yield psb, pread.result(), pread.added_flux()
+
+
 def stack_objects(objs):
     """Turn a list of scalar GSObjects with the same tree structure into one batched object."""
     raise GalSimIncompatibleValuesError(

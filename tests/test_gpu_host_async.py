@@ -30,3 +30,25 @@ def test_pipelined_reads_match_synchronous_reads():
     r = pending.pop(0)
     np.testing.assert_array_equal(r.result(), expected[-1])
     np.testing.assert_array_equal(r.added_flux(), fluxes[-1])
+
+
+@pytest.mark.parametrize('fixed', [False, True])
+def test_draw_batches_matches_draw_batch(fixed):
+    """draw_batches (next batch planned on a worker thread, reads on a copy stream) yields every
+    batch's pixels and fluxes exactly as draw_batch draws them, in order."""
+    size = dict(nx=40, ny=40) if fixed else {}
+    expected = []
+    for seed in range(5):
+        sb = galsim.draw_batch(_obj(seed), scale=0.2, dtype=np.float32, **size)
+        expected.append((sb.host(copy=True), np.array(sb.added_flux), list(sb.offsets)))
+    got = [(sb, pix.copy(), flux.copy()) for sb, pix, flux in
+           galsim.draw_batches((_obj(seed) for seed in range(5)), scale=0.2, dtype=np.float32, **size)]
+    assert len(got) == len(expected)
+    for (sb, pix, flux), (epix, eflux, eoff) in zip(got, expected):
+        assert list(sb.offsets) == eoff
+        np.testing.assert_array_equal(pix, epix)
+        np.testing.assert_array_equal(flux, eflux)
+
+
+def test_draw_batches_empty_sequence():
+    assert list(galsim.draw_batches(iter(()), scale=0.2)) == []
