@@ -26,7 +26,7 @@ from .box import Box, Pixel
 from .interpolant import (Interpolant, Delta, Nearest, SincInterpolant, Linear, Cubic, Quintic,
                           Lanczos, convert_interpolant)
 from .interpolatedimage import InterpolatedImage
-from .noise import BaseDeviate, BaseNoise, GaussianNoise, PoissonNoise, CCDNoise
+from .noise import BaseDeviate, BaseNoise, GaussianNoise, PoissonNoise, CCDNoise, VariableGaussianNoise
 from . import fits
 from .fits import FitsHeader
 from .compound import Convolve, Convolution, Add, Sum, Transform, Transformation, _Transform

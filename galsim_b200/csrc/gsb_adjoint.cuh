@@ -204,13 +204,13 @@ __device__ __forceinline__ void adjoint_point_factored(const gsb_template& tpl, 
     const int hk = g.n / 2;
     const T kx = T(i) * T(dk), ky = T(j) * T(dk);
     const int na = S.n_atoms;
-    Cx<T> val[kAdjAtoms], e[kAdjAtoms], pre[kAdjAtoms];
+    // ld[a] holds a leaf atom's derivatives, or a phase atom's unit phasor in (gx, gy)
+    Cx<T> val[kAdjAtoms], pre[kAdjAtoms];
     LeafD<T> ld[kAdjAtoms];
     Cx<T> run = cx<T>(T(1), T(0));
 #pragma unroll
     for (int a = 0; a < kAdjAtoms; ++a) {
         val[a] = cx<T>(T(1), T(0));
-        e[a] = val[a];
         ld[a] = LeafD<T>{T(0), T(0), T(0), T(0), T(0)};
         if (a < na) {
             const int kind = S.atom_kind[a];
@@ -221,8 +221,9 @@ __device__ __forceinline__ void adjoint_point_factored(const gsb_template& tpl, 
                 tt -= rint(tt);
                 T sn, cs;
                 sincospi(T(-2. * tt), &sn, &cs);
-                e[a] = cx<T>(cs, sn);
-                val[a] = cscale<T>(e[a], T(S.phase[p].flux_scaling));
+                ld[a].gx = cs;
+                ld[a].gy = sn;
+                val[a] = cscale<T>(cx<T>(cs, sn), T(S.phase[p].flux_scaling));
             } else if (kind == kAtomScale) {
                 val[a] = cx<T>(T(S.scale[S.atom_arg[a]]), T(0));
             } else if (o1 - o0 == 1) {
@@ -251,7 +252,7 @@ __device__ __forceinline__ void adjoint_point_factored(const gsb_template& tpl, 
             const int o0 = S.atom_o0[a], o1 = S.atom_o1[a];
             if (kind == kAtomPhase) {
                 const gsb_phase& P = S.phase[S.atom_arg[a]];
-                const Cx<T> we = cmul<T>(w, e[a]);
+                const Cx<T> we = cmul<T>(w, cx<T>(ld[a].gx, ld[a].gy));
                 const T z = T(P.flux_scaling) * we.y;
                 const T cxp = T(P.cenx), cyp = T(P.ceny);
                 ga[a][0] += z * (T(P.jac[0]) * kx + T(P.jac[2]) * ky);
@@ -382,19 +383,21 @@ __global__ void __launch_bounds__(adj_warps<T, N>() * 32) adjoint_fused_kernel(c
         __syncthreads();
 
         // ---- column phase: forward-sign DFT along y, then the reverse pass per alias ----
+        // Each lane accumulates its gradient terms over all of its warp's columns; the warp
+        // reduces them once per stamp.
         T acc[kMaxGrad];
         T ga[kAdjAtoms][kGradPerPhase];
+        if (subtree)
+            for (int k = 0; k < ng; ++k) acc[k] = T(0);
+#pragma unroll
+        for (int t = 0; t < kAdjAtoms; ++t)
+#pragma unroll
+            for (int e = 0; e < kGradPerPhase; ++e) ga[t][e] = T(0);
         for (int c = warp; c < H; c += NW) {
             for (int y = lane; y < N; y += 32)
                 buf[y] = pmod(y - G.ymin, N) < G.ny ? W[(size_t)c * WS + y] : cx<T>(T(0), T(0));
             __syncwarp();
             warp_fft<T, N, +1>(buf, tw);
-            if (subtree)
-                for (int k = 0; k < ng; ++k) acc[k] = T(0);
-#pragma unroll
-            for (int t = 0; t < kAdjAtoms; ++t)
-#pragma unroll
-                for (int e = 0; e < kGradPerPhase; ++e) ga[t][e] = T(0);
             const T wc = (c == 0 || 2 * c == N) ? inv_n2 : T(2) * inv_n2;
             const int alo = ceil_div(-hk - c, N), ahi = floor_div(hk - c, N);
             for (int r = lane; r < N; r += 32) {
@@ -416,36 +419,36 @@ __global__ void __launch_bounds__(adj_warps<T, N>() * 32) adjoint_fused_kernel(c
                     }
                 }
             }
-            if (subtree) {
-                for (int k = 0; k < ng; ++k) {
-                    double v = double(acc[k]);
-                    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-                    if (lane == 0) atomicAdd(&A.gacc[k], v);
-                }
-            }
-            if (factored) {
-                const int pbase = kGradPerLeaf * a.tpl.n_leaves;
-                const int sbase = pbase + kGradPerPhase * a.tpl.n_phases;
-#pragma unroll
-                for (int t = 0; t < kAdjAtoms; ++t) {
-                    if (t >= S.n_atoms) break;
-                    const int kind = S.atom_kind[t];
-                    int base, cnt;
-                    if (kind == kAtomPhase) { base = pbase + kGradPerPhase * S.atom_arg[t]; cnt = kGradPerPhase; }
-                    else if (kind == kAtomScale) { base = sbase + S.atom_arg[t]; cnt = 1; }
-                    else if (S.atom_o1[t] - S.atom_o0[t] == 1 && want_leaf(a.want, S.atom_arg[t])) {
-                        base = kGradPerLeaf * S.atom_arg[t]; cnt = kGradPerLeaf;
-                    } else continue;
-#pragma unroll
-                    for (int e = 0; e < kGradPerPhase; ++e) {
-                        if (e >= cnt) break;
-                        double v = double(ga[t][e]);
-                        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-                        if (lane == 0) atomicAdd(&A.gacc[base + e], v);
-                    }
-                }
-            }
             __syncwarp();
+        }
+        if (subtree) {
+            for (int k = 0; k < ng; ++k) {
+                double v = double(acc[k]);
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                if (lane == 0) atomicAdd(&A.gacc[k], v);
+            }
+        }
+        if (factored) {
+            const int pbase = kGradPerLeaf * a.tpl.n_leaves;
+            const int sbase = pbase + kGradPerPhase * a.tpl.n_phases;
+#pragma unroll
+            for (int t = 0; t < kAdjAtoms; ++t) {
+                if (t >= S.n_atoms) break;
+                const int kind = S.atom_kind[t];
+                int base, cnt;
+                if (kind == kAtomPhase) { base = pbase + kGradPerPhase * S.atom_arg[t]; cnt = kGradPerPhase; }
+                else if (kind == kAtomScale) { base = sbase + S.atom_arg[t]; cnt = 1; }
+                else if (S.atom_o1[t] - S.atom_o0[t] == 1 && want_leaf(a.want, S.atom_arg[t])) {
+                    base = kGradPerLeaf * S.atom_arg[t]; cnt = kGradPerLeaf;
+                } else continue;
+#pragma unroll
+                for (int e = 0; e < kGradPerPhase; ++e) {
+                    if (e >= cnt) break;
+                    double v = double(ga[t][e]);
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                    if (lane == 0) atomicAdd(&A.gacc[base + e], v);
+                }
+            }
         }
         __syncthreads();
         // Sersic leaves given by half-light radius: r0 = hlr / r_e(n), so at fixed hlr

@@ -299,7 +299,8 @@ struct NoiseArgs {
     int n_stamps;
     void* image;
     int dtype;
-    double* scratch;       // FP64 value per pixel (Poisson / CCD), indexed like the image
+    double* scratch;       // FP64 value per pixel (Poisson / CCD; the variances of variable
+                           // Gaussian noise), indexed like the image
     long long* used;       // draws used per stamp (Poisson pass -> read-noise pass)
 };
 
@@ -328,7 +329,13 @@ __global__ void __launch_bounds__(kNoiseWarps * 32) gauss_kernel(const __grid_co
     mt_seed(st.x, sp.seed, lane);
     st.skip(sp.skip);
     T* img = pix_ptr<T>(a.image, sp.offset);
-    gaussian_run(st, sp.npix, a.p.sigma, [&](long long j, double d) { img[j] = img[j] + T(d); });
+    if (a.kind == GSB_NOISE_VARIABLE_GAUSSIAN) {
+        // unit deviates scaled by each pixel's own sigma (GaussianDeviate::generateFromVariance)
+        const double* var = a.scratch + sp.offset;
+        gaussian_run(st, sp.npix, 1., [&](long long j, double d) { img[j] = img[j] + T(d * sqrt(var[j])); });
+    } else {
+        gaussian_run(st, sp.npix, a.p.sigma, [&](long long j, double d) { img[j] = img[j] + T(d); });
+    }
     if (lane == 0 && a.used) a.used[s] = st.used;      // draws consumed since seeding
 }
 
@@ -639,7 +646,7 @@ template <typename T>
 int launch_noise(const NoiseArgs& a, int max_npix, cudaStream_t stream)
 {
     const int warp_grid = (a.n_stamps + kNoiseWarps - 1) / kNoiseWarps;
-    if (a.kind == GSB_NOISE_GAUSSIAN) {
+    if (a.kind == GSB_NOISE_GAUSSIAN || a.kind == GSB_NOISE_VARIABLE_GAUSSIAN) {
         gauss_kernel<T><<<warp_grid, kNoiseWarps * 32, 0, stream>>>(a);
         GSB_CUDA_CHECK(cudaGetLastError());
         return GSB_OK;
@@ -683,10 +690,12 @@ extern "C" int gsb_add_noise(int kind, const gsb_noise_params* p, const gsb_nois
 {
     if (!p || n_stamps < 0 || (n_stamps > 0 && (!d_stamps || !d_image)))
         return set_error(GSB_ERR_INVALID, "null argument");
-    if (kind < GSB_NOISE_GAUSSIAN || kind > GSB_NOISE_CCD)
+    if (kind < GSB_NOISE_GAUSSIAN || kind > GSB_NOISE_VARIABLE_GAUSSIAN)
         return set_error(GSB_ERR_INVALID, "unknown noise kind");
+    if (kind == GSB_NOISE_VARIABLE_GAUSSIAN && n_stamps > 0 && !d_scratch)
+        return set_error(GSB_ERR_INVALID, "variable Gaussian noise needs the variance of every pixel in d_scratch");
     if (dtype != GSB_F32 && dtype != GSB_F64) return set_error(GSB_ERR_INVALID, "image dtype must be F32 or F64");
-    if (kind != GSB_NOISE_GAUSSIAN && (!d_scratch || !d_used))
+    if ((kind == GSB_NOISE_POISSON || kind == GSB_NOISE_CCD) && (!d_scratch || !d_used))
         return set_error(GSB_ERR_INVALID, "Poisson and CCD noise need the FP64 scratch and the draw counts");
     if (max_npix < 0) return set_error(GSB_ERR_INVALID, "negative pixel count");
     if (kind == GSB_NOISE_GAUSSIAN && !(p->sigma >= 0.)) return set_error(GSB_ERR_INVALID, "sigma must be >= 0");

@@ -122,8 +122,9 @@ class InterpolatedImage(GSObject):
                                convert_interpolant(k_interpolant).withGSParams(self._gsparams))
         if depixelize:
             raise GalSimNotImplementedError("InterpolatedImage(depixelize=True) is not built")
-        if noise_pad_size or noise_pad:
-            raise GalSimNotImplementedError("InterpolatedImage noise padding is not built")
+        self._noise_pad = self._check_noise_pad(noise_pad_size, noise_pad)
+        self._noise_pad_size = noise_pad_size
+        self._rng = rng
         if pad_factor <= 0.:
             raise GalSimRangeError("Invalid pad_factor <= 0 in InterpolatedImage", pad_factor, 0.)
         if scale is not None and wcs is not None:
@@ -144,12 +145,57 @@ class InterpolatedImage(GSObject):
         self._force_stepk = float(_force_stepk)
         self._force_maxk = float(_force_maxk)
         self._build_args = (images, scale, wcs, flux, normalization, pad_factor, pad_image, offset,
-                            use_true_center)
+                            use_true_center, noise_pad_size, noise_pad, rng)
         self._build(*self._build_args)
 
     # -- construction (interpolatedimage.py:303-400, 590-660) ---------------------------------
+    @staticmethod
+    def _check_noise_pad(noise_pad_size, noise_pad):
+        """The argument checks of _buildRealImage / _buildNoisePadImage for noise padding
+        (interpolatedimage.py:463-476, 527-550); returns the variance of the Gaussian padding
+        noise (0 for none).  Padding with correlated noise (a CorrelatedNoise, an image or a file
+        name) is not built."""
+        if noise_pad_size:
+            if noise_pad_size < 0:
+                raise GalSimValueError("noise_pad_size may not be negative", noise_pad_size)
+            if not noise_pad:
+                raise GalSimIncompatibleValuesError(
+                    "Must provide noise_pad if noise_pad_size > 0",
+                    noise_pad=noise_pad, noise_pad_size=noise_pad_size)
+        elif noise_pad:
+            raise GalSimIncompatibleValuesError(
+                "Must provide noise_pad_size if noise_pad != 0",
+                noise_pad=noise_pad, noise_pad_size=noise_pad_size)
+        if not noise_pad:
+            return 0.
+        try:
+            var = float(noise_pad)
+        except (TypeError, ValueError):
+            if isinstance(noise_pad, (Image, str)) or hasattr(noise_pad, 'getVariance'):
+                raise GalSimNotImplementedError("noise padding with correlated noise (a "
+                                                "CorrelatedNoise, an image or a file) is not built")
+            raise GalSimValueError(
+                "Input noise_pad must be a float/int, a CorrelatedNoise, Image, or filename "
+                "containing an image to use to make a CorrelatedNoise.", noise_pad)
+        if var < 0.:
+            raise GalSimRangeError("Noise variance may not be negative.", var, 0.)
+        return var
+
+    def _noise_pad_region(self, noise_pad_size, var, rng, w):
+        """The Gaussian noise padding of _buildNoisePadImage (interpolatedimage.py:521-566):
+        a noise_pad_size square (in pixels: ceil(size / scale), rounded up to a good FFT
+        size) centred on (0, 0), filled with GaussianNoise(BaseDeviate(rng), sqrt(var)) drawn on
+        the GPU with the reference's stream.  Returns (bounds, array)."""
+        from .noise import BaseDeviate, GaussianNoise
+        from .image import ImageD
+        n = Image.good_fft_size(int(math.ceil(noise_pad_size / w.scale)))
+        half = n // 2
+        nim = ImageD(n, n, init_value=0.)
+        nim.addNoise(GaussianNoise(BaseDeviate(rng), sigma=math.sqrt(var)))
+        return _BoundsI(-half, -half + n - 1, -half, -half + n - 1), nim.array, n
+
     def _build(self, images, scale, wcs, flux, normalization, pad_factor, pad_image, offset,
-               use_true_center):
+               use_true_center, noise_pad_size=0, noise_pad=0., rng=None):
         x_code = self._x_interpolant._code if self._x_interpolant._code is not None else 0
         flags = 0
         if self._force_stepk <= 0. and self._calculate_stepk:
@@ -183,6 +229,18 @@ class InterpolatedImage(GSObject):
             if pad_factor > 1.:
                 pad_size = int(math.ceil(pad_factor * pad_size))
             nz = b
+            npad = None
+            if noise_pad:
+                # drawn once per image: a rebuild (withGSParams) keeps the same padding, as the
+                # reference's copy keeps its padded image
+                cache = self.__dict__.setdefault('_noise_regions', {})
+                if len(sources) not in cache:
+                    cache[len(sources)] = self._noise_pad_region(noise_pad_size, self._noise_pad, rng, w)
+                nb, narr, nsize = cache[len(sources)]
+                pad_size = max(pad_size, nsize)
+                npad = (nb, narr)
+                nz = _BoundsI(min(nz.xmin, nb.xmin), max(nz.xmax, nb.xmax),
+                              min(nz.ymin, nb.ymin), max(nz.ymax, nb.ymax))
             pim = None
             if pad_image is not None:
                 pim = pad_image.view(dtype=np.float64)
@@ -193,6 +251,10 @@ class InterpolatedImage(GSObject):
                               min(nz.ymin, pb.ymin), max(nz.ymax, pb.ymax))
             N = Image.good_fft_size(pad_size)
             region = np.zeros((nz.ymax - nz.ymin + 1, nz.xmax - nz.xmin + 1))
+            if npad is not None:
+                nb, narr = npad
+                region[nb.ymin - nz.ymin:nb.ymax - nz.ymin + 1,
+                       nb.xmin - nz.xmin:nb.xmax - nz.xmin + 1] = narr
             if pim is not None:
                 pb = pim.bounds
                 region[pb.ymin - nz.ymin:pb.ymax - nz.ymin + 1,

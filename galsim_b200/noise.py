@@ -1,4 +1,5 @@
-"""Random streams and noise: BaseDeviate, GaussianNoise, PoissonNoise, CCDNoise
+"""Random streams and noise: BaseDeviate, GaussianNoise, PoissonNoise, CCDNoise,
+VariableGaussianNoise
 (galsim/random.py, galsim/noise.py).
 
 A BaseDeviate is the reference's random stream, named by its seed and the number of raw
@@ -93,7 +94,7 @@ NOISE_STAMP_DTYPE = np.dtype({'names': ['offset', 'npix', 'pad', 'seed', 'skip']
                               'formats': ['i8', 'i4', 'i4', 'i8', 'i8'],
                               'offsets': [0, 8, 12, 16, 24], 'itemsize': 32})
 
-GAUSSIAN, POISSON, CCD = 0, 1, 2
+GAUSSIAN, POISSON, CCD, VARIABLE_GAUSSIAN = 0, 1, 2, 3
 
 
 def _sky_split(sky_level, dtype):
@@ -106,9 +107,10 @@ def _sky_split(sky_level, dtype):
     return float(frac_sky), float(int_sky), bool(same)
 
 
-def _apply(kind, params, flat, offsets, npix, seeds, skips):
+def _apply(kind, params, flat, offsets, npix, seeds, skips, scratch=None):
     """Run gsb_add_noise on a device tensor `flat` (float32 / float64) with per-stamp records;
-    returns the per-stamp draw counts after the call."""
+    returns the per-stamp draw counts after the call.  `scratch` (FP64, laid out like `flat`)
+    carries the per-pixel variances of variable Gaussian noise."""
     import torch
     dev = _lib.Device.torch_device()
     B = len(offsets)
@@ -127,7 +129,8 @@ def _apply(kind, params, flat, offsets, npix, seeds, skips):
         dt = _lib.F64
     else:
         raise GalSimNotImplementedError("noise is applied to float32 / float64 images here")
-    scratch = torch.empty(flat.numel() if kind != GAUSSIAN else 1, dtype=torch.float64, device=dev)
+    if scratch is None:
+        scratch = torch.empty(flat.numel() if kind in (POISSON, CCD) else 1, dtype=torch.float64, device=dev)
     used = torch.empty(B, dtype=torch.int64, device=dev)
     _lib.check(_lib.lib().gsb_add_noise(kind, ctypes.byref(params), _lib.ptr(d_rec), B,
                                         int(np.max(npix)) if B else 0, _lib.ptr(flat), dt,
@@ -319,4 +322,82 @@ class CCDNoise(BaseNoise):
             self.rng, self.sky_level, self.gain, self.read_noise)
 
 
-__all__ = ['BaseDeviate', 'BaseNoise', 'GaussianNoise', 'PoissonNoise', 'CCDNoise']
+class VariableGaussianNoise(BaseNoise):
+    """Gaussian noise with its own variance in every pixel (noise.py:590-664): pixel i gets the
+    i-th unit deviate of the stream times sqrt(var_image[i]) (GaussianDeviate.generateFromVariance,
+    Random.cpp:402-450), added in the image's type."""
+
+    def __init__(self, rng, var_image):
+        from .image import ImageD
+        BaseNoise.__init__(self, rng)
+        self._var_image = ImageD(var_image)
+
+    var_image = property(lambda self: self._var_image)
+
+    def applyTo(self, image):
+        from .image import Image
+        from .errors import GalSimIncompatibleValuesError
+        if not isinstance(image, Image):
+            raise TypeError("Provided image must be a galsim.Image")
+        if image.array.shape != self.var_image.array.shape:
+            raise GalSimIncompatibleValuesError(
+                "Provided image shape does not match the shape of var_image",
+                image=image, var_image=self.var_image)
+        self._applyTo(image)
+
+    def _params(self, dtype):
+        return VARIABLE_GAUSSIAN, NoiseParamsC()
+
+    def _variances(self, n_rep):
+        """The variances as an FP64 device buffer laid out like n_rep stamps of the image."""
+        import torch
+        var = np.ascontiguousarray(self._var_image.array, dtype=np.float64).reshape(-1)
+        t = torch.from_numpy(var).to(_lib.Device.torch_device())
+        return t.repeat(n_rep) if n_rep > 1 else t
+
+    def _applyTo(self, image):
+        import torch
+        arr = image.array
+        if arr.dtype not in (np.float32, np.float64):
+            raise GalSimNotImplementedError("noise is applied to float32 / float64 images here")
+        host = np.ascontiguousarray(arr)
+        flat = torch.from_numpy(host.reshape(-1).copy()).to(_lib.Device.torch_device())
+        st = self._rng._stream
+        used = _apply(VARIABLE_GAUSSIAN, NoiseParamsC(), flat, [0], [host.size], [st.seed], [st.used],
+                      scratch=self._variances(1))
+        arr[...] = flat.cpu().numpy().reshape(arr.shape)
+        st.used = int(used[0])
+
+    def _apply_batch(self, sb, seeds, skips=None):
+        from .errors import GalSimIncompatibleValuesError
+        B = len(sb.offsets)
+        shape = self._var_image.array.shape
+        if (np.any(np.asarray(sb.ny) != shape[0]) or np.any(np.asarray(sb.nx) != shape[1]) or
+                np.any(np.asarray(sb.offsets, np.int64) != np.arange(B, dtype=np.int64) * shape[0] * shape[1])):
+            raise GalSimIncompatibleValuesError(
+                "every stamp must have the shape of var_image", var_image=self.var_image)
+        seeds = np.broadcast_to(np.asarray(seeds, dtype=np.int64), (B,))
+        if np.any(seeds == 0):
+            raise GalSimValueError("stamp seeds must be nonzero", seeds)
+        skips = np.zeros(B, np.int64) if skips is None else np.broadcast_to(np.asarray(skips, np.int64), (B,))
+        npix = np.full(B, shape[0] * shape[1], np.int32)
+        return _apply(VARIABLE_GAUSSIAN, NoiseParamsC(), sb.flat, np.asarray(sb.offsets, np.int64), npix,
+                      seeds, skips, scratch=self._variances(B))
+
+    def copy(self, rng=None):
+        return VariableGaussianNoise(self.rng if rng is None else rng, self.var_image)
+
+    def _getVariance(self):
+        raise GalSimError("No single variance value for VariableGaussianNoise")
+
+    def _withVariance(self, variance):
+        raise GalSimError("Changing the variance is not allowed for VariableGaussianNoise")
+
+    def _withScaledVariance(self, variance):
+        raise GalSimError("Changing the variance is not allowed for VariableGaussianNoise")
+
+    def __repr__(self):
+        return 'galsim.VariableGaussianNoise(rng=%r, var_image%r)' % (self.rng, self.var_image)
+
+
+__all__ = ['BaseDeviate', 'BaseNoise', 'GaussianNoise', 'PoissonNoise', 'CCDNoise', 'VariableGaussianNoise']

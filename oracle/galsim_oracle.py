@@ -1212,14 +1212,15 @@ class OInterpolatedImageLeaf(OLeaf):
 
 
 class OInterpolatedImage(OObj):
-    """InterpolatedImage(image, scale=..., ...) (interpolatedimage.py:303-400, 481-500,
-    590-685): the padded frame, flux, stepk / maxk in world units, and the world profile
+    """InterpolatedImage(image, scale=..., ...) (interpolatedimage.py:303-400, 447-566,
+    590-685): the padded frame (with Gaussian noise padding from a BaseDeviate seed), flux,
+    stepk / maxk in world units, and the world profile
     Transform(Shift(SBInterpolatedImage, -offset), scale, flux_ratio)."""
 
     def __init__(self, array, scale, x_interp='quintic', k_interp='quintic', flux=None,
                  normalization='flux', pad_factor=4., offset=(0., 0.), use_true_center=True,
                  calculate_stepk=True, calculate_maxk=True, pad_image=None, force_stepk=0.,
-                 force_maxk=0., gsp=DEFAULT):
+                 force_maxk=0., noise_pad_size=0., noise_pad=0., rng_seed=None, gsp=DEFAULT):
         arr = np.asarray(array, dtype=float)
         ny, nx = arr.shape
         # setCenter(0, 0): pixel [0, 0] at (-(nx // 2), -(ny // 2))
@@ -1233,11 +1234,22 @@ class OInterpolatedImage(OObj):
         pad = max(nx, ny)
         if pad_factor > 1.:
             pad = int(math.ceil(pad_factor * pad))
+        npad = 0
+        if noise_pad:
+            # Gaussian noise padding (interpolatedimage.py:463-471, 521-566): a square of
+            # good_fft_size(ceil(size / scale)) pixels centred on (0, 0)
+            npad = good_fft_size(int(math.ceil(noise_pad_size / scale)))
+            pad = max(pad, npad)
         if pad_image is not None:
             pad = max(pad, *np.shape(pad_image))
         N = good_fft_size(pad)
         xim = np.zeros((N, N))
         nz = np.zeros((N, N), dtype=bool)
+        if npad:
+            noise = gaussian_noise(np.zeros((npad, npad)), base_deviate(rng_seed), math.sqrt(noise_pad))
+            h = npad // 2
+            xim[N // 2 - h:N // 2 - h + npad, N // 2 - h:N // 2 - h + npad] = noise
+            nz[N // 2 - h:N // 2 - h + npad, N // 2 - h:N // 2 - h + npad] = True
         if pad_image is not None:
             pim = np.asarray(pad_image, dtype=float)
             pny, pnx = pim.shape
@@ -1731,6 +1743,17 @@ def gaussian_noise(image, rng, sigma):
     cast to the image dtype and added."""
     g = ONormal(0., sigma)
     noise = np.array([g(rng) for _ in range(image.size)]).reshape(image.shape)
+    image += noise.astype(image.dtype)
+    return image
+
+
+def variable_gaussian_noise(image, rng, var):
+    """VariableGaussianNoise._applyTo (noise.py:633-636, GaussianDeviate::generateFromVariance,
+    Random.cpp:402-450): a fresh unit normal (pair cache cleared) per pixel in row-major order
+    times sqrt(variance), cast to the image dtype and added."""
+    g = ONormal(0., 1.)
+    v = np.asarray(var, dtype=np.float64).reshape(-1)
+    noise = np.array([g(rng) * math.sqrt(v[i]) for i in range(image.size)]).reshape(image.shape)
     image += noise.astype(image.dtype)
     return image
 

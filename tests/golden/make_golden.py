@@ -66,6 +66,8 @@ def profile(galsim, spec):
         kw = dict(spec[3])
         if 'pad_image' in kw:
             kw['pad_image'] = galsim.Image(IMAGES[kw['pad_image']])
+        if 'rng_seed' in kw:
+            kw['rng'] = galsim.BaseDeviate(kw.pop('rng_seed'))
         return galsim.InterpolatedImage(galsim.Image(IMAGES[spec[1]], scale=spec[2]), **kw)
     raise ValueError(kind)
 
@@ -133,6 +135,15 @@ INTERP_DRAW_CASES = [
     ('ii_delta_x', ('ii', 'gal24', 0.2, {'x_interpolant': 'delta'}), 32, 32, 0.2, 'f8', (0., 0.)),
     ('ii_two_images', ('conv', [('sum', [('ii', 'gal24', 0.2, {'flux': 40.}), ('exp', 0.6, 20.)]),
                                 II_PSF]), 48, 48, 0.2, 'f4', (0., 0.)),
+    # Gaussian noise padding (the padding's noise from a seeded BaseDeviate), inside the
+    # pad_factor frame and larger than it
+    ('ii_noise_pad', ('conv', [('exp', 0.4, 1.), ('ii', 'psf32', 0.2, {'noise_pad_size': 8.,
+                                                                       'noise_pad': 1e-4,
+                                                                       'rng_seed': 2024})]),
+     48, 48, 0.2, 'f8', (0., 0.)),
+    ('ii_noise_pad_big', ('ii', 'gal24', 0.3, {'noise_pad_size': 30., 'noise_pad': 2e-3,
+                                               'rng_seed': 77, 'pad_factor': 2.}),
+     64, 64, 0.3, 'f8', (0., 0.)),
     ('ii_calc_floats', ('conv', [('exp', 0.3, 1.), ('ii', 'psf32', 0.2, {'calculate_maxk': 3.0,
                                                                          'calculate_stepk': 0.5})]),
      48, 48, 0.2, 'f8', (0., 0.)),
@@ -351,6 +362,19 @@ NOISE_CASES = [
     ('ccd_odd_f4', 'ccd', 'odd', 'f4', 93, dict(sky_level=5.25, gain=2.5, read_noise=0.)),
 ]
 NOISE_BATCH_SEEDS = [1001, 1002, 1003, 1004]
+# VariableGaussianNoise: (name, image source, dtype, seed); the variance image is
+# 0.25 + 0.01 * |input| + a ramp, so it varies from pixel to pixel and stays positive
+VARNOISE_CASES = [
+    ('var_gal_f4', 'gal', 'f4', 311),
+    ('var_odd_f8', 'odd', 'f8', 312),
+    ('var_zero_f4', 'zero', 'f4', 313),
+]
+
+
+def variance_image(arr):
+    ny, nx = arr.shape
+    ramp = np.add.outer(np.arange(ny) * 0.03, np.arange(nx) * 0.02)
+    return 0.25 + 0.01 * np.abs(arr.astype(np.float64)) + ramp
 
 
 def noise_input(galsim, src, dtype):
@@ -396,6 +420,20 @@ def main_noise(ref_root):
         out['batch_in_%d' % i] = im.array.copy()
         im.addNoise(galsim.CCDNoise(galsim.BaseDeviate(seed), sky_level=50., gain=1.3, read_noise=5.))
         out['batch_out_%d' % i] = im.array.copy()
+    for name, src, dt, seed in VARNOISE_CASES:
+        im = noise_input(galsim, src, np.dtype(dt).type)
+        out['in_' + name] = im.array.copy()
+        out['var_' + name] = variance_image(im.array)
+        im.addNoise(galsim.VariableGaussianNoise(galsim.BaseDeviate(seed), galsim.ImageD(out['var_' + name])))
+        out['out_' + name] = im.array.copy()
+    # variable noise on an odd-sized image, then Gaussian noise from the same stream
+    rng = galsim.BaseDeviate(4343)
+    a = galsim.ImageF(9, 7, init_value=0.)
+    b = galsim.ImageF(6, 5, init_value=1.)
+    a.addNoise(galsim.VariableGaussianNoise(rng, galsim.ImageD(variance_image(a.array))))
+    b.addNoise(galsim.GaussianNoise(rng, sigma=2.))
+    out['varstream_a'] = a.array.copy()
+    out['varstream_b'] = b.array.copy()
     np.savez_compressed(os.path.join(HERE, 'reference_noise.npz'), **out)
     print('wrote', os.path.join(HERE, 'reference_noise.npz'), len(out), 'arrays')
 

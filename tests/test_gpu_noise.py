@@ -86,3 +86,46 @@ def test_many_blocks_and_odd_counts_vs_oracle():
         im.addNoise(galsim.GaussianNoise(r, sigma=2.5))
         assert np.allclose(im.array, ref, rtol=1e-13, atol=1e-13), (seed, np.abs(im.array - ref).max())
         assert r._stream.used == skip + 2 * ((ref.size + 1) // 2)
+
+
+@pytest.mark.parametrize('case', MG.VARNOISE_CASES, ids=[c[0] for c in MG.VARNOISE_CASES])
+def test_variable_gaussian_noise_vs_reference(case):
+    name, src, dt, seed = case
+    im = galsim.Image(GOLD['in_' + name].copy())
+    im.addNoise(galsim.VariableGaussianNoise(galsim.BaseDeviate(seed), galsim.ImageD(GOLD['var_' + name])))
+    assert_close(im.array, GOLD['out_' + name])
+
+
+def test_variable_then_gaussian_stream_vs_reference():
+    rng = galsim.BaseDeviate(4343)
+    a = galsim.ImageF(9, 7, init_value=0.)
+    b = galsim.ImageF(6, 5, init_value=1.)
+    a.addNoise(galsim.VariableGaussianNoise(rng, galsim.ImageD(MG.variance_image(a.array))))
+    assert rng._stream.used == 64
+    b.addNoise(galsim.GaussianNoise(rng, sigma=2.))
+    assert_close(a.array, GOLD['varstream_a'])
+    assert_close(b.array, GOLD['varstream_b'])
+
+
+def test_variable_gaussian_noise_batch_vs_oracle():
+    """One variance image for every stamp of a batch, each stamp with its own seed."""
+    from galsim_b200.batch import StampBatch
+    var = MG.variance_image(np.zeros((24, 20)))
+    B = 5
+    base = np.random.default_rng(3).standard_normal((B, 24, 20)).astype(np.float32)
+    dev = galsim._lib.Device.torch_device()
+    flat = torch.as_tensor(base.reshape(-1).copy(), device=dev)
+    nx, ny = np.full(B, 20), np.full(B, 24)
+    sb = StampBatch(flat, np.arange(B) * 480, nx, ny, None, None, None, None, None, np.float32, 0.2, None)
+    seeds = [71, 72, 73, 74, 75]
+    used = sb.addNoise(galsim.VariableGaussianNoise(None, galsim.ImageD(var)), seeds=seeds)
+    assert np.all(used == used[0])
+    for i, seed in enumerate(seeds):
+        ref = base[i].copy()
+        O.variable_gaussian_noise(ref, O.base_deviate(seed), var)
+        assert_close(sb.array(i), ref)
+
+
+def test_variable_gaussian_noise_shape_mismatch():
+    with pytest.raises(galsim.GalSimIncompatibleValuesError):
+        galsim.ImageF(5, 4).addNoise(galsim.VariableGaussianNoise(galsim.BaseDeviate(1), galsim.ImageD(4, 5)))

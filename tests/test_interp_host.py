@@ -33,8 +33,20 @@ def test_constructor_errors_follow_the_reference():
         galsim.InterpolatedImage(galsim.Image(np.zeros((8, 8)), scale=0.2))
     with pytest.raises(galsim.GalSimUndefinedBoundsError):
         galsim.InterpolatedImage(galsim.Image(scale=0.2))
+    # noise padding: the argument rules of _buildRealImage / _buildNoisePadImage (the Gaussian
+    # padding itself is drawn on the GPU; correlated-noise padding is not built)
+    with pytest.raises(galsim.GalSimIncompatibleValuesError):
+        galsim.InterpolatedImage(im, noise_pad=0.1)
+    with pytest.raises(galsim.GalSimIncompatibleValuesError):
+        galsim.InterpolatedImage(im, noise_pad_size=10)
+    with pytest.raises(galsim.GalSimValueError):
+        galsim.InterpolatedImage(im, noise_pad_size=-1, noise_pad=0.1)
+    with pytest.raises(galsim.GalSimRangeError):
+        galsim.InterpolatedImage(im, noise_pad_size=10, noise_pad=-0.1)
     with pytest.raises(galsim.GalSimNotImplementedError):
-        galsim.InterpolatedImage(im, noise_pad_size=10, noise_pad=0.1)
+        galsim.InterpolatedImage(im, noise_pad_size=10, noise_pad=galsim.ImageD(8, 8))
+    with pytest.raises(galsim.GalSimValueError):
+        galsim.InterpolatedImage(im, noise_pad_size=10, noise_pad=[1, 2])
     with pytest.raises(galsim.GalSimNotImplementedError):
         galsim.InterpolatedImage(im, depixelize=True)
     with pytest.raises(galsim.GalSimValueError):

@@ -47,3 +47,21 @@ def test_batch_seeds():
         img = GOLD['batch_in_%d' % i].copy()
         O.ccd_noise(img, O.base_deviate(seed), 50., 1.3, 5.)
         assert np.array_equal(img, GOLD['batch_out_%d' % i])
+
+
+@pytest.mark.parametrize('case', MG.VARNOISE_CASES, ids=[c[0] for c in MG.VARNOISE_CASES])
+def test_variable_gaussian_noise_matches_reference(case):
+    name = case[0]
+    img = GOLD['in_' + name].copy()
+    O.variable_gaussian_noise(img, O.base_deviate(case[3]), GOLD['var_' + name])
+    assert np.array_equal(img, GOLD['out_' + name]), np.abs(img - GOLD['out_' + name]).max()
+
+
+def test_variable_then_gaussian_stream():
+    rng = O.base_deviate(4343)
+    a = np.zeros((7, 9), np.float32)
+    b = np.ones((5, 6), np.float32)
+    O.variable_gaussian_noise(a, rng, MG.variance_image(a))
+    O.gaussian_noise(b, rng, 2.)
+    assert np.array_equal(a, GOLD['varstream_a'])
+    assert np.array_equal(b, GOLD['varstream_b'])
