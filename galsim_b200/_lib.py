@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(HERE, 'libgsb.so')
 
 MAX_OPS, MAX_LEAVES, MAX_PHASES, MAX_SCALES = 32, 8, 8, 8
 GAUSSIAN, EXPONENTIAL, SERSIC, MOFFAT, KOLMOGOROV, AIRY, BOX, INTERPOLATED = range(8)
-INTERP_DELTA, INTERP_NEAREST, INTERP_LINEAR, INTERP_CUBIC, INTERP_QUINTIC = range(5)
+INTERP_DELTA, INTERP_NEAREST, INTERP_LINEAR, INTERP_CUBIC, INTERP_QUINTIC, INTERP_LANCZOS = range(6)
 IMAGE_STEPK, IMAGE_MAXK, IMAGE_MAX_N = 1, 2, 4096
 OP_LEAF, OP_MUL, OP_ADD, OP_PHASE, OP_SCALE = 1, 2, 3, 4, 5
 LEAF_JAC_GENERAL, LEAF_SIZE_IS_HLR = 1, 2
@@ -60,10 +60,10 @@ XLEAF_JAC = 1
 
 IMAGE_DESC_DTYPE = np.dtype({'names': ['N', 'nx', 'ny', 'x0', 'y0', 'bx0', 'bx1', 'by0', 'by1',
                                          'x_interp', 'flags', 'pix_offset', 'flux', 'stepk_target',
-                                         'maxk_limit'],
-                              'formats': ['i4'] * 11 + ['i8', 'f8', 'f8', 'f8'],
-                              'offsets': [0, 4, 8, 12, 16, 20, 24, 28, 32, 36, 40, 48, 56, 64, 72],
-                              'itemsize': 80})
+                                         'maxk_limit', 'x_table'],
+                              'formats': ['i4'] * 11 + ['i8', 'f8', 'f8', 'f8', 'u8'],
+                              'offsets': [0, 4, 8, 12, 16, 20, 24, 28, 32, 36, 40, 48, 56, 64, 72, 80],
+                              'itemsize': 88})
 
 # gsb_fits_hdu (include/gsb.h)
 FITS_HDU_DTYPE = np.dtype({'names': ['header_src', 'header_len', 'data_src', 'n_elem', 'dst'],

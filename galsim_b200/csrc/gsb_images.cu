@@ -154,7 +154,9 @@ __global__ void __launch_bounds__(kScanThreads) kimage_scan_kernel(const ImageSl
         double thresh = maxk_threshold * d.flux;
         thresh *= thresh;
         const double max_maxk = d.maxk_limit > 0. ? d.maxk_limit
-                                                  : interp_urange(d.x_interp, kacc) / (1. / (2. * kPi));
+                                                  : (d.x_interp == GSB_INTERP_LANCZOS ? d.x_table[3]
+                                                                                      : interp_urange(d.x_interp, kacc)) /
+                                                        (1. / (2. * kPi));
         int max_ix = int(ceil(max_maxk / dk));
         if (max_ix > No2) max_ix = No2;
         for (int ix = threadIdx.x; ix <= max_ix; ix += blockDim.x) above[ix] = 0;
@@ -223,8 +225,10 @@ int images_build(gsb_tables* t, int count, const gsb_image_desc* h_desc, const d
             (d.bx0 > 0 || d.bx1 < 0 || d.by0 > 0 || d.by1 < 0 || d.bx0 < d.x0 || d.by0 < d.y0 ||
              d.bx1 >= d.x0 + d.nx || d.by1 >= d.y0 + d.ny))
             return set_error(GSB_ERR_INVALID, "stepk bounds must contain (0, 0) and lie in the region");
-        if (d.x_interp < GSB_INTERP_DELTA || d.x_interp > GSB_INTERP_QUINTIC)
+        if (d.x_interp < GSB_INTERP_DELTA || d.x_interp > GSB_INTERP_LANCZOS)
             return set_error(GSB_ERR_INVALID, "unknown x interpolant");
+        if ((d.x_interp == GSB_INTERP_LANCZOS) != (d.x_table != nullptr))
+            return set_error(GSB_ERR_INVALID, "a Lanczos x interpolant needs its x_table (and only it)");
         if (d.pix_offset < 0) return set_error(GSB_ERR_INVALID, "negative pixel offset");
         slots[i].desc = d;
         slots[i].k_offset = k_total;

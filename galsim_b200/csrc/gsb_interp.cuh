@@ -92,6 +92,27 @@ __host__ __device__ inline double interp_urange(int code, double kacc)
     return 0.;
 }
 
+// The Lanczos transform from its table (Lanczos::uval, src/Interpolant.cpp:914-919): 0 above
+// uMax, else the natural cubic spline through the nodes, found as the reference's Table finds
+// an interval of equally spaced arguments (the first node index i >= 1 with u <= u_i,
+// i = ceil((u - u_0) / du) clipped to 1..n-1).  Table layout: header {n, du, u_0, uMax}, then
+// {u, F, F'', 0} per node.
+__device__ inline double table_uval(const double* tab, double u)
+{
+    u = fabs(u);
+    const double4 hd = reinterpret_cast<const double4*>(tab)[0];
+    if (u > hd.w) return 0.;
+    const int n = int(hd.x);
+    const double4* nd = reinterpret_cast<const double4*>(tab) + 1;
+    double fi = ceil((u - hd.z) / hd.y);
+    int i = fi < 1. ? 1 : (fi > double(n - 1) ? n - 1 : int(fi));
+    const double4 a = nd[i - 1], b = nd[i];
+    const double h = b.x - a.x;
+    const double aa = (b.x - u) / h;
+    const double bb = 1. - aa;
+    return aa * a.y + bb * b.y + ((aa * aa * aa - aa) * a.z + (bb * bb * bb - bb) * b.z) * (h * h) / 6.;
+}
+
 // K(p, q) of the half-plane k-image (stored p-major: K[p N + q], p = 0..N/2) for p, q already
 // reduced to 0..N-1.
 template <typename T>
@@ -143,7 +164,10 @@ __device__ __noinline__ void ii_axis_taps(const LeafParams& L, double kp, bool s
     int n = p2 - p1 + 1;
     n = n < 0 ? 0 : (n > kInterpMaxTaps ? kInterpMaxTaps : n);
     constexpr double kUscale = 1. / (2. * kPi);
-    const double u = interp_uval<double>(xc, kp * kUscale) * (with_flux ? L.flux : 1.);
+    const double ux = kp * kUscale;
+    const double u = (xc == GSB_INTERP_LANCZOS
+                          ? table_uval(reinterpret_cast<const double*>(__double_as_longlong(L.d[5])), ux)
+                          : interp_uval<double>(xc, ux)) * (with_flux ? L.flux : 1.);
     // p - s = (p - p1) + (p1 - s): an integer plus a fraction, exact before the rounding to T
     const T off = T(double(p1) - s);
 #pragma unroll
@@ -183,7 +207,8 @@ __device__ __noinline__ Cx<T> ii_sum(const LeafParams& L, const IITaps<T>& ex, c
 
 // InterpolatedImage leaf at k index (i, j) of a grid with spacing dk.
 // d[0] = (N/2) / pi (k to sample index), d[1] = maxk1 (x interpolant cut-off), d[2] / d[3] =
-// x / k interpolant codes, d[4] = N, d[6] / d[7] = FP64 / FP32 k-image addresses.
+// x / k interpolant codes, d[4] = N, d[5] = the x interpolant's table address (Lanczos),
+// d[6] / d[7] = FP64 / FP32 k-image addresses.
 template <typename T>
 __device__ __noinline__ Cx<T> ii_kvalue(const LeafParams& L, double dk, int i, int j)
 {

@@ -1157,12 +1157,16 @@ __global__ void prepare_leaves_kernel(const __grid_constant__ gsb_template tpl, 
         const int slot = L.table;
         const int xc = int(L.p[0]), kc = int(L.p[1]);
         if (slot < 0 || slot >= images.count) { atomicOr(status_out, 16); break; }
-        if (xc < GSB_INTERP_DELTA || xc > GSB_INTERP_QUINTIC || kc < GSB_INTERP_NEAREST ||
+        if (xc < GSB_INTERP_DELTA || xc > GSB_INTERP_LANCZOS || kc < GSB_INTERP_NEAREST ||
             kc > GSB_INTERP_QUINTIC) { atomicOr(status_out, 32); break; }
         const ImageSlot& I = images.slots[slot];
+        if (xc != I.desc.x_interp) { atomicOr(status_out, 32); break; }
         const int N = I.desc.N;
         L.d[0] = (N / 2) / kPi;
-        L.d[1] = interp_urange(xc, gsp.kvalue_accuracy) / (1. / (2. * kPi));
+        // a Lanczos x interpolant's urange is its table's uMax (Lanczos::urange)
+        L.d[1] = (xc == GSB_INTERP_LANCZOS ? I.desc.x_table[3] : interp_urange(xc, gsp.kvalue_accuracy)) /
+                 (1. / (2. * kPi));
+        L.d[5] = __longlong_as_double((long long)I.desc.x_table);
         L.d[2] = xc;
         L.d[3] = kc;
         L.d[4] = N;

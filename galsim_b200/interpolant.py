@@ -3,10 +3,14 @@
 The classes carry what InterpolatedImage needs on the host: the kernel's support (xrange,
 ixrange), its Fourier extent (urange, krange), GSParams handling, equality and names.  Their
 kernels run on the GPU (galsim_b200/csrc/gsb_interp.cuh): Delta (as x interpolant only),
-Nearest, Linear, Cubic and Quintic.  Lanczos and SincInterpolant can be constructed, but an
-InterpolatedImage using them raises GalSimNotImplementedError when it is sized or drawn.
+Nearest, Linear, Cubic and Quintic, and Lanczos as the x interpolant (its transform tabulated
+on the host exactly as the reference tabulates it, then read from a device table).  Lanczos as
+the k interpolant and SincInterpolant can be constructed, but an InterpolatedImage using them
+raises GalSimNotImplementedError when it is sized or drawn.
 """
 import math
+
+import numpy as np
 
 from . import _lib
 from .errors import GalSimValueError
@@ -138,8 +142,123 @@ class Quintic(Interpolant):
     krange = property(lambda self: 1.6058208066649935 / self._gsparams.kvalue_accuracy ** (1. / 3.))
 
 
+def _si(x):
+    """The sine integral Si(x) = int_0^x sin(t) / t dt (FP64)."""
+    from scipy.special import sici
+    return sici(x)[0]
+
+
+class _LanczosTable(object):
+    """The Fourier transform of the Lanczos kernel tabulated as the reference tabulates it
+    (Lanczos::Lanczos, uCalc, uCalcRaw; src/Interpolant.cpp:719-895): the kernel's transform
+        F(u) = [(vm - 1) Si(pi (vm - 1)) - (vm + 1) Si(pi (vm + 1))
+                - (vp - 1) Si(pi (vp - 1)) + (vp + 1) Si(pi (vp + 1))] / 2 pi,
+        vp = n (2u + 1),  vm = n (2u - 1),
+    with conserve_dc the convolution by the transform of the DC-correcting factor
+    sum_j C_j (F(u - j) + F(u + j)) built from K_j = F(j), j = 1..5.  The table's abscissae are
+    u = 0, du, 2 du, ... (accumulated by repeated addition, du = table_spacing
+    (kvalue_accuracy / 200)^(1/4) / n) until u - uMax >= 1/n and u >= 1.1, where uMax is the
+    last u with |F| > kvalue_accuracy; F is interpolated by a natural cubic spline.  The
+    device reads the nodes as (u, F, F'') in one buffer (device())."""
+    _cache = {}
+
+    def __init__(self, n, conserve_dc, table_spacing, kvalue_accuracy):
+        nd = float(n)
+        self.n = n
+
+        def raw(u):
+            u = np.asarray(u, dtype=float)
+            vp = nd * (2. * u + 1.)
+            vm = nd * (2. * u - 1.)
+            r = ((vm - 1.) * _si(math.pi * (vm - 1.)) - (vm + 1.) * _si(math.pi * (vm + 1.)) -
+                 (vp - 1.) * _si(math.pi * (vp - 1.)) + (vp + 1.) * _si(math.pi * (vp + 1.)))
+            return r / (2. * math.pi)
+
+        K = [0.] + [float(raw(float(j))) for j in range(1, 6)]
+        C = [1. + 2. * (K[1] * (1. + 3. * K[1] + K[2] + K[3]) + K[2] + K[3] + K[4] + K[5]),
+             -K[1] * (1. + 4. * K[1] + K[2] + 2. * K[3]),
+             K[1] * (K[1] - 2. * K[2] + K[3]) - K[2],
+             K[1] * (K[1] - 2. * K[3]) - K[3],
+             K[1] * K[3] - K[4],
+             -K[5]]
+        self.K, self.C = K, C
+
+        def ucalc(u):
+            r = raw(u)
+            if conserve_dc:
+                r = r * C[0]
+                for j in range(1, 6):
+                    r = r + C[j] * (raw(u + j) + raw(u - j))
+            return r
+
+        ustep = table_spacing * (kvalue_accuracy / 200.) ** 0.25 / nd
+        # the reference's loop: for (u = 0; u - uMax < 1/n || u < 1.1; u += du) { add u;
+        # uMax = u where |F(u)| > kvalue_accuracy }; the abscissae are accumulated in its
+        # order, the values evaluated a chunk at a time and the loop condition walked in order
+        us, vals = [], np.empty(0)
+        u = 0.
+        umax = 0.
+        k = 0
+        while True:
+            if k == len(us):
+                chunk = []
+                for _ in range(1024):
+                    chunk.append(u)
+                    u += ustep
+                us.extend(chunk)
+                vals = np.concatenate([vals, ucalc(np.array(chunk))])
+            uk = us[k]
+            if not (uk - umax < 1. / nd or uk < 1.1):
+                break
+            if abs(vals[k]) > kvalue_accuracy:
+                umax = uk
+            k += 1
+        us, vals = us[:k], vals[:k]
+        from .table import _LookupTable
+        self.umax = umax
+        self.table = _LookupTable(np.array(us), np.array(vals), 'spline')
+
+    @classmethod
+    def get(cls, n, conserve_dc, gsparams):
+        key = (n, conserve_dc, gsparams.table_spacing, gsparams.kvalue_accuracy)
+        t = cls._cache.get(key)
+        if t is None:
+            t = cls(n, conserve_dc, gsparams.table_spacing, gsparams.kvalue_accuracy)
+            cls._cache[key] = t
+        return t
+
+    def uval(self, u):
+        """F(|u|), 0 beyond uMax (Lanczos::uval)."""
+        u = np.abs(np.asarray(u, dtype=float))
+        v = self.table(np.minimum(u, self.table.x_max))
+        return np.where(u > self.umax, 0., v)
+
+    def device(self):
+        """The table as one FP64 device buffer of 4 (n + 1) doubles: a header (node count,
+        mean spacing, u of the first node, uMax), then per node (u, F(u), F''(u), 0)."""
+        import torch
+        dev = _lib.Device.torch_device()
+        key = ('dev', dev.index)
+        t = self.__dict__.get(key)
+        if t is None:
+            tb = self.table
+            n = len(tb.x)
+            a = np.zeros((n + 1, 4))
+            a[0] = (n, (tb.x[-1] - tb.x[0]) / (n - 1), tb.x[0], self.umax)
+            a[1:, 0] = tb.x
+            a[1:, 1] = tb.f
+            a[1:, 2] = tb._y2
+            t = torch.from_numpy(a.reshape(-1)).to(dev)
+            self.__dict__[key] = t
+        return t
+
+
 class Lanczos(Interpolant):
-    """Lanczos filter sinc(x) sinc(x / n) (interpolant.py:604-670); not built on the GPU."""
+    """Lanczos filter sinc(x) sinc(x / n) with the DC-conserving correction
+    (interpolant.py:604-670, src/Interpolant.cpp:560-930).  On the GPU it serves as an
+    InterpolatedImage's x interpolant (its transform from the reference's spline table,
+    _LanczosTable); as the k interpolant it is not built."""
+    _code = _lib.INTERP_LANCZOS
 
     def __init__(self, n, conserve_dc=True, tol=None, gsparams=None):
         if tol is not None:
@@ -154,9 +273,19 @@ class Lanczos(Interpolant):
     ixrange = property(lambda self: 2 * self._n)
 
     @property
+    def _table(self):
+        return _LanczosTable.get(self._n, self._conserve_dc, self._gsparams)
+
+    @property
+    def urange(self):
+        return self._table.umax
+
+    @property
     def krange(self):
-        from .errors import GalSimNotImplementedError
-        raise GalSimNotImplementedError("Lanczos interpolants are not built on the GPU")
+        return 2. * math.pi * self._table.umax
+
+    def uval(self, u):
+        return self._table.uval(u)
 
     def _args(self):
         return (self._n, self._conserve_dc)

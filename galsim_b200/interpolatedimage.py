@@ -14,8 +14,11 @@ Batches: `image` may be a list of Images (every option applies to each); the obj
 a batch of len(image) profiles, each with its own padded frame.  A single image broadcasts
 against batched objects it is combined with.
 
-Not built: noise padding (it needs the reference's random-number streams), depixelize, FITS
-file names, non-PixelScale WCS, and Lanczos / sinc interpolants.
+Noise padding with Gaussian noise of a given variance (noise_pad a number) fills its square of
+the frame with the reference's stream (BaseDeviate(rng), drawn on the GPU) before the pad image
+and the image are placed.  Not built: padding with correlated noise (a CorrelatedNoise, an
+image or a file), depixelize, FITS file names, non-PixelScale WCS, the sinc interpolant and
+Lanczos as the k interpolant (Lanczos as the x interpolant is built).
 """
 import math
 
@@ -28,7 +31,7 @@ from .errors import (GalSimIncompatibleValuesError, GalSimNotImplementedError, G
 from .gsobject import GSObject
 from .gsparams import GSParams
 from .image import Image
-from .interpolant import Delta, Quintic, convert_interpolant
+from .interpolant import Delta, Lanczos, Quintic, convert_interpolant
 from .position import _PositionD
 from .wcs import BaseWCS, PixelScale
 
@@ -38,7 +41,7 @@ class _ImageSource(object):
     and the scan settings for its stepk / maxk (one gsb_image_desc)."""
 
     def __init__(self, region, N, x0, y0, stepk_bounds, x_code, flags, nz_flux, stepk_target,
-                 maxk_limit):
+                 maxk_limit, x_interpolant=None):
         self.region = np.ascontiguousarray(region, dtype=np.float64)
         self.N = int(N)
         self.x0, self.y0 = int(x0), int(y0)
@@ -48,6 +51,7 @@ class _ImageSource(object):
         self.nz_flux = float(nz_flux)
         self.stepk_target = float(stepk_target)
         self.maxk_limit = float(maxk_limit)
+        self.x_interpolant = x_interpolant   # a Lanczos x interpolant carries a device table
 
     def desc(self, pix_offset):
         d = np.zeros((), dtype=_lib.IMAGE_DESC_DTYPE)
@@ -61,6 +65,8 @@ class _ImageSource(object):
         d['flux'] = self.nz_flux
         d['stepk_target'] = self.stepk_target
         d['maxk_limit'] = self.maxk_limit
+        d['x_table'] = (self.x_interpolant._table.device().data_ptr()
+                        if isinstance(self.x_interpolant, Lanczos) else 0)
         return d
 
 
@@ -79,10 +85,11 @@ class _ImageLeaf(GSObject):
 
     def _flatten(self, bld, jac):
         xi, ki = self._x_interpolant, self._k_interpolant
-        if xi._code is None or ki._code is None or isinstance(ki, Delta):
+        if xi._code is None or ki._code is None or isinstance(ki, (Delta, Lanczos)):
             raise GalSimNotImplementedError(
                 "InterpolatedImage with x interpolant %s and k interpolant %s is not built on the "
-                "GPU (x: Delta, Nearest, Linear, Cubic, Quintic; k: the same but Delta)" % (xi, ki))
+                "GPU (x: Delta, Nearest, Linear, Cubic, Quintic, Lanczos; k: Nearest, Linear, "
+                "Cubic, Quintic)" % (xi, ki))
         bld.add_leaf(_lib.INTERPOLATED, jac, 1., (float(xi._code), float(ki._code), 0.))
         bld.image_sources[len(bld.leaves) - 1] = self._sources
 
@@ -277,7 +284,7 @@ class InterpolatedImage(GSObject):
             thresh = (1. - self._gsparams.folding_threshold) * image_flux
             sources.append(_ImageSource(region, N, nz.xmin, nz.ymin, (b.xmin, b.xmax, b.ymin, b.ymax),
                                         x_code, flags, float(np.sum(region, dtype=np.float64)),
-                                        thresh, maxk_limit))
+                                        thresh, maxk_limit, self._x_interpolant))
             scales.append(w.scale)
             offsets.append((off.x, off.y))
             fluxes.append(f)

@@ -57,7 +57,9 @@ enum {
     GSB_INTERP_NEAREST = 1,
     GSB_INTERP_LINEAR  = 2,
     GSB_INTERP_CUBIC   = 3,
-    GSB_INTERP_QUINTIC = 4
+    GSB_INTERP_QUINTIC = 4,
+    GSB_INTERP_LANCZOS = 5    /* x interpolant only: the transform from the image's x_table
+                                 (the reference's spline table of Lanczos::uCalc)          */
 };
 
 /* Program opcodes.  A program is evaluated per k-point on a small stack of complex values:
@@ -237,6 +239,11 @@ typedef struct gsb_image_desc {
     double stepk_target;    /* (1 - folding_threshold) * image flux (interpolatedimage.py:657) */
     double maxk_limit;      /* max_maxk of calculateMaxK in image units; 0 = the x
                                interpolant's 2 pi urange (SBInterpolatedImage.cpp:135-151) */
+    const double* x_table;  /* GSB_INTERP_LANCZOS: device table of the x interpolant's
+                               transform, 4 (n + 1) doubles: {n, mean spacing, u_0, uMax},
+                               then per node {u, F(u), F''(u), 0} of a natural cubic spline
+                               on equally spaced u (Lanczos::Lanczos, Interpolant.cpp:787-895);
+                               NULL for the other interpolants */
 } gsb_image_desc;
 
 #define GSB_IMAGE_STEPK 1

@@ -1063,9 +1063,94 @@ def _sinc(u):
     return np.where(np.abs(u) < 1.e-4, 1. - (PI * PI / 6.) * u * u, v)
 
 
-def interp_uval(name, u):
-    """Fourier transforms of the kernels (Interpolant.cpp:176, 251-255, 292-302, 435-461)."""
+def _lanczos_name(name):
+    """(n, conserve_dc) of 'lanczosN' / 'lanczosNF' / 'lanczosNT' (interpolant.py:64-110), else None."""
+    if not name.startswith('lanczos'):
+        return None
+    body = name[7:].upper()
+    dc = not body.endswith('F')
+    return int(body.rstrip('FT')), dc
+
+
+_LANCZOS = {}
+
+
+def lanczos_table(n, conserve_dc=True, gsp=DEFAULT):
+    """The reference's tabulated Lanczos transform (Lanczos::Lanczos / uCalc / uCalcRaw,
+    Interpolant.cpp:719-895): F(u) from sine integrals, with the DC-conserving convolution when
+    conserve_dc, at u = 0, du, 2 du, ... (repeated addition, du = table_spacing (kvalue_accuracy
+    / 200)^(1/4) / n) while u - uMax < 1/n or u < 1.1, uMax the last u with |F| > kvalue_accuracy;
+    returned as (u, F, F'' of the natural cubic spline, uMax)."""
+    key = (n, conserve_dc, gsp.table_spacing, gsp.kvalue_accuracy)
+    if key in _LANCZOS:
+        return _LANCZOS[key]
+    nd = float(n)
+    si = lambda x: special.sici(x)[0]
+
+    def raw(u):
+        vp, vm = nd * (2. * u + 1.), nd * (2. * u - 1.)
+        return ((vm - 1.) * si(PI * (vm - 1.)) - (vm + 1.) * si(PI * (vm + 1.)) -
+                (vp - 1.) * si(PI * (vp - 1.)) + (vp + 1.) * si(PI * (vp + 1.))) / (2. * PI)
+
+    K = [0.] + [float(raw(float(j))) for j in range(1, 6)]
+    C = [1. + 2. * (K[1] * (1. + 3. * K[1] + K[2] + K[3]) + K[2] + K[3] + K[4] + K[5]),
+         -K[1] * (1. + 4. * K[1] + K[2] + 2. * K[3]), K[1] * (K[1] - 2. * K[2] + K[3]) - K[2],
+         K[1] * (K[1] - 2. * K[3]) - K[3], K[1] * K[3] - K[4], -K[5]]
+
+    def ucalc(u):
+        r = raw(u)
+        if conserve_dc:
+            r = r * C[0] + sum(C[j] * (raw(u + j) + raw(u - j)) for j in range(1, 6))
+        return r
+
+    du = gsp.table_spacing * (gsp.kvalue_accuracy / 200.) ** 0.25 / nd
+    us, fs = [], []
+    u, umax = 0., 0.
+    while u - umax < 1. / nd or u < 1.1:
+        f = float(ucalc(u))
+        us.append(u)
+        fs.append(f)
+        if abs(f) > gsp.kvalue_accuracy:
+            umax = u
+        u += du
+    x, f = np.array(us), np.array(fs)
+    # natural cubic spline: h_{i-1} y2_{i-1} + 2 (h_{i-1} + h_i) y2_i + h_i y2_{i+1} = 6 (slope jumps)
+    h = np.diff(x)
+    m = len(x)
+    ab = np.zeros((3, m - 2))
+    ab[0, 1:] = h[1:-1]
+    ab[1] = 2. * (h[:-1] + h[1:])
+    ab[2, :-1] = h[1:-1]
+    rhs = 6. * (np.diff(f[1:]) / h[1:] - np.diff(f[:-1]) / h[:-1])
+    from scipy.linalg import solve_banded
+    y2 = np.zeros(m)
+    y2[1:-1] = solve_banded((1, 1), ab, rhs)
+    _LANCZOS[key] = (x, f, y2, umax)
+    return _LANCZOS[key]
+
+
+def lanczos_uval(n, conserve_dc, u, gsp=DEFAULT):
+    """Lanczos::uval: the spline of lanczos_table at |u|, 0 above uMax; the interval from the
+    equal-spacing lookup of the reference's Table (first node index i >= 1 with u <= u_i)."""
+    x, f, y2, umax = lanczos_table(n, conserve_dc, gsp)
+    u = np.abs(np.asarray(u, dtype=float))
+    m = len(x)
+    da = (x[-1] - x[0]) / (m - 1)
+    i = np.clip(np.ceil((u - x[0]) / da), 1, m - 1).astype(np.int64)
+    hh = x[i] - x[i - 1]
+    aa = (x[i] - u) / hh
+    bb = 1. - aa
+    v = aa * f[i - 1] + bb * f[i] + ((aa ** 3 - aa) * y2[i - 1] + (bb ** 3 - bb) * y2[i]) * hh * hh / 6.
+    return np.where(u > umax, 0., v)
+
+
+def interp_uval(name, u, gsp=DEFAULT):
+    """Fourier transforms of the kernels (Interpolant.cpp:176, 251-255, 292-302, 435-461;
+    Lanczos from its table, 914-919)."""
     u = np.asarray(u, dtype=float)
+    lz = _lanczos_name(name)
+    if lz is not None:
+        return lanczos_uval(lz[0], lz[1], u, gsp)
     if name == 'delta':
         return np.ones_like(u)
     s = _sinc(u)
@@ -1083,11 +1168,23 @@ def interp_uval(name, u):
     raise ValueError(name)
 
 
-INTERP_XRANGE = {'delta': 0., 'nearest': 0.5, 'linear': 1., 'cubic': 2., 'quintic': 3.}
+class _XRange(dict):
+    """Interpolant::xrange by name; 'lanczosN' has range n."""
+
+    def __missing__(self, name):
+        return float(_lanczos_name(name)[0])
 
 
-def interp_urange(name, kacc):
-    """Interpolant::urange (include/galsim/Interpolant.h:237-428, Interpolant.cpp:364, 518)."""
+INTERP_XRANGE = _XRange({'delta': 0., 'nearest': 0.5, 'linear': 1., 'cubic': 2., 'quintic': 3.})
+
+
+def interp_urange(name, kacc, gsp=None):
+    """Interpolant::urange (include/galsim/Interpolant.h:237-428, Interpolant.cpp:364, 518;
+    Lanczos: its table's uMax)."""
+    lz = _lanczos_name(name)
+    if lz is not None:
+        g = gsp if gsp is not None else OGSParams(kvalue_accuracy=kacc)
+        return lanczos_table(lz[0], lz[1], g)[3]
     return {'delta': lambda: 1. / kacc,
             'nearest': lambda: 1. / (PI * kacc),
             'linear': lambda: math.sqrt(1. / kacc) / PI,
@@ -1095,8 +1192,10 @@ def interp_urange(name, kacc):
             'quintic': lambda: math.pow((25. * math.sqrt(5.) / 108.) / kacc, 1. / 3.) / PI}[name]()
 
 
-def interp_krange(name, kacc):
-    """Interpolant.krange (interpolant.py:264, 328, 462, 528, 597)."""
+def interp_krange(name, kacc, gsp=None):
+    """Interpolant.krange (interpolant.py:264, 328, 462, 528, 597, 667)."""
+    if _lanczos_name(name) is not None:
+        return 2. * PI * interp_urange(name, kacc, gsp)
     return {'delta': 2. * PI / kacc, 'nearest': 2. / kacc, 'linear': 2. / kacc ** 0.5,
             'cubic': 1.7320508075688774 / kacc ** (1. / 3.),
             'quintic': 1.6058208066649935 / kacc ** (1. / 3.)}[name]
@@ -1137,7 +1236,7 @@ class OInterpolatedImageLeaf(OLeaf):
         self.xr = INTERP_XRANGE[k_interp]
         self.kscale = (N // 2) / PI
         self.uscale = 1. / (2. * PI)
-        self.maxk1 = interp_urange(x_interp, gsp.kvalue_accuracy) / self.uscale
+        self.maxk1 = interp_urange(x_interp, gsp.kvalue_accuracy, gsp) / self.uscale
         self.gsp = gsp
 
     def _taps(self, s, shortcut):
@@ -1164,7 +1263,7 @@ class OInterpolatedImageLeaf(OLeaf):
         N = self.N
         vals = self.K[(py[..., :, None] % N), (px[..., None, :] % N)]
         s = np.einsum('...ba,...a,...b->...', vals, wx, wy)
-        fac = interp_uval(self.xi, KX * self.uscale) * interp_uval(self.xi, KY * self.uscale)
+        fac = interp_uval(self.xi, KX * self.uscale, self.gsp) * interp_uval(self.xi, KY * self.uscale, self.gsp)
         out = fac * s
         return np.where((np.abs(KX) > self.maxk1) | (np.abs(KY) > self.maxk1), 0., out)
 
@@ -1282,7 +1381,7 @@ class OInterpolatedImage(OObj):
             mm = 0. if calculate_maxk is True else float(calculate_maxk)
             self.maxk = self.leaf.max_k(nz_flux, mm) / scale
         else:
-            self.maxk = interp_krange(x_interp, gsp.kvalue_accuracy) / scale
+            self.maxk = interp_krange(x_interp, gsp.kvalue_accuracy, gsp) / scale
         prof = self.leaf
         if dx != 0. or dy != 0.:
             prof = OTransform(prof, offset=(-dx, -dy))

@@ -144,6 +144,16 @@ INTERP_DRAW_CASES = [
     ('ii_noise_pad_big', ('ii', 'gal24', 0.3, {'noise_pad_size': 30., 'noise_pad': 2e-3,
                                                'rng_seed': 77, 'pad_factor': 2.}),
      64, 64, 0.3, 'f8', (0., 0.)),
+    # Lanczos x interpolants (their transform from the reference's spline table), with and
+    # without the DC correction, FP64 and FP32 draws
+    ('ii_lanczos5_x', ('conv', [('exp', 0.4, 1.), ('ii', 'psf32', 0.2, {'x_interpolant': 'lanczos5'})]),
+     48, 48, 0.2, 'f8', (0., 0.)),
+    ('ii_lanczos3F_x_cubic_k', ('ii', 'gal24', 0.25, {'x_interpolant': 'lanczos3F',
+                                                      'k_interpolant': 'cubic'}),
+     40, 40, 0.25, 'f8', (0.2, -0.1)),
+    ('ii_lanczos7_x_f4', ('conv', [('sersic', 2.5, 0.5, 1e3), ('ii', 'psf31x33', 0.2,
+                                                               {'x_interpolant': 'lanczos7'})]),
+     48, 48, 0.2, 'f4', (0., 0.)),
     ('ii_calc_floats', ('conv', [('exp', 0.3, 1.), ('ii', 'psf32', 0.2, {'calculate_maxk': 3.0,
                                                                          'calculate_stepk': 0.5})]),
      48, 48, 0.2, 'f8', (0., 0.)),

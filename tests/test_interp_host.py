@@ -89,6 +89,12 @@ def test_interpolants():
     assert galsim.Linear().krange == 2. / 1e-5 ** 0.5
     assert galsim.Nearest().ixrange == 1 and galsim.Quintic().ixrange == 6
     assert galsim.Delta().krange == 2. * math.pi / 1e-5
+    # Lanczos: the transform's extent is its table's uMax (Lanczos::urange); the transform is 1
+    # at u = 0 and, conserving DC, vanishes at the other integers to the table's accuracy
+    lz = galsim.Lanczos(5)
+    assert lz.krange == 2. * math.pi * lz.urange and 3. < lz.urange < 6.
+    assert abs(lz.uval(0.) - 1.) < 1e-5 and abs(lz.uval(1.)) < 1e-5
+    assert galsim.Lanczos(3, tol=1e-4).urange < galsim.Lanczos(3).urange
 
 
 def test_program_layout():
@@ -108,13 +114,18 @@ def test_program_layout():
     gal = galsim.Exponential(half_light_radius=np.array([0.4, 0.6]))
     p2 = Program(galsim.Convolve(gal, iib))
     assert p2.B == 2 and len(p2.bld.image_sources[1]) == 2
+    # a Lanczos x interpolant is built (its transform from a device table); as the k
+    # interpolant it is not
+    p3 = Program(galsim.InterpolatedImage(_img(), x_interpolant='lanczos3'))
+    assert p3.bld.leaves[0]['p'][0, 0] == _lib.INTERP_LANCZOS
     with pytest.raises(galsim.GalSimNotImplementedError):
-        Program(galsim.InterpolatedImage(_img(), x_interpolant='lanczos3'))
+        Program(galsim.InterpolatedImage(_img(), k_interpolant='lanczos3'))
     with pytest.raises(galsim.GalSimNotImplementedError):
         Program(galsim.InterpolatedImage(_img(), k_interpolant='delta'))
 
 
 def test_image_desc_layout_matches_the_c_struct():
     d = _lib.IMAGE_DESC_DTYPE
-    assert d.itemsize == 80
+    assert d.itemsize == 88
     assert d.fields['pix_offset'][1] == 48 and d.fields['maxk_limit'][1] == 72
+    assert d.fields['x_table'][1] == 80
