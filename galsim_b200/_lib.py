@@ -23,6 +23,7 @@ OP_LEAF, OP_MUL, OP_ADD, OP_PHASE, OP_SCALE = 1, 2, 3, 4, 5
 LEAF_JAC_GENERAL, LEAF_SIZE_IS_HLR = 1, 2
 PHASE_JAC_GENERAL = 1
 F32, F64 = 0, 1
+I16, I32, U16, U32 = 2, 3, 4, 5        # integer image types (gsb_add_noise)
 TABLES_DN = 1
 WANT_ALL = 0xffffffff
 GRAD_PER_LEAF, GRAD_PER_PHASE = 6, 7

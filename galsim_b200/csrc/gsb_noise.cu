@@ -304,6 +304,34 @@ struct NoiseArgs {
     long long* used;       // draws used per stamp (Poisson pass -> read-noise pass)
 };
 
+// A double as a pixel of type T the way the reference's numpy casts it (astype / copyto with
+// casting='unsafe', a C conversion on x86): floats round to nearest; integers truncate toward
+// zero and keep the low bits of the type's width (a negative value in an unsigned image wraps,
+// as x86's conversion through a wider signed integer leaves it).
+template <typename T>
+__device__ __forceinline__ T to_pixel(double v) { return T(v); }
+template <>
+__device__ __forceinline__ int16_t to_pixel<int16_t>(double v) { return int16_t(int(v)); }
+template <>
+__device__ __forceinline__ uint16_t to_pixel<uint16_t>(double v) { return uint16_t(int(v)); }
+template <>
+__device__ __forceinline__ int32_t to_pixel<int32_t>(double v) { return int32_t(v); }
+template <>
+__device__ __forceinline__ uint32_t to_pixel<uint32_t>(double v) { return uint32_t((long long)v); }
+
+// pixel += noise.astype(T): in the pixel type, integers wrapping at their width
+template <typename T>
+__device__ __forceinline__ T add_pixel(T a, double d) { return a + to_pixel<T>(d); }
+template <>
+__device__ __forceinline__ int32_t add_pixel<int32_t>(int32_t a, double d)
+{
+    return int32_t(uint32_t(a) + uint32_t(to_pixel<int32_t>(d)));
+}
+template <>
+__device__ __forceinline__ int16_t add_pixel<int16_t>(int16_t a, double d) { return int16_t(a + to_pixel<int16_t>(d)); }
+template <>
+__device__ __forceinline__ uint16_t add_pixel<uint16_t>(uint16_t a, double d) { return uint16_t(a + to_pixel<uint16_t>(d)); }
+
 // The cast back into the image and the sky bookkeeping of PoissonNoise / CCDNoise._applyTo:
 // frac_sky is subtracted in FP64 before the cast, int_sky after it (in the image type when the
 // caller's int_sky has the image's type, as Image.__isub__ does).
@@ -311,8 +339,9 @@ template <typename T>
 __device__ __forceinline__ T finish_pixel(double w, const gsb_noise_params& p)
 {
     if (p.frac_sky != 0.) w -= p.frac_sky;
-    T out = T(w);
-    if (p.int_sky != 0.) out = p.int_sky_same_dtype ? T(out - T(p.int_sky)) : T(double(out) - p.int_sky);
+    T out = to_pixel<T>(w);
+    if (p.int_sky != 0.)
+        out = p.int_sky_same_dtype ? T(out - T(p.int_sky)) : to_pixel<T>(double(out) - p.int_sky);
     return out;
 }
 
@@ -332,9 +361,9 @@ __global__ void __launch_bounds__(kNoiseWarps * 32) gauss_kernel(const __grid_co
     if (a.kind == GSB_NOISE_VARIABLE_GAUSSIAN) {
         // unit deviates scaled by each pixel's own sigma (GaussianDeviate::generateFromVariance)
         const double* var = a.scratch + sp.offset;
-        gaussian_run(st, sp.npix, 1., [&](long long j, double d) { img[j] = img[j] + T(d * sqrt(var[j])); });
+        gaussian_run(st, sp.npix, 1., [&](long long j, double d) { img[j] = add_pixel<T>(img[j], d * sqrt(var[j])); });
     } else {
-        gaussian_run(st, sp.npix, a.p.sigma, [&](long long j, double d) { img[j] = img[j] + T(d); });
+        gaussian_run(st, sp.npix, a.p.sigma, [&](long long j, double d) { img[j] = add_pixel<T>(img[j], d); });
     }
     if (lane == 0 && a.used) a.used[s] = st.used;      // draws consumed since seeding
 }
@@ -677,7 +706,15 @@ int add_noise(int kind, const gsb_noise_params* p, const gsb_noise_stamp* d_stam
     a.dtype = dtype;
     a.scratch = d_scratch;
     a.used = d_used;
-    return dtype == GSB_F32 ? launch_noise<float>(a, max_npix, stream) : launch_noise<double>(a, max_npix, stream);
+    switch (dtype) {
+      case GSB_F32: return launch_noise<float>(a, max_npix, stream);
+      case GSB_F64: return launch_noise<double>(a, max_npix, stream);
+      case GSB_I16: return launch_noise<int16_t>(a, max_npix, stream);
+      case GSB_I32: return launch_noise<int32_t>(a, max_npix, stream);
+      case GSB_U16: return launch_noise<uint16_t>(a, max_npix, stream);
+      case GSB_U32: return launch_noise<uint32_t>(a, max_npix, stream);
+    }
+    return set_error(GSB_ERR_INVALID, "unknown image dtype");
 }
 
 }  // namespace gsb
@@ -694,7 +731,7 @@ extern "C" int gsb_add_noise(int kind, const gsb_noise_params* p, const gsb_nois
         return set_error(GSB_ERR_INVALID, "unknown noise kind");
     if (kind == GSB_NOISE_VARIABLE_GAUSSIAN && n_stamps > 0 && !d_scratch)
         return set_error(GSB_ERR_INVALID, "variable Gaussian noise needs the variance of every pixel in d_scratch");
-    if (dtype != GSB_F32 && dtype != GSB_F64) return set_error(GSB_ERR_INVALID, "image dtype must be F32 or F64");
+    if (dtype < GSB_F32 || dtype > GSB_U32) return set_error(GSB_ERR_INVALID, "image dtype must be F32, F64, I16, I32, U16 or U32");
     if ((kind == GSB_NOISE_POISSON || kind == GSB_NOISE_CCD) && (!d_scratch || !d_used))
         return set_error(GSB_ERR_INVALID, "Poisson and CCD noise need the FP64 scratch and the draw counts");
     if (max_npix < 0) return set_error(GSB_ERR_INVALID, "negative pixel count");

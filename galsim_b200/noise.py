@@ -107,6 +107,23 @@ def _sky_split(sky_level, dtype):
     return float(frac_sky), float(int_sky), bool(same)
 
 
+def _torch_codes():
+    import torch
+    return {torch.float32: _lib.F32, torch.float64: _lib.F64, torch.int16: _lib.I16,
+            torch.int32: _lib.I32, torch.uint16: _lib.U16, torch.uint32: _lib.U32}
+
+
+class _Codes(dict):
+    def get(self, k, default=None):
+        if not self:
+            self.update(_torch_codes())
+        return dict.get(self, k, default)
+
+
+_TORCH_CODES = _Codes()
+_IMAGE_TYPES = (np.float32, np.float64, np.int16, np.int32, np.uint16, np.uint32)
+
+
 def _apply(kind, params, flat, offsets, npix, seeds, skips, scratch=None):
     """Run gsb_add_noise on a device tensor `flat` (float32 / float64) with per-stamp records;
     returns the per-stamp draw counts after the call.  `scratch` (FP64, laid out like `flat`)
@@ -123,12 +140,10 @@ def _apply(kind, params, flat, offsets, npix, seeds, skips, scratch=None):
     rec['seed'] = np.broadcast_to(np.asarray(seeds, np.int64), (B,))[order]
     rec['skip'] = np.broadcast_to(np.asarray(skips, np.int64), (B,))[order]
     d_rec = _lib.to_device(rec)
-    if flat.dtype == torch.float32:
-        dt = _lib.F32
-    elif flat.dtype == torch.float64:
-        dt = _lib.F64
-    else:
-        raise GalSimNotImplementedError("noise is applied to float32 / float64 images here")
+    dt = _TORCH_CODES.get(flat.dtype)
+    if dt is None:
+        raise GalSimNotImplementedError("noise is applied to float32 / float64 / int16 / int32 / "
+                                        "uint16 / uint32 images")
     if scratch is None:
         scratch = torch.empty(flat.numel() if kind in (POISSON, CCD) else 1, dtype=torch.float64, device=dev)
     used = torch.empty(B, dtype=torch.int64, device=dev)
@@ -196,8 +211,9 @@ class BaseNoise(object):
     def _applyTo(self, image):
         import torch
         arr = image.array
-        if arr.dtype not in (np.float32, np.float64):
-            raise GalSimNotImplementedError("noise is applied to float32 / float64 images here")
+        if arr.dtype not in _IMAGE_TYPES:
+            raise GalSimNotImplementedError("noise is applied to float32 / float64 / int16 / int32 / "
+                                            "uint16 / uint32 images")
         kind, params = self._params(arr.dtype)
         host = np.ascontiguousarray(arr)
         flat = torch.from_numpy(host.reshape(-1).copy()).to(_lib.Device.torch_device())
@@ -358,8 +374,9 @@ class VariableGaussianNoise(BaseNoise):
     def _applyTo(self, image):
         import torch
         arr = image.array
-        if arr.dtype not in (np.float32, np.float64):
-            raise GalSimNotImplementedError("noise is applied to float32 / float64 images here")
+        if arr.dtype not in _IMAGE_TYPES:
+            raise GalSimNotImplementedError("noise is applied to float32 / float64 / int16 / int32 / "
+                                            "uint16 / uint32 images")
         host = np.ascontiguousarray(arr)
         flat = torch.from_numpy(host.reshape(-1).copy()).to(_lib.Device.torch_device())
         st = self._rng._stream

@@ -144,7 +144,9 @@ typedef struct gsb_stamp {
 } gsb_stamp;
 
 /* Output dtypes */
-enum { GSB_F32 = 0, GSB_F64 = 1 };
+enum { GSB_F32 = 0, GSB_F64 = 1,
+       /* integer image types, accepted by gsb_add_noise only */
+       GSB_I16 = 2, GSB_I32 = 3, GSB_U16 = 4, GSB_U32 = 5 };
 
 typedef struct gsb_tables gsb_tables;   /* opaque: device-resident FT tables */
 
@@ -338,7 +340,9 @@ typedef struct gsb_noise_params {
     int32_t pad;
 } gsb_noise_params;
 
-/* Add noise of `kind` to n_stamps stamps of d_image (GSB_F32 or GSB_F64); max_npix bounds the
+/* Add noise of `kind` to n_stamps stamps of d_image (GSB_F32, GSB_F64, or an integer type:
+ * GSB_I16 / I32 / U16 / U32, cast as numpy's unsafe cast does on the reference's host --
+ * truncation toward zero, wrapping to the type's width); max_npix bounds the
  * stamps' pixel counts.  Poisson and CCD noise need d_scratch (one double per pixel, addressed
  * like d_image) and d_used.  GSB_NOISE_VARIABLE_GAUSSIAN (VariableGaussianNoise, noise.py:590-636,
  * Random.cpp:402-450) reads each pixel's variance from d_scratch (FP64, addressed like d_image,

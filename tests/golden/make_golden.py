@@ -370,6 +370,13 @@ NOISE_CASES = [
     ('ccd_gal_f4', 'ccd', 'gal', 'f4', 91, dict(sky_level=35.5, gain=1.7, read_noise=4.4)),
     ('ccd_gal_f8_gain0', 'ccd', 'gal', 'f8', 92, dict(sky_level=20., gain=0., read_noise=3.)),
     ('ccd_odd_f4', 'ccd', 'odd', 'f4', 93, dict(sky_level=5.25, gain=2.5, read_noise=0.)),
+    # integer images: numpy's unsafe casts, the integer part of the sky subtracted after the cast
+    ('gauss_gal_i4', 'gauss', 'gal', 'i4', 94, dict(sigma=2.5)),
+    ('gauss_odd_u2', 'gauss', 'odd', 'u2', 95, dict(sigma=1.5)),
+    ('poisson_gal_i2_sky', 'poisson', 'gal', 'i2', 96, dict(sky_level=12.3)),
+    ('poisson_odd_u4', 'poisson', 'odd', 'u4', 97, dict(sky_level=3.)),
+    ('ccd_gal_u2', 'ccd', 'gal', 'u2', 98, dict(sky_level=40.7, gain=1.7, read_noise=4.4)),
+    ('ccd_gal_i4_gain0', 'ccd', 'gal', 'i4', 99, dict(sky_level=20.5, gain=0., read_noise=3.)),
 ]
 NOISE_BATCH_SEEDS = [1001, 1002, 1003, 1004]
 # VariableGaussianNoise: (name, image source, dtype, seed); the variance image is

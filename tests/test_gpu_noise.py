@@ -4,7 +4,7 @@ fixtures made by the reference and against the oracle.
 The integer Poisson draws and the stream positions must agree exactly; the Gaussian deviates
 go through CUDA's FP64 log / cos / sin, which may differ from the host's in the last bit, so
 float64 results are held to 1e-13 relative and float32 results to one unit in the last place
-(in practice they are bit-identical)."""
+(in practice they are bit-identical); integer images must hold the same integers."""
 import numpy as np
 import pytest
 
@@ -29,7 +29,10 @@ def product_noise(kind, seed, p):
 
 def assert_close(got, ref):
     assert got.dtype == ref.dtype
-    if ref.dtype == np.float32:
+    if np.issubdtype(ref.dtype, np.integer):
+        # integer images: the same integers (casts truncate, the sky's integer part is exact)
+        assert np.array_equal(got, ref), np.abs(got.astype(np.int64) - ref).max()
+    elif ref.dtype == np.float32:
         ulp = np.spacing(np.abs(ref).astype(np.float32))
         assert np.all(np.abs(got.astype(np.float64) - ref) <= ulp), np.abs(got - ref).max()
     else:
