@@ -113,6 +113,58 @@ __device__ inline double table_uval(const double* tab, double u)
     return aa * a.y + bb * b.y + ((aa * aa * aa - aa) * a.z + (bb * bb * bb - bb) * b.z) * (h * h) / 6.;
 }
 
+// The Lanczos kernel as the k interpolant (Lanczos::xCalc, src/Interpolant.cpp:563-716):
+// n sin(pi x) sin(pi x / n) / (pi x)^2 for |x| < n (sin(pi x) from sin(pi x / n) by the
+// multiple-angle identities for n = 2, 3; the two-term series below |x| = 1e-4), divided, with
+// conserve_dc, by the DC-correcting factor 1 - sum_j 2 K_j (1 - cos(2 pi j x)), j = 1..5,
+// written as the reference writes it in powers of s^2 = sin^2(pi x).  kt = {n, conserve_dc,
+// K_1 .. K_5, 0}, K_j the kernel's transform at u = j.
+template <typename T>
+__device__ __forceinline__ T lanczos_xval(const double* kt, T x)
+{
+    x = fabs(x);
+    const int n = int(kt[0]);
+    const T nd = T(n);
+    if (x >= nd) return T(0);
+    constexpr T kPiT = T(3.141592653589793238462643383279502884);
+    T res, s;
+    if (x > T(1.e-4)) {
+        if (n == 1) {
+            s = sinpi(x);
+            const T t = s / (kPiT * x);
+            res = t * t;
+        } else if (n == 2) {
+            T sn, cn;
+            sincospi(x / T(2), &sn, &cn);
+            s = T(2) * sn * cn;
+            res = (T(2) / (kPiT * kPiT)) * s * sn / (x * x);
+        } else if (n == 3) {
+            const T sn = sinpi(x / T(3));
+            s = sn * (T(3) - T(4) * sn * sn);
+            res = (T(3) / (kPiT * kPiT)) * s * sn / (x * x);
+        } else {
+            s = sinpi(x);
+            const T sn = sinpi(x / nd);
+            res = (nd / (kPiT * kPiT)) * s * sn / (x * x);
+        }
+    } else {
+        const T pix = kPiT * x;
+        const T t = (T(1) / T(6)) * pix * pix;
+        s = pix * (T(1) - t);
+        res = T(1) - t * (T(1) + T(1) / (nd * nd));
+    }
+    if (kt[1] != 0.) {
+        const T q = s * s;
+        const T K1 = T(kt[2]), K2 = T(kt[3]), K3 = T(kt[4]), K4 = T(kt[5]), K5 = T(kt[6]);
+        const T f = T(1) - T(4) * K1 * q - T(16) * K2 * q * (T(1) - q) -
+                    T(4) * K3 * q * (T(9) - q * (T(24) - T(16) * q)) -
+                    T(64) * K4 * q * (T(1) - q * (T(5) - q * (T(8) - T(4) * q))) -
+                    T(4) * K5 * q * (T(25) - q * (T(200) - q * (T(560) - q * (T(640) - T(256) * q))));
+        res /= f;
+    }
+    return res;
+}
+
 // K(p, q) of the half-plane k-image (stored p-major: K[p N + q], p = 0..N/2) for p, q already
 // reduced to 0..N-1.
 template <typename T>
@@ -149,7 +201,9 @@ __device__ __noinline__ void ii_axis_taps(const LeafParams& L, double kp, bool s
     e.p0 = 0;
     if (fabs(kp) > L.d[1]) return;
     const int N = int(L.d[4]);
-    const int kc = int(L.d[3]), xc = int(L.d[2]);
+    const int codes = int(L.d[2]);
+    const int xc = codes & 15, kc = codes >> 4;
+    const double* kt = reinterpret_cast<const double*>(__double_as_longlong(L.d[3]));
     const double s = kp * L.d[0];
     constexpr double kSmall = 10. * 2.220446049250313e-16;
     const double fl = floor(s + 0.01);
@@ -157,7 +211,7 @@ __device__ __noinline__ void ii_axis_taps(const LeafParams& L, double kp, bool s
     if (shortcut && fabs(s - fl) < kSmall * (fabs(s) + 1.)) {
         p1 = p2 = int(fl);
     } else {
-        const double xr = interp_xrange(kc);
+        const double xr = kc == GSB_INTERP_LANCZOS ? kt[0] : interp_xrange(kc);
         p1 = int(ceil(s - xr));
         p2 = int(floor(s + xr));
     }
@@ -171,7 +225,10 @@ __device__ __noinline__ void ii_axis_taps(const LeafParams& L, double kp, bool s
     // p - s = (p - p1) + (p1 - s): an integer plus a fraction, exact before the rounding to T
     const T off = T(double(p1) - s);
 #pragma unroll
-    for (int t = 0; t < kInterpMaxTaps; ++t) e.w[t] = t < n ? T(u * double(interp_xval<T>(kc, T(t) + off))) : T(0);
+    for (int t = 0; t < kInterpMaxTaps; ++t)
+        e.w[t] = t < n ? T(u * double(kc == GSB_INTERP_LANCZOS ? lanczos_xval<T>(kt, T(t) + off)
+                                                              : interp_xval<T>(kc, T(t) + off)))
+                       : T(0);
     int pw = p1 % N;
     e.p0 = pw < 0 ? pw + N : pw;
     e.n = n;
@@ -207,8 +264,9 @@ __device__ __noinline__ Cx<T> ii_sum(const LeafParams& L, const IITaps<T>& ex, c
 
 // InterpolatedImage leaf at k index (i, j) of a grid with spacing dk.
 // d[0] = (N/2) / pi (k to sample index), d[1] = maxk1 (x interpolant cut-off), d[2] / d[3] =
-// x / k interpolant codes, d[4] = N, d[5] = the x interpolant's table address (Lanczos),
-// d[6] / d[7] = FP64 / FP32 k-image addresses.
+// x interpolant code + 16 k interpolant code, d[3] = the k interpolant's coefficient block
+// address (Lanczos), d[4] = N, d[5] = the x interpolant's table address (Lanczos), d[6] / d[7] =
+// FP64 / FP32 k-image addresses.
 template <typename T>
 __device__ __noinline__ Cx<T> ii_kvalue(const LeafParams& L, double dk, int i, int j)
 {

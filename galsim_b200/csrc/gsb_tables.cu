@@ -1158,17 +1158,24 @@ __global__ void prepare_leaves_kernel(const __grid_constant__ gsb_template tpl, 
         const int xc = int(L.p[0]), kc = int(L.p[1]);
         if (slot < 0 || slot >= images.count) { atomicOr(status_out, 16); break; }
         if (xc < GSB_INTERP_DELTA || xc > GSB_INTERP_LANCZOS || kc < GSB_INTERP_NEAREST ||
-            kc > GSB_INTERP_QUINTIC) { atomicOr(status_out, 32); break; }
+            kc > GSB_INTERP_LANCZOS) { atomicOr(status_out, 32); break; }
+        // a Lanczos k interpolant: p[2] holds its coefficient block {n, conserve_dc, K_1..5};
+        // n <= 3 (at most 7 taps per axis)
+        const double* kt = reinterpret_cast<const double*>(__double_as_longlong(L.p[2]));
+        if (kc == GSB_INTERP_LANCZOS && (kt == nullptr || kt[0] < 1. || kt[0] > 3.)) {
+            atomicOr(status_out, 512);
+            break;
+        }
         const ImageSlot& I = images.slots[slot];
-        if (xc != I.desc.x_interp) { atomicOr(status_out, 32); break; }
+        if (xc != I.desc.x_interp) { atomicOr(status_out, 1024); break; }
         const int N = I.desc.N;
         L.d[0] = (N / 2) / kPi;
         // a Lanczos x interpolant's urange is its table's uMax (Lanczos::urange)
         L.d[1] = (xc == GSB_INTERP_LANCZOS ? I.desc.x_table[3] : interp_urange(xc, gsp.kvalue_accuracy)) /
                  (1. / (2. * kPi));
         L.d[5] = __longlong_as_double((long long)I.desc.x_table);
-        L.d[2] = xc;
-        L.d[3] = kc;
+        L.d[2] = xc + 16 * kc;
+        L.d[3] = __longlong_as_double(kc == GSB_INTERP_LANCZOS ? (long long)kt : 0LL);
         L.d[4] = N;
         L.d[6] = __longlong_as_double((long long)(images.k64 + I.k_offset));
         L.d[7] = __longlong_as_double((long long)(images.k32 + I.k_offset));
@@ -1616,7 +1623,12 @@ int prepare_leaves(const gsb_template* tpl, int n_stamps, const gsb_gsparams* gs
     if (h_status & 8) return set_error(GSB_ERR_INVALID, "unknown leaf type");
     if (h_status & 16) return set_error(GSB_ERR_INVALID, "InterpolatedImage leaf names no built image slot");
     if (h_status & 32) return set_error(GSB_ERR_UNSUPPORTED, "interpolant not built (x: Delta, Nearest, "
-                                                             "Linear, Cubic, Quintic; k: the same but Delta)");
+                                                             "Linear, Cubic, Quintic, Lanczos; k: the same "
+                                                             "but Delta)");
+    if (h_status & 512) return set_error(GSB_ERR_INVALID, "a Lanczos k interpolant needs its coefficient "
+                                                          "block in p[2] (n <= 3)");
+    if (h_status & 1024) return set_error(GSB_ERR_INVALID, "InterpolatedImage leaf's x interpolant differs "
+                                                           "from its image slot's");
     if (h_status & 2) return set_error(GSB_ERR_NUMERIC, "Sersic radius root finding failed");
     if (h_status & 4) return set_error(GSB_ERR_NUMERIC, "Moffat maxk root finding failed");
     if (h_status & 64) return set_error(GSB_ERR_INVALID, "truncated Moffat leaf names no built Moffat table slot");

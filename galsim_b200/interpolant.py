@@ -3,10 +3,11 @@
 The classes carry what InterpolatedImage needs on the host: the kernel's support (xrange,
 ixrange), its Fourier extent (urange, krange), GSParams handling, equality and names.  Their
 kernels run on the GPU (galsim_b200/csrc/gsb_interp.cuh): Delta (as x interpolant only),
-Nearest, Linear, Cubic and Quintic, and Lanczos as the x interpolant (its transform tabulated
-on the host exactly as the reference tabulates it, then read from a device table).  Lanczos as
-the k interpolant and SincInterpolant can be constructed, but an InterpolatedImage using them
-raises GalSimNotImplementedError when it is sized or drawn.
+Nearest, Linear, Cubic and Quintic, Lanczos as the x interpolant (its transform tabulated
+on the host exactly as the reference tabulates it, then read from a device table) and as the
+k interpolant for n <= 3.  SincInterpolant and larger Lanczos k interpolants can be
+constructed, but an InterpolatedImage using them raises GalSimNotImplementedError when it is
+sized or drawn.
 """
 import math
 
@@ -217,6 +218,7 @@ class _LanczosTable(object):
         from .table import _LookupTable
         self.umax = umax
         self.table = _LookupTable(np.array(us), np.array(vals), 'spline')
+        self.conserve_dc = conserve_dc
 
     @classmethod
     def get(cls, n, conserve_dc, gsparams):
@@ -232,6 +234,19 @@ class _LanczosTable(object):
         u = np.abs(np.asarray(u, dtype=float))
         v = self.table(np.minimum(u, self.table.x_max))
         return np.where(u > self.umax, 0., v)
+
+    def kdevice(self):
+        """The kernel's coefficients for its use as the k interpolant (Lanczos::xCalc): one FP64
+        device buffer {n, conserve_dc, K_1 .. K_5, 0}."""
+        import torch
+        dev = _lib.Device.torch_device()
+        key = ('kdev', dev.index)
+        t = self.__dict__.get(key)
+        if t is None:
+            a = np.array([self.n, 1. if self.conserve_dc else 0.] + list(self.K[1:6]) + [0.])
+            t = torch.from_numpy(a).to(dev)
+            self.__dict__[key] = t
+        return t
 
     def device(self):
         """The table as one FP64 device buffer of 4 (n + 1) doubles: a header (node count,
@@ -257,7 +272,8 @@ class Lanczos(Interpolant):
     """Lanczos filter sinc(x) sinc(x / n) with the DC-conserving correction
     (interpolant.py:604-670, src/Interpolant.cpp:560-930).  On the GPU it serves as an
     InterpolatedImage's x interpolant (its transform from the reference's spline table,
-    _LanczosTable); as the k interpolant it is not built."""
+    _LanczosTable) and, for n <= 3 (at most 7 taps per axis), as its k interpolant (the kernel
+    itself, with the DC correction's coefficients K_1..K_5 from the same table object)."""
     _code = _lib.INTERP_LANCZOS
 
     def __init__(self, n, conserve_dc=True, tol=None, gsparams=None):

@@ -18,7 +18,7 @@ Noise padding with Gaussian noise of a given variance (noise_pad a number) fills
 the frame with the reference's stream (BaseDeviate(rng), drawn on the GPU) before the pad image
 and the image are placed.  Not built: padding with correlated noise (a CorrelatedNoise, an
 image or a file), depixelize, FITS file names, non-PixelScale WCS, the sinc interpolant and
-Lanczos as the k interpolant (Lanczos as the x interpolant is built).
+Lanczos(n > 3) as the k interpolant.
 """
 import math
 
@@ -85,13 +85,17 @@ class _ImageLeaf(GSObject):
 
     def _flatten(self, bld, jac):
         xi, ki = self._x_interpolant, self._k_interpolant
-        if xi._code is None or ki._code is None or isinstance(ki, (Delta, Lanczos)):
+        if (xi._code is None or ki._code is None or isinstance(ki, Delta) or
+                (isinstance(ki, Lanczos) and ki.n > 3)):
             raise GalSimNotImplementedError(
                 "InterpolatedImage with x interpolant %s and k interpolant %s is not built on the "
                 "GPU (x: Delta, Nearest, Linear, Cubic, Quintic, Lanczos; k: Nearest, Linear, "
-                "Cubic, Quintic)" % (xi, ki))
+                "Cubic, Quintic, Lanczos(n <= 3))" % (xi, ki))
         bld.add_leaf(_lib.INTERPOLATED, jac, 1., (float(xi._code), float(ki._code), 0.))
         bld.image_sources[len(bld.leaves) - 1] = self._sources
+        # a Lanczos k interpolant's coefficient block goes into p[2] when the records are
+        # uploaded (Program.upload), where the device exists
+        bld.image_kinterp[len(bld.leaves) - 1] = ki if isinstance(ki, Lanczos) else None
 
     def withGSParams(self, gsparams=None, **kwargs):
         return self

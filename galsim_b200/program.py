@@ -48,6 +48,7 @@ class Builder(object):
         self.phases = []
         self.scales = []
         self.image_sources = {}   # InterpolatedImage leaf -> its _ImageSource list (1 or B)
+        self.image_kinterp = {}   # InterpolatedImage leaf -> its Lanczos k interpolant (or None)
 
     def _bcast(self, v):
         a = np.asarray(v, dtype=np.float64)
@@ -202,6 +203,11 @@ class Program(object):
                         self.image_order.append(src)
                     slots.append(slot_of[id(src)])
                 leaves['table'][:, l] = np.broadcast_to(np.array(slots, dtype=np.int32), (B,))
+                ki = self.bld.image_kinterp.get(l)
+                if ki is not None:
+                    # the coefficient block's device address, as the bits of p[2]
+                    addr = np.array([ki._table.kdevice().data_ptr()], dtype=np.uint64).view(np.float64)[0]
+                    leaves['p'][:, l, 2] = addr
         self.d_leaves = _lib.to_device(leaves)
         self.d_info = torch.empty(B * L * 2, dtype=torch.float64, device=_lib.Device.torch_device())
         if self.sersic_n is None and not self.image_order and self.moffat_beta is None:

@@ -47,8 +47,9 @@ enum {
     GSB_KOLMOGOROV  = 4,   /* p = {lam_over_r0}                            */
     GSB_AIRY        = 5,   /* p = {lam_over_diam, obscuration}             */
     GSB_BOX         = 6,   /* p = {width, height}                          */
-    GSB_INTERPOLATED = 7   /* p = {x interpolant, k interpolant, 0}; `table` names an image
-                              slot built by gsb_images_build (SBInterpolatedImage.cpp) */
+    GSB_INTERPOLATED = 7   /* p = {x interpolant, k interpolant, the bits of a Lanczos k
+                              interpolant's device coefficient block or 0}; `table` names an
+                              image slot built by gsb_images_build (SBInterpolatedImage.cpp) */
 };
 
 /* Interpolant codes of GSB_INTERPOLATED leaves (galsim/interpolant.py, src/Interpolant.cpp). */
@@ -58,8 +59,10 @@ enum {
     GSB_INTERP_LINEAR  = 2,
     GSB_INTERP_CUBIC   = 3,
     GSB_INTERP_QUINTIC = 4,
-    GSB_INTERP_LANCZOS = 5    /* x interpolant only: the transform from the image's x_table
-                                 (the reference's spline table of Lanczos::uCalc)          */
+    GSB_INTERP_LANCZOS = 5    /* as x interpolant: the transform from the image's x_table
+                                 (the reference's spline table of Lanczos::uCalc); as k
+                                 interpolant (n <= 3): the kernel Lanczos::xCalc, with the
+                                 leaf's p[2] the address of {n, conserve_dc, K_1..K_5, 0}  */
 };
 
 /* Program opcodes.  A program is evaluated per k-point on a small stack of complex values:

@@ -1037,8 +1037,34 @@ def apply_phases(kimage, xmin, ymin, dk, jac, cx, cy, fs):
 # InterpolatedImage (interpolatedimage.py:303-685, src/SBInterpolatedImage.cpp,
 # src/Interpolant.cpp)
 # ---------------------------------------------------------------------------------------------
+def lanczos_xval(n, conserve_dc, x):
+    """Lanczos::xCalc (Interpolant.cpp:563-716): n sin(pi x) sin(pi x / n) / (pi x)^2 on |x| < n
+    (series below 1e-4), divided with conserve_dc by 1 - sum_j 2 K_j (1 - cos(2 pi j x)),
+    K_j the kernel's transform at u = j (uCalcRaw)."""
+    x = np.abs(np.asarray(x, dtype=float))
+    nd = float(n)
+    with np.errstate(invalid='ignore', divide='ignore'):
+        s = np.sin(PI * x)
+        res = nd * s * np.sin(PI * x / nd) / (PI * x) ** 2
+    pix = PI * x
+    t = pix * pix / 6.
+    small = x <= 1.e-4
+    s = np.where(small, pix * (1. - t), s)
+    res = np.where(small, 1. - t * (1. + 1. / (nd * nd)), res)
+    if conserve_dc:
+        K = lanczos_k(n)
+        c = 1.
+        for j in range(1, 6):
+            c = c - 2. * K[j] * (1. - np.cos(2. * PI * j * x))
+        res = res / c
+    return np.where(x >= nd, 0., res)
+
+
 def interp_xval(name, x):
-    """Real-space kernels: Nearest / Linear / Cubic / Quintic (Interpolant.cpp:171-432)."""
+    """Real-space kernels: Nearest / Linear / Cubic / Quintic (Interpolant.cpp:171-432), Lanczos."""
+    lz = _lanczos_name(name)
+    if lz is not None:
+        return lanczos_xval(lz[0], lz[1], x)
     x = np.abs(np.asarray(x, dtype=float))
     if name == 'nearest':
         return np.where(x > 0.5, 0., 1.)
@@ -1127,6 +1153,18 @@ def lanczos_table(n, conserve_dc=True, gsp=DEFAULT):
     y2[1:-1] = solve_banded((1, 1), ab, rhs)
     _LANCZOS[key] = (x, f, y2, umax)
     return _LANCZOS[key]
+
+
+def lanczos_k(n):
+    """K_j = F(j), j = 1..5, of the uncorrected Lanczos transform (Lanczos::Lanczos)."""
+    nd = float(n)
+    si = lambda x: special.sici(x)[0]
+
+    def raw(u):
+        vp, vm = nd * (2. * u + 1.), nd * (2. * u - 1.)
+        return ((vm - 1.) * si(PI * (vm - 1.)) - (vm + 1.) * si(PI * (vm + 1.)) -
+                (vp - 1.) * si(PI * (vp - 1.)) + (vp + 1.) * si(PI * (vp + 1.))) / (2. * PI)
+    return [0.] + [float(raw(float(j))) for j in range(1, 6)]
 
 
 def lanczos_uval(n, conserve_dc, u, gsp=DEFAULT):

@@ -154,6 +154,11 @@ INTERP_DRAW_CASES = [
     ('ii_lanczos7_x_f4', ('conv', [('sersic', 2.5, 0.5, 1e3), ('ii', 'psf31x33', 0.2,
                                                                {'x_interpolant': 'lanczos7'})]),
      48, 48, 0.2, 'f4', (0., 0.)),
+    # Lanczos k interpolants (n <= 3), with and without the DC correction
+    ('ii_lanczos3_k', ('conv', [('exp', 0.4, 1.), ('ii', 'psf32', 0.2, {'k_interpolant': 'lanczos3'})]),
+     48, 48, 0.2, 'f8', (0., 0.)),
+    ('ii_lanczos2F_k_f4', ('ii', 'gal24', 0.25, {'x_interpolant': 'lanczos5', 'k_interpolant': 'lanczos2F'}),
+     40, 40, 0.25, 'f4', (0.1, 0.2)),
     ('ii_calc_floats', ('conv', [('exp', 0.3, 1.), ('ii', 'psf32', 0.2, {'calculate_maxk': 3.0,
                                                                          'calculate_stepk': 0.5})]),
      48, 48, 0.2, 'f8', (0., 0.)),
@@ -164,6 +169,8 @@ INTERP_DRAW_CASES = [
 INTERP_KIMAGE_CASES = [
     ('k_ii', ('ii', 'psf31x33', 0.25, {}), 0.3, 21),
     ('k_ii_shear', ('shear', 0.15, -0.1, ('ii', 'psf32', 0.2, {'x_interpolant': 'cubic'})), 0.35, 21),
+    ('k_ii_lanczos', ('shear', 0.1, 0.05, ('ii', 'psf31x33', 0.2, {'x_interpolant': 'lanczos5',
+                                                                  'k_interpolant': 'lanczos3'})), 0.3, 21),
 ]
 
 INTERP_SIZE_CASES = [c[1] for c in INTERP_DRAW_CASES if c[1][0] == 'ii'] + [

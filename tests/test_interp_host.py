@@ -114,12 +114,14 @@ def test_program_layout():
     gal = galsim.Exponential(half_light_radius=np.array([0.4, 0.6]))
     p2 = Program(galsim.Convolve(gal, iib))
     assert p2.B == 2 and len(p2.bld.image_sources[1]) == 2
-    # a Lanczos x interpolant is built (its transform from a device table); as the k
-    # interpolant it is not
-    p3 = Program(galsim.InterpolatedImage(_img(), x_interpolant='lanczos3'))
+    # a Lanczos x interpolant is built (its transform from a device table), and a Lanczos k
+    # interpolant up to n = 3 (7 taps per axis)
+    p3 = Program(galsim.InterpolatedImage(_img(), x_interpolant='lanczos5', k_interpolant='lanczos3'))
     assert p3.bld.leaves[0]['p'][0, 0] == _lib.INTERP_LANCZOS
+    assert p3.bld.leaves[0]['p'][0, 1] == _lib.INTERP_LANCZOS
+    assert p3.bld.image_kinterp[0].n == 3
     with pytest.raises(galsim.GalSimNotImplementedError):
-        Program(galsim.InterpolatedImage(_img(), k_interpolant='lanczos3'))
+        Program(galsim.InterpolatedImage(_img(), k_interpolant='lanczos4'))
     with pytest.raises(galsim.GalSimNotImplementedError):
         Program(galsim.InterpolatedImage(_img(), k_interpolant='delta'))
 
