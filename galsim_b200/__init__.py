@@ -26,7 +26,8 @@ from .box import Box, Pixel
 from .interpolant import (Interpolant, Delta, Nearest, SincInterpolant, Linear, Cubic, Quintic,
                           Lanczos, convert_interpolant)
 from .interpolatedimage import InterpolatedImage
-from .noise import BaseDeviate, BaseNoise, GaussianNoise, PoissonNoise, CCDNoise, VariableGaussianNoise
+from .noise import BaseDeviate, BaseNoise, GaussianNoise, PoissonNoise, CCDNoise, VariableGaussianNoise, DeviateNoise
+from .random import UniformDeviate, GaussianDeviate, PoissonDeviate
 from . import fits
 from .fits import FitsHeader
 from .compound import Convolve, Convolution, Add, Sum, Transform, Transformation, _Transform

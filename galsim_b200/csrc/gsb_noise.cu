@@ -190,6 +190,27 @@ __device__ void gaussian_run(WarpStream& st, long long n, double sigma, Op op)
     __syncwarp();
 }
 
+// Uniform deviates u_j = word_j 2^-32 (boost uniform_01 on the 32-bit engine: one word each)
+// for j = 0..n-1 from the stream's position; op(j, u) consumes them.
+template <typename Op>
+__device__ void uniform_run(WarpStream& st, long long n, Op op)
+{
+    long long m0 = 0;
+    while (m0 < n) {
+        if (st.i == kMtN) {
+            mt_twist(st.x, st.lane);
+            st.i = 0;
+        }
+        const long long take = min((long long)(kMtN - st.i), n - m0);
+        for (long long k = st.lane; k < take; k += 32)
+            op(m0 + k, double(mt_temper(st.x[st.i + int(k)])) * (1. / 4294967296.));
+        m0 += take;
+        st.i += int(take);
+        st.used += take;
+        __syncwarp();
+    }
+}
+
 // log k! for k < 10 (the table PTRD uses below the Stirling branch).
 __device__ __forceinline__ double log_factorial_small(int k)
 {
@@ -358,7 +379,9 @@ __global__ void __launch_bounds__(kNoiseWarps * 32) gauss_kernel(const __grid_co
     mt_seed(st.x, sp.seed, lane);
     st.skip(sp.skip);
     T* img = pix_ptr<T>(a.image, sp.offset);
-    if (a.kind == GSB_NOISE_VARIABLE_GAUSSIAN) {
+    if (a.kind == GSB_NOISE_UNIFORM) {
+        uniform_run(st, sp.npix, [&](long long j, double u) { img[j] = add_pixel<T>(img[j], u); });
+    } else if (a.kind == GSB_NOISE_VARIABLE_GAUSSIAN) {
         // unit deviates scaled by each pixel's own sigma (GaussianDeviate::generateFromVariance)
         const double* var = a.scratch + sp.offset;
         gaussian_run(st, sp.npix, 1., [&](long long j, double d) { img[j] = add_pixel<T>(img[j], d * sqrt(var[j])); });
@@ -675,7 +698,7 @@ template <typename T>
 int launch_noise(const NoiseArgs& a, int max_npix, cudaStream_t stream)
 {
     const int warp_grid = (a.n_stamps + kNoiseWarps - 1) / kNoiseWarps;
-    if (a.kind == GSB_NOISE_GAUSSIAN || a.kind == GSB_NOISE_VARIABLE_GAUSSIAN) {
+    if (a.kind == GSB_NOISE_GAUSSIAN || a.kind == GSB_NOISE_VARIABLE_GAUSSIAN || a.kind == GSB_NOISE_UNIFORM) {
         gauss_kernel<T><<<warp_grid, kNoiseWarps * 32, 0, stream>>>(a);
         GSB_CUDA_CHECK(cudaGetLastError());
         return GSB_OK;
@@ -727,7 +750,7 @@ extern "C" int gsb_add_noise(int kind, const gsb_noise_params* p, const gsb_nois
 {
     if (!p || n_stamps < 0 || (n_stamps > 0 && (!d_stamps || !d_image)))
         return set_error(GSB_ERR_INVALID, "null argument");
-    if (kind < GSB_NOISE_GAUSSIAN || kind > GSB_NOISE_VARIABLE_GAUSSIAN)
+    if (kind < GSB_NOISE_GAUSSIAN || kind > GSB_NOISE_UNIFORM)
         return set_error(GSB_ERR_INVALID, "unknown noise kind");
     if (kind == GSB_NOISE_VARIABLE_GAUSSIAN && n_stamps > 0 && !d_scratch)
         return set_error(GSB_ERR_INVALID, "variable Gaussian noise needs the variance of every pixel in d_scratch");

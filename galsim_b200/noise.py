@@ -94,7 +94,7 @@ NOISE_STAMP_DTYPE = np.dtype({'names': ['offset', 'npix', 'pad', 'seed', 'skip']
                               'formats': ['i8', 'i4', 'i4', 'i8', 'i8'],
                               'offsets': [0, 8, 12, 16, 24], 'itemsize': 32})
 
-GAUSSIAN, POISSON, CCD, VARIABLE_GAUSSIAN = 0, 1, 2, 3
+GAUSSIAN, POISSON, CCD, VARIABLE_GAUSSIAN, UNIFORM = 0, 1, 2, 3, 4
 
 
 def _sky_split(sky_level, dtype):
@@ -417,4 +417,42 @@ class VariableGaussianNoise(BaseNoise):
         return 'galsim.VariableGaussianNoise(rng=%r, var_image%r)' % (self.rng, self.var_image)
 
 
-__all__ = ['BaseDeviate', 'BaseNoise', 'GaussianNoise', 'PoissonNoise', 'CCDNoise', 'VariableGaussianNoise']
+class DeviateNoise(BaseNoise):
+    """Noise drawn from a deviate (noise.py:532-588): dev.generate fills one value per pixel in
+    row-major order (on the GPU, galsim_b200.random), added to the image in its type."""
+
+    def __init__(self, dev):
+        BaseNoise.__init__(self, dev)
+
+    def _applyTo(self, image):
+        arr = image.array
+        noise = np.empty(arr.size, dtype=float)
+        self._rng.generate(noise)
+        arr[...] += noise.reshape(arr.shape).astype(arr.dtype)
+
+    def _apply_batch(self, sb, seeds, skips=None):
+        raise GalSimNotImplementedError("DeviateNoise on a stamp batch is not built")
+
+    def _getVariance(self):
+        raise GalSimError("No single variance value for DeviateNoise")
+
+    def _withVariance(self, variance):
+        raise GalSimError("Changing the variance is not allowed for DeviateNoise")
+
+    def _withScaledVariance(self, variance):
+        raise GalSimError("Changing the variance is not allowed for DeviateNoise")
+
+    def copy(self, rng=None):
+        if rng is None:
+            dev = self.rng
+        else:
+            dev = self.rng.duplicate()
+            dev.reset(rng)
+        return DeviateNoise(dev)
+
+    def __repr__(self):
+        return 'galsim.DeviateNoise(dev=%r)' % self.rng
+
+
+__all__ = ['BaseDeviate', 'BaseNoise', 'GaussianNoise', 'PoissonNoise', 'CCDNoise', 'VariableGaussianNoise',
+           'DeviateNoise']

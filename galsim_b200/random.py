@@ -1,0 +1,230 @@
+"""Random deviates: UniformDeviate, GaussianDeviate, PoissonDeviate (galsim/random.py:309-531,
+src/Random.cpp).
+
+Each deviate is a BaseDeviate stream (seed + raw 32-bit draws taken) with the distribution of
+the reference on top, and the deviates themselves are drawn on the GPU by the noise kernels
+(galsim_b200/csrc/gsb_noise.cu, `gsb_add_noise` applied to a zero FP64 buffer): uniform_01 as
+one word / 2^32, the Box-Muller pairs of boost 1.48's normal_distribution, and its
+poisson_distribution (inversion below mean 10, PTRD above).  What the reference keeps inside a
+deviate object between calls is kept here on the host: a GaussianDeviate's second Box-Muller
+value (the pair cache, used by the next call, cleared by generate and clearCache), and a
+PoissonDeviate's normal branch (means above 2^30 or 0) with its own pair cache.  Single draws
+are one small launch each; generate() fills an array in one launch.
+"""
+import numpy as np
+
+from . import _lib
+from .errors import GalSimRangeError, GalSimValueError
+from .noise import BaseDeviate, NoiseParamsC, _apply, GAUSSIAN, POISSON, UNIFORM
+
+__all__ = ['UniformDeviate', 'GaussianDeviate', 'PoissonDeviate']
+
+_MAX_POISSON = float(1 << 30)
+
+
+def _draw(stream, kind, n, params=None, values=None):
+    """n deviates of `kind` from `stream` (advanced past them) as a host FP64 array: the noise
+    kernel applied to a zero buffer (or to `values`, the per-element expectations of Poisson
+    draws)."""
+    import torch
+    if n == 0:
+        return np.zeros(0)
+    dev = _lib.Device.torch_device()
+    if values is None:
+        flat = torch.zeros(n, dtype=torch.float64, device=dev)
+    else:
+        flat = torch.from_numpy(np.ascontiguousarray(values, dtype=np.float64).reshape(-1)).to(dev)
+    used = _apply(kind, params if params is not None else NoiseParamsC(), flat, [0], [n],
+                  [stream.seed], [stream.used])
+    stream.used = int(used[0])
+    return flat.cpu().numpy()
+
+
+def _fill(array, vals, add=False):
+    """Write (or add) vals into a numpy array of any shape, as the reference's generate /
+    add_generate do (through an FP64 copy, cast back with casting='unsafe')."""
+    vals = np.asarray(vals).reshape(array.shape)
+    if add:
+        vals = np.asarray(array, dtype=float) + vals
+    np.copyto(array, vals, casting='unsafe')
+
+
+class UniformDeviate(BaseDeviate):
+    """Uniform deviates in [0, 1) (random.py:309-343): one raw word each, divided by 2^32."""
+
+    def __init__(self, seed=None):
+        BaseDeviate.__init__(self, seed)
+
+    def __call__(self):
+        return float(_draw(self._stream, UNIFORM, 1)[0])
+
+    def raw(self):
+        """The next raw 32-bit word of the stream."""
+        return int(_draw(self._stream, UNIFORM, 1)[0] * 4294967296.)
+
+    def clearCache(self):
+        pass
+
+    def generate(self, array):
+        _fill(array, _draw(self._stream, UNIFORM, int(np.size(array))))
+
+    def add_generate(self, array):
+        _fill(array, _draw(self._stream, UNIFORM, int(np.size(array))), add=True)
+
+    def duplicate(self):
+        ret = UniformDeviate.__new__(UniformDeviate)
+        ret._stream = BaseDeviate.duplicate(self)._stream
+        return ret
+
+    def __repr__(self):
+        return 'galsim.UniformDeviate(seed=%r)' % self._stream.seed
+
+
+class GaussianDeviate(BaseDeviate):
+    """Gaussian deviates of a mean and sigma (random.py:345-413): Box-Muller pairs, the cosine
+    value first; the sine value of the last pair is kept for the next call (boost 1.48
+    normal_distribution), and each value is (unit deviate * sigma) + mean."""
+
+    def __init__(self, seed=None, mean=0., sigma=1.):
+        if sigma < 0.:
+            raise GalSimRangeError("GaussianDeviate sigma must be > 0.", sigma, 0.)
+        BaseDeviate.__init__(self, seed)
+        self._mean = float(mean)
+        self._sigma = float(sigma)
+        self._cache = None
+
+    mean = property(lambda self: self._mean)
+    sigma = property(lambda self: self._sigma)
+    generates_in_pairs = property(lambda self: True)
+
+    def clearCache(self):
+        self._cache = None
+
+    def reset(self, seed=None):
+        BaseDeviate.reset(self, seed)
+        self._cache = None
+
+    def _units(self, n):
+        """n unit deviates continuing the pair sequence (the cache first); an odd tail leaves
+        its pair's second value in the cache."""
+        out = []
+        if n and self._cache is not None:
+            out.append(self._cache)
+            self._cache = None
+            n -= 1
+        if n:
+            m = n + (n & 1)
+            p = NoiseParamsC()
+            p.sigma = 1.
+            z = _draw(self._stream, GAUSSIAN, m, p)
+            out.extend(z[:n])
+            if m > n:
+                self._cache = float(z[n])
+        return np.array(out, dtype=float)
+
+    def __call__(self):
+        return float(self._units(1)[0] * self._sigma + self._mean)
+
+    def generate(self, array):
+        self._cache = None
+        _fill(array, self._units(int(np.size(array))) * self._sigma + self._mean)
+
+    def add_generate(self, array):
+        self._cache = None
+        _fill(array, self._units(int(np.size(array))) * self._sigma + self._mean, add=True)
+
+    def generate_from_variance(self, array):
+        """Unit deviates times sqrt(array) (GaussianDeviate::generateFromVariance,
+        Random.cpp:402-450); the pair cache is cleared before and after."""
+        self._cache = None
+        var = np.asarray(array, dtype=float).reshape(-1)
+        z = self._units(var.size)
+        self._cache = None
+        _fill(array, z * np.sqrt(var))
+
+    def duplicate(self):
+        ret = GaussianDeviate.__new__(GaussianDeviate)
+        ret._stream = BaseDeviate.duplicate(self)._stream
+        ret._mean, ret._sigma, ret._cache = self._mean, self._sigma, self._cache
+        return ret
+
+    def __repr__(self):
+        return 'galsim.GaussianDeviate(seed=%r, mean=%r, sigma=%r)' % (
+            self._stream.seed, self._mean, self._sigma)
+
+
+class PoissonDeviate(BaseDeviate):
+    """Poisson deviates of a mean (random.py:468-531, PoissonDeviateImpl in Random.cpp:499-606):
+    boost 1.48's poisson_distribution for 0 < mean <= 2^30; for mean 0 and above 2^30 the
+    normal approximation N(mean, sqrt(mean)) with its own pair cache (kept while the deviate
+    stays on that branch)."""
+
+    def __init__(self, seed=None, mean=1.):
+        if mean < 0:
+            raise GalSimValueError("PoissonDeviate is only defined for mean >= 0.", mean)
+        BaseDeviate.__init__(self, seed)
+        self._mean = float(mean)
+        self._cache = None
+
+    mean = property(lambda self: self._mean)
+    has_reliable_discard = property(lambda self: False)
+
+    def _normal_branch(self):
+        return self._mean > _MAX_POISSON or self._mean == 0.
+
+    def clearCache(self):
+        self._cache = None
+
+    def reset(self, seed=None):
+        BaseDeviate.reset(self, seed)
+        self._cache = None
+
+    def _values(self, n):
+        if not self._normal_branch():
+            p = NoiseParamsC()
+            return _draw(self._stream, POISSON, n, p, values=np.full(n, self._mean))
+        # the normal branch: Gaussian pairs with the deviate's cache
+        out = []
+        if n and self._cache is not None:
+            out.append(self._cache)
+            self._cache = None
+            n -= 1
+        if n:
+            m = n + (n & 1)
+            p = NoiseParamsC()
+            p.sigma = 1.
+            z = _draw(self._stream, GAUSSIAN, m, p)
+            out.extend(z[:n])
+            if m > n:
+                self._cache = float(z[n])
+        return np.array(out, dtype=float) * np.sqrt(self._mean) + self._mean
+
+    def __call__(self):
+        return float(self._values(1)[0])
+
+    def generate(self, array):
+        self._cache = None
+        _fill(array, self._values(int(np.size(array))))
+
+    def add_generate(self, array):
+        self._cache = None
+        _fill(array, self._values(int(np.size(array))), add=True)
+
+    def generate_from_expectation(self, array):
+        """Each element replaced by a draw with that element as the mean (elements equal to 0
+        stay 0 and take no draws; PoissonDeviate::generateFromExpectation, Random.cpp:594-606),
+        in one launch of the Poisson kernel; the normal branch's pair cache starts empty."""
+        a = np.asarray(array, dtype=float)
+        if np.any(a < 0):
+            raise GalSimValueError("Expectation array may not have values < 0.", array)
+        self._cache = None
+        _fill(array, _draw(self._stream, POISSON, int(a.size), NoiseParamsC(), values=a.reshape(-1)))
+
+    def duplicate(self):
+        ret = PoissonDeviate.__new__(PoissonDeviate)
+        ret._stream = BaseDeviate.duplicate(self)._stream
+        ret._mean, ret._cache = self._mean, self._cache
+        return ret
+
+    def __repr__(self):
+        return 'galsim.PoissonDeviate(seed=%r, mean=%r)' % (self._stream.seed, self._mean)

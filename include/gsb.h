@@ -321,7 +321,8 @@ int gsb_weighted_stamp_sum(const void* d_flat, int in_dtype, const int64_t* d_of
  * whose third draw seeds the mt19937), positioned `skip` raw 32-bit draws into its stream
  * (0 for a fresh BaseDeviate); the deviates follow Boost.Random 1.48 as the reference vendors it
  * (uniform_01, Box-Muller normal pairs, inversion / PTRD Poisson). */
-enum { GSB_NOISE_GAUSSIAN = 0, GSB_NOISE_POISSON = 1, GSB_NOISE_CCD = 2, GSB_NOISE_VARIABLE_GAUSSIAN = 3 };
+enum { GSB_NOISE_GAUSSIAN = 0, GSB_NOISE_POISSON = 1, GSB_NOISE_CCD = 2, GSB_NOISE_VARIABLE_GAUSSIAN = 3,
+       GSB_NOISE_UNIFORM = 4 };
 
 typedef struct gsb_noise_stamp {
     int64_t offset;    /* first pixel of the stamp in the image buffer (elements) */
@@ -349,7 +350,9 @@ typedef struct gsb_noise_params {
  * stamps' pixel counts.  Poisson and CCD noise need d_scratch (one double per pixel, addressed
  * like d_image) and d_used.  GSB_NOISE_VARIABLE_GAUSSIAN (VariableGaussianNoise, noise.py:590-636,
  * Random.cpp:402-450) reads each pixel's variance from d_scratch (FP64, addressed like d_image,
- * left unchanged) and adds unit deviates times its square root; p->sigma is ignored.  d_used (may be NULL for Gaussian noise) receives, per stamp, the raw
+ * left unchanged) and adds unit deviates times its square root; p->sigma is ignored.
+ * GSB_NOISE_UNIFORM adds uniform deviates in [0, 1), one 32-bit word each (UniformDeviate,
+ * boost uniform_01: word / 2^32), the deviates of the product's UniformDeviate and DeviateNoise.  d_used (may be NULL for Gaussian noise) receives, per stamp, the raw
  * draws consumed since seeding (skip + this call's draws), so a caller can continue the stream.
  * Gaussian: one warp per stamp.  Poisson / CCD: the expectations in parallel, then one warp per
  * stamp walks its sequential stream (speculative draws of 32 pixels at once, committed up to the

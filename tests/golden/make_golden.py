@@ -401,6 +401,59 @@ def variance_image(arr):
     return 0.25 + 0.01 * np.abs(arr.astype(np.float64)) + ramp
 
 
+def deviate_sequences(galsim):
+    """Draws from the reference's deviates (or the product's, with the same API): single calls
+    and generate() interleaved (the Gaussian pair cache across them), generate_from_variance,
+    the Poisson inversion / PTRD / normal (mean 0 and above 2^30) branches,
+    generate_from_expectation, streams shared between deviates, and DeviateNoise on images."""
+    out = {}
+    u = galsim.UniformDeviate(1234)
+    a = [u() for _ in range(5)]
+    g = np.empty(7)
+    u.generate(g)
+    out['uniform'] = np.concatenate([a, g, [u(), u()]])
+    gd = galsim.GaussianDeviate(2345, mean=1.5, sigma=2.5)
+    a = [gd() for _ in range(3)]
+    g = np.empty(5)
+    gd.generate(g)
+    b = [gd(), gd()]
+    v = np.array([0.5, 2., 0., 9.])
+    gd.generate_from_variance(v)
+    out['gaussian'] = np.concatenate([a, g, b, v, [gd()]])
+    pd = galsim.PoissonDeviate(3456, mean=7.3)
+    a = [pd() for _ in range(4)]
+    g = np.empty(6)
+    pd.generate(g)
+    pd2 = galsim.PoissonDeviate(pd, mean=120.)
+    b = [pd2() for _ in range(3)]
+    g2 = np.empty(5)
+    pd2.generate(g2)
+    pz = galsim.PoissonDeviate(pd, mean=0.)
+    c = [pz() for _ in range(3)]
+    ph = galsim.PoissonDeviate(pd, mean=float(2 ** 31))
+    d = [ph() for _ in range(3)]
+    g3 = np.empty(3)
+    ph.generate(g3)
+    d.append(ph())
+    e = np.array([0., 3.2, 50., 0., float(2 ** 31), 7.])
+    pd.generate_from_expectation(e)
+    out['poisson'] = np.concatenate([a, g, b, g2, c, d, g3, e, [pd()]])
+    # one stream shared: a uniform, then Gaussian values, then uniforms again
+    s = galsim.UniformDeviate(4567)
+    sg = galsim.GaussianDeviate(s, sigma=3.)
+    out['shared'] = np.array([s(), sg(), sg(), sg(), s(), s()])
+    for name, dev in (('uniform', galsim.UniformDeviate(5678)),
+                      ('gauss', galsim.GaussianDeviate(6789, mean=-2., sigma=0.5)),
+                      ('poisson', galsim.PoissonDeviate(7890, mean=4.5))):
+        im = galsim.ImageF(7, 5, init_value=10.)
+        im.addNoise(galsim.DeviateNoise(dev))
+        imi = galsim.ImageI(6, 3, init_value=3)
+        imi.addNoise(galsim.DeviateNoise(dev))
+        out['devnoise_' + name] = im.array.copy()
+        out['devnoise_i_' + name] = imi.array.copy()
+    return out
+
+
 def noise_input(galsim, src, dtype):
     if src == 'zero':
         return galsim.Image(17, 13, dtype=dtype, init_value=0.)
@@ -450,6 +503,7 @@ def main_noise(ref_root):
         out['var_' + name] = variance_image(im.array)
         im.addNoise(galsim.VariableGaussianNoise(galsim.BaseDeviate(seed), galsim.ImageD(out['var_' + name])))
         out['out_' + name] = im.array.copy()
+    out.update({'dev_' + k: v for k, v in deviate_sequences(galsim).items()})
     # variable noise on an odd-sized image, then Gaussian noise from the same stream
     rng = galsim.BaseDeviate(4343)
     a = galsim.ImageF(9, 7, init_value=0.)

@@ -132,3 +132,36 @@ def test_variable_gaussian_noise_batch_vs_oracle():
 def test_variable_gaussian_noise_shape_mismatch():
     with pytest.raises(galsim.GalSimIncompatibleValuesError):
         galsim.ImageF(5, 4).addNoise(galsim.VariableGaussianNoise(galsim.BaseDeviate(1), galsim.ImageD(4, 5)))
+
+
+def test_deviates_vs_reference():
+    """UniformDeviate / GaussianDeviate / PoissonDeviate sequences and DeviateNoise: the same
+    script as the reference's fixture (make_golden.deviate_sequences) run on this package."""
+    mine = MG.deviate_sequences(galsim)
+    for k, v in mine.items():
+        ref = GOLD['dev_' + k]
+        assert v.shape == ref.shape, k
+        if k.startswith('devnoise'):
+            assert_close(v, ref)
+        elif k in ('gaussian', 'shared'):
+            assert np.allclose(v, ref, rtol=1e-13, atol=1e-13), (k, np.abs(v - ref).max())
+        else:
+            assert np.array_equal(v, ref), (k, v, ref)
+
+
+def test_deviate_errors_and_state():
+    with pytest.raises(galsim.GalSimRangeError):
+        galsim.GaussianDeviate(1, sigma=-1.)
+    with pytest.raises(galsim.GalSimValueError):
+        galsim.PoissonDeviate(1, mean=-1.)
+    with pytest.raises(galsim.GalSimValueError):
+        galsim.PoissonDeviate(1).generate_from_expectation(np.array([1., -2.]))
+    g = galsim.GaussianDeviate(77)
+    g()
+    d = g.duplicate()
+    assert g() == d() and g() == d()            # the pair cache travels with the copy
+    u = galsim.UniformDeviate(5)
+    w = u.raw()
+    assert u._stream.used > 0 and 0 <= w < 2 ** 32
+    with pytest.raises(galsim.GalSimError):
+        galsim.DeviateNoise(galsim.UniformDeviate(1)).getVariance()

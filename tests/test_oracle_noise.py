@@ -65,3 +65,83 @@ def test_variable_then_gaussian_stream():
     O.gaussian_noise(b, rng, 2.)
     assert np.array_equal(a, GOLD['varstream_a'])
     assert np.array_equal(b, GOLD['varstream_b'])
+
+
+def _ogen(f, n):
+    return [f() for _ in range(n)]
+
+
+def test_deviate_sequences_match_reference():
+    """The oracle's deviates (uniform_01, the boost 1.48 normal with its pair cache, the
+    PoissonDeviate mean switching) reproduce the reference's deviate fixture script
+    (make_golden.deviate_sequences) draw for draw."""
+    r = O.base_deviate(1234)
+    u = lambda: O.uniform01(r)
+    assert np.array_equal(_ogen(u, 14), GOLD['dev_uniform'])
+
+    r = O.base_deviate(2345)
+    n = O.ONormal(1.5, 2.5)
+    a = _ogen(lambda: n(r), 3)
+    n.reset()                                    # generate clears the cache
+    g = _ogen(lambda: n(r), 5)
+    b = _ogen(lambda: n(r), 2)                   # the first from the cache
+    unit = O.ONormal(0., 1.)                     # generate_from_variance: mean 0, sigma 1, fresh
+    v = [unit(r) * np.sqrt(x) for x in (0.5, 2., 0., 9.)]
+    n.reset()
+    out = np.concatenate([a, g, b, v, [n(r)]])
+    assert np.allclose(out, GOLD['dev_gaussian'], rtol=0, atol=0)
+
+    r = O.base_deviate(3456)
+    pd = O.OPoissonDeviate(r)
+    pd.set_mean(7.3)
+    a = _ogen(pd, 4) + _ogen(pd, 6)
+    pd2 = O.OPoissonDeviate(r)
+    pd2.set_mean(120.)
+    b = _ogen(pd2, 3) + _ogen(pd2, 5)
+    pz = O.OPoissonDeviate(r)
+    pz.set_mean(0.)
+    c = _ogen(pz, 3)
+    ph = O.OPoissonDeviate(r)
+    ph.set_mean(float(2 ** 31))
+    d = _ogen(ph, 3)
+    ph.gd.reset()                                # generate clears the normal branch's cache
+    g3 = _ogen(ph, 3)
+    d += _ogen(ph, 1) + g3                       # the script lists the call after it first
+    e = []
+    for m in (0., 3.2, 50., 0., float(2 ** 31), 7.):
+        if m > 0.:
+            pd.set_mean(m)
+            e.append(pd())
+        else:
+            e.append(0.)
+    pd.set_mean(7.3)
+    out = np.concatenate([a, b, c, d, e, [pd()]])
+    assert np.array_equal(out, GOLD['dev_poisson'])
+
+    r = O.base_deviate(4567)
+    sg = O.ONormal(0., 3.)
+    s = [O.uniform01(r), sg(r), sg(r), sg(r), O.uniform01(r), O.uniform01(r)]
+    assert np.array_equal(s, GOLD['dev_shared'])
+
+
+def test_deviate_noise_matches_reference():
+    for name, seed in (('uniform', 5678), ('gauss', 6789), ('poisson', 7890)):
+        r = O.base_deviate(seed)
+        if name == 'uniform':
+            gen = lambda k: np.array([O.uniform01(r) for _ in range(k)])
+        elif name == 'gauss':
+            nrm = O.ONormal(-2., 0.5)
+
+            def gen(k):
+                nrm.reset()
+                return np.array([nrm(r) for _ in range(k)])
+        else:
+            pdv = O.OPoissonDeviate(r)
+            pdv.set_mean(4.5)
+            gen = lambda k: np.array([pdv() for _ in range(k)])
+        im = np.full((5, 7), 10., np.float32)
+        im += gen(35).reshape(5, 7).astype(np.float32)
+        imi = np.full((3, 6), 3, np.int32)
+        imi += gen(18).reshape(3, 6).astype(np.int32)
+        assert np.array_equal(im, GOLD['dev_devnoise_' + name])
+        assert np.array_equal(imi, GOLD['dev_devnoise_i_' + name])
