@@ -16,7 +16,7 @@ LIB = os.path.join(HERE, 'libgsb.so')
 SOURCES = ['gsb_api.cu', 'gsb_tables.cu', 'gsb_draw.cu', 'gsb_draw_f32_small.cu',
            'gsb_draw_f32_large.cu', 'gsb_draw_f64_small.cu', 'gsb_draw_f64_large.cu', 'gsb_draw_large.cu',
            'gsb_noalloc.cu', 'gsb_adjoint.cu', 'gsb_adjoint_f32_small.cu', 'gsb_adjoint_f32_large.cu',
-           'gsb_adjoint_f64_small.cu', 'gsb_adjoint_f64_large.cu', 'gsb_images.cu', 'gsb_noise.cu',
+           'gsb_adjoint_f64_small.cu', 'gsb_adjoint_f64_large.cu', 'gsb_adjoint_large.cu', 'gsb_images.cu', 'gsb_noise.cu',
            'gsb_fits.cu', 'gsb_standalone.cu', 'gsb_chromatic.cu', 'gsb_real.cu']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
@@ -33,7 +33,16 @@ def _stale():
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, 'include', 'gsb.h')]
-    return any(os.path.getmtime(d) > t for d in deps)
+    if any(os.path.getmtime(d) > t for d in deps):
+        return True
+    # a source added since the library was linked, or an object older than its source
+    build_dir = os.path.join(HERE, '_build')
+    for src in SOURCES:
+        obj = os.path.join(build_dir, src.replace('.cu', '.o'))
+        if os.path.isdir(build_dir) and (not os.path.exists(obj) or
+                                         os.path.getmtime(obj) < os.path.getmtime(os.path.join(CSRC, src))):
+            return True
+    return False
 
 
 def build(force=False, verbose=False):

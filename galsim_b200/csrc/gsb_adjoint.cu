@@ -35,6 +35,10 @@ static bool adjoint_workspace_f64(int N, int n_stamps, size_t* bytes)
     return adjoint_workspace_f64_small(N, n_stamps, bytes) || adjoint_workspace_f64_large(N, n_stamps, bytes);
 }
 
+bool is_large_fft(int N);
+size_t adjoint_large_workspace_size(int N, int n_stamps, int precision);
+int adjoint_large(const AdjArgs& args, int N, int precision, size_t work_bytes, cudaStream_t stream);
+
 int adjoint_grad_count(const gsb_template* tpl) { return grad_count(*tpl); }
 
 size_t adjoint_workspace_size(int N, int n_stamps, int precision)
@@ -42,6 +46,7 @@ size_t adjoint_workspace_size(int N, int n_stamps, int precision)
     size_t b = 0;
     if (precision == GSB_F64 ? adjoint_workspace_f64(N, n_stamps, &b) : adjoint_workspace_f32(N, n_stamps, &b))
         return b;
+    if (is_large_fft(N)) return adjoint_large_workspace_size(N, n_stamps, precision);
     return 0;
 }
 
@@ -75,10 +80,11 @@ int adjoint_images(const gsb_template* tpl, int n_stamps, const gsb_leaf* d_leav
     bool handled = false;
     const int rc = precision == GSB_F64 ? adjoint_launch_f64(N, args, work_bytes, stream, &handled)
                                         : adjoint_launch_f32(N, args, work_bytes, stream, &handled);
-    if (!handled)
-        return set_error(GSB_ERR_UNSUPPORTED, "adjoint FFT size " + std::to_string(N) +
-                                              " is not built (supported: 2^a or 3*2^a, 32..1024)");
-    return rc;
+    if (handled) return rc;
+    // N > 1024: the split row / column kernels of the large draw path, in reverse
+    if (is_large_fft(N)) return adjoint_large(args, N, precision, work_bytes, stream);
+    return set_error(GSB_ERR_UNSUPPORTED, "adjoint FFT size " + std::to_string(N) +
+                                          " is not built (supported: 2^a or 3*2^a, 32..16384)");
 }
 
 }  // namespace gsb

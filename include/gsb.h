@@ -540,7 +540,9 @@ int gsb_adjoint_grad_count(const gsb_template* tpl);
 /* Scratch bytes gsb_adjoint_images needs for a bucket of stamps of FFT size N. */
 size_t gsb_adjoint_workspace_size(int N, int n_stamps, int precision);
 
-/* Reverse mode of gsb_draw_images for one FFT-size bucket (N in 32..1024): given
+/* Reverse mode of gsb_draw_images for one FFT-size bucket (N in 32..16384; above 1024 the split
+ * row / column kernels of the large draw path in reverse, with per-stamp slabs in the
+ * workspace): given
  * d_cotangent = dL/d(image), laid out exactly as the images gsb_draw_images writes for the same
  * stamps (out_offset, nx, ny; dtype cot_dtype), write d_grad[s * count + e] = dL/d(entry e of
  * stamp s) (FP64, count from gsb_adjoint_grad_count).  The derivatives are analytic (each

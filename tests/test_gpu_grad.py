@@ -88,7 +88,61 @@ def _fd(plan, base, w, field, idx, h, sizes):
 
 @pytest.mark.parametrize('name,obj', list(_trees()), ids=[t[0] for t in _trees()])
 def test_record_gradients_fp64_vs_finite_differences(name, obj):
-    plan = autodiff.RecordPlan(obj, 40, 40, 0.2, dtype=np.float64, precision='fp64')
+    _check_record_gradients(name, obj, 40, 40, 0.2)
+
+
+def _large_trees():
+    """Trees drawn with FFT sizes above 1024 (the split large-FFT path and its adjoint)."""
+    rng = np.random.default_rng(17)
+    B = 2
+
+    def u(a, b):
+        return rng.uniform(a, b, B)
+
+    g1536 = galsim.GSParams(minimum_fft_size=1536)
+    yield 'sersic_airy_N1536', 1536, galsim.Convolve(
+        galsim.Sersic(n=u(1.5, 3.5), half_light_radius=u(0.4, 0.7), flux=u(1e3, 5e3), gsparams=g1536)
+        .shear(g1=u(-0.2, 0.2), g2=u(-0.2, 0.2)).shift(u(-0.1, 0.1), u(-0.1, 0.1)),
+        galsim.Airy(lam_over_diam=0.1, obscuration=0.3, gsparams=g1536), galsim.Pixel(0.05, gsparams=g1536))
+    g2048 = galsim.GSParams(minimum_fft_size=2048)
+    yield 'exp_gauss_sum_moffat_N2048', 2048, galsim.Convolve(
+        galsim.Add(galsim.Exponential(half_light_radius=u(0.3, 0.5), flux=u(500., 900.), gsparams=g2048)
+                   .shear(g1=u(-0.2, 0.2), g2=u(-0.2, 0.2)),
+                   galsim.Gaussian(sigma=u(0.1, 0.2), flux=u(100., 300.), gsparams=g2048)
+                   .shift(u(-0.1, 0.1), u(-0.1, 0.1))),
+        galsim.Moffat(beta=3.0, fwhm=0.4, gsparams=g2048), galsim.Pixel(0.05, gsparams=g2048))
+
+
+@pytest.mark.parametrize('name,N,obj', list(_large_trees()), ids=[t[0] for t in _large_trees()])
+def test_record_gradients_large_fft_fp64_vs_finite_differences(name, N, obj):
+    """The adjoint of the split large-FFT path (N > 1024) against FP64 central differences."""
+    plan = _check_record_gradients(name, obj, 64, 64, 0.05)
+    assert np.all(plan.last.N == N)
+
+
+@pytest.mark.parametrize('name,N,obj', list(_large_trees()), ids=[t[0] for t in _large_trees()])
+def test_large_fft_adjoint_fp32_vs_fp64(name, N, obj):
+    w = None
+    grads = []
+    for prec, dt in (('fp64', np.float64), ('fp32', np.float32)):
+        plan = autodiff.RecordPlan(obj, 64, 64, 0.05, dtype=dt, precision=prec)
+        base = plan.records()
+        plan.set_records(base)
+        img = plan.draw()
+        assert np.all(plan.last.N == N)
+        if w is None:
+            w = np.random.default_rng(5).standard_normal(tuple(img.shape))
+        grads.append(plan.adjoint(torch.as_tensor(w, device=img.device, dtype=img.dtype)))
+    for field in autodiff.RECORD_FIELDS:
+        a, b = grads[0][field].cpu().numpy(), grads[1][field].cpu().numpy()
+        if a.size == 0:
+            continue
+        top = np.abs(a).max()
+        assert np.abs(a - b).max() <= 1e-4 * max(top, 1e-30), (name, field, np.abs(a - b).max(), top)
+
+
+def _check_record_gradients(name, obj, nx, ny, scale):
+    plan = autodiff.RecordPlan(obj, nx, ny, scale, dtype=np.float64, precision='fp64')
     base = plan.records()
     plan.set_records(base)
     img = plan.draw()
@@ -125,6 +179,7 @@ def test_record_gradients_fp64_vs_finite_differences(name, obj):
                 assert err <= 1e-5 * max(abs(fd), 1e-2 * scale_ref), (name, field, full, ga[full], fd)
                 checked += 1
     assert checked > 20
+    return plan
 
 
 def _fit_problem(B=6, seed=11):
