@@ -37,7 +37,7 @@ from .sed import SED
 from .bandpass import Bandpass
 from . import integ, dcr
 from .chromatic import (ChromaticObject, ChromaticTransformation, SimpleChromaticTransformation,
-                        ChromaticAtmosphere, ChromaticSum, ChromaticConvolution)
+                        ChromaticAtmosphere, ChromaticAiry, ChromaticSum, ChromaticConvolution)
 from ._lib import set_device
 from . import autodiff
 from . import config

@@ -41,7 +41,7 @@ from .errors import (GalSimError, GalSimSEDError, GalSimValueError, GalSimIncomp
                      GalSimNotImplementedError)
 
 __all__ = ['ChromaticObject', 'ChromaticTransformation', 'SimpleChromaticTransformation',
-           'ChromaticAtmosphere', 'ChromaticSum', 'ChromaticConvolution', 'draw_batch_chromatic']
+           'ChromaticAtmosphere', 'ChromaticAiry', 'ChromaticSum', 'ChromaticConvolution', 'draw_batch_chromatic']
 
 
 def _remove_setup_kwargs(kwargs):
@@ -576,6 +576,70 @@ class ChromaticAtmosphere(ChromaticObject):
     def __repr__(self):
         return 'galsim.ChromaticAtmosphere(%r, base_wavelength=%r, alpha=%r)' % (
             self.base_obj, self.base_wavelength, self.alpha)
+
+
+class ChromaticAiry(ChromaticObject):
+    """An Airy PSF whose diffraction limit scales with wavelength (chromatic.py:3765-3885): at
+    wavelength w, Airy(lam_over_diam * w / lam) with the other Airy arguments (flux, obscuration)
+    unchanged; the fiducial lam_over_diam is given, or (1e-9 lam / diam) radians in scale_unit."""
+
+    def __init__(self, lam, diam=None, lam_over_diam=None, scale_unit=None, gsparams=None, **kwargs):
+        from .angle import radians
+        if scale_unit is None:
+            scale_unit = arcsec
+        elif isinstance(scale_unit, str):
+            scale_unit = AngleUnit.from_name(scale_unit)
+        self.scale_unit = scale_unit
+        self._gsparams = GSParams.check(gsparams)
+        if (diam is None) == (lam_over_diam is None):
+            raise GalSimIncompatibleValuesError(
+                "Need to specify telescope diameter OR wavelength/diam ratio",
+                diam=diam, lam_over_diam=lam_over_diam)
+        if diam is not None:
+            self.lam_over_diam = (1.e-9 * lam / diam) * (radians / self.scale_unit)
+        else:
+            self.lam_over_diam = float(lam_over_diam)
+        self.lam = float(lam)
+        self.kwargs = kwargs
+        self.separable = False
+        self.interpolated = False
+        self.deinterpolated = self
+
+    @property
+    def sed(self):
+        return SED(1, 'nm', '1')
+
+    gsparams = property(lambda self: self._gsparams)
+
+    def withGSParams(self, gsparams=None, **kwargs):
+        if gsparams == self.gsparams and not kwargs:
+            return self
+        ret = copy.copy(self)
+        ret._gsparams = GSParams.check(gsparams, self.gsparams, **kwargs)
+        return ret
+
+    def _airy(self, lod):
+        from .profiles import Airy
+        return Airy(lam_over_diam=lod, scale_unit=self.scale_unit, gsparams=self.gsparams, **self.kwargs)
+
+    def evaluateAtWavelength(self, wave):
+        return self._airy(self.lam_over_diam * (wave / self.lam))
+
+    def _evaluate_batch(self, waves):
+        return self._airy(self.lam_over_diam * (np.asarray(waves, dtype=float) / self.lam))
+
+    def __eq__(self, other):
+        return (self is other or
+                (isinstance(other, ChromaticAiry) and self.lam == other.lam and
+                 self.lam_over_diam == other.lam_over_diam and self.scale_unit == other.scale_unit and
+                 self.gsparams == other.gsparams and self.kwargs == other.kwargs))
+
+    def __hash__(self):
+        return hash(("galsim.ChromaticAiry", self.lam, self.lam_over_diam, self.scale_unit,
+                     self.gsparams, frozenset(self.kwargs.items())))
+
+    def __repr__(self):
+        return 'galsim.ChromaticAiry(lam=%r, lam_over_diam=%r)' % (self.lam, self.lam_over_diam)
 
 
 class ChromaticSum(ChromaticObject):

@@ -65,11 +65,20 @@ def case(galsim, name):
         psf = galsim.ChromaticObject(galsim.Moffat(beta=3.5, fwhm=0.5)).shift(lambda w: ((w - 500.) * 1e-3, 0.))
         obj = galsim.Convolve(galsim.Gaussian(sigma=0.4, flux=2.) * s1, psf)
         return obj, b1, dict(nx=32, ny=32, scale=0.2, offset=(0.3, -0.2))
+    if name == 'airy_gal':
+        psf = galsim.ChromaticAiry(lam=500., diam=0.5, obscuration=0.3)
+        obj = galsim.Convolve(galsim.Exponential(half_light_radius=0.3) * s1, psf)
+        return obj, b1, dict(nx=48, ny=48, scale=0.1)
+    if name == 'atm_airy_f8':
+        psf = galsim.Convolve(galsim.ChromaticAtmosphere(galsim.Kolmogorov(fwhm=0.5), 600., zenith_angle=20. * deg),
+                              galsim.ChromaticAiry(lam=600., lam_over_diam=0.15))
+        obj = galsim.Convolve(galsim.Sersic(n=2., half_light_radius=0.3) * s2, psf)
+        return obj, b2, dict(nx=40, ny=40, scale=0.15, dtype=np.float64)
     raise ValueError(name)
 
 
 CASES = ['sep_moffat', 'sep_z_kolm_f8', 'atm_kolm', 'atm_kolm_trapz', 'atm_kolm_midpt', 'atm_kolm_f8',
-         'atm_bulge_disk', 'dilate_star', 'shift_gal_psf']
+         'atm_bulge_disk', 'dilate_star', 'shift_gal_psf', 'airy_gal', 'atm_airy_f8']
 REFRACTION_WAVES = [350., 420.5, 500., 633., 800., 1000.]
 
 
