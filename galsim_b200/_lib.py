@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(HERE, 'libgsb.so')
 
 MAX_OPS, MAX_LEAVES, MAX_PHASES, MAX_SCALES = 32, 8, 8, 8
 GAUSSIAN, EXPONENTIAL, SERSIC, MOFFAT, KOLMOGOROV, AIRY, BOX, INTERPOLATED = range(8)
-INTERP_DELTA, INTERP_NEAREST, INTERP_LINEAR, INTERP_CUBIC, INTERP_QUINTIC, INTERP_LANCZOS = range(6)
+INTERP_DELTA, INTERP_NEAREST, INTERP_LINEAR, INTERP_CUBIC, INTERP_QUINTIC, INTERP_LANCZOS, INTERP_SINC = range(7)
 IMAGE_STEPK, IMAGE_MAXK, IMAGE_MAX_N = 1, 2, 4096
 OP_LEAF, OP_MUL, OP_ADD, OP_PHASE, OP_SCALE = 1, 2, 3, 4, 5
 LEAF_JAC_GENERAL, LEAF_SIZE_IS_HLR = 1, 2

@@ -225,7 +225,7 @@ int images_build(gsb_tables* t, int count, const gsb_image_desc* h_desc, const d
             (d.bx0 > 0 || d.bx1 < 0 || d.by0 > 0 || d.by1 < 0 || d.bx0 < d.x0 || d.by0 < d.y0 ||
              d.bx1 >= d.x0 + d.nx || d.by1 >= d.y0 + d.ny))
             return set_error(GSB_ERR_INVALID, "stepk bounds must contain (0, 0) and lie in the region");
-        if (d.x_interp < GSB_INTERP_DELTA || d.x_interp > GSB_INTERP_LANCZOS)
+        if (d.x_interp < GSB_INTERP_DELTA || d.x_interp > GSB_INTERP_SINC)
             return set_error(GSB_ERR_INVALID, "unknown x interpolant");
         if ((d.x_interp == GSB_INTERP_LANCZOS) != (d.x_table != nullptr))
             return set_error(GSB_ERR_INVALID, "a Lanczos x interpolant needs its x_table (and only it)");

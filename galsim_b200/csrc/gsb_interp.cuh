@@ -60,6 +60,10 @@ template <typename T>
 __device__ __forceinline__ T interp_uval(int code, T u)
 {
     if (code == GSB_INTERP_DELTA) return T(1);
+    if (code == GSB_INTERP_SINC) {
+        const T a = fabs(u);
+        return a > T(0.5) ? T(0) : (a < T(0.5) ? T(1) : T(0.5));
+    }
     const T s = sinc_ref<T>(u);
     switch (code) {
       case GSB_INTERP_NEAREST: return s;
@@ -88,6 +92,7 @@ __host__ __device__ inline double interp_urange(int code, double kacc)
       case GSB_INTERP_LINEAR: return sqrt(1. / kacc) / kPi;
       case GSB_INTERP_CUBIC: return pow((3. * sqrt(3.) / 8.) / kacc, 1. / 3.) / kPi;
       case GSB_INTERP_QUINTIC: return pow((25. * sqrt(5.) / 108.) / kacc, 1. / 3.) / kPi;
+      case GSB_INTERP_SINC: return 0.5;
     }
     return 0.;
 }

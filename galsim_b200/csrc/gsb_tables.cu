@@ -1157,7 +1157,7 @@ __global__ void prepare_leaves_kernel(const __grid_constant__ gsb_template tpl, 
         const int slot = L.table;
         const int xc = int(L.p[0]), kc = int(L.p[1]);
         if (slot < 0 || slot >= images.count) { atomicOr(status_out, 16); break; }
-        if (xc < GSB_INTERP_DELTA || xc > GSB_INTERP_LANCZOS || kc < GSB_INTERP_NEAREST ||
+        if (xc < GSB_INTERP_DELTA || xc > GSB_INTERP_SINC || kc < GSB_INTERP_NEAREST ||
             kc > GSB_INTERP_LANCZOS) { atomicOr(status_out, 32); break; }
         // a Lanczos k interpolant: p[2] holds its coefficient block {n, conserve_dc, K_1..5};
         // n <= 3 (at most 7 taps per axis)

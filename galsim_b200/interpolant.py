@@ -5,9 +5,9 @@ ixrange), its Fourier extent (urange, krange), GSParams handling, equality and n
 kernels run on the GPU (galsim_b200/csrc/gsb_interp.cuh): Delta (as x interpolant only),
 Nearest, Linear, Cubic and Quintic, Lanczos as the x interpolant (its transform tabulated
 on the host exactly as the reference tabulates it, then read from a device table) and as the
-k interpolant for n <= 3.  SincInterpolant and larger Lanczos k interpolants can be
-constructed, but an InterpolatedImage using them raises GalSimNotImplementedError when it is
-sized or drawn.
+k interpolant for n <= 3, and SincInterpolant as the x interpolant.  Sinc and larger Lanczos
+k interpolants can be constructed, but an InterpolatedImage using them raises
+GalSimNotImplementedError when it is sized or drawn.
 """
 import math
 
@@ -111,7 +111,10 @@ class Nearest(Interpolant):
 
 
 class SincInterpolant(Interpolant):
-    """Sinc interpolation (interpolant.py:349-417); not built on the GPU (infinite support)."""
+    """Sinc interpolation (interpolant.py:349-417): as the x interpolant its transform is the
+    box |u| < 1/2 (SincInterpolant::uval); as the k interpolant (infinite support) it is not
+    built."""
+    _code = _lib.INTERP_SINC
     xrange = property(lambda self: 1. / (math.pi * self._gsparams.kvalue_accuracy))
     ixrange = property(lambda self: 2 * int(math.ceil(self.xrange)))
     krange = property(lambda self: math.pi)

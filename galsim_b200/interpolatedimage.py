@@ -17,8 +17,9 @@ against batched objects it is combined with.
 Noise padding with Gaussian noise of a given variance (noise_pad a number) fills its square of
 the frame with the reference's stream (BaseDeviate(rng), drawn on the GPU) before the pad image
 and the image are placed.  Not built: padding with correlated noise (a CorrelatedNoise, an
-image or a file), depixelize, FITS file names, non-PixelScale WCS, the sinc interpolant and
-Lanczos(n > 3) as the k interpolant.
+image or a file), depixelize, FITS file names, non-PixelScale WCS, and sinc or Lanczos(n > 3)
+as the k interpolant (sinc as the x interpolant is built: its transform is the box |u| < 1/2,
+and its infinite support makes stepk tiny unless forced).
 """
 import math
 
@@ -31,7 +32,7 @@ from .errors import (GalSimIncompatibleValuesError, GalSimNotImplementedError, G
 from .gsobject import GSObject
 from .gsparams import GSParams
 from .image import Image
-from .interpolant import Delta, Lanczos, Quintic, convert_interpolant
+from .interpolant import Delta, Lanczos, Quintic, SincInterpolant, convert_interpolant
 from .position import _PositionD
 from .wcs import BaseWCS, PixelScale
 
@@ -85,11 +86,11 @@ class _ImageLeaf(GSObject):
 
     def _flatten(self, bld, jac):
         xi, ki = self._x_interpolant, self._k_interpolant
-        if (xi._code is None or ki._code is None or isinstance(ki, Delta) or
+        if (xi._code is None or ki._code is None or isinstance(ki, (Delta, SincInterpolant)) or
                 (isinstance(ki, Lanczos) and ki.n > 3)):
             raise GalSimNotImplementedError(
                 "InterpolatedImage with x interpolant %s and k interpolant %s is not built on the "
-                "GPU (x: Delta, Nearest, Linear, Cubic, Quintic, Lanczos; k: Nearest, Linear, "
+                "GPU (x: Delta, Nearest, Linear, Cubic, Quintic, Lanczos, Sinc; k: Nearest, Linear, "
                 "Cubic, Quintic, Lanczos(n <= 3))" % (xi, ki))
         bld.add_leaf(_lib.INTERPOLATED, jac, 1., (float(xi._code), float(ki._code), 0.))
         bld.image_sources[len(bld.leaves) - 1] = self._sources

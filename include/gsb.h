@@ -59,10 +59,12 @@ enum {
     GSB_INTERP_LINEAR  = 2,
     GSB_INTERP_CUBIC   = 3,
     GSB_INTERP_QUINTIC = 4,
-    GSB_INTERP_LANCZOS = 5    /* as x interpolant: the transform from the image's x_table
+    GSB_INTERP_LANCZOS = 5,   /* as x interpolant: the transform from the image's x_table
                                  (the reference's spline table of Lanczos::uCalc); as k
                                  interpolant (n <= 3): the kernel Lanczos::xCalc, with the
                                  leaf's p[2] the address of {n, conserve_dc, K_1..K_5, 0}  */
+    GSB_INTERP_SINC    = 6    /* x interpolant only: uval = 1 below |u| = 1/2, 1/2 at it, 0
+                                 above (SincInterpolant::uval, Interpolant.cpp:204-209)    */
 };
 
 /* Program opcodes.  A program is evaluated per k-point on a small stack of complex values:

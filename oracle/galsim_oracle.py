@@ -1191,6 +1191,9 @@ def interp_uval(name, u, gsp=DEFAULT):
         return lanczos_uval(lz[0], lz[1], u, gsp)
     if name == 'delta':
         return np.ones_like(u)
+    if name == 'sinc':
+        a = np.abs(u)
+        return np.where(a > 0.5, 0., np.where(a < 0.5, 1., 0.5))
     s = _sinc(u)
     if name == 'nearest':
         return s
@@ -1213,7 +1216,8 @@ class _XRange(dict):
         return float(_lanczos_name(name)[0])
 
 
-INTERP_XRANGE = _XRange({'delta': 0., 'nearest': 0.5, 'linear': 1., 'cubic': 2., 'quintic': 3.})
+INTERP_XRANGE = _XRange({'delta': 0., 'nearest': 0.5, 'linear': 1., 'cubic': 2., 'quintic': 3.,
+                         'sinc': 1. / (PI * 1.e-5)})   # sinc: 1 / (pi kvalue_accuracy), default GSParams
 
 
 def interp_urange(name, kacc, gsp=None):
@@ -1223,7 +1227,8 @@ def interp_urange(name, kacc, gsp=None):
     if lz is not None:
         g = gsp if gsp is not None else OGSParams(kvalue_accuracy=kacc)
         return lanczos_table(lz[0], lz[1], g)[3]
-    return {'delta': lambda: 1. / kacc,
+    return {'sinc': lambda: 0.5,
+            'delta': lambda: 1. / kacc,
             'nearest': lambda: 1. / (PI * kacc),
             'linear': lambda: math.sqrt(1. / kacc) / PI,
             'cubic': lambda: math.pow((3. * math.sqrt(3.) / 8.) / kacc, 1. / 3.) / PI,
@@ -1234,7 +1239,7 @@ def interp_krange(name, kacc, gsp=None):
     """Interpolant.krange (interpolant.py:264, 328, 462, 528, 597, 667)."""
     if _lanczos_name(name) is not None:
         return 2. * PI * interp_urange(name, kacc, gsp)
-    return {'delta': 2. * PI / kacc, 'nearest': 2. / kacc, 'linear': 2. / kacc ** 0.5,
+    return {'sinc': PI, 'delta': 2. * PI / kacc, 'nearest': 2. / kacc, 'linear': 2. / kacc ** 0.5,
             'cubic': 1.7320508075688774 / kacc ** (1. / 3.),
             'quintic': 1.6058208066649935 / kacc ** (1. / 3.)}[name]
 

@@ -159,6 +159,12 @@ INTERP_DRAW_CASES = [
      48, 48, 0.2, 'f8', (0., 0.)),
     ('ii_lanczos2F_k_f4', ('ii', 'gal24', 0.25, {'x_interpolant': 'lanczos5', 'k_interpolant': 'lanczos2F'}),
      40, 40, 0.25, 'f4', (0.1, 0.2)),
+    # the sinc x interpolant (its transform a box; stepk forced, as its support is infinite;
+    # drawn at another scale than the image's, so that no k point falls on the box's edge,
+    # where the transform jumps)
+    ('ii_sinc_x', ('conv', [('exp', 0.4, 1.), ('ii', 'psf32', 0.2, {'x_interpolant': 'sinc',
+                                                                    '_force_stepk': 0.6})]),
+     56, 56, 0.17, 'f8', (0., 0.)),
     ('ii_calc_floats', ('conv', [('exp', 0.3, 1.), ('ii', 'psf32', 0.2, {'calculate_maxk': 3.0,
                                                                          'calculate_stepk': 0.5})]),
      48, 48, 0.2, 'f8', (0., 0.)),
