@@ -54,9 +54,12 @@ STAMP_DTYPE = np.dtype({'names': ['N', 'Nk', 'xmin', 'ymin', 'nx', 'ny', 'out_of
                         'formats': ['i4', 'i4', 'i4', 'i4', 'i4', 'i4', 'i8'],
                         'offsets': [0, 4, 8, 12, 16, 20, 24], 'itemsize': 32})
 
-XLEAF_DTYPE = np.dtype({'names': ['jac', 'xoff', 'yoff', 'flux_ratio', 'flux', 'p', 'type', 'flags'],
-                        'formats': [('f8', 4), 'f8', 'f8', 'f8', 'f8', ('f8', 3), 'i4', 'i4'],
-                        'offsets': [0, 32, 40, 48, 56, 64, 88, 92], 'itemsize': 96})
+XLEAF_DTYPE = np.dtype({'names': ['jac', 'xoff', 'yoff', 'flux_ratio', 'flux', 'p', 'type', 'flags',
+                                  'region', 'rx0', 'ry0', 'rnx', 'rny', 'ktab'],
+                        'formats': [('f8', 4), 'f8', 'f8', 'f8', 'f8', ('f8', 3), 'i4', 'i4',
+                                    'u8', 'i4', 'i4', 'i4', 'i4', 'u8'],
+                        'offsets': [0, 32, 40, 48, 56, 64, 88, 92, 96, 104, 108, 112, 116, 120],
+                        'itemsize': 128})
 XLEAF_JAC = 1
 
 IMAGE_DESC_DTYPE = np.dtype({'names': ['N', 'nx', 'ny', 'x0', 'y0', 'bx0', 'bx1', 'by0', 'by1',

@@ -9,6 +9,7 @@
 #include <algorithm>
 
 #include "gsb_internal.cuh"
+#include "gsb_interp.cuh"
 
 namespace gsb {
 
@@ -25,6 +26,12 @@ struct XLeafC {
     double c[6];               // per-type constants
     const double4* node;       // Kolmogorov radial spline
     int nnode;
+    // InterpolatedImage: the region, its frame position and size, the x interpolant and its
+    // half-width, a Lanczos kernel's coefficients
+    const double* region;
+    int rx0, ry0, rnx, rny, xc;
+    double xr;
+    const double* ktab;
 };
 
 // SBProfile::draw's pixel-grid mapping for one leaf (imscale 1; x0 = xmin - xoff).
@@ -129,6 +136,16 @@ __device__ void setup_profile(XLeafC& C, const gsb_xleaf& L, const gsb_gsparams&
         C.c[2] = 0.5 * L.p[1];
         break;
       }
+      case GSB_INTERPOLATED: {    // the interpolated pixel values (no normalisation of its own)
+        C.c[0] = L.flux;
+        C.region = L.region;
+        C.rx0 = L.rx0; C.ry0 = L.ry0; C.rnx = L.rnx; C.rny = L.rny;
+        C.xc = int(L.p[0]);
+        C.ktab = L.ktab;
+        C.xr = C.xc == GSB_INTERP_LANCZOS ? L.ktab[0]
+             : C.xc == GSB_INTERP_SINC ? 1. / (kPi * gsp.kvalue_accuracy) : interp_xrange(C.xc);
+        break;
+      }
       default:
         C.type = -1;
     }
@@ -150,6 +167,8 @@ __device__ double kolm_radial(const double4* nd, int n, double r)
     return aa * a.y + bb * b.y + ((aa * aa * aa - aa) * a.z + (bb * bb * bb - bb) * b.z) * (h * h) / 6.;
 }
 
+__device__ double ii_xvalue(const XLeafC& C, double x, double y);
+
 __device__ double xvalue(const XLeafC& C, double u, double v)
 {
     switch (C.type) {
@@ -169,6 +188,8 @@ __device__ double xvalue(const XLeafC& C, double u, double v)
       }
       case GSB_KOLMOGOROV:
         return C.c[0] * kolm_radial(C.node, C.nnode, sqrt(u * u + v * v) * C.c[1]);
+      case GSB_INTERPOLATED:
+        return C.c[0] * ii_xvalue(C, u, v);
       case GSB_AIRY: {
         const double nu = sqrt(u * u + v * v) * C.c[1] * kPi;
         double x;
@@ -179,6 +200,41 @@ __device__ double xvalue(const XLeafC& C, double u, double v)
       }
     }
     return 0.;
+}
+
+// The x interpolant's kernel (Interpolant::xval): the polynomial kernels, Lanczos::xCalc, and
+// sinc(x) for SincInterpolant.
+__device__ double ii_xval(const XLeafC& C, double x)
+{
+    if (C.xc == GSB_INTERP_LANCZOS) return lanczos_xval<double>(C.ktab, x);
+    if (C.xc == GSB_INTERP_SINC) return sinc_ref<double>(x);
+    return interp_xval<double>(C.xc, x);
+}
+
+// SBInterpolatedImage::xValue (SBInterpolatedImage.cpp:167-215): the taps within the x
+// interpolant's half-width of (x, y) (a single tap along an axis where the position is an
+// integer to 10 eps), clipped to the nonzero region, summed row by row.
+__device__ double ii_xvalue(const XLeafC& C, double x, double y)
+{
+    constexpr double kSmall = 10. * 2.220446049250313e-16;
+    int p1, p2, q1, q2;
+    const double fx = floor(x + 0.01), fy = floor(y + 0.01);
+    if (fabs(x - fx) < kSmall * (fabs(x) + 1.)) { p1 = p2 = int(fx); }
+    else { p1 = int(ceil(x - C.xr)); p2 = int(floor(x + C.xr)); }
+    if (fabs(y - fy) < kSmall * (fabs(y) + 1.)) { q1 = q2 = int(fy); }
+    else { q1 = int(ceil(y - C.xr)); q2 = int(floor(y + C.xr)); }
+    const int bx1 = C.rx0 + C.rnx - 1, by1 = C.ry0 + C.rny - 1;
+    if (p2 < C.rx0 || p1 > bx1 || q2 < C.ry0 || q1 > by1) return 0.;
+    p1 = max(p1, C.rx0); p2 = min(p2, bx1);
+    q1 = max(q1, C.ry0); q2 = min(q2, by1);
+    double sum = 0.;
+    for (int q = q1; q <= q2; ++q) {
+        const double* row = C.region + (size_t)(q - C.ry0) * C.rnx - C.rx0;
+        double xsum = 0.;
+        for (int p = p1; p <= p2; ++p) xsum += ii_xval(C, p - x) * row[p];
+        sum += xsum * ii_xval(C, q - y);
+    }
+    return sum;
 }
 
 // SBBox::fillXImage: the diagonal form fills -w/2 <= x < w/2 on the pixel grid, the general

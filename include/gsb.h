@@ -287,9 +287,16 @@ typedef struct gsb_xleaf {
     double flux_ratio;   /* composed flux scaling |det| x flux_ratio (SBProfile::draw's flux_ratio) */
     double flux;         /* the leaf's flux */
     double p[3];         /* as gsb_leaf.p (Sersic: p[1] the scale radius; a truncated Sersic's
-                            flux is that of the truncated profile) */
-    int32_t type;        /* GSB_GAUSSIAN .. GSB_BOX (not GSB_INTERPOLATED) */
+                            flux is that of the truncated profile); GSB_INTERPOLATED: p[0] the
+                            x interpolant (GSB_INTERP_NEAREST .. GSB_INTERP_SINC) */
+    int32_t type;        /* GSB_GAUSSIAN .. GSB_INTERPOLATED */
     int32_t flags;
+    /* GSB_INTERPOLATED (SBInterpolatedImage::xValue, SBInterpolatedImage.cpp:167-215): the
+     * nonzero region of the padded image, FP64 row-major (rnx per row) device memory, its first
+     * pixel at frame position (rx0, ry0); ktab: a Lanczos interpolant's {n, conserve_dc, K_1..K_5} */
+    const double* region;
+    int32_t rx0, ry0, rnx, rny;
+    const double* ktab;
 } gsb_xleaf;
 
 #define GSB_XLEAF_JAC 1

@@ -1061,10 +1061,13 @@ def lanczos_xval(n, conserve_dc, x):
 
 
 def interp_xval(name, x):
-    """Real-space kernels: Nearest / Linear / Cubic / Quintic (Interpolant.cpp:171-432), Lanczos."""
+    """Real-space kernels: Nearest / Linear / Cubic / Quintic (Interpolant.cpp:171-432), Lanczos,
+    sinc."""
     lz = _lanczos_name(name)
     if lz is not None:
         return lanczos_xval(lz[0], lz[1], x)
+    if name == 'sinc':
+        return _sinc(x)
     x = np.abs(np.asarray(x, dtype=float))
     if name == 'nearest':
         return np.where(x > 0.5, 0., 1.)
@@ -1405,6 +1408,9 @@ class OInterpolatedImage(OObj):
         image_flux = float(np.sum(arr, dtype=np.float64))
         # getFlux of the nonzero image: the bounding box of image and pad image
         rows, cols = np.nonzero(nz)
+        # for real-space drawing: the padded image and its nonzero bounds in frame coordinates
+        self.leaf.xim = xim
+        self.leaf.nzb = (cols.min() - N // 2, cols.max() - N // 2, rows.min() - N // 2, rows.max() - N // 2)
         nz_flux = float(np.sum(xim[rows.min():rows.max() + 1, cols.min():cols.max() + 1]))
         if flux is None:
             flux = image_flux * (scale * scale if normalization.lower() in ('sb', 'surface brightness')
@@ -1640,6 +1646,37 @@ def _leaf_xvalue(leaf, u, v):
     raise NotImplementedError(type(leaf).__name__)
 
 
+def ii_xvalue(leaf, u, v):
+    """SBInterpolatedImage::xValue (SBInterpolatedImage.cpp:167-215) at arrays of positions:
+    the x interpolant's taps within its half-width (one tap along an axis at an integer to
+    10 eps), clipped to the nonzero bounds, summed over the padded image."""
+    small = 10. * np.finfo(float).eps
+    xr = INTERP_XRANGE[leaf.xi] if leaf.xi != 'sinc' else 1. / (PI * leaf.gsp.kvalue_accuracy)
+    bx0, bx1, by0, by1 = leaf.nzb
+    N = leaf.N
+    out = np.zeros(np.broadcast(u, v).shape)
+    uu, vv = np.broadcast_arrays(u, v)
+    for idx in np.ndindex(out.shape):
+        x, y = float(uu[idx]), float(vv[idx])
+        fx, fy = math.floor(x + 0.01), math.floor(y + 0.01)
+        if abs(x - fx) < small * (abs(x) + 1.):
+            p1 = p2 = int(fx)
+        else:
+            p1, p2 = int(math.ceil(x - xr)), int(math.floor(x + xr))
+        if abs(y - fy) < small * (abs(y) + 1.):
+            q1 = q2 = int(fy)
+        else:
+            q1, q2 = int(math.ceil(y - xr)), int(math.floor(y + xr))
+        if p2 < bx0 or p1 > bx1 or q2 < by0 or q1 > by1:
+            continue
+        p1, p2, q1, q2 = max(p1, bx0), min(p2, bx1), max(q1, by0), min(q2, by1)
+        wx = interp_xval(leaf.xi, np.arange(p1, p2 + 1) - x)
+        wy = interp_xval(leaf.xi, np.arange(q1, q2 + 1) - y)
+        sub = leaf.xim[q1 + N // 2:q2 + N // 2 + 1, p1 + N // 2:p2 + N // 2 + 1]
+        out[idx] = float(wy @ (sub @ wx))
+    return out
+
+
 def draw_real_leaf(leaf, nx, ny, xmin, ymin, jac, xoff, yoff, flux_ratio):
     """SBProfile::draw with imscale 1 for one leaf: the image positions xmin + i, ymin + j."""
     x0, y0 = xmin - xoff, ymin - yoff
@@ -1673,6 +1710,8 @@ def draw_real_leaf(leaf, nx, ny, xmin, ymin, jac, xoff, yoff, flux_ratio):
         return amp * np.where(inside, norm, 0.)
     u = u0 + i * du + j * duy
     v = v0 + j * dv + i * dvx
+    if isinstance(leaf, OInterpolatedImageLeaf):
+        return amp * ii_xvalue(leaf, u, v)
     return amp * _leaf_xvalue(leaf, u, v)
 
 
@@ -1693,6 +1732,8 @@ def draw_real(obj, nx, ny, xmin, ymin, jac=None, offset=(0., 0.), flux_scaling=1
         return draw_real(obj.original, nx, ny, xmin, ymin, jac, (dx, dy), flux_scaling)
     if isinstance(obj, OSum):
         return sum(draw_real(o, nx, ny, xmin, ymin, jac, offset, flux_scaling) for o in obj.objs)
+    if isinstance(obj, OInterpolatedImage):
+        return draw_real(obj.inner, nx, ny, xmin, ymin, jac, offset, flux_scaling)
     return draw_real_leaf(obj, nx, ny, xmin, ymin, jac, offset[0], offset[1], flux_scaling)
 
 

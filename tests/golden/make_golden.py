@@ -794,12 +794,21 @@ REAL_CASES = [
     ('r_box_rot_f8', ('rotate', 30., ('box', 1.3, 0.9, 3.)), 16, 16, 0.2, 'f8', 'no_pixel', (0.1, 0.1)),
     ('r_sum_f8', ('sum', [('gauss', 0.5, 3.), ('shift', 0.3, 0.2, ('exp', 0.4, 2.)),
                           ('shear', 0.1, 0.3, ('moffat', 2.5, 0.6, 1.))]), 36, 36, 0.15, 'f8', 'no_pixel', (0., 0.)),
+    # InterpolatedImages drawn in real space (their x interpolant over the image's pixels)
+    ('r_ii_quintic_f8', ('ii', 'psf32', 0.2, {}), 40, 40, 0.15, 'f8', 'no_pixel', (0.1, -0.2)),
+    ('r_ii_lanczos3_shear_f8', ('shear', 0.1, -0.05, ('ii', 'gal24', 0.25, {'x_interpolant': 'lanczos3'})),
+     36, 36, 0.2, 'f8', 'no_pixel', (0., 0.)),
+    ('r_ii_cubic_sum_f4', ('sum', [('ii', 'psf31x33', 0.2, {'x_interpolant': 'cubic', 'flux': 3.}),
+                                   ('gauss', 0.4, 1.)]), 32, 32, 0.2, 'f4', 'no_pixel', (0., 0.)),
+    ('r_ii_linear_same_scale_f8', ('ii', 'gal24', 0.2, {'x_interpolant': 'linear'}), 24, 24, 0.2, 'f8',
+     'no_pixel', (0., 0.)),
 ]
 
 
 def main_real(ref_root):
     from ref_import import import_reference_galsim
     galsim = import_reference_galsim(ref_root)
+    source_images()
     out = {}
     for name, spec, nx, ny, scale, dt, method, off in REAL_CASES:
         im = profile(galsim, spec).drawImage(nx=nx, ny=ny, scale=scale, dtype=np.dtype(dt).type, method=method,

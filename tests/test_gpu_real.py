@@ -17,6 +17,8 @@ import make_golden as MG
 
 pytestmark = pytest.mark.gpu
 REF = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden', 'reference_real.npz'))
+import specs  # noqa: E402
+specs.load_interp_images(np.load(os.path.join(specs.HERE, 'reference_interp.npz')))   # the 'ii' cases' images
 
 
 @pytest.mark.parametrize('case', MG.REAL_CASES, ids=[c[0] for c in MG.REAL_CASES])

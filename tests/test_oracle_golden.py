@@ -212,6 +212,7 @@ def test_truncated_moffat_kimage_matches_reference(case):
 
 
 REAL = np.load(specs.HERE + '/reference_real.npz')
+specs.load_interp_images(np.load(specs.HERE + '/reference_interp.npz'))    # the 'ii' cases' images
 
 
 @pytest.mark.parametrize('case', MG.REAL_CASES, ids=[c[0] for c in MG.REAL_CASES])
