@@ -326,6 +326,59 @@ class ChromaticObject(object):
         # (image.added_flux stays what the set-up draw left, as in the reference)
         return image
 
+    def drawKImage(self, bandpass, image=None, integrator='quadratic', **kwargs):
+        """The Fourier transform of the profile integrated over the bandpass (chromatic.py:
+        526-594): the monochromatic k-images at the integrator's wavelengths, as one batch on
+        the GPU, summed with the rule's weights in the rule's order; the keyword arguments are
+        GSObject.drawKImage's."""
+        if self.sed.dimensionless:
+            raise GalSimSEDError("Can only drawK ChromaticObjects with spectral SEDs.", self.sed)
+        prof0 = self.evaluateAtWavelength(bandpass.effective_wavelength)
+        image = prof0.drawKImage(image=image, setup_only=True, **kwargs)
+        _remove_setup_kwargs(kwargs)
+        wave_list, _, _ = combine_wave_list(self, bandpass)
+        if self.separable:
+            multiplier = _get_multiplier(self.sed, bandpass, tuple(wave_list))
+            prof0 *= multiplier / self.sed(bandpass.effective_wavelength)
+            return prof0.drawKImage(image=image, **kwargs)
+        integrator = _get_integrator(integrator, wave_list)
+        if isinstance(integrator, integ.SampleIntegrator):
+            bandpass = Bandpass(_LookupTable(wave_list, bandpass(wave_list), 'linear'), 'nm')
+        add_to_image = kwargs.pop('add_to_image', False)
+        image_int = integrator(self, bandpass, image, kwargs, doK=True)
+        self._last_n_eval = integrator.last_n_eval
+        if add_to_image:
+            image.array[...] += image_int.array
+        else:
+            image.array[...] = image_int.array
+        return image
+
+
+def _integrate_kimages(chrom, waves, weights, image, kwargs):
+    """The integrand of ChromaticObject.drawKImage at all `waves` in one batched k-space pass on
+    the image's grid (its bounds, scale = dk), summed as the rule sums it (integ.py:134-146:
+    0 + g_0 K_0 + g_1 K_1 + ..., complex, in the image's precision)."""
+    from . import _lib
+    from .image import Image
+    from .program import Program
+    kw = dict(kwargs)
+    kw.pop('recenter', None)
+    precision = kw.pop('precision', None)
+    if kw:
+        raise GalSimNotImplementedError("chromatic drawKImage arguments not built: %s" % sorted(kw))
+    profs = chrom._evaluate_batch(np.asarray(waves, dtype=float))
+    b = image.bounds
+    f64 = image.dtype == np.complex128 if precision is None else precision == 'fp64'
+    prog = Program(profs)
+    arrs = prog.draw_kimage(image.scale, b.xmin, b.ymin, b.xmax - b.xmin + 1, b.ymax - b.ymin + 1,
+                            _lib.F64 if f64 else _lib.F32)
+    if prog.B != len(waves):
+        arrs = np.broadcast_to(arrs, (len(waves),) + arrs.shape[1:])
+    acc = 0
+    for g, a in zip(weights, arrs):
+        acc = acc + g * a.astype(image.dtype)
+    return Image(np.asarray(acc, dtype=image.dtype), xmin=b.xmin, ymin=b.ymin, scale=image.scale)
+
 
 def _evaluate_batch(obj, waves):
     """Batched evaluateAtWavelength of a GSObject or ChromaticObject."""

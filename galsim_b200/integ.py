@@ -89,14 +89,13 @@ class ImageIntegrator(object):
     """integ.py:232-271, batched: see the module docstring."""
 
     def __call__(self, chromatic, bandpass, image, drawImageKwargs, doK=False):
-        from .chromatic import _integrate_images
-        if doK:
-            from .errors import GalSimNotImplementedError
-            raise GalSimNotImplementedError("chromatic drawKImage is not built")
+        from .chromatic import _integrate_images, _integrate_kimages
         waves = np.asarray(self.calculateWaves(bandpass), dtype=float)
         self.last_n_eval = len(waves)
         drawImageKwargs.pop('add_to_image', None)
         gs = self.rule.calculateWeights(waves, bandpass)
+        if doK:
+            return _integrate_kimages(chromatic, waves, gs, image, drawImageKwargs)
         return _integrate_images(chromatic, waves, gs, image, drawImageKwargs)
 
 

@@ -82,6 +82,17 @@ CASES = ['sep_moffat', 'sep_z_kolm_f8', 'atm_kolm', 'atm_kolm_trapz', 'atm_kolm_
 REFRACTION_WAVES = [350., 420.5, 500., 633., 800., 1000.]
 
 
+# drawKImage through a bandpass: (name, case of `case`, nx, scale = dk)
+KCASES = [('k_atm_kolm', 'atm_kolm', 25, 0.6), ('k_atm_bulge_disk', 'atm_bulge_disk', 21, 0.8),
+          ('k_shift_gal_psf', 'shift_gal_psf', 23, 0.7), ('k_sep_moffat', 'sep_moffat', 25, 0.6)]
+
+
+def drawk(galsim, kname):
+    _, name, n, dk = [k for k in KCASES if k[0] == kname][0]
+    obj, bp, kw = case(galsim, name)
+    return obj.drawKImage(bp, nx=n, ny=n, scale=dk)
+
+
 def draw(galsim, name):
     obj, bp, kw = case(galsim, name)
     kw = dict(kw)

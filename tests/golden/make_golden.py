@@ -829,6 +829,10 @@ def main_chromatic(ref_root):
         im = CC.draw(galsim, name)
         out['draw_' + name] = im.array
         out['draw_' + name + '_flux'] = np.array(getattr(im, 'added_flux', np.nan))
+    for kname, _, _, _ in CC.KCASES:
+        im = CC.drawk(galsim, kname)
+        out['kdraw_' + kname] = im.array
+        out['kdraw_' + kname + '_xmin'] = np.array([im.bounds.xmin, im.bounds.ymin])
     s1, s2 = CC.seds(galsim)
     b1, b2 = CC.bandpasses(galsim)
     out['effective_wavelength'] = np.array([b1.effective_wavelength, b2.effective_wavelength])

@@ -79,3 +79,14 @@ def test_chromatic_batch_matches_single_draws():
         im = galsim.Convolve(gal(hlr[i], g1[i]), psf).drawImage(b1, nx=32, ny=32, scale=0.2)
         a = st.array(i)
         assert np.abs(a - im.array).max() <= 1e-5 * np.abs(im.array).max(), i
+
+
+@pytest.mark.parametrize('kname', [k[0] for k in CC.KCASES])
+def test_chromatic_drawkimage_vs_reference(kname):
+    """ChromaticObject.drawKImage through a bandpass: the k-images at the integrator's
+    wavelengths drawn as one batch and summed with the rule's weights (FP64)."""
+    im = CC.drawk(galsim, kname)
+    ref = REF['kdraw_' + kname]
+    assert im.array.shape == ref.shape and im.array.dtype == ref.dtype
+    assert (im.bounds.xmin, im.bounds.ymin) == tuple(REF['kdraw_' + kname + '_xmin'])
+    assert np.abs(im.array - ref).max() <= 1e-9 * np.abs(ref).max(), (kname, np.abs(im.array - ref).max())
