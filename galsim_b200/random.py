@@ -5,19 +5,24 @@ Each deviate is a BaseDeviate stream (seed + raw 32-bit draws taken) with the di
 the reference on top, and the deviates themselves are drawn on the GPU by the noise kernels
 (galsim_b200/csrc/gsb_noise.cu, `gsb_add_noise` applied to a zero FP64 buffer): uniform_01 as
 one word / 2^32, the Box-Muller pairs of boost 1.48's normal_distribution, and its
-poisson_distribution (inversion below mean 10, PTRD above).  What the reference keeps inside a
+poisson_distribution (inversion below mean 10, PTRD above); the Weibull, Gamma and Chi-square
+deviates run their boost 1.48 algorithms on the host over the stream's words, read from the GPU
+in blocks and consumed in order.  What the reference keeps inside a
 deviate object between calls is kept here on the host: a GaussianDeviate's second Box-Muller
 value (the pair cache, used by the next call, cleared by generate and clearCache), and a
 PoissonDeviate's normal branch (means above 2^30 or 0) with its own pair cache.  Single draws
 are one small launch each; generate() fills an array in one launch.
 """
+import math
+
 import numpy as np
 
 from . import _lib
 from .errors import GalSimRangeError, GalSimValueError
 from .noise import BaseDeviate, NoiseParamsC, _apply, GAUSSIAN, POISSON, UNIFORM
 
-__all__ = ['UniformDeviate', 'GaussianDeviate', 'PoissonDeviate']
+__all__ = ['UniformDeviate', 'GaussianDeviate', 'PoissonDeviate', 'WeibullDeviate', 'GammaDeviate',
+           'Chi2Deviate']
 
 _MAX_POISSON = float(1 << 30)
 
@@ -228,3 +233,148 @@ class PoissonDeviate(BaseDeviate):
 
     def __repr__(self):
         return 'galsim.PoissonDeviate(seed=%r, mean=%r)' % (self._stream.seed, self._mean)
+
+
+class _Words(object):
+    """Sequential access to a stream's raw 32-bit words for the deviates drawn on the host (a
+    data-dependent number of words each): the words come from the GPU in blocks (the uniform
+    kind, word / 2^32), are consumed in order, and commit() moves the stream past the words
+    used."""
+
+    def __init__(self, stream, block=1024):
+        self.stream = stream
+        self.start = stream.used
+        self.block = block
+        self.buf = np.zeros(0)
+        self.pos = 0
+
+    def uniform01(self):
+        if self.pos == len(self.buf):
+            probe = type(self.stream).__new__(type(self.stream))
+            probe.seed, probe.used = self.stream.seed, self.start + self.pos
+            nxt = _draw(probe, UNIFORM, self.block)
+            self.buf = np.concatenate([self.buf, nxt])
+        u = float(self.buf[self.pos])
+        self.pos += 1
+        return u
+
+    def commit(self):
+        self.stream.used = self.start + self.pos
+
+
+def _host_generate(dev, array, add=False):
+    w = _Words(dev._stream, block=max(64, min(1 << 16, 2 * int(np.size(array)))))
+    vals = np.array([dev._sample(w) for _ in range(int(np.size(array)))], dtype=float)
+    w.commit()
+    _fill(array, vals, add=add)
+
+
+class WeibullDeviate(BaseDeviate):
+    """Weibull deviates of shape a and scale b (random.py:534-588): b (-ln(1 - u))^(1/a), one
+    uniform each (boost 1.48 weibull_distribution), in the host's FP64 math."""
+
+    def __init__(self, seed=None, a=1., b=1.):
+        BaseDeviate.__init__(self, seed)
+        self._a, self._b = float(a), float(b)
+
+    a = property(lambda self: self._a)
+    b = property(lambda self: self._b)
+
+    def _sample(self, w):
+        return self._b * math.pow(-math.log(1. - w.uniform01()), 1. / self._a)
+
+    def __call__(self):
+        w = _Words(self._stream, block=64)
+        v = self._sample(w)
+        w.commit()
+        return v
+
+    def generate(self, array):
+        _host_generate(self, array)
+
+    def add_generate(self, array):
+        _host_generate(self, array, add=True)
+
+    def clearCache(self):
+        pass
+
+    def __repr__(self):
+        return 'galsim.WeibullDeviate(seed=%r, a=%r, b=%r)' % (self._stream.seed, self._a, self._b)
+
+
+def _gamma_sample(w, alpha, beta):
+    """boost 1.48 gamma_distribution (alpha, beta): an exponential for alpha = 1, the tangent
+    rejection method for alpha > 1, and the exponential-mixture rejection for alpha < 1, each
+    uniform from the stream in order."""
+    if alpha == 1.:
+        return -math.log(1. - w.uniform01()) * beta
+    if alpha > 1.:
+        s = math.sqrt(2. * alpha - 1.)
+        while True:
+            y = math.tan(math.pi * w.uniform01())
+            x = s * y + alpha - 1.
+            if x <= 0.:
+                continue
+            if w.uniform01() > (1. + y * y) * math.exp((alpha - 1.) * math.log(x / (alpha - 1.)) - s * y):
+                continue
+            return x * beta
+    p = math.exp(1.) / (alpha + math.exp(1.))
+    while True:
+        u = w.uniform01()
+        y = -math.log(1. - w.uniform01())
+        if u < p:
+            x = math.exp(-y / alpha)
+            q = p * math.exp(-x)
+        else:
+            x = 1. + y
+            q = p + (1. - p) * math.pow(x, alpha - 1.)
+        if u >= q:
+            continue
+        return x * beta
+
+
+class GammaDeviate(BaseDeviate):
+    """Gamma deviates of shape k and scale theta (random.py:590-645, boost 1.48
+    gamma_distribution; a data-dependent number of uniforms each)."""
+
+    def __init__(self, seed=None, k=1., theta=1.):
+        BaseDeviate.__init__(self, seed)
+        self._k, self._theta = float(k), float(theta)
+
+    k = property(lambda self: self._k)
+    theta = property(lambda self: self._theta)
+    has_reliable_discard = property(lambda self: False)
+
+    def _sample(self, w):
+        return _gamma_sample(w, self._k, self._theta)
+
+    __call__ = WeibullDeviate.__call__
+    generate = WeibullDeviate.generate
+    add_generate = WeibullDeviate.add_generate
+    clearCache = WeibullDeviate.clearCache
+
+    def __repr__(self):
+        return 'galsim.GammaDeviate(seed=%r, k=%r, theta=%r)' % (self._stream.seed, self._k, self._theta)
+
+
+class Chi2Deviate(BaseDeviate):
+    """Chi-square deviates with n degrees of freedom (random.py:647-696): 2 Gamma(n / 2, 1)
+    (boost 1.48 chi_squared_distribution)."""
+
+    def __init__(self, seed=None, n=1.):
+        BaseDeviate.__init__(self, seed)
+        self._n = float(n)
+
+    n = property(lambda self: self._n)
+    has_reliable_discard = property(lambda self: False)
+
+    def _sample(self, w):
+        return 2. * _gamma_sample(w, self._n / 2., 1.)
+
+    __call__ = WeibullDeviate.__call__
+    generate = WeibullDeviate.generate
+    add_generate = WeibullDeviate.add_generate
+    clearCache = WeibullDeviate.clearCache
+
+    def __repr__(self):
+        return 'galsim.Chi2Deviate(seed=%r, n=%r)' % (self._stream.seed, self._n)

@@ -1921,6 +1921,40 @@ class OPoissonDeviate(object):
         return self.gd(self.rng) if self.use_gd else float(poisson_draw(self.mean, self.rng))
 
 
+def weibull_draw(rng, a, b):
+    """boost 1.48 weibull_distribution: b (-ln(1 - u))^(1/a)."""
+    return b * math.pow(-math.log(1. - uniform01(rng)), 1. / a)
+
+
+def gamma_draw(rng, alpha, beta):
+    """boost 1.48 gamma_distribution: exponential (alpha = 1), tangent rejection (alpha > 1),
+    exponential-mixture rejection (alpha < 1)."""
+    if alpha == 1.:
+        return -math.log(1. - uniform01(rng)) * beta
+    if alpha > 1.:
+        while True:
+            y = math.tan(PI * uniform01(rng))
+            x = math.sqrt(2. * alpha - 1.) * y + alpha - 1.
+            if x <= 0.:
+                continue
+            if uniform01(rng) > (1. + y * y) * math.exp((alpha - 1.) * math.log(x / (alpha - 1.))
+                                                          - math.sqrt(2. * alpha - 1.) * y):
+                continue
+            return x * beta
+    p = math.exp(1.) / (alpha + math.exp(1.))
+    while True:
+        u = uniform01(rng)
+        y = -math.log(1. - uniform01(rng))
+        if u < p:
+            x = math.exp(-y / alpha)
+            q = p * math.exp(-x)
+        else:
+            x = 1. + y
+            q = p + (1. - p) * math.pow(x, alpha - 1.)
+        if u < q:
+            return x * beta
+
+
 def gaussian_noise(image, rng, sigma):
     """GaussianNoise._applyTo (noise.py:259-263): N(0, sigma) per pixel in row-major order,
     cast to the image dtype and added."""

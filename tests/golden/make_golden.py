@@ -444,6 +444,22 @@ def deviate_sequences(galsim):
     e = np.array([0., 3.2, 50., 0., float(2 ** 31), 7.])
     pd.generate_from_expectation(e)
     out['poisson'] = np.concatenate([a, g, b, g2, c, d, g3, e, [pd()]])
+    # the host-drawn deviates: Weibull, Gamma with k < 1, = 1 and > 1, Chi-square
+    wd = galsim.WeibullDeviate(2468, a=1.7, b=2.2)
+    g = np.empty(6)
+    wd.generate(g)
+    out['weibull'] = np.concatenate([[wd(), wd()], g, [wd()]])
+    vals = []
+    for k, th in ((0.6, 1.3), (1., 2.), (3.5, 0.7)):
+        gm = galsim.GammaDeviate(1357 + int(10 * k), k=k, theta=th)
+        g = np.empty(7)
+        gm.generate(g)
+        vals.append(np.concatenate([[gm(), gm()], g, [gm()]]))
+    out['gamma'] = np.concatenate(vals)
+    cd = galsim.Chi2Deviate(9753, n=5.)
+    g = np.empty(5)
+    cd.generate(g)
+    out['chi2'] = np.concatenate([[cd(), cd()], g, [cd()]])
     # one stream shared: a uniform, then Gaussian values, then uniforms again
     s = galsim.UniformDeviate(4567)
     sg = galsim.GaussianDeviate(s, sigma=3.)

@@ -145,3 +145,22 @@ def test_deviate_noise_matches_reference():
         imi += gen(18).reshape(3, 6).astype(np.int32)
         assert np.array_equal(im, GOLD['dev_devnoise_' + name])
         assert np.array_equal(imi, GOLD['dev_devnoise_i_' + name])
+
+
+def test_host_deviates_match_reference():
+    """Weibull, Gamma (k < 1, = 1, > 1) and Chi-square draws (boost 1.48 algorithms over the
+    stream's uniforms) against the reference's sequences.  The fixture script generates an
+    array first and then makes single calls, listing the first two calls before the array."""
+    def order(f, ng):
+        g = [f() for _ in range(ng)]
+        c = [f() for _ in range(3)]
+        return c[:2] + g + c[2:]
+    r = O.base_deviate(2468)
+    assert np.array_equal(order(lambda: O.weibull_draw(r, 1.7, 2.2), 6), GOLD['dev_weibull'])
+    vals = []
+    for k, th in ((0.6, 1.3), (1., 2.), (3.5, 0.7)):
+        r = O.base_deviate(1357 + int(10 * k))
+        vals += order(lambda: O.gamma_draw(r, k, th), 7)
+    assert np.array_equal(vals, GOLD['dev_gamma'])
+    r = O.base_deviate(9753)
+    assert np.array_equal(order(lambda: 2. * O.gamma_draw(r, 2.5, 1.), 5), GOLD['dev_chi2'])
