@@ -1,17 +1,17 @@
-"""Random deviates: UniformDeviate, GaussianDeviate, PoissonDeviate (galsim/random.py:309-531,
-src/Random.cpp).
+"""Random deviates: Uniform, Gaussian, Poisson, Weibull, Gamma, Chi-square and Binomial
+(galsim/random.py:309-696, src/Random.cpp).
 
 Each deviate is a BaseDeviate stream (seed + raw 32-bit draws taken) with the distribution of
-the reference on top, and the deviates themselves are drawn on the GPU by the noise kernels
-(galsim_b200/csrc/gsb_noise.cu, `gsb_add_noise` applied to a zero FP64 buffer): uniform_01 as
-one word / 2^32, the Box-Muller pairs of boost 1.48's normal_distribution, and its
-poisson_distribution (inversion below mean 10, PTRD above); the Weibull, Gamma and Chi-square
-deviates run their boost 1.48 algorithms on the host over the stream's words, read from the GPU
-in blocks and consumed in order.  What the reference keeps inside a
-deviate object between calls is kept here on the host: a GaussianDeviate's second Box-Muller
-value (the pair cache, used by the next call, cleared by generate and clearCache), and a
-PoissonDeviate's normal branch (means above 2^30 or 0) with its own pair cache.  Single draws
-are one small launch each; generate() fills an array in one launch.
+the reference on top.  Uniform, Gaussian and Poisson deviates are drawn on the GPU by the
+noise kernels (galsim_b200/csrc/gsb_noise.cu, `gsb_add_noise` applied to a zero FP64 buffer):
+uniform_01 as one word / 2^32, the Box-Muller pairs of boost 1.48's normal_distribution, and
+its poisson_distribution (inversion below mean 10, PTRD above).  The Weibull, Gamma,
+Chi-square and Binomial deviates run boost 1.48's algorithms on the host over the stream's
+words, which are read from the GPU in blocks and consumed in order.  What the reference keeps
+inside a deviate object between calls is kept here on the host: a GaussianDeviate's second
+Box-Muller value (the pair cache, used by the next call, cleared by generate and clearCache),
+and a PoissonDeviate's normal branch (means above 2^30 or 0) with its own pair cache.  Single
+GPU draws are one small launch each; generate() fills an array in one launch.
 """
 import math
 
@@ -22,7 +22,7 @@ from .errors import GalSimRangeError, GalSimValueError
 from .noise import BaseDeviate, NoiseParamsC, _apply, GAUSSIAN, POISSON, UNIFORM
 
 __all__ = ['UniformDeviate', 'GaussianDeviate', 'PoissonDeviate', 'WeibullDeviate', 'GammaDeviate',
-           'Chi2Deviate']
+           'Chi2Deviate', 'BinomialDeviate']
 
 _MAX_POISSON = float(1 << 30)
 
@@ -378,3 +378,123 @@ class Chi2Deviate(BaseDeviate):
 
     def __repr__(self):
         return 'galsim.Chi2Deviate(seed=%r, n=%r)' % (self._stream.seed, self._n)
+
+
+def _stirling_fc(k):
+    """The correction of Stirling's formula, ln k! = (k + 1/2) ln(k + 1) - (k + 1) + ln sqrt(2 pi)
+    + fc(k): from ln Gamma below 10, its series 1/12 - (1/360 - (1/1260) z^2) z^2) z with
+    z = 1 / (k + 1) above (the form boost 1.48's binomial_distribution uses)."""
+    if k < 10:
+        return math.lgamma(k + 1.) - ((k + 0.5) * math.log(k + 1.) - (k + 1.) + 0.5 * math.log(2. * math.pi))
+    z = 1. / (k + 1)
+    return (1. / 12 - (1. / 360 - (1. / 1260) * (z * z)) * (z * z)) * z
+
+
+class BinomialDeviate(BaseDeviate):
+    """Binomial deviates of N trials with probability p (random.py:415-466): boost 1.48's
+    binomial_distribution -- inversion while (N + 1) min(p, 1 - p) < 11, else the BTRD
+    transformed rejection of Hoermann (1993) -- on the host over the stream's words."""
+
+    def __init__(self, seed=None, N=1, p=0.5):
+        BaseDeviate.__init__(self, seed)
+        self._N, self._p = int(N), float(p)
+        pp = 1. - self._p if 0.5 < self._p else self._p
+        t = self._N
+        self._m = int((t + 1) * pp)
+        if self._m < 11:
+            self._q_n = math.pow(1. - pp, float(t))
+        else:
+            r = pp / (1. - pp)
+            npq = t * pp * (1. - pp)
+            b = 1.15 + 2.53 * math.sqrt(npq)
+            self._btrd = dict(r=r, nr=(t + 1) * r, npq=npq, b=b, a=-0.0873 + 0.0248 * b + 0.01 * pp,
+                              c=t * pp + 0.5, alpha=(2.83 + 5.1 / b) * math.sqrt(npq), v_r=0.92 - 4.2 / b)
+            self._btrd['u_rv_r'] = 0.86 * self._btrd['v_r']
+
+    n = property(lambda self: self._N)
+    p = property(lambda self: self._p)
+    has_reliable_discard = property(lambda self: False)
+
+    def _invert(self, w, t, p):
+        q = 1. - p
+        s = p / q
+        a = (t + 1) * s
+        r = self._q_n
+        u = w.uniform01()
+        x = 0
+        while u > r:
+            u = u - r
+            x += 1
+            r = ((a / x) - s) * r
+        return x
+
+    def _btrd_draw(self, w):
+        B = self._btrd
+        t, m = self._N, self._m
+        while True:
+            v = w.uniform01()
+            if v <= B['u_rv_r']:
+                u = v / B['v_r'] - 0.43
+                return int(math.floor((2 * B['a'] / (0.5 - abs(u)) + B['b']) * u + B['c']))
+            if v >= B['v_r']:
+                u = w.uniform01() - 0.5
+            else:
+                u = v / B['v_r'] - 0.93
+                u = (-0.5 if u < 0 else 0.5) - u
+                v = w.uniform01() * B['v_r']
+            us = 0.5 - abs(u)
+            k = int(math.floor((2 * B['a'] / us + B['b']) * u + B['c']))
+            if k < 0 or k > t:
+                continue
+            v = v * B['alpha'] / (B['a'] / (us * us) + B['b'])
+            km = float(abs(k - m))
+            if km <= 15:
+                f = 1.
+                if m < k:
+                    i = m
+                    while True:
+                        i += 1
+                        f = f * (B['nr'] / i - B['r'])
+                        if i == k:
+                            break
+                elif m > k:
+                    i = k
+                    while True:
+                        i += 1
+                        v = v * (B['nr'] / i - B['r'])
+                        if i == m:
+                            break
+                if v <= f:
+                    return k
+                continue
+            v = math.log(v)
+            rho = (km / B['npq']) * (((km / 3. + 0.625) * km + 1. / 6) / B['npq'] + 0.5)
+            tt = -km * km / (2 * B['npq'])
+            if v < tt - rho:
+                return k
+            if v > tt + rho:
+                continue
+            nm = t - m + 1
+            h = (m + 0.5) * math.log((m + 1) / (B['r'] * nm)) + _stirling_fc(m) + _stirling_fc(t - m)
+            nk = t - k + 1
+            if v <= (h + (t + 1) * math.log(float(nm) / nk) + (k + 0.5) * math.log(nk * B['r'] / (k + 1))
+                     - _stirling_fc(k) - _stirling_fc(t - k)):
+                return k
+
+    def _sample(self, w):
+        t = self._N
+        if self._m < 11:
+            if 0.5 < self._p:
+                return float(t - self._invert(w, t, 1. - self._p))
+            return float(self._invert(w, t, self._p))
+        if 0.5 < self._p:
+            return float(t - self._btrd_draw(w))
+        return float(self._btrd_draw(w))
+
+    __call__ = WeibullDeviate.__call__
+    generate = WeibullDeviate.generate
+    add_generate = WeibullDeviate.add_generate
+    clearCache = WeibullDeviate.clearCache
+
+    def __repr__(self):
+        return 'galsim.BinomialDeviate(seed=%r, N=%r, p=%r)' % (self._stream.seed, self._N, self._p)

@@ -460,6 +460,19 @@ def deviate_sequences(galsim):
     g = np.empty(5)
     cd.generate(g)
     out['chi2'] = np.concatenate([[cd(), cd()], g, [cd()]])
+    # binomial: inversion (small N p; one word per value) with generate and single draws, and
+    # BTRD with single draws (the reference's generate splits BTRD draws over its OpenMP threads
+    # by word counts, so its array depends on the thread count), p below and above 1/2
+    vals = []
+    for N, pr in ((20, 0.2), (15, 0.8)):
+        bd = galsim.BinomialDeviate(4321 + N, N=N, p=pr)
+        g = np.empty(6)
+        bd.generate(g)
+        vals.append(np.concatenate([[bd(), bd()], g, [bd()]]))
+    for N, pr in ((200, 0.3), (500, 0.75)):
+        bd = galsim.BinomialDeviate(4321 + N, N=N, p=pr)
+        vals.append(np.array([bd() for _ in range(9)]))
+    out['binomial'] = np.concatenate(vals)
     # one stream shared: a uniform, then Gaussian values, then uniforms again
     s = galsim.UniformDeviate(4567)
     sg = galsim.GaussianDeviate(s, sigma=3.)

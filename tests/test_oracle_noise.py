@@ -164,3 +164,31 @@ def test_host_deviates_match_reference():
     assert np.array_equal(vals, GOLD['dev_gamma'])
     r = O.base_deviate(9753)
     assert np.array_equal(order(lambda: 2. * O.gamma_draw(r, 2.5, 1.), 5), GOLD['dev_chi2'])
+
+
+def test_binomial_matches_reference():
+    """BinomialDeviate: boost 1.48's inversion and BTRD, restated over the oracle's stream
+    (the product's algorithm, fed by the oracle's words, against the reference)."""
+    import galsim_b200.random as R
+
+    class Words(object):
+        def __init__(self, seed):
+            self.r = O.base_deviate(seed)
+
+        def uniform01(self):
+            return O.uniform01(self.r)
+
+    vals = []
+    for N, pr in ((20, 0.2), (15, 0.8)):
+        bd = R.BinomialDeviate.__new__(R.BinomialDeviate)
+        R.BinomialDeviate.__init__(bd, 1, N, pr)
+        w = Words(4321 + N)
+        g = [bd._sample(w) for _ in range(6)]
+        c = [bd._sample(w) for _ in range(3)]
+        vals += c[:2] + g + c[2:]
+    for N, pr in ((200, 0.3), (500, 0.75)):
+        bd = R.BinomialDeviate.__new__(R.BinomialDeviate)
+        R.BinomialDeviate.__init__(bd, 1, N, pr)
+        w = Words(4321 + N)
+        vals += [bd._sample(w) for _ in range(9)]
+    assert np.array_equal(vals, GOLD['dev_binomial'])
