@@ -162,6 +162,8 @@ int gsb_tables_destroy(gsb_tables* t)
     cudaFree(t->d_dheader);
     cudaFree(t->d_dnode);
     cudaFree(t->d_dval);
+    if (t->sersic_exec) cudaGraphExecDestroy(t->sersic_exec);
+    if (t->capture_stream) cudaStreamDestroy(t->capture_stream);
     cudaFree(t->d_mheader);
     cudaFree(t->d_mnode);
     cudaFree(t->d_mval);

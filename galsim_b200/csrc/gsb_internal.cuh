@@ -228,6 +228,10 @@ struct gsb_tables {
     double4* d_dnode = nullptr;   // count * stride
     double* d_dval = nullptr;     // scratch: count * stride d/dn Hankel values
     size_t cap_dn_slots = 0, cap_dn_nodes = 0;
+    // the device part of the last Sersic build as a CUDA graph, and what it was captured for
+    cudaGraphExec_t sersic_exec = nullptr;
+    unsigned char sersic_key[256] = {};
+    cudaStream_t capture_stream = nullptr;
     // truncated Moffat slots (gsb_moffat_tables_build)
     int moffat_count = 0;
     int moffat_stride = 0;            // nodes per slot

@@ -10,6 +10,7 @@
 //   kolmogorov_* KolmogorovInfo stepk (src/SBKolmogorov.cpp:338-420).
 //   prepare_*    per-leaf derived constants and stepk / maxk.
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "gsb_internal.cuh"
@@ -1329,51 +1330,98 @@ int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc,
         d_trunc = t->d_trunc;
         GSB_CUDA_CHECK(cudaMemcpyAsync(d_trunc, h_trunc, sizeof(double) * count, cudaMemcpyHostToDevice, stream));
     }
-    // d_status[0]: convergence status; d_status[1 + r]: some table still needs nodes after round r
-    GSB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int) * (1 + kMaxRounds), stream));
-    sersic_setup_kernel<<<(count + 127) / 128, 128, 0, stream>>>(d_n, d_trunc, count, *gsp, t->d_header, stride,
-                                                                 dheader);
-    GSB_CUDA_CHECK(cudaGetLastError());
-    sersic_scan_init_kernel<<<(count + 127) / 128, 128, 0, stream>>>(t->d_header, count, static_cast<SersicScan*>(t->d_scan));
-    GSB_CUDA_CHECK(cudaGetLastError());
-    // Rounds of kRound ln k nodes: integrate, then advance each table's stopping scan.
-    constexpr int kRound = 32;
-    const int threads = 256;
-    if ((stride + kRound - 1) / kRound > kMaxRounds) return set_error(GSB_ERR_UNSUPPORTED, "Sersic table too long");
-    for (int i0 = 0, r = 0; i0 < stride; i0 += kRound, ++r) {
-        const int* prev_live = r > 0 ? d_status + r : nullptr;
-        const long long nwarps = (long long)count * ((kRound + 1) / 2);
-        const long long blocks = (nwarps * 32 + threads - 1) / threads;
-        if (with_dn)
-            sersic_nodes_pair_kernel<true><<<(unsigned)blocks, threads, 0, stream>>>(
-                t->d_header, count, i0, kRound, *gsp, st->og, static_cast<const SersicScan*>(t->d_scan),
-                t->d_val, stride, prev_live, d_status, dheader, dval);
-        else
-            sersic_nodes_pair_kernel<false><<<(unsigned)blocks, threads, 0, stream>>>(
-                t->d_header, count, i0, kRound, *gsp, st->og, static_cast<const SersicScan*>(t->d_scan),
-                t->d_val, stride, prev_live, d_status, nullptr, nullptr);
-        GSB_CUDA_CHECK(cudaGetLastError());
-        if (has_trunc) {
-            const long long tw = (long long)count * kRound;
-            sersic_trunc_nodes_kernel<<<(unsigned)((tw * 32 + threads - 1) / threads), threads, 0, stream>>>(
-                t->d_header, count, i0, kRound, st->og, static_cast<const SersicScan*>(t->d_scan), t->d_val, stride,
-                prev_live, d_status);
-            GSB_CUDA_CHECK(cudaGetLastError());
-        }
-        sersic_scan_kernel<<<(count + 63) / 64, 64, 0, stream>>>(t->d_header, count, stride, i0, kRound,
-                                                                 *gsp, t->d_val, t->d_node, static_cast<SersicScan*>(t->d_scan),
-                                                                 dval, dnode, prev_live, d_status + 1 + r);
-        GSB_CUDA_CHECK(cudaGetLastError());
-    }
+    constexpr int kRoundsNodes = 32;
+    if ((stride + kRoundsNodes - 1) / kRoundsNodes > kMaxRounds) return set_error(GSB_ERR_UNSUPPORTED, "Sersic table too long");
     const size_t fsm = sizeof(double) * 4 * (size_t)stride;
+    if (fsm > 227 * 1024) return set_error(GSB_ERR_UNSUPPORTED, "Sersic table too long");
     if (fsm > 48 * 1024)
         GSB_CUDA_CHECK(cudaFuncSetAttribute(sersic_finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             int(std::min<size_t>(fsm, 227 * 1024))));
-    if (fsm > 227 * 1024) return set_error(GSB_ERR_UNSUPPORTED, "Sersic table too long");
-    sersic_finalize_kernel<<<count, 32, fsm, stream>>>(t->d_header, count, stride, *gsp,
-                                                        static_cast<const SersicScan*>(t->d_scan), t->d_node,
-                                                        dnode, dheader);
-    GSB_CUDA_CHECK(cudaGetLastError());
+    // the device part of the build: set-up, the rounds of nodes and their stopping scans, the
+    // finalisation (no host synchronisation inside)
+    auto enqueue = [&](cudaStream_t stream) -> int {
+        // d_status[0]: convergence status; d_status[1 + r]: some table still needs nodes after round r
+        GSB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int) * (1 + kMaxRounds), stream));
+        sersic_setup_kernel<<<(count + 127) / 128, 128, 0, stream>>>(d_n, d_trunc, count, *gsp, t->d_header, stride,
+                                                                     dheader);
+        GSB_CUDA_CHECK(cudaGetLastError());
+        sersic_scan_init_kernel<<<(count + 127) / 128, 128, 0, stream>>>(t->d_header, count, static_cast<SersicScan*>(t->d_scan));
+        GSB_CUDA_CHECK(cudaGetLastError());
+        // Rounds of kRound ln k nodes: integrate, then advance each table's stopping scan.
+        constexpr int kRound = 32;
+        const int threads = 256;
+        for (int i0 = 0, r = 0; i0 < stride; i0 += kRound, ++r) {
+            const int* prev_live = r > 0 ? d_status + r : nullptr;
+            const long long nwarps = (long long)count * ((kRound + 1) / 2);
+            const long long blocks = (nwarps * 32 + threads - 1) / threads;
+            if (with_dn)
+                sersic_nodes_pair_kernel<true><<<(unsigned)blocks, threads, 0, stream>>>(
+                    t->d_header, count, i0, kRound, *gsp, st->og, static_cast<const SersicScan*>(t->d_scan),
+                    t->d_val, stride, prev_live, d_status, dheader, dval);
+            else
+                sersic_nodes_pair_kernel<false><<<(unsigned)blocks, threads, 0, stream>>>(
+                    t->d_header, count, i0, kRound, *gsp, st->og, static_cast<const SersicScan*>(t->d_scan),
+                    t->d_val, stride, prev_live, d_status, nullptr, nullptr);
+            GSB_CUDA_CHECK(cudaGetLastError());
+            if (has_trunc) {
+                const long long tw = (long long)count * kRound;
+                sersic_trunc_nodes_kernel<<<(unsigned)((tw * 32 + threads - 1) / threads), threads, 0, stream>>>(
+                    t->d_header, count, i0, kRound, st->og, static_cast<const SersicScan*>(t->d_scan), t->d_val, stride,
+                    prev_live, d_status);
+                GSB_CUDA_CHECK(cudaGetLastError());
+            }
+            sersic_scan_kernel<<<(count + 63) / 64, 64, 0, stream>>>(t->d_header, count, stride, i0, kRound,
+                                                                     *gsp, t->d_val, t->d_node, static_cast<SersicScan*>(t->d_scan),
+                                                                     dval, dnode, prev_live, d_status + 1 + r);
+            GSB_CUDA_CHECK(cudaGetLastError());
+        }
+        sersic_finalize_kernel<<<count, 32, fsm, stream>>>(t->d_header, count, stride, *gsp,
+                                                            static_cast<const SersicScan*>(t->d_scan), t->d_node,
+                                                            dnode, dheader);
+        GSB_CUDA_CHECK(cudaGetLastError());
+        return GSB_OK;
+    };
+    // The launches are captured once as a CUDA graph and replayed while the build's shape is
+    // unchanged (table count, node stride, flags, GSParams and buffers: the captured launches
+    // hold them); the captured early-exit rounds then cost a graph node each instead of a launch.
+    struct Key {
+        int count, stride, with_dn, has_trunc;
+        gsb_gsparams gsp;
+        const void* ptr[12];
+    } key;
+    std::memset(&key, 0, sizeof(key));
+    key.count = count;
+    key.stride = stride;
+    key.with_dn = with_dn;
+    key.has_trunc = has_trunc;
+    key.gsp = *gsp;
+    const void* ptrs[12] = {t->d_header, t->d_node, t->d_val, t->d_scan, d_n, d_status, d_trunc, dheader,
+                            dnode, dval, st->og.xw, st->og.root};
+    for (int k = 0; k < 12; ++k) key.ptr[k] = ptrs[k];
+    static_assert(sizeof(Key) <= sizeof(t->sersic_key), "graph key too large");
+    if (!(t->sersic_exec && std::memcmp(t->sersic_key, &key, sizeof(key)) == 0)) {
+        if (t->sersic_exec) { cudaGraphExecDestroy(t->sersic_exec); t->sersic_exec = nullptr; }
+        // captured on a private stream (the caller's may be the legacy default stream, which
+        // cannot be captured); capturing runs nothing
+        if (!t->capture_stream) GSB_CUDA_CHECK(cudaStreamCreateWithFlags(&t->capture_stream, cudaStreamNonBlocking));
+        GSB_CUDA_CHECK(cudaStreamBeginCapture(t->capture_stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue(t->capture_stream);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(t->capture_stream, &graph);
+        if (rc || ce != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            return rc ? rc : set_error(GSB_ERR_CUDA, std::string("table-build capture: ") + cudaGetErrorString(ce));
+        }
+        const cudaError_t ie = cudaGraphInstantiate(&t->sersic_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) {
+            t->sersic_exec = nullptr;
+            return set_error(GSB_ERR_CUDA, std::string("table-build graph: ") + cudaGetErrorString(ie));
+        }
+        std::memcpy(t->sersic_key, &key, sizeof(key));
+    }
+    GSB_CUDA_CHECK(cudaGraphLaunch(t->sersic_exec, stream));
     int h_status = 0;
     GSB_CUDA_CHECK(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
     GSB_CUDA_CHECK(cudaStreamSynchronize(stream));
