@@ -27,7 +27,7 @@ from .interpolant import (Interpolant, Delta, Nearest, SincInterpolant, Linear, 
                           Lanczos, convert_interpolant)
 from .interpolatedimage import InterpolatedImage
 from .noise import BaseDeviate, BaseNoise, GaussianNoise, PoissonNoise, CCDNoise, VariableGaussianNoise, DeviateNoise
-from .random import UniformDeviate, GaussianDeviate, PoissonDeviate, WeibullDeviate, GammaDeviate, Chi2Deviate, BinomialDeviate
+from .random import UniformDeviate, GaussianDeviate, PoissonDeviate, WeibullDeviate, GammaDeviate, Chi2Deviate, BinomialDeviate, DistDeviate
 from . import fits
 from .fits import FitsHeader
 from .compound import Convolve, Convolution, Add, Sum, Transform, Transformation, _Transform

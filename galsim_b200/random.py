@@ -22,7 +22,7 @@ from .errors import GalSimRangeError, GalSimValueError
 from .noise import BaseDeviate, NoiseParamsC, _apply, GAUSSIAN, POISSON, UNIFORM
 
 __all__ = ['UniformDeviate', 'GaussianDeviate', 'PoissonDeviate', 'WeibullDeviate', 'GammaDeviate',
-           'Chi2Deviate', 'BinomialDeviate']
+           'Chi2Deviate', 'BinomialDeviate', 'DistDeviate']
 
 _MAX_POISSON = float(1 << 30)
 
@@ -498,3 +498,65 @@ class BinomialDeviate(BaseDeviate):
 
     def __repr__(self):
         return 'galsim.BinomialDeviate(seed=%r, N=%r, p=%r)' % (self._stream.seed, self._N, self._p)
+
+
+class DistDeviate(BaseDeviate):
+    """Deviates drawn from a tabulated probability density (random.py:698-930): the density's
+    LookupTable gives a CDF by the trapezoid rule on its abscissae, inverted by a linear
+    LookupTable of (CDF, x); each draw is one uniform from the stream (on the GPU) mapped through
+    it.  Densities given as Python callables, expressions or files need the reference's adaptive
+    Gauss-Kronrod integrator over npoints intervals and are not built."""
+
+    def __init__(self, seed=None, function=None, x_min=None, x_max=None, interpolant=None, npoints=None,
+                 clip_neg=False):
+        from .table import LookupTable
+        from .errors import GalSimIncompatibleValuesError, GalSimNotImplementedError
+        BaseDeviate.__init__(self, seed)
+        if function is None:
+            raise TypeError('You must pass a function to DistDeviate!')
+        if isinstance(function, str) or not isinstance(function, LookupTable) or npoints is not None:
+            if not isinstance(function, str) and not hasattr(function, '__call__'):
+                raise TypeError('function must be a callable function or a string')
+            raise GalSimNotImplementedError("DistDeviate from a callable, an expression or a file (the "
+                                            "adaptive integration of the density) is not built")
+        if interpolant:
+            raise GalSimIncompatibleValuesError(
+                "Cannot provide an interpolant with a callable function argument",
+                interpolant=interpolant, function=function)
+        if (x_min not in (None, function.x_min)) or (x_max not in (None, function.x_max)):
+            raise GalSimIncompatibleValuesError(
+                "Cannot provide x_min or x_max with a LookupTable function",
+                function=function, x_min=x_min, x_max=x_max)
+        xarray = np.array(function.x, dtype=float)
+        pdf = np.array(function.f, dtype=float)
+        pdf[1:] = pdf[1:] + pdf[:-1]
+        pdf[1:] *= np.diff(xarray)
+        pdf[0] = 0.
+        if clip_neg:
+            pdf[~(pdf >= 0)] = 0.
+        elif not np.all(pdf >= 0.):
+            raise GalSimValueError('Negative probability found in DistDeviate.', function)
+        cdf = np.cumsum(pdf)
+        cdf /= cdf[-1]
+        self._function = function
+        self._inverse_cdf = LookupTable(cdf, xarray, interpolant='linear')
+        self.x_min = function.x_min
+        self.x_max = function.x_max
+
+    def val(self, p):
+        if p < 0 or p > 1:
+            raise GalSimRangeError('Invalid cumulative probability for DistDeviate', p, 0., 1.)
+        return self._inverse_cdf(p)
+
+    def __call__(self):
+        return self._inverse_cdf(float(_draw(self._stream, UNIFORM, 1)[0]))
+
+    def generate(self, array):
+        p = _draw(self._stream, UNIFORM, int(np.size(array)))
+        np.copyto(array, np.asarray(self._inverse_cdf(p)).reshape(np.shape(array)))
+
+    def clearCache(self):
+        pass
+
+    def __repr__(self):
+        return 'galsim.DistDeviate(seed=%r, function=%r)' % (self._stream.seed, self._function)

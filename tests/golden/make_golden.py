@@ -473,6 +473,12 @@ def deviate_sequences(galsim):
         bd = galsim.BinomialDeviate(4321 + N, N=N, p=pr)
         vals.append(np.array([bd() for _ in range(9)]))
     out['binomial'] = np.concatenate(vals)
+    # DistDeviate from a tabulated density (trapezoid CDF, linear inverse)
+    tab = galsim.LookupTable([0.5, 1., 1.7, 2.5, 4., 6.], [0.2, 1.5, 2.2, 1.1, 0.4, 0.05], interpolant='linear')
+    dd = galsim.DistDeviate(8642, function=tab)
+    g = np.empty(7)
+    dd.generate(g)
+    out['dist'] = np.concatenate([[dd(), dd()], g, [dd(), dd.val(0.37)]])
     # one stream shared: a uniform, then Gaussian values, then uniforms again
     s = galsim.UniformDeviate(4567)
     sg = galsim.GaussianDeviate(s, sigma=3.)

@@ -143,7 +143,7 @@ def test_deviates_vs_reference():
         assert v.shape == ref.shape, k
         if k.startswith('devnoise'):
             assert_close(v, ref)
-        elif k in ('gaussian', 'shared'):
+        elif k in ('gaussian', 'shared', 'dist'):
             assert np.allclose(v, ref, rtol=1e-13, atol=1e-13), (k, np.abs(v - ref).max())
         else:
             assert np.array_equal(v, ref), (k, v, ref)

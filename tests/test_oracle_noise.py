@@ -192,3 +192,18 @@ def test_binomial_matches_reference():
         w = Words(4321 + N)
         vals += [bd._sample(w) for _ in range(9)]
     assert np.array_equal(vals, GOLD['dev_binomial'])
+
+
+def test_dist_deviate_matches_reference():
+    """DistDeviate from a tabulated density: the inverse CDF (trapezoid rule, linear inverse
+    table) of the stream's uniforms against the reference's draws (host only)."""
+    import galsim_b200 as galsim
+    tab = galsim.LookupTable([0.5, 1., 1.7, 2.5, 4., 6.], [0.2, 1.5, 2.2, 1.1, 0.4, 0.05], interpolant='linear')
+    dd = galsim.DistDeviate(1, function=tab)
+    r = O.base_deviate(8642)
+    u = [O.uniform01(r) for _ in range(10)]
+    order = u[7:9] + u[:7] + u[9:]
+    mine = [dd.val(p) for p in order] + [dd.val(0.37)]
+    assert np.allclose(mine, GOLD['dev_dist'], rtol=1e-14, atol=0)
+    with pytest.raises(galsim.GalSimNotImplementedError):
+        galsim.DistDeviate(1, function=lambda x: x, x_min=0., x_max=1.)
