@@ -22,6 +22,9 @@ namespace {
 
 constexpr int kLevMin = 5;
 constexpr int kMaxRounds = 128;      // rounds of ln k nodes per table build (status flags)
+// ln k nodes per table and round: a table's nodes past its stopping point are integrated only
+// up to the end of the round in which its scan stops (even: the nodes go in pairs)
+constexpr int kTableRound = 64;
 constexpr int kLevMax = 20;
 constexpr long long kNroot = 1000000;
 
@@ -1330,8 +1333,7 @@ int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc,
         d_trunc = t->d_trunc;
         GSB_CUDA_CHECK(cudaMemcpyAsync(d_trunc, h_trunc, sizeof(double) * count, cudaMemcpyHostToDevice, stream));
     }
-    constexpr int kRoundsNodes = 32;
-    if ((stride + kRoundsNodes - 1) / kRoundsNodes > kMaxRounds) return set_error(GSB_ERR_UNSUPPORTED, "Sersic table too long");
+    if ((stride + kTableRound - 1) / kTableRound > kMaxRounds) return set_error(GSB_ERR_UNSUPPORTED, "Sersic table too long");
     const size_t fsm = sizeof(double) * 4 * (size_t)stride;
     if (fsm > 227 * 1024) return set_error(GSB_ERR_UNSUPPORTED, "Sersic table too long");
     if (fsm > 48 * 1024)
@@ -1348,7 +1350,7 @@ int sersic_tables_build(gsb_tables* t, const double* h_n, const double* h_trunc,
         sersic_scan_init_kernel<<<(count + 127) / 128, 128, 0, stream>>>(t->d_header, count, static_cast<SersicScan*>(t->d_scan));
         GSB_CUDA_CHECK(cudaGetLastError());
         // Rounds of kRound ln k nodes: integrate, then advance each table's stopping scan.
-        constexpr int kRound = 32;
+        constexpr int kRound = kTableRound;
         const int threads = 256;
         for (int i0 = 0, r = 0; i0 < stride; i0 += kRound, ++r) {
             const int* prev_live = r > 0 ? d_status + r : nullptr;
