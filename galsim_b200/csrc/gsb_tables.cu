@@ -93,7 +93,7 @@ __device__ inline double warp_total(double v)
 // Running-sum estimate refresh: every chunk for the first kEagerChunks chunks (short sums stop
 // there), then every kLazyChunks chunks.
 constexpr int kEagerChunks = 2;
-constexpr int kLazyChunks = 8;
+constexpr int kLazyChunks = 16;
 
 // Sum_i w_i f(x_i / k) / k^2 for h = 2^-lev with the reference's stopping rule: stop at the
 // first term whose magnitude is below 1e-15 |running sum| (Hankel.cpp:117-141).  The integrand
