@@ -568,14 +568,15 @@ TABLES_ISSUE_ACTIVE = 0.747
 
 def table_build_launches(n_values, gsp_kvalue_accuracy=1e-5, table_spacing=1.):
     """Kernel launches of one Sersic table build (gsb_sersic_tables_build): setup, scan init,
-    one (nodes, scan) pair per round of 32 ln k nodes over the table stride, and the finalize.
+    one (nodes, scan) pair per round of 64 ln k nodes over the table stride (kTableRound in
+    csrc/gsb_tables.cu), and the finalize.
     The stride is the node count of the largest n (sersic_stride in csrc/gsb_tables.cu)."""
     nmax = float(np.max(n_values))
     kderiv6 = math.exp(math.lgamma(8. * nmax) - math.lgamma(2. * nmax)) / 2304.
     kmin = (gsp_kvalue_accuracy / kderiv6) ** (1. / 6.)
     dlogk = table_spacing * math.sqrt(math.sqrt(gsp_kvalue_accuracy / 10.))
     stride = int((math.log(500.) - (math.log(kmin) - 0.001)) / dlogk) + 4
-    return 3 + 2 * ((stride + 31) // 32)
+    return 3 + 2 * ((stride + 63) // 64)
 
 
 def algorithmic_bytes(N, nx, ny):
@@ -1158,9 +1159,9 @@ def run_gpu(args):
                          'kernel': 'draw_fused_kernel, all FFT-size buckets concurrent (one draw-graph replay)',
                          'kernel_ms': k_ms},
             'roofline_tables': tables_roof,
-            # per step: the Sersic table build, one leaf-prepare launch and one fused draw per
-            # FFT-size bucket
-            'gpu_launches': int(args.steps * (table_build_launches(params[:, 0]) + 1 + nb)),
+            # per step: the Sersic table build, one leaf-prepare launch, the leaf gather into
+            # bucket order, one fused draw per FFT-size bucket and the added-flux scatter
+            'gpu_launches': int(args.steps * (table_build_launches(params[:, 0]) + 3 + nb)),
             'fp32_error_vs_reference': fp32_err,
             'mixed_batch': mixed,
             'large_stamps': large,

@@ -110,6 +110,7 @@ def lib():
             'gsb_add_noise': (i, [i, vp, vp, i, i, vp, i, vp, vp, vp]),
             'gsb_fits_pack': (i, [vp, i, vp, ctypes.c_longlong, vp, ctypes.c_longlong, i, vp,
                                   ctypes.c_longlong, vp]),
+            'gsb_permute_records': (i, [vp, vp, vp, ctypes.c_int64, ctypes.c_int64, i, vp]),
             'gsb_adjoint_grad_count': (i, [ctypes.POINTER(TemplateC)]),
             'gsb_adjoint_workspace_size': (sz, [i, i, i]),
             'gsb_adjoint_images': (i, [ctypes.POINTER(TemplateC), i, ctypes.POINTER(GSParamsC), vp, vp,
@@ -263,6 +264,19 @@ def to_device(arr):
 
 def ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def permute_records(dst, src, perm, scatter=False, stream=None):
+    """gsb_permute_records on device tensors: dst[i] = src[perm[i]] (gather) or
+    dst[perm[i]] = src[i] (scatter), one record per leading-dimension row; perm int64 on the
+    device.  Asynchronous on `stream` (default: the current stream)."""
+    count = int(perm.numel())
+    rec = (src.numel() * src.element_size()) // count if count else 0
+    if rec == 0:
+        return dst
+    check(lib().gsb_permute_records(ptr(dst), ptr(src), ptr(perm), count, rec, 1 if scatter else 0,
+                                    stream if stream is not None else Device.stream()))
+    return dst
 
 
 class Tables(object):

@@ -102,6 +102,25 @@ DeviceState* device_state()
     return &g_state[dev & 63];
 }
 
+// Record reordering for the FFT-size buckets: gather dst[i] = src[perm[i]] (scatter = 0) or
+// scatter dst[perm[i]] = src[i] (scatter = 1), records of `words` 8-byte words, one warp per
+// record (consecutive lanes on consecutive words).  Entries of perm outside [0, count) are
+// skipped: their destination record is left as it was.
+__global__ void permute_records_kernel(unsigned long long* __restrict__ dst,
+                                       const unsigned long long* __restrict__ src,
+                                       const long long* __restrict__ perm, long long count,
+                                       long long words, int scatter)
+{
+    const long long r = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= count) return;
+    const long long p = perm[r];
+    if (p < 0 || p >= count) return;
+    const unsigned long long* s = src + (scatter ? r : p) * words;
+    unsigned long long* d = dst + (scatter ? p : r) * words;
+    for (long long w = lane; w < words; w += 32) d[w] = s[w];
+}
+
 }  // namespace gsb
 
 using namespace gsb;
@@ -330,6 +349,27 @@ int gsb_draw_kimages(const gsb_template* tpl, int n_stamps, const gsb_gsparams* 
     if (!(dk > 0.)) return set_error(GSB_ERR_INVALID, "dk must be > 0");
     return draw_kimages(tpl, n_stamps, d_leaves, d_phases, d_scales, t, dk, kxmin, kymin, nkx, nky,
                         d_out, out_dtype, (cudaStream_t)stream);
+}
+
+int gsb_permute_records(void* d_dst, const void* d_src, const int64_t* d_perm, int64_t count,
+                        int64_t record_bytes, int scatter, void* stream)
+{
+    if (count < 0 || record_bytes <= 0 || record_bytes % 8 || (scatter != 0 && scatter != 1))
+        return set_error(GSB_ERR_INVALID, "bad argument");
+    if (count == 0) return GSB_OK;
+    if (!d_dst || !d_src || !d_perm) return set_error(GSB_ERR_INVALID, "null device pointer");
+    if (d_dst == d_src) return set_error(GSB_ERR_INVALID, "d_dst must not alias d_src");
+    if ((reinterpret_cast<uintptr_t>(d_dst) | reinterpret_cast<uintptr_t>(d_src) |
+         reinterpret_cast<uintptr_t>(d_perm)) & 7)
+        return set_error(GSB_ERR_INVALID, "device pointers must be 8-byte aligned");
+    const long long threads = 256, warps = threads / 32;
+    const long long blocks = (count + warps - 1) / warps;
+    permute_records_kernel<<<(unsigned)blocks, (unsigned)threads, 0, (cudaStream_t)stream>>>(
+        static_cast<unsigned long long*>(d_dst), static_cast<const unsigned long long*>(d_src),
+        reinterpret_cast<const long long*>(d_perm), count, record_bytes / 8, scatter);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(GSB_ERR_CUDA, cudaGetErrorString(e));
+    return GSB_OK;
 }
 
 int gsb_draw_set_variant(int variant) { return draw_set_variant(variant); }

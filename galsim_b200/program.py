@@ -309,7 +309,8 @@ class Program(object):
         stamps['ny'] = ny
         stamps['out_offset'] = offsets
         perm = torch.from_numpy(order).to(dev)
-        lv = self.d_leaves.view(B, L * _lib.LEAF_DTYPE.itemsize).index_select(0, perm).contiguous()
+        lv = torch.empty(B * L * _lib.LEAF_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+        _lib.permute_records(lv, self.d_leaves, perm)
         ph = (_lib.to_device(stack_records(self.bld.phases)[order]) if self.bld.phases else None)
         sc = (_lib.to_device(np.stack(self.bld.scales, axis=1)[order]) if self.bld.scales else None)
         st = _lib.to_device(stamps[order])
@@ -350,7 +351,7 @@ class Program(object):
                 precision, _lib.ptr(work), ctypes.c_size_t(wbytes), ctypes.c_void_p(st.cuda_stream)))
         for st in streams:
             main.wait_stream(st)
-        flux.index_copy_(0, g['perm'], flux_sorted)
+        _lib.permute_records(flux, flux_sorted, g['perm'], scatter=True)
 
     def _workspaces(self, g, precision):
         import torch
@@ -387,8 +388,7 @@ class Program(object):
             if gs is not None and gs['key'] == key:
                 g = gs['geom']
                 # refresh the inputs in place (the records may have changed since)
-                torch.index_select(self.d_leaves.view(B, self.L * _lib.LEAF_DTYPE.itemsize), 0, g['perm'],
-                                   out=g['lv'])
+                _lib.permute_records(g['lv'], self.d_leaves, g['perm'])
                 if g['ph'] is not None:
                     g['ph'].copy_(_lib.to_device(stack_records(self.bld.phases)[g['order']]))
                 if g['sc'] is not None:
@@ -446,7 +446,7 @@ class Program(object):
                 ctypes.c_uint(int(want) & 0xffffffff), precision, _lib.ptr(work),
                 ctypes.c_size_t(int(wbytes)), stream))
         grad = torch.empty_like(grad_sorted)
-        grad[g['perm']] = grad_sorted
+        _lib.permute_records(grad, grad_sorted, g['perm'], scatter=True, stream=stream)
         return grad
 
     def draw_kimage(self, dk, kxmin, kymin, nkx, nky, dtype):

@@ -429,6 +429,17 @@ int gsb_draw_bucket(const gsb_template* tpl, int n_stamps, const gsb_gsparams* g
                     void* d_out, int out_dtype, int add_to_image, double* d_added_flux,
                     int precision, void* d_workspace, size_t workspace_bytes, void* stream);
 
+/* Reorders device records between the caller's stamp order and the FFT-size bucket order that
+ * gsb_draw_bucket draws (stamps sorted by N, each bucket contiguous), replacing the per-object
+ * order of drawFFT calls (gsobject.py:2014-2045) with one launch: scatter = 0 gathers
+ * dst[i] = src[perm[i]] (leaf, phase and scale records into bucket order); scatter = 1 scatters
+ * dst[perm[i]] = src[i] (per-stamp results such as the added flux back to the caller's order).
+ * count records of record_bytes (a multiple of 8) each; d_dst, d_src and d_perm 8-byte aligned,
+ * d_dst not aliasing d_src.  Entries of d_perm outside [0, count) are skipped.  Asynchronous on
+ * `stream`; no allocation, graph-capturable. */
+int gsb_permute_records(void* d_dst, const void* d_src, const int64_t* d_perm, int64_t count,
+                        int64_t record_bytes, int scatter, void* stream);
+
 /* Kernel variant for buckets of FFT size N <= 1024: 0 = automatic (default), 1 = always the
  * fused one-CTA-per-stamp kernel, 2 = the split column/row kernels where N >= 192.  In automatic
  * mode the first draw of each (device, precision, N, floor(log2 stamps)) class with fewer than

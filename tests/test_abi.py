@@ -53,3 +53,21 @@ def test_good_fft_size_host_function():
     ins, outs = gold['good_fft_in'], gold['good_fft_out']
     assert [_lib.good_fft_size(int(v)) for v in ins] == list(outs)
     assert np.array_equal(good_fft_size_array(ins), outs)
+
+
+def test_permute_records_argument_checks():
+    """gsb_permute_records refuses bad sizes, null and unaligned pointers and aliasing before
+    any device work; a zero count is a no-op."""
+    from galsim_b200 import _lib
+    lib = _lib.lib()
+    vp = ctypes.c_void_p
+    GSB_OK, GSB_ERR_INVALID = 0, -1
+    assert lib.gsb_permute_records(None, None, None, 0, 8, 0, None) == GSB_OK
+    assert lib.gsb_permute_records(vp(64), vp(128), vp(256), 4, 12, 0, None) == GSB_ERR_INVALID
+    assert lib.gsb_permute_records(vp(64), vp(128), vp(256), 4, 0, 0, None) == GSB_ERR_INVALID
+    assert lib.gsb_permute_records(vp(64), vp(128), vp(256), -1, 8, 0, None) == GSB_ERR_INVALID
+    assert lib.gsb_permute_records(vp(64), vp(128), vp(256), 4, 8, 2, None) == GSB_ERR_INVALID
+    assert lib.gsb_permute_records(None, vp(128), vp(256), 4, 8, 0, None) == GSB_ERR_INVALID
+    assert lib.gsb_permute_records(vp(64), vp(64), vp(256), 4, 8, 1, None) == GSB_ERR_INVALID
+    assert lib.gsb_permute_records(vp(68), vp(128), vp(256), 4, 8, 0, None) == GSB_ERR_INVALID
+    assert b'aligned' in lib.gsb_last_error()
