@@ -71,7 +71,8 @@ __device__ __forceinline__ void stockham_pass(Cx<T>* buf, const Cx<T>* tw, int l
             for (int r = 0; r < R; ++r) v[t][r] = buf[b + r * NB];
 #pragma unroll
             for (int r = 1; r < R; ++r) {
-                const int idx = (r * k * TSTEP) % N;
+                // r k TSTEP <= (R - 1)(NS - 1) N / (NS R) < N: no reduction mod N needed
+                const int idx = r * k * TSTEP;
                 Cx<T> w = tw[idx];
                 if (SIGN < 0) w.y = -w.y;
                 v[t][r] = cmul<T>(v[t][r], w);
@@ -144,7 +145,8 @@ __device__ void block_fft(Cx<T>* buf, int N, const double2* __restrict__ tw)
                 const int k = b % NS;
                 for (int r = 0; r < R; ++r) v[t][r] = buf[b + r * NB];
                 for (int r = 1; r < R; ++r) {
-                    const double2 w = __ldg(&tw[(long long)(r * k) * tstep % N]);
+                    // r k tstep <= (R - 1)(NS - 1) N / (NS R) < N
+                    const double2 w = __ldg(&tw[r * k * tstep]);
                     v[t][r] = cmul<T>(v[t][r], cx<T>(T(w.x), SIGN > 0 ? T(w.y) : T(-w.y)));
                 }
                 if (R == 4) dft_small<T, 4, SIGN>(v[t]);
