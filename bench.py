@@ -1100,6 +1100,12 @@ def run_gpu(args):
 
     fit = run_fit_step(args, galsim, dev, max(args.steps, 3), max(args.warmup, 2))
     mixed = run_mixed(galsim, dev, max(args.steps, 3), max(args.warmup, 2)) if not args.no_extra else None
+    if not args.no_extra:
+        # the large stamps' multi-GB workspaces are allocated inside their timed run_batch
+        # calls; releasing the earlier stages' cached blocks first makes those allocations
+        # the same as in a process that draws only large stamps
+        torch.cuda.synchronize(dev)
+        torch.cuda.empty_cache()
     large = run_large(galsim, dev) if not args.no_extra else None
     chrom = run_chromatic(galsim, dev, max(args.steps, 3), max(args.warmup, 2)) if not args.no_extra else None
     interp = (run_interp(galsim, dev, params, max(args.steps, 3), max(args.warmup, 2),
