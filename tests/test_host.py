@@ -110,3 +110,22 @@ def test_torch_shear_matrix_matches_shear():
     m = shear_matrix(torch.as_tensor(g1), torch.as_tensor(g2)).numpy()
     ref = galsim.Shear(g1=g1, g2=g2).getMatrix()
     np.testing.assert_allclose(m, ref, rtol=1e-15, atol=1e-15)
+
+
+def test_bench_table_launch_count_follows_the_round_size():
+    """bench.py's gpu_launches claim counts one (nodes, scan) pair per round of kTableRound ln k
+    nodes; the count must follow the round size the table build is compiled with."""
+    import os
+    import re
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = open(os.path.join(root, 'galsim_b200', 'csrc', 'gsb_tables.cu')).read()
+    rnd = int(re.search(r'constexpr int kTableRound = (\d+);', src).group(1))
+    sys.path.insert(0, root)
+    import bench
+    for n in (0.5, 1.5, 4.0, 6.2):
+        kderiv6 = math.exp(math.lgamma(8. * n) - math.lgamma(2. * n)) / 2304.
+        kmin = (1e-5 / kderiv6) ** (1. / 6.)
+        dlogk = math.sqrt(math.sqrt(1e-6))
+        stride = int((math.log(500.) - (math.log(kmin) - 0.001)) / dlogk) + 4
+        assert bench.table_build_launches(np.array([n])) == 3 + 2 * ((stride + rnd - 1) // rnd)
